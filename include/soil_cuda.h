@@ -1,0 +1,239 @@
+/*
+ * soil_cuda.h — C ABI of the B200 (sm_100a) substrate hot path of SOIL.
+ *
+ * The reference (SueHeir/soil, Rust) exposes this path as ECS plugins and
+ * resources, not as an FFI.  Every entry point below replaces one reference
+ * system or resource accessor; the citation beside it names the reference
+ * function (path inside the reference project, file:line) whose behaviour it
+ * reproduces.  A Rust host binds these with `extern "C"`.
+ *
+ * Conventions
+ *   - Every function returns an `int` status (soil_status).  Nothing panics or
+ *     throws across the ABI; `soil_last_error(ctx)` holds a one-line message
+ *     for the last failure on that context.
+ *   - A context is externally synchronised: one host thread at a time.  Each
+ *     system owns one CUDA stream; device work is stream-ordered and the host
+ *     calls that return data synchronise that stream.
+ *   - Host arrays of 3-vectors are interleaved `[n][3]` f64, the reference's
+ *     `Vec<[f64; 3]>` layout (crates/soil_core/src/atom.rs:406-431).  On the
+ *     device every column is structure-of-arrays.
+ *   - Boxes are fully periodic (single rank, periodic self-ghosts); a shear
+ *     drive makes them triclinic (Lees–Edwards, xy tilt only).
+ */
+#ifndef SOIL_CUDA_H
+#define SOIL_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SOIL_ABI_VERSION 1
+
+typedef enum soil_status {
+    SOIL_OK = 0,
+    SOIL_ERR_INVALID = 1,   /* bad argument or call order (reference: panic!/expect) */
+    SOIL_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+    SOIL_ERR_CAPACITY = 3,  /* a size is beyond a fixed limit; state is unchanged */
+    SOIL_ERR_OOM = 4,       /* device allocation failed or the HBM budget is exceeded */
+    SOIL_ERR_STATE = 5,     /* call not valid in the current state */
+    SOIL_ERR_TIMEOUT = 6,   /* a bounded device wait ran out */
+    SOIL_ERR_NOT_FOUND = 7, /* unknown column / job id */
+    SOIL_ERR_NO_DEVICE = 8  /* no CUDA device, or the device is not sm_100 */
+} soil_status;
+
+/* CommState (crates/soil_core/src/lib.rs:86-94). */
+typedef enum soil_comm_state {
+    SOIL_FULL_REBUILD = 0,
+    SOIL_COMMUNICATE_ONLY = 1
+} soil_comm_state;
+
+/* AtomData column classes: #[forward], #[reverse], #[zero]
+ * (crates/soil_derive/src/lib.rs:47-52, 392-500). */
+#define SOIL_COL_FORWARD 1u
+#define SOIL_COL_REVERSE 2u
+#define SOIL_COL_ZERO 4u
+
+/* Pair-filter precision of the neighbor build. */
+#define SOIL_FILTER_FP64 0        /* every candidate tested in FP64 */
+#define SOIL_FILTER_FP32_RECHECK 1 /* FP32 reject test with margin, FP64 recheck of the rest */
+
+/* Box: [lo, hi) per axis, all axes periodic (DomainConfig, domain.rs:43-78). */
+typedef struct soil_box {
+    double lo[3];
+    double hi[3];
+} soil_box;
+
+/* TOML [neighbor] (NeighborConfig, crates/soil_core/src/neighbor.rs:47-80),
+ * plus two fields the reference does not have:
+ *   additive_skin — an absolute pair skin s.  The caller stores
+ *     cutoff_radius = r + s/2, so the pair cutoff (c_i + c_j)*skin_fraction
+ *     equals r_i + r_j + s at skin_fraction = 1; the per-atom displacement
+ *     budget becomes (skin_fraction-1)*min_c + s/2 and the ghost buffer twice
+ *     that.  s = 0 is exactly the reference.
+ *   filter — SOIL_FILTER_FP64 or SOIL_FILTER_FP32_RECHECK (same lists). */
+typedef struct soil_neigh_cfg {
+    double skin_fraction; /* default 1.0 */
+    double bin_size;      /* default 1.0 */
+    uint64_t every;       /* default 0 (displacement-based only) */
+    uint64_t sort_every;  /* default 1000 (0 = disabled) */
+    int32_t check;        /* default 1 */
+    int32_t newton;       /* default 1 (half list + reverse comm) */
+    double additive_skin; /* default 0.0 */
+    int32_t filter;       /* default SOIL_FILTER_FP64 */
+    int32_t reserved;
+} soil_neigh_cfg;
+
+/* Snapshot of a system's counters. */
+typedef struct soil_counts {
+    uint64_t nlocal;
+    uint64_t nghost;
+    uint64_t npairs;             /* neighbor_indices.len() */
+    uint64_t step;               /* completed timesteps */
+    uint64_t rebuilds;           /* neighbor builds so far */
+    uint64_t sorts;              /* spatial sorts that ran (permutation applied or identity) */
+    uint64_t steps_since_build;  /* Neighbor.steps_since_build */
+    uint64_t filter_candidates;  /* pair candidates tested in the last build */
+    uint64_t filter_rechecked;   /* of those, re-tested in FP64 (FP32 mode) */
+    int32_t comm_state;          /* soil_comm_state */
+    int32_t triclinic;
+    int32_t bin_count[3];        /* Neighbor.bin_count */
+    int32_t nstencil_forward;    /* Neighbor.bin_stencil_forward.len() */
+    double ghost_cutoff;         /* Neighbor.ghost_cutoff */
+    double max_cutoff;           /* Neighbor.cached_max_cutoff */
+    double tilt_xy;              /* Domain.tilt[0] */
+} soil_counts;
+
+/* Device pointers handed to a force hook; valid until the next rebuild.
+ * Column c, component k of atom i is columns[c][k * stride + i]. */
+typedef struct soil_dev_view {
+    uint64_t nlocal;
+    uint64_t nghost;
+    uint64_t npairs;
+    uint64_t stride;
+    const double* x;
+    const double* y;
+    const double* z;
+    const double* vx;
+    const double* vy;
+    const double* vz;
+    double* fx;
+    double* fy;
+    double* fz;
+    const double* mass;
+    const double* inv_mass;
+    const double* cutoff_radius;
+    const uint32_t* tag;
+    const uint32_t* neighbor_offsets; /* nlocal + 1 */
+    const uint32_t* neighbor_indices; /* npairs */
+    int32_t ncolumns;
+    int32_t newton;
+    double* const* columns;           /* device array of ncolumns device pointers */
+    void* stream;                     /* cudaStream_t the hook must launch on */
+} soil_dev_view;
+
+/* Force hook (the device analogue of a Force-phase system, and of the
+ * prototype's GpuForce::record, crates/soil_gpu/src/gpu_state.rs:45-55).
+ * Called once per step after ghosts are current and forces are zero; it must
+ * only enqueue work on view->stream.  Return 0 on success. */
+typedef int (*soil_force_fn)(const soil_dev_view* view, void* user);
+
+typedef struct soil_ctx soil_ctx;
+typedef struct soil_sys soil_sys;
+
+/* ---- lifecycle ---------------------------------------------------------- */
+int soil_abi_version(void);
+/* Create a context on CUDA device `device`; hbm_budget_bytes = 0 means no cap. */
+int soil_ctx_create(int device, uint64_t hbm_budget_bytes, soil_ctx** out);
+int soil_ctx_destroy(soil_ctx* ctx);
+const char* soil_last_error(const soil_ctx* ctx);
+/* Device bytes currently held by all systems of the context. */
+int soil_ctx_bytes_in_use(const soil_ctx* ctx, uint64_t* out);
+
+/* ---- systems ------------------------------------------------------------ */
+/* Domain + Atom + Neighbor + CommTopology resources of one simulation
+ * (AtomPlugin atom.rs:609-621, DomainPlugin domain.rs:406-449,
+ *  NeighborPlugin neighbor.rs:516-567, CommunicationPlugin comm.rs:157-202).
+ * dt = Atom.dt. */
+int soil_sys_create(soil_ctx* ctx, const soil_box* box, const soil_neigh_cfg* cfg,
+                    double dt, soil_sys** out);
+int soil_sys_destroy(soil_sys* sys);
+
+/* register_atom_data! (atom.rs:106-118): one f64 column of `width` values
+ * per atom, flags from SOIL_COL_*.  Must precede soil_sys_setup; a duplicate
+ * name returns SOIL_ERR_INVALID (the reference panics). */
+int soil_sys_register_column(soil_sys* sys, const char* name, int32_t width,
+                             uint32_t flags, int32_t* col_out);
+
+/* Append n local atoms (push_test_atom / unpack_atom, atom.rs:561-574,
+ * 539-553).  inv_mass = 1/mass.  columns[c] is n*width_c f64 for column c or
+ * NULL for zeros; `columns` may be NULL.  Only before soil_sys_setup. */
+int soil_sys_add_atoms(soil_sys* sys, uint64_t n, const uint32_t* tag,
+                       const uint32_t* type, const double* pos3,
+                       const double* vel3, const double* mass,
+                       const double* cutoff_radius, const double* const* columns);
+
+/* neighbor_setup (neighbor.rs:604-665) + comm_setup (comm.rs:253-283). */
+int soil_sys_setup(soil_sys* sys);
+
+/* [deform] xy = { style = "erate", rate } — Lees–Edwards shear
+ * (soil_deform/src/lib.rs:346-420 setup, 559-603 per step). */
+int soil_sys_set_shear(soil_sys* sys, double erate);
+
+/* Built-in consumer: linear repulsion f = k*overlap along the pair normal
+ * (docs/src/tutorial/write-your-own-physics.md:56-110) with the radius read
+ * from column `radius_col` (a #[forward] width-1 column).  k = 0 disables. */
+int soil_sys_set_harmonic(soil_sys* sys, double k, int32_t radius_col);
+
+/* Install (fn != NULL) or remove a force hook; replaces the built-in consumer. */
+int soil_sys_set_force_hook(soil_sys* sys, soil_force_fn fn, void* user);
+
+/* Run nsteps full timesteps: every phase below in the reference schedule
+ * order (schedule.rs:22-52).  Returns when the work is enqueued and the
+ * rebuild decisions are taken; call soil_sys_sync to wait. */
+int soil_step(soil_sys* sys, uint64_t nsteps);
+int soil_sys_sync(soil_sys* sys);
+int soil_sys_stream(soil_sys* sys, void** cuda_stream_out);
+
+/* ---- per-phase systems (each applies its reference run condition) ------- */
+int soil_phase_deform(soil_sys* sys);          /* apply_deform       soil_deform/src/lib.rs:435-604 */
+int soil_phase_initial(soil_sys* sys);         /* initial_integration soil_verlet/src/lib.rs:131-162 */
+int soil_phase_decide_rebuild(soil_sys* sys);  /* decide_rebuild     neighbor.rs:796-822 */
+int soil_phase_remove_ghosts(soil_sys* sys);   /* remove_ghost_atoms atom.rs:625-629 */
+int soil_phase_zero_forces(soil_sys* sys);     /* zero_all_forces    atom.rs:631-635 */
+int soil_phase_pbc(soil_sys* sys);             /* pbc / pbc_triclinic domain.rs:611-729 */
+int soil_phase_sort(soil_sys* sys);            /* sort_atoms_by_bin  neighbor.rs:834-997 */
+int soil_phase_borders(soil_sys* sys);         /* borders            comm.rs:682-860 */
+int soil_phase_forward_comm(soil_sys* sys);    /* forward_comm_borders comm.rs:582-592 */
+int soil_phase_neighbor(soil_sys* sys);        /* bin_neighbor_list  neighbor.rs:1013-1319 */
+int soil_phase_force(soil_sys* sys);           /* Force phase: hook or built-in consumer */
+int soil_phase_reverse_comm(soil_sys* sys);    /* reverse_send_force comm.rs:938-1024 */
+int soil_phase_final(soil_sys* sys);           /* final_integration  soil_verlet/src/lib.rs:175-194 */
+
+/* ---- read-back (synchronising) ------------------------------------------ */
+int soil_sys_counts(soil_sys* sys, soil_counts* out);
+/* Atoms [first, first+n) of local+ghost storage; any output may be NULL. */
+int soil_sys_get_atoms(soil_sys* sys, uint64_t first, uint64_t n, uint32_t* tag,
+                       double* pos3, double* vel3, double* force3,
+                       int32_t* image3, int32_t* origin_index);
+int soil_sys_get_column(soil_sys* sys, int32_t col, uint64_t first, uint64_t n,
+                        double* out /* n*width */);
+/* Neighbor.neighbor_offsets (nlocal+1) and neighbor_indices (npairs). */
+int soil_sys_get_neighbor(soil_sys* sys, uint32_t* offsets, uint32_t* indices);
+/* Number of ghost swaps recorded by the last borders (6 on one rank). */
+int soil_sys_num_swaps(soil_sys* sys, int32_t* out);
+/* SwapData (comm.rs:114-124) of swap s; send_indices has recv_count entries. */
+int soil_sys_get_swap(soil_sys* sys, int32_t s, uint64_t* recv_start,
+                      uint64_t* recv_count, double periodic_offset[3],
+                      double vel_offset[3], uint32_t* send_indices);
+/* Permutation applied by the last spatial sort (perm[new] = old), nlocal entries. */
+int soil_sys_get_sort_perm(soil_sys* sys, uint32_t* perm);
+/* Device pointers for an external consumer (valid until the next rebuild). */
+int soil_sys_view(soil_sys* sys, soil_dev_view* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SOIL_CUDA_H */

@@ -1,0 +1,214 @@
+// k_bins.cu — binning and the stable counting sort used by both the spatial
+// sort (sort_atoms_by_bin, neighbor.rs:834-997) and the neighbor build's bin
+// fill (bin_neighbor_list, neighbor.rs:1046-1125).
+//
+// The reference's counting sort is stable: inside a cell atoms keep
+// ascending index.  The device version counts with warp-aggregated atomics
+// (__match_any_sync on the cell id, one atomicAdd per distinct cell per
+// warp), scans, scatters with the same aggregated atomics (order inside a cell
+// is then arbitrary), and restores the stable order by sorting each cell's
+// segment by atom index.  Cells hold ~2 atoms on average, so that last pass
+// is a short insertion sort per cell.
+#include "kernels.cuh"
+
+namespace soil {
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Warp-aggregated increment of counts[key] for the valid lanes.
+__device__ __forceinline__ void aggregated_count(uint32_t* counts, uint32_t key, bool valid) {
+    const uint32_t k = valid ? key : 0xffffffffu;
+    const unsigned peers = __match_any_sync(0xffffffffu, k);
+    const int leader = __ffs(peers) - 1;
+    if (valid && (int)(threadIdx.x & 31) == leader) atomicAdd(&counts[key], (uint32_t)__popc(peers));
+}
+
+__global__ void __launch_bounds__(kBlock) k_cells(uint64_t first, uint64_t n, AtomCols c, Grid gr,
+                                                  uint32_t* cell_out, uint32_t* counts) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
+        const uint64_t i = i0 + threadIdx.x;
+        const bool valid = i < n;
+        uint32_t cell = 0;
+        if (valid) {
+            const uint64_t a = first + i;
+            cell = cell_of(gr, c.x[a], c.y[a], c.z[a]);
+            cell_out[i] = cell;
+        }
+        aggregated_count(counts, cell, valid);
+    }
+}
+
+void launch_cells(cudaStream_t st, uint64_t first, uint64_t n, const AtomCols& c, const Grid& gr,
+                  uint32_t* cell_out, uint32_t* counts) {
+    if (n == 0) return;
+    k_cells<<<grid_for(n), kBlock, 0, st>>>(first, n, c, gr, cell_out, counts);
+}
+
+__global__ void __launch_bounds__(kBlock) k_count_cells(uint64_t n, const uint32_t* cell,
+                                                        uint32_t* counts) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
+        const uint64_t i = i0 + threadIdx.x;
+        const bool valid = i < n;
+        aggregated_count(counts, valid ? cell[i] : 0u, valid);
+    }
+}
+
+void launch_count_cells(cudaStream_t st, uint64_t n, const uint32_t* cell, uint32_t* counts) {
+    if (n == 0) return;
+    k_count_cells<<<grid_for(n), kBlock, 0, st>>>(n, cell, counts);
+}
+
+__global__ void __launch_bounds__(kBlock) k_scatter(uint64_t n, const uint32_t* cell,
+                                                    uint32_t* cursor, uint32_t* out) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
+        const uint64_t i = i0 + threadIdx.x;
+        const bool valid = i < n;
+        const uint32_t key = valid ? cell[i] : 0xffffffffu;
+        const unsigned peers = __match_any_sync(0xffffffffu, key);
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if (valid && lane == leader) base = atomicAdd(&cursor[key], (uint32_t)__popc(peers));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (valid) out[base + __popc(peers & lanemask_lt())] = (uint32_t)i;
+    }
+}
+
+void launch_scatter(cudaStream_t st, uint64_t n, const uint32_t* cell, uint32_t* cursor,
+                    uint32_t* out) {
+    if (n == 0) return;
+    k_scatter<<<grid_for(n), kBlock, 0, st>>>(n, cell, cursor, out);
+}
+
+// Restore the stable (ascending index) order inside every segment.
+__global__ void __launch_bounds__(kBlock) k_segsort(uint64_t nseg, const uint32_t* start,
+                                                    uint32_t* items) {
+    for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < nseg;
+         s += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t b = start[s], e = start[s + 1];
+        if (e - b < 2) continue;
+        for (uint32_t k = b + 1; k < e; ++k) {
+            const uint32_t v = items[k];
+            uint32_t j = k;
+            while (j > b && items[j - 1] > v) {
+                items[j] = items[j - 1];
+                --j;
+            }
+            items[j] = v;
+        }
+    }
+}
+
+void launch_segsort(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint32_t* items) {
+    if (nseg == 0) return;
+    k_segsort<<<grid_for(nseg), kBlock, 0, st>>>(nseg, start, items);
+}
+
+// Atom::apply_permutation + AtomDataRegistry::apply_permutation_all
+// (atom.rs:479-490, 284-289): every column gathered through perm.
+__global__ void __launch_bounds__(kBlock) k_perm_gather(uint64_t n, const uint32_t* perm,
+                                                        AtomCols s, AtomCols d) {
+    const uint64_t cap = s.cap, dcap = d.cap;
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n;
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t p = perm[k];
+        d.x[k] = s.x[p];
+        d.y[k] = s.y[p];
+        d.z[k] = s.z[p];
+        d.vx[k] = s.vx[p];
+        d.vy[k] = s.vy[p];
+        d.vz[k] = s.vz[p];
+        d.fx[k] = s.fx[p];
+        d.fy[k] = s.fy[p];
+        d.fz[k] = s.fz[p];
+        d.mass[k] = s.mass[p];
+        d.inv_mass[k] = s.inv_mass[p];
+        d.cut[k] = s.cut[p];
+        d.tag[k] = s.tag[p];
+        d.type[k] = s.type[p];
+        d.img[k] = s.img[p];
+        d.img[dcap + k] = s.img[cap + p];
+        d.img[2 * dcap + k] = s.img[2 * cap + p];
+        d.origin[k] = s.origin[p];
+        for (int q = 0; q < s.nplanes; ++q) d.planes[q][k] = s.planes[q][p];
+    }
+}
+
+void launch_perm_gather(cudaStream_t st, uint64_t n, const uint32_t* perm, const AtomCols& src,
+                        const AtomCols& dst) {
+    if (n == 0) return;
+    k_perm_gather<<<grid_for(n), kBlock, 0, st>>>(n, perm, src, dst);
+}
+
+__global__ void __launch_bounds__(kBlock) k_identity(uint64_t n, const uint32_t* perm,
+                                                     DevFlags* flags) {
+    bool diff = false;
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n;
+         k += (uint64_t)gridDim.x * blockDim.x)
+        diff |= perm[k] != (uint32_t)k;
+    if (__ballot_sync(0xffffffffu, diff) && (threadIdx.x & 31) == 0)
+        atomicOr(&flags->not_identity, 1u);
+}
+
+void launch_identity_check(cudaStream_t st, uint64_t n, const uint32_t* perm, DevFlags* flags) {
+    if (n == 0) return;
+    k_identity<<<grid_for(n), kBlock, 0, st>>>(n, perm, flags);
+}
+
+__global__ void __launch_bounds__(kBlock) k_permute_u32(uint64_t n, const uint32_t* perm,
+                                                        const uint32_t* in, uint32_t* out) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n;
+         k += (uint64_t)gridDim.x * blockDim.x)
+        out[k] = in[perm[k]];
+}
+
+void launch_permute_u32(cudaStream_t st, uint64_t n, const uint32_t* perm, const uint32_t* in,
+                        uint32_t* out) {
+    if (n == 0) return;
+    k_permute_u32<<<grid_for(n), kBlock, 0, st>>>(n, perm, in, out);
+}
+
+// atom_sorted_idx and sorted_pos of bin_neighbor_list (neighbor.rs:1101-1125),
+// plus the sorted cutoffs and the FP32 grid-relative copies the filter reads.
+__global__ void __launch_bounds__(kBlock) k_sorted_views(uint64_t n, const uint32_t* sorted,
+                                                         AtomCols c, uint32_t* asi, double* spx,
+                                                         double* spy, double* spz, double* scut,
+                                                         float* spx32, float* spy32, float* spz32,
+                                                         float* scut32, double o0, double o1,
+                                                         double o2) {
+    for (uint64_t m = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; m < n;
+         m += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t a = sorted[m];
+        asi[a] = (uint32_t)m;
+        const double x = c.x[a], y = c.y[a], z = c.z[a];
+        spx[m] = x;
+        spy[m] = y;
+        spz[m] = z;
+        if (scut) scut[m] = c.cut[a];
+        if (spx32) {
+            spx32[m] = (float)(x - o0);
+            spy32[m] = (float)(y - o1);
+            spz32[m] = (float)(z - o2);
+            scut32[m] = (float)c.cut[a];
+        }
+    }
+}
+
+void launch_sorted_views(cudaStream_t st, uint64_t n, const uint32_t* sorted, const AtomCols& c,
+                         uint32_t* atom_sorted_idx, double* spx, double* spy, double* spz,
+                         double* scut, float* spx32, float* spy32, float* spz32, float* scut32,
+                         const double origin[3]) {
+    if (n == 0) return;
+    k_sorted_views<<<grid_for(n), kBlock, 0, st>>>(n, sorted, c, atom_sorted_idx, spx, spy, spz,
+                                                   scut, spx32, spy32, spz32, scut32, origin[0],
+                                                   origin[1], origin[2]);
+}
+
+}  // namespace soil

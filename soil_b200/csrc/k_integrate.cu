@@ -1,0 +1,330 @@
+// k_integrate.cu — velocity-Verlet half-steps, force zeroing, periodic wrap,
+// the shear streaming profile and the build-position snapshot.
+//
+// All of these are HBM-bound streams over SoA f64 columns (0.1 flop/byte):
+// one thread per atom, grid-stride, coalesced 8-byte accesses.
+#include "kernels.cuh"
+
+namespace soil {
+
+unsigned grid_for(uint64_t n, int block, int per_sm) {
+    uint64_t need = (n + block - 1) / block;
+    uint64_t cap = 148ull * per_sm;
+    if (need < 1) need = 1;
+    return (unsigned)(need < cap ? need : cap);
+}
+
+// Displacement test of decide_rebuild (displacement_exceeded, fully periodic
+// fast path, neighbor.rs:711-731): nearest image by d - L*round(d/L), FMA sum.
+__device__ __forceinline__ bool moved_too_far(double px, double py, double pz, double qx, double qy,
+                                              double qz, const double box[3], const double ibox[3],
+                                              double thr_sq) {
+    double dx = px - qx, dy = py - qy, dz = pz - qz;
+    dx -= box[0] * round(dx * ibox[0]);
+    dy -= box[1] * round(dy * ibox[1]);
+    dz -= box[2] * round(dz * ibox[2]);
+    return fma(dx, dx, fma(dy, dy, dz * dz)) > thr_sq;
+}
+
+struct CheckArgs {
+    const double* lbx;
+    const double* lby;
+    const double* lbz;
+    uint64_t n_check;
+    double thr_sq;
+    double box[3];
+    double ibox[3];
+    DevFlags* flags;
+};
+
+// initial_integration, soil_verlet/src/lib.rs:131-162:
+//   h = 0.5*dt*inv_m;  v += h*F;  x += v*dt
+template <bool FUSE_FINAL>
+__global__ void __launch_bounds__(kBlock) k_initial(uint64_t n, AtomCols c, double dt,
+                                                    int zero_force, CheckArgs ck) {
+    bool hit = false;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const double h = 0.5 * dt * c.inv_mass[i];
+        const double fx = c.fx[i], fy = c.fy[i], fz = c.fz[i];
+        double vx = c.vx[i], vy = c.vy[i], vz = c.vz[i];
+        if (FUSE_FINAL) {  // final_integration of the previous step, same forces
+            vx = vx + h * fx;
+            vy = vy + h * fy;
+            vz = vz + h * fz;
+        }
+        const double v0 = vx + h * fx;
+        const double v1 = vy + h * fy;
+        const double v2 = vz + h * fz;
+        c.vx[i] = v0;
+        c.vy[i] = v1;
+        c.vz[i] = v2;
+        const double x = c.x[i] + v0 * dt;
+        const double y = c.y[i] + v1 * dt;
+        const double z = c.z[i] + v2 * dt;
+        c.x[i] = x;
+        c.y[i] = y;
+        c.z[i] = z;
+        if (zero_force) {  // zero_all_forces, atom.rs:631-635 (locals part)
+            c.fx[i] = 0.0;
+            c.fy[i] = 0.0;
+            c.fz[i] = 0.0;
+        }
+        if (i < ck.n_check)
+            hit |= moved_too_far(x, y, z, ck.lbx[i], ck.lby[i], ck.lbz[i], ck.box, ck.ibox, ck.thr_sq);
+    }
+    if (ck.flags) {
+        unsigned any = __ballot_sync(0xffffffffu, hit);
+        if (any && (threadIdx.x & 31) == 0) atomicOr(&ck.flags->rebuild, 1u);
+    }
+}
+
+static CheckArgs make_check(const double* lbx, const double* lby, const double* lbz,
+                            uint64_t n_check, double thr_sq, const double box[3],
+                            DevFlags* flags) {
+    CheckArgs ck;
+    ck.lbx = lbx;
+    ck.lby = lby;
+    ck.lbz = lbz;
+    ck.n_check = lbx ? n_check : 0;
+    ck.thr_sq = thr_sq;
+    for (int d = 0; d < 3; ++d) {
+        ck.box[d] = box ? box[d] : 1.0;
+        ck.ibox[d] = 1.0 / ck.box[d];  // ibx = 1.0 / bx (neighbor.rs:716-718)
+    }
+    ck.flags = lbx ? flags : nullptr;
+    return ck;
+}
+
+void launch_initial(cudaStream_t st, uint64_t n, const AtomCols& c, double dt, bool zero_force,
+                    const double* lbx, const double* lby, const double* lbz, uint64_t n_check,
+                    double thr_sq, const double box[3], DevFlags* flags) {
+    if (n == 0) return;
+    CheckArgs ck = make_check(lbx, lby, lbz, n_check, thr_sq, box, flags);
+    k_initial<false><<<grid_for(n), kBlock, 0, st>>>(n, c, dt, zero_force ? 1 : 0, ck);
+}
+
+void launch_final_initial(cudaStream_t st, uint64_t n, const AtomCols& c, double dt,
+                          bool zero_force, const double* lbx, const double* lby,
+                          const double* lbz, uint64_t n_check, double thr_sq,
+                          const double box[3], DevFlags* flags) {
+    if (n == 0) return;
+    CheckArgs ck = make_check(lbx, lby, lbz, n_check, thr_sq, box, flags);
+    k_initial<true><<<grid_for(n), kBlock, 0, st>>>(n, c, dt, zero_force ? 1 : 0, ck);
+}
+
+// final_integration, soil_verlet/src/lib.rs:175-194: v += h*F
+__global__ void __launch_bounds__(kBlock) k_final(uint64_t n, AtomCols c, double dt) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const double h = 0.5 * dt * c.inv_mass[i];
+        c.vx[i] = c.vx[i] + h * c.fx[i];
+        c.vy[i] = c.vy[i] + h * c.fy[i];
+        c.vz[i] = c.vz[i] + h * c.fz[i];
+    }
+}
+
+void launch_final(cudaStream_t st, uint64_t n, const AtomCols& c, double dt) {
+    if (n == 0) return;
+    k_final<<<grid_for(n), kBlock, 0, st>>>(n, c, dt);
+}
+
+struct ZeroPlanes {
+    int idx[kMaxPlanes];
+    int n;
+};
+
+__global__ void __launch_bounds__(kBlock) k_zero(uint64_t n, AtomCols c, ZeroPlanes zp) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        c.fx[i] = 0.0;
+        c.fy[i] = 0.0;
+        c.fz[i] = 0.0;
+        for (int k = 0; k < zp.n; ++k) c.planes[zp.idx[k]][i] = 0.0;
+    }
+}
+
+void launch_zero_forces(cudaStream_t st, uint64_t n, const AtomCols& c, const int* zero_planes,
+                        int nzero) {
+    if (n == 0) return;
+    ZeroPlanes zp;
+    zp.n = nzero;
+    for (int k = 0; k < nzero; ++k) zp.idx[k] = zero_planes[k];
+    k_zero<<<grid_for(n), kBlock, 0, st>>>(n, c, zp);
+}
+
+// wrap_periodic, domain.rs:594-605
+__device__ __forceinline__ double wrap1(double p, double low, double sz, int32_t& img) {
+    const double high = low + sz;
+    if (p < low) {
+        img -= 1;
+        return p + sz;
+    }
+    if (p >= high) {
+        img += 1;
+        return p - sz;
+    }
+    return p;
+}
+
+// pbc fully periodic fast path (domain.rs:626-636) / pbc_triclinic (domain.rs:674-729)
+__global__ void __launch_bounds__(kBlock) k_pbc(uint64_t n, AtomCols c, Geom g, double bv0,
+                                                double bv1, double bv2) {
+    const uint64_t cap = c.cap;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        int32_t i0 = c.img[i], i1 = c.img[cap + i], i2 = c.img[2 * cap + i];
+        if (!g.triclinic) {
+            c.x[i] = wrap1(c.x[i], g.lo[0], g.size[0], i0);
+            c.y[i] = wrap1(c.y[i], g.lo[1], g.size[1], i1);
+            c.z[i] = wrap1(c.z[i], g.lo[2], g.size[2], i2);
+        } else {
+            double l0, l1, l2;
+            x2lamda(g, c.x[i], c.y[i], c.z[i], l0, l1, l2);
+            int32_t d0 = 0, d1 = 0, d2 = 0;
+            if (l0 < 0.0) { l0 += 1.0; d0 = -1; } else if (l0 >= 1.0) { l0 -= 1.0; d0 = 1; }
+            if (l1 < 0.0) { l1 += 1.0; d1 = -1; } else if (l1 >= 1.0) { l1 -= 1.0; d1 = 1; }
+            if (l2 < 0.0) { l2 += 1.0; d2 = -1; } else if (l2 >= 1.0) { l2 -= 1.0; d2 = 1; }
+            double rx, ry, rz;
+            lamda2x(g, l0, l1, l2, rx, ry, rz);
+            c.x[i] = rx;
+            c.y[i] = ry;
+            c.z[i] = rz;
+            i0 += d0;
+            i1 += d1;
+            i2 += d2;
+            if (d1 != 0) {  // Lees–Edwards velocity remap
+                const double s = (double)d1;
+                c.vx[i] = c.vx[i] - s * bv0;
+                c.vy[i] = c.vy[i] - s * bv1;
+                c.vz[i] = c.vz[i] - s * bv2;
+            }
+        }
+        c.img[i] = i0;
+        c.img[cap + i] = i1;
+        c.img[2 * cap + i] = i2;
+    }
+}
+
+void launch_pbc(cudaStream_t st, uint64_t nlocal, const AtomCols& c, const Geom& g,
+                const double bvel[3]) {
+    if (nlocal == 0) return;
+    k_pbc<<<grid_for(nlocal), kBlock, 0, st>>>(nlocal, c, g, bvel[0], bvel[1], bvel[2]);
+}
+
+// soil_deform/src/lib.rs:568-574: vel.x += rate*(y - yc) on the first shear step
+__global__ void __launch_bounds__(kBlock) k_shear_profile(uint64_t n, AtomCols c, double rate,
+                                                          double yc) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        c.vx[i] = c.vx[i] + rate * (c.y[i] - yc);
+}
+
+void launch_shear_profile(cudaStream_t st, uint64_t n, const AtomCols& c, double rate, double yc) {
+    if (n == 0) return;
+    k_shear_profile<<<grid_for(n), kBlock, 0, st>>>(n, c, rate, yc);
+}
+
+__global__ void __launch_bounds__(kBlock) k_save_pos(uint64_t n, AtomCols c, double* lbx,
+                                                     double* lby, double* lbz) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        lbx[i] = c.x[i];
+        lby[i] = c.y[i];
+        lbz[i] = c.z[i];
+    }
+}
+
+void launch_save_positions(cudaStream_t st, uint64_t n, const AtomCols& c, double* lbx,
+                           double* lby, double* lbz) {
+    if (n == 0) return;
+    k_save_pos<<<grid_for(n), kBlock, 0, st>>>(n, c, lbx, lby, lbz);
+}
+
+}  // namespace soil
+
+namespace soil {
+
+// displacement_exceeded as a standalone pass (per-phase API path)
+__global__ void __launch_bounds__(kBlock) k_disp_check(uint64_t n, AtomCols c, CheckArgs ck) {
+    bool hit = false;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        hit |= moved_too_far(c.x[i], c.y[i], c.z[i], ck.lbx[i], ck.lby[i], ck.lbz[i], ck.box,
+                             ck.ibox, ck.thr_sq);
+    if (__ballot_sync(0xffffffffu, hit) && (threadIdx.x & 31) == 0)
+        atomicOr(&ck.flags->rebuild, 1u);
+}
+
+void launch_disp_check(cudaStream_t st, uint64_t n, const AtomCols& c, const double* lbx,
+                       const double* lby, const double* lbz, double thr_sq, const double box[3],
+                       DevFlags* flags) {
+    if (n == 0) return;
+    CheckArgs ck = make_check(lbx, lby, lbz, n, thr_sq, box, flags);
+    k_disp_check<<<grid_for(n), kBlock, 0, st>>>(n, c, ck);
+}
+
+// [n][3] interleaved <-> three SoA planes (host-facing layout of Vec<[f64;3]>)
+__global__ void __launch_bounds__(kBlock) k_deinterleave3(uint64_t n, const double* src, double* a,
+                                                          double* b, double* c) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        a[i] = src[3 * i];
+        b[i] = src[3 * i + 1];
+        c[i] = src[3 * i + 2];
+    }
+}
+__global__ void __launch_bounds__(kBlock) k_interleave3(uint64_t n, double* dst, const double* a,
+                                                        const double* b, const double* c) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        dst[3 * i] = a[i];
+        dst[3 * i + 1] = b[i];
+        dst[3 * i + 2] = c[i];
+    }
+}
+__global__ void __launch_bounds__(kBlock) k_interleave3i(uint64_t n, int32_t* dst, const int32_t* a,
+                                                         const int32_t* b, const int32_t* c) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        dst[3 * i] = a[i];
+        dst[3 * i + 1] = b[i];
+        dst[3 * i + 2] = c[i];
+    }
+}
+// column of width w: [n][w] interleaved <-> w planes of stride cap
+__global__ void __launch_bounds__(kBlock) k_deinterleave_w(uint64_t n, int w, const double* src,
+                                                           double* dst0, uint64_t cap) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        for (int k = 0; k < w; ++k) dst0[k * cap + i] = src[(uint64_t)w * i + k];
+}
+__global__ void __launch_bounds__(kBlock) k_interleave_w(uint64_t n, int w, double* dst,
+                                                         const double* src0, uint64_t cap) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        for (int k = 0; k < w; ++k) dst[(uint64_t)w * i + k] = src0[k * cap + i];
+}
+
+void launch_deinterleave3(cudaStream_t st, uint64_t n, const double* src, double* a, double* b,
+                          double* c) {
+    if (n) k_deinterleave3<<<grid_for(n), kBlock, 0, st>>>(n, src, a, b, c);
+}
+void launch_interleave3(cudaStream_t st, uint64_t n, double* dst, const double* a, const double* b,
+                        const double* c) {
+    if (n) k_interleave3<<<grid_for(n), kBlock, 0, st>>>(n, dst, a, b, c);
+}
+void launch_interleave3i(cudaStream_t st, uint64_t n, int32_t* dst, const int32_t* a,
+                         const int32_t* b, const int32_t* c) {
+    if (n) k_interleave3i<<<grid_for(n), kBlock, 0, st>>>(n, dst, a, b, c);
+}
+void launch_deinterleave_w(cudaStream_t st, uint64_t n, int w, const double* src, double* dst0,
+                           uint64_t cap) {
+    if (n) k_deinterleave_w<<<grid_for(n), kBlock, 0, st>>>(n, w, src, dst0, cap);
+}
+void launch_interleave_w(cudaStream_t st, uint64_t n, int w, double* dst, const double* src0,
+                         uint64_t cap) {
+    if (n) k_interleave_w<<<grid_for(n), kBlock, 0, st>>>(n, w, dst, src0, cap);
+}
+
+}  // namespace soil

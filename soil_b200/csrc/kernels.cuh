@@ -1,0 +1,155 @@
+// kernels.cuh — launch wrappers of the soil_b200 CUDA kernels.
+// Each wrapper enqueues on `st` and returns immediately.
+#pragma once
+
+#include "soil_internal.cuh"
+
+namespace soil {
+
+// Grid for a grid-stride kernel: enough CTAs to fill the 148 SMs several
+// times, never more than the work needs.
+unsigned grid_for(uint64_t n, int block = kBlock, int per_sm = 8);
+
+// ---- integrate (k_integrate.cu) -------------------------------------------
+// initial_integration (+ optional fused force zeroing and displacement check)
+void launch_initial(cudaStream_t st, uint64_t n, const AtomCols& c, double dt, bool zero_force,
+                    const double* lbx, const double* lby, const double* lbz, uint64_t n_check,
+                    double thr_sq, const double box[3], DevFlags* flags);
+// final_integration
+void launch_final(cudaStream_t st, uint64_t n, const AtomCols& c, double dt);
+// final_integration of step t fused with initial_integration of step t+1
+void launch_final_initial(cudaStream_t st, uint64_t n, const AtomCols& c, double dt,
+                          bool zero_force, const double* lbx, const double* lby,
+                          const double* lbz, uint64_t n_check, double thr_sq,
+                          const double box[3], DevFlags* flags);
+// zero_all_forces over [0, n) + the #[zero] planes
+void launch_zero_forces(cudaStream_t st, uint64_t n, const AtomCols& c, const int* zero_planes,
+                        int nzero);
+// pbc (orthogonal) / pbc_triclinic over locals
+void launch_pbc(cudaStream_t st, uint64_t nlocal, const AtomCols& c, const Geom& g,
+                const double bvel[3]);
+// soil_deform first-step streaming profile vx += rate*(y - yc)
+void launch_shear_profile(cudaStream_t st, uint64_t n, const AtomCols& c, double rate, double yc);
+// displacement_exceeded over [0, n) into flags->rebuild
+void launch_disp_check(cudaStream_t st, uint64_t n, const AtomCols& c, const double* lbx,
+                       const double* lby, const double* lbz, double thr_sq, const double box[3],
+                       DevFlags* flags);
+// host-layout conversions ([n][3] or [n][w] interleaved <-> SoA planes)
+void launch_deinterleave3(cudaStream_t st, uint64_t n, const double* src, double* a, double* b,
+                          double* c);
+void launch_interleave3(cudaStream_t st, uint64_t n, double* dst, const double* a, const double* b,
+                        const double* c);
+void launch_interleave3i(cudaStream_t st, uint64_t n, int32_t* dst, const int32_t* a,
+                         const int32_t* b, const int32_t* c);
+void launch_deinterleave_w(cudaStream_t st, uint64_t n, int w, const double* src, double* dst0,
+                           uint64_t cap);
+void launch_interleave_w(cudaStream_t st, uint64_t n, int w, double* dst, const double* src0,
+                         uint64_t cap);
+// copy of x,y,z[0,n) (save_build_positions)
+void launch_save_positions(cudaStream_t st, uint64_t n, const AtomCols& c, double* lbx,
+                           double* lby, double* lbz);
+
+// ---- scan (k_scan.cu) -----------------------------------------------------
+// Exclusive scan: out[0..n] with out[n] = total.  `temp` holds
+// scan_temp_words(n) u32.
+uint64_t scan_temp_words(uint64_t n);
+void exclusive_scan_u32(cudaStream_t st, const uint32_t* in, uint32_t* out, uint64_t n,
+                        uint32_t* temp);
+
+// ---- bins (k_bins.cu) -----------------------------------------------------
+// cell[i] = cell_of(pos[first+i]) and counts[cell]++ for i in [0, n)
+void launch_cells(cudaStream_t st, uint64_t first, uint64_t n, const AtomCols& c, const Grid& gr,
+                  uint32_t* cell_out, uint32_t* counts);
+// counts[cell[i]]++ for i in [0, n) (cells already known)
+void launch_count_cells(cudaStream_t st, uint64_t n, const uint32_t* cell, uint32_t* counts);
+// out[cursor[cell[i]]++] = i (unordered within a cell)
+void launch_scatter(cudaStream_t st, uint64_t n, const uint32_t* cell, uint32_t* cursor,
+                    uint32_t* out);
+// sort every segment [start[s], start[s+1]) ascending -> stable counting sort
+void launch_segsort(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint32_t* items);
+// dst[k] = src[perm[k]] for every column, k in [0, n)
+void launch_perm_gather(cudaStream_t st, uint64_t n, const uint32_t* perm, const AtomCols& src,
+                        const AtomCols& dst);
+// flags->not_identity |= any perm[k] != k
+void launch_identity_check(cudaStream_t st, uint64_t n, const uint32_t* perm, DevFlags* flags);
+// out[k] = cell[perm[k]]
+void launch_permute_u32(cudaStream_t st, uint64_t n, const uint32_t* perm, const uint32_t* in,
+                        uint32_t* out);
+// inverse[sorted[m]] = m, sorted positions / cutoffs by bin order
+void launch_sorted_views(cudaStream_t st, uint64_t n, const uint32_t* sorted, const AtomCols& c,
+                         uint32_t* atom_sorted_idx, double* spx, double* spy, double* spz,
+                         double* scut, float* spx32, float* spy32, float* spz32, float* scut32,
+                         const double origin[3]);
+
+// ---- ghosts (k_ghost.cu) --------------------------------------------------
+struct BorderDim {
+    int dim;
+    int triclinic;
+    Geom geom;
+    double thresh_lo;  // orthogonal: lo_face + gc;   triclinic: lo_face + cut_l
+    double thresh_hi;  // orthogonal: hi_face - gc;   triclinic: hi_face - cut_l
+    double shift[2][3];
+    double vshift[2][3];
+    int swap_id[2];
+};
+constexpr int kBorderTile = 2048;
+void launch_border_count(cudaStream_t st, uint64_t scan_end, const AtomCols& c,
+                         const BorderDim& bd, uint32_t* tile_lo, uint32_t* tile_hi);
+// Appends the lo ghosts at recv_lo + rank and the hi ghosts at recv_hi + rank.
+void launch_border_scatter(cudaStream_t st, uint64_t scan_end, uint64_t nlocal, const AtomCols& c,
+                           const BorderDim& bd, const uint32_t* tile_off_lo,
+                           const uint32_t* tile_off_hi, uint64_t recv_lo, uint64_t recv_hi,
+                           uint32_t* send_lo, uint32_t* send_hi, uint32_t* ghost_root,
+                           uint32_t* ghost_chain);
+// forward_comm: every ghost from its root local atom through its swap chain
+void launch_forward(cudaStream_t st, uint64_t nlocal, uint64_t nghost, const AtomCols& c,
+                    const uint32_t* ghost_root, const uint32_t* ghost_chain, const SwapConst& sc,
+                    const int* fwd_planes, int nfwd, bool zero_force);
+// reverse_accumulate of one swap: F[send[k]] += F[recv_start + k] (+ #[reverse] planes)
+void launch_reverse_swap(cudaStream_t st, uint64_t count, uint64_t recv_start,
+                         const uint32_t* send, const AtomCols& c, const int* rev_planes,
+                         int nrev);
+
+// ---- neighbor (k_neighbor.cu) ---------------------------------------------
+struct PairParams {
+    const uint32_t* atom_cell;
+    const uint32_t* atom_sorted_idx;
+    const uint32_t* bin_start;
+    const uint32_t* sorted_atoms;
+    const double* spx;
+    const double* spy;
+    const double* spz;
+    const double* scut;   // sorted cutoff radii (polydisperse path)
+    const float* spx32;   // FP32 grid-relative sorted positions (FP32 filter)
+    const float* spy32;
+    const float* spz32;
+    const float* scut32;
+    const int32_t* stencil;
+    int nstencil;
+    uint32_t ncells;      // bin_total_cells: stencil cells outside it are skipped and flagged
+    int has_self;
+    int newton;
+    int uniform;
+    int filter;
+    double cut_sq;        // uniform: cached_uniform_cutoff_sq
+    double sf_sq;         // skin_fraction^2
+    double sf;            // skin_fraction
+    float eps32;          // FP32 margin
+    double origin[3];     // grid origin used for the FP32 coordinates
+};
+void launch_pair_count(cudaStream_t st, uint64_t nlocal, const AtomCols& c, const PairParams& p,
+                       uint32_t* rowcount, DevFlags* flags);
+void launch_pair_fill(cudaStream_t st, uint64_t nlocal, const AtomCols& c, const PairParams& p,
+                      const uint32_t* offsets, uint32_t* indices);
+// incoming (transposed) lists: for each atom j, the rows i with j in row(i)
+void launch_in_count(cudaStream_t st, uint64_t nlocal, const uint32_t* offsets,
+                     const uint32_t* indices, uint32_t* incount);
+void launch_in_scatter(cudaStream_t st, uint64_t nlocal, const uint32_t* offsets,
+                       const uint32_t* indices, uint32_t* cursor, uint32_t* in_list);
+
+// ---- force (k_force.cu) ---------------------------------------------------
+void launch_harmonic(cudaStream_t st, uint64_t nlocal, uint64_t ntotal, const AtomCols& c,
+                     const double* radius, double k, int newton, const uint32_t* offsets,
+                     const uint32_t* indices, const uint32_t* in_start, const uint32_t* in_list);
+
+}  // namespace soil

@@ -1,0 +1,1357 @@
+// soil_capi.cu — host side of the soil_b200 library: the C ABI of
+// include/soil_cuda.h, device memory of one system, and the timestep
+// orchestration in the reference schedule order (schedule.rs:22-52):
+//
+//   PreInitialIntegration  apply_deform            soil_phase_deform
+//   InitialIntegration     initial_integration     soil_phase_initial
+//   PostInitialIntegration decide_rebuild, remove_ghost_atoms, zero_all_forces
+//   PreExchange            pbc
+//   PreNeighbor            sort_atoms_by_bin, borders | forward_comm_borders
+//   Neighbor               bin_neighbor_list
+//   Force                  force hook / built-in consumer
+//   PostForce              reverse_send_force
+//   FinalIntegration       final_integration
+//
+// Scalar bookkeeping (CommState, counters, bin grid, stencil, swap ranges)
+// lives on the host exactly as in the reference resources; all per-atom work
+// runs on the device.  The host reads back a few words where the reference
+// branches on data: the displacement flag, the identity flag of a periodic
+// sort, ghost totals and the pair total of a rebuild.
+#include <cfloat>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "kernels.cuh"
+
+using namespace soil;
+
+struct soil_ctx {
+    int device = 0;
+    uint64_t budget = 0;
+    uint64_t in_use = 0;
+    std::string err;
+};
+
+namespace {
+
+enum { FULL_REBUILD = SOIL_FULL_REBUILD, COMMUNICATE_ONLY = SOIL_COMMUNICATE_ONLY };
+
+struct ColMeta {
+    std::string name;
+    int width;
+    unsigned flags;
+    int plane0;
+};
+
+template <class T>
+struct DArr {
+    T* p = nullptr;
+    uint64_t cap = 0;  // elements
+};
+
+struct SwapHost {
+    uint64_t recv_start = 0, recv_count = 0;
+    double off[3] = {0, 0, 0};
+    double voff[3] = {0, 0, 0};
+};
+
+}  // namespace
+
+struct soil_sys {
+    soil_ctx* ctx = nullptr;
+    cudaStream_t st = nullptr;
+    double dt = 1.0;
+
+    // ---- Domain (domain.rs:105-142), one rank ----
+    double blo[3], bhi[3], size[3], sub_lo[3], sub_hi[3], sub_len[3];
+    double sub_lam_lo[3] = {0, 0, 0}, sub_lam_hi[3] = {1, 1, 1};
+    double tilt[3] = {0, 0, 0}, bvel[3] = {0, 0, 0};
+    bool triclinic = false, bounds_changed = false;
+    double domain_ghost_cutoff = 0.0;
+
+    // ---- Neighbor scalars (neighbor.rs:87-174) ----
+    double skin_fraction = 1.0, bin_min_size = 1.0, additive_skin = 0.0;
+    uint64_t every = 0, sort_every = 1000;
+    bool check = true, newton = true;
+    int filter = SOIL_FILTER_FP64;
+    double bin_size[3] = {1, 1, 1}, bin_origin[3] = {0, 0, 0};
+    int32_t bin_count[3] = {1, 1, 1};
+    uint64_t total_cells = 0;
+    std::vector<int32_t> stencil, stencil_fwd;
+    bool stencil_self = false;
+    double pbc_box[3] = {0, 0, 0};
+    double ghost_cutoff = 0.0, cached_min_skin = DBL_MAX, cached_max_cutoff = 0.0;
+    bool has_uniform = false;
+    double uniform_cut_sq = 0.0;
+    uint64_t steps_since_build = 0, sort_counter = 0;
+    bool local_cells_valid = false;
+    uint64_t last_build_n = 0;  // last_build_pos.len()
+    double cut_min_local = DBL_MAX, cut_max_local = -DBL_MAX;
+
+    // ---- Atom counts / CommState ----
+    uint64_t nlocal = 0, nghost = 0, npairs = 0;
+    int state = FULL_REBUILD;
+    SwapHost swaps[kNumSwaps];
+    int nswaps = 0;
+
+    // ---- deform / consumer ----
+    bool shear = false, shear_initialized = false, deform_initialized = false;
+    double shear_rate = 0.0;
+    uint64_t deform_step = 0;
+    double harmonic_k = 0.0;
+    int radius_col = -1;
+    soil_force_fn hook = nullptr;
+    void* hook_user = nullptr;
+    bool in_lists_valid = false;
+
+    // ---- columns ----
+    std::vector<ColMeta> cols;
+    int nplanes = 0;
+
+    // ---- device memory ----
+    uint64_t acap = 0;
+    AtomCols A{}, B{};
+    DArr<double> lbx, lby, lbz;
+    DArr<uint32_t> sort_cell, sort_perm, sorted_local_cell;
+    DArr<uint32_t> cell_counts, cell_start, cell_cursor;
+    DArr<uint32_t> atom_cell, sorted_atoms, asi, rowcount, offsets, indices;
+    DArr<double> spx, spy, spz, scut;
+    DArr<float> spx32, spy32, spz32, scut32;
+    DArr<uint32_t> in_count, in_start, in_cursor, in_list;
+    DArr<uint32_t> ghost_root, ghost_chain;
+    DArr<uint32_t> send[kNumSwaps];
+    DArr<uint32_t> tile_lo, tile_hi, tile_off_lo, tile_off_hi;
+    DArr<uint32_t> scan_tmp;
+    DArr<int32_t> d_stencil;
+    DArr<double> stage;  // host-layout staging for uploads/downloads
+    DArr<double*> d_colptrs;
+    DevFlags* dflags = nullptr;
+    DevFlags* hflags = nullptr;  // pinned mirror
+    uint32_t* hword = nullptr;   // pinned scratch words
+
+    // ---- bookkeeping ----
+    bool setup_done = false, perm_valid = false, pending_final = false;
+    uint64_t steps_done = 0, rebuilds = 0, sorts = 0;
+};
+
+namespace {
+
+int fail(soil_ctx* ctx, int status, const char* fmt, ...) {
+    if (ctx) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        ctx->err = buf;
+    }
+    return status;
+}
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(s->ctx, SOIL_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                                  \
+    } while (0)
+
+#define TRY(call)                        \
+    do {                                 \
+        int r_ = (call);                 \
+        if (r_ != SOIL_OK) return r_;    \
+    } while (0)
+
+int dev_alloc(soil_sys* s, void** p, uint64_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (s->ctx->budget && s->ctx->in_use + bytes > s->ctx->budget)
+        return fail(s->ctx, SOIL_ERR_OOM, "HBM budget exceeded: %llu + %llu > %llu bytes",
+                    (unsigned long long)s->ctx->in_use, (unsigned long long)bytes,
+                    (unsigned long long)s->ctx->budget);
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(s->ctx, SOIL_ERR_OOM, "cudaMalloc(%llu): %s", (unsigned long long)bytes,
+                    cudaGetErrorString(e));
+    }
+    s->ctx->in_use += bytes;
+    return SOIL_OK;
+}
+
+void dev_free(soil_sys* s, void* p, uint64_t bytes) {
+    if (!p) return;
+    cudaFree(p);
+    if (bytes == 0) bytes = 16;
+    s->ctx->in_use -= bytes;
+}
+
+// Grow `a` to hold `need` elements; the first `keep` elements survive.
+template <class T>
+int ensure(soil_sys* s, DArr<T>& a, uint64_t need, uint64_t keep = 0) {
+    if (need <= a.cap && a.p) return SOIL_OK;
+    uint64_t ncap = need + need / 4 + 64;
+    void* np = nullptr;
+    TRY(dev_alloc(s, &np, ncap * sizeof(T)));
+    if (a.p && keep) CK(cudaMemcpyAsync(np, a.p, keep * sizeof(T), cudaMemcpyDeviceToDevice, s->st));
+    if (a.p) {
+        CK(cudaStreamSynchronize(s->st));
+        dev_free(s, a.p, a.cap * sizeof(T));
+    }
+    a.p = (T*)np;
+    a.cap = ncap;
+    return SOIL_OK;
+}
+
+// ---- per-atom columns -------------------------------------------------------
+constexpr int kDoubleCols = 12;  // x y z vx vy vz fx fy fz mass inv_mass cut
+
+double** dcol(AtomCols& c, int k) {
+    double** t[kDoubleCols] = {&c.x, &c.y, &c.z, &c.vx, &c.vy, &c.vz,
+                               &c.fx, &c.fy, &c.fz, &c.mass, &c.inv_mass, &c.cut};
+    return t[k];
+}
+
+void free_cols(soil_sys* s, AtomCols& c) {
+    for (int k = 0; k < kDoubleCols; ++k) {
+        dev_free(s, *dcol(c, k), c.cap * 8);
+        *dcol(c, k) = nullptr;
+    }
+    dev_free(s, c.tag, c.cap * 4);
+    dev_free(s, c.type, c.cap * 4);
+    dev_free(s, c.img, c.cap * 12);
+    dev_free(s, c.origin, c.cap * 4);
+    for (int q = 0; q < c.nplanes; ++q) dev_free(s, c.planes[q], c.cap * 8);
+    c.tag = c.type = nullptr;
+    c.img = c.origin = nullptr;
+}
+
+// Allocate a column set of capacity `cap`, copying [0, keep) from `old`.
+int alloc_cols(soil_sys* s, AtomCols& c, uint64_t cap, const AtomCols* old, uint64_t keep) {
+    AtomCols n{};
+    n.cap = cap;
+    n.nplanes = s->nplanes;
+    for (int k = 0; k < kDoubleCols; ++k) TRY(dev_alloc(s, (void**)dcol(n, k), cap * 8));
+    TRY(dev_alloc(s, (void**)&n.tag, cap * 4));
+    TRY(dev_alloc(s, (void**)&n.type, cap * 4));
+    TRY(dev_alloc(s, (void**)&n.img, cap * 12));
+    TRY(dev_alloc(s, (void**)&n.origin, cap * 4));
+    for (int q = 0; q < s->nplanes; ++q) TRY(dev_alloc(s, (void**)&n.planes[q], cap * 8));
+    if (old && keep) {
+        AtomCols o = *old;
+        for (int k = 0; k < kDoubleCols; ++k)
+            CK(cudaMemcpyAsync(*dcol(n, k), *dcol(o, k), keep * 8, cudaMemcpyDeviceToDevice, s->st));
+        CK(cudaMemcpyAsync(n.tag, o.tag, keep * 4, cudaMemcpyDeviceToDevice, s->st));
+        CK(cudaMemcpyAsync(n.type, o.type, keep * 4, cudaMemcpyDeviceToDevice, s->st));
+        for (int d = 0; d < 3; ++d)
+            CK(cudaMemcpyAsync(n.img + d * cap, o.img + d * o.cap, keep * 4, cudaMemcpyDeviceToDevice,
+                               s->st));
+        CK(cudaMemcpyAsync(n.origin, o.origin, keep * 4, cudaMemcpyDeviceToDevice, s->st));
+        for (int q = 0; q < s->nplanes; ++q)
+            CK(cudaMemcpyAsync(n.planes[q], o.planes[q], keep * 8, cudaMemcpyDeviceToDevice, s->st));
+    }
+    c = n;
+    return SOIL_OK;
+}
+
+int update_colptrs(soil_sys* s) {
+    if (s->cols.empty()) return SOIL_OK;
+    TRY(ensure(s, s->d_colptrs, kMaxCols));
+    double* h[kMaxCols] = {};
+    for (size_t c = 0; c < s->cols.size(); ++c) h[c] = s->A.planes[s->cols[c].plane0];
+    CK(cudaMemcpyAsync(s->d_colptrs.p, h, sizeof(h), cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return SOIL_OK;
+}
+
+// Capacity for `need` atoms (locals + ghosts); the first `keep` survive.
+int grow_atoms(soil_sys* s, uint64_t need, uint64_t keep) {
+    if (need <= s->acap && s->A.x) return SOIL_OK;
+    if (need >= 0x7fffffffull)
+        return fail(s->ctx, SOIL_ERR_CAPACITY, "atom count %llu exceeds the u32 index range",
+                    (unsigned long long)need);
+    uint64_t ncap = need + need / 4 + 1024;
+    AtomCols nA{}, nB{};
+    TRY(alloc_cols(s, nA, ncap, s->A.x ? &s->A : nullptr, keep));
+    TRY(alloc_cols(s, nB, ncap, nullptr, 0));
+    CK(cudaStreamSynchronize(s->st));
+    if (s->A.x) free_cols(s, s->A);
+    if (s->B.x) free_cols(s, s->B);
+    s->A = nA;
+    s->B = nB;
+    s->acap = ncap;
+    // ghost-indexed arrays keep their [0, keep - nlocal) prefix
+    uint64_t gkeep = keep > s->nlocal ? keep - s->nlocal : 0;
+    TRY(ensure(s, s->ghost_root, ncap, gkeep));
+    TRY(ensure(s, s->ghost_chain, ncap, gkeep));
+    TRY(update_colptrs(s));
+    return SOIL_OK;
+}
+
+int sync(soil_sys* s) {
+    CK(cudaStreamSynchronize(s->st));
+    CK(cudaGetLastError());
+    return SOIL_OK;
+}
+
+int check_launch(soil_sys* s) {
+    CK(cudaGetLastError());
+    return SOIL_OK;
+}
+
+Geom geom_of(const soil_sys* s) {
+    Geom g;
+    for (int d = 0; d < 3; ++d) {
+        g.lo[d] = s->blo[d];
+        g.size[d] = s->size[d];
+        g.tilt[d] = s->tilt[d];
+    }
+    g.triclinic = s->triclinic ? 1 : 0;
+    return g;
+}
+
+Grid grid_of(const soil_sys* s) {
+    Grid gr;
+    for (int d = 0; d < 3; ++d) {
+        gr.origin[d] = s->bin_origin[d];
+        gr.inv_bs[d] = 1.0 / s->bin_size[d];
+        gr.n[d] = s->bin_count[d];
+    }
+    gr.geom = geom_of(s);
+    return gr;
+}
+
+// ---- bin grid (host) ----------------------------------------------------------
+// compute_bin_grid, neighbor.rs:311-397 (one rank)
+void compute_bin_grid(soil_sys* s);
+
+void compute_bin_grid_triclinic(soil_sys* s, double max_cutoff, double min_bin) {
+    // neighbor.rs:411-495
+    const double* l = s->size;
+    const double xy = s->tilt[0];
+    double sub_l[3];
+    for (int d = 0; d < 3; ++d) sub_l[d] = s->sub_lam_hi[d] - s->sub_lam_lo[d];
+    int32_t ni[3];
+    for (int d = 0; d < 3; ++d) ni[d] = sat_i32(std::fmax(std::floor(sub_l[d] * l[d] / min_bin), 1.0));
+    double bl[3], real_bin[3];
+    for (int d = 0; d < 3; ++d) bl[d] = sub_l[d] / (double)ni[d];
+    for (int d = 0; d < 3; ++d) real_bin[d] = bl[d] * l[d];
+    const double ghost_cut = s->domain_ghost_cutoff > max_cutoff ? s->domain_ghost_cutoff : max_cutoff;
+    int32_t sr[3];
+    for (int d = 0; d < 3; ++d) sr[d] = sat_i32(std::ceil(max_cutoff / real_bin[d]));
+    const int32_t skew = sat_i32(std::ceil(std::fabs(xy) / real_bin[0]));
+    const int32_t sx = sat_i32(std::ceil(ghost_cut / real_bin[0])) + sr[0] + skew;
+    const int32_t sy = sat_i32(std::ceil(ghost_cut / real_bin[1])) + sr[1];
+    const int32_t sz = sat_i32(std::ceil(ghost_cut / real_bin[2])) + sr[2];
+    const int32_t nx = ni[0] + 2 * sx, ny = ni[1] + 2 * sy, nz = ni[2] + 2 * sz;
+    s->bin_count[0] = nx;
+    s->bin_count[1] = ny;
+    s->bin_count[2] = nz;
+    for (int d = 0; d < 3; ++d) s->bin_size[d] = bl[d];
+    s->total_cells = (uint64_t)(nx * ny * nz);
+    s->bin_origin[0] = s->sub_lam_lo[0] - bl[0] * (double)sx;
+    s->bin_origin[1] = s->sub_lam_lo[1] - bl[1] * (double)sy;
+    s->bin_origin[2] = s->sub_lam_lo[2] - bl[2] * (double)sz;
+    const double cutoff_sq = max_cutoff * max_cutoff;
+    s->stencil.clear();
+    s->stencil_fwd.clear();
+    s->stencil_self = false;
+    for (int32_t dx = -sx; dx <= sx; ++dx)
+        for (int32_t dy = -sy; dy <= sy; ++dy)
+            for (int32_t dz = -sz; dz <= sz; ++dz) {
+                const double m1 = (double)(std::abs(dy) > 0 ? std::abs(dy) - 1 : 0) * bl[1];
+                const double m2 = (double)(std::abs(dz) > 0 ? std::abs(dz) - 1 : 0) * bl[2];
+                const double dyz_sq = (l[1] * m1) * (l[1] * m1) + (l[2] * m2) * (l[2] * m2);
+                if (dyz_sq >= cutoff_sq) continue;
+                const double budget = std::sqrt(cutoff_sq - dyz_sq);
+                const double a_lo = l[0] * ((double)dx - 1.0) * bl[0];
+                const double a_hi = l[0] * ((double)dx + 1.0) * bl[0];
+                const double b1 = xy * ((double)dy - 1.0) * bl[1];
+                const double b2 = xy * ((double)dy + 1.0) * bl[1];
+                const double b_lo = b1 <= b2 ? b1 : b2;
+                const double b_hi = b1 <= b2 ? b2 : b1;
+                const double lo = a_lo + b_lo;
+                const double hi = a_hi + b_hi;
+                if (hi >= -budget && lo <= budget) {
+                    const int32_t off = dx * ny * nz + dy * nz + dz;
+                    s->stencil.push_back(off);
+                    if (off > 0) s->stencil_fwd.push_back(off);
+                    else if (off == 0) s->stencil_self = true;
+                }
+            }
+    for (int d = 0; d < 3; ++d) s->pbc_box[d] = l[d];
+}
+
+void compute_bin_grid(soil_sys* s) {
+    const double max_cutoff = s->cached_max_cutoff;
+    const double min_bin = std::fmax(s->bin_min_size, max_cutoff);
+    if (s->triclinic) {
+        compute_bin_grid_triclinic(s, max_cutoff, min_bin);
+        return;
+    }
+    int32_t ni[3];
+    double abs_[3];
+    for (int d = 0; d < 3; ++d) ni[d] = sat_i32(std::fmax(std::floor(s->sub_len[d] / min_bin), 1.0));
+    for (int d = 0; d < 3; ++d) abs_[d] = s->sub_len[d] / (double)ni[d];
+    const double ghost_cut = s->domain_ghost_cutoff > max_cutoff ? s->domain_ghost_cutoff : max_cutoff;
+    int32_t sv[3];
+    for (int d = 0; d < 3; ++d)
+        sv[d] = sat_i32(std::ceil(ghost_cut / abs_[d])) + sat_i32(std::ceil(max_cutoff / abs_[d]));
+    const int32_t nx = ni[0] + 2 * sv[0], ny = ni[1] + 2 * sv[1], nz = ni[2] + 2 * sv[2];
+    s->bin_count[0] = nx;
+    s->bin_count[1] = ny;
+    s->bin_count[2] = nz;
+    for (int d = 0; d < 3; ++d) s->bin_size[d] = abs_[d];
+    s->total_cells = (uint64_t)(nx * ny * nz);
+    for (int d = 0; d < 3; ++d) s->bin_origin[d] = s->sub_lo[d] - abs_[d] * (double)sv[d];
+    const double cutoff_sq = max_cutoff * max_cutoff;
+    s->stencil.clear();
+    s->stencil_fwd.clear();
+    s->stencil_self = false;
+    for (int32_t dx = -sv[0]; dx <= sv[0]; ++dx)
+        for (int32_t dy = -sv[1]; dy <= sv[1]; ++dy)
+            for (int32_t dz = -sv[2]; dz <= sv[2]; ++dz) {
+                const double mdx = (double)(std::abs(dx) > 0 ? std::abs(dx) - 1 : 0) * abs_[0];
+                const double mdy = (double)(std::abs(dy) > 0 ? std::abs(dy) - 1 : 0) * abs_[1];
+                const double mdz = (double)(std::abs(dz) > 0 ? std::abs(dz) - 1 : 0) * abs_[2];
+                if (mdx * mdx + mdy * mdy + mdz * mdz < cutoff_sq) {
+                    const int32_t off = dx * ny * nz + dy * nz + dz;
+                    s->stencil.push_back(off);
+                    if (off > 0) s->stencil_fwd.push_back(off);
+                    else if (off == 0) s->stencil_self = true;
+                }
+            }
+    for (int d = 0; d < 3; ++d) s->pbc_box[d] = s->bhi[d] - s->blo[d];
+}
+
+double displacement_threshold_sq(const soil_sys* s) {
+    // displacement_exceeded, neighbor.rs:700-702; additive_skin adds s/2 per atom
+    double per_atom_skin = (s->skin_fraction - 1.0) * s->cached_min_skin;
+    if (s->additive_skin != 0.0) per_atom_skin = per_atom_skin + 0.5 * s->additive_skin;
+    return per_atom_skin * per_atom_skin;
+}
+
+void zero_planes_of(const soil_sys* s, unsigned flag, int* out, int* n) {
+    *n = 0;
+    for (const ColMeta& c : s->cols)
+        if (c.flags & flag)
+            for (int w = 0; w < c.width; ++w) out[(*n)++] = c.plane0 + w;
+}
+
+bool builtin_consumer(const soil_sys* s) {
+    return s->hook == nullptr && s->harmonic_k != 0.0 && s->radius_col >= 0;
+}
+
+// ---------------------------------------------------------------------------
+// Phases
+// ---------------------------------------------------------------------------
+int phase_deform(soil_sys* s) {
+    // apply_deform xy branch, soil_deform/src/lib.rs:435-604
+    if (!s->deform_initialized || !s->shear) return SOIL_OK;
+    s->deform_step += 1;
+    const double rate = s->shear_rate;
+    const double lx = s->size[0], ly = s->size[1];
+    const double dv = rate * ly;
+    if (!s->shear_initialized) {
+        const double yc = 0.5 * (s->blo[1] + s->bhi[1]);
+        launch_shear_profile(s->st, s->nlocal, s->A, rate, yc);
+        s->shear_initialized = true;
+    }
+    const double raw = rate * s->dt * (double)s->deform_step * ly;
+    const double xy = raw - lx * std::round(raw / lx);
+    s->tilt[0] = xy;
+    s->bvel[0] = dv;
+    s->triclinic = true;
+    s->bounds_changed = true;
+    s->last_build_n = 0;  // neighbor.last_build_pos.clear()
+    return check_launch(s);
+}
+
+int phase_initial(soil_sys* s) {
+    launch_initial(s->st, s->nlocal, s->A, s->dt, false, nullptr, nullptr, nullptr, 0, 0.0, nullptr,
+                   nullptr);
+    return check_launch(s);
+}
+
+// needs_rebuild (neighbor.rs:762-784) given the displacement answer.
+bool needs_rebuild_with(const soil_sys* s, bool disp) {
+    if (s->last_build_n != s->nlocal || s->nlocal == 0) return true;
+    if (s->state == FULL_REBUILD) return true;
+    if (s->every == 0) return disp;
+    if (s->check) return s->steps_since_build >= s->every || disp;
+    return s->steps_since_build >= s->every;
+}
+
+bool displacement_needed(const soil_sys* s) {
+    if (s->last_build_n != s->nlocal || s->nlocal == 0) return false;
+    if (s->every == 0) return true;
+    if (s->check) return s->steps_since_build < s->every;
+    return false;
+}
+
+int read_flags(soil_sys* s) {
+    CK(cudaMemcpyAsync(s->hflags, s->dflags, sizeof(DevFlags), cudaMemcpyDeviceToHost, s->st));
+    return sync(s);
+}
+
+int phase_decide_rebuild(soil_sys* s) {
+    // decide_rebuild, neighbor.rs:796-822 (run_if CommunicateOnly)
+    if (s->state != COMMUNICATE_ONLY) return SOIL_OK;
+    bool disp = false;
+    if (displacement_needed(s)) {
+        CK(cudaMemsetAsync(&s->dflags->rebuild, 0, 4, s->st));
+        launch_disp_check(s->st, s->nlocal, s->A, s->lbx.p, s->lby.p, s->lbz.p,
+                          displacement_threshold_sq(s), s->pbc_box, s->dflags);
+        TRY(check_launch(s));
+        TRY(read_flags(s));
+        disp = s->hflags->rebuild != 0;
+    }
+    if (needs_rebuild_with(s, disp)) s->state = FULL_REBUILD;
+    else s->steps_since_build += 1;
+    return SOIL_OK;
+}
+
+int phase_remove_ghosts(soil_sys* s) {
+    if (s->state != FULL_REBUILD) return SOIL_OK;
+    s->nghost = 0;
+    return SOIL_OK;
+}
+
+int phase_zero_forces(soil_sys* s) {
+    int zp[kMaxPlanes], nz;
+    zero_planes_of(s, SOIL_COL_ZERO, zp, &nz);
+    launch_zero_forces(s->st, s->nlocal + s->nghost, s->A, zp, nz);
+    return check_launch(s);
+}
+
+int phase_pbc(soil_sys* s) {
+    if (s->state != FULL_REBUILD) return SOIL_OK;
+    launch_pbc(s->st, s->nlocal, s->A, geom_of(s), s->bvel);
+    return check_launch(s);
+}
+
+int phase_sort(soil_sys* s) {
+    // sort_atoms_by_bin, neighbor.rs:834-997
+    if (s->bounds_changed) {
+        if (s->cached_max_cutoff > 0.0) compute_bin_grid(s);  // recompute_bins
+        s->bounds_changed = false;
+        s->state = FULL_REBUILD;
+    }
+    s->sort_counter += 1;
+    const bool periodic_sort = s->sort_every > 0 && s->sort_counter >= s->sort_every;
+    if (periodic_sort) s->sort_counter = 0;
+    const uint64_t nl = s->nlocal;
+    s->local_cells_valid = false;
+    if (nl == 0 || s->total_cells == 0) return SOIL_OK;
+    const bool full_rebuild = s->state == FULL_REBUILD;
+    if (!periodic_sort && !full_rebuild) return SOIL_OK;
+
+    const uint64_t nc = s->total_cells;
+    TRY(ensure(s, s->sort_cell, s->acap));
+    TRY(ensure(s, s->sort_perm, s->acap));
+    TRY(ensure(s, s->sorted_local_cell, s->acap));
+    TRY(ensure(s, s->cell_counts, nc + 1));
+    TRY(ensure(s, s->cell_start, nc + 2));
+    TRY(ensure(s, s->cell_cursor, nc + 1));
+    TRY(ensure(s, s->scan_tmp, scan_temp_words(nc + s->acap + 2)));
+    CK(cudaMemsetAsync(s->cell_counts.p, 0, nc * 4, s->st));
+    launch_cells(s->st, 0, nl, s->A, grid_of(s), s->sort_cell.p, s->cell_counts.p);
+    exclusive_scan_u32(s->st, s->cell_counts.p, s->cell_start.p, nc, s->scan_tmp.p);
+    CK(cudaMemcpyAsync(s->cell_cursor.p, s->cell_start.p, nc * 4, cudaMemcpyDeviceToDevice, s->st));
+    launch_scatter(s->st, nl, s->sort_cell.p, s->cell_cursor.p, s->sort_perm.p);
+    launch_segsort(s->st, nc, s->cell_start.p, s->sort_perm.p);
+    launch_permute_u32(s->st, nl, s->sort_perm.p, s->sort_cell.p, s->sorted_local_cell.p);
+    TRY(check_launch(s));
+    s->local_cells_valid = true;
+    s->perm_valid = true;
+    s->sorts += 1;
+
+    bool apply = true;
+    if (periodic_sort) {
+        CK(cudaMemsetAsync(&s->dflags->not_identity, 0, 4, s->st));
+        launch_identity_check(s->st, nl, s->sort_perm.p, s->dflags);
+        TRY(check_launch(s));
+        TRY(read_flags(s));
+        apply = s->hflags->not_identity != 0;
+    }
+    if (apply) {
+        // every column gathered through perm; ghosts (if any) are discarded by
+        // the borders that always follows a permutation
+        launch_perm_gather(s->st, nl, s->sort_perm.p, s->A, s->B);
+        TRY(check_launch(s));
+        std::swap(s->A, s->B);
+        TRY(update_colptrs(s));
+        // last_build_pos is re-saved by the neighbor build that follows every
+        // permutation, so its permutation is not needed.
+    }
+    if (periodic_sort && apply) {
+        s->last_build_n = 0;
+        s->state = FULL_REBUILD;
+    }
+    return SOIL_OK;
+}
+
+int phase_borders(soil_sys* s) {
+    // borders, comm.rs:682-860 (single rank: all six swaps are self-sends)
+    if (s->state != FULL_REBUILD) return SOIL_OK;
+    s->nghost = 0;
+    uint64_t scan_end = s->nlocal, cur = s->nlocal;
+    const double gc = s->domain_ghost_cutoff;
+    for (int dim = 0; dim < 3; ++dim) {
+        BorderDim bd;
+        bd.dim = dim;
+        bd.triclinic = s->triclinic ? 1 : 0;
+        bd.geom = geom_of(s);
+        if (s->triclinic) {
+            const double inflate = dim == 0 ? 1.0 + std::fabs(s->tilt[0]) / s->size[1] : 1.0;
+            const double cut_l = (gc / s->size[dim]) * inflate;
+            bd.thresh_lo = s->sub_lam_lo[dim] + cut_l;
+            bd.thresh_hi = s->sub_lam_hi[dim] - cut_l;
+        } else {
+            bd.thresh_lo = s->sub_lo[dim] + gc;
+            bd.thresh_hi = s->sub_hi[dim] - gc;
+        }
+        for (int sw = 0; sw < 2; ++sw) {
+            const double po = sw == 0 ? 1.0 : -1.0;  // comm_setup periodic_swap (comm.rs:265-280)
+            double* sh = bd.shift[sw];
+            if (dim == 0) { sh[0] = po * s->size[0]; sh[1] = 0.0; sh[2] = 0.0; }
+            else if (dim == 1) { sh[0] = po * s->tilt[0]; sh[1] = po * s->size[1]; sh[2] = 0.0; }
+            else { sh[0] = po * s->tilt[1]; sh[1] = po * s->tilt[2]; sh[2] = po * s->size[2]; }
+            for (int d = 0; d < 3; ++d) bd.vshift[sw][d] = dim == 1 ? po * s->bvel[d] : 0.0;
+            bd.swap_id[sw] = 2 * dim + sw;
+        }
+        const uint64_t tiles = (scan_end + kBorderTile - 1) / kBorderTile;
+        TRY(ensure(s, s->tile_lo, tiles + 2));
+        TRY(ensure(s, s->tile_hi, tiles + 2));
+        TRY(ensure(s, s->tile_off_lo, tiles + 2));
+        TRY(ensure(s, s->tile_off_hi, tiles + 2));
+        TRY(ensure(s, s->scan_tmp, scan_temp_words(tiles + 2)));
+        uint32_t n_lo = 0, n_hi = 0;
+        if (tiles) {
+            launch_border_count(s->st, scan_end, s->A, bd, s->tile_lo.p, s->tile_hi.p);
+            exclusive_scan_u32(s->st, s->tile_lo.p, s->tile_off_lo.p, tiles, s->scan_tmp.p);
+            exclusive_scan_u32(s->st, s->tile_hi.p, s->tile_off_hi.p, tiles, s->scan_tmp.p);
+            CK(cudaMemcpyAsync(&s->hword[0], s->tile_off_lo.p + tiles, 4, cudaMemcpyDeviceToHost, s->st));
+            CK(cudaMemcpyAsync(&s->hword[1], s->tile_off_hi.p + tiles, 4, cudaMemcpyDeviceToHost, s->st));
+            TRY(sync(s));
+            n_lo = s->hword[0];
+            n_hi = s->hword[1];
+        }
+        TRY(grow_atoms(s, cur + n_lo + n_hi, cur));
+        TRY(ensure(s, s->send[2 * dim], (uint64_t)n_lo + 1));
+        TRY(ensure(s, s->send[2 * dim + 1], (uint64_t)n_hi + 1));
+        const uint64_t recv_lo = cur, recv_hi = cur + n_lo;
+        if (n_lo + n_hi)
+            launch_border_scatter(s->st, scan_end, s->nlocal, s->A, bd, s->tile_off_lo.p,
+                                  s->tile_off_hi.p, recv_lo, recv_hi, s->send[2 * dim].p,
+                                  s->send[2 * dim + 1].p, s->ghost_root.p, s->ghost_chain.p);
+        TRY(check_launch(s));
+        for (int sw = 0; sw < 2; ++sw) {
+            SwapHost& h = s->swaps[2 * dim + sw];
+            h.recv_start = sw == 0 ? recv_lo : recv_hi;
+            h.recv_count = sw == 0 ? n_lo : n_hi;
+            for (int d = 0; d < 3; ++d) {
+                h.off[d] = bd.shift[sw][d];
+                h.voff[d] = bd.vshift[sw][d];
+            }
+        }
+        cur += n_lo + n_hi;
+        s->nghost = cur - s->nlocal;
+        scan_end = cur;
+    }
+    s->nswaps = kNumSwaps;
+    return SOIL_OK;
+}
+
+SwapConst swap_const(const soil_sys* s) {
+    SwapConst sc;
+    for (int k = 0; k < kNumSwaps; ++k)
+        for (int d = 0; d < 3; ++d) {
+            sc.off[k][d] = s->swaps[k].off[d];
+            sc.voff[k][d] = s->swaps[k].voff[d];
+        }
+    return sc;
+}
+
+int forward_comm(soil_sys* s, bool zero_ghost_force) {
+    int fp[kMaxPlanes], nf;
+    zero_planes_of(s, SOIL_COL_FORWARD, fp, &nf);
+    launch_forward(s->st, s->nlocal, s->nghost, s->A, s->ghost_root.p, s->ghost_chain.p,
+                   swap_const(s), fp, nf, zero_ghost_force);
+    return check_launch(s);
+}
+
+int phase_forward_comm(soil_sys* s) {
+    if (s->state != COMMUNICATE_ONLY) return SOIL_OK;
+    return forward_comm(s, false);
+}
+
+int build_in_lists(soil_sys* s) {
+    const uint64_t total = s->nlocal + s->nghost;
+    TRY(ensure(s, s->in_count, total + 1));
+    TRY(ensure(s, s->in_start, total + 2));
+    TRY(ensure(s, s->in_cursor, total + 1));
+    TRY(ensure(s, s->in_list, s->npairs + 1));
+    TRY(ensure(s, s->scan_tmp, scan_temp_words(total + 2)));
+    CK(cudaMemsetAsync(s->in_count.p, 0, total * 4, s->st));
+    launch_in_count(s->st, s->nlocal, s->offsets.p, s->indices.p, s->in_count.p);
+    exclusive_scan_u32(s->st, s->in_count.p, s->in_start.p, total, s->scan_tmp.p);
+    CK(cudaMemcpyAsync(s->in_cursor.p, s->in_start.p, total * 4, cudaMemcpyDeviceToDevice, s->st));
+    launch_in_scatter(s->st, s->nlocal, s->offsets.p, s->indices.p, s->in_cursor.p, s->in_list.p);
+    launch_segsort(s->st, total, s->in_start.p, s->in_list.p);
+    TRY(check_launch(s));
+    s->in_lists_valid = true;
+    return SOIL_OK;
+}
+
+int phase_neighbor(soil_sys* s) {
+    // bin_neighbor_list, neighbor.rs:1013-1319
+    if (s->state != FULL_REBUILD) return SOIL_OK;
+    s->state = COMMUNICATE_ONLY;
+    const uint64_t nl = s->nlocal, total = s->nlocal + s->nghost;
+    // save_build_positions (neighbor.rs:669-690); the local cutoff radii never
+    // change after setup, so their min/max are cached there.
+    TRY(ensure(s, s->lbx, s->acap));
+    TRY(ensure(s, s->lby, s->acap));
+    TRY(ensure(s, s->lbz, s->acap));
+    launch_save_positions(s->st, nl, s->A, s->lbx.p, s->lby.p, s->lbz.p);
+    s->last_build_n = nl;
+    s->steps_since_build = 0;
+    s->cached_min_skin = s->cut_min_local;
+    if (std::fabs(s->cut_max_local - s->cut_min_local) < 1e-15) {
+        const double cutoff = 2.0 * s->cut_min_local * s->skin_fraction;
+        s->has_uniform = true;
+        s->uniform_cut_sq = cutoff * cutoff;
+    } else {
+        s->has_uniform = false;
+    }
+    const uint64_t nc = s->total_cells;
+    TRY(ensure(s, s->atom_cell, s->acap));
+    TRY(ensure(s, s->sorted_atoms, s->acap));
+    TRY(ensure(s, s->asi, s->acap));
+    TRY(ensure(s, s->rowcount, s->acap));
+    TRY(ensure(s, s->offsets, s->acap + 2));
+    TRY(ensure(s, s->spx, s->acap));
+    TRY(ensure(s, s->spy, s->acap));
+    TRY(ensure(s, s->spz, s->acap));
+    const bool fp32 = s->filter == SOIL_FILTER_FP32_RECHECK;
+    if (!s->has_uniform) TRY(ensure(s, s->scut, s->acap));
+    if (fp32) {
+        TRY(ensure(s, s->spx32, s->acap));
+        TRY(ensure(s, s->spy32, s->acap));
+        TRY(ensure(s, s->spz32, s->acap));
+        TRY(ensure(s, s->scut32, s->acap));
+    }
+    TRY(ensure(s, s->cell_counts, nc + 1));
+    TRY(ensure(s, s->cell_start, nc + 2));
+    TRY(ensure(s, s->cell_cursor, nc + 1));
+    TRY(ensure(s, s->scan_tmp, scan_temp_words(nc + s->acap + 2)));
+    CK(cudaMemsetAsync(s->cell_counts.p, 0, nc * 4, s->st));
+    const Grid gr = grid_of(s);
+    if (s->local_cells_valid) {  // reuse the sort's local cells (neighbor.rs:1049-1066)
+        CK(cudaMemcpyAsync(s->atom_cell.p, s->sorted_local_cell.p, nl * 4, cudaMemcpyDeviceToDevice,
+                           s->st));
+        launch_count_cells(s->st, nl, s->atom_cell.p, s->cell_counts.p);
+        launch_cells(s->st, nl, total - nl, s->A, gr, s->atom_cell.p + nl, s->cell_counts.p);
+    } else {
+        launch_cells(s->st, 0, total, s->A, gr, s->atom_cell.p, s->cell_counts.p);
+    }
+    s->local_cells_valid = false;
+    exclusive_scan_u32(s->st, s->cell_counts.p, s->cell_start.p, nc, s->scan_tmp.p);
+    CK(cudaMemcpyAsync(s->cell_cursor.p, s->cell_start.p, nc * 4, cudaMemcpyDeviceToDevice, s->st));
+    launch_scatter(s->st, total, s->atom_cell.p, s->cell_cursor.p, s->sorted_atoms.p);
+    launch_segsort(s->st, nc, s->cell_start.p, s->sorted_atoms.p);
+    // FP32 coordinates are relative to the box corner; M bounds their magnitude
+    double M = 0.0;
+    for (int d = 0; d < 3; ++d) M = std::fmax(M, s->size[d]);
+    M += 2.0 * s->domain_ghost_cutoff + std::fabs(s->tilt[0]) + 4.0 * s->cached_max_cutoff;
+    launch_sorted_views(s->st, total, s->sorted_atoms.p, s->A, s->asi.p, s->spx.p, s->spy.p,
+                        s->spz.p, s->has_uniform ? nullptr : s->scut.p, fp32 ? s->spx32.p : nullptr,
+                        fp32 ? s->spy32.p : nullptr, fp32 ? s->spz32.p : nullptr,
+                        fp32 ? s->scut32.p : nullptr, s->blo);
+    const std::vector<int32_t>& sten = s->newton ? s->stencil_fwd : s->stencil;
+    TRY(ensure(s, s->d_stencil, sten.size() + 1));
+    if (!sten.empty())
+        CK(cudaMemcpyAsync(s->d_stencil.p, sten.data(), sten.size() * 4, cudaMemcpyHostToDevice, s->st));
+    PairParams p;
+    p.atom_cell = s->atom_cell.p;
+    p.atom_sorted_idx = s->asi.p;
+    p.bin_start = s->cell_start.p;
+    p.sorted_atoms = s->sorted_atoms.p;
+    p.spx = s->spx.p;
+    p.spy = s->spy.p;
+    p.spz = s->spz.p;
+    p.scut = s->scut.p;
+    p.spx32 = s->spx32.p;
+    p.spy32 = s->spy32.p;
+    p.spz32 = s->spz32.p;
+    p.scut32 = s->scut32.p;
+    p.stencil = s->d_stencil.p;
+    p.nstencil = (int)sten.size();
+    p.ncells = (uint32_t)nc;
+    p.has_self = s->stencil_self ? 1 : 0;
+    p.newton = s->newton ? 1 : 0;
+    p.uniform = s->has_uniform ? 1 : 0;
+    p.filter = s->filter;
+    p.cut_sq = s->uniform_cut_sq;
+    p.sf_sq = s->skin_fraction * s->skin_fraction;
+    p.sf = s->skin_fraction;
+    p.eps32 = (float)(1e-6 * (1.0 + s->cached_max_cutoff) + 4e-7 * M);
+    for (int d = 0; d < 3; ++d) p.origin[d] = s->blo[d];
+    CK(cudaMemsetAsync(&s->dflags->candidates, 0, 16, s->st));
+    CK(cudaMemsetAsync(&s->dflags->error, 0, 4, s->st));
+    launch_pair_count(s->st, nl, s->A, p, s->rowcount.p, s->dflags);
+    exclusive_scan_u32(s->st, s->rowcount.p, s->offsets.p, nl, s->scan_tmp.p);
+    CK(cudaMemcpyAsync(&s->hword[0], s->offsets.p + nl, 4, cudaMemcpyDeviceToHost, s->st));
+    TRY(check_launch(s));
+    TRY(read_flags(s));
+    const uint64_t np = s->hword[0];
+    TRY(ensure(s, s->indices, np + 1));
+    if (s->hflags->error)
+        return fail(s->ctx, SOIL_ERR_INVALID, "neighbor stencil left the bin grid (atom outside the ghost layers)");
+    launch_pair_fill(s->st, nl, s->A, p, s->offsets.p, s->indices.p);
+    TRY(check_launch(s));
+    s->npairs = np;
+    s->rebuilds += 1;
+    s->in_lists_valid = false;
+    if (builtin_consumer(s)) TRY(build_in_lists(s));
+    return SOIL_OK;
+}
+
+int make_view(soil_sys* s, soil_dev_view* v) {
+    std::memset(v, 0, sizeof(*v));
+    v->nlocal = s->nlocal;
+    v->nghost = s->nghost;
+    v->npairs = s->npairs;
+    v->stride = s->acap;
+    v->x = s->A.x; v->y = s->A.y; v->z = s->A.z;
+    v->vx = s->A.vx; v->vy = s->A.vy; v->vz = s->A.vz;
+    v->fx = s->A.fx; v->fy = s->A.fy; v->fz = s->A.fz;
+    v->mass = s->A.mass;
+    v->inv_mass = s->A.inv_mass;
+    v->cutoff_radius = s->A.cut;
+    v->tag = s->A.tag;
+    v->neighbor_offsets = s->offsets.p;
+    v->neighbor_indices = s->indices.p;
+    v->ncolumns = (int32_t)s->cols.size();
+    v->newton = s->newton ? 1 : 0;
+    v->columns = s->d_colptrs.p;
+    v->stream = (void*)s->st;
+    return SOIL_OK;
+}
+
+int phase_force(soil_sys* s) {
+    if (s->hook) {
+        soil_dev_view v;
+        make_view(s, &v);
+        int r = s->hook(&v, s->hook_user);
+        if (r != 0) return fail(s->ctx, SOIL_ERR_INVALID, "force hook returned %d", r);
+        return check_launch(s);
+    }
+    if (!builtin_consumer(s)) return SOIL_OK;
+    if (!s->in_lists_valid) TRY(build_in_lists(s));
+    launch_harmonic(s->st, s->nlocal, s->nlocal + s->nghost, s->A,
+                    s->A.planes[s->cols[s->radius_col].plane0], s->harmonic_k, s->newton ? 1 : 0,
+                    s->offsets.p, s->indices.p, s->in_start.p, s->in_list.p);
+    return check_launch(s);
+}
+
+int phase_reverse_comm(soil_sys* s) {
+    // reverse_send_force, comm.rs:938-1024: rounds last to first, lo then hi
+    if (!s->newton) return SOIL_OK;
+    int rp[kMaxPlanes], nr;
+    zero_planes_of(s, SOIL_COL_REVERSE, rp, &nr);
+    for (int end = s->nswaps; end > 0; end -= 2) {
+        const int start = end >= 2 ? end - 2 : 0;
+        for (int k = start; k < end; ++k)
+            launch_reverse_swap(s->st, s->swaps[k].recv_count, s->swaps[k].recv_start, s->send[k].p,
+                                s->A, rp, nr);
+    }
+    return check_launch(s);
+}
+
+int phase_final(soil_sys* s) {
+    launch_final(s->st, s->nlocal, s->A, s->dt);
+    s->steps_done += 1;
+    return check_launch(s);
+}
+
+// One full timestep.  Fusions that keep every result bit-identical:
+//  - force zeroing folded into initial (locals) and forward comm (ghosts),
+//    or dropped when the built-in consumer overwrites every force;
+//  - the displacement check folded into the initial integration pass;
+//  - final(t) folded into initial(t+1) when nothing touches velocities
+//    between them (the streaming profile of the first shear step does).
+int full_step(soil_sys* s, bool last) {
+    const bool profile_now = s->deform_initialized && s->shear && !s->shear_initialized;
+    if (profile_now && s->pending_final) {
+        launch_final(s->st, s->nlocal, s->A, s->dt);
+        s->pending_final = false;
+    }
+    TRY(phase_deform(s));
+    const bool overwrite = builtin_consumer(s);
+    int zp[kMaxPlanes], nz;
+    zero_planes_of(s, SOIL_COL_ZERO, zp, &nz);
+    const bool fused_zero = !overwrite && nz == 0;
+    const bool check = s->state == COMMUNICATE_ONLY && displacement_needed(s);
+    if (check) CK(cudaMemsetAsync(&s->dflags->rebuild, 0, 4, s->st));
+    if (s->pending_final)
+        launch_final_initial(s->st, s->nlocal, s->A, s->dt, fused_zero,
+                             check ? s->lbx.p : nullptr, s->lby.p, s->lbz.p, s->nlocal,
+                             displacement_threshold_sq(s), s->pbc_box, s->dflags);
+    else
+        launch_initial(s->st, s->nlocal, s->A, s->dt, fused_zero, check ? s->lbx.p : nullptr,
+                       s->lby.p, s->lbz.p, s->nlocal, displacement_threshold_sq(s), s->pbc_box,
+                       s->dflags);
+    s->pending_final = false;
+    TRY(check_launch(s));
+    // decide_rebuild
+    if (s->state == COMMUNICATE_ONLY) {
+        bool disp = false;
+        if (check) {
+            TRY(read_flags(s));
+            disp = s->hflags->rebuild != 0;
+        }
+        if (needs_rebuild_with(s, disp)) s->state = FULL_REBUILD;
+        else s->steps_since_build += 1;
+    }
+    TRY(phase_remove_ghosts(s));
+    if (!fused_zero && (nz > 0 || !overwrite)) TRY(phase_zero_forces(s));
+    TRY(phase_pbc(s));
+    TRY(phase_sort(s));
+    TRY(phase_borders(s));
+    if (s->state == COMMUNICATE_ONLY) TRY(forward_comm(s, fused_zero));
+    TRY(phase_neighbor(s));
+    TRY(phase_force(s));
+    TRY(phase_reverse_comm(s));
+    if (last) {
+        TRY(phase_final(s));
+    } else {
+        s->pending_final = true;
+        s->steps_done += 1;
+    }
+    return SOIL_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int soil_abi_version(void) { return SOIL_ABI_VERSION; }
+
+int soil_ctx_create(int device, uint64_t hbm_budget_bytes, soil_ctx** out) {
+    if (!out) return SOIL_ERR_INVALID;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= device || device < 0) {
+        cudaGetLastError();
+        return SOIL_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) {
+        cudaGetLastError();
+        return SOIL_ERR_NO_DEVICE;
+    }
+    soil_ctx* c = new (std::nothrow) soil_ctx();
+    if (!c) return SOIL_ERR_OOM;
+    c->device = device;
+    c->budget = hbm_budget_bytes;
+    *out = c;
+    return SOIL_OK;
+}
+
+int soil_ctx_destroy(soil_ctx* ctx) {
+    delete ctx;
+    return SOIL_OK;
+}
+
+const char* soil_last_error(const soil_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int soil_ctx_bytes_in_use(const soil_ctx* ctx, uint64_t* out) {
+    if (!ctx || !out) return SOIL_ERR_INVALID;
+    *out = ctx->in_use;
+    return SOIL_OK;
+}
+
+int soil_sys_create(soil_ctx* ctx, const soil_box* box, const soil_neigh_cfg* cfg, double dt,
+                    soil_sys** out) {
+    if (!ctx || !box || !cfg || !out) return SOIL_ERR_INVALID;
+    *out = nullptr;
+    for (int d = 0; d < 3; ++d)
+        if (!(box->hi[d] > box->lo[d]))
+            return fail(ctx, SOIL_ERR_INVALID, "box axis %d has hi <= lo", d);
+    if (!(cfg->skin_fraction >= 1.0) || !(cfg->bin_size > 0.0) || cfg->additive_skin < 0.0 ||
+        (cfg->filter != SOIL_FILTER_FP64 && cfg->filter != SOIL_FILTER_FP32_RECHECK))
+        return fail(ctx, SOIL_ERR_INVALID, "invalid neighbor config");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, SOIL_ERR_NO_DEVICE, "cudaSetDevice(%d) failed", ctx->device);
+    }
+    soil_sys* s = new (std::nothrow) soil_sys();
+    if (!s) return SOIL_ERR_OOM;
+    s->ctx = ctx;
+    if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete s;
+        return fail(ctx, SOIL_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    // decompose_domain on a 1x1x1 grid (domain.rs:235-296)
+    for (int d = 0; d < 3; ++d) {
+        s->blo[d] = box->lo[d];
+        s->bhi[d] = box->hi[d];
+        s->size[d] = box->hi[d] - box->lo[d];
+        const double delta = s->size[d] / 1.0;
+        s->sub_lo[d] = box->lo[d] + delta * 0.0;
+        s->sub_hi[d] = box->lo[d] + delta * 1.0;
+        s->sub_len[d] = delta;
+    }
+    s->dt = dt;
+    s->skin_fraction = cfg->skin_fraction;
+    s->bin_min_size = cfg->bin_size;
+    s->every = cfg->every;
+    s->sort_every = cfg->sort_every;
+    s->check = cfg->check != 0;
+    s->newton = cfg->newton != 0;
+    s->additive_skin = cfg->additive_skin;
+    s->filter = cfg->filter;
+    int r;
+    if ((r = dev_alloc(s, (void**)&s->dflags, sizeof(DevFlags))) != SOIL_OK ||
+        cudaMallocHost((void**)&s->hflags, sizeof(DevFlags)) != cudaSuccess ||
+        cudaMallocHost((void**)&s->hword, 64) != cudaSuccess) {
+        cudaGetLastError();
+        soil_sys_destroy(s);
+        return r != SOIL_OK ? r : fail(ctx, SOIL_ERR_OOM, "pinned allocation failed");
+    }
+    cudaMemsetAsync(s->dflags, 0, sizeof(DevFlags), s->st);
+    *out = s;
+    return SOIL_OK;
+}
+
+int soil_sys_destroy(soil_sys* s) {
+    if (!s) return SOIL_OK;
+    if (s->st) cudaStreamSynchronize(s->st);
+    if (s->A.x) free_cols(s, s->A);
+    if (s->B.x) free_cols(s, s->B);
+    auto fr = [&](auto& a) {
+        dev_free(s, a.p, a.cap * sizeof(*a.p));
+        a.p = nullptr;
+        a.cap = 0;
+    };
+    fr(s->lbx); fr(s->lby); fr(s->lbz);
+    fr(s->sort_cell); fr(s->sort_perm); fr(s->sorted_local_cell);
+    fr(s->cell_counts); fr(s->cell_start); fr(s->cell_cursor);
+    fr(s->atom_cell); fr(s->sorted_atoms); fr(s->asi); fr(s->rowcount); fr(s->offsets); fr(s->indices);
+    fr(s->spx); fr(s->spy); fr(s->spz); fr(s->scut);
+    fr(s->spx32); fr(s->spy32); fr(s->spz32); fr(s->scut32);
+    fr(s->in_count); fr(s->in_start); fr(s->in_cursor); fr(s->in_list);
+    fr(s->ghost_root); fr(s->ghost_chain);
+    for (auto& a : s->send) fr(a);
+    fr(s->tile_lo); fr(s->tile_hi); fr(s->tile_off_lo); fr(s->tile_off_hi);
+    fr(s->scan_tmp); fr(s->d_stencil); fr(s->stage); fr(s->d_colptrs);
+    if (s->dflags) dev_free(s, s->dflags, sizeof(DevFlags));
+    if (s->hflags) cudaFreeHost(s->hflags);
+    if (s->hword) cudaFreeHost(s->hword);
+    if (s->st) cudaStreamDestroy(s->st);
+    delete s;
+    return SOIL_OK;
+}
+
+int soil_sys_register_column(soil_sys* s, const char* name, int32_t width, uint32_t flags,
+                             int32_t* col_out) {
+    if (!s || !name || width <= 0) return SOIL_ERR_INVALID;
+    if (s->setup_done || s->nlocal > 0)
+        return fail(s->ctx, SOIL_ERR_STATE, "columns must be registered before atoms are added");
+    for (const ColMeta& c : s->cols)
+        if (c.name == name)
+            return fail(s->ctx, SOIL_ERR_INVALID, "AtomData column '%s' already registered", name);
+    if ((int)s->cols.size() >= kMaxCols || s->nplanes + width > kMaxPlanes)
+        return fail(s->ctx, SOIL_ERR_CAPACITY, "at most %d columns / %d f64 planes", kMaxCols,
+                    kMaxPlanes);
+    s->cols.push_back({name, (int)width, flags, s->nplanes});
+    s->nplanes += width;
+    if (col_out) *col_out = (int32_t)s->cols.size() - 1;
+    return SOIL_OK;
+}
+
+int soil_sys_add_atoms(soil_sys* s, uint64_t n, const uint32_t* tag, const uint32_t* type,
+                       const double* pos3, const double* vel3, const double* mass,
+                       const double* cutoff_radius, const double* const* columns) {
+    if (!s || (n && (!tag || !pos3 || !vel3 || !mass || !cutoff_radius))) return SOIL_ERR_INVALID;
+    if (s->setup_done) return fail(s->ctx, SOIL_ERR_STATE, "atoms must be added before setup");
+    for (uint64_t i = 0; i < n; ++i)
+        if (!(mass[i] > 0.0) || !(cutoff_radius[i] >= 0.0))
+            return fail(s->ctx, SOIL_ERR_INVALID, "atom %llu: mass must be > 0 and cutoff >= 0",
+                        (unsigned long long)i);
+    const uint64_t base = s->nlocal;
+    TRY(grow_atoms(s, base + n, base));
+    if (n == 0) return SOIL_OK;
+    TRY(ensure(s, s->stage, 3 * n));
+    double* st3 = s->stage.p;
+    CK(cudaMemcpyAsync(st3, pos3, n * 24, cudaMemcpyHostToDevice, s->st));
+    launch_deinterleave3(s->st, n, st3, s->A.x + base, s->A.y + base, s->A.z + base);
+    CK(cudaStreamSynchronize(s->st));
+    CK(cudaMemcpyAsync(st3, vel3, n * 24, cudaMemcpyHostToDevice, s->st));
+    launch_deinterleave3(s->st, n, st3, s->A.vx + base, s->A.vy + base, s->A.vz + base);
+    CK(cudaMemsetAsync(s->A.fx + base, 0, n * 8, s->st));
+    CK(cudaMemsetAsync(s->A.fy + base, 0, n * 8, s->st));
+    CK(cudaMemsetAsync(s->A.fz + base, 0, n * 8, s->st));
+    CK(cudaMemcpyAsync(s->A.mass + base, mass, n * 8, cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemcpyAsync(s->A.cut + base, cutoff_radius, n * 8, cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemcpyAsync(s->A.tag + base, tag, n * 4, cudaMemcpyHostToDevice, s->st));
+    if (type) CK(cudaMemcpyAsync(s->A.type + base, type, n * 4, cudaMemcpyHostToDevice, s->st));
+    else CK(cudaMemsetAsync(s->A.type + base, 0, n * 4, s->st));
+    for (int d = 0; d < 3; ++d) CK(cudaMemsetAsync(s->A.img + d * s->acap + base, 0, n * 4, s->st));
+    CK(cudaMemsetAsync(s->A.origin + base, 0, n * 4, s->st));
+    std::vector<double> inv(n);
+    for (uint64_t i = 0; i < n; ++i) inv[i] = 1.0 / mass[i];
+    CK(cudaMemcpyAsync(s->A.inv_mass + base, inv.data(), n * 8, cudaMemcpyHostToDevice, s->st));
+    for (size_t c = 0; c < s->cols.size(); ++c) {
+        const ColMeta& m = s->cols[c];
+        if (columns && columns[c]) {
+            TRY(ensure(s, s->stage, (uint64_t)m.width * n));
+            CK(cudaMemcpyAsync(s->stage.p, columns[c], (uint64_t)m.width * n * 8,
+                               cudaMemcpyHostToDevice, s->st));
+            launch_deinterleave_w(s->st, n, m.width, s->stage.p, s->A.planes[m.plane0] + base, s->acap);
+            CK(cudaStreamSynchronize(s->st));
+        } else {
+            for (int w = 0; w < m.width; ++w)
+                CK(cudaMemsetAsync(s->A.planes[m.plane0 + w] + base, 0, n * 8, s->st));
+        }
+    }
+    TRY(check_launch(s));
+    TRY(sync(s));
+    for (uint64_t i = 0; i < n; ++i) {
+        s->cut_min_local = std::fmin(s->cut_min_local, cutoff_radius[i]);
+        s->cut_max_local = std::fmax(s->cut_max_local, cutoff_radius[i]);
+    }
+    s->nlocal += n;
+    return SOIL_OK;
+}
+
+int soil_sys_setup(soil_sys* s) {
+    if (!s) return SOIL_ERR_INVALID;
+    if (s->setup_done) return fail(s->ctx, SOIL_ERR_STATE, "setup already done");
+    TRY(grow_atoms(s, s->nlocal + 1, s->nlocal));
+    // comm_setup (comm.rs:253-283): rank 0 of 1x1x1, every axis periodic; the
+    // shifts are applied in phase_borders.
+    // neighbor_setup (neighbor.rs:604-665), comm size 1
+    double max_skin = 0.0;
+    if (s->nlocal) max_skin = std::fmax(0.0, s->cut_max_local);
+    const double max_cutoff = max_skin > 0.0 ? 2.0 * max_skin * s->skin_fraction : s->bin_min_size;
+    const double min_skin = s->nlocal ? s->cut_min_local : DBL_MAX;
+    double buffer = 0.0;
+    if (min_skin < DBL_MAX * 0.5) {
+        buffer = (s->skin_fraction - 1.0) * min_skin;
+        if (s->additive_skin != 0.0) buffer = buffer + 0.5 * s->additive_skin;
+    }
+    const double ghost_cut = std::fmax(max_cutoff + 2.0 * buffer, s->domain_ghost_cutoff);
+    s->ghost_cutoff = ghost_cut;
+    s->cached_max_cutoff = max_cutoff;
+    s->domain_ghost_cutoff = ghost_cut;
+    if (s->bin_min_size < max_cutoff) s->bin_min_size = max_cutoff;
+    compute_bin_grid(s);
+    if (s->total_cells >= 0x7fffffffull)
+        return fail(s->ctx, SOIL_ERR_CAPACITY, "bin grid of %llu cells is too large",
+                    (unsigned long long)s->total_cells);
+    // setup_deform (soil_deform/src/lib.rs:346-420)
+    s->shear_initialized = false;
+    s->deform_initialized = true;
+    s->deform_step = 0;
+    s->setup_done = true;
+    TRY(update_colptrs(s));
+    return SOIL_OK;
+}
+
+int soil_sys_set_shear(soil_sys* s, double erate) {
+    if (!s) return SOIL_ERR_INVALID;
+    if (s->setup_done) return fail(s->ctx, SOIL_ERR_STATE, "set the shear rate before setup");
+    s->shear = true;
+    s->shear_rate = erate;
+    return SOIL_OK;
+}
+
+int soil_sys_set_harmonic(soil_sys* s, double k, int32_t radius_col) {
+    if (!s) return SOIL_ERR_INVALID;
+    if (k != 0.0 && (radius_col < 0 || (size_t)radius_col >= s->cols.size() ||
+                     s->cols[radius_col].width != 1))
+        return fail(s->ctx, SOIL_ERR_INVALID, "radius column must be a registered width-1 column");
+    s->harmonic_k = k;
+    s->radius_col = radius_col;
+    s->in_lists_valid = false;
+    return SOIL_OK;
+}
+
+int soil_sys_set_force_hook(soil_sys* s, soil_force_fn fn, void* user) {
+    if (!s) return SOIL_ERR_INVALID;
+    s->hook = fn;
+    s->hook_user = user;
+    return SOIL_OK;
+}
+
+int soil_step(soil_sys* s, uint64_t nsteps) {
+    if (!s) return SOIL_ERR_INVALID;
+    if (!s->setup_done) return fail(s->ctx, SOIL_ERR_STATE, "soil_sys_setup has not run");
+    for (uint64_t k = 0; k < nsteps; ++k) TRY(full_step(s, k + 1 == nsteps));
+    return SOIL_OK;
+}
+
+int soil_sys_sync(soil_sys* s) {
+    if (!s) return SOIL_ERR_INVALID;
+    return sync(s);
+}
+
+int soil_sys_stream(soil_sys* s, void** out) {
+    if (!s || !out) return SOIL_ERR_INVALID;
+    *out = (void*)s->st;
+    return SOIL_OK;
+}
+
+#define PHASE_ENTRY(name)                                                                  \
+    int soil_phase_##name(soil_sys* s) {                                                   \
+        if (!s) return SOIL_ERR_INVALID;                                                   \
+        if (!s->setup_done) return fail(s->ctx, SOIL_ERR_STATE, "soil_sys_setup has not run"); \
+        if (s->pending_final) {                                                            \
+            launch_final(s->st, s->nlocal, s->A, s->dt);                                   \
+            s->pending_final = false;                                                      \
+        }                                                                                  \
+        return phase_##name(s);                                                            \
+    }
+PHASE_ENTRY(deform)
+PHASE_ENTRY(initial)
+PHASE_ENTRY(decide_rebuild)
+PHASE_ENTRY(remove_ghosts)
+PHASE_ENTRY(zero_forces)
+PHASE_ENTRY(pbc)
+PHASE_ENTRY(sort)
+PHASE_ENTRY(borders)
+PHASE_ENTRY(forward_comm)
+PHASE_ENTRY(neighbor)
+PHASE_ENTRY(force)
+PHASE_ENTRY(reverse_comm)
+PHASE_ENTRY(final)
+
+int soil_sys_counts(soil_sys* s, soil_counts* o) {
+    if (!s || !o) return SOIL_ERR_INVALID;
+    std::memset(o, 0, sizeof(*o));
+    o->nlocal = s->nlocal;
+    o->nghost = s->nghost;
+    o->npairs = s->npairs;
+    o->step = s->steps_done;
+    o->rebuilds = s->rebuilds;
+    o->sorts = s->sorts;
+    o->steps_since_build = s->steps_since_build;
+    o->filter_candidates = s->hflags ? s->hflags->candidates : 0;
+    o->filter_rechecked = s->hflags ? s->hflags->rechecked : 0;
+    o->comm_state = s->state;
+    o->triclinic = s->triclinic ? 1 : 0;
+    for (int d = 0; d < 3; ++d) o->bin_count[d] = s->bin_count[d];
+    o->nstencil_forward = (int32_t)s->stencil_fwd.size();
+    o->ghost_cutoff = s->ghost_cutoff;
+    o->max_cutoff = s->cached_max_cutoff;
+    o->tilt_xy = s->tilt[0];
+    return SOIL_OK;
+}
+
+static int flush_pending(soil_sys* s) {
+    if (s->pending_final) {
+        launch_final(s->st, s->nlocal, s->A, s->dt);
+        s->pending_final = false;
+    }
+    return check_launch(s);
+}
+
+int soil_sys_get_atoms(soil_sys* s, uint64_t first, uint64_t n, uint32_t* tag, double* pos3,
+                       double* vel3, double* force3, int32_t* image3, int32_t* origin_index) {
+    if (!s) return SOIL_ERR_INVALID;
+    if (first + n > s->nlocal + s->nghost) return fail(s->ctx, SOIL_ERR_INVALID, "range out of bounds");
+    if (n == 0) return SOIL_OK;
+    TRY(flush_pending(s));
+    TRY(ensure(s, s->stage, 3 * n));
+    const uint64_t f = first;
+    auto get3 = [&](double* dst, double* a, double* b, double* c) -> int {
+        if (!dst) return SOIL_OK;
+        launch_interleave3(s->st, n, s->stage.p, a + f, b + f, c + f);
+        CK(cudaMemcpyAsync(dst, s->stage.p, n * 24, cudaMemcpyDeviceToHost, s->st));
+        CK(cudaStreamSynchronize(s->st));
+        return SOIL_OK;
+    };
+    TRY(get3(pos3, s->A.x, s->A.y, s->A.z));
+    TRY(get3(vel3, s->A.vx, s->A.vy, s->A.vz));
+    TRY(get3(force3, s->A.fx, s->A.fy, s->A.fz));
+    if (tag) CK(cudaMemcpyAsync(tag, s->A.tag + f, n * 4, cudaMemcpyDeviceToHost, s->st));
+    if (origin_index) CK(cudaMemcpyAsync(origin_index, s->A.origin + f, n * 4, cudaMemcpyDeviceToHost, s->st));
+    if (image3) {
+        int32_t* st3 = (int32_t*)s->stage.p;
+        launch_interleave3i(s->st, n, st3, s->A.img + f, s->A.img + s->acap + f,
+                            s->A.img + 2 * s->acap + f);
+        CK(cudaMemcpyAsync(image3, st3, n * 12, cudaMemcpyDeviceToHost, s->st));
+    }
+    TRY(check_launch(s));
+    return sync(s);
+}
+
+int soil_sys_get_column(soil_sys* s, int32_t col, uint64_t first, uint64_t n, double* out) {
+    if (!s || !out || col < 0 || (size_t)col >= s->cols.size()) return SOIL_ERR_INVALID;
+    if (first + n > s->nlocal + s->nghost) return fail(s->ctx, SOIL_ERR_INVALID, "range out of bounds");
+    if (n == 0) return SOIL_OK;
+    TRY(flush_pending(s));
+    const ColMeta& m = s->cols[col];
+    TRY(ensure(s, s->stage, (uint64_t)m.width * n));
+    launch_interleave_w(s->st, n, m.width, s->stage.p, s->A.planes[m.plane0] + first, s->acap);
+    CK(cudaMemcpyAsync(out, s->stage.p, (uint64_t)m.width * n * 8, cudaMemcpyDeviceToHost, s->st));
+    TRY(check_launch(s));
+    return sync(s);
+}
+
+int soil_sys_get_neighbor(soil_sys* s, uint32_t* offsets, uint32_t* indices) {
+    if (!s) return SOIL_ERR_INVALID;
+    if (s->rebuilds == 0) return fail(s->ctx, SOIL_ERR_STATE, "no neighbor list built yet");
+    if (offsets) CK(cudaMemcpyAsync(offsets, s->offsets.p, (s->nlocal + 1) * 4, cudaMemcpyDeviceToHost, s->st));
+    if (indices && s->npairs)
+        CK(cudaMemcpyAsync(indices, s->indices.p, s->npairs * 4, cudaMemcpyDeviceToHost, s->st));
+    return sync(s);
+}
+
+int soil_sys_num_swaps(soil_sys* s, int32_t* out) {
+    if (!s || !out) return SOIL_ERR_INVALID;
+    *out = s->nswaps;
+    return SOIL_OK;
+}
+
+int soil_sys_get_swap(soil_sys* s, int32_t k, uint64_t* recv_start, uint64_t* recv_count,
+                      double periodic_offset[3], double vel_offset[3], uint32_t* send_indices) {
+    if (!s || k < 0 || k >= s->nswaps) return SOIL_ERR_INVALID;
+    const SwapHost& h = s->swaps[k];
+    if (recv_start) *recv_start = h.recv_start;
+    if (recv_count) *recv_count = h.recv_count;
+    for (int d = 0; d < 3; ++d) {
+        if (periodic_offset) periodic_offset[d] = h.off[d];
+        if (vel_offset) vel_offset[d] = h.voff[d];
+    }
+    if (send_indices && h.recv_count)
+        CK(cudaMemcpyAsync(send_indices, s->send[k].p, h.recv_count * 4, cudaMemcpyDeviceToHost, s->st));
+    return sync(s);
+}
+
+int soil_sys_get_sort_perm(soil_sys* s, uint32_t* perm) {
+    if (!s || !perm) return SOIL_ERR_INVALID;
+    if (!s->perm_valid) return fail(s->ctx, SOIL_ERR_STATE, "no spatial sort has run");
+    CK(cudaMemcpyAsync(perm, s->sort_perm.p, s->nlocal * 4, cudaMemcpyDeviceToHost, s->st));
+    return sync(s);
+}
+
+int soil_sys_view(soil_sys* s, soil_dev_view* out) {
+    if (!s || !out) return SOIL_ERR_INVALID;
+    TRY(flush_pending(s));
+    return make_view(s, out);
+}
+
+}  // extern "C"

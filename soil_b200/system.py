@@ -1,0 +1,233 @@
+"""Python binding of the soil_b200 C ABI (include/soil_cuda.h).
+
+``Context`` owns a CUDA device handle and an optional HBM budget; ``System``
+is one periodic simulation (the reference's Atom + Domain + Neighbor +
+CommTopology resources) whose every phase runs in libsoil_cuda.so.  There is
+no CPU path: a missing library or device raises.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+
+
+def _p(a, ct):
+    return a.ctypes.data_as(C.POINTER(ct)) if a is not None else None
+
+
+class Context:
+    def __init__(self, device=0, hbm_budget_bytes=0):
+        self.lib = abi.load_library()
+        h = C.c_void_p()
+        st = self.lib.soil_ctx_create(device, hbm_budget_bytes, C.byref(h))
+        if st != abi.SOIL_OK:
+            raise abi.SoilError(st, "soil_ctx_create", f"(device {device})")
+        self.h = h
+
+    def error(self):
+        return self.lib.soil_last_error(self.h).decode(errors="replace")
+
+    def check(self, st, where):
+        if st != abi.SOIL_OK:
+            raise abi.SoilError(st, where, self.error())
+
+    def bytes_in_use(self):
+        v = C.c_uint64()
+        self.check(self.lib.soil_ctx_bytes_in_use(self.h, C.byref(v)), "bytes_in_use")
+        return v.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.soil_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class System:
+    """One simulation on the GPU; mirrors oracle.OracleSystem method by method."""
+
+    def __init__(self, ctx, box, cfg, dt):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        h = C.c_void_p()
+        ctx.check(self.lib.soil_sys_create(ctx.h, C.byref(box), C.byref(cfg), dt, C.byref(h)),
+                  "soil_sys_create")
+        self.h = h
+        self.columns = []
+        self._hook = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.soil_sys_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _c(self, st, where):
+        self.ctx.check(st, where)
+
+    def register_column(self, name, width, flags):
+        c = C.c_int32()
+        self._c(self.lib.soil_sys_register_column(self.h, name.encode(), width, flags, C.byref(c)),
+                "register_column")
+        self.columns.append((name, width, flags))
+        return c.value
+
+    def add_atoms(self, tag, pos, vel, mass, cutoff, columns=None, atom_type=None):
+        n = len(tag)
+        tag = np.ascontiguousarray(tag, dtype=np.uint32)
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(n, 3)
+        vel = np.ascontiguousarray(vel, dtype=np.float64).reshape(n, 3)
+        mass = np.ascontiguousarray(mass, dtype=np.float64)
+        cutoff = np.ascontiguousarray(cutoff, dtype=np.float64)
+        ty = np.ascontiguousarray(atom_type, dtype=np.uint32) if atom_type is not None else None
+        keep = []
+        arr = None
+        if self.columns:
+            arr = (C.POINTER(C.c_double) * len(self.columns))()
+            for c in range(len(self.columns)):
+                if columns is not None and columns[c] is not None:
+                    a = np.ascontiguousarray(columns[c], dtype=np.float64)
+                    keep.append(a)
+                    arr[c] = _p(a, C.c_double)
+        self._c(self.lib.soil_sys_add_atoms(self.h, n, _p(tag, C.c_uint32), _p(ty, C.c_uint32),
+                                            _p(pos, C.c_double), _p(vel, C.c_double),
+                                            _p(mass, C.c_double), _p(cutoff, C.c_double), arr),
+                "add_atoms")
+
+    def setup(self):
+        self._c(self.lib.soil_sys_setup(self.h), "setup")
+
+    def set_shear(self, rate):
+        self._c(self.lib.soil_sys_set_shear(self.h, rate), "set_shear")
+
+    def set_harmonic(self, k, radius_col):
+        self._c(self.lib.soil_sys_set_harmonic(self.h, k, radius_col), "set_harmonic")
+
+    def set_force_hook(self, fn, user=None):
+        """fn(view: SoilDevView, user) -> int, called once per step."""
+        if fn is None:
+            self._hook = None
+            self._c(self.lib.soil_sys_set_force_hook(self.h, abi.SOIL_FORCE_FN(), None), "hook")
+            return
+        cb = abi.SOIL_FORCE_FN(lambda v, u: fn(v.contents, user))
+        self._hook = cb
+        self._c(self.lib.soil_sys_set_force_hook(self.h, cb, None), "hook")
+
+    def step(self, n=1):
+        self._c(self.lib.soil_step(self.h, n), "soil_step")
+
+    def sync(self):
+        self._c(self.lib.soil_sys_sync(self.h), "sync")
+
+    def stream(self):
+        v = C.c_void_p()
+        self._c(self.lib.soil_sys_stream(self.h, C.byref(v)), "stream")
+        return v.value
+
+    def phase(self, name):
+        self._c(getattr(self.lib, "soil_phase_" + name)(self.h), "phase " + name)
+
+    def counts(self):
+        c = abi.SoilCounts()
+        self._c(self.lib.soil_sys_counts(self.h, C.byref(c)), "counts")
+        return c
+
+    def atoms(self, first=0, n=None, local_only=False):
+        c = self.counts()
+        total = c.nlocal + (0 if local_only else c.nghost)
+        if n is None:
+            n = total - first
+        tag = np.zeros(n, np.uint32)
+        pos = np.zeros((n, 3))
+        vel = np.zeros((n, 3))
+        force = np.zeros((n, 3))
+        image = np.zeros((n, 3), np.int32)
+        origin = np.zeros(n, np.int32)
+        self._c(self.lib.soil_sys_get_atoms(self.h, first, n, _p(tag, C.c_uint32),
+                                            _p(pos, C.c_double), _p(vel, C.c_double),
+                                            _p(force, C.c_double), _p(image, C.c_int32),
+                                            _p(origin, C.c_int32)), "get_atoms")
+        return dict(tag=tag, pos=pos, vel=vel, force=force, image=image, origin=origin)
+
+    def column(self, col, first=0, n=None):
+        c = self.counts()
+        total = c.nlocal + c.nghost
+        if n is None:
+            n = total - first
+        w = self.columns[col][1]
+        out = np.zeros(n * w)
+        self._c(self.lib.soil_sys_get_column(self.h, col, first, n, _p(out, C.c_double)), "column")
+        return out.reshape(n, w)
+
+    def neighbor(self):
+        c = self.counts()
+        off = np.zeros(c.nlocal + 1, np.uint32)
+        idx = np.zeros(c.npairs, np.uint32)
+        self._c(self.lib.soil_sys_get_neighbor(self.h, _p(off, C.c_uint32), _p(idx, C.c_uint32)),
+                "neighbor")
+        return off, idx
+
+    def swaps(self):
+        n = C.c_int32()
+        self._c(self.lib.soil_sys_num_swaps(self.h, C.byref(n)), "num_swaps")
+        out = []
+        for s in range(n.value):
+            rs, rc = C.c_uint64(), C.c_uint64()
+            off = np.zeros(3)
+            voff = np.zeros(3)
+            self._c(self.lib.soil_sys_get_swap(self.h, s, C.byref(rs), C.byref(rc),
+                                               _p(off, C.c_double), _p(voff, C.c_double), None),
+                    "get_swap")
+            send = np.zeros(rc.value, np.uint32)
+            self._c(self.lib.soil_sys_get_swap(self.h, s, None, None, None, None,
+                                               _p(send, C.c_uint32)), "get_swap")
+            out.append(dict(recv_start=rs.value, recv_count=rc.value, offset=off,
+                            vel_offset=voff, send=send))
+        return out
+
+    def sort_perm(self):
+        n = self.counts().nlocal
+        perm = np.zeros(n, np.uint32)
+        self._c(self.lib.soil_sys_get_sort_perm(self.h, _p(perm, C.c_uint32)), "sort_perm")
+        return perm
+
+    def view(self):
+        v = abi.SoilDevView()
+        self._c(self.lib.soil_sys_view(self.h, C.byref(v)), "view")
+        return v
+
+
+def from_workload(ctx, w):
+    """GPU system for a workloads.Workload (radius registered as column 0)."""
+    s = System(ctx, w.box, w.cfg, w.dt)
+    rc = s.register_column("radius", 1, abi.SOIL_COL_FORWARD)
+    s.add_atoms(w.tag, w.pos, w.vel, w.mass, w.cutoff, columns=[w.radius])
+    if w.harmonic_k:
+        s.set_harmonic(w.harmonic_k, rc)
+    if w.shear_rate:
+        s.set_shear(w.shear_rate)
+    s.setup()
+    return s
+
+
+def pairs(offsets, indices, nlocal):
+    """Neighbor::pairs(nlocal) (neighbor.rs:224-242): every (i, j) of the CSR
+    half list, rows ascending, CSR order inside a row."""
+    for i in range(nlocal):
+        for k in range(int(offsets[i]), int(offsets[i + 1])):
+            yield i, int(indices[k])
+
+
+def classify_boundary_atoms(offsets, indices, nlocal):
+    """classify_boundary_atoms (neighbor.rs:1327-1336): True for a local atom
+    with at least one ghost neighbour (index >= nlocal)."""
+    out = np.zeros(nlocal, dtype=bool)
+    for i in range(nlocal):
+        row = indices[int(offsets[i]):int(offsets[i + 1])]
+        out[i] = bool(np.any(row >= nlocal))
+    return out

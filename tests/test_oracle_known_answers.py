@@ -1,0 +1,183 @@
+"""The reference's own known-answer tests, ported against the CPU oracle.
+
+The reference ships no golden files; these inline tests are its only fixed
+answers for this path.  Each test cites the reference test it ports.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from soil_b200 import abi, system, workloads as W
+
+
+def one_atom_sys(pos, vel, dt, box=10.0, radius=0.001, mass=1.0, lo=-5.0):
+    b = W.make_box(box, lo=lo)
+    s = oracle.OracleSystem(b, W.default_cfg(), dt)
+    s.add_atoms([0], [pos], [vel], [mass], [radius])
+    return s
+
+
+def test_initial_integration_updates_position_and_velocity():
+    # soil_verlet/src/lib.rs:220-233: v = 1 + 0.5*0.01*2 = 1.01, x = 0.0101
+    s = one_atom_sys([0.0, 0.0, 0.0], [1.0, 0.0, 0.0], 0.01)
+    s.set_atom_state(0, force=[2.0, 0.0, 0.0])
+    s.phase("initial")
+    a = s.atoms()
+    assert abs(a["vel"][0, 0] - 1.01) < 1e-10
+    assert abs(a["pos"][0, 0] - 0.0101) < 1e-10
+
+
+def test_final_integration_updates_velocity_only():
+    # soil_verlet/src/lib.rs:416-428
+    s = one_atom_sys([0.0, 0.0, 0.0], [1.0, 0.0, 0.0], 0.01)
+    s.set_atom_state(0, force=[2.0, 0.0, 0.0])
+    s.phase("final")
+    a = s.atoms()
+    assert abs(a["vel"][0, 0] - 1.01) < 1e-10
+    assert abs(a["pos"][0, 0]) < 1e-10
+
+
+def test_free_particle_constant_velocity():
+    # soil_verlet/src/lib.rs:339-372: 1000 steps of dt 1e-3 at v = (1.5, -2.3, 0.7)
+    s = one_atom_sys([0.0, 0.0, 0.0], [1.5, -2.3, 0.7], 0.001, box=100.0, lo=-50.0)
+    for _ in range(1000):
+        s.phase("initial")
+        s.phase("final")
+    a = s.atoms()
+    assert abs(a["pos"][0, 0] - 1.5) < 1e-10
+    assert abs(a["pos"][0, 1] + 2.3) < 1e-10
+    assert abs(a["vel"][0, 0] - 1.5) < 1e-10
+
+
+def test_free_fall_parabola_and_pinned_atom():
+    # soil_verlet/examples/free_fall.rs:85-96: x = x0 + v0 t + g t^2/2 to 1e-9;
+    # an inv_mass = 0 atom never moves (here: mass huge is not 1/0, so use the
+    # integrator directly with a constant force m*g re-applied every step)
+    g, m, dt, n = -9.81, 2.0, 1e-4, 10000
+    s = one_atom_sys([0.0, 0.0, 10.0], [0.0, 0.0, 5.0], dt, box=1000.0, lo=-500.0, mass=m)
+    for _ in range(n):
+        s.set_atom_state(0, force=[0.0, 0.0, m * g])
+        s.phase("initial")
+        s.set_atom_state(0, force=[0.0, 0.0, m * g])
+        s.phase("final")
+    t = n * dt
+    a = s.atoms()
+    assert abs(a["pos"][0, 2] - (10.0 + 5.0 * t + 0.5 * g * t * t)) < 1e-9
+    assert abs(a["vel"][0, 2] - (5.0 + g * t)) < 1e-9
+
+
+def tilted(xy=1.2, bvel=0.0):
+    b = abi.SoilBox()
+    for d, L in enumerate((4.0, 3.0, 2.0)):
+        b.lo[d] = 0.0
+        b.hi[d] = L
+    s = oracle.OracleSystem(b, W.default_cfg(), 1.0)
+    s.set_domain_tilt(xy, bvel, True)
+    return s
+
+
+def test_lamda_roundtrip_with_tilt():
+    # domain.rs:1015-1029
+    s = tilted()
+    for r in ([0.3, 0.7, 0.9], [3.9, 2.9, 0.1], [2.0, 1.5, 1.0]):
+        back = s.lamda2x(s.x2lamda(r))
+        assert np.all(np.abs(back - r) < 1e-12)
+    lam = s.x2lamda([1.2, 3.0, 0.0])
+    assert abs(lam[1] - 1.0) < 1e-12 and abs(lam[0]) < 1e-12
+
+
+def test_triclinic_pbc_wraps_and_remaps_velocity():
+    # domain.rs:1031-1058
+    s = tilted(1.2, 5.0)
+    s.add_atoms([0], [[2.0, 3.03, 1.0]], [[7.0, 0.0, 0.0]], [1.0], [0.1])
+    s.set_domain_tilt(1.2, 5.0, True)
+    s.set_state(abi.SOIL_FULL_REBUILD)
+    s.phase("pbc")
+    a = s.atoms()
+    assert abs(a["pos"][0, 1] - 0.03) < 1e-9
+    assert abs(a["pos"][0, 0] - 0.8) < 1e-9
+    assert abs(a["vel"][0, 0] - 2.0) < 1e-12
+    assert a["image"][0, 1] == 1
+
+
+def binned_pairs(s, n):
+    off, idx = s.neighbor()
+    out = set()
+    for i, j in system.pairs(off, idx, n):
+        out.add((min(i, j), max(i, j)))
+    return out
+
+
+def reference_all_pairs(pos, radii, sf):
+    # neighbor.rs:1433-1454
+    n = len(pos)
+    res = set()
+    for i in range(n):
+        for j in range(i + 1, n):
+            d = math.sqrt(sum((pos[j][k] - pos[i][k]) ** 2 for k in range(3)))
+            if d < (radii[i] + radii[j]) * sf:
+                res.add((i, j))
+    return res
+
+
+def test_bin_neighbor_list_finds_close_pair():
+    # neighbor.rs:1360-1402
+    b = W.make_box(2.0)
+    s = oracle.OracleSystem(b, W.default_cfg(), 1.0)
+    s.add_atoms([0, 1], [[0.5, 0.5, 0.5], [1.0, 0.5, 0.5]], np.zeros((2, 3)), [1.0, 1.0], [0.5, 0.5])
+    s.setup()
+    s.phase("neighbor")
+    off, idx = s.neighbor()
+    assert 1 in idx[off[0]:off[1]]
+
+
+@pytest.mark.parametrize("triclinic", [False, True])
+def test_bin_neighbor_list_matches_reference(triclinic):
+    # neighbor.rs:1456-1535 (orthogonal, 30 atoms) and 1537-1619 (tilt xy = 1, 40 atoms)
+    n = 40 if triclinic else 30
+    amp = 1.4 if triclinic else 1.5
+    pos = [[math.sin(i * 0.31) * amp + 2.0, math.cos(i * 0.67) * amp + 2.0,
+            math.sin(i * 0.97) * amp + 2.0] for i in range(n)]
+    b = W.make_box(4.0)
+    s = oracle.OracleSystem(b, W.default_cfg(bin_size=0.5), 1.0)
+    s.add_atoms(np.arange(n), pos, np.zeros((n, 3)), np.ones(n), np.full(n, 0.3))
+    if triclinic:
+        s.set_domain_tilt(1.0, 0.0, True)
+    s.setup()
+    s.phase("neighbor")
+    ref = reference_all_pairs(pos, [0.3] * n, 1.0)
+    got = binned_pairs(s, n)
+    assert ref <= got          # the reference test: containment
+    if not triclinic:
+        assert ref == got      # and, with no ghosts and no false positives, equality
+
+
+def test_pair_iter_matches_manual():
+    # neighbor.rs:1404-1413
+    assert list(system.pairs([0, 2, 3, 3], [1, 2, 2], 3)) == [(0, 1), (0, 2), (1, 2)]
+
+
+def test_pair_iter_empty():
+    # neighbor.rs:1415-1427
+    assert list(system.pairs([0, 0, 0], [], 2)) == []
+    assert list(system.pairs([0], [], 0)) == []
+
+
+def test_classify_boundary_atoms_flags_ghost_neighbours():
+    # neighbor.rs:1343-1354
+    mask = system.classify_boundary_atoms(np.array([0, 1, 3, 3]), np.array([1, 0, 3]), 3)
+    assert list(mask) == [False, True, False]
+
+
+def test_shear_tilt_box_flip():
+    # soil_deform/src/lib.rs:579-587: xy = raw - Lx*round(raw/Lx), raw = rate*dt*step*Ly
+    w = W.mono("flip", 1, 200, 0.3, 1e-2, 0, shear_rate=30.0)
+    s = oracle.from_workload(w)
+    L = w.L
+    for step in range(1, 8):
+        s.step(1)
+        raw = 30.0 * 1e-2 * step * L
+        assert s.counts().tilt_xy == raw - L * round(raw / L)
+        assert abs(s.counts().tilt_xy) <= 0.5 * L + 1e-12
