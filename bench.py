@@ -1,0 +1,409 @@
+#!/usr/bin/env python
+"""bench.py — atom-steps/s of the SOIL substrate hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl soil|reference]
+                    [--config c1|c2|c3] [--filter fp64|fp32]
+
+One "step" is one velocity-Verlet timestep of the whole hot path (integrate,
+rebuild check, ghost comm, spatial sort + neighbor build when due, the
+repulsion consumer, reverse comm) over one periodic system.  The default
+workload is the large single system: 4,194,304 polydisperse spheres
+(r ~ U[0.4, 0.6], packing fraction 0.50), harmonic repulsion k = 1e3,
+dt = 1e-4, seeded synthetic inputs.  State is FP64 throughout.
+
+A single system does not shard on one rank (no spatial decomposition), so
+with --gpus N every rank runs an independent replica; `value` is the
+atom-steps of all ranks over the slowest rank's device time (weak scaling).
+
+Printed JSON keys beyond the base contract:
+  neighbor_builds_per_s  rebuilds inside the timed region / its duration
+  roofline               dominant kernel: algorithmic bytes / mean launch time
+  cpu_baseline           the CPU oracle on a bounded sample of the same system
+  e2e                    the same metric through the C ABI from pinned host
+                         buffers (upload, setup, K steps, download of pos/vel)
+  phases                 device ms per phase over the timed region
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+from soil_b200 import abi, workloads  # noqa: E402
+
+# Algorithmic bytes per unit of each timed phase (FP64 SoA; one read or
+# write of each value the phase must touch).
+#   integrate: final(t) fused with initial(t+1) + displacement check:
+#              R x,v,F,inv_m (80) + R last-build pos (24) + W x,v (48) = 152 B/local
+#   force:     R pos+radius of every atom (32) + W force (24) + R row/transposed
+#              offsets (8) + R 4 B per list entry (each pair is listed in a
+#              row and in a transposed row: 8 B per pair)
+#   forward:   R root+chain (8) + R root pos,vel (48) + W pos,vel (48)
+#              + forward columns (16 B per f64) per ghost
+#   reverse:   R send index (4) + R ghost F (24) + RMW owner F (48) per ghost
+#   final:     80 B/local
+BYTES_PER_UNIT = {
+    "integrate": lambda c, fw: 152 * c.nlocal,
+    "final": lambda c, fw: 80 * c.nlocal,
+    "force": lambda c, fw: 64 * (c.nlocal + c.nghost) + 8 * c.npairs,
+    "forward": lambda c, fw: (104 + 16 * fw) * c.nghost,
+    "reverse": lambda c, fw: 76 * c.nghost,
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic(kernel, workload):
+    """DRAM bytes per atom of `kernel` from a committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    e = d.get(kernel)
+    if not e or e.get("workload") != workload:
+        return None
+    return e
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                mhz.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def make_workload(name, filt, natoms=None):
+    f = abi.SOIL_FILTER_FP32_RECHECK if filt == "fp32" else abi.SOIL_FILTER_FP64
+    if natoms:  # reduced size of the same configuration (profiling runs)
+        w = {"c1": workloads.config1, "c2": workloads.config2,
+             "c3": workloads.config3}[name](n=natoms)
+        w.cfg.filter = f
+        return w, f"{name} reduced to {natoms} atoms"
+    if name == "c1":
+        w = workloads.config1()
+        w.cfg.filter = f
+        desc = "C1 plain: 32,768 monodisperse spheres d=1, phi 0.30, F=0, dt 1e-3"
+    elif name == "c3":
+        w = workloads.config3()
+        w.cfg.filter = f
+        desc = ("C3 Lees-Edwards shear: 1,048,576 monodisperse spheres d=1, phi 0.40, "
+                "xy rate 0.1, harmonic k=1e3, dt 1e-4")
+    else:
+        w = workloads.config2(filt=f)
+        desc = ("C2 large single system: 4,194,304 polydisperse spheres r~U[0.4,0.6], "
+                "phi 0.50, harmonic k=1e3, dt 1e-4")
+    return w, desc
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline(w, budget_s=20.0, max_steps=10000):
+    """The CPU oracle (single thread, as the reference path) on a bounded
+    sample of the same system: setup, then steps until ~budget_s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    t0 = time.perf_counter()
+    o = oracle.from_workload(w)
+    t_setup = time.perf_counter() - t0
+    steps, t = 0, 0.0
+    while t < budget_s and steps < max_steps:
+        t1 = time.perf_counter()
+        o.step(1)
+        t += time.perf_counter() - t1
+        steps += 1
+    c = o.counts()
+    return {"value": w.n * steps / t, "unit": "atom-steps/s", "cores": 1, "kind": "port",
+            "sample": (f"{steps} timesteps of the full {w.n}-atom system from its initial state, "
+                       f"{c.rebuilds} neighbor builds included (setup {t_setup:.1f}s excluded), "
+                       "C++ oracle -O3, one thread"),
+            "steps": steps, "seconds": t, "rebuilds": int(c.rebuilds)}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    w, desc = make_workload(args.config, args.filter, args.natoms)
+    cb = cpu_baseline(w, budget_s=120.0, max_steps=args.steps)
+    line = {
+        "impl": "reference", "metric": "atom-steps/s", "value": cb["value"],
+        "unit": "atom-steps/s", "n_gpus": args.gpus, "steps": cb["steps"],
+        "warmup": 0, "ms_per_step": 1e3 * cb["seconds"] / cb["steps"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded SplitMix64 positions/radii, Box-Muller velocities)",
+        "config": {"workload": desc, "n_atoms": w.n, "filter": args.filter},
+        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": cb["value"], "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_soil(args, world, rank, local):
+    import torch
+    from soil_b200 import system
+
+    w, desc = make_workload(args.config, args.filter, args.natoms)
+    fwd_width = 1  # the radius column
+    lib = abi.load_library()
+    ctx = system.Context(local)
+    s = system.from_workload(ctx, w)
+    stream = torch.cuda.ExternalStream(s.stream(), device=torch.device("cuda", local))
+
+    # warm-up: the first step builds the neighbor list; time every phase on
+    # the remaining warm-up steps to find the dominant kernel
+    s.step(1)
+    s.set_timing((1 << abi.SOIL_NUM_TIMERS) - 1)
+    s.step(max(args.warmup - 1, 2))
+    ms0, _, iv0 = s.get_timing()
+    light = {abi.TIMER_NAMES[t]: ms0[t] / max(iv0[t], 1) for t in range(abi.SOIL_NUM_TIMERS)
+             if abi.TIMER_NAMES[t] in BYTES_PER_UNIT}
+    dominant = max(light, key=light.get)
+    s.set_timing(1 << abi.TIMER_NAMES.index(dominant))
+
+    c0 = s.counts()
+    launches0 = lib.soil_kernel_launches()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    torch.cuda.synchronize()
+    s.sync()
+    barrier(world)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    s.step(args.steps)
+    ev1.record(stream)
+    s.sync()
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = ev0.elapsed_time(ev1)
+    clocks = sampler.stop()
+    launches = lib.soil_kernel_launches() - launches0
+    c1 = s.counts()
+    ms_dom, launches_dom, iv_dom = s.get_timing()
+    k = abi.TIMER_NAMES.index(dominant)
+    ms_max = max_over_ranks(ms, world)
+
+    value = world * w.n * args.steps / (ms_max * 1e-3)
+    rebuilds = int(c1.rebuilds - c0.rebuilds)
+    peak, peak_kind = load_peaks()
+    per_launch_ms = ms_dom[k] / max(launches_dom[k], 1)
+    alg_bytes = BYTES_PER_UNIT[dominant](c1, fwd_width)
+    achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
+    tr = load_traffic(dominant, args.config)
+    traffic = None
+    if tr:
+        traffic = tr["dram_bytes_per_atom"] * (c1.nlocal if dominant in ("integrate", "final")
+                                               else c1.nlocal + c1.nghost)
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
+                "mean_launch_ms": per_launch_ms, "launches": int(launches_dom[k])}
+
+    # per-phase breakdown (warm-up steps) for the record
+    phases = {abi.TIMER_NAMES[t]: round(ms0[t], 4) for t in range(abi.SOIL_NUM_TIMERS) if iv0[t]}
+    del s
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(ctx, w, args.steps, world)
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(w)
+        cb = {k2: cb[k2] for k2 in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        line = {
+            "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded SplitMix64 positions/radii, Box-Muller velocities)",
+            "config": {"workload": desc, "n_atoms": w.n, "filter": args.filter,
+                       "box_L": w.L, "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (per-atom state ~%d MB)" %
+                             (c1.nlocal * 200 // 2**20),
+                       "ghosts": int(c1.nghost), "pairs": int(c1.npairs)},
+            "neighbor_builds_per_s": world * rebuilds / (ms_max * 1e-3),
+            "rebuilds": rebuilds,
+            "roofline": roofline,
+            "cpu_baseline": cb,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "phases_warmup_ms": phases,
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_e2e(ctx, w, steps, world):
+    """Same metric through the C ABI from pinned host buffers: upload the
+    initial state, set up, run `steps`, read back positions and velocities."""
+    import torch
+    from soil_b200 import system
+
+    def pinned(a):
+        t = torch.empty(a.shape, dtype={np.float64: torch.float64, np.uint32: torch.int32}[
+            a.dtype.type], pin_memory=True)
+        v = t.numpy().view(a.dtype)
+        v[...] = a
+        return t, v
+
+    keep = []
+    host = {}
+    for name in ("tag", "pos", "vel", "mass", "cutoff", "radius"):
+        t, v = pinned(getattr(w, name))
+        keep.append(t)
+        host[name] = v
+    out_pos = pinned(np.zeros((w.n, 3)))
+    out_vel = pinned(np.zeros((w.n, 3)))
+    h2d = sum(host[k].nbytes for k in host)
+    barrier(world)
+    t0 = time.perf_counter()
+    s = system.System(ctx, w.box, w.cfg, w.dt)
+    rc = s.register_column("radius", 1, abi.SOIL_COL_FORWARD)
+    s.add_atoms(host["tag"], host["pos"], host["vel"], host["mass"], host["cutoff"],
+                columns=[host["radius"]])
+    if w.harmonic_k:
+        s.set_harmonic(w.harmonic_k, rc)
+    if w.shear_rate:
+        s.set_shear(w.shear_rate)
+    s.setup()
+    s.step(steps)
+    s.read_local_state(out_pos[1], out_vel[1])
+    t1 = time.perf_counter()
+    barrier(world)
+    dt = max_over_ranks(t1 - t0, world)
+    d2h = out_pos[1].nbytes + out_vel[1].nbytes
+    s.close()
+    return {"value": world * w.n * steps / dt, "unit": "atom-steps/s",
+            "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps,
+            "seconds": dt, "what": "host arrays -> soil_sys_add_atoms/setup -> soil_step(K) "
+                                   "-> soil_sys_get_atoms(pos, vel)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["soil", "reference"], default="soil")
+    ap.add_argument("--config", choices=["c1", "c2", "c3"], default="c2")
+    ap.add_argument("--filter", choices=["fp64", "fp32"], default="fp64")
+    ap.add_argument("--natoms", type=int, default=None,
+                    help="reduced system size (profiling only; not a bench line)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    world, rank, local = dist_init()
+    try:
+        if args.impl == "reference":
+            return run_reference(args, world, rank)
+        return run_soil(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -233,6 +233,21 @@ int soil_sys_get_sort_perm(soil_sys* sys, uint32_t* perm);
 /* Device pointers for an external consumer (valid until the next rebuild). */
 int soil_sys_view(soil_sys* sys, soil_dev_view* out);
 
+/* ---- instrumentation (no reference counterpart: the reference has only
+ * wall-clock thermo columns, soil_print/src/lib.rs:20-26) ------------------ */
+/* Kernels this library has launched in this process. */
+uint64_t soil_kernel_launches(void);
+/* Phase timers of soil_step: CUDA events recorded on the system stream
+ * around each phase.  0 integrate (deform + initial, with the previous final
+ * fused in), 1 zero, 2 pbc, 3 sort, 4 borders, 5 forward, 6 neighbor,
+ * 7 force, 8 reverse, 9 final. */
+#define SOIL_NUM_TIMERS 10
+/* Time the phases whose bit is set in `mask` (0 disables); resets the sums. */
+int soil_sys_set_timing(soil_sys* sys, uint32_t mask);
+/* Summed milliseconds, kernel launches and timed intervals per timer. */
+int soil_sys_get_timing(soil_sys* sys, double* ms, uint64_t* launches, uint64_t* intervals);
+const char* soil_timer_name(int32_t i);
+
 #ifdef __cplusplus
 }
 #endif

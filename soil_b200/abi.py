@@ -155,7 +155,15 @@ PROTOTYPES = {
     "soil_sys_get_swap": (C.c_int, [P, i32, pu64, pu64, pdbl, pdbl, pu32]),
     "soil_sys_get_sort_perm": (C.c_int, [P, pu32]),
     "soil_sys_view": (C.c_int, [P, C.POINTER(SoilDevView)]),
+    "soil_kernel_launches": (C.c_uint64, []),
+    "soil_sys_set_timing": (C.c_int, [P, u32]),
+    "soil_sys_get_timing": (C.c_int, [P, pdbl, pu64, pu64]),
+    "soil_timer_name": (C.c_char_p, [i32]),
 }
+
+SOIL_NUM_TIMERS = 10
+TIMER_NAMES = ["integrate", "zero", "pbc", "sort", "borders", "forward", "neighbor", "force",
+               "reverse", "final"]
 
 PHASES = [
     "deform", "initial", "decide_rebuild", "remove_ghosts", "zero_forces", "pbc",

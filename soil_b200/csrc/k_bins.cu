@@ -46,6 +46,7 @@ __global__ void __launch_bounds__(kBlock) k_cells(uint64_t first, uint64_t n, At
 void launch_cells(cudaStream_t st, uint64_t first, uint64_t n, const AtomCols& c, const Grid& gr,
                   uint32_t* cell_out, uint32_t* counts) {
     if (n == 0) return;
+    note_launch();
     k_cells<<<grid_for(n), kBlock, 0, st>>>(first, n, c, gr, cell_out, counts);
 }
 
@@ -61,6 +62,7 @@ __global__ void __launch_bounds__(kBlock) k_count_cells(uint64_t n, const uint32
 
 void launch_count_cells(cudaStream_t st, uint64_t n, const uint32_t* cell, uint32_t* counts) {
     if (n == 0) return;
+    note_launch();
     k_count_cells<<<grid_for(n), kBlock, 0, st>>>(n, cell, counts);
 }
 
@@ -84,6 +86,7 @@ __global__ void __launch_bounds__(kBlock) k_scatter(uint64_t n, const uint32_t* 
 void launch_scatter(cudaStream_t st, uint64_t n, const uint32_t* cell, uint32_t* cursor,
                     uint32_t* out) {
     if (n == 0) return;
+    note_launch();
     k_scatter<<<grid_for(n), kBlock, 0, st>>>(n, cell, cursor, out);
 }
 
@@ -108,6 +111,7 @@ __global__ void __launch_bounds__(kBlock) k_segsort(uint64_t nseg, const uint32_
 
 void launch_segsort(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint32_t* items) {
     if (nseg == 0) return;
+    note_launch();
     k_segsort<<<grid_for(nseg), kBlock, 0, st>>>(nseg, start, items);
 }
 
@@ -144,6 +148,7 @@ __global__ void __launch_bounds__(kBlock) k_perm_gather(uint64_t n, const uint32
 void launch_perm_gather(cudaStream_t st, uint64_t n, const uint32_t* perm, const AtomCols& src,
                         const AtomCols& dst) {
     if (n == 0) return;
+    note_launch();
     k_perm_gather<<<grid_for(n), kBlock, 0, st>>>(n, perm, src, dst);
 }
 
@@ -159,6 +164,7 @@ __global__ void __launch_bounds__(kBlock) k_identity(uint64_t n, const uint32_t*
 
 void launch_identity_check(cudaStream_t st, uint64_t n, const uint32_t* perm, DevFlags* flags) {
     if (n == 0) return;
+    note_launch();
     k_identity<<<grid_for(n), kBlock, 0, st>>>(n, perm, flags);
 }
 
@@ -172,6 +178,7 @@ __global__ void __launch_bounds__(kBlock) k_permute_u32(uint64_t n, const uint32
 void launch_permute_u32(cudaStream_t st, uint64_t n, const uint32_t* perm, const uint32_t* in,
                         uint32_t* out) {
     if (n == 0) return;
+    note_launch();
     k_permute_u32<<<grid_for(n), kBlock, 0, st>>>(n, perm, in, out);
 }
 
@@ -206,6 +213,7 @@ void launch_sorted_views(cudaStream_t st, uint64_t n, const uint32_t* sorted, co
                          double* scut, float* spx32, float* spy32, float* spz32, float* scut32,
                          const double origin[3]) {
     if (n == 0) return;
+    note_launch();
     k_sorted_views<<<grid_for(n), kBlock, 0, st>>>(n, sorted, c, atom_sorted_idx, spx, spy, spz,
                                                    scut, spx32, spy32, spz32, scut32, origin[0],
                                                    origin[1], origin[2]);

@@ -98,6 +98,7 @@ void launch_harmonic(cudaStream_t st, uint64_t nlocal, uint64_t ntotal, const At
                      const double* radius, double k, int newton, const uint32_t* offsets,
                      const uint32_t* indices, const uint32_t* in_start, const uint32_t* in_list) {
     if (ntotal == 0) return;
+    note_launch();
     k_harmonic<<<grid_for(ntotal), kBlock, 0, st>>>(nlocal, ntotal, c, radius, k, newton, offsets,
                                                     indices, in_start, in_list);
 }

@@ -61,6 +61,7 @@ void launch_border_count(cudaStream_t st, uint64_t scan_end, const AtomCols& c,
                          const BorderDim& bd, uint32_t* tile_lo, uint32_t* tile_hi) {
     const uint64_t tiles = (scan_end + kBorderTile - 1) / kBorderTile;
     if (tiles == 0) return;
+    note_launch();
     k_border_count<<<(unsigned)tiles, kBlock, 0, st>>>(scan_end, c, bd, tile_lo, tile_hi);
 }
 
@@ -146,6 +147,7 @@ void launch_border_scatter(cudaStream_t st, uint64_t scan_end, uint64_t nlocal, 
                            uint32_t* ghost_chain) {
     const uint64_t tiles = (scan_end + kBorderTile - 1) / kBorderTile;
     if (tiles == 0) return;
+    note_launch();
     k_border_scatter<<<(unsigned)tiles, kBlock, 0, st>>>(scan_end, nlocal, c, bd, tile_off_lo,
                                                          tile_off_hi, recv_lo, recv_hi, send_lo,
                                                          send_hi, ghost_root, ghost_chain);
@@ -198,6 +200,7 @@ void launch_forward(cudaStream_t st, uint64_t nlocal, uint64_t nghost, const Ato
     PlaneList pl;
     pl.n = nfwd;
     for (int k = 0; k < nfwd; ++k) pl.idx[k] = fwd_planes[k];
+    note_launch();
     k_forward<<<grid_for(nghost), kBlock, 0, st>>>(nlocal, nghost, c, ghost_root, ghost_chain, sc,
                                                    pl, zero_force ? 1 : 0);
 }
@@ -223,6 +226,7 @@ void launch_reverse_swap(cudaStream_t st, uint64_t count, uint64_t recv_start,
     PlaneList pl;
     pl.n = nrev;
     for (int k = 0; k < nrev; ++k) pl.idx[k] = rev_planes[k];
+    note_launch();
     k_reverse_swap<<<grid_for(count), kBlock, 0, st>>>(count, recv_start, send, c, pl);
 }
 

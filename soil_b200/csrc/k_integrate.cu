@@ -3,9 +3,15 @@
 //
 // All of these are HBM-bound streams over SoA f64 columns (0.1 flop/byte):
 // one thread per atom, grid-stride, coalesced 8-byte accesses.
+#include <atomic>
+
 #include "kernels.cuh"
 
 namespace soil {
+
+static std::atomic<uint64_t> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+uint64_t launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
 
 unsigned grid_for(uint64_t n, int block, int per_sm) {
     uint64_t need = (n + block - 1) / block;
@@ -101,6 +107,7 @@ void launch_initial(cudaStream_t st, uint64_t n, const AtomCols& c, double dt, b
                     double thr_sq, const double box[3], DevFlags* flags) {
     if (n == 0) return;
     CheckArgs ck = make_check(lbx, lby, lbz, n_check, thr_sq, box, flags);
+    note_launch();
     k_initial<false><<<grid_for(n), kBlock, 0, st>>>(n, c, dt, zero_force ? 1 : 0, ck);
 }
 
@@ -110,6 +117,7 @@ void launch_final_initial(cudaStream_t st, uint64_t n, const AtomCols& c, double
                           const double box[3], DevFlags* flags) {
     if (n == 0) return;
     CheckArgs ck = make_check(lbx, lby, lbz, n_check, thr_sq, box, flags);
+    note_launch();
     k_initial<true><<<grid_for(n), kBlock, 0, st>>>(n, c, dt, zero_force ? 1 : 0, ck);
 }
 
@@ -126,6 +134,7 @@ __global__ void __launch_bounds__(kBlock) k_final(uint64_t n, AtomCols c, double
 
 void launch_final(cudaStream_t st, uint64_t n, const AtomCols& c, double dt) {
     if (n == 0) return;
+    note_launch();
     k_final<<<grid_for(n), kBlock, 0, st>>>(n, c, dt);
 }
 
@@ -150,6 +159,7 @@ void launch_zero_forces(cudaStream_t st, uint64_t n, const AtomCols& c, const in
     ZeroPlanes zp;
     zp.n = nzero;
     for (int k = 0; k < nzero; ++k) zp.idx[k] = zero_planes[k];
+    note_launch();
     k_zero<<<grid_for(n), kBlock, 0, st>>>(n, c, zp);
 }
 
@@ -209,6 +219,7 @@ __global__ void __launch_bounds__(kBlock) k_pbc(uint64_t n, AtomCols c, Geom g, 
 void launch_pbc(cudaStream_t st, uint64_t nlocal, const AtomCols& c, const Geom& g,
                 const double bvel[3]) {
     if (nlocal == 0) return;
+    note_launch();
     k_pbc<<<grid_for(nlocal), kBlock, 0, st>>>(nlocal, c, g, bvel[0], bvel[1], bvel[2]);
 }
 
@@ -222,6 +233,7 @@ __global__ void __launch_bounds__(kBlock) k_shear_profile(uint64_t n, AtomCols c
 
 void launch_shear_profile(cudaStream_t st, uint64_t n, const AtomCols& c, double rate, double yc) {
     if (n == 0) return;
+    note_launch();
     k_shear_profile<<<grid_for(n), kBlock, 0, st>>>(n, c, rate, yc);
 }
 
@@ -238,6 +250,7 @@ __global__ void __launch_bounds__(kBlock) k_save_pos(uint64_t n, AtomCols c, dou
 void launch_save_positions(cudaStream_t st, uint64_t n, const AtomCols& c, double* lbx,
                            double* lby, double* lbz) {
     if (n == 0) return;
+    note_launch();
     k_save_pos<<<grid_for(n), kBlock, 0, st>>>(n, c, lbx, lby, lbz);
 }
 
@@ -261,6 +274,7 @@ void launch_disp_check(cudaStream_t st, uint64_t n, const AtomCols& c, const dou
                        DevFlags* flags) {
     if (n == 0) return;
     CheckArgs ck = make_check(lbx, lby, lbz, n, thr_sq, box, flags);
+    note_launch();
     k_disp_check<<<grid_for(n), kBlock, 0, st>>>(n, c, ck);
 }
 
@@ -308,23 +322,38 @@ __global__ void __launch_bounds__(kBlock) k_interleave_w(uint64_t n, int w, doub
 
 void launch_deinterleave3(cudaStream_t st, uint64_t n, const double* src, double* a, double* b,
                           double* c) {
-    if (n) k_deinterleave3<<<grid_for(n), kBlock, 0, st>>>(n, src, a, b, c);
+    if (n) {
+        note_launch();
+        k_deinterleave3<<<grid_for(n), kBlock, 0, st>>>(n, src, a, b, c);
+    }
 }
 void launch_interleave3(cudaStream_t st, uint64_t n, double* dst, const double* a, const double* b,
                         const double* c) {
-    if (n) k_interleave3<<<grid_for(n), kBlock, 0, st>>>(n, dst, a, b, c);
+    if (n) {
+        note_launch();
+        k_interleave3<<<grid_for(n), kBlock, 0, st>>>(n, dst, a, b, c);
+    }
 }
 void launch_interleave3i(cudaStream_t st, uint64_t n, int32_t* dst, const int32_t* a,
                          const int32_t* b, const int32_t* c) {
-    if (n) k_interleave3i<<<grid_for(n), kBlock, 0, st>>>(n, dst, a, b, c);
+    if (n) {
+        note_launch();
+        k_interleave3i<<<grid_for(n), kBlock, 0, st>>>(n, dst, a, b, c);
+    }
 }
 void launch_deinterleave_w(cudaStream_t st, uint64_t n, int w, const double* src, double* dst0,
                            uint64_t cap) {
-    if (n) k_deinterleave_w<<<grid_for(n), kBlock, 0, st>>>(n, w, src, dst0, cap);
+    if (n) {
+        note_launch();
+        k_deinterleave_w<<<grid_for(n), kBlock, 0, st>>>(n, w, src, dst0, cap);
+    }
 }
 void launch_interleave_w(cudaStream_t st, uint64_t n, int w, double* dst, const double* src0,
                          uint64_t cap) {
-    if (n) k_interleave_w<<<grid_for(n), kBlock, 0, st>>>(n, w, dst, src0, cap);
+    if (n) {
+        note_launch();
+        k_interleave_w<<<grid_for(n), kBlock, 0, st>>>(n, w, dst, src0, cap);
+    }
 }
 
 }  // namespace soil

@@ -115,6 +115,7 @@ static void dispatch_pairs(cudaStream_t st, uint64_t nlocal, const AtomCols& c, 
                            DevFlags* flags) {
     const unsigned g = grid_for(nlocal);
     const bool fp32 = p.filter == SOIL_FILTER_FP32_RECHECK;
+    note_launch();
     if (p.uniform) {
         if (fp32) k_pairs<true, true, FILL><<<g, kBlock, 0, st>>>(nlocal, c, p, rowcount, offsets, indices, flags);
         else k_pairs<true, false, FILL><<<g, kBlock, 0, st>>>(nlocal, c, p, rowcount, offsets, indices, flags);
@@ -146,6 +147,7 @@ __global__ void __launch_bounds__(kBlock) k_in_count(uint64_t nlocal, const uint
 void launch_in_count(cudaStream_t st, uint64_t nlocal, const uint32_t* offsets,
                      const uint32_t* indices, uint32_t* incount) {
     if (nlocal == 0) return;
+    note_launch();
     k_in_count<<<grid_for(nlocal), kBlock, 0, st>>>(nlocal, offsets, indices, incount);
 }
 
@@ -161,6 +163,7 @@ __global__ void __launch_bounds__(kBlock) k_in_scatter(uint64_t nlocal, const ui
 void launch_in_scatter(cudaStream_t st, uint64_t nlocal, const uint32_t* offsets,
                        const uint32_t* indices, uint32_t* cursor, uint32_t* in_list) {
     if (nlocal == 0) return;
+    note_launch();
     k_in_scatter<<<grid_for(nlocal), kBlock, 0, st>>>(nlocal, offsets, indices, cursor, in_list);
 }
 

@@ -77,8 +77,11 @@ void exclusive_scan_u32(cudaStream_t st, const uint32_t* in, uint32_t* out, uint
         cudaMemsetAsync(out, 0, sizeof(uint32_t), st);
         return;
     }
+    note_launch();
     k_scan_reduce<<<(unsigned)ntiles, kBlock, 0, st>>>(in, n, temp);
+    note_launch();
     k_scan_partials<<<1, kBlock, 0, st>>>(temp, ntiles);
+    note_launch();
     k_scan_down<<<(unsigned)ntiles, kBlock, 0, st>>>(in, out, n, temp, ntiles);
 }
 

@@ -10,6 +10,10 @@ namespace soil {
 // times, never more than the work needs.
 unsigned grid_for(uint64_t n, int block = kBlock, int per_sm = 8);
 
+// Process-wide count of kernel launches issued by this library.
+void note_launch();
+uint64_t launches_so_far();
+
 // ---- integrate (k_integrate.cu) -------------------------------------------
 // initial_integration (+ optional fused force zeroing and displacement check)
 void launch_initial(cudaStream_t st, uint64_t n, const AtomCols& c, double dt, bool zero_force,

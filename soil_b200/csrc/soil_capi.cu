@@ -135,6 +135,22 @@ struct soil_sys {
     DevFlags* hflags = nullptr;  // pinned mirror
     uint32_t* hword = nullptr;   // pinned scratch words
 
+    // ---- phase timers ----
+    struct TimedSpan {
+        int timer;
+        cudaEvent_t a, b;
+        uint64_t launches;
+    };
+    uint32_t timing_mask = 0;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<TimedSpan> spans;
+    double timer_ms[SOIL_NUM_TIMERS] = {};
+    uint64_t timer_launches[SOIL_NUM_TIMERS] = {};
+    uint64_t timer_intervals[SOIL_NUM_TIMERS] = {};
+    int open_timer = -1;
+    cudaEvent_t open_ev = nullptr;
+    uint64_t open_launches = 0;
+
     // ---- bookkeeping ----
     bool setup_done = false, perm_valid = false, pending_final = false;
     uint64_t steps_done = 0, rebuilds = 0, sorts = 0;
@@ -291,6 +307,65 @@ int grow_atoms(soil_sys* s, uint64_t need, uint64_t keep) {
     TRY(ensure(s, s->ghost_chain, ncap, gkeep));
     TRY(update_colptrs(s));
     return SOIL_OK;
+}
+
+// ---- phase timers -------------------------------------------------------------
+enum { T_INTEGRATE, T_ZERO, T_PBC, T_SORT, T_BORDERS, T_FORWARD, T_NEIGHBOR, T_FORCE, T_REVERSE,
+       T_FINAL };
+const char* kTimerNames[SOIL_NUM_TIMERS] = {"integrate", "zero",     "pbc",   "sort",    "borders",
+                                            "forward",   "neighbor", "force", "reverse", "final"};
+
+cudaEvent_t take_event(soil_sys* s) {
+    if (s->ev_pool.empty()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        return e;
+    }
+    cudaEvent_t e = s->ev_pool.back();
+    s->ev_pool.pop_back();
+    return e;
+}
+
+void timer_begin(soil_sys* s, int t) {
+    if (!(s->timing_mask & (1u << t))) return;
+    cudaEvent_t e = take_event(s);
+    if (!e) return;
+    cudaEventRecord(e, s->st);
+    s->open_timer = t;
+    s->open_ev = e;
+    s->open_launches = launches_so_far();
+}
+
+void timer_end(soil_sys* s, int t) {
+    if (s->open_timer != t) return;
+    cudaEvent_t e = take_event(s);
+    if (e) {
+        cudaEventRecord(e, s->st);
+        s->spans.push_back({t, s->open_ev, e, launches_so_far() - s->open_launches});
+    } else {
+        s->ev_pool.push_back(s->open_ev);
+    }
+    s->open_timer = -1;
+}
+
+// Fold completed spans into the sums (the stream must be idle).
+void resolve_timers(soil_sys* s) {
+    for (auto& sp : s->spans) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, sp.a, sp.b) == cudaSuccess) {
+            s->timer_ms[sp.timer] += ms;
+            s->timer_launches[sp.timer] += sp.launches;
+            s->timer_intervals[sp.timer] += 1;
+        } else {
+            cudaGetLastError();
+        }
+        s->ev_pool.push_back(sp.a);
+        s->ev_pool.push_back(sp.b);
+    }
+    s->spans.clear();
 }
 
 int sync(soil_sys* s) {
@@ -893,6 +968,7 @@ int full_step(soil_sys* s, bool last) {
         launch_final(s->st, s->nlocal, s->A, s->dt);
         s->pending_final = false;
     }
+    timer_begin(s, T_INTEGRATE);
     TRY(phase_deform(s));
     const bool overwrite = builtin_consumer(s);
     int zp[kMaxPlanes], nz;
@@ -910,6 +986,7 @@ int full_step(soil_sys* s, bool last) {
                        s->dflags);
     s->pending_final = false;
     TRY(check_launch(s));
+    timer_end(s, T_INTEGRATE);
     // decide_rebuild
     if (s->state == COMMUNICATE_ONLY) {
         bool disp = false;
@@ -921,16 +998,34 @@ int full_step(soil_sys* s, bool last) {
         else s->steps_since_build += 1;
     }
     TRY(phase_remove_ghosts(s));
+    timer_begin(s, T_ZERO);
     if (!fused_zero && (nz > 0 || !overwrite)) TRY(phase_zero_forces(s));
+    timer_end(s, T_ZERO);
+    timer_begin(s, T_PBC);
     TRY(phase_pbc(s));
+    timer_end(s, T_PBC);
+    timer_begin(s, T_SORT);
     TRY(phase_sort(s));
+    timer_end(s, T_SORT);
+    timer_begin(s, T_BORDERS);
     TRY(phase_borders(s));
+    timer_end(s, T_BORDERS);
+    timer_begin(s, T_FORWARD);
     if (s->state == COMMUNICATE_ONLY) TRY(forward_comm(s, fused_zero));
+    timer_end(s, T_FORWARD);
+    timer_begin(s, T_NEIGHBOR);
     TRY(phase_neighbor(s));
+    timer_end(s, T_NEIGHBOR);
+    timer_begin(s, T_FORCE);
     TRY(phase_force(s));
+    timer_end(s, T_FORCE);
+    timer_begin(s, T_REVERSE);
     TRY(phase_reverse_comm(s));
+    timer_end(s, T_REVERSE);
     if (last) {
+        timer_begin(s, T_FINAL);
         TRY(phase_final(s));
+        timer_end(s, T_FINAL);
     } else {
         s->pending_final = true;
         s->steps_done += 1;
@@ -1056,6 +1151,8 @@ int soil_sys_destroy(soil_sys* s) {
     for (auto& a : s->send) fr(a);
     fr(s->tile_lo); fr(s->tile_hi); fr(s->tile_off_lo); fr(s->tile_off_hi);
     fr(s->scan_tmp); fr(s->d_stencil); fr(s->stage); fr(s->d_colptrs);
+    resolve_timers(s);
+    for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
     if (s->dflags) dev_free(s, s->dflags, sizeof(DevFlags));
     if (s->hflags) cudaFreeHost(s->hflags);
     if (s->hword) cudaFreeHost(s->hword);
@@ -1352,6 +1449,37 @@ int soil_sys_view(soil_sys* s, soil_dev_view* out) {
     if (!s || !out) return SOIL_ERR_INVALID;
     TRY(flush_pending(s));
     return make_view(s, out);
+}
+
+uint64_t soil_kernel_launches(void) { return launches_so_far(); }
+
+int soil_sys_set_timing(soil_sys* s, uint32_t mask) {
+    if (!s) return SOIL_ERR_INVALID;
+    TRY(sync(s));
+    resolve_timers(s);
+    s->timing_mask = mask;
+    for (int t = 0; t < SOIL_NUM_TIMERS; ++t) {
+        s->timer_ms[t] = 0.0;
+        s->timer_launches[t] = 0;
+        s->timer_intervals[t] = 0;
+    }
+    return SOIL_OK;
+}
+
+int soil_sys_get_timing(soil_sys* s, double* ms, uint64_t* launches, uint64_t* intervals) {
+    if (!s) return SOIL_ERR_INVALID;
+    TRY(sync(s));
+    resolve_timers(s);
+    for (int t = 0; t < SOIL_NUM_TIMERS; ++t) {
+        if (ms) ms[t] = s->timer_ms[t];
+        if (launches) launches[t] = s->timer_launches[t];
+        if (intervals) intervals[t] = s->timer_intervals[t];
+    }
+    return SOIL_OK;
+}
+
+const char* soil_timer_name(int32_t i) {
+    return (i >= 0 && i < SOIL_NUM_TIMERS) ? kTimerNames[i] : "";
 }
 
 }  // extern "C"

@@ -196,6 +196,26 @@ class System:
         self._c(self.lib.soil_sys_get_sort_perm(self.h, _p(perm, C.c_uint32)), "sort_perm")
         return perm
 
+    def read_local_state(self, pos_out, vel_out):
+        """Positions and velocities of the locals into caller arrays ([n][3] f64,
+        pinned or pageable), without other copies."""
+        n = self.counts().nlocal
+        assert pos_out.shape == (n, 3) and vel_out.shape == (n, 3)
+        self._c(self.lib.soil_sys_get_atoms(self.h, 0, n, None, _p(pos_out, C.c_double),
+                                            _p(vel_out, C.c_double), None, None, None),
+                "get_atoms")
+
+    def set_timing(self, mask):
+        self._c(self.lib.soil_sys_set_timing(self.h, mask), "set_timing")
+
+    def get_timing(self):
+        ms = np.zeros(abi.SOIL_NUM_TIMERS)
+        la = np.zeros(abi.SOIL_NUM_TIMERS, np.uint64)
+        iv = np.zeros(abi.SOIL_NUM_TIMERS, np.uint64)
+        self._c(self.lib.soil_sys_get_timing(self.h, _p(ms, C.c_double), _p(la, C.c_uint64),
+                                             _p(iv, C.c_uint64)), "get_timing")
+        return ms, la, iv
+
     def view(self):
         v = abi.SoilDevView()
         self._c(self.lib.soil_sys_view(self.h, C.byref(v)), "view")

@@ -1,0 +1,80 @@
+"""The C ABI library loads without a GPU and matches include/soil_cuda.h.
+
+No compute entry point is called here; only symbol presence, the version
+query, struct layouts and the no-device error path are checked.
+"""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+from soil_b200 import abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "soil_cuda.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(soil_\w+)\s*\(", text, flags=re.M)
+    return sorted(set(n for n in names if not n.startswith("soil_force_fn")))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = abi.load_library()
+    names = declared_functions()
+    assert len(names) >= 40
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_prototype_table_matches_header():
+    assert sorted(abi.PROTOTYPES) == declared_functions()
+
+
+def test_abi_version():
+    assert abi.load_library().soil_abi_version() == 1
+
+
+def test_no_device_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    h = C.c_void_p()
+    st = abi.load_library().soil_ctx_create(0, 0, C.byref(h))
+    assert st == abi.SOIL_ERR_NO_DEVICE and not h.value
+
+
+def test_struct_layouts_match_header(tmp_path):
+    src = tmp_path / "layout.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "soil_cuda.h"
+int main(void) {
+  printf("%zu %zu %zu %zu\n", sizeof(soil_box), sizeof(soil_neigh_cfg), sizeof(soil_counts),
+         sizeof(soil_dev_view));
+  printf("%zu %zu %zu\n", offsetof(soil_neigh_cfg, additive_skin), offsetof(soil_counts, comm_state),
+         offsetof(soil_counts, tilt_xy));
+  printf("%zu %zu\n", offsetof(soil_dev_view, columns), offsetof(soil_dev_view, stream));
+  return 0;
+}
+''')
+    exe = tmp_path / "layout"
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    out = subprocess.check_output([str(exe)]).decode().split()
+    got = [int(x) for x in out]
+    want = [C.sizeof(abi.SoilBox), C.sizeof(abi.SoilNeighCfg), C.sizeof(abi.SoilCounts),
+            C.sizeof(abi.SoilDevView),
+            abi.SoilNeighCfg.additive_skin.offset, abi.SoilCounts.comm_state.offset,
+            abi.SoilCounts.tilt_xy.offset,
+            abi.SoilDevView.columns.offset, abi.SoilDevView.stream.offset]
+    assert got == want
+
+
+def test_missing_library_raises(tmp_path):
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        abi.load_library(str(tmp_path / "nope.so"))
