@@ -233,6 +233,28 @@ int soil_sys_get_sort_perm(soil_sys* sys, uint32_t* perm);
 /* Device pointers for an external consumer (valid until the next rebuild). */
 int soil_sys_view(soil_sys* sys, soil_dev_view* out);
 
+/* Stable counting sort of n positions by bin cell that allocates no device
+ * memory.  This has no counterpart in the reference: it serves hosts that
+ * cannot allocate device memory once they run (a fixed HBM plan, or an
+ * allocator that owns the device), giving the same permutation as the
+ * spatial sort of soil_phase_sort.  The caller passes device arrays d_x,
+ * d_y, d_z (n positions), d_cell (n outputs: the cell of each atom) and
+ * d_perm (n outputs: perm[new] = old, stable inside a cell), plus the bin
+ * grid (origin, bin_size, bin_count; box_lo, box_size, tilt and triclinic
+ * for lamda binning) and a cudaStream_t (NULL = default stream).  Work is
+ * enqueued on `stream`.  Scratch is one 16 MiB static device array per GPU,
+ * held until process exit; grids above 2,097,152 cells return
+ * SOIL_ERR_CAPACITY.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current; make that first
+ * call before any stream capture.  Calls share the array: calls that overlap
+ * on the GPU race and must be serialised.  ctx may be NULL (no message). */
+int soil_bin_sort_noalloc(soil_ctx* ctx, const double* d_x, const double* d_y,
+                          const double* d_z, uint64_t n, const double origin[3],
+                          const double bin_size[3], const int32_t bin_count[3],
+                          const double box_lo[3], const double box_size[3],
+                          const double tilt[3], int32_t triclinic, uint32_t* d_cell,
+                          uint32_t* d_perm, void* stream);
+
 /* ---- instrumentation (no reference counterpart: the reference has only
  * wall-clock thermo columns, soil_print/src/lib.rs:20-26) ------------------ */
 /* Kernels this library has launched in this process. */

@@ -155,6 +155,8 @@ PROTOTYPES = {
     "soil_sys_get_swap": (C.c_int, [P, i32, pu64, pu64, pdbl, pdbl, pu32]),
     "soil_sys_get_sort_perm": (C.c_int, [P, pu32]),
     "soil_sys_view": (C.c_int, [P, C.POINTER(SoilDevView)]),
+    "soil_bin_sort_noalloc": (C.c_int, [P, P, P, P, u64, pdbl, pdbl, pi32, pdbl, pdbl, pdbl, i32,
+                                        P, P, P]),
     "soil_kernel_launches": (C.c_uint64, []),
     "soil_sys_set_timing": (C.c_int, [P, u32]),
     "soil_sys_get_timing": (C.c_int, [P, pdbl, pu64, pu64]),

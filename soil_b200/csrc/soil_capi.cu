@@ -1035,6 +1035,14 @@ int full_step(soil_sys* s, bool last) {
 
 }  // namespace
 
+namespace soil {
+// Records `msg` as the context's last error (ctx may be NULL) and returns status.
+int set_ctx_error(soil_ctx* ctx, int status, const char* msg) {
+    if (ctx) ctx->err = msg;
+    return status;
+}
+}  // namespace soil
+
 // ===========================================================================
 // C ABI
 // ===========================================================================
