@@ -183,40 +183,29 @@ void launch_permute_u32(cudaStream_t st, uint64_t n, const uint32_t* perm, const
 }
 
 // atom_sorted_idx and sorted_pos of bin_neighbor_list (neighbor.rs:1101-1125),
-// plus the sorted cutoffs and the FP32 grid-relative copies the filter reads.
+// as one record {x, y, z, cutoff_radius} per sorted slot, plus the FP32
+// grid-relative copy the FP32 filter reads.
 __global__ void __launch_bounds__(kBlock) k_sorted_views(uint64_t n, const uint32_t* sorted,
-                                                         AtomCols c, uint32_t* asi, double* spx,
-                                                         double* spy, double* spz, double* scut,
-                                                         float* spx32, float* spy32, float* spz32,
-                                                         float* scut32, double o0, double o1,
+                                                         AtomCols c, uint32_t* asi, double4* sp,
+                                                         float4* spf, double o0, double o1,
                                                          double o2) {
     for (uint64_t m = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; m < n;
          m += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t a = sorted[m];
         asi[a] = (uint32_t)m;
-        const double x = c.x[a], y = c.y[a], z = c.z[a];
-        spx[m] = x;
-        spy[m] = y;
-        spz[m] = z;
-        if (scut) scut[m] = c.cut[a];
-        if (spx32) {
-            spx32[m] = (float)(x - o0);
-            spy32[m] = (float)(y - o1);
-            spz32[m] = (float)(z - o2);
-            scut32[m] = (float)c.cut[a];
-        }
+        const double x = c.x[a], y = c.y[a], z = c.z[a], cut = c.cut[a];
+        sp[m] = make_double4(x, y, z, cut);
+        if (spf) spf[m] = make_float4((float)(x - o0), (float)(y - o1), (float)(z - o2), (float)cut);
     }
 }
 
 void launch_sorted_views(cudaStream_t st, uint64_t n, const uint32_t* sorted, const AtomCols& c,
-                         uint32_t* atom_sorted_idx, double* spx, double* spy, double* spz,
-                         double* scut, float* spx32, float* spy32, float* spz32, float* scut32,
+                         uint32_t* atom_sorted_idx, double4* sp, float4* spf,
                          const double origin[3]) {
     if (n == 0) return;
     note_launch();
-    k_sorted_views<<<grid_for(n), kBlock, 0, st>>>(n, sorted, c, atom_sorted_idx, spx, spy, spz,
-                                                   scut, spx32, spy32, spz32, scut32, origin[0],
-                                                   origin[1], origin[2]);
+    k_sorted_views<<<grid_for(n), kBlock, 0, st>>>(n, sorted, c, atom_sorted_idx, sp, spf,
+                                                   origin[0], origin[1], origin[2]);
 }
 
 }  // namespace soil

@@ -3,10 +3,11 @@
 // borders (comm.rs:682-860): for dim in x,y,z the lo swap (shift +L) then
 // the hi swap (shift -L) scan the locals plus the ghosts of earlier dims in
 // index order and append every atom inside the face slab.  The device version
-// is an order-preserving stream compaction: per 2048-atom tile count the lo
-// and hi selections, scan the tile counts, then each tile re-derives its
-// flags, ranks them with a CTA scan and writes the ghosts at their final
-// slots — so ghost order, send lists and recv ranges equal the reference's.
+// is an order-preserving stream compaction: per 512-atom tile count the lo
+// and hi selections (storing each atom's face flags), scan the tile counts,
+// then each tile ranks its flags with a CTA scan and writes the ghosts at
+// their final slots — so ghost order, send lists and recv ranges equal the
+// reference's.
 //
 // forward_comm (comm.rs:400-432): the reference packs pos+offset from the
 // source (a local or an earlier ghost) swap by swap.  Every ghost therefore
@@ -15,8 +16,8 @@
 // ghosts with the exact same additions.
 //
 // reverse_send_force (comm.rs:938-1024): swaps are folded last to first,
-// lo before hi, F[send[k]] += F[recv_start+k]; one launch per swap keeps
-// that order (targets inside a swap are distinct, so no atomics).
+// lo before hi, F[send[k]] += F[recv_start+k].  Per local atom that is a
+// post-order walk of its image tree, done by one thread (see below).
 #include "block_scan.cuh"
 #include "kernels.cuh"
 
@@ -38,9 +39,14 @@ __device__ __forceinline__ void border_flags(const AtomCols& c, const BorderDim&
     hi = v >= bd.thresh_hi;
 }
 
-__global__ void __launch_bounds__(kBlock) k_border_count(uint64_t scan_end, AtomCols c, BorderDim bd,
+// Border state shared by the kernels of one borders pass (device memory):
+//   bs[0..3]   scan_end of dim d (bs[0] = nlocal; bs[d+1] = bs[d] + lo_d + hi_d)
+//   bs[4..6]   lo totals, bs[7..9] hi totals, bs[10] overflow flag
+__global__ void __launch_bounds__(kBlock) k_border_count(uint32_t* bs, uint64_t cap, AtomCols c,
+                                                         BorderDim bd, uint8_t* face,
                                                          uint32_t* tile_lo, uint32_t* tile_hi) {
     __shared__ uint32_t tot;
+    const uint64_t scan_end = bs[bd.dim] < cap ? bs[bd.dim] : cap;  // a short pass is redone
     const uint64_t base = (uint64_t)blockIdx.x * kBorderTile + (uint64_t)threadIdx.x * kBorderItems;
     uint32_t nlo = 0, nhi = 0;
     for (int k = 0; k < kBorderItems; ++k) {
@@ -48,6 +54,7 @@ __global__ void __launch_bounds__(kBlock) k_border_count(uint64_t scan_end, Atom
         if (i >= scan_end) break;
         bool lo, hi;
         border_flags(c, bd, i, lo, hi);
+        face[i] = (uint8_t)((lo ? 1 : 0) | (hi ? 2 : 0));
         nlo += lo;
         nhi += hi;
     }
@@ -57,12 +64,31 @@ __global__ void __launch_bounds__(kBlock) k_border_count(uint64_t scan_end, Atom
     if (threadIdx.x == 0) tile_hi[blockIdx.x] = tot;
 }
 
-void launch_border_count(cudaStream_t st, uint64_t scan_end, const AtomCols& c,
-                         const BorderDim& bd, uint32_t* tile_lo, uint32_t* tile_hi) {
-    const uint64_t tiles = (scan_end + kBorderTile - 1) / kBorderTile;
-    if (tiles == 0) return;
-    note_launch();
-    k_border_count<<<(unsigned)tiles, kBlock, 0, st>>>(scan_end, c, bd, tile_lo, tile_hi);
+// One CTA: exclusive scans of the lo and hi tile counts, the dim's totals and
+// the next dim's scan_end.
+__global__ void __launch_bounds__(kBlock) k_border_scan(uint32_t* bs, int dim, uint32_t ntiles,
+                                                        const uint32_t* tile_lo,
+                                                        const uint32_t* tile_hi, uint32_t* off_lo,
+                                                        uint32_t* off_hi) {
+    __shared__ uint32_t tot;
+    uint32_t carry[2] = {0, 0};
+    for (int h = 0; h < 2; ++h) {
+        const uint32_t* in = h == 0 ? tile_lo : tile_hi;
+        uint32_t* out = h == 0 ? off_lo : off_hi;
+        for (uint32_t b0 = 0; b0 < ntiles; b0 += kBlock) {
+            const uint32_t t = b0 + threadIdx.x;
+            const uint32_t v = t < ntiles ? in[t] : 0u;
+            const uint32_t pre = block_exclusive_scan(v, &tot) + carry[h];
+            if (t < ntiles) out[t] = pre;
+            carry[h] += tot;
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) {
+        bs[4 + dim] = carry[0];
+        bs[7 + dim] = carry[1];
+        bs[dim + 1] = bs[dim] + carry[0] + carry[1];
+    }
 }
 
 // Ghost g := image of atom i through swap `s` (pack_border + unpack_atom,
@@ -107,50 +133,65 @@ __device__ __forceinline__ void write_ghost(const AtomCols& c, uint64_t g, uint6
 }
 
 __global__ void __launch_bounds__(kBlock) k_border_scatter(
-    uint64_t scan_end, uint64_t nlocal, AtomCols c, BorderDim bd, const uint32_t* tile_off_lo,
-    const uint32_t* tile_off_hi, uint64_t recv_lo, uint64_t recv_hi, uint32_t* send_lo,
+    uint32_t* bs, uint64_t nlocal, uint64_t cap, AtomCols c, BorderDim bd, const uint8_t* face,
+    const uint32_t* tile_off_lo, const uint32_t* tile_off_hi, uint32_t* send_lo,
     uint32_t* send_hi, uint32_t* root, uint32_t* chain) {
     __shared__ uint32_t tot;
+    const uint64_t scan_end = bs[bd.dim] < cap ? bs[bd.dim] : cap;
+    const uint64_t recv_lo = bs[bd.dim];
+    const uint64_t recv_hi = scan_end + bs[4 + bd.dim];
     const uint64_t base = (uint64_t)blockIdx.x * kBorderTile + (uint64_t)threadIdx.x * kBorderItems;
     uint32_t flo = 0, fhi = 0;  // bit k: item k selected
     for (int k = 0; k < kBorderItems; ++k) {
         const uint64_t i = base + k;
         if (i >= scan_end) break;
-        bool lo, hi;
-        border_flags(c, bd, i, lo, hi);
-        flo |= (uint32_t)lo << k;
-        fhi |= (uint32_t)hi << k;
+        const uint32_t f = face[i];
+        flo |= (f & 1u) << k;
+        fhi |= ((f >> 1) & 1u) << k;
     }
     uint32_t rlo = block_exclusive_scan(__popc(flo), &tot) + tile_off_lo[blockIdx.x];
     uint32_t rhi = block_exclusive_scan(__popc(fhi), &tot) + tile_off_hi[blockIdx.x];
     for (int k = 0; k < kBorderItems; ++k) {
         const uint64_t i = base + k;
         if ((flo >> k) & 1u) {
-            write_ghost(c, recv_lo + rlo, i, bd.shift[0], bd.vshift[0], bd.swap_id[0], nlocal, root,
-                        chain);
-            send_lo[rlo] = (uint32_t)i;
+            if (recv_lo + rlo < cap) {
+                write_ghost(c, recv_lo + rlo, i, bd.shift[0], bd.vshift[0], bd.swap_id[0], nlocal,
+                            root, chain);
+                send_lo[rlo] = (uint32_t)i;
+            } else {
+                bs[10] = 1u;  // out of capacity: the host grows the arrays and repeats borders
+            }
             ++rlo;
         }
         if ((fhi >> k) & 1u) {
-            write_ghost(c, recv_hi + rhi, i, bd.shift[1], bd.vshift[1], bd.swap_id[1], nlocal, root,
-                        chain);
-            send_hi[rhi] = (uint32_t)i;
+            if (recv_hi + rhi < cap) {
+                write_ghost(c, recv_hi + rhi, i, bd.shift[1], bd.vshift[1], bd.swap_id[1], nlocal,
+                            root, chain);
+                send_hi[rhi] = (uint32_t)i;
+            } else {
+                bs[10] = 1u;
+            }
             ++rhi;
         }
     }
 }
 
-void launch_border_scatter(cudaStream_t st, uint64_t scan_end, uint64_t nlocal, const AtomCols& c,
-                           const BorderDim& bd, const uint32_t* tile_off_lo,
-                           const uint32_t* tile_off_hi, uint64_t recv_lo, uint64_t recv_hi,
-                           uint32_t* send_lo, uint32_t* send_hi, uint32_t* ghost_root,
-                           uint32_t* ghost_chain) {
-    const uint64_t tiles = (scan_end + kBorderTile - 1) / kBorderTile;
-    if (tiles == 0) return;
+// One dim of borders: count, scan, scatter (no host synchronisation).
+void launch_border_dim(cudaStream_t st, uint32_t* bs, uint64_t nlocal, uint64_t cap,
+                       const AtomCols& c, const BorderDim& bd, uint32_t max_tiles,
+                       uint8_t* face_flags, uint32_t* tile_lo, uint32_t* tile_hi,
+                       uint32_t* tile_off_lo, uint32_t* tile_off_hi, uint32_t* send_lo,
+                       uint32_t* send_hi, uint32_t* ghost_root, uint32_t* ghost_chain) {
+    if (max_tiles == 0) return;
     note_launch();
-    k_border_scatter<<<(unsigned)tiles, kBlock, 0, st>>>(scan_end, nlocal, c, bd, tile_off_lo,
-                                                         tile_off_hi, recv_lo, recv_hi, send_lo,
-                                                         send_hi, ghost_root, ghost_chain);
+    k_border_count<<<max_tiles, kBlock, 0, st>>>(bs, cap, c, bd, face_flags, tile_lo, tile_hi);
+    note_launch();
+    k_border_scan<<<1, kBlock, 0, st>>>(bs, bd.dim, max_tiles, tile_lo, tile_hi, tile_off_lo,
+                                        tile_off_hi);
+    note_launch();
+    k_border_scatter<<<max_tiles, kBlock, 0, st>>>(bs, nlocal, cap, c, bd, face_flags, tile_off_lo,
+                                                   tile_off_hi, send_lo, send_hi, ghost_root,
+                                                   ghost_chain);
 }
 
 struct PlaneList {
@@ -205,29 +246,105 @@ void launch_forward(cudaStream_t st, uint64_t nlocal, uint64_t nghost, const Ato
                                                    pl, zero_force ? 1 : 0);
 }
 
-__global__ void __launch_bounds__(kBlock) k_reverse_swap(uint64_t count, uint64_t recv_start,
-                                                         const uint32_t* send, AtomCols c,
-                                                         PlaneList rev) {
-    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < count;
-         k += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t o = send[k];
-        const uint64_t g = recv_start + k;
-        c.fx[o] = c.fx[o] + c.fx[g];
-        c.fy[o] = c.fy[o] + c.fy[g];
-        c.fz[o] = c.fz[o] + c.fz[g];
-        for (int q = 0; q < rev.n; ++q) c.planes[rev.idx[q]][o] = c.planes[rev.idx[q]][o] + c.planes[rev.idx[q]][g];
+// ---- reverse comm as one fold per image tree ------------------------------
+// The reference folds ghost forces swap by swap, last round first, lo before
+// hi: target X receives, in order, its children through swaps 4, 5, 2, 3, 0, 1,
+// each child already holding its own children's folds.  That is a post-order
+// walk of each local atom's image tree with children ordered by that swap
+// priority, so sorting a root's ghosts by a key built from their swap chains
+// (priority per level, 7 past the end) and applying F[origin[g]] += F[g] in
+// key order reproduces every addition of the reference, intermediate ghosts
+// included.
+__device__ __forceinline__ uint32_t fold_key(uint32_t chain) {
+    const uint32_t len = chain >> 12;
+    uint32_t key = 0;
+    for (uint32_t k = 0; k < 3; ++k) {
+        uint32_t pr = 7;
+        if (k < len) {
+            const uint32_t sw = (chain >> (3 * k)) & 7u;
+            pr = (2u - sw / 2u) * 2u + (sw & 1u);  // swaps 4,5,2,3,0,1 -> 0..5
+        }
+        key = key * 8u + pr;
+    }
+    return key;
+}
+
+__global__ void __launch_bounds__(kBlock) k_fold_count(uint64_t nghost, const uint32_t* root,
+                                                       uint32_t* counts) {
+    for (uint64_t gi = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gi < nghost;
+         gi += (uint64_t)gridDim.x * blockDim.x)
+        atomicAdd(&counts[root[gi]], 1u);
+}
+
+__global__ void __launch_bounds__(kBlock) k_fold_scatter(uint64_t nghost, const uint32_t* root,
+                                                         uint32_t* cursor, uint32_t* list) {
+    for (uint64_t gi = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gi < nghost;
+         gi += (uint64_t)gridDim.x * blockDim.x)
+        list[atomicAdd(&cursor[root[gi]], 1u)] = (uint32_t)gi;
+}
+
+// per root: ghosts in post-order (key), ties impossible (one ghost per chain)
+__global__ void __launch_bounds__(kBlock) k_fold_order(uint64_t nlocal, const uint32_t* start,
+                                                       uint32_t* list, const uint32_t* chain) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nlocal;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t b = start[t], e = start[t + 1];
+        for (uint32_t k = b + 1; k < e; ++k) {
+            const uint32_t v = list[k];
+            const uint32_t kv = fold_key(chain[v]);
+            uint32_t j = k;
+            while (j > b && fold_key(chain[list[j - 1]]) > kv) {
+                list[j] = list[j - 1];
+                --j;
+            }
+            list[j] = v;
+        }
     }
 }
 
-void launch_reverse_swap(cudaStream_t st, uint64_t count, uint64_t recv_start,
-                         const uint32_t* send, const AtomCols& c, const int* rev_planes,
-                         int nrev) {
-    if (count == 0) return;
+void launch_fold_build(cudaStream_t st, uint64_t nlocal, uint64_t nghost,
+                       const uint32_t* ghost_root, const uint32_t* ghost_chain, uint32_t* counts,
+                       uint32_t* start, uint32_t* cursor, uint32_t* list, uint32_t* scan_tmp) {
+    cudaMemsetAsync(counts, 0, nlocal * sizeof(uint32_t), st);
+    if (nghost) {
+        note_launch();
+        k_fold_count<<<grid_for(nghost), kBlock, 0, st>>>(nghost, ghost_root, counts);
+    }
+    exclusive_scan_u32(st, counts, start, nlocal, scan_tmp);
+    if (nghost == 0) return;
+    cudaMemcpyAsync(cursor, start, nlocal * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+    note_launch();
+    k_fold_scatter<<<grid_for(nghost), kBlock, 0, st>>>(nghost, ghost_root, cursor, list);
+    note_launch();
+    k_fold_order<<<grid_for(nlocal), kBlock, 0, st>>>(nlocal, start, list, ghost_chain);
+}
+
+__global__ void __launch_bounds__(kBlock) k_reverse_fold(uint64_t nlocal, const uint32_t* start,
+                                                         const uint32_t* list, AtomCols c,
+                                                         PlaneList rev) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nlocal;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t b = start[t], e = start[t + 1];
+        for (uint32_t q = b; q < e; ++q) {
+            const uint64_t g = nlocal + list[q];
+            const uint32_t o = (uint32_t)c.origin[g];
+            c.fx[o] = c.fx[o] + c.fx[g];
+            c.fy[o] = c.fy[o] + c.fy[g];
+            c.fz[o] = c.fz[o] + c.fz[g];
+            for (int k = 0; k < rev.n; ++k)
+                c.planes[rev.idx[k]][o] = c.planes[rev.idx[k]][o] + c.planes[rev.idx[k]][g];
+        }
+    }
+}
+
+void launch_reverse_fold(cudaStream_t st, uint64_t nlocal, const uint32_t* start,
+                         const uint32_t* list, const AtomCols& c, const int* rev_planes, int nrev) {
+    if (nlocal == 0) return;
     PlaneList pl;
     pl.n = nrev;
     for (int k = 0; k < nrev; ++k) pl.idx[k] = rev_planes[k];
     note_launch();
-    k_reverse_swap<<<grid_for(count), kBlock, 0, st>>>(count, recv_start, send, c, pl);
+    k_reverse_fold<<<grid_for(nlocal), kBlock, 0, st>>>(nlocal, start, list, c, pl);
 }
 
 }  // namespace soil

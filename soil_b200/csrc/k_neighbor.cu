@@ -4,10 +4,19 @@
 //
 // Row order is the reference's: the self-cell tail (sorted slots after the
 // atom's own slot), then every forward-stencil cell in stencil order, each
-// cell in sorted (ascending index) order.  A count pass sizes the rows, an
-// exclusive scan gives neighbor_offsets, a fill pass writes the indices.
+// cell in sorted (ascending index) order.
 //
-// Filter: FP64 `fma(dx,dx,fma(dy,dy,dz*dz)) < cut^2` exactly as the
+// Pass 1 (k_pairs_rows): one thread per local row scans its candidates in
+// that order, keeps the first K accepted indices in fixed per-row slots and
+// records the row length.  An exclusive scan of the lengths gives
+// neighbor_offsets; pass 2 (k_pairs_fill) copies every row into place and
+// re-derives, sequentially and in the same order, the rare rows longer than
+// K.  (A warp-per-cell variant with ballot compaction was measured slower:
+// one dependent-load chain per warp, no overlap across rows.)
+//
+// Candidates are read as one 32-byte record {x, y, z, cutoff} per sorted slot
+// (sorted_pos of the reference plus the cutoff radius of the polydisperse
+// test).  Filter: FP64 `fma(dx,dx,fma(dy,dy,dz*dz)) < cut^2` exactly as the
 // reference, or (FP32 mode) a float test on grid-relative coordinates that
 // only REJECTS candidates provably outside the cutoff — the margin eps bounds
 // the float rounding of coordinates, differences and squares — followed by
@@ -16,125 +25,174 @@
 
 namespace soil {
 
-template <bool UNIFORM, bool FP32, bool FILL>
-__global__ void __launch_bounds__(kBlock) k_pairs(uint64_t nlocal, AtomCols c, PairParams p,
-                                                  uint32_t* rowcount, const uint32_t* offsets,
-                                                  uint32_t* indices, DevFlags* flags) {
-    uint64_t n_cand = 0, n_rechk = 0;
-    float lim_uniform = 0.0f;
-    if (UNIFORM && FP32) {
-        const float cut = (float)sqrt(p.cut_sq) + p.eps32;
-        lim_uniform = cut * cut;
+template <bool UNIFORM, bool FP32>
+struct Filter {
+    double cut_sq, sf_sq;
+    float sf32, eps32, lim_uniform;
+
+    __device__ __forceinline__ explicit Filter(const PairParams& p)
+        : cut_sq(p.cut_sq), sf_sq(p.sf_sq), sf32((float)p.sf), eps32(p.eps32), lim_uniform(0.f) {
+        if (UNIFORM && FP32) {
+            const float cut = (float)sqrt(p.cut_sq) + p.eps32;
+            lim_uniform = cut * cut;
+        }
     }
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nlocal;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t my_cell = p.atom_cell[i];
-        const double pix = c.x[i], piy = c.y[i], piz = c.z[i];
-        const double si = c.cut[i];
-        float pix32 = 0.f, piy32 = 0.f, piz32 = 0.f, si32 = 0.f;
+
+    // The reference pair test for the candidate in sorted slot m; *rechk counts
+    // FP64 re-tests in FP32 mode.
+    __device__ __forceinline__ bool operator()(const PairParams& p, const double4& pi,
+                                               const float4& pif, uint32_t m,
+                                               uint32_t* rechk) const {
         if (FP32) {
-            pix32 = (float)(pix - p.origin[0]);
-            piy32 = (float)(piy - p.origin[1]);
-            piz32 = (float)(piz - p.origin[2]);
-            si32 = (float)si;
-        }
-        uint32_t cnt = 0;
-        uint32_t out = FILL ? offsets[i] : 0u;
-
-        auto test = [&](uint32_t m) -> bool {
-            if (FP32) {
-                if (!FILL) ++n_cand;
-                const float dx = p.spx32[m] - pix32;
-                const float dy = p.spy32[m] - piy32;
-                const float dz = p.spz32[m] - piz32;
-                const float r2 = dx * dx + dy * dy + dz * dz;
-                float lim = lim_uniform;
-                if (!UNIFORM) {
-                    const float cu = (si32 + p.scut32[m]) * (float)p.sf + p.eps32;
-                    lim = cu * cu;
-                }
-                if (r2 > lim) return false;
-                if (!FILL) ++n_rechk;
-            } else if (!FILL) {
-                ++n_cand;
+            const float4 q = p.spf[m];
+            const float dx = q.x - pif.x;
+            const float dy = q.y - pif.y;
+            const float dz = q.z - pif.z;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            float lim = lim_uniform;
+            if (!UNIFORM) {
+                const float cu = (pif.w + q.w) * sf32 + eps32;
+                lim = cu * cu;
             }
-            const double dx = p.spx[m] - pix;
-            const double dy = p.spy[m] - piy;
-            const double dz = p.spz[m] - piz;
-            const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
-            if (UNIFORM) return r2 < p.cut_sq;
-            const double sum_skin = si + p.scut[m];
-            return r2 < sum_skin * sum_skin * p.sf_sq;
-        };
-        auto take = [&](uint32_t m) {
-            if (FILL) indices[out++] = p.sorted_atoms[m];
-            else ++cnt;
-        };
-
-        if (p.has_self) {
-            const uint32_t e = p.bin_start[my_cell + 1];
-            if (p.newton) {
-                for (uint32_t m = p.atom_sorted_idx[i] + 1; m < e; ++m)
-                    if (test(m)) take(m);
-            } else {
-                for (uint32_t m = p.bin_start[my_cell]; m < e; ++m) {
-                    if (p.sorted_atoms[m] == (uint32_t)i) continue;
-                    if (test(m)) take(m);
-                }
-            }
+            if (r2 > lim) return false;
+            ++*rechk;
         }
-        for (int s = 0; s < p.nstencil; ++s) {
-            const int32_t off = p.stencil[s];
-            if (!p.newton && off == 0) continue;
-            const uint32_t cc = (uint32_t)((int32_t)my_cell + off);
-            if (cc >= p.ncells) {  // the grid's ghost layers make this unreachable
-                if (flags) atomicOr(&flags->error, 1u);
-                continue;
-            }
-            const uint32_t b = p.bin_start[cc], e = p.bin_start[cc + 1];
-            for (uint32_t m = b; m < e; ++m)
-                if (test(m)) take(m);
-        }
-        if (!FILL) rowcount[i] = cnt;
+        const double4 q = p.sp[m];
+        const double dx = q.x - pi.x;
+        const double dy = q.y - pi.y;
+        const double dz = q.z - pi.z;
+        const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+        if (UNIFORM) return r2 < cut_sq;
+        const double sum_skin = pi.w + q.w;
+        return r2 < sum_skin * sum_skin * sf_sq;
     }
-    if (!FILL) {
-        for (int o = 16; o > 0; o >>= 1) {
-            n_cand += __shfl_down_sync(0xffffffffu, n_cand, o);
-            n_rechk += __shfl_down_sync(0xffffffffu, n_rechk, o);
+};
+
+// Row of local atom i, sequentially in reference order.  FILL writes the
+// indices to out[]; returns the row length.
+template <bool UNIFORM, bool FP32, bool FILL>
+__device__ uint32_t row_scan(const PairParams& p, const Filter<UNIFORM, FP32>& test, uint64_t i,
+                             uint32_t* out, uint32_t cap, uint32_t* rechk, uint32_t* cand,
+                             DevFlags* flags) {
+    const uint32_t my_cell = p.atom_cell[i];
+    const uint32_t mi = p.atom_sorted_idx[i];
+    const double4 pi = p.sp[mi];
+    const float4 pif = FP32 ? p.spf[mi] : make_float4(0.f, 0.f, 0.f, 0.f);
+    uint32_t cnt = 0;
+    if (p.has_self) {
+        const uint32_t e = p.bin_start[my_cell + 1];
+        const uint32_t b = p.newton ? mi + 1 : p.bin_start[my_cell];
+        for (uint32_t m = b; m < e; ++m) {
+            if (!p.newton && m == mi) continue;
+            ++*cand;
+            if (test(p, pi, pif, m, rechk)) {
+                if (FILL && cnt < cap) out[cnt] = p.sorted_atoms[m];
+                ++cnt;
+            }
         }
-        if ((threadIdx.x & 31) == 0) {
-            atomicAdd((unsigned long long*)&flags->candidates, (unsigned long long)n_cand);
-            atomicAdd((unsigned long long*)&flags->rechecked, (unsigned long long)n_rechk);
+    }
+    for (int s = 0; s < p.nstencil; ++s) {
+        const int32_t off = p.stencil[s];
+        if (!p.newton && off == 0) continue;
+        const uint32_t cc = (uint32_t)((int32_t)my_cell + off);
+        if (cc >= p.ncells) {  // the grid's ghost layers make this unreachable
+            if (flags) atomicOr(&flags->error, 1u);
+            continue;
+        }
+        const uint32_t e = p.bin_start[cc + 1];
+        *cand += e - p.bin_start[cc];
+        for (uint32_t m = p.bin_start[cc]; m < e; ++m)
+            if (test(p, pi, pif, m, rechk)) {
+                if (FILL && cnt < cap) out[cnt] = p.sorted_atoms[m];
+                ++cnt;
+            }
+    }
+    return cnt;
+}
+
+// Pass 1: one thread per local row (rows of a warp are neighbours in space, so
+// their candidate records are shared through L1); the first K entries go to
+// the row's slots, the length to rowcount.
+template <bool UNIFORM, bool FP32>
+__global__ void __launch_bounds__(kBlock) k_pairs_rows(PairParams p, uint32_t* rowcount,
+                                                       uint32_t* slots, DevFlags* flags) {
+    const Filter<UNIFORM, FP32> test(p);
+    const uint32_t K = (uint32_t)p.row_slots;
+    uint32_t n_rechk = 0, n_cand32 = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < p.nlocal;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        rowcount[i] = row_scan<UNIFORM, FP32, true>(p, test, i, slots + i * K, K, &n_rechk,
+                                                    &n_cand32, flags);
+    uint64_t n_cand = n_cand32;
+    uint64_t r = n_rechk;
+    for (int o = 16; o > 0; o >>= 1) {
+        n_cand += __shfl_down_sync(0xffffffffu, n_cand, o);
+        r += __shfl_down_sync(0xffffffffu, r, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd((unsigned long long*)&flags->candidates, (unsigned long long)n_cand);
+        atomicAdd((unsigned long long*)&flags->rechecked, (unsigned long long)r);
+    }
+}
+
+// Pass 2: rows into their CSR place; rows longer than K are re-derived.
+template <bool UNIFORM, bool FP32>
+__global__ void __launch_bounds__(kBlock) k_pairs_fill(PairParams p, const uint32_t* rowcount,
+                                                       const uint32_t* slots,
+                                                       const uint32_t* offsets, uint32_t* indices) {
+    const Filter<UNIFORM, FP32> test(p);
+    const uint32_t K = (uint32_t)p.row_slots;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < p.nlocal;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t cnt = rowcount[i];
+        uint32_t* out = indices + offsets[i];
+        if (cnt <= K) {
+            const uint32_t* row = slots + i * K;
+            for (uint32_t k = 0; k < cnt; ++k) out[k] = row[k];
+        } else {
+            uint32_t rk = 0, cd = 0;
+            row_scan<UNIFORM, FP32, true>(p, test, i, out, 0xffffffffu, &rk, &cd, nullptr);
         }
     }
 }
 
-template <bool FILL>
-static void dispatch_pairs(cudaStream_t st, uint64_t nlocal, const AtomCols& c, const PairParams& p,
-                           uint32_t* rowcount, const uint32_t* offsets, uint32_t* indices,
-                           DevFlags* flags) {
-    const unsigned g = grid_for(nlocal);
-    const bool fp32 = p.filter == SOIL_FILTER_FP32_RECHECK;
+template <bool UNIFORM, bool FP32>
+static void launch_pairs_t(cudaStream_t st, const PairParams& p, uint32_t* rowcount,
+                           uint32_t* slots, const uint32_t* offsets, uint32_t* indices,
+                           DevFlags* flags, bool fill) {
     note_launch();
+    if (!fill)
+        k_pairs_rows<UNIFORM, FP32><<<grid_for(p.nlocal), kBlock, 0, st>>>(p, rowcount, slots,
+                                                                            flags);
+    else
+        k_pairs_fill<UNIFORM, FP32><<<grid_for(p.nlocal), kBlock, 0, st>>>(p, rowcount, slots,
+                                                                            offsets, indices);
+}
+
+static void dispatch_pairs(cudaStream_t st, const PairParams& p, uint32_t* rowcount,
+                           uint32_t* slots, const uint32_t* offsets, uint32_t* indices,
+                           DevFlags* flags, bool fill) {
+    const bool fp32 = p.filter == SOIL_FILTER_FP32_RECHECK;
     if (p.uniform) {
-        if (fp32) k_pairs<true, true, FILL><<<g, kBlock, 0, st>>>(nlocal, c, p, rowcount, offsets, indices, flags);
-        else k_pairs<true, false, FILL><<<g, kBlock, 0, st>>>(nlocal, c, p, rowcount, offsets, indices, flags);
+        if (fp32) launch_pairs_t<true, true>(st, p, rowcount, slots, offsets, indices, flags, fill);
+        else launch_pairs_t<true, false>(st, p, rowcount, slots, offsets, indices, flags, fill);
     } else {
-        if (fp32) k_pairs<false, true, FILL><<<g, kBlock, 0, st>>>(nlocal, c, p, rowcount, offsets, indices, flags);
-        else k_pairs<false, false, FILL><<<g, kBlock, 0, st>>>(nlocal, c, p, rowcount, offsets, indices, flags);
+        if (fp32) launch_pairs_t<false, true>(st, p, rowcount, slots, offsets, indices, flags, fill);
+        else launch_pairs_t<false, false>(st, p, rowcount, slots, offsets, indices, flags, fill);
     }
 }
 
-void launch_pair_count(cudaStream_t st, uint64_t nlocal, const AtomCols& c, const PairParams& p,
-                       uint32_t* rowcount, DevFlags* flags) {
-    if (nlocal == 0) return;
-    dispatch_pairs<false>(st, nlocal, c, p, rowcount, nullptr, nullptr, flags);
+void launch_pair_count(cudaStream_t st, const PairParams& p, uint32_t* rowcount, uint32_t* slots,
+                       DevFlags* flags) {
+    if (p.nlocal == 0 || p.ncells == 0) return;
+    dispatch_pairs(st, p, rowcount, slots, nullptr, nullptr, flags, false);
 }
 
-void launch_pair_fill(cudaStream_t st, uint64_t nlocal, const AtomCols& c, const PairParams& p,
-                      const uint32_t* offsets, uint32_t* indices) {
-    if (nlocal == 0) return;
-    dispatch_pairs<true>(st, nlocal, c, p, nullptr, offsets, indices, nullptr);
+void launch_pair_fill(cudaStream_t st, const PairParams& p, const uint32_t* rowcount,
+                      const uint32_t* slots, const uint32_t* offsets, uint32_t* indices) {
+    if (p.nlocal == 0) return;
+    dispatch_pairs(st, p, const_cast<uint32_t*>(rowcount), const_cast<uint32_t*>(slots), offsets,
+                   indices, nullptr, true);
 }
 
 __global__ void __launch_bounds__(kBlock) k_in_count(uint64_t nlocal, const uint32_t* offsets,

@@ -79,10 +79,10 @@ void launch_identity_check(cudaStream_t st, uint64_t n, const uint32_t* perm, De
 // out[k] = cell[perm[k]]
 void launch_permute_u32(cudaStream_t st, uint64_t n, const uint32_t* perm, const uint32_t* in,
                         uint32_t* out);
-// inverse[sorted[m]] = m, sorted positions / cutoffs by bin order
+// inverse[sorted[m]] = m and the sorted records sp[m] = {x, y, z, cutoff}
+// (plus the FP32 grid-relative copy spf when spf != nullptr)
 void launch_sorted_views(cudaStream_t st, uint64_t n, const uint32_t* sorted, const AtomCols& c,
-                         uint32_t* atom_sorted_idx, double* spx, double* spy, double* spz,
-                         double* scut, float* spx32, float* spy32, float* spz32, float* scut32,
+                         uint32_t* atom_sorted_idx, double4* sp, float4* spf,
                          const double origin[3]);
 
 // ---- ghosts (k_ghost.cu) --------------------------------------------------
@@ -96,23 +96,28 @@ struct BorderDim {
     double vshift[2][3];
     int swap_id[2];
 };
-constexpr int kBorderTile = 2048;
-void launch_border_count(cudaStream_t st, uint64_t scan_end, const AtomCols& c,
-                         const BorderDim& bd, uint32_t* tile_lo, uint32_t* tile_hi);
-// Appends the lo ghosts at recv_lo + rank and the hi ghosts at recv_hi + rank.
-void launch_border_scatter(cudaStream_t st, uint64_t scan_end, uint64_t nlocal, const AtomCols& c,
-                           const BorderDim& bd, const uint32_t* tile_off_lo,
-                           const uint32_t* tile_off_hi, uint64_t recv_lo, uint64_t recv_hi,
-                           uint32_t* send_lo, uint32_t* send_hi, uint32_t* ghost_root,
-                           uint32_t* ghost_chain);
+constexpr int kBorderTile = 512;
+// One dim of borders on the device: the dim's scan range and recv offsets are
+// read from bs (see k_ghost.cu); ghosts beyond `cap` set bs[10].
+void launch_border_dim(cudaStream_t st, uint32_t* bs, uint64_t nlocal, uint64_t cap,
+                       const AtomCols& c, const BorderDim& bd, uint32_t max_tiles,
+                       uint8_t* face_flags, uint32_t* tile_lo, uint32_t* tile_hi,
+                       uint32_t* tile_off_lo, uint32_t* tile_off_hi, uint32_t* send_lo,
+                       uint32_t* send_hi, uint32_t* ghost_root, uint32_t* ghost_chain);
+constexpr int kBorderStateWords = 16;
 // forward_comm: every ghost from its root local atom through its swap chain
 void launch_forward(cudaStream_t st, uint64_t nlocal, uint64_t nghost, const AtomCols& c,
                     const uint32_t* ghost_root, const uint32_t* ghost_chain, const SwapConst& sc,
                     const int* fwd_planes, int nfwd, bool zero_force);
-// reverse_accumulate of one swap: F[send[k]] += F[recv_start + k] (+ #[reverse] planes)
-void launch_reverse_swap(cudaStream_t st, uint64_t count, uint64_t recv_start,
-                         const uint32_t* send, const AtomCols& c, const int* rev_planes,
-                         int nrev);
+// Fold program of reverse comm, built after borders: ghosts grouped by root
+// local atom (start[nlocal+1], list[nghost]) in post-order of the swap tree.
+void launch_fold_build(cudaStream_t st, uint64_t nlocal, uint64_t nghost,
+                       const uint32_t* ghost_root, const uint32_t* ghost_chain, uint32_t* counts,
+                       uint32_t* start, uint32_t* cursor, uint32_t* list, uint32_t* scan_tmp);
+// reverse_send_force: F[origin[g]] += F[g] (+ #[reverse] planes) over every
+// root's image tree in fold order
+void launch_reverse_fold(cudaStream_t st, uint64_t nlocal, const uint32_t* start,
+                         const uint32_t* list, const AtomCols& c, const int* rev_planes, int nrev);
 
 // ---- neighbor (k_neighbor.cu) ---------------------------------------------
 struct PairParams {
@@ -120,31 +125,29 @@ struct PairParams {
     const uint32_t* atom_sorted_idx;
     const uint32_t* bin_start;
     const uint32_t* sorted_atoms;
-    const double* spx;
-    const double* spy;
-    const double* spz;
-    const double* scut;   // sorted cutoff radii (polydisperse path)
-    const float* spx32;   // FP32 grid-relative sorted positions (FP32 filter)
-    const float* spy32;
-    const float* spz32;
-    const float* scut32;
+    const double4* sp;    // sorted {x, y, z, cutoff_radius}
+    const float4* spf;    // FP32 grid-relative {x, y, z, cutoff_radius} (FP32 filter)
     const int32_t* stencil;
     int nstencil;
     uint32_t ncells;      // bin_total_cells: stencil cells outside it are skipped and flagged
+    uint64_t nlocal;
     int has_self;
     int newton;
     int uniform;
     int filter;
+    int row_slots;        // K: row entries kept by pass 1 per atom
     double cut_sq;        // uniform: cached_uniform_cutoff_sq
     double sf_sq;         // skin_fraction^2
     double sf;            // skin_fraction
     float eps32;          // FP32 margin
-    double origin[3];     // grid origin used for the FP32 coordinates
 };
-void launch_pair_count(cudaStream_t st, uint64_t nlocal, const AtomCols& c, const PairParams& p,
-                       uint32_t* rowcount, DevFlags* flags);
-void launch_pair_fill(cudaStream_t st, uint64_t nlocal, const AtomCols& c, const PairParams& p,
-                      const uint32_t* offsets, uint32_t* indices);
+// Pass 1: row lengths into rowcount[], the first K entries of each row into
+// slots[i*K ...]; filter statistics into flags.
+void launch_pair_count(cudaStream_t st, const PairParams& p, uint32_t* rowcount, uint32_t* slots,
+                       DevFlags* flags);
+// Pass 2: rows into neighbor_indices at offsets[] (rows longer than K re-derived).
+void launch_pair_fill(cudaStream_t st, const PairParams& p, const uint32_t* rowcount,
+                      const uint32_t* slots, const uint32_t* offsets, uint32_t* indices);
 // incoming (transposed) lists: for each atom j, the rows i with j in row(i)
 void launch_in_count(cudaStream_t st, uint64_t nlocal, const uint32_t* offsets,
                      const uint32_t* indices, uint32_t* incount);

@@ -120,13 +120,16 @@ struct soil_sys {
     DArr<double> lbx, lby, lbz;
     DArr<uint32_t> sort_cell, sort_perm, sorted_local_cell;
     DArr<uint32_t> cell_counts, cell_start, cell_cursor;
-    DArr<uint32_t> atom_cell, sorted_atoms, asi, rowcount, offsets, indices;
-    DArr<double> spx, spy, spz, scut;
-    DArr<float> spx32, spy32, spz32, scut32;
+    DArr<uint32_t> atom_cell, sorted_atoms, asi, rowcount, offsets, indices, row_slots;
+    DArr<double4> sp;
+    DArr<float4> spf;
     DArr<uint32_t> in_count, in_start, in_cursor, in_list;
     DArr<uint32_t> ghost_root, ghost_chain;
+    DArr<uint32_t> fold_count, fold_start, fold_cursor, fold_list;  // reverse-comm fold program
     DArr<uint32_t> send[kNumSwaps];
-    DArr<uint32_t> tile_lo, tile_hi, tile_off_lo, tile_off_hi;
+    DArr<uint32_t> tile_lo, tile_hi, tile_off_lo, tile_off_hi, bstate;
+    DArr<uint8_t> face_flags;
+    uint64_t last_nghost = 0;
     DArr<uint32_t> scan_tmp;
     DArr<int32_t> d_stencil;
     DArr<double> stage;  // host-layout staging for uploads/downloads
@@ -226,6 +229,7 @@ int ensure(soil_sys* s, DArr<T>& a, uint64_t need, uint64_t keep = 0) {
 
 // ---- per-atom columns -------------------------------------------------------
 constexpr int kDoubleCols = 12;  // x y z vx vy vz fx fy fz mass inv_mass cut
+constexpr int kRowSlots = 16;    // neighbor entries per atom kept by the first pair pass
 
 double** dcol(AtomCols& c, int k) {
     double** t[kDoubleCols] = {&c.x, &c.y, &c.z, &c.vx, &c.vy, &c.vz,
@@ -672,13 +676,16 @@ int phase_sort(soil_sys* s) {
 }
 
 int phase_borders(soil_sys* s) {
-    // borders, comm.rs:682-860 (single rank: all six swaps are self-sends)
+    // borders, comm.rs:682-860 (single rank: all six swaps are self-sends).
+    // All three dims run on the device back to back; the host reads the swap
+    // totals once at the end.  If the ghosts did not fit, the arrays grow and
+    // the (deterministic) pass is repeated.
     if (s->state != FULL_REBUILD) return SOIL_OK;
     s->nghost = 0;
-    uint64_t scan_end = s->nlocal, cur = s->nlocal;
     const double gc = s->domain_ghost_cutoff;
+    BorderDim bds[3];
     for (int dim = 0; dim < 3; ++dim) {
-        BorderDim bd;
+        BorderDim& bd = bds[dim];
         bd.dim = dim;
         bd.triclinic = s->triclinic ? 1 : 0;
         bd.geom = geom_of(s);
@@ -700,47 +707,62 @@ int phase_borders(soil_sys* s) {
             for (int d = 0; d < 3; ++d) bd.vshift[sw][d] = dim == 1 ? po * s->bvel[d] : 0.0;
             bd.swap_id[sw] = 2 * dim + sw;
         }
-        const uint64_t tiles = (scan_end + kBorderTile - 1) / kBorderTile;
-        TRY(ensure(s, s->tile_lo, tiles + 2));
-        TRY(ensure(s, s->tile_hi, tiles + 2));
-        TRY(ensure(s, s->tile_off_lo, tiles + 2));
-        TRY(ensure(s, s->tile_off_hi, tiles + 2));
-        TRY(ensure(s, s->scan_tmp, scan_temp_words(tiles + 2)));
-        uint32_t n_lo = 0, n_hi = 0;
-        if (tiles) {
-            launch_border_count(s->st, scan_end, s->A, bd, s->tile_lo.p, s->tile_hi.p);
-            exclusive_scan_u32(s->st, s->tile_lo.p, s->tile_off_lo.p, tiles, s->scan_tmp.p);
-            exclusive_scan_u32(s->st, s->tile_hi.p, s->tile_off_hi.p, tiles, s->scan_tmp.p);
-            CK(cudaMemcpyAsync(&s->hword[0], s->tile_off_lo.p + tiles, 4, cudaMemcpyDeviceToHost, s->st));
-            CK(cudaMemcpyAsync(&s->hword[1], s->tile_off_hi.p + tiles, 4, cudaMemcpyDeviceToHost, s->st));
-            TRY(sync(s));
-            n_lo = s->hword[0];
-            n_hi = s->hword[1];
-        }
-        TRY(grow_atoms(s, cur + n_lo + n_hi, cur));
-        TRY(ensure(s, s->send[2 * dim], (uint64_t)n_lo + 1));
-        TRY(ensure(s, s->send[2 * dim + 1], (uint64_t)n_hi + 1));
-        const uint64_t recv_lo = cur, recv_hi = cur + n_lo;
-        if (n_lo + n_hi)
-            launch_border_scatter(s->st, scan_end, s->nlocal, s->A, bd, s->tile_off_lo.p,
-                                  s->tile_off_hi.p, recv_lo, recv_hi, s->send[2 * dim].p,
-                                  s->send[2 * dim + 1].p, s->ghost_root.p, s->ghost_chain.p);
+    }
+    // room for the ghosts of the last pass plus a margin
+    const uint64_t want = s->nlocal + s->last_nghost + s->last_nghost / 4 + 4096;
+    TRY(grow_atoms(s, want, s->nlocal));
+    TRY(ensure(s, s->bstate, kBorderStateWords));
+    uint32_t* hb = s->hword;
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        const uint64_t cap = s->acap;
+        const uint32_t max_tiles = (uint32_t)((cap + kBorderTile - 1) / kBorderTile);
+        TRY(ensure(s, s->tile_lo, max_tiles + 2));
+        TRY(ensure(s, s->tile_hi, max_tiles + 2));
+        TRY(ensure(s, s->tile_off_lo, max_tiles + 2));
+        TRY(ensure(s, s->tile_off_hi, max_tiles + 2));
+        for (int k = 0; k < kNumSwaps; ++k) TRY(ensure(s, s->send[k], cap + 1));
+        TRY(ensure(s, s->face_flags, cap + 1));
+        uint32_t init[kBorderStateWords] = {};
+        init[0] = (uint32_t)s->nlocal;
+        CK(cudaMemcpyAsync(s->bstate.p, init, sizeof init, cudaMemcpyHostToDevice, s->st));
+        for (int dim = 0; dim < 3; ++dim)
+            launch_border_dim(s->st, s->bstate.p, s->nlocal, cap, s->A, bds[dim], max_tiles,
+                              s->face_flags.p, s->tile_lo.p, s->tile_hi.p, s->tile_off_lo.p,
+                              s->tile_off_hi.p,
+                              s->send[2 * dim].p, s->send[2 * dim + 1].p, s->ghost_root.p,
+                              s->ghost_chain.p);
         TRY(check_launch(s));
+        CK(cudaMemcpyAsync(hb, s->bstate.p, kBorderStateWords * 4, cudaMemcpyDeviceToHost, s->st));
+        TRY(sync(s));
+        if (!hb[10]) break;
+        if (attempt == 3) return fail(s->ctx, SOIL_ERR_CAPACITY, "ghost capacity did not converge");
+        TRY(grow_atoms(s, (uint64_t)hb[3] + 1024, s->nlocal));  // hb[3]: atoms incl. all ghosts
+    }
+    for (int dim = 0; dim < 3; ++dim) {
+        const uint64_t recv_lo = hb[dim], n_lo = hb[4 + dim], n_hi = hb[7 + dim];
         for (int sw = 0; sw < 2; ++sw) {
             SwapHost& h = s->swaps[2 * dim + sw];
-            h.recv_start = sw == 0 ? recv_lo : recv_hi;
+            h.recv_start = sw == 0 ? recv_lo : recv_lo + n_lo;
             h.recv_count = sw == 0 ? n_lo : n_hi;
             for (int d = 0; d < 3; ++d) {
-                h.off[d] = bd.shift[sw][d];
-                h.voff[d] = bd.vshift[sw][d];
+                h.off[d] = bds[dim].shift[sw][d];
+                h.voff[d] = bds[dim].vshift[sw][d];
             }
         }
-        cur += n_lo + n_hi;
-        s->nghost = cur - s->nlocal;
-        scan_end = cur;
     }
+    s->nghost = (uint64_t)hb[3] - s->nlocal;
+    s->last_nghost = s->nghost;
     s->nswaps = kNumSwaps;
-    return SOIL_OK;
+    // fold program of reverse comm for these ghosts
+    const uint64_t nl = s->nlocal;
+    TRY(ensure(s, s->fold_count, nl + 1));
+    TRY(ensure(s, s->fold_start, nl + 2));
+    TRY(ensure(s, s->fold_cursor, nl + 1));
+    TRY(ensure(s, s->fold_list, s->nghost + 1));
+    TRY(ensure(s, s->scan_tmp, scan_temp_words(nl + 2)));
+    launch_fold_build(s->st, nl, s->nghost, s->ghost_root.p, s->ghost_chain.p, s->fold_count.p,
+                      s->fold_start.p, s->fold_cursor.p, s->fold_list.p, s->scan_tmp.p);
+    return check_launch(s);
 }
 
 SwapConst swap_const(const soil_sys* s) {
@@ -811,17 +833,10 @@ int phase_neighbor(soil_sys* s) {
     TRY(ensure(s, s->asi, s->acap));
     TRY(ensure(s, s->rowcount, s->acap));
     TRY(ensure(s, s->offsets, s->acap + 2));
-    TRY(ensure(s, s->spx, s->acap));
-    TRY(ensure(s, s->spy, s->acap));
-    TRY(ensure(s, s->spz, s->acap));
+    TRY(ensure(s, s->sp, s->acap));
     const bool fp32 = s->filter == SOIL_FILTER_FP32_RECHECK;
-    if (!s->has_uniform) TRY(ensure(s, s->scut, s->acap));
-    if (fp32) {
-        TRY(ensure(s, s->spx32, s->acap));
-        TRY(ensure(s, s->spy32, s->acap));
-        TRY(ensure(s, s->spz32, s->acap));
-        TRY(ensure(s, s->scut32, s->acap));
-    }
+    if (fp32) TRY(ensure(s, s->spf, s->acap));
+    TRY(ensure(s, s->row_slots, (uint64_t)nl * kRowSlots + 1));
     TRY(ensure(s, s->cell_counts, nc + 1));
     TRY(ensure(s, s->cell_start, nc + 2));
     TRY(ensure(s, s->cell_cursor, nc + 1));
@@ -845,10 +860,8 @@ int phase_neighbor(soil_sys* s) {
     double M = 0.0;
     for (int d = 0; d < 3; ++d) M = std::fmax(M, s->size[d]);
     M += 2.0 * s->domain_ghost_cutoff + std::fabs(s->tilt[0]) + 4.0 * s->cached_max_cutoff;
-    launch_sorted_views(s->st, total, s->sorted_atoms.p, s->A, s->asi.p, s->spx.p, s->spy.p,
-                        s->spz.p, s->has_uniform ? nullptr : s->scut.p, fp32 ? s->spx32.p : nullptr,
-                        fp32 ? s->spy32.p : nullptr, fp32 ? s->spz32.p : nullptr,
-                        fp32 ? s->scut32.p : nullptr, s->blo);
+    launch_sorted_views(s->st, total, s->sorted_atoms.p, s->A, s->asi.p, s->sp.p,
+                        fp32 ? s->spf.p : nullptr, s->blo);
     const std::vector<int32_t>& sten = s->newton ? s->stencil_fwd : s->stencil;
     TRY(ensure(s, s->d_stencil, sten.size() + 1));
     if (!sten.empty())
@@ -858,17 +871,13 @@ int phase_neighbor(soil_sys* s) {
     p.atom_sorted_idx = s->asi.p;
     p.bin_start = s->cell_start.p;
     p.sorted_atoms = s->sorted_atoms.p;
-    p.spx = s->spx.p;
-    p.spy = s->spy.p;
-    p.spz = s->spz.p;
-    p.scut = s->scut.p;
-    p.spx32 = s->spx32.p;
-    p.spy32 = s->spy32.p;
-    p.spz32 = s->spz32.p;
-    p.scut32 = s->scut32.p;
+    p.sp = s->sp.p;
+    p.spf = s->spf.p;
     p.stencil = s->d_stencil.p;
     p.nstencil = (int)sten.size();
     p.ncells = (uint32_t)nc;
+    p.nlocal = nl;
+    p.row_slots = kRowSlots;
     p.has_self = s->stencil_self ? 1 : 0;
     p.newton = s->newton ? 1 : 0;
     p.uniform = s->has_uniform ? 1 : 0;
@@ -877,10 +886,9 @@ int phase_neighbor(soil_sys* s) {
     p.sf_sq = s->skin_fraction * s->skin_fraction;
     p.sf = s->skin_fraction;
     p.eps32 = (float)(1e-6 * (1.0 + s->cached_max_cutoff) + 4e-7 * M);
-    for (int d = 0; d < 3; ++d) p.origin[d] = s->blo[d];
     CK(cudaMemsetAsync(&s->dflags->candidates, 0, 16, s->st));
     CK(cudaMemsetAsync(&s->dflags->error, 0, 4, s->st));
-    launch_pair_count(s->st, nl, s->A, p, s->rowcount.p, s->dflags);
+    launch_pair_count(s->st, p, s->rowcount.p, s->row_slots.p, s->dflags);
     exclusive_scan_u32(s->st, s->rowcount.p, s->offsets.p, nl, s->scan_tmp.p);
     CK(cudaMemcpyAsync(&s->hword[0], s->offsets.p + nl, 4, cudaMemcpyDeviceToHost, s->st));
     TRY(check_launch(s));
@@ -889,7 +897,7 @@ int phase_neighbor(soil_sys* s) {
     TRY(ensure(s, s->indices, np + 1));
     if (s->hflags->error)
         return fail(s->ctx, SOIL_ERR_INVALID, "neighbor stencil left the bin grid (atom outside the ghost layers)");
-    launch_pair_fill(s->st, nl, s->A, p, s->offsets.p, s->indices.p);
+    launch_pair_fill(s->st, p, s->rowcount.p, s->row_slots.p, s->offsets.p, s->indices.p);
     TRY(check_launch(s));
     s->npairs = np;
     s->rebuilds += 1;
@@ -939,14 +947,10 @@ int phase_force(soil_sys* s) {
 int phase_reverse_comm(soil_sys* s) {
     // reverse_send_force, comm.rs:938-1024: rounds last to first, lo then hi
     if (!s->newton) return SOIL_OK;
+    if (s->nswaps == 0 || s->nghost == 0) return SOIL_OK;
     int rp[kMaxPlanes], nr;
     zero_planes_of(s, SOIL_COL_REVERSE, rp, &nr);
-    for (int end = s->nswaps; end > 0; end -= 2) {
-        const int start = end >= 2 ? end - 2 : 0;
-        for (int k = start; k < end; ++k)
-            launch_reverse_swap(s->st, s->swaps[k].recv_count, s->swaps[k].recv_start, s->send[k].p,
-                                s->A, rp, nr);
-    }
+    launch_reverse_fold(s->st, s->nlocal, s->fold_start.p, s->fold_list.p, s->A, rp, nr);
     return check_launch(s);
 }
 
@@ -1152,12 +1156,13 @@ int soil_sys_destroy(soil_sys* s) {
     fr(s->sort_cell); fr(s->sort_perm); fr(s->sorted_local_cell);
     fr(s->cell_counts); fr(s->cell_start); fr(s->cell_cursor);
     fr(s->atom_cell); fr(s->sorted_atoms); fr(s->asi); fr(s->rowcount); fr(s->offsets); fr(s->indices);
-    fr(s->spx); fr(s->spy); fr(s->spz); fr(s->scut);
-    fr(s->spx32); fr(s->spy32); fr(s->spz32); fr(s->scut32);
+    fr(s->row_slots); fr(s->sp); fr(s->spf);
     fr(s->in_count); fr(s->in_start); fr(s->in_cursor); fr(s->in_list);
     fr(s->ghost_root); fr(s->ghost_chain);
+    fr(s->fold_count); fr(s->fold_start); fr(s->fold_cursor); fr(s->fold_list);
     for (auto& a : s->send) fr(a);
-    fr(s->tile_lo); fr(s->tile_hi); fr(s->tile_off_lo); fr(s->tile_off_hi);
+    fr(s->tile_lo); fr(s->tile_hi); fr(s->tile_off_lo); fr(s->tile_off_hi); fr(s->bstate);
+    fr(s->face_flags);
     fr(s->scan_tmp); fr(s->d_stencil); fr(s->stage); fr(s->d_colptrs);
     resolve_timers(s);
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
