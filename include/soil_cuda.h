@@ -142,6 +142,7 @@ typedef int (*soil_force_fn)(const soil_dev_view* view, void* user);
 
 typedef struct soil_ctx soil_ctx;
 typedef struct soil_sys soil_sys;
+typedef struct soil_batch soil_batch;
 
 /* ---- lifecycle ---------------------------------------------------------- */
 int soil_abi_version(void);
@@ -254,6 +255,29 @@ int soil_bin_sort_noalloc(soil_ctx* ctx, const double* d_x, const double* d_y,
                           const double box_lo[3], const double box_size[3],
                           const double tilt[3], int32_t triclinic, uint32_t* d_cell,
                           uint32_t* d_perm, void* stream);
+
+/* ---- batched stepping (many independent systems, one launch per phase) ----
+ * The reference steps one system per App; soil_batch steps many set-up
+ * systems together, each box through exactly the phases and arithmetic of
+ * soil_step, so every system's trajectory, CSR lists, ghost maps and sort
+ * permutations are bit-identical to stepping it alone.  Members must use the
+ * built-in harmonic consumer (soil_sys_set_harmonic), have no force hook and
+ * no SOIL_COL_ZERO column.  While batched, a system's stream is the batch's
+ * stream; every soil_sys_* readback stays valid between soil_batch_step calls.
+ * Destroying a batched system removes it from its batch first. */
+int soil_batch_create(soil_ctx* ctx, soil_batch** out);
+/* Detaches every member (the systems themselves are not destroyed). */
+int soil_batch_destroy(soil_batch* batch);
+int soil_batch_add(soil_batch* batch, soil_sys* sys);
+int soil_batch_remove(soil_batch* batch, soil_sys* sys);
+int soil_batch_size(soil_batch* batch, uint32_t* nsys);
+/* nsteps timesteps of every member (final half-kick applied after the last). */
+int soil_batch_step(soil_batch* batch, uint64_t nsteps);
+int soil_batch_sync(soil_batch* batch);
+int soil_batch_stream(soil_batch* batch, void** stream);
+/* Batched steps taken, host waits on the device, device bytes of the batch tables. */
+int soil_batch_stats(soil_batch* batch, uint64_t* steps, uint64_t* host_waits,
+                     uint64_t* device_bytes);
 
 /* ---- instrumentation (no reference counterpart: the reference has only
  * wall-clock thermo columns, soil_print/src/lib.rs:20-26) ------------------ */

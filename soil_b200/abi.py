@@ -157,6 +157,15 @@ PROTOTYPES = {
     "soil_sys_view": (C.c_int, [P, C.POINTER(SoilDevView)]),
     "soil_bin_sort_noalloc": (C.c_int, [P, P, P, P, u64, pdbl, pdbl, pi32, pdbl, pdbl, pdbl, i32,
                                         P, P, P]),
+    "soil_batch_create": (C.c_int, [P, PP]),
+    "soil_batch_destroy": (C.c_int, [P]),
+    "soil_batch_add": (C.c_int, [P, P]),
+    "soil_batch_remove": (C.c_int, [P, P]),
+    "soil_batch_size": (C.c_int, [P, pu32]),
+    "soil_batch_step": (C.c_int, [P, u64]),
+    "soil_batch_sync": (C.c_int, [P]),
+    "soil_batch_stream": (C.c_int, [P, PP]),
+    "soil_batch_stats": (C.c_int, [P, pu64, pu64, pu64]),
     "soil_kernel_launches": (C.c_uint64, []),
     "soil_sys_set_timing": (C.c_int, [P, u32]),
     "soil_sys_get_timing": (C.c_int, [P, pdbl, pu64, pu64]),

@@ -1,0 +1,459 @@
+// device_ops.cuh — per-element device operations shared by the single-system
+// kernels and the batched (segmented) kernels, so a box computes exactly the
+// same arithmetic whether it runs alone or inside a batch.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace soil {
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Warp-aggregated increment of counts[key] for the valid lanes.
+__device__ __forceinline__ void aggregated_count(uint32_t* counts, uint32_t key, bool valid) {
+    const uint32_t k = valid ? key : 0xffffffffu;
+    const unsigned peers = __match_any_sync(0xffffffffu, k);
+    const int leader = __ffs(peers) - 1;
+    if (valid && (int)(threadIdx.x & 31) == leader) atomicAdd(&counts[key], (uint32_t)__popc(peers));
+}
+
+// Displacement test of decide_rebuild (displacement_exceeded, fully periodic
+// fast path, neighbor.rs:711-731): nearest image by d - L*round(d/L), FMA sum.
+__device__ __forceinline__ bool moved_too_far(double px, double py, double pz, double qx, double qy,
+                                              double qz, const double box[3], const double ibox[3],
+                                              double thr_sq) {
+    double dx = px - qx, dy = py - qy, dz = pz - qz;
+    dx -= box[0] * round(dx * ibox[0]);
+    dy -= box[1] * round(dy * ibox[1]);
+    dz -= box[2] * round(dz * ibox[2]);
+    return fma(dx, dx, fma(dy, dy, dz * dz)) > thr_sq;
+}
+
+// wrap_periodic, domain.rs:594-605
+__device__ __forceinline__ double wrap1(double p, double low, double sz, int32_t& img) {
+    const double high = low + sz;
+    if (p < low) {
+        img -= 1;
+        return p + sz;
+    }
+    if (p >= high) {
+        img += 1;
+        return p - sz;
+    }
+    return p;
+}
+
+__device__ __forceinline__ void border_flags(const AtomCols& c, const BorderDim& bd, uint64_t i,
+                                             bool& lo, bool& hi) {
+    double v;
+    if (!bd.triclinic) {
+        v = bd.dim == 0 ? c.x[i] : (bd.dim == 1 ? c.y[i] : c.z[i]);
+    } else {  // face test in lamda coordinates (comm.rs:305-327)
+        double l0, l1, l2;
+        x2lamda(bd.geom, c.x[i], c.y[i], c.z[i], l0, l1, l2);
+        v = bd.dim == 0 ? l0 : (bd.dim == 1 ? l1 : l2);
+    }
+    lo = v < bd.thresh_lo;
+    hi = v >= bd.thresh_hi;
+}
+
+// Ghost g := image of atom i through swap `s` (pack_border + unpack_atom,
+// atom.rs:520-553; registry pack_all/unpack_all for every column).
+__device__ __forceinline__ void write_ghost(const AtomCols& c, uint64_t g, uint64_t i,
+                                            const double* shift, const double* vshift, int s,
+                                            uint64_t nlocal, uint32_t* root, uint32_t* chain) {
+    const uint64_t cap = c.cap;
+    c.x[g] = c.x[i] + shift[0];
+    c.y[g] = c.y[i] + shift[1];
+    c.z[g] = c.z[i] + shift[2];
+    c.vx[g] = c.vx[i] + vshift[0];
+    c.vy[g] = c.vy[i] + vshift[1];
+    c.vz[g] = c.vz[i] + vshift[2];
+    c.fx[g] = c.fx[i];
+    c.fy[g] = c.fy[i];
+    c.fz[g] = c.fz[i];
+    const double m = c.mass[i];
+    c.mass[g] = m;
+    c.inv_mass[g] = 1.0 / m;
+    c.cut[g] = c.cut[i];
+    c.tag[g] = c.tag[i];
+    c.type[g] = c.type[i];
+    c.img[g] = c.img[i];
+    c.img[cap + g] = c.img[cap + i];
+    c.img[2 * cap + g] = c.img[2 * cap + i];
+    c.origin[g] = (int32_t)i;
+    for (int q = 0; q < c.nplanes; ++q) c.planes[q][g] = c.planes[q][i];
+    // chain: swap ids in 3-bit fields (application order), length in bits 12-13
+    uint32_t r, code;
+    if (i < nlocal) {
+        r = (uint32_t)i;
+        code = (1u << 12) | (uint32_t)s;
+    } else {
+        r = root[i - nlocal];
+        const uint32_t pc = chain[i - nlocal];
+        const uint32_t len = pc >> 12;
+        code = (pc & 0xfffu) | ((uint32_t)s << (3 * len)) | ((len + 1) << 12);
+    }
+    root[g - nlocal] = r;
+    chain[g - nlocal] = code;
+}
+
+__device__ __forceinline__ uint32_t fold_key(uint32_t chain) {
+    const uint32_t len = chain >> 12;
+    uint32_t key = 0;
+    for (uint32_t k = 0; k < 3; ++k) {
+        uint32_t pr = 7;
+        if (k < len) {
+            const uint32_t sw = (chain >> (3 * k)) & 7u;
+            pr = (2u - sw / 2u) * 2u + (sw & 1u);  // swaps 4,5,2,3,0,1 -> 0..5
+        }
+        key = key * 8u + pr;
+    }
+    return key;
+}
+
+struct PairForce {
+    bool hit;
+    double fx, fy, fz;
+};
+
+__device__ __forceinline__ PairForce pair_force(const AtomCols& c, const double* rad, double K,
+                                                uint32_t i, uint32_t j) {
+    PairForce f;
+    f.hit = false;
+    const double ri = rad[i], rj = rad[j];
+    const double sum_r = ri + rj;
+    const double dx = c.x[j] - c.x[i];
+    const double dy = c.y[j] - c.y[i];
+    const double dz = c.z[j] - c.z[i];
+    const double dist_sq = dx * dx + dy * dy + dz * dz;
+    if (dist_sq >= sum_r * sum_r || dist_sq == 0.0) return f;
+    const double dist = sqrt(dist_sq);
+    const double overlap = sum_r - dist;
+    const double inv_dist = 1.0 / dist;
+    const double fmag = K * overlap;
+    f.hit = true;
+    f.fx = -fmag * dx * inv_dist;
+    f.fy = -fmag * dy * inv_dist;
+    f.fz = -fmag * dz * inv_dist;
+    return f;
+}
+
+template <bool UNIFORM, bool FP32>
+struct Filter {
+    double cut_sq, sf_sq;
+    float sf32, eps32, lim_uniform;
+
+    __device__ __forceinline__ explicit Filter(const PairParams& p)
+        : cut_sq(p.cut_sq), sf_sq(p.sf_sq), sf32((float)p.sf), eps32(p.eps32), lim_uniform(0.f) {
+        if (UNIFORM && FP32) {
+            const float cut = (float)sqrt(p.cut_sq) + p.eps32;
+            lim_uniform = cut * cut;
+        }
+    }
+
+    // The reference pair test for the candidate in sorted slot m; *rechk counts
+    // FP64 re-tests in FP32 mode.
+    __device__ __forceinline__ bool operator()(const PairParams& p, const double4& pi,
+                                               const float4& pif, uint32_t m,
+                                               uint32_t* rechk) const {
+        if (FP32) {
+            const float4 q = p.spf[m];
+            const float dx = q.x - pif.x;
+            const float dy = q.y - pif.y;
+            const float dz = q.z - pif.z;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            float lim = lim_uniform;
+            if (!UNIFORM) {
+                const float cu = (pif.w + q.w) * sf32 + eps32;
+                lim = cu * cu;
+            }
+            if (r2 > lim) return false;
+            ++*rechk;
+        }
+        const double4 q = p.sp[m];
+        const double dx = q.x - pi.x;
+        const double dy = q.y - pi.y;
+        const double dz = q.z - pi.z;
+        const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+        if (UNIFORM) return r2 < cut_sq;
+        const double sum_skin = pi.w + q.w;
+        return r2 < sum_skin * sum_skin * sf_sq;
+    }
+};
+
+// Row of local atom i, sequentially in reference order.  FILL writes the
+// indices to out[]; returns the row length.
+template <bool UNIFORM, bool FP32, bool FILL>
+__device__ uint32_t row_scan(const PairParams& p, const Filter<UNIFORM, FP32>& test, uint64_t i,
+                             uint32_t* out, uint32_t cap, uint32_t* rechk, uint32_t* cand,
+                             DevFlags* flags) {
+    const uint32_t my_cell = p.atom_cell[i];
+    const uint32_t mi = p.atom_sorted_idx[i];
+    const double4 pi = p.sp[mi];
+    const float4 pif = FP32 ? p.spf[mi] : make_float4(0.f, 0.f, 0.f, 0.f);
+    uint32_t cnt = 0;
+    if (p.has_self) {
+        const uint32_t e = p.bin_start[my_cell + 1];
+        const uint32_t b = p.newton ? mi + 1 : p.bin_start[my_cell];
+        for (uint32_t m = b; m < e; ++m) {
+            if (!p.newton && m == mi) continue;
+            ++*cand;
+            if (test(p, pi, pif, m, rechk)) {
+                if (FILL && cnt < cap) out[cnt] = p.sorted_atoms[m];
+                ++cnt;
+            }
+        }
+    }
+    for (int s = 0; s < p.nstencil; ++s) {
+        const int32_t off = p.stencil[s];
+        if (!p.newton && off == 0) continue;
+        const uint32_t cc = (uint32_t)((int32_t)my_cell + off);
+        if (cc >= p.ncells) {  // the grid's ghost layers make this unreachable
+            if (flags) atomicOr(&flags->error, 1u);
+            continue;
+        }
+        const uint32_t e = p.bin_start[cc + 1];
+        *cand += e - p.bin_start[cc];
+        for (uint32_t m = p.bin_start[cc]; m < e; ++m)
+            if (test(p, pi, pif, m, rechk)) {
+                if (FILL && cnt < cap) out[cnt] = p.sorted_atoms[m];
+                ++cnt;
+            }
+    }
+    return cnt;
+}
+
+// ---- per-atom bodies of the kernels ----------------------------------------
+
+// initial_integration (soil_verlet/src/lib.rs:131-162) of atom i, optionally
+// preceded by final_integration of the previous step with the same forces;
+// returns the new position.
+__device__ __forceinline__ void initial_atom(const AtomCols& c, uint64_t i, double dt,
+                                             bool fuse_final, bool zero_force, double& x,
+                                             double& y, double& z) {
+    const double h = 0.5 * dt * c.inv_mass[i];
+    const double fx = c.fx[i], fy = c.fy[i], fz = c.fz[i];
+    double vx = c.vx[i], vy = c.vy[i], vz = c.vz[i];
+    if (fuse_final) {  // final_integration of the previous step, same forces
+        vx = vx + h * fx;
+        vy = vy + h * fy;
+        vz = vz + h * fz;
+    }
+    const double v0 = vx + h * fx;
+    const double v1 = vy + h * fy;
+    const double v2 = vz + h * fz;
+    c.vx[i] = v0;
+    c.vy[i] = v1;
+    c.vz[i] = v2;
+    x = c.x[i] + v0 * dt;
+    y = c.y[i] + v1 * dt;
+    z = c.z[i] + v2 * dt;
+    c.x[i] = x;
+    c.y[i] = y;
+    c.z[i] = z;
+    if (zero_force) {  // zero_all_forces, atom.rs:631-635 (locals part)
+        c.fx[i] = 0.0;
+        c.fy[i] = 0.0;
+        c.fz[i] = 0.0;
+    }
+}
+
+// final_integration, soil_verlet/src/lib.rs:175-194: v += h*F
+__device__ __forceinline__ void final_atom(const AtomCols& c, uint64_t i, double dt) {
+    const double h = 0.5 * dt * c.inv_mass[i];
+    c.vx[i] = c.vx[i] + h * c.fx[i];
+    c.vy[i] = c.vy[i] + h * c.fy[i];
+    c.vz[i] = c.vz[i] + h * c.fz[i];
+}
+
+// pbc fully periodic fast path (domain.rs:626-636) / pbc_triclinic (domain.rs:674-729)
+__device__ __forceinline__ void pbc_atom(const AtomCols& c, uint64_t i, const Geom& g, double bv0,
+                                         double bv1, double bv2) {
+    const uint64_t cap = c.cap;
+    int32_t i0 = c.img[i], i1 = c.img[cap + i], i2 = c.img[2 * cap + i];
+    if (!g.triclinic) {
+        c.x[i] = wrap1(c.x[i], g.lo[0], g.size[0], i0);
+        c.y[i] = wrap1(c.y[i], g.lo[1], g.size[1], i1);
+        c.z[i] = wrap1(c.z[i], g.lo[2], g.size[2], i2);
+    } else {
+        double l0, l1, l2;
+        x2lamda(g, c.x[i], c.y[i], c.z[i], l0, l1, l2);
+        int32_t d0 = 0, d1 = 0, d2 = 0;
+        if (l0 < 0.0) { l0 += 1.0; d0 = -1; } else if (l0 >= 1.0) { l0 -= 1.0; d0 = 1; }
+        if (l1 < 0.0) { l1 += 1.0; d1 = -1; } else if (l1 >= 1.0) { l1 -= 1.0; d1 = 1; }
+        if (l2 < 0.0) { l2 += 1.0; d2 = -1; } else if (l2 >= 1.0) { l2 -= 1.0; d2 = 1; }
+        double rx, ry, rz;
+        lamda2x(g, l0, l1, l2, rx, ry, rz);
+        c.x[i] = rx;
+        c.y[i] = ry;
+        c.z[i] = rz;
+        i0 += d0;
+        i1 += d1;
+        i2 += d2;
+        if (d1 != 0) {  // Lees–Edwards velocity remap
+            const double s = (double)d1;
+            c.vx[i] = c.vx[i] - s * bv0;
+            c.vy[i] = c.vy[i] - s * bv1;
+            c.vz[i] = c.vz[i] - s * bv2;
+        }
+    }
+    c.img[i] = i0;
+    c.img[cap + i] = i1;
+    c.img[2 * cap + i] = i2;
+}
+
+// forward_comm of ghost gi (index nlocal + gi): its root local atom plus the
+// offsets of its swap chain, added in chain order (comm.rs:400-432).
+__device__ __forceinline__ void forward_ghost(const AtomCols& c, uint64_t nlocal, uint64_t gi,
+                                              const uint32_t* root, const uint32_t* chain,
+                                              const SwapConst& sc, const PlaneList& fwd,
+                                              bool zero_force) {
+    const uint64_t g = nlocal + gi;
+    const uint32_t r = root[gi];
+    const uint32_t code = chain[gi];
+    const uint32_t len = code >> 12;
+    double px = c.x[r], py = c.y[r], pz = c.z[r];
+    double vx = c.vx[r], vy = c.vy[r], vz = c.vz[r];
+    for (uint32_t k = 0; k < len; ++k) {
+        const int s = (code >> (3 * k)) & 7;
+        px = px + sc.off[s][0];
+        py = py + sc.off[s][1];
+        pz = pz + sc.off[s][2];
+        vx = vx + sc.voff[s][0];
+        vy = vy + sc.voff[s][1];
+        vz = vz + sc.voff[s][2];
+    }
+    c.x[g] = px;
+    c.y[g] = py;
+    c.z[g] = pz;
+    c.vx[g] = vx;
+    c.vy[g] = vy;
+    c.vz[g] = vz;
+    for (int q = 0; q < fwd.n; ++q) c.planes[fwd.idx[q]][g] = c.planes[fwd.idx[q]][r];
+    if (zero_force) {
+        c.fx[g] = 0.0;
+        c.fy[g] = 0.0;
+        c.fz[g] = 0.0;
+    }
+}
+
+// Force on atom a gathered in the reference's pair order (see k_force.cu).
+__device__ __forceinline__ void harmonic_atom(const AtomCols& c, uint64_t a, uint64_t nlocal,
+                                              const double* rad, double K, int newton,
+                                              const uint32_t* offsets, const uint32_t* indices,
+                                              const uint32_t* in_start, const uint32_t* in_list) {
+    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
+    const bool local = a < nlocal;
+    // reference applies -f to j only when newton || j < nlocal
+    const bool receives = newton || local;
+    uint32_t q = in_start[a];
+    const uint32_t qe = in_start[a + 1];
+    if (receives) {
+        for (; q < qe; ++q) {
+            const uint32_t i = in_list[q];
+            if (i > a) break;  // later rows come after this atom's own row
+            const PairForce f = pair_force(c, rad, K, i, (uint32_t)a);
+            if (f.hit) {
+                Fx = Fx - f.fx;
+                Fy = Fy - f.fy;
+                Fz = Fz - f.fz;
+            }
+        }
+    }
+    if (local) {
+        for (uint32_t p = offsets[a]; p < offsets[a + 1]; ++p) {
+            const PairForce f = pair_force(c, rad, K, (uint32_t)a, indices[p]);
+            if (f.hit) {
+                Fx = Fx + f.fx;
+                Fy = Fy + f.fy;
+                Fz = Fz + f.fz;
+            }
+        }
+    }
+    if (receives) {
+        for (; q < qe; ++q) {
+            const uint32_t i = in_list[q];
+            const PairForce f = pair_force(c, rad, K, i, (uint32_t)a);
+            if (f.hit) {
+                Fx = Fx - f.fx;
+                Fy = Fy - f.fy;
+                Fz = Fz - f.fz;
+            }
+        }
+    }
+    c.fx[a] = Fx;
+    c.fy[a] = Fy;
+    c.fz[a] = Fz;
+}
+
+// reverse_send_force for the image tree of local atom t, in fold order.
+__device__ __forceinline__ void fold_root(const AtomCols& c, uint64_t nlocal, uint64_t t,
+                                          const uint32_t* start, const uint32_t* list,
+                                          const PlaneList& rev) {
+    const uint32_t b = start[t], e = start[t + 1];
+    for (uint32_t q = b; q < e; ++q) {
+        const uint64_t g = nlocal + list[q];
+        const uint32_t o = (uint32_t)c.origin[g];
+        c.fx[o] = c.fx[o] + c.fx[g];
+        c.fy[o] = c.fy[o] + c.fy[g];
+        c.fz[o] = c.fz[o] + c.fz[g];
+        for (int k = 0; k < rev.n; ++k)
+            c.planes[rev.idx[k]][o] = c.planes[rev.idx[k]][o] + c.planes[rev.idx[k]][g];
+    }
+}
+
+// one sorted slot of the neighbor build's bin order (neighbor.rs:1101-1125)
+__device__ __forceinline__ void sorted_view(const AtomCols& c, uint64_t m, const uint32_t* sorted,
+                                            uint32_t* asi, double4* sp, float4* spf, double o0,
+                                            double o1, double o2) {
+    const uint32_t a = sorted[m];
+    asi[a] = (uint32_t)m;
+    const double x = c.x[a], y = c.y[a], z = c.z[a], cut = c.cut[a];
+    sp[m] = make_double4(x, y, z, cut);
+    if (spf) spf[m] = make_float4((float)(x - o0), (float)(y - o1), (float)(z - o2), (float)cut);
+}
+
+// restore ascending order of one segment (the stable counting sort's last step)
+__device__ __forceinline__ void insertion_sort(uint32_t* items, uint32_t b, uint32_t e) {
+    for (uint32_t k = b + 1; k < e; ++k) {
+        const uint32_t v = items[k];
+        uint32_t j = k;
+        while (j > b && items[j - 1] > v) {
+            items[j] = items[j - 1];
+            --j;
+        }
+        items[j] = v;
+    }
+}
+
+// one atom of the spatial sort's permutation gather (atom.rs:479-490)
+__device__ __forceinline__ void perm_gather_atom(const AtomCols& s, const AtomCols& d, uint64_t k,
+                                                 uint32_t p) {
+    const uint64_t cap = s.cap, dcap = d.cap;
+    d.x[k] = s.x[p];
+    d.y[k] = s.y[p];
+    d.z[k] = s.z[p];
+    d.vx[k] = s.vx[p];
+    d.vy[k] = s.vy[p];
+    d.vz[k] = s.vz[p];
+    d.fx[k] = s.fx[p];
+    d.fy[k] = s.fy[p];
+    d.fz[k] = s.fz[p];
+    d.mass[k] = s.mass[p];
+    d.inv_mass[k] = s.inv_mass[p];
+    d.cut[k] = s.cut[p];
+    d.tag[k] = s.tag[p];
+    d.type[k] = s.type[p];
+    d.img[k] = s.img[p];
+    d.img[dcap + k] = s.img[cap + p];
+    d.img[2 * dcap + k] = s.img[2 * cap + p];
+    d.origin[k] = s.origin[p];
+    for (int q = 0; q < s.nplanes; ++q) d.planes[q][k] = s.planes[q][p];
+}
+
+}  // namespace soil

@@ -1,0 +1,546 @@
+// k_batch.cu — segmented kernels of the batched engine (see batch.cuh).
+//
+// Three launch shapes:
+//   element spans   blocks walk the flattened element range in chunks of
+//                   kBlock * kSpanItems, locate the chunk's segment once and
+//                   advance per element (boxes hold hundreds of atoms or more);
+//   segment per CTA exclusive scans, one CTA per box;
+//   tile spans      border tiles, one CTA per tile (the tile's CTA-wide scan
+//                   ranks its ghosts in order).
+// Every element calls the same device function as the single-system kernels.
+#include "batch.cuh"
+#include "block_scan.cuh"
+#include "sys_internal.cuh"
+
+namespace soil {
+
+constexpr int kSpanItems = 4;
+
+__device__ __forceinline__ uint32_t seg_of(const Span& sp, uint64_t g) {
+    uint32_t lo = 0, hi = sp.nseg - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (sp.start[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// f(box, element index inside the box, segment) for every element of the span.
+template <class F>
+__device__ __forceinline__ void for_span(const Span& sp, F f) {
+    __shared__ uint32_t sh_seg;
+    const uint64_t chunk = (uint64_t)blockDim.x * kSpanItems;
+    for (uint64_t g0 = (uint64_t)blockIdx.x * chunk; g0 < sp.total; g0 += (uint64_t)gridDim.x * chunk) {
+        if (threadIdx.x == 0) sh_seg = seg_of(sp, g0);
+        __syncthreads();
+        uint32_t k = sh_seg;
+        __syncthreads();
+        for (int it = 0; it < kSpanItems; ++it) {
+            const uint64_t g = g0 + (uint64_t)it * blockDim.x + threadIdx.x;
+            if (g >= sp.total) break;
+            while (g >= sp.start[k + 1]) ++k;
+            f(sp.box[k], (uint64_t)sp.base[k] + (g - sp.start[k]), k);
+        }
+    }
+}
+
+static unsigned span_grid(const Span& sp) { return grid_for((sp.total + kSpanItems - 1) / kSpanItems); }
+
+#define SPAN_KERNEL(name, ...)                                                        \
+    __global__ void __launch_bounds__(kBlock) name(Span sp, BatchArgs A) {            \
+        for_span(sp, [&](uint32_t b, uint64_t i, uint32_t k) {                        \
+            const BoxDev& D = A.dev[b];                                               \
+            const BoxStep& S = A.step[b];                                             \
+            (void)D;                                                                  \
+            (void)S;                                                                  \
+            (void)k;                                                                  \
+            __VA_ARGS__                                                               \
+        });                                                                           \
+    }
+
+#define SPAN_LAUNCH(fn, kern)                                        \
+    void fn(cudaStream_t st, const Span& sp, const BatchArgs& a) {   \
+        if (sp.total == 0) return;                                   \
+        note_launch();                                               \
+        kern<<<span_grid(sp), kBlock, 0, st>>>(sp, a);               \
+    }
+
+// ---- integrate --------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) kb_initial(Span sp, BatchArgs A) {
+    for_span(sp, [&](uint32_t b, uint64_t i, uint32_t k) {
+        const BoxDev& D = A.dev[b];
+        const BoxStep& S = A.step[b];
+        const uint8_t f = sp.flag[k];
+        const AtomCols& c = D.set[S.post];  // current at the start of a step
+        double x, y, z;
+        initial_atom(c, i, S.dt, (f & 2) != 0, (f & 4) != 0, x, y, z);
+        if ((f & 1) && moved_too_far(x, y, z, D.lbx[i], D.lby[i], D.lbz[i], S.box, S.ibox, S.thr_sq))
+            atomicOr(&A.flags[b].rebuild, 1u);
+    });
+}
+SPAN_LAUNCH(b_initial, kb_initial)
+
+SPAN_KERNEL(kb_final, { final_atom(D.set[S.post], i, S.dt); })
+SPAN_LAUNCH(b_final, kb_final)
+
+// soil_deform/src/lib.rs:568-574 (first shear step)
+SPAN_KERNEL(kb_profile, {
+    const AtomCols& c = D.set[S.post];
+    c.vx[i] = c.vx[i] + D.shear_rate * (c.y[i] - D.yc);
+})
+SPAN_LAUNCH(b_profile, kb_profile)
+
+SPAN_KERNEL(kb_zero_forces, {
+    const AtomCols& c = D.set[S.cur];
+    c.fx[i] = 0.0;
+    c.fy[i] = 0.0;
+    c.fz[i] = 0.0;
+    for (int q = 0; q < D.zero.n; ++q) c.planes[D.zero.idx[q]][i] = 0.0;
+})
+SPAN_LAUNCH(b_zero_forces, kb_zero_forces)
+
+SPAN_KERNEL(kb_pbc, { pbc_atom(D.set[S.cur], i, S.geom, S.bvel[0], S.bvel[1], S.bvel[2]); })
+SPAN_LAUNCH(b_pbc, kb_pbc)
+
+// ---- bins -----------------------------------------------------------------
+__device__ __forceinline__ uint32_t* counts_of(const BoxDev& D, int which) {
+    if (which == BA_IN) return D.in_count;
+    if (which == BA_FOLD) return D.fold_count;
+    return D.cell_counts;
+}
+
+__global__ void __launch_bounds__(kBlock) kb_zero_counts(Span sp, BatchArgs A, int which) {
+    for_span(sp, [&](uint32_t b, uint64_t i, uint32_t) { counts_of(A.dev[b], which)[i] = 0u; });
+}
+void b_zero_counts(cudaStream_t st, const Span& sp, const BatchArgs& a, int which) {
+    if (sp.total == 0) return;
+    note_launch();
+    kb_zero_counts<<<span_grid(sp), kBlock, 0, st>>>(sp, a, which);
+}
+
+__global__ void __launch_bounds__(kBlock) kb_cells(Span sp, BatchArgs A, int neighbor) {
+    for_span(sp, [&](uint32_t b, uint64_t i, uint32_t) {
+        const BoxDev& D = A.dev[b];
+        const BoxStep& S = A.step[b];
+        const AtomCols& c = D.set[neighbor ? S.post : S.cur];
+        const uint32_t cell = cell_of(S.grid, c.x[i], c.y[i], c.z[i]);
+        (neighbor ? D.atom_cell : D.sort_cell)[i] = cell;
+        atomicAdd(&D.cell_counts[cell], 1u);
+    });
+}
+void b_cells(cudaStream_t st, const Span& sp, const BatchArgs& a, bool neighbor) {
+    if (sp.total == 0) return;
+    note_launch();
+    kb_cells<<<span_grid(sp), kBlock, 0, st>>>(sp, a, neighbor ? 1 : 0);
+}
+
+SPAN_KERNEL(kb_copy_count_local_cells, {
+    const uint32_t cell = D.sorted_local_cell[i];
+    D.atom_cell[i] = cell;
+    atomicAdd(&D.cell_counts[cell], 1u);
+})
+SPAN_LAUNCH(b_copy_count_local_cells, kb_copy_count_local_cells)
+
+// One CTA per segment: out = exclusive scan of in over the segment's n
+// elements (out[n] = total), optional cursor copy.
+__global__ void __launch_bounds__(kBlock) kb_scan(Span sp, BatchArgs A, int which) {
+    __shared__ uint32_t tot;
+    for (uint32_t k = blockIdx.x; k < sp.nseg; k += gridDim.x) {
+        const uint32_t b = sp.box[k];
+        const BoxDev& D = A.dev[b];
+        const uint64_t n = sp.start[k + 1] - sp.start[k];
+        const uint32_t* in;
+        uint32_t *out, *cursor;
+        if (which == BA_ROWS) { in = D.rowcount; out = D.offsets; cursor = nullptr; }
+        else if (which == BA_IN) { in = D.in_count; out = D.in_start; cursor = D.in_cursor; }
+        else if (which == BA_FOLD) { in = D.fold_count; out = D.fold_start; cursor = D.fold_cursor; }
+        else { in = D.cell_counts; out = D.cell_start; cursor = D.cell_cursor; }
+        uint32_t carry = 0;
+        for (uint64_t b0 = 0; b0 < n; b0 += kBlock) {
+            const uint64_t t = b0 + threadIdx.x;
+            const uint32_t v = t < n ? in[t] : 0u;
+            const uint32_t pre = block_exclusive_scan(v, &tot) + carry;
+            if (t < n) {
+                out[t] = pre;
+                if (cursor) cursor[t] = pre;
+            }
+            carry += tot;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            out[n] = carry;
+            if (which == BA_ROWS) A.totals[b] = carry;
+        }
+        __syncthreads();
+    }
+}
+void b_scan(cudaStream_t st, const Span& sp, const BatchArgs& a, int which) {
+    if (sp.nseg == 0) return;
+    note_launch();
+    kb_scan<<<sp.nseg < 148u * 8u ? sp.nseg : 148u * 8u, kBlock, 0, st>>>(sp, a, which);
+}
+
+__global__ void __launch_bounds__(kBlock) kb_scatter(Span sp, BatchArgs A, int neighbor) {
+    for_span(sp, [&](uint32_t b, uint64_t i, uint32_t) {
+        const BoxDev& D = A.dev[b];
+        const uint32_t cell = (neighbor ? D.atom_cell : D.sort_cell)[i];
+        (neighbor ? D.sorted_atoms : D.sort_perm)[atomicAdd(&D.cell_cursor[cell], 1u)] = (uint32_t)i;
+    });
+}
+void b_scatter(cudaStream_t st, const Span& sp, const BatchArgs& a, bool neighbor) {
+    if (sp.total == 0) return;
+    note_launch();
+    kb_scatter<<<span_grid(sp), kBlock, 0, st>>>(sp, a, neighbor ? 1 : 0);
+}
+
+__global__ void __launch_bounds__(kBlock) kb_segsort(Span sp, BatchArgs A, int which) {
+    for_span(sp, [&](uint32_t b, uint64_t s, uint32_t) {
+        const BoxDev& D = A.dev[b];
+        if (which == BA_IN) insertion_sort(D.in_list, D.in_start[s], D.in_start[s + 1]);
+        else insertion_sort(which == BA_NEIGH_CELLS ? D.sorted_atoms : D.sort_perm,
+                            D.cell_start[s], D.cell_start[s + 1]);
+    });
+}
+void b_segsort(cudaStream_t st, const Span& sp, const BatchArgs& a, int which) {
+    if (sp.total == 0) return;
+    note_launch();
+    kb_segsort<<<span_grid(sp), kBlock, 0, st>>>(sp, a, which);
+}
+
+SPAN_KERNEL(kb_permute_cells, { D.sorted_local_cell[i] = D.sort_cell[D.sort_perm[i]]; })
+SPAN_LAUNCH(b_permute_cells, kb_permute_cells)
+
+SPAN_KERNEL(kb_identity, {
+    if (D.sort_perm[i] != (uint32_t)i) atomicOr(&A.flags[b].not_identity, 1u);
+})
+SPAN_LAUNCH(b_identity, kb_identity)
+
+SPAN_KERNEL(kb_perm_gather, { perm_gather_atom(D.set[S.cur], D.set[S.post], i, D.sort_perm[i]); })
+SPAN_LAUNCH(b_perm_gather, kb_perm_gather)
+
+// ---- borders ----------------------------------------------------------------
+constexpr int kBorderItemsB = kBorderTile / kBlock;
+
+__device__ __forceinline__ BorderDim border_dim_of(const BoxStep& S, int dim) {
+    BorderDim bd;
+    bd.dim = dim;
+    bd.triclinic = S.geom.triclinic;
+    bd.geom = S.geom;
+    bd.thresh_lo = S.thresh_lo[dim];
+    bd.thresh_hi = S.thresh_hi[dim];
+    return bd;
+}
+
+// Tile spans: one CTA per tile; f(box, tile index, scan_end, cap).
+template <class F>
+__device__ __forceinline__ void for_tiles(const Span& sp, F f) {
+    __shared__ uint32_t sh_seg;
+    for (uint64_t g = blockIdx.x; g < sp.total; g += gridDim.x) {
+        if (threadIdx.x == 0) sh_seg = seg_of(sp, g);
+        __syncthreads();
+        const uint32_t k = sh_seg;
+        __syncthreads();
+        f(sp.box[k], (uint64_t)sp.base[k] + (g - sp.start[k]));
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) kb_border_count(Span sp, BatchArgs A, int dim) {
+    __shared__ uint32_t tot;
+    for_tiles(sp, [&](uint32_t b, uint64_t tile) {
+        const BoxDev& D = A.dev[b];
+        const BoxStep& S = A.step[b];
+        const uint32_t* bs = A.bstate + (uint64_t)b * kBorderStateWords;
+        const uint64_t cap = D.cap;
+        const uint64_t scan_end = bs[dim] < cap ? bs[dim] : cap;
+        const BorderDim bd = border_dim_of(S, dim);
+        const AtomCols& c = D.set[S.post];
+        const uint64_t base = tile * kBorderTile + (uint64_t)threadIdx.x * kBorderItemsB;
+        uint32_t nlo = 0, nhi = 0;
+        for (int q = 0; q < kBorderItemsB; ++q) {
+            const uint64_t i = base + q;
+            if (i >= scan_end) break;
+            bool lo, hi;
+            border_flags(c, bd, i, lo, hi);
+            D.face_flags[i] = (uint8_t)((lo ? 1 : 0) | (hi ? 2 : 0));
+            nlo += lo;
+            nhi += hi;
+        }
+        block_exclusive_scan(nlo, &tot);
+        if (threadIdx.x == 0) D.tile_lo[tile] = tot;
+        block_exclusive_scan(nhi, &tot);
+        if (threadIdx.x == 0) D.tile_hi[tile] = tot;
+    });
+}
+void b_border_count(cudaStream_t st, const Span& sp, const BatchArgs& a, int dim) {
+    if (sp.total == 0) return;
+    note_launch();
+    kb_border_count<<<grid_for(sp.total * kBlock), kBlock, 0, st>>>(sp, a, dim);
+}
+
+__global__ void __launch_bounds__(kBlock) kb_border_scan(Span sp, BatchArgs A, int dim) {
+    __shared__ uint32_t tot;
+    for (uint32_t k = blockIdx.x; k < sp.nseg; k += gridDim.x) {
+        const uint32_t b = sp.box[k];
+        const BoxDev& D = A.dev[b];
+        uint32_t* bs = A.bstate + (uint64_t)b * kBorderStateWords;
+        const uint64_t ntiles = sp.start[k + 1] - sp.start[k];
+        uint32_t carry[2] = {0, 0};
+        for (int h = 0; h < 2; ++h) {
+            const uint32_t* in = h == 0 ? D.tile_lo : D.tile_hi;
+            uint32_t* out = h == 0 ? D.tile_off_lo : D.tile_off_hi;
+            for (uint64_t b0 = 0; b0 < ntiles; b0 += kBlock) {
+                const uint64_t t = b0 + threadIdx.x;
+                const uint32_t v = t < ntiles ? in[t] : 0u;
+                const uint32_t pre = block_exclusive_scan(v, &tot) + carry[h];
+                if (t < ntiles) out[t] = pre;
+                carry[h] += tot;
+                __syncthreads();
+            }
+        }
+        if (threadIdx.x == 0) {
+            bs[4 + dim] = carry[0];
+            bs[7 + dim] = carry[1];
+            bs[dim + 1] = bs[dim] + carry[0] + carry[1];
+        }
+        __syncthreads();
+    }
+}
+void b_border_scan(cudaStream_t st, const Span& sp, const BatchArgs& a, int dim) {
+    if (sp.nseg == 0) return;
+    note_launch();
+    kb_border_scan<<<sp.nseg < 148u * 8u ? sp.nseg : 148u * 8u, kBlock, 0, st>>>(sp, a, dim);
+}
+
+__global__ void __launch_bounds__(kBlock) kb_border_scatter(Span sp, BatchArgs A, int dim) {
+    __shared__ uint32_t tot;
+    for_tiles(sp, [&](uint32_t b, uint64_t tile) {
+        const BoxDev& D = A.dev[b];
+        const BoxStep& S = A.step[b];
+        uint32_t* bs = A.bstate + (uint64_t)b * kBorderStateWords;
+        const uint64_t cap = D.cap;
+        const uint64_t scan_end = bs[dim] < cap ? bs[dim] : cap;
+        const uint64_t recv_lo = bs[dim];
+        const uint64_t recv_hi = recv_lo + bs[4 + dim];
+        const AtomCols& c = D.set[S.post];
+        const uint64_t base = tile * kBorderTile + (uint64_t)threadIdx.x * kBorderItemsB;
+        uint32_t flo = 0, fhi = 0;
+        for (int q = 0; q < kBorderItemsB; ++q) {
+            const uint64_t i = base + q;
+            if (i >= scan_end) break;
+            const uint32_t f = D.face_flags[i];
+            flo |= (f & 1u) << q;
+            fhi |= ((f >> 1) & 1u) << q;
+        }
+        uint32_t rlo = block_exclusive_scan(__popc(flo), &tot) + D.tile_off_lo[tile];
+        uint32_t rhi = block_exclusive_scan(__popc(fhi), &tot) + D.tile_off_hi[tile];
+        const int s_lo = 2 * dim, s_hi = 2 * dim + 1;
+        for (int q = 0; q < kBorderItemsB; ++q) {
+            const uint64_t i = base + q;
+            if ((flo >> q) & 1u) {
+                if (recv_lo + rlo < cap) {
+                    write_ghost(c, recv_lo + rlo, i, S.sc.off[s_lo], S.sc.voff[s_lo], s_lo, S.nlocal,
+                                D.ghost_root, D.ghost_chain);
+                    D.send[s_lo][rlo] = (uint32_t)i;
+                } else {
+                    bs[10] = 1u;
+                }
+                ++rlo;
+            }
+            if ((fhi >> q) & 1u) {
+                if (recv_hi + rhi < cap) {
+                    write_ghost(c, recv_hi + rhi, i, S.sc.off[s_hi], S.sc.voff[s_hi], s_hi, S.nlocal,
+                                D.ghost_root, D.ghost_chain);
+                    D.send[s_hi][rhi] = (uint32_t)i;
+                } else {
+                    bs[10] = 1u;
+                }
+                ++rhi;
+            }
+        }
+    });
+}
+void b_border_scatter(cudaStream_t st, const Span& sp, const BatchArgs& a, int dim) {
+    if (sp.total == 0) return;
+    note_launch();
+    kb_border_scatter<<<grid_for(sp.total * kBlock), kBlock, 0, st>>>(sp, a, dim);
+}
+
+SPAN_KERNEL(kb_fold_count, { atomicAdd(&D.fold_count[D.ghost_root[i]], 1u); })
+SPAN_LAUNCH(b_fold_count, kb_fold_count)
+
+SPAN_KERNEL(kb_fold_scatter, {
+    D.fold_list[atomicAdd(&D.fold_cursor[D.ghost_root[i]], 1u)] = (uint32_t)i;
+})
+SPAN_LAUNCH(b_fold_scatter, kb_fold_scatter)
+
+SPAN_KERNEL(kb_fold_order, {
+    const uint32_t s0 = D.fold_start[i], e = D.fold_start[i + 1];
+    for (uint32_t q = s0 + 1; q < e; ++q) {
+        const uint32_t v = D.fold_list[q];
+        const uint32_t kv = fold_key(D.ghost_chain[v]);
+        uint32_t j = q;
+        while (j > s0 && fold_key(D.ghost_chain[D.fold_list[j - 1]]) > kv) {
+            D.fold_list[j] = D.fold_list[j - 1];
+            --j;
+        }
+        D.fold_list[j] = v;
+    }
+})
+SPAN_LAUNCH(b_fold_order, kb_fold_order)
+
+SPAN_KERNEL(kb_forward, {
+    forward_ghost(D.set[S.post], S.nlocal, i, D.ghost_root, D.ghost_chain, S.sc, D.fwd, false);
+})
+SPAN_LAUNCH(b_forward, kb_forward)
+
+// ---- neighbor build ---------------------------------------------------------
+SPAN_KERNEL(kb_save_positions, {
+    const AtomCols& c = D.set[S.post];
+    D.lbx[i] = c.x[i];
+    D.lby[i] = c.y[i];
+    D.lbz[i] = c.z[i];
+})
+SPAN_LAUNCH(b_save_positions, kb_save_positions)
+
+SPAN_KERNEL(kb_sorted_views, {
+    sorted_view(D.set[S.post], i, D.sorted_atoms, D.asi, D.sp, S.filter ? D.spf : nullptr,
+                S.geom.lo[0], S.geom.lo[1], S.geom.lo[2]);
+})
+SPAN_LAUNCH(b_sorted_views, kb_sorted_views)
+
+__device__ __forceinline__ PairParams pair_params(const BoxDev& D, const BoxStep& S) {
+    PairParams p;
+    p.atom_cell = D.atom_cell;
+    p.atom_sorted_idx = D.asi;
+    p.bin_start = D.cell_start;
+    p.sorted_atoms = D.sorted_atoms;
+    p.sp = D.sp;
+    p.spf = D.spf;
+    p.stencil = S.stencil;
+    p.nstencil = S.nstencil;
+    p.ncells = S.ncells;
+    p.nlocal = S.nlocal;
+    p.has_self = S.has_self;
+    p.newton = S.newton;
+    p.uniform = S.uniform;
+    p.filter = S.filter;
+    p.row_slots = soil_host::kRowSlotsPerAtom;
+    p.cut_sq = S.cut_sq;
+    p.sf_sq = S.sf_sq;
+    p.sf = S.sf;
+    p.eps32 = S.eps32;
+    return p;
+}
+
+template <bool UNIFORM, bool FP32>
+__device__ __forceinline__ void pairs_row(const PairParams& p, uint64_t i, uint32_t* rowcount,
+                                          uint32_t* slots, DevFlags* flags, uint32_t& cd,
+                                          uint32_t& rk) {
+    const Filter<UNIFORM, FP32> test(p);
+    const uint32_t K = (uint32_t)p.row_slots;
+    rowcount[i] = row_scan<UNIFORM, FP32, true>(p, test, i, slots + i * K, K, &rk, &cd, flags);
+}
+
+__device__ __forceinline__ void add_filter_stats(DevFlags* f, uint32_t cd, uint32_t rk) {
+    if (cd) atomicAdd((unsigned long long*)&f->candidates, (unsigned long long)cd);
+    if (rk) atomicAdd((unsigned long long*)&f->rechecked, (unsigned long long)rk);
+}
+
+// Pair count pass over the rows of every box in the span.  The candidate and
+// recheck statistics are summed per box inside each warp (lanes matched by
+// box) before one atomic per box and warp.
+__global__ void __launch_bounds__(kBlock) kb_pairs_rows(Span sp, BatchArgs A) {
+    __shared__ uint32_t sh_seg;
+    const uint64_t chunk = (uint64_t)blockDim.x * kSpanItems;
+    for (uint64_t g0 = (uint64_t)blockIdx.x * chunk; g0 < sp.total; g0 += (uint64_t)gridDim.x * chunk) {
+        if (threadIdx.x == 0) sh_seg = seg_of(sp, g0);
+        __syncthreads();
+        uint32_t k = sh_seg;
+        __syncthreads();
+        uint32_t cur = 0xffffffffu, cd = 0, rk = 0;
+        for (int it = 0; it < kSpanItems; ++it) {
+            const uint64_t g = g0 + (uint64_t)it * blockDim.x + threadIdx.x;
+            if (g >= sp.total) break;
+            while (g >= sp.start[k + 1]) ++k;
+            const uint32_t b = sp.box[k];
+            const uint64_t i = (uint64_t)sp.base[k] + (g - sp.start[k]);
+            if (b != cur) {
+                if (cur != 0xffffffffu) add_filter_stats(A.flags + cur, cd, rk);
+                cur = b;
+                cd = 0;
+                rk = 0;
+            }
+            const BoxDev& D = A.dev[b];
+            const BoxStep& S = A.step[b];
+            const PairParams p = pair_params(D, S);
+            DevFlags* fl = A.flags + b;
+            if (S.uniform) {
+                if (S.filter) pairs_row<true, true>(p, i, D.rowcount, D.row_slots, fl, cd, rk);
+                else pairs_row<true, false>(p, i, D.rowcount, D.row_slots, fl, cd, rk);
+            } else {
+                if (S.filter) pairs_row<false, true>(p, i, D.rowcount, D.row_slots, fl, cd, rk);
+                else pairs_row<false, false>(p, i, D.rowcount, D.row_slots, fl, cd, rk);
+            }
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, cur);
+        const uint32_t scd = __reduce_add_sync(peers, cd);
+        const uint32_t srk = __reduce_add_sync(peers, rk);
+        if (cur != 0xffffffffu && (int)(threadIdx.x & 31) == __ffs(peers) - 1)
+            add_filter_stats(A.flags + cur, scd, srk);
+    }
+}
+SPAN_LAUNCH(b_pairs_rows, kb_pairs_rows)
+
+template <bool UNIFORM, bool FP32>
+__device__ __forceinline__ void fill_row(const PairParams& p, uint64_t i, const uint32_t* rowcount,
+                                         const uint32_t* slots, const uint32_t* offsets,
+                                         uint32_t* indices) {
+    const uint32_t K = (uint32_t)p.row_slots;
+    const uint32_t cnt = rowcount[i];
+    uint32_t* out = indices + offsets[i];
+    if (cnt <= K) {
+        const uint32_t* row = slots + i * K;
+        for (uint32_t q = 0; q < cnt; ++q) out[q] = row[q];
+    } else {
+        const Filter<UNIFORM, FP32> test(p);
+        uint32_t rk = 0, cd = 0;
+        row_scan<UNIFORM, FP32, true>(p, test, i, out, 0xffffffffu, &rk, &cd, nullptr);
+    }
+}
+
+SPAN_KERNEL(kb_pairs_fill, {
+    const PairParams p = pair_params(D, S);
+    if (S.uniform) {
+        if (S.filter) fill_row<true, true>(p, i, D.rowcount, D.row_slots, D.offsets, D.indices);
+        else fill_row<true, false>(p, i, D.rowcount, D.row_slots, D.offsets, D.indices);
+    } else {
+        if (S.filter) fill_row<false, true>(p, i, D.rowcount, D.row_slots, D.offsets, D.indices);
+        else fill_row<false, false>(p, i, D.rowcount, D.row_slots, D.offsets, D.indices);
+    }
+})
+SPAN_LAUNCH(b_pairs_fill, kb_pairs_fill)
+
+SPAN_KERNEL(kb_in_count, {
+    for (uint32_t q = D.offsets[i]; q < D.offsets[i + 1]; ++q) atomicAdd(&D.in_count[D.indices[q]], 1u);
+})
+SPAN_LAUNCH(b_in_count, kb_in_count)
+
+SPAN_KERNEL(kb_in_scatter, {
+    for (uint32_t q = D.offsets[i]; q < D.offsets[i + 1]; ++q)
+        D.in_list[atomicAdd(&D.in_cursor[D.indices[q]], 1u)] = (uint32_t)i;
+})
+SPAN_LAUNCH(b_in_scatter, kb_in_scatter)
+
+// ---- force and reverse comm ---------------------------------------------------
+SPAN_KERNEL(kb_harmonic, {
+    const AtomCols& c = D.set[S.post];
+    harmonic_atom(c, i, S.nlocal, c.planes[D.radius_plane], S.K, S.newton, D.offsets, D.indices,
+                  D.in_start, D.in_list);
+})
+SPAN_LAUNCH(b_harmonic, kb_harmonic)
+
+SPAN_KERNEL(kb_reverse, { fold_root(D.set[S.post], S.nlocal, i, D.fold_start, D.fold_list, D.rev); })
+SPAN_LAUNCH(b_reverse, kb_reverse)
+
+}  // namespace soil

@@ -9,23 +9,10 @@
 // is then arbitrary), and restores the stable order by sorting each cell's
 // segment by atom index.  Cells hold ~2 atoms on average, so that last pass
 // is a short insertion sort per cell.
+#include "device_ops.cuh"
 #include "kernels.cuh"
 
 namespace soil {
-
-__device__ __forceinline__ unsigned lanemask_lt() {
-    unsigned m;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-    return m;
-}
-
-// Warp-aggregated increment of counts[key] for the valid lanes.
-__device__ __forceinline__ void aggregated_count(uint32_t* counts, uint32_t key, bool valid) {
-    const uint32_t k = valid ? key : 0xffffffffu;
-    const unsigned peers = __match_any_sync(0xffffffffu, k);
-    const int leader = __ffs(peers) - 1;
-    if (valid && (int)(threadIdx.x & 31) == leader) atomicAdd(&counts[key], (uint32_t)__popc(peers));
-}
 
 __global__ void __launch_bounds__(kBlock) k_cells(uint64_t first, uint64_t n, AtomCols c, Grid gr,
                                                   uint32_t* cell_out, uint32_t* counts) {
@@ -94,19 +81,8 @@ void launch_scatter(cudaStream_t st, uint64_t n, const uint32_t* cell, uint32_t*
 __global__ void __launch_bounds__(kBlock) k_segsort(uint64_t nseg, const uint32_t* start,
                                                     uint32_t* items) {
     for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < nseg;
-         s += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t b = start[s], e = start[s + 1];
-        if (e - b < 2) continue;
-        for (uint32_t k = b + 1; k < e; ++k) {
-            const uint32_t v = items[k];
-            uint32_t j = k;
-            while (j > b && items[j - 1] > v) {
-                items[j] = items[j - 1];
-                --j;
-            }
-            items[j] = v;
-        }
-    }
+         s += (uint64_t)gridDim.x * blockDim.x)
+        insertion_sort(items, start[s], start[s + 1]);
 }
 
 void launch_segsort(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint32_t* items) {
@@ -119,30 +95,9 @@ void launch_segsort(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint3
 // (atom.rs:479-490, 284-289): every column gathered through perm.
 __global__ void __launch_bounds__(kBlock) k_perm_gather(uint64_t n, const uint32_t* perm,
                                                         AtomCols s, AtomCols d) {
-    const uint64_t cap = s.cap, dcap = d.cap;
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n;
-         k += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t p = perm[k];
-        d.x[k] = s.x[p];
-        d.y[k] = s.y[p];
-        d.z[k] = s.z[p];
-        d.vx[k] = s.vx[p];
-        d.vy[k] = s.vy[p];
-        d.vz[k] = s.vz[p];
-        d.fx[k] = s.fx[p];
-        d.fy[k] = s.fy[p];
-        d.fz[k] = s.fz[p];
-        d.mass[k] = s.mass[p];
-        d.inv_mass[k] = s.inv_mass[p];
-        d.cut[k] = s.cut[p];
-        d.tag[k] = s.tag[p];
-        d.type[k] = s.type[p];
-        d.img[k] = s.img[p];
-        d.img[dcap + k] = s.img[cap + p];
-        d.img[2 * dcap + k] = s.img[2 * cap + p];
-        d.origin[k] = s.origin[p];
-        for (int q = 0; q < s.nplanes; ++q) d.planes[q][k] = s.planes[q][p];
-    }
+         k += (uint64_t)gridDim.x * blockDim.x)
+        perm_gather_atom(s, d, k, perm[k]);
 }
 
 void launch_perm_gather(cudaStream_t st, uint64_t n, const uint32_t* perm, const AtomCols& src,
@@ -190,13 +145,8 @@ __global__ void __launch_bounds__(kBlock) k_sorted_views(uint64_t n, const uint3
                                                          float4* spf, double o0, double o1,
                                                          double o2) {
     for (uint64_t m = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; m < n;
-         m += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t a = sorted[m];
-        asi[a] = (uint32_t)m;
-        const double x = c.x[a], y = c.y[a], z = c.z[a], cut = c.cut[a];
-        sp[m] = make_double4(x, y, z, cut);
-        if (spf) spf[m] = make_float4((float)(x - o0), (float)(y - o1), (float)(z - o2), (float)cut);
-    }
+         m += (uint64_t)gridDim.x * blockDim.x)
+        sorted_view(c, m, sorted, asi, sp, spf, o0, o1, o2);
 }
 
 void launch_sorted_views(cudaStream_t st, uint64_t n, const uint32_t* sorted, const AtomCols& c,

@@ -19,25 +19,12 @@
 // lo before hi, F[send[k]] += F[recv_start+k].  Per local atom that is a
 // post-order walk of its image tree, done by one thread (see below).
 #include "block_scan.cuh"
+#include "device_ops.cuh"
 #include "kernels.cuh"
 
 namespace soil {
 
 constexpr int kBorderItems = kBorderTile / kBlock;
-
-__device__ __forceinline__ void border_flags(const AtomCols& c, const BorderDim& bd, uint64_t i,
-                                             bool& lo, bool& hi) {
-    double v;
-    if (!bd.triclinic) {
-        v = bd.dim == 0 ? c.x[i] : (bd.dim == 1 ? c.y[i] : c.z[i]);
-    } else {  // face test in lamda coordinates (comm.rs:305-327)
-        double l0, l1, l2;
-        x2lamda(bd.geom, c.x[i], c.y[i], c.z[i], l0, l1, l2);
-        v = bd.dim == 0 ? l0 : (bd.dim == 1 ? l1 : l2);
-    }
-    lo = v < bd.thresh_lo;
-    hi = v >= bd.thresh_hi;
-}
 
 // Border state shared by the kernels of one borders pass (device memory):
 //   bs[0..3]   scan_end of dim d (bs[0] = nlocal; bs[d+1] = bs[d] + lo_d + hi_d)
@@ -89,47 +76,6 @@ __global__ void __launch_bounds__(kBlock) k_border_scan(uint32_t* bs, int dim, u
         bs[7 + dim] = carry[1];
         bs[dim + 1] = bs[dim] + carry[0] + carry[1];
     }
-}
-
-// Ghost g := image of atom i through swap `s` (pack_border + unpack_atom,
-// atom.rs:520-553; registry pack_all/unpack_all for every column).
-__device__ __forceinline__ void write_ghost(const AtomCols& c, uint64_t g, uint64_t i,
-                                            const double* shift, const double* vshift, int s,
-                                            uint64_t nlocal, uint32_t* root, uint32_t* chain) {
-    const uint64_t cap = c.cap;
-    c.x[g] = c.x[i] + shift[0];
-    c.y[g] = c.y[i] + shift[1];
-    c.z[g] = c.z[i] + shift[2];
-    c.vx[g] = c.vx[i] + vshift[0];
-    c.vy[g] = c.vy[i] + vshift[1];
-    c.vz[g] = c.vz[i] + vshift[2];
-    c.fx[g] = c.fx[i];
-    c.fy[g] = c.fy[i];
-    c.fz[g] = c.fz[i];
-    const double m = c.mass[i];
-    c.mass[g] = m;
-    c.inv_mass[g] = 1.0 / m;
-    c.cut[g] = c.cut[i];
-    c.tag[g] = c.tag[i];
-    c.type[g] = c.type[i];
-    c.img[g] = c.img[i];
-    c.img[cap + g] = c.img[cap + i];
-    c.img[2 * cap + g] = c.img[2 * cap + i];
-    c.origin[g] = (int32_t)i;
-    for (int q = 0; q < c.nplanes; ++q) c.planes[q][g] = c.planes[q][i];
-    // chain: swap ids in 3-bit fields (application order), length in bits 12-13
-    uint32_t r, code;
-    if (i < nlocal) {
-        r = (uint32_t)i;
-        code = (1u << 12) | (uint32_t)s;
-    } else {
-        r = root[i - nlocal];
-        const uint32_t pc = chain[i - nlocal];
-        const uint32_t len = pc >> 12;
-        code = (pc & 0xfffu) | ((uint32_t)s << (3 * len)) | ((len + 1) << 12);
-    }
-    root[g - nlocal] = r;
-    chain[g - nlocal] = code;
 }
 
 __global__ void __launch_bounds__(kBlock) k_border_scatter(
@@ -194,44 +140,12 @@ void launch_border_dim(cudaStream_t st, uint32_t* bs, uint64_t nlocal, uint64_t 
                                                    ghost_chain);
 }
 
-struct PlaneList {
-    int idx[kMaxPlanes];
-    int n;
-};
-
 __global__ void __launch_bounds__(kBlock) k_forward(uint64_t nlocal, uint64_t nghost, AtomCols c,
                                                     const uint32_t* root, const uint32_t* chain,
                                                     SwapConst sc, PlaneList fwd, int zero_force) {
     for (uint64_t gi = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gi < nghost;
-         gi += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t g = nlocal + gi;
-        const uint32_t r = root[gi];
-        const uint32_t code = chain[gi];
-        const uint32_t len = code >> 12;
-        double px = c.x[r], py = c.y[r], pz = c.z[r];
-        double vx = c.vx[r], vy = c.vy[r], vz = c.vz[r];
-        for (uint32_t k = 0; k < len; ++k) {
-            const int s = (code >> (3 * k)) & 7;
-            px = px + sc.off[s][0];
-            py = py + sc.off[s][1];
-            pz = pz + sc.off[s][2];
-            vx = vx + sc.voff[s][0];
-            vy = vy + sc.voff[s][1];
-            vz = vz + sc.voff[s][2];
-        }
-        c.x[g] = px;
-        c.y[g] = py;
-        c.z[g] = pz;
-        c.vx[g] = vx;
-        c.vy[g] = vy;
-        c.vz[g] = vz;
-        for (int q = 0; q < fwd.n; ++q) c.planes[fwd.idx[q]][g] = c.planes[fwd.idx[q]][r];
-        if (zero_force) {
-            c.fx[g] = 0.0;
-            c.fy[g] = 0.0;
-            c.fz[g] = 0.0;
-        }
-    }
+         gi += (uint64_t)gridDim.x * blockDim.x)
+        forward_ghost(c, nlocal, gi, root, chain, sc, fwd, zero_force != 0);
 }
 
 void launch_forward(cudaStream_t st, uint64_t nlocal, uint64_t nghost, const AtomCols& c,
@@ -255,20 +169,6 @@ void launch_forward(cudaStream_t st, uint64_t nlocal, uint64_t nghost, const Ato
 // (priority per level, 7 past the end) and applying F[origin[g]] += F[g] in
 // key order reproduces every addition of the reference, intermediate ghosts
 // included.
-__device__ __forceinline__ uint32_t fold_key(uint32_t chain) {
-    const uint32_t len = chain >> 12;
-    uint32_t key = 0;
-    for (uint32_t k = 0; k < 3; ++k) {
-        uint32_t pr = 7;
-        if (k < len) {
-            const uint32_t sw = (chain >> (3 * k)) & 7u;
-            pr = (2u - sw / 2u) * 2u + (sw & 1u);  // swaps 4,5,2,3,0,1 -> 0..5
-        }
-        key = key * 8u + pr;
-    }
-    return key;
-}
-
 __global__ void __launch_bounds__(kBlock) k_fold_count(uint64_t nghost, const uint32_t* root,
                                                        uint32_t* counts) {
     for (uint64_t gi = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gi < nghost;
@@ -323,18 +223,8 @@ __global__ void __launch_bounds__(kBlock) k_reverse_fold(uint64_t nlocal, const 
                                                          const uint32_t* list, AtomCols c,
                                                          PlaneList rev) {
     for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nlocal;
-         t += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t b = start[t], e = start[t + 1];
-        for (uint32_t q = b; q < e; ++q) {
-            const uint64_t g = nlocal + list[q];
-            const uint32_t o = (uint32_t)c.origin[g];
-            c.fx[o] = c.fx[o] + c.fx[g];
-            c.fy[o] = c.fy[o] + c.fy[g];
-            c.fz[o] = c.fz[o] + c.fz[g];
-            for (int k = 0; k < rev.n; ++k)
-                c.planes[rev.idx[k]][o] = c.planes[rev.idx[k]][o] + c.planes[rev.idx[k]][g];
-        }
-    }
+         t += (uint64_t)gridDim.x * blockDim.x)
+        fold_root(c, nlocal, t, start, list, rev);
 }
 
 void launch_reverse_fold(cudaStream_t st, uint64_t nlocal, const uint32_t* start,

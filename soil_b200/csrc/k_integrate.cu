@@ -5,6 +5,7 @@
 // one thread per atom, grid-stride, coalesced 8-byte accesses.
 #include <atomic>
 
+#include "device_ops.cuh"
 #include "kernels.cuh"
 
 namespace soil {
@@ -18,18 +19,6 @@ unsigned grid_for(uint64_t n, int block, int per_sm) {
     uint64_t cap = 148ull * per_sm;
     if (need < 1) need = 1;
     return (unsigned)(need < cap ? need : cap);
-}
-
-// Displacement test of decide_rebuild (displacement_exceeded, fully periodic
-// fast path, neighbor.rs:711-731): nearest image by d - L*round(d/L), FMA sum.
-__device__ __forceinline__ bool moved_too_far(double px, double py, double pz, double qx, double qy,
-                                              double qz, const double box[3], const double ibox[3],
-                                              double thr_sq) {
-    double dx = px - qx, dy = py - qy, dz = pz - qz;
-    dx -= box[0] * round(dx * ibox[0]);
-    dy -= box[1] * round(dy * ibox[1]);
-    dz -= box[2] * round(dz * ibox[2]);
-    return fma(dx, dx, fma(dy, dy, dz * dz)) > thr_sq;
 }
 
 struct CheckArgs {
@@ -51,31 +40,8 @@ __global__ void __launch_bounds__(kBlock) k_initial(uint64_t n, AtomCols c, doub
     bool hit = false;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x) {
-        const double h = 0.5 * dt * c.inv_mass[i];
-        const double fx = c.fx[i], fy = c.fy[i], fz = c.fz[i];
-        double vx = c.vx[i], vy = c.vy[i], vz = c.vz[i];
-        if (FUSE_FINAL) {  // final_integration of the previous step, same forces
-            vx = vx + h * fx;
-            vy = vy + h * fy;
-            vz = vz + h * fz;
-        }
-        const double v0 = vx + h * fx;
-        const double v1 = vy + h * fy;
-        const double v2 = vz + h * fz;
-        c.vx[i] = v0;
-        c.vy[i] = v1;
-        c.vz[i] = v2;
-        const double x = c.x[i] + v0 * dt;
-        const double y = c.y[i] + v1 * dt;
-        const double z = c.z[i] + v2 * dt;
-        c.x[i] = x;
-        c.y[i] = y;
-        c.z[i] = z;
-        if (zero_force) {  // zero_all_forces, atom.rs:631-635 (locals part)
-            c.fx[i] = 0.0;
-            c.fy[i] = 0.0;
-            c.fz[i] = 0.0;
-        }
+        double x, y, z;
+        initial_atom(c, i, dt, FUSE_FINAL, zero_force != 0, x, y, z);
         if (i < ck.n_check)
             hit |= moved_too_far(x, y, z, ck.lbx[i], ck.lby[i], ck.lbz[i], ck.box, ck.ibox, ck.thr_sq);
     }
@@ -124,12 +90,8 @@ void launch_final_initial(cudaStream_t st, uint64_t n, const AtomCols& c, double
 // final_integration, soil_verlet/src/lib.rs:175-194: v += h*F
 __global__ void __launch_bounds__(kBlock) k_final(uint64_t n, AtomCols c, double dt) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        const double h = 0.5 * dt * c.inv_mass[i];
-        c.vx[i] = c.vx[i] + h * c.fx[i];
-        c.vy[i] = c.vy[i] + h * c.fy[i];
-        c.vz[i] = c.vz[i] + h * c.fz[i];
-    }
+         i += (uint64_t)gridDim.x * blockDim.x)
+        final_atom(c, i, dt);
 }
 
 void launch_final(cudaStream_t st, uint64_t n, const AtomCols& c, double dt) {
@@ -138,12 +100,7 @@ void launch_final(cudaStream_t st, uint64_t n, const AtomCols& c, double dt) {
     k_final<<<grid_for(n), kBlock, 0, st>>>(n, c, dt);
 }
 
-struct ZeroPlanes {
-    int idx[kMaxPlanes];
-    int n;
-};
-
-__global__ void __launch_bounds__(kBlock) k_zero(uint64_t n, AtomCols c, ZeroPlanes zp) {
+__global__ void __launch_bounds__(kBlock) k_zero(uint64_t n, AtomCols c, PlaneList zp) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x) {
         c.fx[i] = 0.0;
@@ -156,64 +113,19 @@ __global__ void __launch_bounds__(kBlock) k_zero(uint64_t n, AtomCols c, ZeroPla
 void launch_zero_forces(cudaStream_t st, uint64_t n, const AtomCols& c, const int* zero_planes,
                         int nzero) {
     if (n == 0) return;
-    ZeroPlanes zp;
+    PlaneList zp;
     zp.n = nzero;
     for (int k = 0; k < nzero; ++k) zp.idx[k] = zero_planes[k];
     note_launch();
     k_zero<<<grid_for(n), kBlock, 0, st>>>(n, c, zp);
 }
 
-// wrap_periodic, domain.rs:594-605
-__device__ __forceinline__ double wrap1(double p, double low, double sz, int32_t& img) {
-    const double high = low + sz;
-    if (p < low) {
-        img -= 1;
-        return p + sz;
-    }
-    if (p >= high) {
-        img += 1;
-        return p - sz;
-    }
-    return p;
-}
-
 // pbc fully periodic fast path (domain.rs:626-636) / pbc_triclinic (domain.rs:674-729)
 __global__ void __launch_bounds__(kBlock) k_pbc(uint64_t n, AtomCols c, Geom g, double bv0,
                                                 double bv1, double bv2) {
-    const uint64_t cap = c.cap;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        int32_t i0 = c.img[i], i1 = c.img[cap + i], i2 = c.img[2 * cap + i];
-        if (!g.triclinic) {
-            c.x[i] = wrap1(c.x[i], g.lo[0], g.size[0], i0);
-            c.y[i] = wrap1(c.y[i], g.lo[1], g.size[1], i1);
-            c.z[i] = wrap1(c.z[i], g.lo[2], g.size[2], i2);
-        } else {
-            double l0, l1, l2;
-            x2lamda(g, c.x[i], c.y[i], c.z[i], l0, l1, l2);
-            int32_t d0 = 0, d1 = 0, d2 = 0;
-            if (l0 < 0.0) { l0 += 1.0; d0 = -1; } else if (l0 >= 1.0) { l0 -= 1.0; d0 = 1; }
-            if (l1 < 0.0) { l1 += 1.0; d1 = -1; } else if (l1 >= 1.0) { l1 -= 1.0; d1 = 1; }
-            if (l2 < 0.0) { l2 += 1.0; d2 = -1; } else if (l2 >= 1.0) { l2 -= 1.0; d2 = 1; }
-            double rx, ry, rz;
-            lamda2x(g, l0, l1, l2, rx, ry, rz);
-            c.x[i] = rx;
-            c.y[i] = ry;
-            c.z[i] = rz;
-            i0 += d0;
-            i1 += d1;
-            i2 += d2;
-            if (d1 != 0) {  // Lees–Edwards velocity remap
-                const double s = (double)d1;
-                c.vx[i] = c.vx[i] - s * bv0;
-                c.vy[i] = c.vy[i] - s * bv1;
-                c.vz[i] = c.vz[i] - s * bv2;
-            }
-        }
-        c.img[i] = i0;
-        c.img[cap + i] = i1;
-        c.img[2 * cap + i] = i2;
-    }
+         i += (uint64_t)gridDim.x * blockDim.x)
+        pbc_atom(c, i, g, bv0, bv1, bv2);
 }
 
 void launch_pbc(cudaStream_t st, uint64_t nlocal, const AtomCols& c, const Geom& g,

@@ -21,94 +21,10 @@
 // only REJECTS candidates provably outside the cutoff — the margin eps bounds
 // the float rounding of coordinates, differences and squares — followed by
 // the exact FP64 test on the rest, so the lists are identical in both modes.
+#include "device_ops.cuh"
 #include "kernels.cuh"
 
 namespace soil {
-
-template <bool UNIFORM, bool FP32>
-struct Filter {
-    double cut_sq, sf_sq;
-    float sf32, eps32, lim_uniform;
-
-    __device__ __forceinline__ explicit Filter(const PairParams& p)
-        : cut_sq(p.cut_sq), sf_sq(p.sf_sq), sf32((float)p.sf), eps32(p.eps32), lim_uniform(0.f) {
-        if (UNIFORM && FP32) {
-            const float cut = (float)sqrt(p.cut_sq) + p.eps32;
-            lim_uniform = cut * cut;
-        }
-    }
-
-    // The reference pair test for the candidate in sorted slot m; *rechk counts
-    // FP64 re-tests in FP32 mode.
-    __device__ __forceinline__ bool operator()(const PairParams& p, const double4& pi,
-                                               const float4& pif, uint32_t m,
-                                               uint32_t* rechk) const {
-        if (FP32) {
-            const float4 q = p.spf[m];
-            const float dx = q.x - pif.x;
-            const float dy = q.y - pif.y;
-            const float dz = q.z - pif.z;
-            const float r2 = dx * dx + dy * dy + dz * dz;
-            float lim = lim_uniform;
-            if (!UNIFORM) {
-                const float cu = (pif.w + q.w) * sf32 + eps32;
-                lim = cu * cu;
-            }
-            if (r2 > lim) return false;
-            ++*rechk;
-        }
-        const double4 q = p.sp[m];
-        const double dx = q.x - pi.x;
-        const double dy = q.y - pi.y;
-        const double dz = q.z - pi.z;
-        const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
-        if (UNIFORM) return r2 < cut_sq;
-        const double sum_skin = pi.w + q.w;
-        return r2 < sum_skin * sum_skin * sf_sq;
-    }
-};
-
-// Row of local atom i, sequentially in reference order.  FILL writes the
-// indices to out[]; returns the row length.
-template <bool UNIFORM, bool FP32, bool FILL>
-__device__ uint32_t row_scan(const PairParams& p, const Filter<UNIFORM, FP32>& test, uint64_t i,
-                             uint32_t* out, uint32_t cap, uint32_t* rechk, uint32_t* cand,
-                             DevFlags* flags) {
-    const uint32_t my_cell = p.atom_cell[i];
-    const uint32_t mi = p.atom_sorted_idx[i];
-    const double4 pi = p.sp[mi];
-    const float4 pif = FP32 ? p.spf[mi] : make_float4(0.f, 0.f, 0.f, 0.f);
-    uint32_t cnt = 0;
-    if (p.has_self) {
-        const uint32_t e = p.bin_start[my_cell + 1];
-        const uint32_t b = p.newton ? mi + 1 : p.bin_start[my_cell];
-        for (uint32_t m = b; m < e; ++m) {
-            if (!p.newton && m == mi) continue;
-            ++*cand;
-            if (test(p, pi, pif, m, rechk)) {
-                if (FILL && cnt < cap) out[cnt] = p.sorted_atoms[m];
-                ++cnt;
-            }
-        }
-    }
-    for (int s = 0; s < p.nstencil; ++s) {
-        const int32_t off = p.stencil[s];
-        if (!p.newton && off == 0) continue;
-        const uint32_t cc = (uint32_t)((int32_t)my_cell + off);
-        if (cc >= p.ncells) {  // the grid's ghost layers make this unreachable
-            if (flags) atomicOr(&flags->error, 1u);
-            continue;
-        }
-        const uint32_t e = p.bin_start[cc + 1];
-        *cand += e - p.bin_start[cc];
-        for (uint32_t m = p.bin_start[cc]; m < e; ++m)
-            if (test(p, pi, pif, m, rechk)) {
-                if (FILL && cnt < cap) out[cnt] = p.sorted_atoms[m];
-                ++cnt;
-            }
-    }
-    return cnt;
-}
 
 // Pass 1: one thread per local row (rows of a warp are neighbours in space, so
 // their candidate records are shared through L1); the first K entries go to

@@ -27,139 +27,11 @@
 #include <utility>
 #include <vector>
 
-#include "kernels.cuh"
+#include "sys_internal.cuh"
 
 using namespace soil;
 
-struct soil_ctx {
-    int device = 0;
-    uint64_t budget = 0;
-    uint64_t in_use = 0;
-    std::string err;
-};
-
-namespace {
-
-enum { FULL_REBUILD = SOIL_FULL_REBUILD, COMMUNICATE_ONLY = SOIL_COMMUNICATE_ONLY };
-
-struct ColMeta {
-    std::string name;
-    int width;
-    unsigned flags;
-    int plane0;
-};
-
-template <class T>
-struct DArr {
-    T* p = nullptr;
-    uint64_t cap = 0;  // elements
-};
-
-struct SwapHost {
-    uint64_t recv_start = 0, recv_count = 0;
-    double off[3] = {0, 0, 0};
-    double voff[3] = {0, 0, 0};
-};
-
-}  // namespace
-
-struct soil_sys {
-    soil_ctx* ctx = nullptr;
-    cudaStream_t st = nullptr;
-    double dt = 1.0;
-
-    // ---- Domain (domain.rs:105-142), one rank ----
-    double blo[3], bhi[3], size[3], sub_lo[3], sub_hi[3], sub_len[3];
-    double sub_lam_lo[3] = {0, 0, 0}, sub_lam_hi[3] = {1, 1, 1};
-    double tilt[3] = {0, 0, 0}, bvel[3] = {0, 0, 0};
-    bool triclinic = false, bounds_changed = false;
-    double domain_ghost_cutoff = 0.0;
-
-    // ---- Neighbor scalars (neighbor.rs:87-174) ----
-    double skin_fraction = 1.0, bin_min_size = 1.0, additive_skin = 0.0;
-    uint64_t every = 0, sort_every = 1000;
-    bool check = true, newton = true;
-    int filter = SOIL_FILTER_FP64;
-    double bin_size[3] = {1, 1, 1}, bin_origin[3] = {0, 0, 0};
-    int32_t bin_count[3] = {1, 1, 1};
-    uint64_t total_cells = 0;
-    std::vector<int32_t> stencil, stencil_fwd;
-    bool stencil_self = false;
-    double pbc_box[3] = {0, 0, 0};
-    double ghost_cutoff = 0.0, cached_min_skin = DBL_MAX, cached_max_cutoff = 0.0;
-    bool has_uniform = false;
-    double uniform_cut_sq = 0.0;
-    uint64_t steps_since_build = 0, sort_counter = 0;
-    bool local_cells_valid = false;
-    uint64_t last_build_n = 0;  // last_build_pos.len()
-    double cut_min_local = DBL_MAX, cut_max_local = -DBL_MAX;
-
-    // ---- Atom counts / CommState ----
-    uint64_t nlocal = 0, nghost = 0, npairs = 0;
-    int state = FULL_REBUILD;
-    SwapHost swaps[kNumSwaps];
-    int nswaps = 0;
-
-    // ---- deform / consumer ----
-    bool shear = false, shear_initialized = false, deform_initialized = false;
-    double shear_rate = 0.0;
-    uint64_t deform_step = 0;
-    double harmonic_k = 0.0;
-    int radius_col = -1;
-    soil_force_fn hook = nullptr;
-    void* hook_user = nullptr;
-    bool in_lists_valid = false;
-
-    // ---- columns ----
-    std::vector<ColMeta> cols;
-    int nplanes = 0;
-
-    // ---- device memory ----
-    uint64_t acap = 0;
-    AtomCols A{}, B{};
-    DArr<double> lbx, lby, lbz;
-    DArr<uint32_t> sort_cell, sort_perm, sorted_local_cell;
-    DArr<uint32_t> cell_counts, cell_start, cell_cursor;
-    DArr<uint32_t> atom_cell, sorted_atoms, asi, rowcount, offsets, indices, row_slots;
-    DArr<double4> sp;
-    DArr<float4> spf;
-    DArr<uint32_t> in_count, in_start, in_cursor, in_list;
-    DArr<uint32_t> ghost_root, ghost_chain;
-    DArr<uint32_t> fold_count, fold_start, fold_cursor, fold_list;  // reverse-comm fold program
-    DArr<uint32_t> send[kNumSwaps];
-    DArr<uint32_t> tile_lo, tile_hi, tile_off_lo, tile_off_hi, bstate;
-    DArr<uint8_t> face_flags;
-    uint64_t last_nghost = 0;
-    DArr<uint32_t> scan_tmp;
-    DArr<int32_t> d_stencil;
-    DArr<double> stage;  // host-layout staging for uploads/downloads
-    DArr<double*> d_colptrs;
-    DevFlags* dflags = nullptr;
-    DevFlags* hflags = nullptr;  // pinned mirror
-    uint32_t* hword = nullptr;   // pinned scratch words
-
-    // ---- phase timers ----
-    struct TimedSpan {
-        int timer;
-        cudaEvent_t a, b;
-        uint64_t launches;
-    };
-    uint32_t timing_mask = 0;
-    std::vector<cudaEvent_t> ev_pool;
-    std::vector<TimedSpan> spans;
-    double timer_ms[SOIL_NUM_TIMERS] = {};
-    uint64_t timer_launches[SOIL_NUM_TIMERS] = {};
-    uint64_t timer_intervals[SOIL_NUM_TIMERS] = {};
-    int open_timer = -1;
-    cudaEvent_t open_ev = nullptr;
-    uint64_t open_launches = 0;
-
-    // ---- bookkeeping ----
-    bool setup_done = false, perm_valid = false, pending_final = false;
-    uint64_t steps_done = 0, rebuilds = 0, sorts = 0;
-};
-
-namespace {
+namespace soil_host {
 
 int fail(soil_ctx* ctx, int status, const char* fmt, ...) {
     if (ctx) {
@@ -172,20 +44,6 @@ int fail(soil_ctx* ctx, int status, const char* fmt, ...) {
     }
     return status;
 }
-
-#define CK(call)                                                                              \
-    do {                                                                                      \
-        cudaError_t e_ = (call);                                                              \
-        if (e_ != cudaSuccess)                                                                \
-            return fail(s->ctx, SOIL_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
-                        __FILE__, __LINE__);                                                  \
-    } while (0)
-
-#define TRY(call)                        \
-    do {                                 \
-        int r_ = (call);                 \
-        if (r_ != SOIL_OK) return r_;    \
-    } while (0)
 
 int dev_alloc(soil_sys* s, void** p, uint64_t bytes) {
     if (bytes == 0) bytes = 16;
@@ -210,26 +68,9 @@ void dev_free(soil_sys* s, void* p, uint64_t bytes) {
     s->ctx->in_use -= bytes;
 }
 
-// Grow `a` to hold `need` elements; the first `keep` elements survive.
-template <class T>
-int ensure(soil_sys* s, DArr<T>& a, uint64_t need, uint64_t keep = 0) {
-    if (need <= a.cap && a.p) return SOIL_OK;
-    uint64_t ncap = need + need / 4 + 64;
-    void* np = nullptr;
-    TRY(dev_alloc(s, &np, ncap * sizeof(T)));
-    if (a.p && keep) CK(cudaMemcpyAsync(np, a.p, keep * sizeof(T), cudaMemcpyDeviceToDevice, s->st));
-    if (a.p) {
-        CK(cudaStreamSynchronize(s->st));
-        dev_free(s, a.p, a.cap * sizeof(T));
-    }
-    a.p = (T*)np;
-    a.cap = ncap;
-    return SOIL_OK;
-}
-
 // ---- per-atom columns -------------------------------------------------------
 constexpr int kDoubleCols = 12;  // x y z vx vy vz fx fy fz mass inv_mass cut
-constexpr int kRowSlots = 16;    // neighbor entries per atom kept by the first pair pass
+constexpr int kRowSlots = kRowSlotsPerAtom;  // neighbor entries per atom kept by the first pair pass
 
 double** dcol(AtomCols& c, int k) {
     double** t[kDoubleCols] = {&c.x, &c.y, &c.z, &c.vx, &c.vy, &c.vz,
@@ -280,12 +121,13 @@ int alloc_cols(soil_sys* s, AtomCols& c, uint64_t cap, const AtomCols* old, uint
 }
 
 int update_colptrs(soil_sys* s) {
-    if (s->cols.empty()) return SOIL_OK;
+    if (s->cols.empty() || !s->colptrs_dirty) return SOIL_OK;
     TRY(ensure(s, s->d_colptrs, kMaxCols));
     double* h[kMaxCols] = {};
     for (size_t c = 0; c < s->cols.size(); ++c) h[c] = s->A.planes[s->cols[c].plane0];
     CK(cudaMemcpyAsync(s->d_colptrs.p, h, sizeof(h), cudaMemcpyHostToDevice, s->st));
     CK(cudaStreamSynchronize(s->st));
+    s->colptrs_dirty = false;
     return SOIL_OK;
 }
 
@@ -309,7 +151,7 @@ int grow_atoms(soil_sys* s, uint64_t need, uint64_t keep) {
     uint64_t gkeep = keep > s->nlocal ? keep - s->nlocal : 0;
     TRY(ensure(s, s->ghost_root, ncap, gkeep));
     TRY(ensure(s, s->ghost_chain, ncap, gkeep));
-    TRY(update_colptrs(s));
+    s->colptrs_dirty = true;
     return SOIL_OK;
 }
 
@@ -529,16 +371,17 @@ bool builtin_consumer(const soil_sys* s) {
 // ---------------------------------------------------------------------------
 // Phases
 // ---------------------------------------------------------------------------
-int phase_deform(soil_sys* s) {
-    // apply_deform xy branch, soil_deform/src/lib.rs:435-604
-    if (!s->deform_initialized || !s->shear) return SOIL_OK;
+// apply_deform xy branch, soil_deform/src/lib.rs:435-604, host part.  Returns
+// true when the one-time streaming profile must be applied to the locals.
+bool deform_host(soil_sys* s) {
+    if (!s->deform_initialized || !s->shear) return false;
     s->deform_step += 1;
     const double rate = s->shear_rate;
     const double lx = s->size[0], ly = s->size[1];
     const double dv = rate * ly;
+    bool profile = false;
     if (!s->shear_initialized) {
-        const double yc = 0.5 * (s->blo[1] + s->bhi[1]);
-        launch_shear_profile(s->st, s->nlocal, s->A, rate, yc);
+        profile = true;
         s->shear_initialized = true;
     }
     const double raw = rate * s->dt * (double)s->deform_step * ly;
@@ -548,6 +391,13 @@ int phase_deform(soil_sys* s) {
     s->triclinic = true;
     s->bounds_changed = true;
     s->last_build_n = 0;  // neighbor.last_build_pos.clear()
+    return profile;
+}
+
+double profile_center(const soil_sys* s) { return 0.5 * (s->blo[1] + s->bhi[1]); }
+
+int phase_deform(soil_sys* s) {
+    if (deform_host(s)) launch_shear_profile(s->st, s->nlocal, s->A, s->shear_rate, profile_center(s));
     return check_launch(s);
 }
 
@@ -614,22 +464,22 @@ int phase_pbc(soil_sys* s) {
     return check_launch(s);
 }
 
-int phase_sort(soil_sys* s) {
-    // sort_atoms_by_bin, neighbor.rs:834-997
+// sort_atoms_by_bin (neighbor.rs:834-997), host part: grid recompute, sort
+// counter, whether the sort runs (*run) and whether it is a periodic sort.
+int sort_plan(soil_sys* s, bool* run, bool* periodic) {
+    *run = false;
     if (s->bounds_changed) {
         if (s->cached_max_cutoff > 0.0) compute_bin_grid(s);  // recompute_bins
         s->bounds_changed = false;
         s->state = FULL_REBUILD;
     }
     s->sort_counter += 1;
-    const bool periodic_sort = s->sort_every > 0 && s->sort_counter >= s->sort_every;
-    if (periodic_sort) s->sort_counter = 0;
-    const uint64_t nl = s->nlocal;
+    *periodic = s->sort_every > 0 && s->sort_counter >= s->sort_every;
+    if (*periodic) s->sort_counter = 0;
     s->local_cells_valid = false;
-    if (nl == 0 || s->total_cells == 0) return SOIL_OK;
-    const bool full_rebuild = s->state == FULL_REBUILD;
-    if (!periodic_sort && !full_rebuild) return SOIL_OK;
-
+    if (s->nlocal == 0 || s->total_cells == 0) return SOIL_OK;
+    if (!*periodic && s->state != FULL_REBUILD) return SOIL_OK;
+    *run = true;
     const uint64_t nc = s->total_cells;
     TRY(ensure(s, s->sort_cell, s->acap));
     TRY(ensure(s, s->sort_perm, s->acap));
@@ -638,6 +488,33 @@ int phase_sort(soil_sys* s) {
     TRY(ensure(s, s->cell_start, nc + 2));
     TRY(ensure(s, s->cell_cursor, nc + 1));
     TRY(ensure(s, s->scan_tmp, scan_temp_words(nc + s->acap + 2)));
+    return SOIL_OK;
+}
+
+// After the sort kernels ran: bookkeeping, and the column swap if the
+// permutation was applied (periodic sorts of an identity order do not apply).
+void sort_done(soil_sys* s, bool apply, bool periodic) {
+    s->local_cells_valid = true;
+    s->perm_valid = true;
+    s->sorts += 1;
+    if (apply) {
+        std::swap(s->A, s->B);
+        s->colptrs_dirty = true;
+        // last_build_pos is re-saved by the neighbor build that follows every
+        // permutation, so its permutation is not needed.
+    }
+    if (periodic && apply) {
+        s->last_build_n = 0;
+        s->state = FULL_REBUILD;
+    }
+}
+
+int phase_sort(soil_sys* s) {
+    bool run, periodic_sort;
+    TRY(sort_plan(s, &run, &periodic_sort));
+    if (!run) return SOIL_OK;
+    const uint64_t nl = s->nlocal;
+    const uint64_t nc = s->total_cells;
     CK(cudaMemsetAsync(s->cell_counts.p, 0, nc * 4, s->st));
     launch_cells(s->st, 0, nl, s->A, grid_of(s), s->sort_cell.p, s->cell_counts.p);
     exclusive_scan_u32(s->st, s->cell_counts.p, s->cell_start.p, nc, s->scan_tmp.p);
@@ -646,9 +523,6 @@ int phase_sort(soil_sys* s) {
     launch_segsort(s->st, nc, s->cell_start.p, s->sort_perm.p);
     launch_permute_u32(s->st, nl, s->sort_perm.p, s->sort_cell.p, s->sorted_local_cell.p);
     TRY(check_launch(s));
-    s->local_cells_valid = true;
-    s->perm_valid = true;
-    s->sorts += 1;
 
     bool apply = true;
     if (periodic_sort) {
@@ -663,15 +537,8 @@ int phase_sort(soil_sys* s) {
         // the borders that always follows a permutation
         launch_perm_gather(s->st, nl, s->sort_perm.p, s->A, s->B);
         TRY(check_launch(s));
-        std::swap(s->A, s->B);
-        TRY(update_colptrs(s));
-        // last_build_pos is re-saved by the neighbor build that follows every
-        // permutation, so its permutation is not needed.
     }
-    if (periodic_sort && apply) {
-        s->last_build_n = 0;
-        s->state = FULL_REBUILD;
-    }
+    sort_done(s, apply, periodic_sort);
     return SOIL_OK;
 }
 
@@ -682,8 +549,41 @@ int phase_borders(soil_sys* s) {
     // the (deterministic) pass is repeated.
     if (s->state != FULL_REBUILD) return SOIL_OK;
     s->nghost = 0;
-    const double gc = s->domain_ghost_cutoff;
     BorderDim bds[3];
+    border_setup(s, bds);
+    TRY(borders_reserve(s));
+    uint32_t* hb = s->hword;
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        const uint64_t cap = s->acap;
+        const uint32_t max_tiles = (uint32_t)((cap + kBorderTile - 1) / kBorderTile);
+        TRY(borders_arrays(s));
+        uint32_t init[kBorderStateWords] = {};
+        init[0] = (uint32_t)s->nlocal;
+        CK(cudaMemcpyAsync(s->bstate.p, init, sizeof init, cudaMemcpyHostToDevice, s->st));
+        for (int dim = 0; dim < 3; ++dim)
+            launch_border_dim(s->st, s->bstate.p, s->nlocal, cap, s->A, bds[dim], max_tiles,
+                              s->face_flags.p, s->tile_lo.p, s->tile_hi.p, s->tile_off_lo.p,
+                              s->tile_off_hi.p, s->send[2 * dim].p, s->send[2 * dim + 1].p,
+                              s->ghost_root.p, s->ghost_chain.p);
+        TRY(check_launch(s));
+        CK(cudaMemcpyAsync(hb, s->bstate.p, kBorderStateWords * 4, cudaMemcpyDeviceToHost, s->st));
+        TRY(sync(s));
+        if (!hb[10]) break;
+        if (attempt == 3) return fail(s->ctx, SOIL_ERR_CAPACITY, "ghost capacity did not converge");
+        TRY(grow_atoms(s, (uint64_t)hb[3] + 1024, s->nlocal));  // hb[3]: atoms incl. all ghosts
+    }
+    TRY(borders_done(s, hb, bds));
+    launch_fold_build(s->st, s->nlocal, s->nghost, s->ghost_root.p, s->ghost_chain.p,
+                      s->fold_count.p, s->fold_start.p, s->fold_cursor.p, s->fold_list.p,
+                      s->scan_tmp.p);
+    return check_launch(s);
+}
+
+// Face thresholds and image shifts of the three border dims (comm.rs:288-358,
+// 736-761): lo swap shift +L, hi swap -L, the y shift carrying the tilt and
+// the Lees–Edwards velocity jump.
+void border_setup(const soil_sys* s, BorderDim bds[3]) {
+    const double gc = s->domain_ghost_cutoff;
     for (int dim = 0; dim < 3; ++dim) {
         BorderDim& bd = bds[dim];
         bd.dim = dim;
@@ -708,36 +608,31 @@ int phase_borders(soil_sys* s) {
             bd.swap_id[sw] = 2 * dim + sw;
         }
     }
-    // room for the ghosts of the last pass plus a margin
+}
+
+// Capacity for this pass's ghosts: those of the last pass plus a margin.
+int borders_reserve(soil_sys* s) {
     const uint64_t want = s->nlocal + s->last_nghost + s->last_nghost / 4 + 4096;
     TRY(grow_atoms(s, want, s->nlocal));
+    return borders_arrays(s);
+}
+
+int borders_arrays(soil_sys* s) {
+    const uint64_t cap = s->acap;
+    const uint32_t max_tiles = (uint32_t)((cap + kBorderTile - 1) / kBorderTile);
     TRY(ensure(s, s->bstate, kBorderStateWords));
-    uint32_t* hb = s->hword;
-    for (int attempt = 0; attempt < 4; ++attempt) {
-        const uint64_t cap = s->acap;
-        const uint32_t max_tiles = (uint32_t)((cap + kBorderTile - 1) / kBorderTile);
-        TRY(ensure(s, s->tile_lo, max_tiles + 2));
-        TRY(ensure(s, s->tile_hi, max_tiles + 2));
-        TRY(ensure(s, s->tile_off_lo, max_tiles + 2));
-        TRY(ensure(s, s->tile_off_hi, max_tiles + 2));
-        for (int k = 0; k < kNumSwaps; ++k) TRY(ensure(s, s->send[k], cap + 1));
-        TRY(ensure(s, s->face_flags, cap + 1));
-        uint32_t init[kBorderStateWords] = {};
-        init[0] = (uint32_t)s->nlocal;
-        CK(cudaMemcpyAsync(s->bstate.p, init, sizeof init, cudaMemcpyHostToDevice, s->st));
-        for (int dim = 0; dim < 3; ++dim)
-            launch_border_dim(s->st, s->bstate.p, s->nlocal, cap, s->A, bds[dim], max_tiles,
-                              s->face_flags.p, s->tile_lo.p, s->tile_hi.p, s->tile_off_lo.p,
-                              s->tile_off_hi.p,
-                              s->send[2 * dim].p, s->send[2 * dim + 1].p, s->ghost_root.p,
-                              s->ghost_chain.p);
-        TRY(check_launch(s));
-        CK(cudaMemcpyAsync(hb, s->bstate.p, kBorderStateWords * 4, cudaMemcpyDeviceToHost, s->st));
-        TRY(sync(s));
-        if (!hb[10]) break;
-        if (attempt == 3) return fail(s->ctx, SOIL_ERR_CAPACITY, "ghost capacity did not converge");
-        TRY(grow_atoms(s, (uint64_t)hb[3] + 1024, s->nlocal));  // hb[3]: atoms incl. all ghosts
-    }
+    TRY(ensure(s, s->tile_lo, max_tiles + 2));
+    TRY(ensure(s, s->tile_hi, max_tiles + 2));
+    TRY(ensure(s, s->tile_off_lo, max_tiles + 2));
+    TRY(ensure(s, s->tile_off_hi, max_tiles + 2));
+    for (int k = 0; k < kNumSwaps; ++k) TRY(ensure(s, s->send[k], cap + 1));
+    TRY(ensure(s, s->face_flags, cap + 1));
+    return SOIL_OK;
+}
+
+// Swap records and ghost count from a finished pass (hb: its border state),
+// and room for the reverse-comm fold program.
+int borders_done(soil_sys* s, const uint32_t* hb, const BorderDim bds[3]) {
     for (int dim = 0; dim < 3; ++dim) {
         const uint64_t recv_lo = hb[dim], n_lo = hb[4 + dim], n_hi = hb[7 + dim];
         for (int sw = 0; sw < 2; ++sw) {
@@ -753,16 +648,13 @@ int phase_borders(soil_sys* s) {
     s->nghost = (uint64_t)hb[3] - s->nlocal;
     s->last_nghost = s->nghost;
     s->nswaps = kNumSwaps;
-    // fold program of reverse comm for these ghosts
     const uint64_t nl = s->nlocal;
     TRY(ensure(s, s->fold_count, nl + 1));
     TRY(ensure(s, s->fold_start, nl + 2));
     TRY(ensure(s, s->fold_cursor, nl + 1));
     TRY(ensure(s, s->fold_list, s->nghost + 1));
     TRY(ensure(s, s->scan_tmp, scan_temp_words(nl + 2)));
-    launch_fold_build(s->st, nl, s->nghost, s->ghost_root.p, s->ghost_chain.p, s->fold_count.p,
-                      s->fold_start.p, s->fold_cursor.p, s->fold_list.p, s->scan_tmp.p);
-    return check_launch(s);
+    return SOIL_OK;
 }
 
 SwapConst swap_const(const soil_sys* s) {
@@ -806,17 +698,16 @@ int build_in_lists(soil_sys* s) {
     return SOIL_OK;
 }
 
-int phase_neighbor(soil_sys* s) {
-    // bin_neighbor_list, neighbor.rs:1013-1319
-    if (s->state != FULL_REBUILD) return SOIL_OK;
+// bin_neighbor_list (neighbor.rs:1013-1319), host part: the CommState
+// transition, save_build_positions bookkeeping (neighbor.rs:669-690; the local
+// cutoff radii never change after setup, so their min/max are cached there),
+// the uniform-cutoff decision and room for the build.
+int neighbor_plan(soil_sys* s) {
     s->state = COMMUNICATE_ONLY;
-    const uint64_t nl = s->nlocal, total = s->nlocal + s->nghost;
-    // save_build_positions (neighbor.rs:669-690); the local cutoff radii never
-    // change after setup, so their min/max are cached there.
+    const uint64_t nl = s->nlocal;
     TRY(ensure(s, s->lbx, s->acap));
     TRY(ensure(s, s->lby, s->acap));
     TRY(ensure(s, s->lbz, s->acap));
-    launch_save_positions(s->st, nl, s->A, s->lbx.p, s->lby.p, s->lbz.p);
     s->last_build_n = nl;
     s->steps_since_build = 0;
     s->cached_min_skin = s->cut_min_local;
@@ -834,13 +725,31 @@ int phase_neighbor(soil_sys* s) {
     TRY(ensure(s, s->rowcount, s->acap));
     TRY(ensure(s, s->offsets, s->acap + 2));
     TRY(ensure(s, s->sp, s->acap));
-    const bool fp32 = s->filter == SOIL_FILTER_FP32_RECHECK;
-    if (fp32) TRY(ensure(s, s->spf, s->acap));
+    if (s->filter == SOIL_FILTER_FP32_RECHECK) TRY(ensure(s, s->spf, s->acap));
     TRY(ensure(s, s->row_slots, (uint64_t)nl * kRowSlots + 1));
     TRY(ensure(s, s->cell_counts, nc + 1));
     TRY(ensure(s, s->cell_start, nc + 2));
     TRY(ensure(s, s->cell_cursor, nc + 1));
     TRY(ensure(s, s->scan_tmp, scan_temp_words(nc + s->acap + 2)));
+    return SOIL_OK;
+}
+
+// Margin of the FP32 prefilter: FP32 coordinates are relative to the box
+// corner and M bounds their magnitude.
+float pair_eps(const soil_sys* s) {
+    double M = 0.0;
+    for (int d = 0; d < 3; ++d) M = std::fmax(M, s->size[d]);
+    M += 2.0 * s->domain_ghost_cutoff + std::fabs(s->tilt[0]) + 4.0 * s->cached_max_cutoff;
+    return (float)(1e-6 * (1.0 + s->cached_max_cutoff) + 4e-7 * M);
+}
+
+int phase_neighbor(soil_sys* s) {
+    if (s->state != FULL_REBUILD) return SOIL_OK;
+    TRY(neighbor_plan(s));
+    const uint64_t nl = s->nlocal, total = s->nlocal + s->nghost;
+    const uint64_t nc = s->total_cells;
+    const bool fp32 = s->filter == SOIL_FILTER_FP32_RECHECK;
+    launch_save_positions(s->st, nl, s->A, s->lbx.p, s->lby.p, s->lbz.p);
     CK(cudaMemsetAsync(s->cell_counts.p, 0, nc * 4, s->st));
     const Grid gr = grid_of(s);
     if (s->local_cells_valid) {  // reuse the sort's local cells (neighbor.rs:1049-1066)
@@ -856,10 +765,6 @@ int phase_neighbor(soil_sys* s) {
     CK(cudaMemcpyAsync(s->cell_cursor.p, s->cell_start.p, nc * 4, cudaMemcpyDeviceToDevice, s->st));
     launch_scatter(s->st, total, s->atom_cell.p, s->cell_cursor.p, s->sorted_atoms.p);
     launch_segsort(s->st, nc, s->cell_start.p, s->sorted_atoms.p);
-    // FP32 coordinates are relative to the box corner; M bounds their magnitude
-    double M = 0.0;
-    for (int d = 0; d < 3; ++d) M = std::fmax(M, s->size[d]);
-    M += 2.0 * s->domain_ghost_cutoff + std::fabs(s->tilt[0]) + 4.0 * s->cached_max_cutoff;
     launch_sorted_views(s->st, total, s->sorted_atoms.p, s->A, s->asi.p, s->sp.p,
                         fp32 ? s->spf.p : nullptr, s->blo);
     const std::vector<int32_t>& sten = s->newton ? s->stencil_fwd : s->stencil;
@@ -885,7 +790,7 @@ int phase_neighbor(soil_sys* s) {
     p.cut_sq = s->uniform_cut_sq;
     p.sf_sq = s->skin_fraction * s->skin_fraction;
     p.sf = s->skin_fraction;
-    p.eps32 = (float)(1e-6 * (1.0 + s->cached_max_cutoff) + 4e-7 * M);
+    p.eps32 = pair_eps(s);
     CK(cudaMemsetAsync(&s->dflags->candidates, 0, 16, s->st));
     CK(cudaMemsetAsync(&s->dflags->error, 0, 4, s->st));
     launch_pair_count(s->st, p, s->rowcount.p, s->row_slots.p, s->dflags);
@@ -908,6 +813,7 @@ int phase_neighbor(soil_sys* s) {
 
 int make_view(soil_sys* s, soil_dev_view* v) {
     std::memset(v, 0, sizeof(*v));
+    TRY(update_colptrs(s));
     v->nlocal = s->nlocal;
     v->nghost = s->nghost;
     v->npairs = s->npairs;
@@ -931,7 +837,7 @@ int make_view(soil_sys* s, soil_dev_view* v) {
 int phase_force(soil_sys* s) {
     if (s->hook) {
         soil_dev_view v;
-        make_view(s, &v);
+        TRY(make_view(s, &v));
         int r = s->hook(&v, s->hook_user);
         if (r != 0) return fail(s->ctx, SOIL_ERR_INVALID, "force hook returned %d", r);
         return check_launch(s);
@@ -1037,7 +943,9 @@ int full_step(soil_sys* s, bool last) {
     return SOIL_OK;
 }
 
-}  // namespace
+}  // namespace soil_host
+
+using namespace soil_host;
 
 namespace soil {
 // Records `msg` as the context's last error (ctx may be NULL) and returns status.
@@ -1144,6 +1052,7 @@ int soil_sys_create(soil_ctx* ctx, const soil_box* box, const soil_neigh_cfg* cf
 
 int soil_sys_destroy(soil_sys* s) {
     if (!s) return SOIL_OK;
+    if (s->batch) soil_batch_remove(s->batch, s);
     if (s->st) cudaStreamSynchronize(s->st);
     if (s->A.x) free_cols(s, s->A);
     if (s->B.x) free_cols(s, s->B);

@@ -112,6 +112,12 @@ struct SwapConst {
     double voff[kNumSwaps][3];
 };
 
+// Indices of registered f64 planes taking part in an operation.
+struct PlaneList {
+    int idx[kMaxPlanes];
+    int n;
+};
+
 // Device-resident counters the host reads back in one copy.
 struct DevFlags {
     uint32_t rebuild;        // displacement check tripped

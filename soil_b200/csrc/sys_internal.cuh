@@ -1,0 +1,212 @@
+// sys_internal.cuh — host-side state of one system (the reference's Atom,
+// Domain, Neighbor and CommTopology resources) and the helpers that the
+// single-system entry points and the batch engine share.
+#pragma once
+
+#include <cfloat>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+using namespace soil;
+
+struct soil_ctx {
+    int device = 0;
+    uint64_t budget = 0;
+    uint64_t in_use = 0;
+    std::string err;
+};
+
+namespace soil_host {
+
+enum { FULL_REBUILD = SOIL_FULL_REBUILD, COMMUNICATE_ONLY = SOIL_COMMUNICATE_ONLY };
+
+struct ColMeta {
+    std::string name;
+    int width;
+    unsigned flags;
+    int plane0;
+};
+
+template <class T>
+struct DArr {
+    T* p = nullptr;
+    uint64_t cap = 0;  // elements
+};
+
+struct SwapHost {
+    uint64_t recv_start = 0, recv_count = 0;
+    double off[3] = {0, 0, 0};
+    double voff[3] = {0, 0, 0};
+};
+
+}  // namespace soil_host
+
+using soil_host::ColMeta;
+using soil_host::DArr;
+using soil_host::SwapHost;
+
+struct soil_sys {
+    soil_ctx* ctx = nullptr;
+    cudaStream_t st = nullptr;
+    double dt = 1.0;
+
+    // ---- Domain (domain.rs:105-142), one rank ----
+    double blo[3], bhi[3], size[3], sub_lo[3], sub_hi[3], sub_len[3];
+    double sub_lam_lo[3] = {0, 0, 0}, sub_lam_hi[3] = {1, 1, 1};
+    double tilt[3] = {0, 0, 0}, bvel[3] = {0, 0, 0};
+    bool triclinic = false, bounds_changed = false;
+    double domain_ghost_cutoff = 0.0;
+
+    // ---- Neighbor scalars (neighbor.rs:87-174) ----
+    double skin_fraction = 1.0, bin_min_size = 1.0, additive_skin = 0.0;
+    uint64_t every = 0, sort_every = 1000;
+    bool check = true, newton = true;
+    int filter = SOIL_FILTER_FP64;
+    double bin_size[3] = {1, 1, 1}, bin_origin[3] = {0, 0, 0};
+    int32_t bin_count[3] = {1, 1, 1};
+    uint64_t total_cells = 0;
+    std::vector<int32_t> stencil, stencil_fwd;
+    bool stencil_self = false;
+    double pbc_box[3] = {0, 0, 0};
+    double ghost_cutoff = 0.0, cached_min_skin = DBL_MAX, cached_max_cutoff = 0.0;
+    bool has_uniform = false;
+    double uniform_cut_sq = 0.0;
+    uint64_t steps_since_build = 0, sort_counter = 0;
+    bool local_cells_valid = false;
+    uint64_t last_build_n = 0;  // last_build_pos.len()
+    double cut_min_local = DBL_MAX, cut_max_local = -DBL_MAX;
+
+    // ---- Atom counts / CommState ----
+    uint64_t nlocal = 0, nghost = 0, npairs = 0;
+    int state = soil_host::FULL_REBUILD;
+    SwapHost swaps[kNumSwaps];
+    int nswaps = 0;
+
+    // ---- deform / consumer ----
+    bool shear = false, shear_initialized = false, deform_initialized = false;
+    double shear_rate = 0.0;
+    uint64_t deform_step = 0;
+    double harmonic_k = 0.0;
+    int radius_col = -1;
+    soil_force_fn hook = nullptr;
+    void* hook_user = nullptr;
+    bool in_lists_valid = false;
+
+    // ---- columns ----
+    std::vector<ColMeta> cols;
+    int nplanes = 0;
+
+    // ---- device memory ----
+    uint64_t acap = 0;
+    AtomCols A{}, B{};
+    DArr<double> lbx, lby, lbz;
+    DArr<uint32_t> sort_cell, sort_perm, sorted_local_cell;
+    DArr<uint32_t> cell_counts, cell_start, cell_cursor;
+    DArr<uint32_t> atom_cell, sorted_atoms, asi, rowcount, offsets, indices, row_slots;
+    DArr<double4> sp;
+    DArr<float4> spf;
+    DArr<uint32_t> in_count, in_start, in_cursor, in_list;
+    DArr<uint32_t> ghost_root, ghost_chain;
+    DArr<uint32_t> fold_count, fold_start, fold_cursor, fold_list;  // reverse-comm fold program
+    DArr<uint32_t> send[kNumSwaps];
+    DArr<uint32_t> tile_lo, tile_hi, tile_off_lo, tile_off_hi, bstate;
+    DArr<uint8_t> face_flags;
+    uint64_t last_nghost = 0;
+    DArr<uint32_t> scan_tmp;
+    DArr<int32_t> d_stencil;
+    DArr<double> stage;  // host-layout staging for uploads/downloads
+    DArr<double*> d_colptrs;
+    bool colptrs_dirty = true;  // d_colptrs no longer matches A (refreshed by make_view)
+    DevFlags* dflags = nullptr;
+    DevFlags* hflags = nullptr;  // pinned mirror
+    uint32_t* hword = nullptr;   // pinned scratch words
+
+    // ---- phase timers ----
+    struct TimedSpan {
+        int timer;
+        cudaEvent_t a, b;
+        uint64_t launches;
+    };
+    uint32_t timing_mask = 0;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<TimedSpan> spans;
+    double timer_ms[SOIL_NUM_TIMERS] = {};
+    uint64_t timer_launches[SOIL_NUM_TIMERS] = {};
+    uint64_t timer_intervals[SOIL_NUM_TIMERS] = {};
+    int open_timer = -1;
+    cudaEvent_t open_ev = nullptr;
+    uint64_t open_launches = 0;
+
+    // ---- bookkeeping ----
+    soil_batch* batch = nullptr;  // batch this system is stepped in (its stream is the batch's)
+    bool setup_done = false, perm_valid = false, pending_final = false;
+    uint64_t steps_done = 0, rebuilds = 0, sorts = 0;
+};
+
+
+namespace soil_host {
+
+int fail(soil_ctx* ctx, int status, const char* fmt, ...);
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(s->ctx, SOIL_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                                  \
+    } while (0)
+
+#define TRY(call)                        \
+    do {                                 \
+        int r_ = (call);                 \
+        if (r_ != SOIL_OK) return r_;    \
+    } while (0)
+
+int dev_alloc(soil_sys* s, void** p, uint64_t bytes);
+void dev_free(soil_sys* s, void* p, uint64_t bytes);
+
+// Grow `a` to hold `need` elements; the first `keep` elements survive.
+template <class T>
+int ensure(soil_sys* s, DArr<T>& a, uint64_t need, uint64_t keep = 0) {
+    if (need <= a.cap && a.p) return SOIL_OK;
+    uint64_t ncap = need + need / 4 + 64;
+    void* np = nullptr;
+    TRY(dev_alloc(s, &np, ncap * sizeof(T)));
+    if (a.p && keep) CK(cudaMemcpyAsync(np, a.p, keep * sizeof(T), cudaMemcpyDeviceToDevice, s->st));
+    if (a.p) {
+        CK(cudaStreamSynchronize(s->st));
+        dev_free(s, a.p, a.cap * sizeof(T));
+    }
+    a.p = (T*)np;
+    a.cap = ncap;
+    return SOIL_OK;
+}
+
+int grow_atoms(soil_sys* s, uint64_t need, uint64_t keep);
+int update_colptrs(soil_sys* s);
+bool deform_host(soil_sys* s);
+double profile_center(const soil_sys* s);
+int sort_plan(soil_sys* s, bool* run, bool* periodic);
+void sort_done(soil_sys* s, bool apply, bool periodic);
+void border_setup(const soil_sys* s, BorderDim bds[3]);
+int borders_reserve(soil_sys* s);
+int borders_arrays(soil_sys* s);
+int borders_done(soil_sys* s, const uint32_t* hb, const BorderDim bds[3]);
+int neighbor_plan(soil_sys* s);
+float pair_eps(const soil_sys* s);
+int sync(soil_sys* s);
+int check_launch(soil_sys* s);
+Geom geom_of(const soil_sys* s);
+Grid grid_of(const soil_sys* s);
+void compute_bin_grid(soil_sys* s);
+double displacement_threshold_sq(const soil_sys* s);
+void zero_planes_of(const soil_sys* s, unsigned flag, int* out, int* n);
+bool builtin_consumer(const soil_sys* s);
+bool needs_rebuild_with(const soil_sys* s, bool disp);
+bool displacement_needed(const soil_sys* s);
+SwapConst swap_const(const soil_sys* s);
+constexpr int kRowSlotsPerAtom = 16;
+
+}  // namespace soil_host

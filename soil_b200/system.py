@@ -222,6 +222,58 @@ class System:
         return v
 
 
+class Batch:
+    """Many set-up systems stepped together (soil_batch_*): one launch per phase
+    over every member, each member bit-identical to stepping it alone."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        h = C.c_void_p()
+        ctx.check(self.lib.soil_batch_create(ctx.h, C.byref(h)), "soil_batch_create")
+        self.h = h
+        self.members = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.soil_batch_destroy(self.h)
+            self.h = None
+            self.members = []
+
+    def __del__(self):
+        self.close()
+
+    def add(self, system):
+        self.ctx.check(self.lib.soil_batch_add(self.h, system.h), "soil_batch_add")
+        self.members.append(system)
+
+    def remove(self, system):
+        self.ctx.check(self.lib.soil_batch_remove(self.h, system.h), "soil_batch_remove")
+        self.members.remove(system)
+
+    def __len__(self):
+        n = C.c_uint32()
+        self.ctx.check(self.lib.soil_batch_size(self.h, C.byref(n)), "soil_batch_size")
+        return n.value
+
+    def step(self, n=1):
+        self.ctx.check(self.lib.soil_batch_step(self.h, n), "soil_batch_step")
+
+    def sync(self):
+        self.ctx.check(self.lib.soil_batch_sync(self.h), "soil_batch_sync")
+
+    def stream(self):
+        v = C.c_void_p()
+        self.ctx.check(self.lib.soil_batch_stream(self.h, C.byref(v)), "soil_batch_stream")
+        return v.value
+
+    def stats(self):
+        st, w, b = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        self.ctx.check(self.lib.soil_batch_stats(self.h, C.byref(st), C.byref(w), C.byref(b)),
+                       "soil_batch_stats")
+        return dict(steps=st.value, host_waits=w.value, device_bytes=b.value)
+
+
 def from_workload(ctx, w):
     """GPU system for a workloads.Workload (radius registered as column 0)."""
     s = System(ctx, w.box, w.cfg, w.dt)

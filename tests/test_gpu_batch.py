@@ -1,0 +1,118 @@
+"""Batched stepping (soil_batch_*): every member is bit-identical to the same
+system stepped alone with soil_step, and to the CPU oracle.
+
+The boxes mix sizes, packing fractions, shear (sheared boxes rebuild every
+step, the others only on displacement), both filter modes, Newton on and off
+and a short sort period (periodic spatial sorts that find the identity and
+ones that do not).  Batches are stepped in chunks that differ from the alone
+runs, so the deferred final half-kick is flushed at different steps.
+"""
+import numpy as np
+import pytest
+
+from helpers import assert_same_lists, assert_same_state, pair
+from soil_b200 import abi, system, workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def mixed_boxes(count=8, nmax=3000):
+    ws = []
+    for i in range(count):
+        w = W.config4_box(i, nmin=256, nmax=nmax, steps=40)
+        if i % 4 == 3:
+            w.cfg.filter = abi.SOIL_FILTER_FP32_RECHECK
+        if i % 4 == 2:
+            w.cfg.sort_every = 7
+        if i == 5:
+            w.cfg.newton = 0
+        ws.append(w)
+    # a fast-sheared box whose tilt wraps inside the run
+    ws.append(W.mono("fast-shear", 9, 1500, 0.4, 1e-3, 40, harmonic_k=1e3, shear_rate=5.0))
+    return ws
+
+
+def assert_same(a, b, what, filter_stats=True):
+    assert_same_state(a, b, what)
+    assert_same_lists(a, b, what)
+    np.testing.assert_array_equal(a.sort_perm(), b.sort_perm(), err_msg=f"{what} sort perm")
+    ca, cb = a.counts(), b.counts()
+    assert ca.sorts == cb.sorts, what
+    if filter_stats:  # the oracle does not count filter candidates
+        assert (ca.filter_candidates, ca.filter_rechecked) == \
+            (cb.filter_candidates, cb.filter_rechecked), what
+
+
+def test_batch_equals_alone(ctx):
+    ws = mixed_boxes()
+    alone = [system.from_workload(ctx, w) for w in ws]
+    mixed = [system.from_workload(ctx, w) for w in ws]
+    for s in alone:
+        s.step(13)
+        s.step(27)
+    batch = system.Batch(ctx)
+    for s in mixed:
+        batch.add(s)
+    assert len(batch) == len(ws)
+    batch.step(5)
+    batch.step(1)
+    batch.step(34)
+    for k, (a, m) in enumerate(zip(alone, mixed)):
+        assert_same(a, m, f"box {k} ({ws[k].name})")
+    assert any(m.counts().rebuilds > 2 for m in mixed)
+    st = batch.stats()
+    assert st["steps"] == 40
+    batch.close()
+    for s in alone + mixed:
+        s.close()
+
+
+def test_batch_equals_oracle(ctx):
+    ws = mixed_boxes(count=4, nmax=1200)
+    pairs = [pair(ctx, w) for w in ws]
+    batch = system.Batch(ctx)
+    for g, _ in pairs:
+        batch.add(g)
+    batch.step(25)
+    for k, (g, o) in enumerate(pairs):
+        o.step(25)
+        assert_same(g, o, f"box {k} ({ws[k].name})", filter_stats=False)
+    batch.close()
+
+
+def test_batch_membership_changes(ctx):
+    """Boxes join and leave between steps (the served loop's pattern); each
+    box's result only depends on its own step count."""
+    ws = mixed_boxes(count=6, nmax=2000)
+    sched = {0: (0, 30), 1: (0, 12), 2: (5, 30), 3: (12, 30), 4: (5, 22), 5: (0, 30)}
+    mixed = [system.from_workload(ctx, w) for w in ws]
+    batch = system.Batch(ctx)
+    t = 0
+    for edge in (5, 12, 22, 30):
+        for k, (t0, t1) in sched.items():
+            if t0 == t:
+                batch.add(mixed[k])
+            if t1 == t:
+                batch.remove(mixed[k])
+        batch.step(edge - t)
+        t = edge
+    for k, (t0, t1) in sched.items():
+        if t1 == t:
+            batch.remove(mixed[k])
+    assert len(batch) == 0
+    for k, (t0, t1) in sched.items():
+        a = system.from_workload(ctx, ws[k])
+        a.step(t1 - t0)
+        assert_same(a, mixed[k], f"box {k}")
+        a.close()
+    batch.close()
+
+
+def test_batch_rejects_unsupported(ctx):
+    w = W.config1(n=1024, steps=10)  # no consumer
+    s = system.from_workload(ctx, w)
+    batch = system.Batch(ctx)
+    with pytest.raises(abi.SoilError):
+        batch.add(s)
+    batch.close()
+    s.close()
