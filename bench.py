@@ -333,6 +333,180 @@ def run_soil(args, world, rank, local):
     return 0
 
 
+# ---- batched configuration ------------------------------------------------------
+C4_DESC = ("C4 batched: 4,096 independent periodic boxes, N log-uniform [256, 65,536] "
+           "(47.3M atoms), phi U[0.20,0.55], r~U[0.4,0.6], half sheared at rate U[0.01,0.2], "
+           "harmonic k=1e3, dt 1e-4")
+
+
+def lpt_partition(sizes, world):
+    """Greedy longest-processing-time assignment of boxes to ranks."""
+    order = sorted(range(len(sizes)), key=lambda i: -sizes[i])
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda q: load[q])
+        parts[r].append(i)
+        load[r] += sizes[i]
+    return [sorted(p) for p in parts]
+
+
+def batched_cpu_baseline(ws, budget_s=15.0):
+    """The CPU oracle on a sample of the boxes: one thread, and one thread per
+    host core each stepping its own box (ctypes releases the GIL)."""
+    import concurrent.futures as cf
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    cores = os.cpu_count() or 1
+
+    def run(w, budget):
+        o = oracle.from_workload(w)
+        steps, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < budget:
+            o.step(1)
+            steps += 1
+        return w.n * steps, time.perf_counter() - t0
+
+    one = run(ws[0], budget_s)
+    sample = ws[:cores]
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=cores) as ex:
+        res = list(ex.map(lambda w: run(w, budget_s), sample))
+    wall = time.perf_counter() - t0
+    return {"value": sum(r[0] for r in res) / wall, "unit": "atom-steps/s", "cores": cores,
+            "kind": "port", "one_core_value": one[0] / one[1],
+            "sample": (f"{len(sample)} boxes ({sum(w.n for w in sample)} atoms), one per host "
+                       f"thread, ~{budget_s:.0f}s each from their initial state; one-core figure "
+                       f"from box 0 ({ws[0].n} atoms) alone; C++ oracle -O3")}
+
+
+def run_batched(args, world, rank, local):
+    import torch
+    from soil_b200 import system
+
+    nbox = args.boxes
+    sizes = [workloads.config4_size(i) for i in range(nbox)]
+    mine = lpt_partition(sizes, world)[rank]
+    t0 = time.perf_counter()
+    ws = [workloads.config4_box(i, steps=args.steps) for i in mine]
+    natoms = sum(w.n for w in ws)
+    log(f"[c4] rank {rank}: {len(ws)} boxes, {natoms} atoms generated in "
+        f"{time.perf_counter() - t0:.1f}s")
+    lib = abi.load_library()
+    ctx = system.Context(local)
+    t0 = time.perf_counter()
+    boxes = [system.from_workload(ctx, w) for w in ws]
+    log(f"[c4] systems set up in {time.perf_counter() - t0:.1f}s")
+
+    # plain per-system path: every box stepped alone through soil_step, one
+    # after the other (each box's first step, which builds its lists, untimed)
+    plain_ms = 0.0
+    for s in (boxes if args.plain_steps > 0 else []):
+        s.step(1)
+        st = torch.cuda.ExternalStream(s.stream(), device=torch.device("cuda", local))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        s.step(args.plain_steps)
+        e1.record(st)
+        s.sync()
+        plain_ms += e0.elapsed_time(e1)
+    plain_ms = max_over_ranks(plain_ms, world)
+    plain_value = (sum_over_ranks(natoms, world) * args.plain_steps / (plain_ms * 1e-3)
+                   if args.plain_steps > 0 else None)
+
+    batch = system.Batch(ctx)
+    for s in boxes:
+        batch.add(s)
+    stream = torch.cuda.ExternalStream(batch.stream(), device=torch.device("cuda", local))
+    batch.step(args.warmup)
+    batch.set_timing(True)
+    rb0 = sum(s.counts().rebuilds for s in boxes)
+    st0 = batch.stats()
+    launches0 = lib.soil_kernel_launches()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    batch.sync()
+    torch.cuda.synchronize()
+    barrier(world)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    batch.step(args.steps)
+    ev1.record(stream)
+    batch.sync()
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = ev0.elapsed_time(ev1)
+    clocks = sampler.stop()
+    launches = lib.soil_kernel_launches() - launches0
+    tim = batch.get_timing()
+    st1 = batch.stats()
+    cs = [s.counts() for s in boxes]
+    rebuilds = sum(c.rebuilds for c in cs) - rb0
+    ms_max = max_over_ranks(ms, world)
+    total_atoms = sum_over_ranks(natoms, world)
+    value = total_atoms * args.steps / (ms_max * 1e-3)
+
+    # roofline of the consumer kernel (one launch per step over every box):
+    # R pos+radius of every atom, W force, R offsets, R each pair twice
+    force_ms = tim["force"][0] / max(tim["force"][1], 1)
+    force_bytes = sum(64 * (c.nlocal + c.nghost) + 8 * c.npairs for c in cs)
+    peak, peak_kind = load_peaks()
+    achieved = force_bytes / (force_ms * 1e-3) / 1e9
+    tr = load_traffic("batched_force", "c4")
+    roofline = {"bound": "hbm", "kernel": "kb_harmonic (all boxes, one launch)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": peak_kind,
+                "traffic": tr["dram_bytes_per_launch"] if tr else None,
+                "algorithmic_bytes_per_launch": force_bytes, "mean_launch_ms": force_ms,
+                "launches": tim["force"][1]}
+    stages = {k: round(v[0] / max(v[1], 1), 4) for k, v in tim.items()}
+    host = {k: round(v / args.steps, 4) for k, v in batch.get_host_timing().items()}
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = batched_cpu_baseline(ws)
+    if rank == 0:
+        line = {
+            "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded SplitMix64 per box, Box-Muller velocities)",
+            "config": {"workload": C4_DESC, "boxes": nbox, "n_atoms": total_atoms,
+                       "parallelism": "boxes LPT-partitioned over ranks" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (~%d GB of per-atom state)" %
+                             (total_atoms * 250 // 2**30)},
+            "plain_per_system": {"value": plain_value, "unit": "atom-steps/s",
+                                 "steps_per_box": args.plain_steps,
+                                 "what": "each box alone through soil_step, one after another"},
+            "batched_over_plain": value / plain_value if plain_value else None,
+            "neighbor_builds_per_s": rebuilds / (ms_max * 1e-3),
+            "host_waits_per_step": (st1["host_waits"] - st0["host_waits"]) / args.steps,
+            "stage_ms_per_step": stages,
+            "host_ms_per_step": host,
+            "roofline": roofline,
+            "cpu_baseline": cb,
+            "e2e": None,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    batch.close()
+    return 0
+
+
+def sum_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def run_e2e(ctx, w, steps, world):
     """Same metric through the C ABI from pinned host buffers: upload the
     initial state, set up, run `steps`, read back positions and velocities."""
@@ -385,7 +559,11 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["soil", "reference"], default="soil")
-    ap.add_argument("--config", choices=["c1", "c2", "c3"], default="c2")
+    ap.add_argument("--config", choices=["c1", "c2", "c3", "c4"], default="c2")
+    ap.add_argument("--boxes", type=int, default=workloads.C4_BOXES,
+                    help="c4: number of boxes (4096 is the configuration)")
+    ap.add_argument("--plain-steps", type=int, default=4,
+                    help="c4: timed steps of each box alone (plain path; 0 skips it)")
     ap.add_argument("--filter", choices=["fp64", "fp32"], default="fp64")
     ap.add_argument("--natoms", type=int, default=None,
                     help="reduced system size (profiling only; not a bench line)")
@@ -398,6 +576,8 @@ def main():
     try:
         if args.impl == "reference":
             return run_reference(args, world, rank)
+        if args.config == "c4":
+            return run_batched(args, world, rank, local)
         return run_soil(args, world, rank, local)
     finally:
         if world > 1:

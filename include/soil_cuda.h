@@ -265,6 +265,9 @@ int soil_bin_sort_noalloc(soil_ctx* ctx, const double* d_x, const double* d_y,
  * no SOIL_COL_ZERO column.  While batched, a system's stream is the batch's
  * stream; every soil_sys_* readback stays valid between soil_batch_step calls.
  * Destroying a batched system removes it from its batch first. */
+/* Host planning of a step runs per box on a thread pool: SOIL_HOST_THREADS
+ * threads (default: hardware threads, at most 16), used when a step plans at
+ * least SOIL_HOST_MIN_PARALLEL boxes (default 64). */
 int soil_batch_create(soil_ctx* ctx, soil_batch** out);
 /* Detaches every member (the systems themselves are not destroyed). */
 int soil_batch_destroy(soil_batch* batch);
@@ -275,9 +278,26 @@ int soil_batch_size(soil_batch* batch, uint32_t* nsys);
 int soil_batch_step(soil_batch* batch, uint64_t nsteps);
 int soil_batch_sync(soil_batch* batch);
 int soil_batch_stream(soil_batch* batch, void** stream);
-/* Batched steps taken, host waits on the device, device bytes of the batch tables. */
+/* Stage timers of soil_batch_step (CUDA events on the batch stream):
+ * 0 integrate, 1 sort (pbc + spatial sort), 2 borders, 3 neighbor (fold
+ * program, forward comm, pair count pass), 4 lists (CSR fill, incoming
+ * lists), 5 force (the consumer kernel alone), 6 reverse (reverse comm, final),
+ * 7 whole step; the step time minus the stages is time the device waited for
+ * the host. */
+#define SOIL_BATCH_NUM_TIMERS 8
+/* Enables (on != 0) or disables the stage timers; resets every timer sum. */
+int soil_batch_set_timing(soil_batch* batch, int32_t on);
+int soil_batch_get_timing(soil_batch* batch, double* ms, uint64_t* intervals);
+/* Host milliseconds spent planning each part of the step (always measured,
+ * reset by soil_batch_set_timing): 0 integrate, 1 sort, 2 border planning,
+ * 3 border launches, 4 neighbor, 5 lists + force, 6 waiting for the device. */
+#define SOIL_BATCH_NUM_HOST_TIMERS 7
+int soil_batch_get_host_timing(soil_batch* batch, double* ms);
+/* Batched steps taken, host waits on the device, device bytes of the batch
+ * tables, and border passes repeated for a box whose ghosts outgrew its
+ * capacity (each repeat grows that box first). */
 int soil_batch_stats(soil_batch* batch, uint64_t* steps, uint64_t* host_waits,
-                     uint64_t* device_bytes);
+                     uint64_t* device_bytes, uint64_t* border_retries);
 
 /* ---- instrumentation (no reference counterpart: the reference has only
  * wall-clock thermo columns, soil_print/src/lib.rs:20-26) ------------------ */

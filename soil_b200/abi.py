@@ -165,7 +165,10 @@ PROTOTYPES = {
     "soil_batch_step": (C.c_int, [P, u64]),
     "soil_batch_sync": (C.c_int, [P]),
     "soil_batch_stream": (C.c_int, [P, PP]),
-    "soil_batch_stats": (C.c_int, [P, pu64, pu64, pu64]),
+    "soil_batch_stats": (C.c_int, [P, pu64, pu64, pu64, pu64]),
+    "soil_batch_set_timing": (C.c_int, [P, i32]),
+    "soil_batch_get_timing": (C.c_int, [P, pdbl, pu64]),
+    "soil_batch_get_host_timing": (C.c_int, [P, pdbl]),
     "soil_kernel_launches": (C.c_uint64, []),
     "soil_sys_set_timing": (C.c_int, [P, u32]),
     "soil_sys_get_timing": (C.c_int, [P, pdbl, pu64, pu64]),
@@ -175,6 +178,13 @@ PROTOTYPES = {
 SOIL_NUM_TIMERS = 10
 TIMER_NAMES = ["integrate", "zero", "pbc", "sort", "borders", "forward", "neighbor", "force",
                "reverse", "final"]
+
+SOIL_BATCH_NUM_TIMERS = 8
+BATCH_TIMER_NAMES = ["integrate", "sort", "borders", "neighbor", "lists", "force", "reverse",
+                     "step"]
+
+BATCH_HOST_TIMER_NAMES = ["integrate", "sort", "border_plan", "borders", "neighbor", "lists",
+                          "wait"]
 
 PHASES = [
     "deform", "initial", "decide_rebuild", "remove_ghosts", "zero_forces", "pbc",

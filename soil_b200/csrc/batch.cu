@@ -16,10 +16,16 @@
 // event, so a buffer is rewritten only after its previous copy finished.
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cstring>
 #include <deque>
 
+#include <cstdlib>
+#include <memory>
+#include <thread>
+
 #include "batch.cuh"
+#include "host_pool.h"
 #include "sys_internal.cuh"
 
 using namespace soil;
@@ -78,7 +84,7 @@ struct soil_batch {
     cudaStream_t st = nullptr;
     std::vector<soil_sys*> slot;      // nullptr: free slot
     std::vector<cudaStream_t> saved;  // each member's own stream while it is batched
-    std::vector<uint32_t> members;    // occupied slots, ascending
+    std::vector<uint32_t> members;    // occupied slots, largest box first
     uint32_t cap = 0;
     std::vector<BoxDev> h_dev;
     std::vector<BoxStep> h_step;
@@ -95,9 +101,27 @@ struct soil_batch {
     uint32_t* h_totals = nullptr;  // pinned
     uint64_t dev_bytes = 0;
     Stage stage[6];
-    uint64_t steps = 0, waits = 0;
+    uint64_t steps = 0, waits = 0, border_retries = 0;
+    // stage timers: device time between events recorded around each stage
+    struct Timed {
+        int stage;
+        cudaEvent_t a, z;
+    };
+    bool timing = false;
+    std::vector<Timed> timed;
+    std::vector<cudaEvent_t> ev_pool;
+    double stage_ms[SOIL_BATCH_NUM_TIMERS] = {};
+    uint64_t stage_n[SOIL_BATCH_NUM_TIMERS] = {};
+    cudaEvent_t open_a = nullptr;
+    cudaEvent_t step_a = nullptr;
+    // host time per planning section, waits excluded (and summed apart)
+    std::chrono::steady_clock::time_point hlast;
+    double host_ms[SOIL_BATCH_NUM_HOST_TIMERS] = {};
+    double wait_pending_ms = 0.0;
+    std::unique_ptr<HostPool> pool;  // per-box planning threads
+    size_t min_parallel = 64;        // fewer boxes are planned on the calling thread
     // per-step scratch
-    std::vector<uint8_t> check, full_at_pbc, run, periodic, apply, rebuild;
+    std::vector<uint8_t> check, full_at_pbc, run, periodic, apply, rebuild, planned;
 };
 
 namespace {
@@ -106,16 +130,12 @@ enum { G_INTEGRATE, G_SORT, G_SORT_APPLY, G_BORDERS, G_NEIGHBOR, G_FORCE };
 
 int balloc(soil_batch* b, void** p, uint64_t bytes) {
     if (bytes == 0) bytes = 16;
-    soil_ctx* c = b->ctx;
-    if (c->budget && c->in_use + bytes > c->budget)
-        return fail(c, SOIL_ERR_OOM, "HBM budget exceeded: %llu + %llu > %llu bytes",
-                    (unsigned long long)c->in_use, (unsigned long long)bytes,
-                    (unsigned long long)c->budget);
+    TRY(ctx_reserve(b->ctx, bytes));
     if (cudaMalloc(p, bytes) != cudaSuccess) {
         cudaGetLastError();
-        return fail(c, SOIL_ERR_OOM, "cudaMalloc(%llu) failed", (unsigned long long)bytes);
+        ctx_release(b->ctx, bytes);
+        return fail(b->ctx, SOIL_ERR_OOM, "cudaMalloc(%llu) failed", (unsigned long long)bytes);
     }
-    c->in_use += bytes;
     b->dev_bytes += bytes;
     return SOIL_OK;
 }
@@ -124,14 +144,34 @@ void bfree(soil_batch* b, void* p, uint64_t bytes) {
     if (!p) return;
     cudaFree(p);
     if (bytes == 0) bytes = 16;
-    b->ctx->in_use -= bytes;
+    ctx_release(b->ctx, bytes);
     b->dev_bytes -= bytes;
+}
+
+enum { HT_INTEGRATE, HT_SORT, HT_BORDER_PLAN, HT_BORDERS, HT_NEIGHBOR, HT_LISTS, HT_WAIT };
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
 int wait(soil_batch* b) {
     b->waits += 1;
-    BCK(cudaStreamSynchronize(b->st));
+    const auto t0 = std::chrono::steady_clock::now();
+    const cudaError_t e = cudaStreamSynchronize(b->st);
+    const double w = ms_since(t0);
+    b->host_ms[HT_WAIT] += w;
+    b->wait_pending_ms += w;
+    BCK(e);
     return SOIL_OK;
+}
+
+// close a host planning section: its time since the last mark, waits excluded
+void mark(soil_batch* b, int section) {
+    const auto now = std::chrono::steady_clock::now();
+    b->host_ms[section] += std::chrono::duration<double, std::milli>(now - b->hlast).count() -
+                           b->wait_pending_ms;
+    b->wait_pending_ms = 0.0;
+    b->hlast = now;
 }
 
 // ---- stages -------------------------------------------------------------------
@@ -229,6 +269,55 @@ int stage_commit(soil_batch* b, Stage& g) {
     BCK(cudaEventRecord(g.ev, b->st));
     g.pending = true;
     return SOIL_OK;
+}
+
+// ---- stage timers ---------------------------------------------------------------
+enum { BT_INTEGRATE, BT_SORT, BT_BORDERS, BT_NEIGHBOR, BT_LISTS, BT_FORCE, BT_REVERSE, BT_STEP };
+
+cudaEvent_t take_ev(soil_batch* b) {
+    if (!b->ev_pool.empty()) {
+        cudaEvent_t e = b->ev_pool.back();
+        b->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return e;
+}
+
+void tic(soil_batch* b) {
+    if (!b->timing) return;
+    b->open_a = take_ev(b);
+    if (b->open_a) cudaEventRecord(b->open_a, b->st);
+}
+
+void toc(soil_batch* b, int stage) {
+    if (!b->timing || !b->open_a) return;
+    cudaEvent_t z = take_ev(b);
+    if (!z) return;
+    cudaEventRecord(z, b->st);
+    b->timed.push_back({stage, b->open_a, z});
+    b->open_a = nullptr;
+}
+
+void resolve_timers(soil_batch* b) {
+    if (b->timed.empty()) return;
+    cudaStreamSynchronize(b->st);
+    for (auto& t : b->timed) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, t.a, t.z) == cudaSuccess) {
+            b->stage_ms[t.stage] += ms;
+            b->stage_n[t.stage] += 1;
+        } else {
+            cudaGetLastError();
+        }
+        b->ev_pool.push_back(t.a);
+        b->ev_pool.push_back(t.z);
+    }
+    b->timed.clear();
 }
 
 // ---- per-box tables -----------------------------------------------------------
@@ -453,7 +542,8 @@ int grow_slots(soil_batch* b, uint32_t need) {
     for (uint32_t k = 0; k < b->cap; ++k)
         if (b->slot[k]) b->dev_dirty[k] = b->step_dirty[k] = 1;
     b->binit.assign((size_t)ncap * kBorderStateWords, 0u);
-    for (auto* v : {&b->check, &b->full_at_pbc, &b->run, &b->periodic, &b->apply, &b->rebuild})
+    for (auto* v : {&b->check, &b->full_at_pbc, &b->run, &b->periodic, &b->apply, &b->rebuild,
+                    &b->planned})
         v->assign(ncap, 0);
     b->cap = ncap;
     return SOIL_OK;
@@ -463,10 +553,13 @@ int grow_slots(soil_batch* b, uint32_t need) {
 uint64_t tiles_of(uint64_t n) { return (n + kBorderTile - 1) / kBorderTile; }
 
 // Border passes of the boxes in R (three dims, count / scan / scatter each).
-int launch_borders(soil_batch* b, const std::vector<uint32_t>& R, Stage& g) {
+// retry: an earlier pass of this step ran; rows of boxes outside R then hold
+// finished results, which the upload of R's initial rows must keep.
+int launch_borders(soil_batch* b, const std::vector<uint32_t>& R, Stage& g, bool retry) {
     TRY(stage_begin(b, g));
     TRY(put_tables(b, g));
-    // initial border state of every box in R (rows of other boxes are unused)
+    if (retry) std::memcpy(b->binit.data(), b->h_bread, (size_t)b->cap * kBorderStateWords * 4);
+    // initial border state of every box in R
     uint32_t lo = b->cap, hi = 0;
     for (uint32_t k : R) {
         uint32_t* w = b->binit.data() + (size_t)k * kBorderStateWords;
@@ -491,15 +584,39 @@ int launch_borders(soil_batch* b, const std::vector<uint32_t>& R, Stage& g) {
     }
     TRY(stage_commit(b, g));
     const BatchArgs a = args_of(b);
+    tic(b);
     for (int dim = 0; dim < 3; ++dim) {
         b_border_count(b->st, g.out[sd[dim]], a, dim);
         b_border_scan(b->st, g.out[sd[dim]], a, dim);
         b_border_scatter(b->st, g.out[sd[dim]], a, dim);
     }
+    toc(b, BT_BORDERS);
     TRY(check_kernels(b));
     BCK(cudaMemcpyAsync(b->h_bread, b->d_bstate, (size_t)b->cap * kBorderStateWords * 4,
                         cudaMemcpyDeviceToHost, b->st));
     return wait(b);
+}
+
+// Host threads plan boxes in parallel; CUDA calls they make (allocations
+// when a box grows) need the context's device current on that thread.
+void bind_device(const soil_batch* b) {
+    thread_local int bound = -1;
+    if (bound != b->ctx->device) {
+        cudaSetDevice(b->ctx->device);
+        bound = b->ctx->device;
+    }
+}
+
+// fn(k) for every slot k of `ks` on the host pool; first failure wins.
+template <class F>
+int for_boxes(soil_batch* b, const std::vector<uint32_t>& ks, F fn) {
+    return b->pool->run(
+        ks.size(),
+        [&](size_t q) -> int {
+            bind_device(b);
+            return fn(ks[q]);
+        },
+        b->min_parallel);
 }
 
 int batch_step(soil_batch* b, bool last) {
@@ -508,6 +625,8 @@ int batch_step(soil_batch* b, bool last) {
     cudaStream_t st = b->st;
 
     // ---- deform, integrate (previous final fused in), displacement check ----
+    b->hlast = std::chrono::steady_clock::now();
+    b->wait_pending_ms = 0.0;
     Stage& g1 = b->stage[G_INTEGRATE];
     TRY(stage_begin(b, g1));
     TRY(put_tables(b, g1));
@@ -529,21 +648,26 @@ int batch_step(soil_batch* b, bool last) {
         s->pending_final = false;
     }
     TRY(stage_commit(b, g1));
+    if (b->timing) {
+        b->step_a = take_ev(b);
+        if (b->step_a) cudaEventRecord(b->step_a, st);
+    }
+    tic(b);
     b_final(st, g1.out[sp_final], a);
     b_profile(st, g1.out[sp_prof], a);
     BCK(cudaMemsetAsync(b->d_flags, 0, (size_t)b->cap * sizeof(DevFlags), st));
     b_initial(st, g1.out[sp_init], a);
+    toc(b, BT_INTEGRATE);
     TRY(check_kernels(b));
     if (any_check) {
         BCK(cudaMemcpyAsync(b->h_flags, b->d_flags, (size_t)b->cap * sizeof(DevFlags),
                             cudaMemcpyDeviceToHost, st));
         TRY(wait(b));
     }
+    mark(b, HT_INTEGRATE);
 
     // ---- decide_rebuild, remove_ghosts, pbc, spatial sort ----
-    std::vector<uint32_t> S, I;
-    bool any_pbc = false;
-    for (uint32_t k : M) {
+    TRY(for_boxes(b, M, [&](uint32_t k) -> int {
         soil_sys* s = b->slot[k];
         if (s->state == COMMUNICATE_ONLY) {
             const bool disp = b->check[k] && b->h_flags[k].rebuild != 0;
@@ -552,20 +676,30 @@ int batch_step(soil_batch* b, bool last) {
         }
         b->full_at_pbc[k] = s->state == FULL_REBUILD;
         if (b->full_at_pbc[k]) s->nghost = 0;  // remove_ghost_atoms
-        any_pbc |= b->full_at_pbc[k] != 0;
         bool run, periodic;
         TRY(sort_plan(s, &run, &periodic));
         b->run[k] = run;
         b->periodic[k] = periodic;
         b->apply[k] = run && !periodic;
-        if (run) {
-            S.push_back(k);
-            if (periodic) I.push_back(k);
-            fill_dev(b, k);
-            TRY(fill_step(b, k, b->apply[k] != 0, nullptr));
-        } else if (b->full_at_pbc[k]) {
-            TRY(fill_step(b, k, false, nullptr));
+        // a box that rebuilds gets its border dims and neighbor parameters now,
+        // so its step row is written once
+        b->planned[k] = s->state == FULL_REBUILD;
+        if (b->planned[k]) {
+            border_setup(s, b->bds[k].data());
+            neighbor_params(s);
         }
+        if (run) fill_dev(b, k);
+        if (run || b->planned[k])
+            TRY(fill_step(b, k, b->apply[k] != 0, b->planned[k] ? b->bds[k].data() : nullptr));
+        return SOIL_OK;
+    }));
+    std::vector<uint32_t> S, I;
+    bool any_pbc = false;
+    for (uint32_t k : M) {
+        any_pbc |= b->full_at_pbc[k] != 0;
+        if (!b->run[k]) continue;
+        S.push_back(k);
+        if (b->periodic[k]) I.push_back(k);
     }
     if (any_pbc || !S.empty()) {
         Stage& g2 = b->stage[G_SORT];
@@ -583,6 +717,7 @@ int batch_step(soil_batch* b, bool last) {
             if (b->apply[k]) g2.spans[s_gather].add_nz(k, s->nlocal, 0);
         }
         TRY(stage_commit(b, g2));
+        tic(b);
         b_pbc(st, g2.out[s_pbc], a);
         b_zero_counts(st, g2.out[s_cells], a, BA_CELLS);
         b_cells(st, g2.out[s_loc], a, false);
@@ -592,6 +727,7 @@ int batch_step(soil_batch* b, bool last) {
         b_permute_cells(st, g2.out[s_loc], a);
         b_identity(st, g2.out[s_id], a);
         b_perm_gather(st, g2.out[s_gather], a);
+        toc(b, BT_SORT);
         TRY(check_kernels(b));
     }
     if (!I.empty()) {
@@ -605,7 +741,7 @@ int batch_step(soil_batch* b, bool last) {
         for (uint32_t k : I) {
             b->apply[k] = b->h_flags[k].not_identity != 0;
             if (b->apply[k]) {
-                TRY(fill_step(b, k, true, nullptr));
+                TRY(fill_step(b, k, true, b->planned[k] ? b->bds[k].data() : nullptr));
                 g2b.spans[s_gather].add_nz(k, b->slot[k]->nlocal, 0);
             }
         }
@@ -615,46 +751,56 @@ int batch_step(soil_batch* b, bool last) {
         TRY(check_kernels(b));
     }
     for (uint32_t k : S) sort_done(b->slot[k], b->apply[k] != 0, b->periodic[k] != 0);
+    mark(b, HT_SORT);
 
     // ---- borders ----
     std::vector<uint32_t> R;
     for (uint32_t k : M) {
+        b->rebuild[k] = b->slot[k]->state == FULL_REBUILD;
+        if (b->rebuild[k]) R.push_back(k);
+    }
+    TRY(for_boxes(b, R, [&](uint32_t k) -> int {
         soil_sys* s = b->slot[k];
-        b->rebuild[k] = s->state == FULL_REBUILD;
-        if (!b->rebuild[k]) continue;
-        R.push_back(k);
         s->nghost = 0;
-        border_setup(s, b->bds[k].data());
+        if (!b->planned[k]) {  // became a rebuild through its periodic sort
+            border_setup(s, b->bds[k].data());
+            neighbor_params(s);
+        }
         TRY(borders_reserve(s));
         fill_dev(b, k);
-        TRY(fill_step(b, k, false, b->bds[k].data()));
-    }
+        // the row needs rewriting when the columns moved (set order changed)
+        if (!b->planned[k] || b->dev_dirty[k]) TRY(fill_step(b, k, false, b->bds[k].data()));
+        return SOIL_OK;
+    }));
+    mark(b, HT_BORDER_PLAN);
     if (!R.empty()) {
         std::vector<uint32_t> todo = R;
         for (int attempt = 0;; ++attempt) {
-            TRY(launch_borders(b, todo, b->stage[G_BORDERS]));
+            TRY(launch_borders(b, todo, b->stage[G_BORDERS], attempt > 0));
             std::vector<uint32_t> over;
             for (uint32_t k : todo)
                 if (b->h_bread[(size_t)k * kBorderStateWords + 10]) over.push_back(k);
             if (over.empty()) break;
             if (attempt == 3) return fail(b->ctx, SOIL_ERR_CAPACITY, "ghost capacity did not converge");
-            for (uint32_t k : over) {
+            b->border_retries += over.size();
+            TRY(for_boxes(b, over, [&](uint32_t k) -> int {
                 soil_sys* s = b->slot[k];
                 const uint32_t* hb = b->h_bread + (size_t)k * kBorderStateWords;
                 TRY(grow_atoms(s, (uint64_t)hb[3] + 1024, s->nlocal));
                 TRY(borders_arrays(s));
                 fill_dev(b, k);
-                TRY(fill_step(b, k, false, b->bds[k].data()));
-            }
+                return fill_step(b, k, false, b->bds[k].data());
+            }));
             todo.swap(over);
         }
-        for (uint32_t k : R) {
+        mark(b, HT_BORDERS);
+        TRY(for_boxes(b, R, [&](uint32_t k) -> int {
             soil_sys* s = b->slot[k];
             TRY(borders_done(s, b->h_bread + (size_t)k * kBorderStateWords, b->bds[k].data()));
             TRY(neighbor_plan(s));
             fill_dev(b, k);
-            TRY(fill_step(b, k, false, b->bds[k].data()));
-        }
+            return SOIL_OK;
+        }));
     }
 
     // ---- fold program, forward comm, neighbor build (pair count pass) ----
@@ -686,6 +832,7 @@ int batch_step(soil_batch* b, bool last) {
         g4.spans[n_rows].add(k, nl, 0);
     }
     TRY(stage_commit(b, g4));
+    tic(b);
     b_zero_counts(st, g4.out[f_scan], a, BA_FOLD);
     b_fold_count(st, g4.out[f_gh], a);
     b_scan(st, g4.out[f_scan], a, BA_FOLD);
@@ -703,12 +850,14 @@ int batch_step(soil_batch* b, bool last) {
         b_sorted_views(st, g4.out[n_all], a);
         b_pairs_rows(st, g4.out[f_loc], a);
         b_scan(st, g4.out[n_rows], a, BA_ROWS);
+        toc(b, BT_NEIGHBOR);
         TRY(check_kernels(b));
         BCK(cudaMemcpyAsync(b->h_totals, b->d_totals, (size_t)b->cap * 4, cudaMemcpyDeviceToHost, st));
         BCK(cudaMemcpyAsync(b->h_flags, b->d_flags, (size_t)b->cap * sizeof(DevFlags),
                             cudaMemcpyDeviceToHost, st));
         TRY(wait(b));
-        for (uint32_t k : R) {
+        mark(b, HT_NEIGHBOR);
+        TRY(for_boxes(b, R, [&](uint32_t k) -> int {
             soil_sys* s = b->slot[k];
             if (b->h_flags[k].error)
                 return fail(b->ctx, SOIL_ERR_INVALID,
@@ -725,7 +874,8 @@ int batch_step(soil_batch* b, bool last) {
             s->hflags->candidates = b->h_flags[k].candidates;
             s->hflags->rechecked = b->h_flags[k].rechecked;
             fill_dev(b, k);
-        }
+            return SOIL_OK;
+        }));
     }
 
     // ---- CSR fill, incoming lists, force, reverse comm, final ----
@@ -746,7 +896,9 @@ int batch_step(soil_batch* b, bool last) {
         if (s->newton && s->nghost) g5.spans[v_loc].add_nz(k, nl, 0);
         g5.spans[l_loc].add_nz(k, nl, 0);
     }
+    toc(b, BT_NEIGHBOR);  // no-op when the rebuild path closed it
     TRY(stage_commit(b, g5));
+    tic(b);
     if (!R.empty()) {
         b_pairs_fill(st, g5.out[r_loc], a);
         b_zero_counts(st, g5.out[r_scan], a, BA_IN);
@@ -755,23 +907,39 @@ int batch_step(soil_batch* b, bool last) {
         b_in_scatter(st, g5.out[r_loc], a);
         b_segsort(st, g5.out[r_all], a, BA_IN);
     }
+    toc(b, BT_LISTS);
+    tic(b);
     b_harmonic(st, g5.out[h_all], a);
+    toc(b, BT_FORCE);
+    tic(b);
     b_reverse(st, g5.out[v_loc], a);
     if (last) b_final(st, g5.out[l_loc], a);
+    toc(b, BT_REVERSE);
+    if (b->timing && b->step_a) {
+        b->open_a = b->step_a;
+        b->step_a = nullptr;
+        toc(b, BT_STEP);
+    }
     TRY(check_kernels(b));
     for (uint32_t k : M) {
         soil_sys* s = b->slot[k];
         s->pending_final = !last;
         s->steps_done += 1;
     }
+    mark(b, HT_LISTS);
     b->steps += 1;
     return SOIL_OK;
 }
 
+// Occupied slots, largest box first: segment-per-CTA kernels then start the
+// longest segments first.
 void rebuild_members(soil_batch* b) {
     b->members.clear();
     for (uint32_t k = 0; k < b->cap; ++k)
         if (b->slot[k]) b->members.push_back(k);
+    std::stable_sort(b->members.begin(), b->members.end(), [&](uint32_t x, uint32_t y) {
+        return b->slot[x]->nlocal > b->slot[y]->nlocal;
+    });
 }
 
 int detach(soil_batch* b, uint32_t k) {
@@ -805,6 +973,12 @@ int soil_batch_create(soil_ctx* ctx, soil_batch** out) {
     soil_batch* b = new (std::nothrow) soil_batch();
     if (!b) return SOIL_ERR_OOM;
     b->ctx = ctx;
+    // planning threads: SOIL_HOST_THREADS, else up to 16 hardware threads
+    int threads = (int)std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
+    if (const char* e = std::getenv("SOIL_HOST_THREADS")) threads = std::max(1, std::atoi(e));
+    if (const char* e = std::getenv("SOIL_HOST_MIN_PARALLEL"))
+        b->min_parallel = (size_t)std::max(1, std::atoi(e));
+    b->pool.reset(new HostPool(threads));
     if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess) {
         cudaGetLastError();
         delete b;
@@ -817,6 +991,10 @@ int soil_batch_create(soil_ctx* ctx, soil_batch** out) {
 int soil_batch_destroy(soil_batch* b) {
     if (!b) return SOIL_OK;
     cudaStreamSynchronize(b->st);
+    resolve_timers(b);
+    for (cudaEvent_t e : b->ev_pool) cudaEventDestroy(e);
+    if (b->open_a) cudaEventDestroy(b->open_a);
+    if (b->step_a) cudaEventDestroy(b->step_a);
     for (uint32_t k = 0; k < b->cap; ++k)
         if (b->slot[k]) detach(b, k);
     for (Stage& g : b->stage) {
@@ -905,11 +1083,41 @@ int soil_batch_stream(soil_batch* b, void** out) {
     return SOIL_OK;
 }
 
-int soil_batch_stats(soil_batch* b, uint64_t* steps, uint64_t* host_waits, uint64_t* device_bytes) {
+int soil_batch_set_timing(soil_batch* b, int32_t on) {
+    if (!b) return SOIL_ERR_INVALID;
+    resolve_timers(b);
+    b->timing = on != 0;
+    for (int t = 0; t < SOIL_BATCH_NUM_TIMERS; ++t) {
+        b->stage_ms[t] = 0.0;
+        b->stage_n[t] = 0;
+    }
+    for (int t = 0; t < SOIL_BATCH_NUM_HOST_TIMERS; ++t) b->host_ms[t] = 0.0;
+    return SOIL_OK;
+}
+
+int soil_batch_get_timing(soil_batch* b, double* ms, uint64_t* intervals) {
+    if (!b) return SOIL_ERR_INVALID;
+    resolve_timers(b);
+    for (int t = 0; t < SOIL_BATCH_NUM_TIMERS; ++t) {
+        if (ms) ms[t] = b->stage_ms[t];
+        if (intervals) intervals[t] = b->stage_n[t];
+    }
+    return SOIL_OK;
+}
+
+int soil_batch_get_host_timing(soil_batch* b, double* ms) {
+    if (!b || !ms) return SOIL_ERR_INVALID;
+    for (int t = 0; t < SOIL_BATCH_NUM_HOST_TIMERS; ++t) ms[t] = b->host_ms[t];
+    return SOIL_OK;
+}
+
+int soil_batch_stats(soil_batch* b, uint64_t* steps, uint64_t* host_waits, uint64_t* device_bytes,
+                     uint64_t* border_retries) {
     if (!b) return SOIL_ERR_INVALID;
     if (steps) *steps = b->steps;
     if (host_waits) *host_waits = b->waits;
     if (device_bytes) *device_bytes = b->dev_bytes;
+    if (border_retries) *border_retries = b->border_retries;
     return SOIL_OK;
 }
 

@@ -143,42 +143,74 @@ SPAN_KERNEL(kb_copy_count_local_cells, {
 SPAN_LAUNCH(b_copy_count_local_cells, kb_copy_count_local_cells)
 
 // One CTA per segment: out = exclusive scan of in over the segment's n
-// elements (out[n] = total), optional cursor copy.
+// elements (out[n] = total), optional cursor copy.  Each thread takes
+// kScanItems consecutive elements per pass (two 16-byte loads when the group
+// is whole; every array is its own allocation, so element 0 is 256-byte
+// aligned).  One CTA per segment lets the block scheduler balance boxes of
+// very different sizes; spans list the largest boxes first.
+constexpr int kScanItems = 8;
+
 __global__ void __launch_bounds__(kBlock) kb_scan(Span sp, BatchArgs A, int which) {
     __shared__ uint32_t tot;
-    for (uint32_t k = blockIdx.x; k < sp.nseg; k += gridDim.x) {
-        const uint32_t b = sp.box[k];
-        const BoxDev& D = A.dev[b];
-        const uint64_t n = sp.start[k + 1] - sp.start[k];
-        const uint32_t* in;
-        uint32_t *out, *cursor;
-        if (which == BA_ROWS) { in = D.rowcount; out = D.offsets; cursor = nullptr; }
-        else if (which == BA_IN) { in = D.in_count; out = D.in_start; cursor = D.in_cursor; }
-        else if (which == BA_FOLD) { in = D.fold_count; out = D.fold_start; cursor = D.fold_cursor; }
-        else { in = D.cell_counts; out = D.cell_start; cursor = D.cell_cursor; }
-        uint32_t carry = 0;
-        for (uint64_t b0 = 0; b0 < n; b0 += kBlock) {
-            const uint64_t t = b0 + threadIdx.x;
-            const uint32_t v = t < n ? in[t] : 0u;
-            const uint32_t pre = block_exclusive_scan(v, &tot) + carry;
-            if (t < n) {
-                out[t] = pre;
-                if (cursor) cursor[t] = pre;
+    const uint32_t k = blockIdx.x;
+    const uint32_t b = sp.box[k];
+    const BoxDev& D = A.dev[b];
+    const uint64_t n = sp.start[k + 1] - sp.start[k];
+    const uint32_t* in;
+    uint32_t *out, *cursor;
+    if (which == BA_ROWS) { in = D.rowcount; out = D.offsets; cursor = nullptr; }
+    else if (which == BA_IN) { in = D.in_count; out = D.in_start; cursor = D.in_cursor; }
+    else if (which == BA_FOLD) { in = D.fold_count; out = D.fold_start; cursor = D.fold_cursor; }
+    else { in = D.cell_counts; out = D.cell_start; cursor = D.cell_cursor; }
+    uint32_t carry = 0;
+    for (uint64_t b0 = 0; b0 < n; b0 += (uint64_t)kBlock * kScanItems) {
+        const uint64_t t0 = b0 + (uint64_t)threadIdx.x * kScanItems;
+        uint32_t v[kScanItems];
+        const bool whole = t0 + kScanItems <= n;
+        if (whole) {
+            const uint4 p = *reinterpret_cast<const uint4*>(in + t0);
+            const uint4 q = *reinterpret_cast<const uint4*>(in + t0 + 4);
+            v[0] = p.x; v[1] = p.y; v[2] = p.z; v[3] = p.w;
+            v[4] = q.x; v[5] = q.y; v[6] = q.z; v[7] = q.w;
+        } else {
+            for (int j = 0; j < kScanItems; ++j) v[j] = t0 + j < n ? in[t0 + j] : 0u;
+        }
+        uint32_t sum = 0;
+        for (int j = 0; j < kScanItems; ++j) sum += v[j];
+        uint32_t run = block_exclusive_scan(sum, &tot) + carry;
+        for (int j = 0; j < kScanItems; ++j) {
+            const uint32_t x = v[j];
+            v[j] = run;
+            run += x;
+        }
+        if (whole) {
+            const uint4 p = make_uint4(v[0], v[1], v[2], v[3]);
+            const uint4 q = make_uint4(v[4], v[5], v[6], v[7]);
+            *reinterpret_cast<uint4*>(out + t0) = p;
+            *reinterpret_cast<uint4*>(out + t0 + 4) = q;
+            if (cursor) {
+                *reinterpret_cast<uint4*>(cursor + t0) = p;
+                *reinterpret_cast<uint4*>(cursor + t0 + 4) = q;
             }
-            carry += tot;
-            __syncthreads();
+        } else {
+            for (int j = 0; j < kScanItems; ++j)
+                if (t0 + j < n) {
+                    out[t0 + j] = v[j];
+                    if (cursor) cursor[t0 + j] = v[j];
+                }
         }
-        if (threadIdx.x == 0) {
-            out[n] = carry;
-            if (which == BA_ROWS) A.totals[b] = carry;
-        }
+        carry += tot;
         __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[n] = carry;
+        if (which == BA_ROWS) A.totals[b] = carry;
     }
 }
 void b_scan(cudaStream_t st, const Span& sp, const BatchArgs& a, int which) {
     if (sp.nseg == 0) return;
     note_launch();
-    kb_scan<<<sp.nseg < 148u * 8u ? sp.nseg : 148u * 8u, kBlock, 0, st>>>(sp, a, which);
+    kb_scan<<<sp.nseg, kBlock, 0, st>>>(sp, a, which);
 }
 
 __global__ void __launch_bounds__(kBlock) kb_scatter(Span sp, BatchArgs A, int neighbor) {

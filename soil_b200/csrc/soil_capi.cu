@@ -40,24 +40,43 @@ int fail(soil_ctx* ctx, int status, const char* fmt, ...) {
         va_start(ap, fmt);
         vsnprintf(buf, sizeof buf, fmt, ap);
         va_end(ap);
+        std::lock_guard<std::mutex> g(ctx->mu);
         ctx->err = buf;
     }
     return status;
 }
 
+// Reserve `bytes` of the context's HBM budget (thread-safe: the batch engine
+// plans boxes on several host threads).
+int ctx_reserve(soil_ctx* ctx, uint64_t bytes) {
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (ctx->budget && ctx->in_use + bytes > ctx->budget) {
+        char buf[160];
+        snprintf(buf, sizeof buf, "HBM budget exceeded: %llu + %llu > %llu bytes",
+                 (unsigned long long)ctx->in_use, (unsigned long long)bytes,
+                 (unsigned long long)ctx->budget);
+        ctx->err = buf;
+        return SOIL_ERR_OOM;
+    }
+    ctx->in_use += bytes;
+    return SOIL_OK;
+}
+
+void ctx_release(soil_ctx* ctx, uint64_t bytes) {
+    std::lock_guard<std::mutex> g(ctx->mu);
+    ctx->in_use -= bytes;
+}
+
 int dev_alloc(soil_sys* s, void** p, uint64_t bytes) {
     if (bytes == 0) bytes = 16;
-    if (s->ctx->budget && s->ctx->in_use + bytes > s->ctx->budget)
-        return fail(s->ctx, SOIL_ERR_OOM, "HBM budget exceeded: %llu + %llu > %llu bytes",
-                    (unsigned long long)s->ctx->in_use, (unsigned long long)bytes,
-                    (unsigned long long)s->ctx->budget);
+    TRY(ctx_reserve(s->ctx, bytes));
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
+        ctx_release(s->ctx, bytes);
         return fail(s->ctx, SOIL_ERR_OOM, "cudaMalloc(%llu): %s", (unsigned long long)bytes,
                     cudaGetErrorString(e));
     }
-    s->ctx->in_use += bytes;
     return SOIL_OK;
 }
 
@@ -65,7 +84,7 @@ void dev_free(soil_sys* s, void* p, uint64_t bytes) {
     if (!p) return;
     cudaFree(p);
     if (bytes == 0) bytes = 16;
-    s->ctx->in_use -= bytes;
+    ctx_release(s->ctx, bytes);
 }
 
 // ---- per-atom columns -------------------------------------------------------
@@ -701,15 +720,9 @@ int build_in_lists(soil_sys* s) {
 // bin_neighbor_list (neighbor.rs:1013-1319), host part: the CommState
 // transition, save_build_positions bookkeeping (neighbor.rs:669-690; the local
 // cutoff radii never change after setup, so their min/max are cached there),
-// the uniform-cutoff decision and room for the build.
-int neighbor_plan(soil_sys* s) {
-    s->state = COMMUNICATE_ONLY;
-    const uint64_t nl = s->nlocal;
-    TRY(ensure(s, s->lbx, s->acap));
-    TRY(ensure(s, s->lby, s->acap));
-    TRY(ensure(s, s->lbz, s->acap));
-    s->last_build_n = nl;
-    s->steps_since_build = 0;
+// the uniform-cutoff decision (neighbor_params, a function of those constants
+// only) and room for the build.
+void neighbor_params(soil_sys* s) {
     s->cached_min_skin = s->cut_min_local;
     if (std::fabs(s->cut_max_local - s->cut_min_local) < 1e-15) {
         const double cutoff = 2.0 * s->cut_min_local * s->skin_fraction;
@@ -718,6 +731,17 @@ int neighbor_plan(soil_sys* s) {
     } else {
         s->has_uniform = false;
     }
+}
+
+int neighbor_plan(soil_sys* s) {
+    s->state = COMMUNICATE_ONLY;
+    const uint64_t nl = s->nlocal;
+    TRY(ensure(s, s->lbx, s->acap));
+    TRY(ensure(s, s->lby, s->acap));
+    TRY(ensure(s, s->lbz, s->acap));
+    s->last_build_n = nl;
+    s->steps_since_build = 0;
+    neighbor_params(s);
     const uint64_t nc = s->total_cells;
     TRY(ensure(s, s->atom_cell, s->acap));
     TRY(ensure(s, s->sorted_atoms, s->acap));
@@ -950,7 +974,10 @@ using namespace soil_host;
 namespace soil {
 // Records `msg` as the context's last error (ctx may be NULL) and returns status.
 int set_ctx_error(soil_ctx* ctx, int status, const char* msg) {
-    if (ctx) ctx->err = msg;
+    if (ctx) {
+        std::lock_guard<std::mutex> g(ctx->mu);
+        ctx->err = msg;
+    }
     return status;
 }
 }  // namespace soil
@@ -992,6 +1019,7 @@ const char* soil_last_error(const soil_ctx* ctx) { return ctx ? ctx->err.c_str()
 
 int soil_ctx_bytes_in_use(const soil_ctx* ctx, uint64_t* out) {
     if (!ctx || !out) return SOIL_ERR_INVALID;
+    std::lock_guard<std::mutex> g(ctx->mu);
     *out = ctx->in_use;
     return SOIL_OK;
 }

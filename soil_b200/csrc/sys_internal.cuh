@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cfloat>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -16,6 +17,7 @@ struct soil_ctx {
     uint64_t budget = 0;
     uint64_t in_use = 0;
     std::string err;
+    mutable std::mutex mu;  // guards in_use and err
 };
 
 namespace soil_host {
@@ -164,6 +166,8 @@ int fail(soil_ctx* ctx, int status, const char* fmt, ...);
         if (r_ != SOIL_OK) return r_;    \
     } while (0)
 
+int ctx_reserve(soil_ctx* ctx, uint64_t bytes);
+void ctx_release(soil_ctx* ctx, uint64_t bytes);
 int dev_alloc(soil_sys* s, void** p, uint64_t bytes);
 void dev_free(soil_sys* s, void* p, uint64_t bytes);
 
@@ -194,6 +198,7 @@ void border_setup(const soil_sys* s, BorderDim bds[3]);
 int borders_reserve(soil_sys* s);
 int borders_arrays(soil_sys* s);
 int borders_done(soil_sys* s, const uint32_t* hb, const BorderDim bds[3]);
+void neighbor_params(soil_sys* s);
 int neighbor_plan(soil_sys* s);
 float pair_eps(const soil_sys* s);
 int sync(soil_sys* s);

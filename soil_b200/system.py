@@ -267,11 +267,30 @@ class Batch:
         self.ctx.check(self.lib.soil_batch_stream(self.h, C.byref(v)), "soil_batch_stream")
         return v.value
 
+    def set_timing(self, on=True):
+        self.ctx.check(self.lib.soil_batch_set_timing(self.h, 1 if on else 0), "batch timing")
+
+    def get_timing(self):
+        """{stage: (ms, intervals)} summed since set_timing."""
+        ms = np.zeros(abi.SOIL_BATCH_NUM_TIMERS)
+        iv = np.zeros(abi.SOIL_BATCH_NUM_TIMERS, np.uint64)
+        self.ctx.check(self.lib.soil_batch_get_timing(self.h, _p(ms, C.c_double),
+                                                      _p(iv, C.c_uint64)), "batch timing")
+        return {n: (float(ms[k]), int(iv[k])) for k, n in enumerate(abi.BATCH_TIMER_NAMES)}
+
+    def get_host_timing(self):
+        """{section: host ms} of step planning since set_timing."""
+        ms = np.zeros(len(abi.BATCH_HOST_TIMER_NAMES))
+        self.ctx.check(self.lib.soil_batch_get_host_timing(self.h, _p(ms, C.c_double)),
+                       "batch host timing")
+        return {n: float(ms[k]) for k, n in enumerate(abi.BATCH_HOST_TIMER_NAMES)}
+
     def stats(self):
-        st, w, b = C.c_uint64(), C.c_uint64(), C.c_uint64()
-        self.ctx.check(self.lib.soil_batch_stats(self.h, C.byref(st), C.byref(w), C.byref(b)),
-                       "soil_batch_stats")
-        return dict(steps=st.value, host_waits=w.value, device_bytes=b.value)
+        st, w, b, r = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
+        self.ctx.check(self.lib.soil_batch_stats(self.h, C.byref(st), C.byref(w), C.byref(b),
+                                                 C.byref(r)), "soil_batch_stats")
+        return dict(steps=st.value, host_waits=w.value, device_bytes=b.value,
+                    border_retries=r.value)
 
 
 def from_workload(ctx, w):

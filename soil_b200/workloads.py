@@ -157,11 +157,20 @@ def config3(n=1048576, steps=5000):
     return mono("C3-shear-1048576", 3, n, 0.40, 1e-4, steps, harmonic_k=1e3, shear_rate=0.1)
 
 
+C4_BOXES = 4096
+
+
+def config4_size(i, nmin=256, nmax=65536):
+    """Atom count of box i of the batched configuration (log-uniform)."""
+    u = uniform(4, i, 90, 1)
+    return int(round(math.exp(math.log(nmin) + (math.log(nmax) - math.log(nmin)) * u[0])))
+
+
 def config4_box(i, nmin=256, nmax=65536, steps=1000):
     """Box i of the batched configuration (seed 4 + box id)."""
     s = 4
     u = uniform(s, i, 90, 4)
-    n = int(round(math.exp(math.log(nmin) + (math.log(nmax) - math.log(nmin)) * u[0])))
+    n = config4_size(i, nmin, nmax)
     phi = 0.20 + 0.35 * u[1]
     rate = 0.0 if i % 2 == 0 else 0.01 + 0.19 * u[2]
     return poly(f"C4-box{i}", s, n, phi, 1e-4, steps, harmonic_k=1e3, shear_rate=rate, box=i)

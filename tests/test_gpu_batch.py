@@ -27,8 +27,11 @@ def mixed_boxes(count=8, nmax=3000):
         if i == 5:
             w.cfg.newton = 0
         ws.append(w)
-    # a fast-sheared box whose tilt wraps inside the run
-    ws.append(W.mono("fast-shear", 9, 1500, 0.4, 1e-3, 40, harmonic_k=1e3, shear_rate=5.0))
+    # a fast-sheared box whose tilt wraps inside the run, with periodic sorts
+    # on top of its every-step rebuilds
+    w = W.mono("fast-shear", 9, 1500, 0.4, 1e-3, 40, harmonic_k=1e3, shear_rate=5.0)
+    w.cfg.sort_every = 5
+    ws.append(w)
     return ws
 
 
@@ -65,6 +68,45 @@ def test_batch_equals_alone(ctx):
     batch.close()
     for s in alone + mixed:
         s.close()
+
+
+def test_batch_threaded_planning_equals_alone(ctx, monkeypatch):
+    """The same boxes planned on four host threads (parallel from one box)."""
+    monkeypatch.setenv("SOIL_HOST_THREADS", "4")
+    monkeypatch.setenv("SOIL_HOST_MIN_PARALLEL", "1")
+    ws = mixed_boxes()
+    alone = [system.from_workload(ctx, w) for w in ws]
+    mixed = [system.from_workload(ctx, w) for w in ws]
+    for s in alone:
+        s.step(31)
+    batch = system.Batch(ctx)
+    for s in mixed:
+        batch.add(s)
+    batch.step(31)
+    for k, (a, m) in enumerate(zip(alone, mixed)):
+        assert_same(a, m, f"box {k} ({ws[k].name})")
+    batch.close()
+
+
+def test_batch_fresh_boxes_ghost_growth(ctx):
+    """Fresh boxes (first step in the batch) whose ghosts outgrow the first
+    reservation, next to small boxes: the border pass is repeated for the
+    large ones only, and every box still matches its alone run."""
+    ws = [W.poly(f"dense{i}", 11, n, 0.55, 1e-4, 10, harmonic_k=1e3, box=i)
+          for i, n in enumerate([20000, 300, 24000, 280, 500, 16000])]
+    ws[2].shear_rate = 0.1
+    alone = [system.from_workload(ctx, w) for w in ws]
+    mixed = [system.from_workload(ctx, w) for w in ws]
+    for s in alone:
+        s.step(6)
+    batch = system.Batch(ctx)
+    for s in mixed:
+        batch.add(s)
+    batch.step(6)
+    for k, (a, m) in enumerate(zip(alone, mixed)):
+        assert_same(a, m, f"box {k} ({ws[k].name})")
+    assert batch.stats()["border_retries"] > 0
+    batch.close()
 
 
 def test_batch_equals_oracle(ctx):
