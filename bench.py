@@ -497,6 +497,116 @@ def run_batched(args, world, rank, local):
     return 0
 
 
+# ---- served configuration ---------------------------------------------------------
+C5_DESC = ("C5 served: Poisson arrivals at 80% of the plain path's measured throughput; "
+           "jobs N log-uniform [1,024, 262,144], phi U[0.20,0.55], r~U[0.4,0.6], shear rate "
+           "U[0,0.2], steps U[500,5,000], FP32+FP64-recheck filter, harmonic k=1e3, dt 1e-4, "
+           "150 GB HBM budget")
+
+
+def run_served(args, world, rank, local):
+    """C5: continuous batching through soil_server_* against the plain path
+    (each job alone through soil_step, one at a time in arrival order)."""
+    import threading
+
+    import torch
+    from soil_b200 import serve, system
+
+    jobs = [workloads.config5_job(i) for i in range(args.jobs)]
+    # partition jobs over ranks (independent units); each rank serves its own
+    mine = lpt_partition([w.n * w.steps for w in jobs], world)[rank]
+    jobs = [jobs[i] for i in mine]
+    work = np.array([w.n * w.steps for w in jobs], dtype=np.float64)
+
+    # plain path: every job alone, `sample` steps after one untimed step; its
+    # service time is setup + steps x the sampled per-step time
+    ctx = system.Context(local)
+    lib = abi.load_library()
+    sample = max(args.plain_steps, 20)
+    service = []
+    for w in jobs:
+        t0 = time.perf_counter()
+        s = system.from_workload(ctx, w)
+        s.step(1)
+        s.sync()
+        t_setup = time.perf_counter() - t0
+        st = torch.cuda.ExternalStream(s.stream(), device=torch.device("cuda", local))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        s.step(sample)
+        e1.record(st)
+        s.sync()
+        per_step = e0.elapsed_time(e1) * 1e-3 / sample
+        service.append(t_setup + per_step * (w.steps - 1) + per_step)
+        s.close()
+    service = np.array(service)
+    plain_rate = work.sum() / service.sum()           # atom-steps/s of the plain path
+    rate = args.load * plain_rate / work.mean()        # jobs/s
+    arrivals = serve.poisson_arrivals(rate, len(jobs), seed=5 + rank)
+    plain_lat = serve.fifo_latencies(arrivals, service)
+    del ctx
+
+    sctx = system.Context(local)
+    sv = serve.Server(sctx, hbm_budget_bytes=int(args.budget_gb * 1e9), quantum_steps=args.quantum)
+    ids = [None] * len(jobs)
+    launches0 = lib.soil_kernel_launches()
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier(world)
+    t_start = time.perf_counter()
+
+    def submitter():
+        for k, w in enumerate(jobs):
+            d = arrivals[k] - (time.perf_counter() - t_start)
+            if d > 0:
+                time.sleep(d)
+            ids[k] = sv.submit(w)
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    th.join()
+    infos = [sv.wait(j) for j in ids]
+    t_end = time.perf_counter()
+    clocks = sampler.stop()
+    launches = lib.soil_kernel_launches() - launches0
+    st = sv.stats()
+    sv.close()
+    states = [i["state"] for i in infos]
+    lat = np.array([i["t_done"] - i["t_submit"] for i in infos])
+    makespan = max_over_ranks(t_end - t_start, world)
+    total_work = sum_over_ranks(float(work.sum()), world)
+    if rank == 0:
+        line = {
+            "metric": "atom-steps/s", "value": total_work / makespan, "unit": "atom-steps/s",
+            "n_gpus": world, "steps": int(sum(w.steps for w in jobs)), "warmup": 0,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded SplitMix64 per job, Box-Muller velocities, seeded "
+                    "Poisson arrivals)",
+            "config": {"workload": C5_DESC, "jobs": len(jobs), "load": args.load,
+                       "arrival_rate_per_s": rate, "quantum_steps": args.quantum,
+                       "budget_gb": args.budget_gb},
+            "served": {"p50_latency_s": float(np.percentile(lat, 50)),
+                       "p99_latency_s": float(np.percentile(lat, 99)),
+                       "mean_latency_s": float(lat.mean()),
+                       "capacity_atom_steps_per_s": st["atom_steps"] / max(st["busy_s"], 1e-9),
+                       "makespan_s": makespan, "max_resident_jobs": st["max_active"],
+                       "states": {x: states.count(x) for x in set(states)}},
+            "plain_per_job": {"value": plain_rate, "unit": "atom-steps/s",
+                              "p50_latency_s": float(np.percentile(plain_lat, 50)),
+                              "p99_latency_s": float(np.percentile(plain_lat, 99)),
+                              "what": ("each job alone through soil_step, one at a time in "
+                                       "arrival order (FIFO); service = measured setup + steps x "
+                                       f"per-step time sampled over {sample} steps")},
+            "served_over_plain_capacity": st["atom_steps"] / max(st["busy_s"], 1e-9) / plain_rate,
+            "roofline": None, "cpu_baseline": None, "e2e": None,
+            "gpu_launches": int(launches), "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def sum_over_ranks(x, world):
     if world == 1:
         return x
@@ -559,11 +669,16 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["soil", "reference"], default="soil")
-    ap.add_argument("--config", choices=["c1", "c2", "c3", "c4"], default="c2")
+    ap.add_argument("--config", choices=["c1", "c2", "c3", "c4", "c5"], default="c2")
+    ap.add_argument("--jobs", type=int, default=48, help="c5: number of jobs")
+    ap.add_argument("--load", type=float, default=0.8,
+                    help="c5: arrival rate as a fraction of the plain path's throughput")
+    ap.add_argument("--quantum", type=int, default=50, help="c5: steps between admissions")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="c5: HBM budget")
     ap.add_argument("--boxes", type=int, default=workloads.C4_BOXES,
                     help="c4: number of boxes (4096 is the configuration)")
     ap.add_argument("--plain-steps", type=int, default=4,
-                    help="c4: timed steps of each box alone (plain path; 0 skips it)")
+                    help="c4/c5: timed steps of each box alone (plain path; 0 skips it in c4)")
     ap.add_argument("--filter", choices=["fp64", "fp32"], default="fp64")
     ap.add_argument("--natoms", type=int, default=None,
                     help="reduced system size (profiling only; not a bench line)")
@@ -578,6 +693,8 @@ def main():
             return run_reference(args, world, rank)
         if args.config == "c4":
             return run_batched(args, world, rank, local)
+        if args.config == "c5":
+            return run_served(args, world, rank, local)
         return run_soil(args, world, rank, local)
     finally:
         if world > 1:

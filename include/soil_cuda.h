@@ -299,6 +299,92 @@ int soil_batch_get_host_timing(soil_batch* batch, double* ms);
 int soil_batch_stats(soil_batch* batch, uint64_t* steps, uint64_t* host_waits,
                      uint64_t* device_bytes, uint64_t* border_retries);
 
+/* ---- served mode (no reference counterpart: the reference runs one App per
+ * process) ------------------------------------------------------------------
+ * A request loop on its own host thread admits jobs first come first served
+ * while their HBM reservation (natoms * bytes_per_atom + bytes_per_job) fits
+ * hbm_budget_bytes and fewer than max_active jobs are resident, keeps every
+ * admitted job resident in one soil_batch, advances them together in quanta
+ * of at most quantum_steps steps (never past any job's own step count), and
+ * retires finished jobs (final state read back, memory freed).  Each job's
+ * result is bit-identical to the same system run alone through soil_step.
+ * The server's context belongs to the loop thread: do not use it elsewhere
+ * while the server exists.  Zero fields take defaults (no budget, 65,536
+ * jobs, 50 steps, 1,024 B/atom, 8 MiB/job). */
+typedef struct soil_server soil_server;
+typedef struct soil_server_cfg {
+    uint64_t hbm_budget_bytes;
+    uint32_t max_active;
+    uint32_t quantum_steps;
+    uint32_t bytes_per_atom;
+    uint32_t bytes_per_job;
+} soil_server_cfg;
+/* One job: a periodic box of spheres with the harmonic consumer (radius
+ * column #[forward]), optional xy shear, run for `steps` timesteps.  Arrays
+ * are copied by soil_server_submit. */
+typedef struct soil_job_spec {
+    soil_box box;
+    soil_neigh_cfg cfg;
+    double dt;
+    uint64_t natoms;
+    const uint32_t* tag;
+    const double* pos3;
+    const double* vel3;
+    const double* mass;
+    const double* cutoff_radius;
+    const double* radius;
+    double harmonic_k;
+    double shear_rate;
+    uint64_t steps;
+} soil_job_spec;
+typedef enum soil_job_state {
+    SOIL_JOB_QUEUED = 0,
+    SOIL_JOB_RUNNING = 1,
+    SOIL_JOB_DONE = 2,
+    SOIL_JOB_FAILED = 3,
+    SOIL_JOB_CANCELLED = 4
+} soil_job_state;
+/* Times are seconds since the server was created (t_admit, t_done < 0: not yet). */
+typedef struct soil_job_info {
+    int32_t state;
+    uint64_t natoms;
+    uint64_t steps;
+    uint64_t steps_done;
+    double t_submit;
+    double t_admit;
+    double t_done;
+} soil_job_info;
+typedef struct soil_server_stats {
+    uint64_t queued;
+    uint64_t admitted;
+    uint64_t completed;
+    uint64_t failed;          /* failed or cancelled */
+    uint64_t atom_steps;      /* sum over batch steps of resident atoms */
+    uint64_t batch_steps;
+    double busy_s;            /* host time inside batch steps */
+    double elapsed_s;
+    uint64_t reserved_bytes;
+    int32_t max_active;       /* most jobs resident at once */
+} soil_server_stats;
+int soil_server_create(soil_ctx* ctx, const soil_server_cfg* cfg, soil_server** out);
+/* Stops the loop; queued and resident jobs end as SOIL_JOB_CANCELLED. */
+int soil_server_destroy(soil_server* server);
+int soil_server_submit(soil_server* server, const soil_job_spec* job, uint64_t* job_id);
+int soil_server_poll(soil_server* server, uint64_t job_id, soil_job_info* info);
+/* Blocks until the job is done, failed or cancelled (timeout_s < 0: no limit);
+ * SOIL_ERR_TIMEOUT when the limit passes first. */
+int soil_server_wait(soil_server* server, uint64_t job_id, double timeout_s, soil_job_info* info);
+int soil_server_cancel(soil_server* server, uint64_t job_id);
+/* Final local atoms of a done job, in the system's final (spatially sorted)
+ * order: tags, positions, velocities, image flags; any output may be NULL. */
+int soil_server_result(soil_server* server, uint64_t job_id, uint32_t* tag, double* pos3,
+                       double* vel3, int32_t* image3);
+/* Forgets a finished job (its results included). */
+int soil_server_release(soil_server* server, uint64_t job_id);
+/* Error message of a failed job. */
+int soil_server_job_error(soil_server* server, uint64_t job_id, char* buf, uint64_t len);
+int soil_server_get_stats(soil_server* server, soil_server_stats* out);
+
 /* ---- instrumentation (no reference counterpart: the reference has only
  * wall-clock thermo columns, soil_print/src/lib.rs:20-26) ------------------ */
 /* Kernels this library has launched in this process. */

@@ -105,6 +105,64 @@ class SoilDevView(C.Structure):
 
 SOIL_FORCE_FN = C.CFUNCTYPE(C.c_int, C.POINTER(SoilDevView), C.c_void_p)
 
+SOIL_JOB_QUEUED, SOIL_JOB_RUNNING, SOIL_JOB_DONE, SOIL_JOB_FAILED, SOIL_JOB_CANCELLED = range(5)
+JOB_STATES = ["queued", "running", "done", "failed", "cancelled"]
+
+
+class SoilServerCfg(C.Structure):
+    _fields_ = [
+        ("hbm_budget_bytes", C.c_uint64),
+        ("max_active", C.c_uint32),
+        ("quantum_steps", C.c_uint32),
+        ("bytes_per_atom", C.c_uint32),
+        ("bytes_per_job", C.c_uint32),
+    ]
+
+
+class SoilJobSpec(C.Structure):
+    _fields_ = [
+        ("box", SoilBox),
+        ("cfg", SoilNeighCfg),
+        ("dt", C.c_double),
+        ("natoms", C.c_uint64),
+        ("tag", C.POINTER(C.c_uint32)),
+        ("pos3", C.POINTER(C.c_double)),
+        ("vel3", C.POINTER(C.c_double)),
+        ("mass", C.POINTER(C.c_double)),
+        ("cutoff_radius", C.POINTER(C.c_double)),
+        ("radius", C.POINTER(C.c_double)),
+        ("harmonic_k", C.c_double),
+        ("shear_rate", C.c_double),
+        ("steps", C.c_uint64),
+    ]
+
+
+class SoilJobInfo(C.Structure):
+    _fields_ = [
+        ("state", C.c_int32),
+        ("natoms", C.c_uint64),
+        ("steps", C.c_uint64),
+        ("steps_done", C.c_uint64),
+        ("t_submit", C.c_double),
+        ("t_admit", C.c_double),
+        ("t_done", C.c_double),
+    ]
+
+
+class SoilServerStats(C.Structure):
+    _fields_ = [
+        ("queued", C.c_uint64),
+        ("admitted", C.c_uint64),
+        ("completed", C.c_uint64),
+        ("failed", C.c_uint64),
+        ("atom_steps", C.c_uint64),
+        ("batch_steps", C.c_uint64),
+        ("busy_s", C.c_double),
+        ("elapsed_s", C.c_double),
+        ("reserved_bytes", C.c_uint64),
+        ("max_active", C.c_int32),
+    ]
+
 P = C.c_void_p
 PP = C.POINTER(C.c_void_p)
 u64 = C.c_uint64
@@ -169,6 +227,16 @@ PROTOTYPES = {
     "soil_batch_set_timing": (C.c_int, [P, i32]),
     "soil_batch_get_timing": (C.c_int, [P, pdbl, pu64]),
     "soil_batch_get_host_timing": (C.c_int, [P, pdbl]),
+    "soil_server_create": (C.c_int, [P, C.POINTER(SoilServerCfg), PP]),
+    "soil_server_destroy": (C.c_int, [P]),
+    "soil_server_submit": (C.c_int, [P, C.POINTER(SoilJobSpec), pu64]),
+    "soil_server_poll": (C.c_int, [P, u64, C.POINTER(SoilJobInfo)]),
+    "soil_server_wait": (C.c_int, [P, u64, dbl, C.POINTER(SoilJobInfo)]),
+    "soil_server_cancel": (C.c_int, [P, u64]),
+    "soil_server_result": (C.c_int, [P, u64, pu32, pdbl, pdbl, pi32]),
+    "soil_server_release": (C.c_int, [P, u64]),
+    "soil_server_job_error": (C.c_int, [P, u64, C.c_char_p, u64]),
+    "soil_server_get_stats": (C.c_int, [P, C.POINTER(SoilServerStats)]),
     "soil_kernel_launches": (C.c_uint64, []),
     "soil_sys_set_timing": (C.c_int, [P, u32]),
     "soil_sys_get_timing": (C.c_int, [P, pdbl, pu64, pu64]),

@@ -16,26 +16,38 @@ namespace soil {
 
 constexpr int kSpanItems = 4;
 
-__device__ __forceinline__ uint32_t seg_of(const Span& sp, uint64_t g) {
-    uint32_t lo = 0, hi = sp.nseg - 1;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi + 1) >> 1;
-        if (sp.start[mid] <= g) lo = mid;
-        else hi = mid - 1;
+// Segment holding flattened element g (the last segment whose start is <= g),
+// found by the 32 lanes of one warp together: each level probes 32 evenly
+// spaced starts, so 4,096 segments take three dependent loads.  Call with all
+// 32 lanes of the warp; every lane returns the answer.
+__device__ __forceinline__ uint32_t seg_of_warp(const Span& sp, uint64_t g) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t lo = 0, hi = sp.nseg;  // start[lo] <= g < start[hi]
+    while (hi - lo > 1) {
+        const uint32_t step = (hi - lo + 31) / 32;
+        const uint32_t idx = lo + lane * step;
+        const bool ok = idx < hi && sp.start[idx] <= g;
+        const unsigned m = __ballot_sync(0xffffffffu, ok);
+        const uint32_t last = 31u - (uint32_t)__clz(m);  // starts are sorted: ok is a prefix
+        lo = lo + last * step;
+        hi = min(hi, lo + step);
     }
     return lo;
 }
 
-// f(box, element index inside the box, segment) for every element of the span.
+// f(box, element index inside the box, segment) for every element of the
+// span.  Chunks go to CTAs cyclically, so the CTAs running at any moment work
+// on neighbouring chunks (the same few boxes, whose data then stays in L2).
+// Each warp looks up the segment of its first element itself (no block
+// barrier) and its lanes walk forward from there.
 template <class F>
 __device__ __forceinline__ void for_span(const Span& sp, F f) {
-    __shared__ uint32_t sh_seg;
     const uint64_t chunk = (uint64_t)blockDim.x * kSpanItems;
-    for (uint64_t g0 = (uint64_t)blockIdx.x * chunk; g0 < sp.total; g0 += (uint64_t)gridDim.x * chunk) {
-        if (threadIdx.x == 0) sh_seg = seg_of(sp, g0);
-        __syncthreads();
-        uint32_t k = sh_seg;
-        __syncthreads();
+    const uint64_t warp0 = threadIdx.x & ~31u;
+    for (uint64_t g0 = (uint64_t)blockIdx.x * chunk; g0 < sp.total;
+         g0 += (uint64_t)gridDim.x * chunk) {
+        const uint64_t gw = g0 + warp0 < sp.total ? g0 + warp0 : g0;
+        uint32_t k = seg_of_warp(sp, gw);
         for (int it = 0; it < kSpanItems; ++it) {
             const uint64_t g = g0 + (uint64_t)it * blockDim.x + threadIdx.x;
             if (g >= sp.total) break;
@@ -264,15 +276,12 @@ __device__ __forceinline__ BorderDim border_dim_of(const BoxStep& S, int dim) {
     return bd;
 }
 
-// Tile spans: one CTA per tile; f(box, tile index, scan_end, cap).
+// Tile spans: one tile per CTA at a time, tiles cyclic over CTAs;
+// f(box, tile index).  Every warp looks the tile's segment up itself.
 template <class F>
 __device__ __forceinline__ void for_tiles(const Span& sp, F f) {
-    __shared__ uint32_t sh_seg;
     for (uint64_t g = blockIdx.x; g < sp.total; g += gridDim.x) {
-        if (threadIdx.x == 0) sh_seg = seg_of(sp, g);
-        __syncthreads();
-        const uint32_t k = sh_seg;
-        __syncthreads();
+        const uint32_t k = seg_of_warp(sp, g);
         f(sp.box[k], (uint64_t)sp.base[k] + (g - sp.start[k]));
     }
 }
@@ -285,6 +294,13 @@ __global__ void __launch_bounds__(kBlock) kb_border_count(Span sp, BatchArgs A, 
         const uint32_t* bs = A.bstate + (uint64_t)b * kBorderStateWords;
         const uint64_t cap = D.cap;
         const uint64_t scan_end = bs[dim] < cap ? bs[dim] : cap;
+        if (tile * kBorderTile >= scan_end) {  // tile past this pass's scan range (uniform)
+            if (threadIdx.x == 0) {
+                D.tile_lo[tile] = 0u;
+                D.tile_hi[tile] = 0u;
+            }
+            return;
+        }
         const BorderDim bd = border_dim_of(S, dim);
         const AtomCols& c = D.set[S.post];
         const uint64_t base = tile * kBorderTile + (uint64_t)threadIdx.x * kBorderItemsB;
@@ -352,6 +368,7 @@ __global__ void __launch_bounds__(kBlock) kb_border_scatter(Span sp, BatchArgs A
         uint32_t* bs = A.bstate + (uint64_t)b * kBorderStateWords;
         const uint64_t cap = D.cap;
         const uint64_t scan_end = bs[dim] < cap ? bs[dim] : cap;
+        if (tile * kBorderTile >= scan_end) return;  // nothing flagged past the range
         const uint64_t recv_lo = bs[dim];
         const uint64_t recv_hi = recv_lo + bs[4 + dim];
         const AtomCols& c = D.set[S.post];
@@ -483,13 +500,12 @@ __device__ __forceinline__ void add_filter_stats(DevFlags* f, uint32_t cd, uint3
 // recheck statistics are summed per box inside each warp (lanes matched by
 // box) before one atomic per box and warp.
 __global__ void __launch_bounds__(kBlock) kb_pairs_rows(Span sp, BatchArgs A) {
-    __shared__ uint32_t sh_seg;
     const uint64_t chunk = (uint64_t)blockDim.x * kSpanItems;
-    for (uint64_t g0 = (uint64_t)blockIdx.x * chunk; g0 < sp.total; g0 += (uint64_t)gridDim.x * chunk) {
-        if (threadIdx.x == 0) sh_seg = seg_of(sp, g0);
-        __syncthreads();
-        uint32_t k = sh_seg;
-        __syncthreads();
+    const uint64_t warp0 = threadIdx.x & ~31u;
+    for (uint64_t g0 = (uint64_t)blockIdx.x * chunk; g0 < sp.total;
+         g0 += (uint64_t)gridDim.x * chunk) {
+        const uint64_t gw = g0 + warp0 < sp.total ? g0 + warp0 : g0;
+        uint32_t k = seg_of_warp(sp, gw);
         uint32_t cur = 0xffffffffu, cd = 0, rk = 0;
         for (int it = 0; it < kSpanItems; ++it) {
             const uint64_t g = g0 + (uint64_t)it * blockDim.x + threadIdx.x;
