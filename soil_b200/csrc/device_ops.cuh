@@ -116,33 +116,6 @@ __device__ __forceinline__ uint32_t fold_key(uint32_t chain) {
     return key;
 }
 
-struct PairForce {
-    bool hit;
-    double fx, fy, fz;
-};
-
-__device__ __forceinline__ PairForce pair_force(const AtomCols& c, const double* rad, double K,
-                                                uint32_t i, uint32_t j) {
-    PairForce f;
-    f.hit = false;
-    const double ri = rad[i], rj = rad[j];
-    const double sum_r = ri + rj;
-    const double dx = c.x[j] - c.x[i];
-    const double dy = c.y[j] - c.y[i];
-    const double dz = c.z[j] - c.z[i];
-    const double dist_sq = dx * dx + dy * dy + dz * dz;
-    if (dist_sq >= sum_r * sum_r || dist_sq == 0.0) return f;
-    const double dist = sqrt(dist_sq);
-    const double overlap = sum_r - dist;
-    const double inv_dist = 1.0 / dist;
-    const double fmag = K * overlap;
-    f.hit = true;
-    f.fx = -fmag * dx * inv_dist;
-    f.fy = -fmag * dy * inv_dist;
-    f.fz = -fmag * dz * inv_dist;
-    return f;
-}
-
 template <bool UNIFORM, bool FP32>
 struct Filter {
     double cut_sq, sf_sq;
@@ -342,7 +315,17 @@ __device__ __forceinline__ void forward_ghost(const AtomCols& c, uint64_t nlocal
     }
 }
 
-// Force on atom a gathered in the reference's pair order (see k_force.cu).
+// Force on atom a from the built-in consumer, in the reference's summation
+// order: -f(i,a) for every earlier row i listing a (ascending i), then
+// +f(a,j) over a's own row, then -f(i,a) for later rows (ghost atoms and, with
+// newton off, non-receiving atoms skip parts).  The three parts run as ONE
+// loop over the flattened sequence (in-list entries below a, the row, the
+// rest of the in-list), so a warp pays the longest sequence of its lanes, not
+// the sum of three per-part maxima.  Each entry evaluates f(i, j) with i the
+// row atom, with the same operations in the same order, so the sums are
+// bit-identical to the sequential reference.  f(i, j) is the tutorial's
+// soft_repulsion_force (docs/src/tutorial/write-your-own-physics.md:56-110):
+// d = x_j - x_i, overlap = (r_i + r_j) - |d|, f_i = -K * overlap * d / |d|.
 __device__ __forceinline__ void harmonic_atom(const AtomCols& c, uint64_t a, uint64_t nlocal,
                                               const double* rad, double K, int newton,
                                               const uint32_t* offsets, const uint32_t* indices,
@@ -351,39 +334,44 @@ __device__ __forceinline__ void harmonic_atom(const AtomCols& c, uint64_t a, uin
     const bool local = a < nlocal;
     // reference applies -f to j only when newton || j < nlocal
     const bool receives = newton || local;
-    uint32_t q = in_start[a];
-    const uint32_t qe = in_start[a + 1];
-    if (receives) {
-        for (; q < qe; ++q) {
-            const uint32_t i = in_list[q];
-            if (i > a) break;  // later rows come after this atom's own row
-            const PairForce f = pair_force(c, rad, K, i, (uint32_t)a);
-            if (f.hit) {
-                Fx = Fx - f.fx;
-                Fy = Fy - f.fy;
-                Fz = Fz - f.fz;
-            }
-        }
-    }
-    if (local) {
-        for (uint32_t p = offsets[a]; p < offsets[a + 1]; ++p) {
-            const PairForce f = pair_force(c, rad, K, (uint32_t)a, indices[p]);
-            if (f.hit) {
-                Fx = Fx + f.fx;
-                Fy = Fy + f.fy;
-                Fz = Fz + f.fz;
-            }
-        }
-    }
-    if (receives) {
-        for (; q < qe; ++q) {
-            const uint32_t i = in_list[q];
-            const PairForce f = pair_force(c, rad, K, i, (uint32_t)a);
-            if (f.hit) {
-                Fx = Fx - f.fx;
-                Fy = Fy - f.fy;
-                Fz = Fz - f.fz;
-            }
+    const uint32_t qs = in_start[a];
+    const uint32_t nin = receives ? in_start[a + 1] - qs : 0u;
+    const uint32_t rs = local ? offsets[a] : 0u;
+    const uint32_t nrow = local ? offsets[a + 1] - rs : 0u;
+    uint32_t npre = 0;  // in-list rows below a (the list is ascending, never a itself)
+    while (npre < nin && in_list[qs + npre] < (uint32_t)a) ++npre;
+    const double xa = c.x[a], ya = c.y[a], za = c.z[a], ra = rad[a];
+    const uint32_t total = nin + nrow;
+    for (uint32_t k = 0; k < total; ++k) {
+        const bool own = k >= npre && k < npre + nrow;
+        const uint32_t o = own ? indices[rs + (k - npre)] : in_list[qs + (k < npre ? k : k - nrow)];
+        const double xo = c.x[o], yo = c.y[o], zo = c.z[o], ro = rad[o];
+        // f(i, j): own row i = a, j = o; in-list i = o, j = a
+        const double ri = own ? ra : ro, rj = own ? ro : ra;
+        const double xi = own ? xa : xo, xj = own ? xo : xa;
+        const double yi = own ? ya : yo, yj = own ? yo : ya;
+        const double zi = own ? za : zo, zj = own ? zo : za;
+        const double sum_r = ri + rj;
+        const double dx = xj - xi;
+        const double dy = yj - yi;
+        const double dz = zj - zi;
+        const double dist_sq = dx * dx + dy * dy + dz * dz;
+        if (dist_sq >= sum_r * sum_r || dist_sq == 0.0) continue;
+        const double dist = sqrt(dist_sq);
+        const double overlap = sum_r - dist;
+        const double inv_dist = 1.0 / dist;
+        const double fmag = K * overlap;
+        const double fx = -fmag * dx * inv_dist;
+        const double fy = -fmag * dy * inv_dist;
+        const double fz = -fmag * dz * inv_dist;
+        if (own) {
+            Fx = Fx + fx;
+            Fy = Fy + fy;
+            Fz = Fz + fz;
+        } else {
+            Fx = Fx - fx;
+            Fy = Fy - fy;
+            Fz = Fz - fz;
         }
     }
     c.fx[a] = Fx;
