@@ -581,12 +581,23 @@ SPAN_KERNEL(kb_in_scatter, {
 SPAN_LAUNCH(b_in_scatter, kb_in_scatter)
 
 // ---- force and reverse comm ---------------------------------------------------
-SPAN_KERNEL(kb_harmonic, {
-    const AtomCols& c = D.set[S.post];
-    harmonic_atom(c, i, S.nlocal, c.planes[D.radius_plane], S.K, S.newton, D.offsets, D.indices,
-                  D.in_start, D.in_list);
-})
-SPAN_LAUNCH(b_harmonic, kb_harmonic)
+// Register-capped like the single-system force kernel (5 blocks per SM) and
+// launched as one resident wave.
+__global__ void __launch_bounds__(kBlock, 5) kb_harmonic(Span sp, BatchArgs A) {
+    for_span(sp, [&](uint32_t b, uint64_t i, uint32_t) {
+        const BoxDev& D = A.dev[b];
+        const BoxStep& S = A.step[b];
+        const AtomCols& c = D.set[S.post];
+        harmonic_atom(c, i, S.nlocal, c.planes[D.radius_plane], S.K, S.newton, D.offsets,
+                      D.indices, D.in_start, D.in_list);
+    });
+}
+void b_harmonic(cudaStream_t st, const Span& sp, const BatchArgs& a) {
+    if (sp.total == 0) return;
+    note_launch();
+    const unsigned g = span_grid(sp);
+    kb_harmonic<<<g < 148u * 5u ? g : 148u * 5u, kBlock, 0, st>>>(sp, a);
+}
 
 SPAN_KERNEL(kb_reverse, { fold_root(D.set[S.post], S.nlocal, i, D.fold_start, D.fold_list, D.rev); })
 SPAN_LAUNCH(b_reverse, kb_reverse)

@@ -15,7 +15,7 @@
 
 namespace soil {
 
-__global__ void __launch_bounds__(kBlock) k_harmonic(uint64_t nlocal, uint64_t ntotal, AtomCols c,
+__global__ void __launch_bounds__(kBlock, 5) k_harmonic(uint64_t nlocal, uint64_t ntotal, AtomCols c,
                                                      const double* rad, double K, int newton,
                                                      const uint32_t* offsets,
                                                      const uint32_t* indices,
@@ -31,8 +31,11 @@ void launch_harmonic(cudaStream_t st, uint64_t nlocal, uint64_t ntotal, const At
                      const uint32_t* indices, const uint32_t* in_start, const uint32_t* in_list) {
     if (ntotal == 0) return;
     note_launch();
-    k_harmonic<<<grid_for(ntotal), kBlock, 0, st>>>(nlocal, ntotal, c, radius, k, newton, offsets,
-                                                    indices, in_start, in_list);
+    // one resident wave (5 blocks of 256 per SM at <= 48 registers), grid-stride
+    const unsigned full = 148u * 5u;
+    const unsigned need = (unsigned)((ntotal + kBlock - 1) / kBlock);
+    k_harmonic<<<need < full ? need : full, kBlock, 0, st>>>(nlocal, ntotal, c, radius, k, newton,
+                                                              offsets, indices, in_start, in_list);
 }
 
 }  // namespace soil
