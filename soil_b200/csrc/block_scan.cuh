@@ -35,4 +35,36 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* t
     return res;
 }
 
+// One CTA scans n values: out[t] (and out2[t] when given) = exclusive prefix
+// of in over [0, n); returns the total.  ITEMS consecutive values per thread
+// per pass, so a pass covers kBlock * ITEMS values.
+template <int ITEMS>
+__device__ __forceinline__ uint32_t cta_scan_array(const uint32_t* in, uint32_t* out,
+                                                   uint32_t* out2, uint64_t n) {
+    __shared__ uint32_t tot;
+    uint32_t carry = 0;
+    for (uint64_t b0 = 0; b0 < n; b0 += (uint64_t)kBlock * ITEMS) {
+        const uint64_t t0 = b0 + (uint64_t)threadIdx.x * ITEMS;
+        uint32_t v[ITEMS];
+        uint32_t sum = 0;
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            v[j] = t0 + j < n ? in[t0 + j] : 0u;
+            sum += v[j];
+        }
+        uint32_t run = block_exclusive_scan(sum, &tot) + carry;
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            if (t0 + j < n) {
+                out[t0 + j] = run;
+                if (out2) out2[t0 + j] = run;
+            }
+            run += v[j];
+        }
+        carry += tot;
+        __syncthreads();
+    }
+    return carry;
+}
+
 }  // namespace soil

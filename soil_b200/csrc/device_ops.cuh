@@ -159,8 +159,13 @@ struct Filter {
     }
 };
 
-// Row of local atom i, sequentially in reference order.  FILL writes the
-// indices to out[]; returns the row length.
+// Row of local atom i, sequentially in reference order: the own cell's
+// candidates (the tail after i's slot with newton, else the whole cell
+// without i), then every stencil cell in stencil order, each in sorted order.
+// The candidate ranges run as ONE loop (the lane moves to its next non-empty
+// range when one ends), so a warp pays for the longest candidate sequence of
+// its lanes rather than the per-cell maximum summed over the stencil.  FILL
+// writes the accepted indices to out[] (at most cap); returns the row length.
 template <bool UNIFORM, bool FP32, bool FILL>
 __device__ uint32_t row_scan(const PairParams& p, const Filter<UNIFORM, FP32>& test, uint64_t i,
                              uint32_t* out, uint32_t cap, uint32_t* rechk, uint32_t* cand,
@@ -170,35 +175,39 @@ __device__ uint32_t row_scan(const PairParams& p, const Filter<UNIFORM, FP32>& t
     const double4 pi = p.sp[mi];
     const float4 pif = FP32 ? p.spf[mi] : make_float4(0.f, 0.f, 0.f, 0.f);
     uint32_t cnt = 0;
+    int s = -1;  // -1: the own cell; s >= 0: stencil cell s
+    uint32_t m = 0, e = 0;
     if (p.has_self) {
-        const uint32_t e = p.bin_start[my_cell + 1];
-        const uint32_t b = p.newton ? mi + 1 : p.bin_start[my_cell];
-        for (uint32_t m = b; m < e; ++m) {
-            if (!p.newton && m == mi) continue;
+        e = p.bin_start[my_cell + 1];
+        m = p.newton ? mi + 1 : p.bin_start[my_cell];
+    }
+    for (;;) {
+        while (m >= e) {  // open the next non-empty stencil cell
+            if (++s >= p.nstencil) return cnt;
+            const int32_t off = p.stencil[s];
+            if (!p.newton && off == 0) continue;  // the own cell was the first range
+            const uint32_t cc = (uint32_t)((int32_t)my_cell + off);
+            if (cc >= p.ncells) {  // the grid's ghost layers make this unreachable
+                if (flags) atomicOr(&flags->error, 1u);
+                continue;
+            }
+            m = p.bin_start[cc];
+            e = p.bin_start[cc + 1];
+            *cand += e - m;
+        }
+        if (s < 0) {  // own cell: i itself is not a candidate
+            if (!p.newton && m == mi) {
+                ++m;
+                continue;
+            }
             ++*cand;
-            if (test(p, pi, pif, m, rechk)) {
-                if (FILL && cnt < cap) out[cnt] = p.sorted_atoms[m];
-                ++cnt;
-            }
         }
-    }
-    for (int s = 0; s < p.nstencil; ++s) {
-        const int32_t off = p.stencil[s];
-        if (!p.newton && off == 0) continue;
-        const uint32_t cc = (uint32_t)((int32_t)my_cell + off);
-        if (cc >= p.ncells) {  // the grid's ghost layers make this unreachable
-            if (flags) atomicOr(&flags->error, 1u);
-            continue;
+        if (test(p, pi, pif, m, rechk)) {
+            if (FILL && cnt < cap) out[cnt] = p.sorted_atoms[m];
+            ++cnt;
         }
-        const uint32_t e = p.bin_start[cc + 1];
-        *cand += e - p.bin_start[cc];
-        for (uint32_t m = p.bin_start[cc]; m < e; ++m)
-            if (test(p, pi, pif, m, rechk)) {
-                if (FILL && cnt < cap) out[cnt] = p.sorted_atoms[m];
-                ++cnt;
-            }
+        ++m;
     }
-    return cnt;
 }
 
 // ---- per-atom bodies of the kernels ----------------------------------------

@@ -327,29 +327,17 @@ void b_border_count(cudaStream_t st, const Span& sp, const BatchArgs& a, int dim
 }
 
 __global__ void __launch_bounds__(kBlock) kb_border_scan(Span sp, BatchArgs A, int dim) {
-    __shared__ uint32_t tot;
     for (uint32_t k = blockIdx.x; k < sp.nseg; k += gridDim.x) {
         const uint32_t b = sp.box[k];
         const BoxDev& D = A.dev[b];
         uint32_t* bs = A.bstate + (uint64_t)b * kBorderStateWords;
         const uint64_t ntiles = sp.start[k + 1] - sp.start[k];
-        uint32_t carry[2] = {0, 0};
-        for (int h = 0; h < 2; ++h) {
-            const uint32_t* in = h == 0 ? D.tile_lo : D.tile_hi;
-            uint32_t* out = h == 0 ? D.tile_off_lo : D.tile_off_hi;
-            for (uint64_t b0 = 0; b0 < ntiles; b0 += kBlock) {
-                const uint64_t t = b0 + threadIdx.x;
-                const uint32_t v = t < ntiles ? in[t] : 0u;
-                const uint32_t pre = block_exclusive_scan(v, &tot) + carry[h];
-                if (t < ntiles) out[t] = pre;
-                carry[h] += tot;
-                __syncthreads();
-            }
-        }
+        const uint32_t nlo = cta_scan_array<8>(D.tile_lo, D.tile_off_lo, nullptr, ntiles);
+        const uint32_t nhi = cta_scan_array<8>(D.tile_hi, D.tile_off_hi, nullptr, ntiles);
         if (threadIdx.x == 0) {
-            bs[4 + dim] = carry[0];
-            bs[7 + dim] = carry[1];
-            bs[dim + 1] = bs[dim] + carry[0] + carry[1];
+            bs[4 + dim] = nlo;
+            bs[7 + dim] = nhi;
+            bs[dim + 1] = bs[dim] + nlo + nhi;
         }
         __syncthreads();
     }
@@ -369,6 +357,7 @@ __global__ void __launch_bounds__(kBlock) kb_border_scatter(Span sp, BatchArgs A
         const uint64_t cap = D.cap;
         const uint64_t scan_end = bs[dim] < cap ? bs[dim] : cap;
         if (tile * kBorderTile >= scan_end) return;  // nothing flagged past the range
+        if (D.tile_lo[tile] == 0u && D.tile_hi[tile] == 0u) return;  // nothing selected
         const uint64_t recv_lo = bs[dim];
         const uint64_t recv_hi = recv_lo + bs[4 + dim];
         const AtomCols& c = D.set[S.post];

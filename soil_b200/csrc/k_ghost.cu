@@ -34,6 +34,13 @@ __global__ void __launch_bounds__(kBlock) k_border_count(uint32_t* bs, uint64_t 
                                                          uint32_t* tile_lo, uint32_t* tile_hi) {
     __shared__ uint32_t tot;
     const uint64_t scan_end = bs[bd.dim] < cap ? bs[bd.dim] : cap;  // a short pass is redone
+    if ((uint64_t)blockIdx.x * kBorderTile >= scan_end) {  // tile past the scan range (uniform)
+        if (threadIdx.x == 0) {
+            tile_lo[blockIdx.x] = 0u;
+            tile_hi[blockIdx.x] = 0u;
+        }
+        return;
+    }
     const uint64_t base = (uint64_t)blockIdx.x * kBorderTile + (uint64_t)threadIdx.x * kBorderItems;
     uint32_t nlo = 0, nhi = 0;
     for (int k = 0; k < kBorderItems; ++k) {
@@ -57,32 +64,23 @@ __global__ void __launch_bounds__(kBlock) k_border_scan(uint32_t* bs, int dim, u
                                                         const uint32_t* tile_lo,
                                                         const uint32_t* tile_hi, uint32_t* off_lo,
                                                         uint32_t* off_hi) {
-    __shared__ uint32_t tot;
-    uint32_t carry[2] = {0, 0};
-    for (int h = 0; h < 2; ++h) {
-        const uint32_t* in = h == 0 ? tile_lo : tile_hi;
-        uint32_t* out = h == 0 ? off_lo : off_hi;
-        for (uint32_t b0 = 0; b0 < ntiles; b0 += kBlock) {
-            const uint32_t t = b0 + threadIdx.x;
-            const uint32_t v = t < ntiles ? in[t] : 0u;
-            const uint32_t pre = block_exclusive_scan(v, &tot) + carry[h];
-            if (t < ntiles) out[t] = pre;
-            carry[h] += tot;
-            __syncthreads();
-        }
-    }
+    const uint32_t nlo = cta_scan_array<8>(tile_lo, off_lo, nullptr, ntiles);
+    const uint32_t nhi = cta_scan_array<8>(tile_hi, off_hi, nullptr, ntiles);
     if (threadIdx.x == 0) {
-        bs[4 + dim] = carry[0];
-        bs[7 + dim] = carry[1];
-        bs[dim + 1] = bs[dim] + carry[0] + carry[1];
+        bs[4 + dim] = nlo;
+        bs[7 + dim] = nhi;
+        bs[dim + 1] = bs[dim] + nlo + nhi;
     }
 }
 
 __global__ void __launch_bounds__(kBlock) k_border_scatter(
     uint32_t* bs, uint64_t nlocal, uint64_t cap, AtomCols c, BorderDim bd, const uint8_t* face,
+    const uint32_t* tile_cnt_lo, const uint32_t* tile_cnt_hi,
     const uint32_t* tile_off_lo, const uint32_t* tile_off_hi, uint32_t* send_lo,
     uint32_t* send_hi, uint32_t* root, uint32_t* chain) {
     __shared__ uint32_t tot;
+    // nothing selected in this tile (counts of the count pass; uniform)
+    if (tile_cnt_lo[blockIdx.x] == 0u && tile_cnt_hi[blockIdx.x] == 0u) return;
     const uint64_t scan_end = bs[bd.dim] < cap ? bs[bd.dim] : cap;
     const uint64_t recv_lo = bs[bd.dim];
     const uint64_t recv_hi = scan_end + bs[4 + bd.dim];
@@ -135,9 +133,9 @@ void launch_border_dim(cudaStream_t st, uint32_t* bs, uint64_t nlocal, uint64_t 
     k_border_scan<<<1, kBlock, 0, st>>>(bs, bd.dim, max_tiles, tile_lo, tile_hi, tile_off_lo,
                                         tile_off_hi);
     note_launch();
-    k_border_scatter<<<max_tiles, kBlock, 0, st>>>(bs, nlocal, cap, c, bd, face_flags, tile_off_lo,
-                                                   tile_off_hi, send_lo, send_hi, ghost_root,
-                                                   ghost_chain);
+    k_border_scatter<<<max_tiles, kBlock, 0, st>>>(bs, nlocal, cap, c, bd, face_flags, tile_lo,
+                                                   tile_hi, tile_off_lo, tile_off_hi, send_lo,
+                                                   send_hi, ghost_root, ghost_chain);
 }
 
 __global__ void __launch_bounds__(kBlock) k_forward(uint64_t nlocal, uint64_t nghost, AtomCols c,
