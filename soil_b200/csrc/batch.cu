@@ -361,13 +361,9 @@ void fill_dev(soil_batch* b, uint32_t k) {
     d.ghost_chain = s->ghost_chain.p;
     for (int q = 0; q < kNumSwaps; ++q) d.send[q] = s->send[q].p;
     d.face_flags = s->face_flags.p;
-    d.tile_lo = s->tile_lo.p;
-    d.tile_hi = s->tile_hi.p;
-    d.tile_off_lo = s->tile_off_lo.p;
-    d.tile_off_hi = s->tile_off_hi.p;
-    d.fold_count = s->fold_count.p;
+    d.bcount = s->bcount.p;
+    d.boff = s->boff.p;
     d.fold_start = s->fold_start.p;
-    d.fold_cursor = s->fold_cursor.p;
     d.fold_list = s->fold_list.p;
     d.cap = s->acap;
     zero_planes_of(s, SOIL_COL_FORWARD, d.fwd.idx, &d.fwd.n);
@@ -550,21 +546,14 @@ int grow_slots(soil_batch* b, uint32_t need) {
 }
 
 // ---- one step -------------------------------------------------------------------
-uint64_t tiles_of(uint64_t n) { return (n + kBorderTile - 1) / kBorderTile; }
-
-// Border passes of the boxes in R (three dims, count / scan / scatter each).
-// retry: an earlier pass of this step ran; rows of boxes outside R then hold
-// finished results, which the upload of R's initial rows must keep.
 int launch_borders(soil_batch* b, const std::vector<uint32_t>& R, Stage& g, bool retry) {
     TRY(stage_begin(b, g));
     TRY(put_tables(b, g));
     if (retry) std::memcpy(b->binit.data(), b->h_bread, (size_t)b->cap * kBorderStateWords * 4);
-    // initial border state of every box in R
+    // border state rows of the boxes in R start at zero
     uint32_t lo = b->cap, hi = 0;
     for (uint32_t k : R) {
-        uint32_t* w = b->binit.data() + (size_t)k * kBorderStateWords;
-        std::memset(w, 0, kBorderStateWords * 4);
-        w[0] = (uint32_t)b->slot[k]->nlocal;
+        std::memset(b->binit.data() + (size_t)k * kBorderStateWords, 0, kBorderStateWords * 4);
         lo = std::min(lo, k);
         hi = std::max(hi, k + 1);
     }
@@ -572,24 +561,14 @@ int launch_borders(soil_batch* b, const std::vector<uint32_t>& R, Stage& g, bool
         TRY(stage_put(b, g, b->d_bstate + (size_t)lo * kBorderStateWords,
                       b->binit.data() + (size_t)lo * kBorderStateWords,
                       (size_t)(hi - lo) * kBorderStateWords * 4));
-    int sd[3];
-    for (int dim = 0; dim < 3; ++dim) {
-        sd[dim] = stage_add(g);
-        for (uint32_t k : R) {
-            const soil_sys* s = b->slot[k];
-            // dim 0 scans the locals; later dims scan up to the capacity bound
-            const uint64_t n = dim == 0 ? s->nlocal : s->acap;
-            g.spans[sd[dim]].add(k, tiles_of(n), 0);
-        }
-    }
+    const int wt = stage_add(g);
+    for (uint32_t k : R) g.spans[wt].add(k, (b->slot[k]->nlocal + 31) / 32, 0);
     TRY(stage_commit(b, g));
     const BatchArgs a = args_of(b);
     tic(b);
-    for (int dim = 0; dim < 3; ++dim) {
-        b_border_count(b->st, g.out[sd[dim]], a, dim);
-        b_border_scan(b->st, g.out[sd[dim]], a, dim);
-        b_border_scatter(b->st, g.out[sd[dim]], a, dim);
-    }
+    b_border_faces(b->st, g.out[wt], a);
+    b_border_cat_scan(b->st, g.out[wt], a);
+    b_border_images(b->st, g.out[wt], a);
     toc(b, BT_BORDERS);
     TRY(check_kernels(b));
     BCK(cudaMemcpyAsync(b->h_bread, b->d_bstate, (size_t)b->cap * kBorderStateWords * 4,
@@ -807,9 +786,9 @@ int batch_step(soil_batch* b, bool last) {
     Stage& g4 = b->stage[G_NEIGHBOR];
     TRY(stage_begin(b, g4));
     TRY(put_tables(b, g4));
-    const int f_loc = stage_add(g4), f_gh = stage_add(g4), f_scan = stage_add(g4),
-              s_fwd = stage_add(g4), n_cells = stage_add(g4), n_copy = stage_add(g4),
-              n_bin = stage_add(g4), n_all = stage_add(g4), n_rows = stage_add(g4);
+    const int f_loc = stage_add(g4), s_fwd = stage_add(g4), n_cells = stage_add(g4),
+              n_copy = stage_add(g4), n_bin = stage_add(g4), n_all = stage_add(g4),
+              n_rows = stage_add(g4);
     for (uint32_t k : M) {
         soil_sys* s = b->slot[k];
         if (!b->rebuild[k]) {
@@ -818,8 +797,6 @@ int batch_step(soil_batch* b, bool last) {
         }
         const uint64_t nl = s->nlocal, ng = s->nghost;
         g4.spans[f_loc].add_nz(k, nl, 0);
-        g4.spans[f_gh].add_nz(k, ng, 0);
-        g4.spans[f_scan].add(k, nl, 0);
         g4.spans[n_cells].add(k, s->total_cells, 0);
         if (s->local_cells_valid) {
             g4.spans[n_copy].add_nz(k, nl, 0);
@@ -833,11 +810,6 @@ int batch_step(soil_batch* b, bool last) {
     }
     TRY(stage_commit(b, g4));
     tic(b);
-    b_zero_counts(st, g4.out[f_scan], a, BA_FOLD);
-    b_fold_count(st, g4.out[f_gh], a);
-    b_scan(st, g4.out[f_scan], a, BA_FOLD);
-    b_fold_scatter(st, g4.out[f_gh], a);
-    b_fold_order(st, g4.out[f_loc], a);
     b_forward(st, g4.out[s_fwd], a);
     if (!R.empty()) {
         b_save_positions(st, g4.out[f_loc], a);

@@ -52,13 +52,9 @@ struct BoxDev {
     uint32_t* ghost_chain;
     uint32_t* send[kNumSwaps];
     uint8_t* face_flags;
-    uint32_t* tile_lo;
-    uint32_t* tile_hi;
-    uint32_t* tile_off_lo;
-    uint32_t* tile_off_hi;
-    uint32_t* fold_count;
+    uint32_t* bcount;      // per-warp chain-category counts of borders
+    uint32_t* boff;        // their offsets
     uint32_t* fold_start;
-    uint32_t* fold_cursor;
     uint32_t* fold_list;
     uint64_t cap;  // atom capacity of both column sets
     PlaneList fwd, rev, zero;
@@ -117,8 +113,7 @@ enum BatchArray {
     BA_CELLS = 0,     // cell_counts -> cell_start (+ cursor), segsort of sort_perm
     BA_NEIGH_CELLS,   // cell_counts -> cell_start (+ cursor), segsort of sorted_atoms
     BA_ROWS,          // rowcount -> offsets (total into totals[box])
-    BA_IN,            // in_count -> in_start (+ cursor), segsort of in_list
-    BA_FOLD           // fold_count -> fold_start (+ cursor)
+    BA_IN             // in_count -> in_start (+ cursor), segsort of in_list
 };
 
 // ---- launchers (k_batch.cu); every one enqueues a single kernel ------------
@@ -140,13 +135,11 @@ void b_segsort(cudaStream_t st, const Span& sp, const BatchArgs& a, int which);
 void b_permute_cells(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_identity(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_perm_gather(cudaStream_t st, const Span& sp, const BatchArgs& a);
-// borders of one dim: element = tile of kBorderTile atoms; scan: CTA per box
-void b_border_count(cudaStream_t st, const Span& sp, const BatchArgs& a, int dim);
-void b_border_scan(cudaStream_t st, const Span& sp, const BatchArgs& a, int dim);
-void b_border_scatter(cudaStream_t st, const Span& sp, const BatchArgs& a, int dim);
-void b_fold_count(cudaStream_t st, const Span& sp, const BatchArgs& a);
-void b_fold_scatter(cudaStream_t st, const Span& sp, const BatchArgs& a);
-void b_fold_order(cudaStream_t st, const Span& sp, const BatchArgs& a);
+// borders + fold program (chain categories, see k_ghost.cu): element = warp
+// tile of 32 locals of a box; the scan runs one CTA per (box, category)
+void b_border_faces(cudaStream_t st, const Span& sp, const BatchArgs& a);
+void b_border_cat_scan(cudaStream_t st, const Span& sp, const BatchArgs& a);
+void b_border_images(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_forward(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_save_positions(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_sorted_views(cudaStream_t st, const Span& sp, const BatchArgs& a);

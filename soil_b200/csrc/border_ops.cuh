@@ -1,0 +1,139 @@
+// border_ops.cuh — warp-tile routines of the borders pass (chain categories,
+// see k_ghost.cu), shared by the single-system and the batched kernels.
+//
+// A warp tile is 32 consecutive locals, one per lane.  Pass 1 stores the face
+// bits and, per category, the tile's member count (counts[k * nw + w]; row
+// kBorderCats holds all images of the tile).  After a per-category scan
+// (offs, same layout), pass 2 ranks each member inside its tile with a ballot
+// and writes its image, its send entry, its ghost root/chain and its root's
+// fold program.  Every routine is called by all 32 lanes of a warp.
+#pragma once
+
+#include "block_scan.cuh"
+#include "device_ops.cuh"
+
+namespace soil {
+
+__device__ __forceinline__ bool cat_member(const BorderCats& cats, uint32_t bits, int k) {
+    return (bits & cats.need[k]) == cats.need[k];
+}
+
+__device__ __forceinline__ uint32_t warp_exclusive_sum(uint32_t v, uint32_t lane) {
+    uint32_t incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += t;
+    }
+    return incl - v;
+}
+
+// Pass 1 for warp tile w: local r = 32 w + lane.
+__device__ __forceinline__ void border_warp_counts(const AtomCols& c, uint64_t nlocal,
+                                                   const Geom& geom, int triclinic,
+                                                   const double* lo, const double* hi,
+                                                   const BorderCats& cats, uint8_t* face,
+                                                   uint32_t* counts, uint64_t nw, uint64_t w,
+                                                   uint32_t lane) {
+    const uint64_t r = w * 32 + lane;
+    uint32_t bits = 0;
+    if (r < nlocal) {
+        bits = face_bits(c, geom, triclinic, lo, hi, r);
+        face[r] = (uint8_t)bits;
+    }
+    uint32_t mine = 0, images = 0;
+    if (__ballot_sync(0xffffffffu, bits != 0u)) {
+        for (int k = 0; k < kBorderCats; ++k) {
+            const uint32_t n = __popc(__ballot_sync(0xffffffffu, cat_member(cats, bits, k)));
+            if (lane == (uint32_t)k) mine = n;
+            images += n;
+        }
+    }
+    if (lane < kBorderCats) counts[lane * nw + w] = mine;
+    if (lane == kBorderCats) counts[kBorderCats * nw + w] = images;
+}
+
+// Per-dim border state in the format the host reads (bs[0..9]) from the
+// category totals bs[kBorderTotals + k].
+__device__ __forceinline__ void border_state_words(const BorderCats& cats, uint64_t nlocal,
+                                                   uint32_t* bs) {
+    bs[0] = (uint32_t)nlocal;
+    for (int d = 0; d < 3; ++d) {
+        uint32_t n[2] = {0, 0};
+        for (int side = 0; side < 2; ++side) {
+            const int s = 2 * d + side;
+            for (int q = 0; q < cats.swap_ncat[s]; ++q)
+                n[side] += bs[kBorderTotals + cats.swap_first[s] + q];
+        }
+        bs[4 + d] = n[0];
+        bs[7 + d] = n[1];
+        bs[d + 1] = bs[d] + n[0] + n[1];
+    }
+}
+
+// Warp tiles per scan chunk: the category scans run one CTA per (category,
+// chunk); chunk prefixes (cpre[k * nchunks + chunk]) are added back here.
+constexpr uint64_t kScanChunk = 8192;
+
+// Pass 2 for warp tile w.  base_lane: on lane k < 26 the first ghost index of
+// category k (nlocal + the totals of the categories before it).  offs holds
+// offsets inside the tile's scan chunk; cpre (NULL: a single chunk) the
+// chunks' prefixes.
+__device__ __forceinline__ void border_warp_images(
+    const AtomCols& c, uint64_t nlocal, uint64_t cap, const double (*shift)[3],
+    const double (*vshift)[3], const BorderCats& cats, const uint8_t* face, const uint32_t* offs,
+    const uint32_t* cpre, uint64_t nchunks, uint64_t nw, uint64_t w, uint32_t lane,
+    uint32_t base_lane, uint32_t* bs, uint32_t* root, uint32_t* chain, uint32_t* const* send,
+    uint32_t* fold_start, uint32_t* fold_list) {
+    const unsigned below = (1u << lane) - 1u;
+    const uint64_t r = w * 32 + lane;
+    const uint32_t bits = r < nlocal ? face[r] : 0u;
+    const uint64_t cw = w / kScanChunk;
+    // lane k <= 26: offset of this tile's members of category k (k = 26: images)
+    const uint32_t off_lane =
+        lane <= (uint32_t)kBorderCats
+            ? offs[lane * nw + w] + (cpre ? cpre[lane * nchunks + cw] : 0u)
+            : 0u;
+    const uint32_t fold0 = __shfl_sync(0xffffffffu, off_lane, kBorderCats);
+    if (!__ballot_sync(0xffffffffu, bits != 0u)) {  // no images: empty fold programs
+        if (r < nlocal) fold_start[r] = fold0;
+        if (r + 1 == nlocal) fold_start[nlocal] = fold0;
+        return;
+    }
+    uint32_t recv[kNumSwaps];
+    for (int s = 0; s < kNumSwaps; ++s)
+        recv[s] = __shfl_sync(0xffffffffu, base_lane, cats.swap_first[s]);
+    uint32_t idx[kBorderCats];
+    uint32_t own = 0;  // images of this lane's root
+    for (int k = 0; k < kBorderCats; ++k) {
+        const bool m = cat_member(cats, bits, k);
+        const unsigned bal = __ballot_sync(0xffffffffu, m);
+        const uint32_t base = __shfl_sync(0xffffffffu, base_lane + off_lane, k);
+        idx[k] = base + __popc(bal & below);
+        own += m;
+    }
+    const uint32_t fs = fold0 + warp_exclusive_sum(own, lane);
+    if (r < nlocal) fold_start[r] = fs;
+    if (r + 1 == nlocal) fold_start[nlocal] = fs + own;
+    if (!bits) return;
+    for (int k = 0; k < kBorderCats; ++k) {
+        if (!cat_member(cats, bits, k)) continue;
+        const uint32_t g = idx[k];
+        if (g >= cap) {
+            bs[10] = 1u;  // out of capacity: the host grows the arrays and repeats
+            continue;
+        }
+        const uint32_t parent = cats.parent[k] < 0 ? (uint32_t)r : idx[cats.parent[k]];
+        write_image(c, shift, vshift, cats, k, g, r, parent, nlocal, root, chain);
+        const int s = cats.swap_of[k];
+        send[s][g - recv[s]] = parent;
+    }
+    uint32_t j = fs;
+    for (int f = 0; f < kBorderCats; ++f) {
+        const int k = cats.fold[f];
+        if (!cat_member(cats, bits, k)) continue;
+        if (idx[k] < cap && j < cap) fold_list[j] = idx[k] - (uint32_t)nlocal;
+        ++j;
+    }
+}
+
+}  // namespace soil

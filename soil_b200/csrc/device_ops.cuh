@@ -61,59 +61,71 @@ __device__ __forceinline__ void border_flags(const AtomCols& c, const BorderDim&
     hi = v >= bd.thresh_hi;
 }
 
-// Ghost g := image of atom i through swap `s` (pack_border + unpack_atom,
-// atom.rs:520-553; registry pack_all/unpack_all for every column).
-__device__ __forceinline__ void write_ghost(const AtomCols& c, uint64_t g, uint64_t i,
-                                            const double* shift, const double* vshift, int s,
-                                            uint64_t nlocal, uint32_t* root, uint32_t* chain) {
-    const uint64_t cap = c.cap;
-    c.x[g] = c.x[i] + shift[0];
-    c.y[g] = c.y[i] + shift[1];
-    c.z[g] = c.z[i] + shift[2];
-    c.vx[g] = c.vx[i] + vshift[0];
-    c.vy[g] = c.vy[i] + vshift[1];
-    c.vz[g] = c.vz[i] + vshift[2];
-    c.fx[g] = c.fx[i];
-    c.fy[g] = c.fy[i];
-    c.fz[g] = c.fz[i];
-    const double m = c.mass[i];
-    c.mass[g] = m;
-    c.inv_mass[g] = 1.0 / m;
-    c.cut[g] = c.cut[i];
-    c.tag[g] = c.tag[i];
-    c.type[g] = c.type[i];
-    c.img[g] = c.img[i];
-    c.img[cap + g] = c.img[cap + i];
-    c.img[2 * cap + g] = c.img[2 * cap + i];
-    c.origin[g] = (int32_t)i;
-    for (int q = 0; q < c.nplanes; ++q) c.planes[q][g] = c.planes[q][i];
-    // chain: swap ids in 3-bit fields (application order), length in bits 12-13
-    uint32_t r, code;
-    if (i < nlocal) {
-        r = (uint32_t)i;
-        code = (1u << 12) | (uint32_t)s;
-    } else {
-        r = root[i - nlocal];
-        const uint32_t pc = chain[i - nlocal];
-        const uint32_t len = pc >> 12;
-        code = (pc & 0xfffu) | ((uint32_t)s << (3 * len)) | ((len + 1) << 12);
+// Face bits of local r for a borders pass: bit 2d = inside the lo slab of
+// dim d, bit 2d+1 = inside the hi slab (comm.rs:305-327; lamda coordinates
+// when triclinic).
+__device__ __forceinline__ uint32_t face_bits(const AtomCols& c, const Geom& geom, int triclinic,
+                                              const double* lo, const double* hi, uint64_t r) {
+    double v0 = c.x[r], v1 = c.y[r], v2 = c.z[r];
+    if (triclinic) {
+        double l0, l1, l2;
+        x2lamda(geom, v0, v1, v2, l0, l1, l2);
+        v0 = l0;
+        v1 = l1;
+        v2 = l2;
     }
-    root[g - nlocal] = r;
-    chain[g - nlocal] = code;
+    uint32_t b = 0;
+    b |= (v0 < lo[0] ? 1u : 0u) | (v0 >= hi[0] ? 2u : 0u);
+    b |= (v1 < lo[1] ? 4u : 0u) | (v1 >= hi[1] ? 8u : 0u);
+    b |= (v2 < lo[2] ? 16u : 0u) | (v2 >= hi[2] ? 32u : 0u);
+    return b;
 }
 
-__device__ __forceinline__ uint32_t fold_key(uint32_t chain) {
-    const uint32_t len = chain >> 12;
-    uint32_t key = 0;
-    for (uint32_t k = 0; k < 3; ++k) {
-        uint32_t pr = 7;
-        if (k < len) {
-            const uint32_t sw = (chain >> (3 * k)) & 7u;
-            pr = (2u - sw / 2u) * 2u + (sw & 1u);  // swaps 4,5,2,3,0,1 -> 0..5
-        }
-        key = key * 8u + pr;
+// Ghost g = image of root r through the swaps of chain category k
+// (pack_border + unpack_atom, atom.rs:520-553, applied swap by swap: the
+// shifts are added in chain order exactly as the reference's ghost of a
+// ghost does); its source (origin) is `parent`.
+__device__ __forceinline__ void write_image(const AtomCols& c, const double (*shift)[3],
+                                            const double (*vshift)[3], const BorderCats& cats,
+                                            int k, uint64_t g, uint64_t r, uint32_t parent,
+                                            uint64_t nlocal, uint32_t* root, uint32_t* chain) {
+    const uint64_t cap = c.cap;
+    double x = c.x[r], y = c.y[r], z = c.z[r];
+    double vx = c.vx[r], vy = c.vy[r], vz = c.vz[r];
+    uint32_t code = 0;
+    for (int t = 0; t < cats.len[k]; ++t) {
+        const int s = cats.sw[k][t];
+        x = x + shift[s][0];
+        y = y + shift[s][1];
+        z = z + shift[s][2];
+        vx = vx + vshift[s][0];
+        vy = vy + vshift[s][1];
+        vz = vz + vshift[s][2];
+        code |= (uint32_t)s << (3 * t);
     }
-    return key;
+    code |= (uint32_t)cats.len[k] << 12;
+    c.x[g] = x;
+    c.y[g] = y;
+    c.z[g] = z;
+    c.vx[g] = vx;
+    c.vy[g] = vy;
+    c.vz[g] = vz;
+    c.fx[g] = c.fx[r];
+    c.fy[g] = c.fy[r];
+    c.fz[g] = c.fz[r];
+    const double m = c.mass[r];
+    c.mass[g] = m;
+    c.inv_mass[g] = 1.0 / m;
+    c.cut[g] = c.cut[r];
+    c.tag[g] = c.tag[r];
+    c.type[g] = c.type[r];
+    c.img[g] = c.img[r];
+    c.img[cap + g] = c.img[cap + r];
+    c.img[2 * cap + g] = c.img[2 * cap + r];
+    c.origin[g] = (int32_t)parent;
+    for (int q = 0; q < c.nplanes; ++q) c.planes[q][g] = c.planes[q][r];
+    root[g - nlocal] = (uint32_t)r;
+    chain[g - nlocal] = code;
 }
 
 template <bool UNIFORM, bool FP32>

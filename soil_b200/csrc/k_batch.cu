@@ -10,6 +10,7 @@
 // Every element calls the same device function as the single-system kernels.
 #include "batch.cuh"
 #include "block_scan.cuh"
+#include "border_ops.cuh"
 #include "sys_internal.cuh"
 
 namespace soil {
@@ -118,7 +119,6 @@ SPAN_LAUNCH(b_pbc, kb_pbc)
 // ---- bins -----------------------------------------------------------------
 __device__ __forceinline__ uint32_t* counts_of(const BoxDev& D, int which) {
     if (which == BA_IN) return D.in_count;
-    if (which == BA_FOLD) return D.fold_count;
     return D.cell_counts;
 }
 
@@ -172,7 +172,6 @@ __global__ void __launch_bounds__(kBlock) kb_scan(Span sp, BatchArgs A, int whic
     uint32_t *out, *cursor;
     if (which == BA_ROWS) { in = D.rowcount; out = D.offsets; cursor = nullptr; }
     else if (which == BA_IN) { in = D.in_count; out = D.in_start; cursor = D.in_cursor; }
-    else if (which == BA_FOLD) { in = D.fold_count; out = D.fold_start; cursor = D.fold_cursor; }
     else { in = D.cell_counts; out = D.cell_start; cursor = D.cell_cursor; }
     uint32_t carry = 0;
     for (uint64_t b0 = 0; b0 < n; b0 += (uint64_t)kBlock * kScanItems) {
@@ -263,169 +262,70 @@ SPAN_LAUNCH(b_identity, kb_identity)
 SPAN_KERNEL(kb_perm_gather, { perm_gather_atom(D.set[S.cur], D.set[S.post], i, D.sort_perm[i]); })
 SPAN_LAUNCH(b_perm_gather, kb_perm_gather)
 
-// ---- borders ----------------------------------------------------------------
-constexpr int kBorderItemsB = kBorderTile / kBlock;
-
-__device__ __forceinline__ BorderDim border_dim_of(const BoxStep& S, int dim) {
-    BorderDim bd;
-    bd.dim = dim;
-    bd.triclinic = S.geom.triclinic;
-    bd.geom = S.geom;
-    bd.thresh_lo = S.thresh_lo[dim];
-    bd.thresh_hi = S.thresh_hi[dim];
-    return bd;
-}
-
-// Tile spans: one tile per CTA at a time, tiles cyclic over CTAs;
-// f(box, tile index).  Every warp looks the tile's segment up itself.
+// ---- borders (chain categories; the single-system kernels are in k_ghost.cu) ---
+// Warp-tile spans: every warp takes one tile of 32 locals of one box;
+// f(box, warp tile index inside the box, segment).
 template <class F>
-__device__ __forceinline__ void for_tiles(const Span& sp, F f) {
-    for (uint64_t g = blockIdx.x; g < sp.total; g += gridDim.x) {
+__device__ __forceinline__ void for_warp_tiles(const Span& sp, F f) {
+    const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x / 32);
+    for (uint64_t g = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32; g < sp.total;
+         g += nwarps) {
         const uint32_t k = seg_of_warp(sp, g);
-        f(sp.box[k], (uint64_t)sp.base[k] + (g - sp.start[k]));
+        f(sp.box[k], (uint64_t)sp.base[k] + (g - sp.start[k]), k);
     }
 }
 
-__global__ void __launch_bounds__(kBlock) kb_border_count(Span sp, BatchArgs A, int dim) {
-    __shared__ uint32_t tot;
-    for_tiles(sp, [&](uint32_t b, uint64_t tile) {
+__global__ void __launch_bounds__(kBlock) kb_border_faces(Span sp, BatchArgs A, BorderCats cats) {
+    const uint32_t lane = threadIdx.x & 31u;
+    for_warp_tiles(sp, [&](uint32_t b, uint64_t w, uint32_t k) {
         const BoxDev& D = A.dev[b];
         const BoxStep& S = A.step[b];
-        const uint32_t* bs = A.bstate + (uint64_t)b * kBorderStateWords;
-        const uint64_t cap = D.cap;
-        const uint64_t scan_end = bs[dim] < cap ? bs[dim] : cap;
-        if (tile * kBorderTile >= scan_end) {  // tile past this pass's scan range (uniform)
-            if (threadIdx.x == 0) {
-                D.tile_lo[tile] = 0u;
-                D.tile_hi[tile] = 0u;
-            }
-            return;
-        }
-        const BorderDim bd = border_dim_of(S, dim);
-        const AtomCols& c = D.set[S.post];
-        const uint64_t base = tile * kBorderTile + (uint64_t)threadIdx.x * kBorderItemsB;
-        uint32_t nlo = 0, nhi = 0;
-        for (int q = 0; q < kBorderItemsB; ++q) {
-            const uint64_t i = base + q;
-            if (i >= scan_end) break;
-            bool lo, hi;
-            border_flags(c, bd, i, lo, hi);
-            D.face_flags[i] = (uint8_t)((lo ? 1 : 0) | (hi ? 2 : 0));
-            nlo += lo;
-            nhi += hi;
-        }
-        block_exclusive_scan(nlo, &tot);
-        if (threadIdx.x == 0) D.tile_lo[tile] = tot;
-        block_exclusive_scan(nhi, &tot);
-        if (threadIdx.x == 0) D.tile_hi[tile] = tot;
+        const uint64_t nw = sp.start[k + 1] - sp.start[k];
+        border_warp_counts(D.set[S.post], S.nlocal, S.geom, S.geom.triclinic, S.thresh_lo,
+                           S.thresh_hi, cats, D.face_flags, D.bcount, nw, w, lane);
     });
 }
-void b_border_count(cudaStream_t st, const Span& sp, const BatchArgs& a, int dim) {
+void b_border_faces(cudaStream_t st, const Span& sp, const BatchArgs& a) {
     if (sp.total == 0) return;
     note_launch();
-    kb_border_count<<<grid_for(sp.total * kBlock), kBlock, 0, st>>>(sp, a, dim);
+    kb_border_faces<<<grid_for(sp.total * 32), kBlock, 0, st>>>(sp, a, border_cats());
 }
 
-__global__ void __launch_bounds__(kBlock) kb_border_scan(Span sp, BatchArgs A, int dim) {
-    for (uint32_t k = blockIdx.x; k < sp.nseg; k += gridDim.x) {
-        const uint32_t b = sp.box[k];
-        const BoxDev& D = A.dev[b];
-        uint32_t* bs = A.bstate + (uint64_t)b * kBorderStateWords;
-        const uint64_t ntiles = sp.start[k + 1] - sp.start[k];
-        const uint32_t nlo = cta_scan_array<8>(D.tile_lo, D.tile_off_lo, nullptr, ntiles);
-        const uint32_t nhi = cta_scan_array<8>(D.tile_hi, D.tile_off_hi, nullptr, ntiles);
-        if (threadIdx.x == 0) {
-            bs[4 + dim] = nlo;
-            bs[7 + dim] = nhi;
-            bs[dim + 1] = bs[dim] + nlo + nhi;
-        }
-        __syncthreads();
-    }
+// one CTA per (box, category): exclusive scan of the warp counts
+__global__ void __launch_bounds__(kBlock) kb_border_cat_scan(Span sp, BatchArgs A) {
+    const uint32_t seg = blockIdx.x / (kBorderCats + 1), k = blockIdx.x % (kBorderCats + 1);
+    const uint32_t b = sp.box[seg];
+    const BoxDev& D = A.dev[b];
+    const uint64_t nw = sp.start[seg + 1] - sp.start[seg];
+    const uint32_t total = cta_scan_array<8>(D.bcount + k * nw, D.boff + k * nw, nullptr, nw);
+    if (threadIdx.x == 0) A.bstate[(uint64_t)b * kBorderStateWords + kBorderTotals + k] = total;
 }
-void b_border_scan(cudaStream_t st, const Span& sp, const BatchArgs& a, int dim) {
+void b_border_cat_scan(cudaStream_t st, const Span& sp, const BatchArgs& a) {
     if (sp.nseg == 0) return;
     note_launch();
-    kb_border_scan<<<sp.nseg < 148u * 8u ? sp.nseg : 148u * 8u, kBlock, 0, st>>>(sp, a, dim);
+    kb_border_cat_scan<<<sp.nseg * (kBorderCats + 1), kBlock, 0, st>>>(sp, a);
 }
 
-__global__ void __launch_bounds__(kBlock) kb_border_scatter(Span sp, BatchArgs A, int dim) {
-    __shared__ uint32_t tot;
-    for_tiles(sp, [&](uint32_t b, uint64_t tile) {
+__global__ void __launch_bounds__(kBlock) kb_border_images(Span sp, BatchArgs A, BorderCats cats) {
+    const uint32_t lane = threadIdx.x & 31u;
+    for_warp_tiles(sp, [&](uint32_t b, uint64_t w, uint32_t k) {
         const BoxDev& D = A.dev[b];
         const BoxStep& S = A.step[b];
         uint32_t* bs = A.bstate + (uint64_t)b * kBorderStateWords;
-        const uint64_t cap = D.cap;
-        const uint64_t scan_end = bs[dim] < cap ? bs[dim] : cap;
-        if (tile * kBorderTile >= scan_end) return;  // nothing flagged past the range
-        if (D.tile_lo[tile] == 0u && D.tile_hi[tile] == 0u) return;  // nothing selected
-        const uint64_t recv_lo = bs[dim];
-        const uint64_t recv_hi = recv_lo + bs[4 + dim];
-        const AtomCols& c = D.set[S.post];
-        const uint64_t base = tile * kBorderTile + (uint64_t)threadIdx.x * kBorderItemsB;
-        uint32_t flo = 0, fhi = 0;
-        for (int q = 0; q < kBorderItemsB; ++q) {
-            const uint64_t i = base + q;
-            if (i >= scan_end) break;
-            const uint32_t f = D.face_flags[i];
-            flo |= (f & 1u) << q;
-            fhi |= ((f >> 1) & 1u) << q;
-        }
-        uint32_t rlo = block_exclusive_scan(__popc(flo), &tot) + D.tile_off_lo[tile];
-        uint32_t rhi = block_exclusive_scan(__popc(fhi), &tot) + D.tile_off_hi[tile];
-        const int s_lo = 2 * dim, s_hi = 2 * dim + 1;
-        for (int q = 0; q < kBorderItemsB; ++q) {
-            const uint64_t i = base + q;
-            if ((flo >> q) & 1u) {
-                if (recv_lo + rlo < cap) {
-                    write_ghost(c, recv_lo + rlo, i, S.sc.off[s_lo], S.sc.voff[s_lo], s_lo, S.nlocal,
-                                D.ghost_root, D.ghost_chain);
-                    D.send[s_lo][rlo] = (uint32_t)i;
-                } else {
-                    bs[10] = 1u;
-                }
-                ++rlo;
-            }
-            if ((fhi >> q) & 1u) {
-                if (recv_hi + rhi < cap) {
-                    write_ghost(c, recv_hi + rhi, i, S.sc.off[s_hi], S.sc.voff[s_hi], s_hi, S.nlocal,
-                                D.ghost_root, D.ghost_chain);
-                    D.send[s_hi][rhi] = (uint32_t)i;
-                } else {
-                    bs[10] = 1u;
-                }
-                ++rhi;
-            }
-        }
+        const uint64_t nw = sp.start[k + 1] - sp.start[k];
+        if (w == 0 && lane == 0) border_state_words(cats, S.nlocal, bs);
+        const uint32_t tot = lane < kBorderCats ? bs[kBorderTotals + lane] : 0u;
+        const uint32_t base_lane = (uint32_t)S.nlocal + warp_exclusive_sum(tot, lane);
+        border_warp_images(D.set[S.post], S.nlocal, D.cap, S.sc.off, S.sc.voff, cats, D.face_flags,
+                           D.boff, nullptr, 1, nw, w, lane, base_lane, bs, D.ghost_root,
+                           D.ghost_chain, D.send, D.fold_start, D.fold_list);
     });
 }
-void b_border_scatter(cudaStream_t st, const Span& sp, const BatchArgs& a, int dim) {
+void b_border_images(cudaStream_t st, const Span& sp, const BatchArgs& a) {
     if (sp.total == 0) return;
     note_launch();
-    kb_border_scatter<<<grid_for(sp.total * kBlock), kBlock, 0, st>>>(sp, a, dim);
+    kb_border_images<<<grid_for(sp.total * 32), kBlock, 0, st>>>(sp, a, border_cats());
 }
-
-SPAN_KERNEL(kb_fold_count, { atomicAdd(&D.fold_count[D.ghost_root[i]], 1u); })
-SPAN_LAUNCH(b_fold_count, kb_fold_count)
-
-SPAN_KERNEL(kb_fold_scatter, {
-    D.fold_list[atomicAdd(&D.fold_cursor[D.ghost_root[i]], 1u)] = (uint32_t)i;
-})
-SPAN_LAUNCH(b_fold_scatter, kb_fold_scatter)
-
-SPAN_KERNEL(kb_fold_order, {
-    const uint32_t s0 = D.fold_start[i], e = D.fold_start[i + 1];
-    for (uint32_t q = s0 + 1; q < e; ++q) {
-        const uint32_t v = D.fold_list[q];
-        const uint32_t kv = fold_key(D.ghost_chain[v]);
-        uint32_t j = q;
-        while (j > s0 && fold_key(D.ghost_chain[D.fold_list[j - 1]]) > kv) {
-            D.fold_list[j] = D.fold_list[j - 1];
-            --j;
-        }
-        D.fold_list[j] = v;
-    }
-})
-SPAN_LAUNCH(b_fold_order, kb_fold_order)
 
 SPAN_KERNEL(kb_forward, {
     forward_ghost(D.set[S.post], S.nlocal, i, D.ghost_root, D.ghost_chain, S.sc, D.fwd, false);

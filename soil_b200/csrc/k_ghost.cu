@@ -2,12 +2,10 @@
 //
 // borders (comm.rs:682-860): for dim in x,y,z the lo swap (shift +L) then
 // the hi swap (shift -L) scan the locals plus the ghosts of earlier dims in
-// index order and append every atom inside the face slab.  The device version
-// is an order-preserving stream compaction: per 512-atom tile count the lo
-// and hi selections (storing each atom's face flags), scan the tile counts,
-// then each tile ranks its flags with a CTA scan and writes the ghosts at
-// their final slots — so ghost order, send lists and recv ranges equal the
-// reference's.
+// index order and append every atom inside the face slab.  On the device the
+// whole pass is an order-preserving compaction over the locals alone (see
+// "borders as chain categories" below), so ghost order, send lists and recv
+// ranges equal the reference's.
 //
 // forward_comm (comm.rs:400-432): the reference packs pos+offset from the
 // source (a local or an earlier ghost) swap by swap.  Every ghost therefore
@@ -18,124 +16,180 @@
 // reverse_send_force (comm.rs:938-1024): swaps are folded last to first,
 // lo before hi, F[send[k]] += F[recv_start+k].  Per local atom that is a
 // post-order walk of its image tree, done by one thread (see below).
-#include "block_scan.cuh"
-#include "device_ops.cuh"
+#include <algorithm>
+#include <vector>
+
+#include "border_ops.cuh"
 #include "kernels.cuh"
 
 namespace soil {
 
-constexpr int kBorderItems = kBorderTile / kBlock;
-
-// Border state shared by the kernels of one borders pass (device memory):
-//   bs[0..3]   scan_end of dim d (bs[0] = nlocal; bs[d+1] = bs[d] + lo_d + hi_d)
-//   bs[4..6]   lo totals, bs[7..9] hi totals, bs[10] overflow flag
-__global__ void __launch_bounds__(kBlock) k_border_count(uint32_t* bs, uint64_t cap, AtomCols c,
-                                                         BorderDim bd, uint8_t* face,
-                                                         uint32_t* tile_lo, uint32_t* tile_hi) {
-    __shared__ uint32_t tot;
-    const uint64_t scan_end = bs[bd.dim] < cap ? bs[bd.dim] : cap;  // a short pass is redone
-    if ((uint64_t)blockIdx.x * kBorderTile >= scan_end) {  // tile past the scan range (uniform)
-        if (threadIdx.x == 0) {
-            tile_lo[blockIdx.x] = 0u;
-            tile_hi[blockIdx.x] = 0u;
-        }
-        return;
-    }
-    const uint64_t base = (uint64_t)blockIdx.x * kBorderTile + (uint64_t)threadIdx.x * kBorderItems;
-    uint32_t nlo = 0, nhi = 0;
-    for (int k = 0; k < kBorderItems; ++k) {
-        const uint64_t i = base + k;
-        if (i >= scan_end) break;
-        bool lo, hi;
-        border_flags(c, bd, i, lo, hi);
-        face[i] = (uint8_t)((lo ? 1 : 0) | (hi ? 2 : 0));
-        nlo += lo;
-        nhi += hi;
-    }
-    block_exclusive_scan(nlo, &tot);
-    if (threadIdx.x == 0) tile_lo[blockIdx.x] = tot;
-    block_exclusive_scan(nhi, &tot);
-    if (threadIdx.x == 0) tile_hi[blockIdx.x] = tot;
-}
-
-// One CTA: exclusive scans of the lo and hi tile counts, the dim's totals and
-// the next dim's scan_end.
-__global__ void __launch_bounds__(kBlock) k_border_scan(uint32_t* bs, int dim, uint32_t ntiles,
-                                                        const uint32_t* tile_lo,
-                                                        const uint32_t* tile_hi, uint32_t* off_lo,
-                                                        uint32_t* off_hi) {
-    const uint32_t nlo = cta_scan_array<8>(tile_lo, off_lo, nullptr, ntiles);
-    const uint32_t nhi = cta_scan_array<8>(tile_hi, off_hi, nullptr, ntiles);
-    if (threadIdx.x == 0) {
-        bs[4 + dim] = nlo;
-        bs[7 + dim] = nhi;
-        bs[dim + 1] = bs[dim] + nlo + nhi;
-    }
-}
-
-__global__ void __launch_bounds__(kBlock) k_border_scatter(
-    uint32_t* bs, uint64_t nlocal, uint64_t cap, AtomCols c, BorderDim bd, const uint8_t* face,
-    const uint32_t* tile_cnt_lo, const uint32_t* tile_cnt_hi,
-    const uint32_t* tile_off_lo, const uint32_t* tile_off_hi, uint32_t* send_lo,
-    uint32_t* send_hi, uint32_t* root, uint32_t* chain) {
-    __shared__ uint32_t tot;
-    // nothing selected in this tile (counts of the count pass; uniform)
-    if (tile_cnt_lo[blockIdx.x] == 0u && tile_cnt_hi[blockIdx.x] == 0u) return;
-    const uint64_t scan_end = bs[bd.dim] < cap ? bs[bd.dim] : cap;
-    const uint64_t recv_lo = bs[bd.dim];
-    const uint64_t recv_hi = scan_end + bs[4 + bd.dim];
-    const uint64_t base = (uint64_t)blockIdx.x * kBorderTile + (uint64_t)threadIdx.x * kBorderItems;
-    uint32_t flo = 0, fhi = 0;  // bit k: item k selected
-    for (int k = 0; k < kBorderItems; ++k) {
-        const uint64_t i = base + k;
-        if (i >= scan_end) break;
-        const uint32_t f = face[i];
-        flo |= (f & 1u) << k;
-        fhi |= ((f >> 1) & 1u) << k;
-    }
-    uint32_t rlo = block_exclusive_scan(__popc(flo), &tot) + tile_off_lo[blockIdx.x];
-    uint32_t rhi = block_exclusive_scan(__popc(fhi), &tot) + tile_off_hi[blockIdx.x];
-    for (int k = 0; k < kBorderItems; ++k) {
-        const uint64_t i = base + k;
-        if ((flo >> k) & 1u) {
-            if (recv_lo + rlo < cap) {
-                write_ghost(c, recv_lo + rlo, i, bd.shift[0], bd.vshift[0], bd.swap_id[0], nlocal,
-                            root, chain);
-                send_lo[rlo] = (uint32_t)i;
-            } else {
-                bs[10] = 1u;  // out of capacity: the host grows the arrays and repeats borders
+// ---- borders as chain categories ---------------------------------------------
+// A ghost made in dim d is tested again only in later dims, with coordinates
+// its shift left unchanged (x shifts move x only, y shifts x and y, never z),
+// so its face bits are its root local's.  Every ghost is therefore a root
+// local plus a chain of swaps (at most one per dim, dims ascending), and the
+// reference's ghost list is 26 chain categories in creation order — dim x:
+// [x-] [x+]; dim y: for each side, [y] after every earlier chain
+// (none, x-, x+); dim z likewise over the nine chains before it — each
+// holding its roots in local index order.  A ghost's source (origin) is the
+// same root's image one chain shorter; the reverse-comm fold of a root visits
+// its images in a fixed category order (build_border_cats' key: per level
+// the swap priority 4,5,2,3,0,1 -> 0..5, 7 past the chain's end).
+namespace {
+BorderCats build_border_cats() {
+    BorderCats t{};
+    struct Chain {
+        int n;
+        int sw[3];
+    };
+    std::vector<Chain> scan{{0, {0, 0, 0}}};  // chains scanned by the current dim
+    std::vector<Chain> cats;
+    for (int d = 0; d < 3; ++d) {
+        std::vector<Chain> made;
+        for (int side = 0; side < 2; ++side) {
+            t.swap_first[2 * d + side] = (uint8_t)cats.size();
+            for (const Chain& c : scan) {
+                Chain n = c;
+                n.sw[n.n++] = 2 * d + side;
+                cats.push_back(n);
+                made.push_back(n);
             }
-            ++rlo;
+            t.swap_ncat[2 * d + side] = (uint8_t)scan.size();
         }
-        if ((fhi >> k) & 1u) {
-            if (recv_hi + rhi < cap) {
-                write_ghost(c, recv_hi + rhi, i, bd.shift[1], bd.vshift[1], bd.swap_id[1], nlocal,
-                            root, chain);
-                send_hi[rhi] = (uint32_t)i;
-            } else {
-                bs[10] = 1u;
+        scan.insert(scan.end(), made.begin(), made.end());
+    }
+    auto key = [](const Chain& c) {
+        uint32_t k = 0;
+        for (int l = 0; l < 3; ++l) {
+            const uint32_t pr = l < c.n ? (2u - (uint32_t)c.sw[l] / 2u) * 2u + ((uint32_t)c.sw[l] & 1u) : 7u;
+            k = k * 8u + pr;
+        }
+        return k;
+    };
+    std::vector<int> order;
+    for (int k = 0; k < kBorderCats; ++k) {
+        const Chain& c = cats[k];
+        t.len[k] = (uint8_t)c.n;
+        uint8_t need = 0;
+        for (int l = 0; l < c.n; ++l) {
+            t.sw[k][l] = (uint8_t)c.sw[l];
+            need |= (uint8_t)(1u << c.sw[l]);
+        }
+        t.need[k] = need;
+        t.swap_of[k] = (uint8_t)c.sw[c.n - 1];
+        t.parent[k] = -1;
+        for (int q = 0; q < kBorderCats && c.n > 1; ++q)
+            if (cats[q].n == c.n - 1 &&
+                std::equal(cats[q].sw, cats[q].sw + cats[q].n, c.sw))
+                t.parent[k] = (int8_t)q;
+        order.push_back(k);
+    }
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return key(cats[a]) < key(cats[b]); });
+    for (int k = 0; k < kBorderCats; ++k) t.fold[k] = (uint8_t)order[k];
+    return t;
+}
+}  // namespace
+
+const BorderCats& border_cats() {
+    static const BorderCats t = build_border_cats();
+    return t;
+}
+
+BorderPass border_pass(const BorderDim bds[3]) {
+    BorderPass bp;
+    bp.geom = bds[0].geom;
+    bp.triclinic = bds[0].triclinic;
+    for (int d = 0; d < 3; ++d) {
+        bp.lo[d] = bds[d].thresh_lo;
+        bp.hi[d] = bds[d].thresh_hi;
+        for (int side = 0; side < 2; ++side)
+            for (int q = 0; q < 3; ++q) {
+                bp.shift[2 * d + side][q] = bds[d].shift[side][q];
+                bp.vshift[2 * d + side][q] = bds[d].vshift[side][q];
             }
-            ++rhi;
+    }
+    return bp;
+}
+
+// Pass 1, one warp per 32 locals: face bits, and per category the number of
+// member roots of the warp (counts[k * nw + w]); counts[26 * nw + w] = all
+// images of the warp's roots.
+__global__ void __launch_bounds__(kBlock) k_border_faces(uint64_t nlocal, AtomCols c, BorderPass bp,
+                                                         BorderCats cats, uint8_t* face,
+                                                         uint32_t* counts, uint64_t nw) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x / 32);
+    for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32; w < nw; w += nwarps)
+        border_warp_counts(c, nlocal, bp.geom, bp.triclinic, bp.lo, bp.hi, cats, face, counts, nw,
+                           w, lane);
+}
+
+// Pass 2: one CTA per (category or all images, chunk of kScanChunk warp
+// tiles) scans the warp counts inside its chunk; ctot gets the chunk totals.
+__global__ void __launch_bounds__(kBlock) k_border_cat_scan(const uint32_t* counts, uint32_t* offs,
+                                                            uint64_t nw, uint32_t* ctot,
+                                                            uint64_t nchunks) {
+    const uint64_t k = blockIdx.x / nchunks, ch = blockIdx.x % nchunks;
+    const uint64_t w0 = ch * kScanChunk;
+    const uint64_t n = nw - w0 < kScanChunk ? nw - w0 : kScanChunk;
+    const uint32_t total = cta_scan_array<8>(counts + k * nw + w0, offs + k * nw + w0, nullptr, n);
+    if (threadIdx.x == 0) ctot[k * nchunks + ch] = total;
+}
+
+// Chunk totals -> exclusive chunk prefixes (in place) and category totals.
+__global__ void __launch_bounds__(kBlock) k_border_chunk_prefix(uint32_t* ctot, uint64_t nchunks,
+                                                                uint32_t* bs) {
+    for (uint32_t k = threadIdx.x; k <= (uint32_t)kBorderCats; k += blockDim.x) {
+        uint32_t acc = 0;
+        for (uint64_t ch = 0; ch < nchunks; ++ch) {
+            const uint32_t v = ctot[k * nchunks + ch];
+            ctot[k * nchunks + ch] = acc;
+            acc += v;
         }
+        bs[kBorderTotals + k] = acc;
     }
 }
 
-// One dim of borders: count, scan, scatter (no host synchronisation).
-void launch_border_dim(cudaStream_t st, uint32_t* bs, uint64_t nlocal, uint64_t cap,
-                       const AtomCols& c, const BorderDim& bd, uint32_t max_tiles,
-                       uint8_t* face_flags, uint32_t* tile_lo, uint32_t* tile_hi,
-                       uint32_t* tile_off_lo, uint32_t* tile_off_hi, uint32_t* send_lo,
-                       uint32_t* send_hi, uint32_t* ghost_root, uint32_t* ghost_chain) {
-    if (max_tiles == 0) return;
+// Pass 3, one warp per 32 locals: every image of the warp's roots at its
+// final index, the swap send lists, ghost root/chain, and each root's fold
+// program (its images in fold order).
+__global__ void __launch_bounds__(kBlock) k_border_images(
+    uint64_t nlocal, uint64_t cap, AtomCols c, BorderPass bp, BorderCats cats, const uint8_t* face,
+    const uint32_t* offs, const uint32_t* cpre, uint64_t nchunks, uint64_t nw, uint32_t* bs,
+    uint32_t* root, uint32_t* chain, SendPtrs send, uint32_t* fold_start, uint32_t* fold_list) {
+    const uint32_t lane = threadIdx.x & 31u;
+    if (blockIdx.x == 0 && threadIdx.x == 0) border_state_words(cats, nlocal, bs);
+    // first ghost index of category `lane` (lanes below 26)
+    const uint32_t tot = lane < kBorderCats ? bs[kBorderTotals + lane] : 0u;
+    const uint32_t base_lane = (uint32_t)nlocal + warp_exclusive_sum(tot, lane);
+    const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x / 32);
+    for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32; w < nw; w += nwarps)
+        border_warp_images(c, nlocal, cap, bp.shift, bp.vshift, cats, face, offs, cpre, nchunks,
+                           nw, w, lane, base_lane, bs, root, chain, send.p, fold_start, fold_list);
+}
+
+void launch_borders(cudaStream_t st, uint64_t nlocal, uint64_t cap, const AtomCols& c,
+                    const BorderPass& bp, uint8_t* face, uint32_t* counts, uint32_t* offs,
+                    uint32_t* bs, uint32_t* ghost_root, uint32_t* ghost_chain,
+                    const SendPtrs& send, uint32_t* fold_start, uint32_t* fold_list) {
+    if (nlocal == 0) return;
+    const BorderCats& cats = border_cats();
+    const uint64_t nw = (nlocal + 31) / 32;
+    const uint64_t nchunks = (nw + kScanChunk - 1) / kScanChunk;
+    uint32_t* ctot = counts + (kBorderCats + 1) * nw;  // chunk totals, then prefixes
+    const unsigned blocks = grid_for(nw * 32);
     note_launch();
-    k_border_count<<<max_tiles, kBlock, 0, st>>>(bs, cap, c, bd, face_flags, tile_lo, tile_hi);
+    k_border_faces<<<blocks, kBlock, 0, st>>>(nlocal, c, bp, cats, face, counts, nw);
     note_launch();
-    k_border_scan<<<1, kBlock, 0, st>>>(bs, bd.dim, max_tiles, tile_lo, tile_hi, tile_off_lo,
-                                        tile_off_hi);
+    k_border_cat_scan<<<(unsigned)((kBorderCats + 1) * nchunks), kBlock, 0, st>>>(counts, offs, nw,
+                                                                                ctot, nchunks);
     note_launch();
-    k_border_scatter<<<max_tiles, kBlock, 0, st>>>(bs, nlocal, cap, c, bd, face_flags, tile_lo,
-                                                   tile_hi, tile_off_lo, tile_off_hi, send_lo,
-                                                   send_hi, ghost_root, ghost_chain);
+    k_border_chunk_prefix<<<1, kBlock, 0, st>>>(ctot, nchunks, bs);
+    note_launch();
+    k_border_images<<<blocks, kBlock, 0, st>>>(nlocal, cap, c, bp, cats, face, offs, ctot, nchunks,
+                                               nw, bs, ghost_root, ghost_chain, send, fold_start,
+                                               fold_list);
 }
 
 __global__ void __launch_bounds__(kBlock) k_forward(uint64_t nlocal, uint64_t nghost, AtomCols c,
@@ -163,60 +217,9 @@ void launch_forward(cudaStream_t st, uint64_t nlocal, uint64_t nghost, const Ato
 // hi: target X receives, in order, its children through swaps 4, 5, 2, 3, 0, 1,
 // each child already holding its own children's folds.  That is a post-order
 // walk of each local atom's image tree with children ordered by that swap
-// priority, so sorting a root's ghosts by a key built from their swap chains
-// (priority per level, 7 past the end) and applying F[origin[g]] += F[g] in
-// key order reproduces every addition of the reference, intermediate ghosts
-// included.
-__global__ void __launch_bounds__(kBlock) k_fold_count(uint64_t nghost, const uint32_t* root,
-                                                       uint32_t* counts) {
-    for (uint64_t gi = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gi < nghost;
-         gi += (uint64_t)gridDim.x * blockDim.x)
-        atomicAdd(&counts[root[gi]], 1u);
-}
-
-__global__ void __launch_bounds__(kBlock) k_fold_scatter(uint64_t nghost, const uint32_t* root,
-                                                         uint32_t* cursor, uint32_t* list) {
-    for (uint64_t gi = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gi < nghost;
-         gi += (uint64_t)gridDim.x * blockDim.x)
-        list[atomicAdd(&cursor[root[gi]], 1u)] = (uint32_t)gi;
-}
-
-// per root: ghosts in post-order (key), ties impossible (one ghost per chain)
-__global__ void __launch_bounds__(kBlock) k_fold_order(uint64_t nlocal, const uint32_t* start,
-                                                       uint32_t* list, const uint32_t* chain) {
-    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nlocal;
-         t += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t b = start[t], e = start[t + 1];
-        for (uint32_t k = b + 1; k < e; ++k) {
-            const uint32_t v = list[k];
-            const uint32_t kv = fold_key(chain[v]);
-            uint32_t j = k;
-            while (j > b && fold_key(chain[list[j - 1]]) > kv) {
-                list[j] = list[j - 1];
-                --j;
-            }
-            list[j] = v;
-        }
-    }
-}
-
-void launch_fold_build(cudaStream_t st, uint64_t nlocal, uint64_t nghost,
-                       const uint32_t* ghost_root, const uint32_t* ghost_chain, uint32_t* counts,
-                       uint32_t* start, uint32_t* cursor, uint32_t* list, uint32_t* scan_tmp) {
-    cudaMemsetAsync(counts, 0, nlocal * sizeof(uint32_t), st);
-    if (nghost) {
-        note_launch();
-        k_fold_count<<<grid_for(nghost), kBlock, 0, st>>>(nghost, ghost_root, counts);
-    }
-    exclusive_scan_u32(st, counts, start, nlocal, scan_tmp);
-    if (nghost == 0) return;
-    cudaMemcpyAsync(cursor, start, nlocal * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
-    note_launch();
-    k_fold_scatter<<<grid_for(nghost), kBlock, 0, st>>>(nghost, ghost_root, cursor, list);
-    note_launch();
-    k_fold_order<<<grid_for(nlocal), kBlock, 0, st>>>(nlocal, start, list, ghost_chain);
-}
-
+// priority; the borders pass writes each root's images in that order (its
+// fold program), and applying F[origin[g]] += F[g] along it reproduces every
+// addition of the reference, intermediate ghosts included.
 __global__ void __launch_bounds__(kBlock) k_reverse_fold(uint64_t nlocal, const uint32_t* start,
                                                          const uint32_t* list, AtomCols c,
                                                          PlaneList rev) {

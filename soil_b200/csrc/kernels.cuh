@@ -96,24 +96,55 @@ struct BorderDim {
     double vshift[2][3];
     int swap_id[2];
 };
-constexpr int kBorderTile = 512;
-// One dim of borders on the device: the dim's scan range and recv offsets are
-// read from bs (see k_ghost.cu); ghosts beyond `cap` set bs[10].
-void launch_border_dim(cudaStream_t st, uint32_t* bs, uint64_t nlocal, uint64_t cap,
-                       const AtomCols& c, const BorderDim& bd, uint32_t max_tiles,
-                       uint8_t* face_flags, uint32_t* tile_lo, uint32_t* tile_hi,
-                       uint32_t* tile_off_lo, uint32_t* tile_off_hi, uint32_t* send_lo,
-                       uint32_t* send_hi, uint32_t* ghost_root, uint32_t* ghost_chain);
-constexpr int kBorderStateWords = 16;
+// Border state words of one borders pass (device memory, read back once):
+//   [0..3] scan_end of dim d, [4..6] lo-swap totals, [7..9] hi-swap totals,
+//   [10] overflow flag, [16 + k] image count of chain category k (k < 26),
+//   [42] all images.
+constexpr int kBorderStateWords = 48;
+constexpr int kBorderCats = 26;
+constexpr int kBorderTotals = 16;
+
+// Geometry of one borders pass: face thresholds per dim, image shifts per
+// swap id (2*dim + side, side 0 = the lo swap).
+struct BorderPass {
+    Geom geom;
+    int triclinic;
+    double lo[3], hi[3];
+    double shift[kNumSwaps][3];
+    double vshift[kNumSwaps][3];
+};
+// Chain categories of ghost images, in the order borders creates them
+// (border_cats in k_ghost.cu): the face bits a root needs for category k,
+// its swap chain, the parent category (-1: the root), the categories in
+// reverse-fold order and the contiguous category range of every swap.
+struct BorderCats {
+    uint8_t need[kBorderCats];
+    uint8_t len[kBorderCats];
+    uint8_t sw[kBorderCats][3];
+    int8_t parent[kBorderCats];
+    uint8_t swap_of[kBorderCats];
+    uint8_t fold[kBorderCats];
+    uint8_t swap_first[kNumSwaps];
+    uint8_t swap_ncat[kNumSwaps];
+};
+const BorderCats& border_cats();
+BorderPass border_pass(const BorderDim bds[3]);
+struct SendPtrs {
+    uint32_t* p[kNumSwaps];
+};
+// borders + the reverse-comm fold program in three launches: face bits and
+// per-warp category counts of the locals, a scan per category, then every
+// image written from its root.  bs must be zero; ghosts beyond `cap` set
+// bs[10].  offs holds (kBorderCats + 1) * nw words and counts that plus
+// (kBorderCats + 1) * ceil(nw / 8192) (nw = ceil(nlocal / 32)).
+void launch_borders(cudaStream_t st, uint64_t nlocal, uint64_t cap, const AtomCols& c,
+                    const BorderPass& bp, uint8_t* face, uint32_t* counts, uint32_t* offs,
+                    uint32_t* bs, uint32_t* ghost_root, uint32_t* ghost_chain,
+                    const SendPtrs& send, uint32_t* fold_start, uint32_t* fold_list);
 // forward_comm: every ghost from its root local atom through its swap chain
 void launch_forward(cudaStream_t st, uint64_t nlocal, uint64_t nghost, const AtomCols& c,
                     const uint32_t* ghost_root, const uint32_t* ghost_chain, const SwapConst& sc,
                     const int* fwd_planes, int nfwd, bool zero_force);
-// Fold program of reverse comm, built after borders: ghosts grouped by root
-// local atom (start[nlocal+1], list[nghost]) in post-order of the swap tree.
-void launch_fold_build(cudaStream_t st, uint64_t nlocal, uint64_t nghost,
-                       const uint32_t* ghost_root, const uint32_t* ghost_chain, uint32_t* counts,
-                       uint32_t* start, uint32_t* cursor, uint32_t* list, uint32_t* scan_tmp);
 // reverse_send_force: F[origin[g]] += F[g] (+ #[reverse] planes) over every
 // root's image tree in fold order
 void launch_reverse_fold(cudaStream_t st, uint64_t nlocal, const uint32_t* start,

@@ -572,18 +572,15 @@ int phase_borders(soil_sys* s) {
     border_setup(s, bds);
     TRY(borders_reserve(s));
     uint32_t* hb = s->hword;
+    const BorderPass bp = border_pass(bds);
     for (int attempt = 0; attempt < 4; ++attempt) {
-        const uint64_t cap = s->acap;
-        const uint32_t max_tiles = (uint32_t)((cap + kBorderTile - 1) / kBorderTile);
         TRY(borders_arrays(s));
-        uint32_t init[kBorderStateWords] = {};
-        init[0] = (uint32_t)s->nlocal;
-        CK(cudaMemcpyAsync(s->bstate.p, init, sizeof init, cudaMemcpyHostToDevice, s->st));
-        for (int dim = 0; dim < 3; ++dim)
-            launch_border_dim(s->st, s->bstate.p, s->nlocal, cap, s->A, bds[dim], max_tiles,
-                              s->face_flags.p, s->tile_lo.p, s->tile_hi.p, s->tile_off_lo.p,
-                              s->tile_off_hi.p, s->send[2 * dim].p, s->send[2 * dim + 1].p,
-                              s->ghost_root.p, s->ghost_chain.p);
+        SendPtrs send;
+        for (int k = 0; k < kNumSwaps; ++k) send.p[k] = s->send[k].p;
+        CK(cudaMemsetAsync(s->bstate.p, 0, kBorderStateWords * 4, s->st));
+        launch_borders(s->st, s->nlocal, s->acap, s->A, bp, s->face_flags.p, s->bcount.p,
+                       s->boff.p, s->bstate.p, s->ghost_root.p, s->ghost_chain.p, send,
+                       s->fold_start.p, s->fold_list.p);
         TRY(check_launch(s));
         CK(cudaMemcpyAsync(hb, s->bstate.p, kBorderStateWords * 4, cudaMemcpyDeviceToHost, s->st));
         TRY(sync(s));
@@ -591,11 +588,7 @@ int phase_borders(soil_sys* s) {
         if (attempt == 3) return fail(s->ctx, SOIL_ERR_CAPACITY, "ghost capacity did not converge");
         TRY(grow_atoms(s, (uint64_t)hb[3] + 1024, s->nlocal));  // hb[3]: atoms incl. all ghosts
     }
-    TRY(borders_done(s, hb, bds));
-    launch_fold_build(s->st, s->nlocal, s->nghost, s->ghost_root.p, s->ghost_chain.p,
-                      s->fold_count.p, s->fold_start.p, s->fold_cursor.p, s->fold_list.p,
-                      s->scan_tmp.p);
-    return check_launch(s);
+    return borders_done(s, hb, bds);
 }
 
 // Face thresholds and image shifts of the three border dims (comm.rs:288-358,
@@ -636,16 +629,18 @@ int borders_reserve(soil_sys* s) {
     return borders_arrays(s);
 }
 
+// Arrays of a borders pass at the current capacity: the fold program is
+// written by the same pass, so it is sized for a full capacity of ghosts.
 int borders_arrays(soil_sys* s) {
     const uint64_t cap = s->acap;
-    const uint32_t max_tiles = (uint32_t)((cap + kBorderTile - 1) / kBorderTile);
+    const uint64_t nw = (s->nlocal + 31) / 32;
     TRY(ensure(s, s->bstate, kBorderStateWords));
-    TRY(ensure(s, s->tile_lo, max_tiles + 2));
-    TRY(ensure(s, s->tile_hi, max_tiles + 2));
-    TRY(ensure(s, s->tile_off_lo, max_tiles + 2));
-    TRY(ensure(s, s->tile_off_hi, max_tiles + 2));
+    TRY(ensure(s, s->bcount, (kBorderCats + 1) * (nw + nw / 8192 + 1) + 1));
+    TRY(ensure(s, s->boff, (kBorderCats + 1) * nw + 1));
     for (int k = 0; k < kNumSwaps; ++k) TRY(ensure(s, s->send[k], cap + 1));
     TRY(ensure(s, s->face_flags, cap + 1));
+    TRY(ensure(s, s->fold_start, s->nlocal + 2));
+    TRY(ensure(s, s->fold_list, cap + 1));
     return SOIL_OK;
 }
 
@@ -667,12 +662,6 @@ int borders_done(soil_sys* s, const uint32_t* hb, const BorderDim bds[3]) {
     s->nghost = (uint64_t)hb[3] - s->nlocal;
     s->last_nghost = s->nghost;
     s->nswaps = kNumSwaps;
-    const uint64_t nl = s->nlocal;
-    TRY(ensure(s, s->fold_count, nl + 1));
-    TRY(ensure(s, s->fold_start, nl + 2));
-    TRY(ensure(s, s->fold_cursor, nl + 1));
-    TRY(ensure(s, s->fold_list, s->nghost + 1));
-    TRY(ensure(s, s->scan_tmp, scan_temp_words(nl + 2)));
     return SOIL_OK;
 }
 
@@ -1068,7 +1057,7 @@ int soil_sys_create(soil_ctx* ctx, const soil_box* box, const soil_neigh_cfg* cf
     int r;
     if ((r = dev_alloc(s, (void**)&s->dflags, sizeof(DevFlags))) != SOIL_OK ||
         cudaMallocHost((void**)&s->hflags, sizeof(DevFlags)) != cudaSuccess ||
-        cudaMallocHost((void**)&s->hword, 64) != cudaSuccess) {
+        cudaMallocHost((void**)&s->hword, kBorderStateWords * 4) != cudaSuccess) {
         cudaGetLastError();
         soil_sys_destroy(s);
         return r != SOIL_OK ? r : fail(ctx, SOIL_ERR_OOM, "pinned allocation failed");
@@ -1096,9 +1085,10 @@ int soil_sys_destroy(soil_sys* s) {
     fr(s->row_slots); fr(s->sp); fr(s->spf);
     fr(s->in_count); fr(s->in_start); fr(s->in_cursor); fr(s->in_list);
     fr(s->ghost_root); fr(s->ghost_chain);
-    fr(s->fold_count); fr(s->fold_start); fr(s->fold_cursor); fr(s->fold_list);
+    fr(s->fold_start); fr(s->fold_list);
     for (auto& a : s->send) fr(a);
-    fr(s->tile_lo); fr(s->tile_hi); fr(s->tile_off_lo); fr(s->tile_off_hi); fr(s->bstate);
+    fr(s->bstate);
+    fr(s->bcount); fr(s->boff);
     fr(s->face_flags);
     fr(s->scan_tmp); fr(s->d_stencil); fr(s->stage); fr(s->d_colptrs);
     resolve_timers(s);

@@ -111,9 +111,10 @@ struct soil_sys {
     DArr<float4> spf;
     DArr<uint32_t> in_count, in_start, in_cursor, in_list;
     DArr<uint32_t> ghost_root, ghost_chain;
-    DArr<uint32_t> fold_count, fold_start, fold_cursor, fold_list;  // reverse-comm fold program
+    DArr<uint32_t> fold_start, fold_list;  // reverse-comm fold program (written by borders)
     DArr<uint32_t> send[kNumSwaps];
-    DArr<uint32_t> tile_lo, tile_hi, tile_off_lo, tile_off_hi, bstate;
+    DArr<uint32_t> bstate;
+    DArr<uint32_t> bcount, boff;  // per-warp chain-category counts / offsets of borders
     DArr<uint8_t> face_flags;
     uint64_t last_nghost = 0;
     DArr<uint32_t> scan_tmp;
