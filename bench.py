@@ -37,7 +37,7 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-from soil_b200 import abi, workloads  # noqa: E402
+from soil_b200 import abi, dist, workloads  # noqa: E402
 
 # Algorithmic bytes per unit of each timed phase (FP64 SoA; one read or
 # write of each value the phase must touch).
@@ -163,33 +163,19 @@ def make_workload(name, filt, natoms=None):
 
 
 def dist_init():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    return world, rank, local
+    return dist.init()
 
 
 def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return dist.max_over_ranks(x, world)
+
+
+def sum_over_ranks(x, world):
+    return dist.sum_over_ranks(x, world)
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    dist.barrier(world)
 
 
 def cpu_baseline(w, budget_s=20.0, max_steps=10000):
@@ -340,15 +326,7 @@ C4_DESC = ("C4 batched: 4,096 independent periodic boxes, N log-uniform [256, 65
 
 
 def lpt_partition(sizes, world):
-    """Greedy longest-processing-time assignment of boxes to ranks."""
-    order = sorted(range(len(sizes)), key=lambda i: -sizes[i])
-    load = [0] * world
-    parts = [[] for _ in range(world)]
-    for i in order:
-        r = min(range(world), key=lambda q: load[q])
-        parts[r].append(i)
-        load[r] += sizes[i]
-    return [sorted(p) for p in parts]
+    return dist.lpt_partition(sizes, world)
 
 
 def batched_cpu_baseline(ws, budget_s=15.0):
@@ -607,16 +585,6 @@ def run_served(args, world, rank, local):
     return 0
 
 
-def sum_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
-
-
 def run_e2e(ctx, w, steps, world):
     """Same metric through the C ABI from pinned host buffers: upload the
     initial state, set up, run `steps`, read back positions and velocities."""
@@ -697,9 +665,7 @@ def main():
             return run_served(args, world, rank, local)
         return run_soil(args, world, rank, local)
     finally:
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+        dist.finalize(world)
 
 
 if __name__ == "__main__":
