@@ -401,6 +401,8 @@ def run_batched(args, world, rank, local):
     batch.set_timing(True)
     rb0 = sum(s.counts().rebuilds for s in boxes)
     st0 = batch.stats()
+    al0 = ctx.alloc_count()
+    load0 = os.getloadavg()
     launches0 = lib.soil_kernel_launches()
     sampler = ClockSampler(local)
     sampler.start()
@@ -421,6 +423,8 @@ def run_batched(args, world, rank, local):
     launches = lib.soil_kernel_launches() - launches0
     tim = batch.get_timing()
     st1 = batch.stats()
+    al1 = ctx.alloc_count()
+    load1 = os.getloadavg()
     cs = [s.counts() for s in boxes]
     rebuilds = sum(c.rebuilds for c in cs) - rb0
     ms_max = max_over_ranks(ms, world)
@@ -464,6 +468,9 @@ def run_batched(args, world, rank, local):
             "host_waits_per_step": (st1["host_waits"] - st0["host_waits"]) / args.steps,
             "stage_ms_per_step": stages,
             "host_ms_per_step": host,
+            "host_threads": os.environ.get("SOIL_HOST_THREADS", "default"),
+            "host_loadavg_1min": [round(load0[0], 2), round(load1[0], 2)],
+            "device_allocs_in_timed_region": al1[0] - al0[0],
             "roofline": roofline,
             "cpu_baseline": cb,
             "e2e": None,
@@ -618,7 +625,11 @@ def run_e2e(ctx, w, steps, world):
     if w.shear_rate:
         s.set_shear(w.shear_rate)
     s.setup()
+    s.sync()
+    t_setup = time.perf_counter()
     s.step(steps)
+    s.sync()
+    t_steps = time.perf_counter()
     s.read_local_state(out_pos[1], out_vel[1])
     t1 = time.perf_counter()
     barrier(world)
@@ -628,7 +639,9 @@ def run_e2e(ctx, w, steps, world):
     return {"value": world * w.n * steps / dt, "unit": "atom-steps/s",
             "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps,
             "seconds": dt, "what": "host arrays -> soil_sys_add_atoms/setup -> soil_step(K) "
-                                   "-> soil_sys_get_atoms(pos, vel)"}
+                                   "-> soil_sys_get_atoms(pos, vel)",
+            "breakdown_s": {"create_upload_setup": t_setup - t0, "steps": t_steps - t_setup,
+                            "readback": t1 - t_steps}}
 
 
 def main():

@@ -152,6 +152,9 @@ int soil_ctx_destroy(soil_ctx* ctx);
 const char* soil_last_error(const soil_ctx* ctx);
 /* Device bytes currently held by all systems of the context. */
 int soil_ctx_bytes_in_use(const soil_ctx* ctx, uint64_t* out);
+/* Device allocations and frees the context has made so far (no reference
+ * counterpart: lets a host check that steady-state steps allocate nothing). */
+int soil_ctx_alloc_count(const soil_ctx* ctx, uint64_t* allocs, uint64_t* frees);
 
 /* ---- systems ------------------------------------------------------------ */
 /* Domain + Atom + Neighbor + CommTopology resources of one simulation

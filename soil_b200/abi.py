@@ -181,6 +181,7 @@ PROTOTYPES = {
     "soil_ctx_destroy": (C.c_int, [P]),
     "soil_last_error": (C.c_char_p, [P]),
     "soil_ctx_bytes_in_use": (C.c_int, [P, pu64]),
+    "soil_ctx_alloc_count": (C.c_int, [P, pu64, pu64]),
     "soil_sys_create": (C.c_int, [P, C.POINTER(SoilBox), C.POINTER(SoilNeighCfg), dbl, PP]),
     "soil_sys_destroy": (C.c_int, [P]),
     "soil_sys_register_column": (C.c_int, [P, C.c_char_p, i32, u32, pi32]),

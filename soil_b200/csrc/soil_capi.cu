@@ -59,12 +59,14 @@ int ctx_reserve(soil_ctx* ctx, uint64_t bytes) {
         return SOIL_ERR_OOM;
     }
     ctx->in_use += bytes;
+    ctx->allocs += 1;
     return SOIL_OK;
 }
 
 void ctx_release(soil_ctx* ctx, uint64_t bytes) {
     std::lock_guard<std::mutex> g(ctx->mu);
     ctx->in_use -= bytes;
+    ctx->frees += 1;
 }
 
 int dev_alloc(soil_sys* s, void** p, uint64_t bytes) {
@@ -112,16 +114,23 @@ void free_cols(soil_sys* s, AtomCols& c) {
 }
 
 // Allocate a column set of capacity `cap`, copying [0, keep) from `old`.
+// On failure nothing stays allocated.
 int alloc_cols(soil_sys* s, AtomCols& c, uint64_t cap, const AtomCols* old, uint64_t keep) {
     AtomCols n{};
     n.cap = cap;
     n.nplanes = s->nplanes;
-    for (int k = 0; k < kDoubleCols; ++k) TRY(dev_alloc(s, (void**)dcol(n, k), cap * 8));
-    TRY(dev_alloc(s, (void**)&n.tag, cap * 4));
-    TRY(dev_alloc(s, (void**)&n.type, cap * 4));
-    TRY(dev_alloc(s, (void**)&n.img, cap * 12));
-    TRY(dev_alloc(s, (void**)&n.origin, cap * 4));
-    for (int q = 0; q < s->nplanes; ++q) TRY(dev_alloc(s, (void**)&n.planes[q], cap * 8));
+    int st = SOIL_OK;
+    for (int k = 0; k < kDoubleCols && st == SOIL_OK; ++k) st = dev_alloc(s, (void**)dcol(n, k), cap * 8);
+    if (st == SOIL_OK) st = dev_alloc(s, (void**)&n.tag, cap * 4);
+    if (st == SOIL_OK) st = dev_alloc(s, (void**)&n.type, cap * 4);
+    if (st == SOIL_OK) st = dev_alloc(s, (void**)&n.img, cap * 12);
+    if (st == SOIL_OK) st = dev_alloc(s, (void**)&n.origin, cap * 4);
+    for (int q = 0; q < s->nplanes && st == SOIL_OK; ++q)
+        st = dev_alloc(s, (void**)&n.planes[q], cap * 8);
+    if (st != SOIL_OK) {
+        free_cols(s, n);
+        return st;
+    }
     if (old && keep) {
         AtomCols o = *old;
         for (int k = 0; k < kDoubleCols; ++k)
@@ -159,7 +168,12 @@ int grow_atoms(soil_sys* s, uint64_t need, uint64_t keep) {
     uint64_t ncap = need + need / 4 + 1024;
     AtomCols nA{}, nB{};
     TRY(alloc_cols(s, nA, ncap, s->A.x ? &s->A : nullptr, keep));
-    TRY(alloc_cols(s, nB, ncap, nullptr, 0));
+    const int st = alloc_cols(s, nB, ncap, nullptr, 0);
+    if (st != SOIL_OK) {  // capacity unchanged: the new A goes back
+        CK(cudaStreamSynchronize(s->st));
+        free_cols(s, nA);
+        return st;
+    }
     CK(cudaStreamSynchronize(s->st));
     if (s->A.x) free_cols(s, s->A);
     if (s->B.x) free_cols(s, s->B);
@@ -1010,6 +1024,14 @@ int soil_ctx_bytes_in_use(const soil_ctx* ctx, uint64_t* out) {
     if (!ctx || !out) return SOIL_ERR_INVALID;
     std::lock_guard<std::mutex> g(ctx->mu);
     *out = ctx->in_use;
+    return SOIL_OK;
+}
+
+int soil_ctx_alloc_count(const soil_ctx* ctx, uint64_t* allocs, uint64_t* frees) {
+    if (!ctx) return SOIL_ERR_INVALID;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (allocs) *allocs = ctx->allocs;
+    if (frees) *frees = ctx->frees;
     return SOIL_OK;
 }
 

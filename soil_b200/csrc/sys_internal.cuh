@@ -17,7 +17,8 @@ struct soil_ctx {
     uint64_t budget = 0;
     uint64_t in_use = 0;
     std::string err;
-    mutable std::mutex mu;  // guards in_use and err
+    uint64_t allocs = 0, frees = 0;
+    mutable std::mutex mu;  // guards in_use, the counters and err
 };
 
 namespace soil_host {

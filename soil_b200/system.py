@@ -37,6 +37,12 @@ class Context:
         self.check(self.lib.soil_ctx_bytes_in_use(self.h, C.byref(v)), "bytes_in_use")
         return v.value
 
+    def alloc_count(self):
+        """(device allocations, frees) made through this context so far."""
+        a, f = C.c_uint64(), C.c_uint64()
+        self.check(self.lib.soil_ctx_alloc_count(self.h, C.byref(a), C.byref(f)), "alloc_count")
+        return a.value, f.value
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.soil_ctx_destroy(self.h)
@@ -117,6 +123,13 @@ class System:
         cb = abi.SOIL_FORCE_FN(lambda v, u: fn(v.contents, user))
         self._hook = cb
         self._c(self.lib.soil_sys_set_force_hook(self.h, cb, None), "hook")
+
+    def set_force_hook_ptr(self, fn_addr, user_addr=None):
+        """Install a native hook by address (a soil_force_fn exported by a
+        shared library); user_addr is passed through to it."""
+        cb = abi.SOIL_FORCE_FN(fn_addr)
+        self._hook = cb
+        self._c(self.lib.soil_sys_set_force_hook(self.h, cb, user_addr), "hook")
 
     def step(self, n=1):
         self._c(self.lib.soil_step(self.h, n), "soil_step")

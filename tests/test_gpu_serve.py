@@ -91,3 +91,26 @@ def test_served_cancel_and_release(ctx):
         sv.poll(a)
     sv.close()
     sctx.close()
+
+
+def test_served_failures_are_isolated(ctx):
+    """Host-side fault injection: a malformed request is refused at submit;
+    a job that does not fit the context's HBM budget fails with an error
+    message and frees what it took; the loop goes on serving."""
+    sctx = system.Context(0, hbm_budget_bytes=64 << 20)
+    sv = serve.Server(sctx, quantum_steps=8)
+    bad = W.config5_job(0, nmin=1024, nmax=2000, smin=20, smax=30)
+    bad.harmonic_k = 0.0  # no consumer: not a servable job
+    with pytest.raises(abi.SoilError):
+        sv.submit(bad)
+    big = W.config5_job(1, nmin=200000, nmax=262144, smin=20, smax=30)
+    small = W.config5_job(2, nmin=1024, nmax=2000, smin=20, smax=30)
+    jb = sv.submit(big)
+    js = sv.submit(small)
+    ib, is_ = sv.wait(jb, timeout=120), sv.wait(js, timeout=120)
+    assert ib["state"] == "failed" and "budget" in sv.error(jb)
+    assert is_["state"] == "done"
+    assert_same_result(sv.result(js), alone_result(ctx, small), "job after a failure")
+    sv.close()
+    assert sctx.bytes_in_use() < (64 << 20)
+    sctx.close()
