@@ -237,6 +237,22 @@ int soil_sys_get_sort_perm(soil_sys* sys, uint32_t* perm);
 /* Device pointers for an external consumer (valid until the next rebuild). */
 int soil_sys_view(soil_sys* sys, soil_dev_view* out);
 
+/* Checkpoint in the reference's restart wire format: RestartData
+ * (soil_print/src/lib.rs:318-418) as write_restart serialises it with bincode 1
+ * (soil_print/src/lib.rs:1390-1445): little endian, fixed-width integers, u64
+ * length before every Vec, fields in declaration order; the locals only, the
+ * registered columns in atom_data_buffers (registration order, each atom's
+ * values in a row).  buf NULL: *len gets the size only.  A buffer that is too
+ * small returns SOIL_ERR_CAPACITY with *len set.  A pending final half-kick is
+ * applied first (the reference writes after FinalIntegration). */
+int soil_sys_save_restart(soil_sys* sys, uint64_t total_cycle, uint8_t* buf, uint64_t cap,
+                          uint64_t* len);
+/* read_restart (soil_print/src/lib.rs:1527-1625): loads a restart into a
+ * system with its columns registered and no atoms (before soil_sys_setup):
+ * tags, types, positions, velocities, forces, masses, cutoff radii, columns;
+ * dt and the step count come from the data. */
+int soil_sys_load_restart(soil_sys* sys, const uint8_t* buf, uint64_t len, uint64_t* total_cycle);
+
 /* Stable counting sort of n positions by bin cell that allocates no device
  * memory.  This has no counterpart in the reference: it serves hosts that
  * cannot allocate device memory once they run (a fixed HBM plan, or an

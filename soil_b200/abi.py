@@ -238,6 +238,8 @@ PROTOTYPES = {
     "soil_server_release": (C.c_int, [P, u64]),
     "soil_server_job_error": (C.c_int, [P, u64, C.c_char_p, u64]),
     "soil_server_get_stats": (C.c_int, [P, C.POINTER(SoilServerStats)]),
+    "soil_sys_save_restart": (C.c_int, [P, u64, P, u64, pu64]),
+    "soil_sys_load_restart": (C.c_int, [P, P, u64, pu64]),
     "soil_kernel_launches": (C.c_uint64, []),
     "soil_sys_set_timing": (C.c_int, [P, u32]),
     "soil_sys_get_timing": (C.c_int, [P, pdbl, pu64, pu64]),

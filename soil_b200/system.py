@@ -229,6 +229,24 @@ class System:
                                              _p(iv, C.c_uint64)), "get_timing")
         return ms, la, iv
 
+    def save_restart(self, total_cycle=None):
+        """The reference's restart bytes (soil_sys_save_restart); total_cycle
+        defaults to the steps taken."""
+        cyc = self.counts().step if total_cycle is None else total_cycle
+        n = C.c_uint64()
+        self._c(self.lib.soil_sys_save_restart(self.h, cyc, None, 0, C.byref(n)), "save_restart")
+        buf = (C.c_uint8 * n.value)()
+        self._c(self.lib.soil_sys_save_restart(self.h, cyc, buf, n.value, C.byref(n)), "save_restart")
+        return bytes(buf)
+
+    def load_restart(self, data):
+        """Load restart bytes into this (empty, columns registered) system; returns
+        the step count stored in them."""
+        buf = (C.c_uint8 * len(data)).from_buffer_copy(data)
+        cyc = C.c_uint64()
+        self._c(self.lib.soil_sys_load_restart(self.h, buf, len(data), C.byref(cyc)), "load_restart")
+        return cyc.value
+
     def view(self):
         v = abi.SoilDevView()
         self._c(self.lib.soil_sys_view(self.h, C.byref(v)), "view")
