@@ -132,6 +132,16 @@ typedef struct soil_dev_view {
     int32_t newton;
     double* const* columns;           /* device array of ncolumns device pointers */
     void* stream;                     /* cudaStream_t the hook must launch on */
+    /* For deterministic consumers (include/soil_consumer.cuh): the transposed
+     * half list — in_list[in_start[a] .. in_start[a+1]) are the rows that list
+     * atom a, ascending — the ghost images' sources and the reverse-comm fold
+     * program (fold_list[fold_start[t] .. fold_start[t+1]) are local t's
+     * images, ghost index minus nlocal, in fold order). */
+    const uint32_t* in_start;         /* nlocal + nghost + 1 */
+    const uint32_t* in_list;          /* npairs */
+    const int32_t* origin;            /* nlocal + nghost: source atom of each ghost */
+    const uint32_t* fold_start;       /* nlocal + 1 */
+    const uint32_t* fold_list;        /* nghost */
 } soil_dev_view;
 
 /* Force hook (the device analogue of a Force-phase system, and of the
@@ -234,7 +244,9 @@ int soil_sys_get_swap(soil_sys* sys, int32_t s, uint64_t* recv_start,
                       double vel_offset[3], uint32_t* send_indices);
 /* Permutation applied by the last spatial sort (perm[new] = old), nlocal entries. */
 int soil_sys_get_sort_perm(soil_sys* sys, uint32_t* perm);
-/* Device pointers for an external consumer (valid until the next rebuild). */
+/* Device pointers for an external consumer (valid until the next rebuild).
+ * Returns after the system's stream has drained, so the pointers may be used
+ * on any stream. */
 int soil_sys_view(soil_sys* sys, soil_dev_view* out);
 
 /* Checkpoint in the reference's restart wire format: RestartData

@@ -100,6 +100,11 @@ class SoilDevView(C.Structure):
         ("newton", C.c_int32),
         ("columns", C.c_void_p),
         ("stream", C.c_void_p),
+        ("in_start", C.c_void_p),
+        ("in_list", C.c_void_p),
+        ("origin", C.c_void_p),
+        ("fold_start", C.c_void_p),
+        ("fold_list", C.c_void_p),
     ]
 
 

@@ -131,10 +131,11 @@ enum { G_INTEGRATE, G_SORT, G_SORT_APPLY, G_BORDERS, G_NEIGHBOR, G_FORCE };
 int balloc(soil_batch* b, void** p, uint64_t bytes) {
     if (bytes == 0) bytes = 16;
     TRY(ctx_reserve(b->ctx, bytes));
-    if (cudaMalloc(p, bytes) != cudaSuccess) {
+    if (cudaMallocFromPoolAsync(p, bytes, b->ctx->pool, b->st) != cudaSuccess) {
         cudaGetLastError();
         ctx_release(b->ctx, bytes);
-        return fail(b->ctx, SOIL_ERR_OOM, "cudaMalloc(%llu) failed", (unsigned long long)bytes);
+        return fail(b->ctx, SOIL_ERR_OOM, "device allocation of %llu bytes failed",
+                    (unsigned long long)bytes);
     }
     b->dev_bytes += bytes;
     return SOIL_OK;
@@ -142,7 +143,7 @@ int balloc(soil_batch* b, void** p, uint64_t bytes) {
 
 void bfree(soil_batch* b, void* p, uint64_t bytes) {
     if (!p) return;
-    cudaFree(p);
+    cudaFreeAsync(p, b->st);  // after the batch's work already enqueued
     if (bytes == 0) bytes = 16;
     ctx_release(b->ctx, bytes);
     b->dev_bytes -= bytes;

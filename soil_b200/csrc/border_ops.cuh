@@ -88,17 +88,19 @@ __device__ __forceinline__ void border_warp_images(
     const uint64_t r = w * 32 + lane;
     const uint32_t bits = r < nlocal ? face[r] : 0u;
     const uint64_t cw = w / kScanChunk;
+    if (!__ballot_sync(0xffffffffu, bits != 0u)) {  // no images: empty fold programs
+        const uint32_t fold0 =
+            offs[kBorderCats * nw + w] + (cpre ? cpre[kBorderCats * nchunks + cw] : 0u);
+        if (r < nlocal) fold_start[r] = fold0;
+        if (r + 1 == nlocal) fold_start[nlocal] = fold0;
+        return;
+    }
     // lane k <= 26: offset of this tile's members of category k (k = 26: images)
     const uint32_t off_lane =
         lane <= (uint32_t)kBorderCats
             ? offs[lane * nw + w] + (cpre ? cpre[lane * nchunks + cw] : 0u)
             : 0u;
     const uint32_t fold0 = __shfl_sync(0xffffffffu, off_lane, kBorderCats);
-    if (!__ballot_sync(0xffffffffu, bits != 0u)) {  // no images: empty fold programs
-        if (r < nlocal) fold_start[r] = fold0;
-        if (r + 1 == nlocal) fold_start[nlocal] = fold0;
-        return;
-    }
     uint32_t recv[kNumSwaps];
     for (int s = 0; s < kNumSwaps; ++s)
         recv[s] = __shfl_sync(0xffffffffu, base_lane, cats.swap_first[s]);

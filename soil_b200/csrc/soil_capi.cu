@@ -72,19 +72,22 @@ void ctx_release(soil_ctx* ctx, uint64_t bytes) {
 int dev_alloc(soil_sys* s, void** p, uint64_t bytes) {
     if (bytes == 0) bytes = 16;
     TRY(ctx_reserve(s->ctx, bytes));
-    cudaError_t e = cudaMalloc(p, bytes);
+    // stream-ordered from the context's pool: no device-wide synchronisation,
+    // and freed memory stays in the pool for the next growth
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes, s->ctx->pool, s->st);
     if (e != cudaSuccess) {
         cudaGetLastError();
         ctx_release(s->ctx, bytes);
-        return fail(s->ctx, SOIL_ERR_OOM, "cudaMalloc(%llu): %s", (unsigned long long)bytes,
+        return fail(s->ctx, SOIL_ERR_OOM, "cudaMallocAsync(%llu): %s", (unsigned long long)bytes,
                     cudaGetErrorString(e));
     }
     return SOIL_OK;
 }
 
+// Frees in stream order after every use already enqueued on the system's stream.
 void dev_free(soil_sys* s, void* p, uint64_t bytes) {
     if (!p) return;
-    cudaFree(p);
+    cudaFreeAsync(p, s->st);
     if (bytes == 0) bytes = 16;
     ctx_release(s->ctx, bytes);
 }
@@ -170,12 +173,10 @@ int grow_atoms(soil_sys* s, uint64_t need, uint64_t keep) {
     TRY(alloc_cols(s, nA, ncap, s->A.x ? &s->A : nullptr, keep));
     const int st = alloc_cols(s, nB, ncap, nullptr, 0);
     if (st != SOIL_OK) {  // capacity unchanged: the new A goes back
-        CK(cudaStreamSynchronize(s->st));
         free_cols(s, nA);
         return st;
     }
-    CK(cudaStreamSynchronize(s->st));
-    if (s->A.x) free_cols(s, s->A);
+    if (s->A.x) free_cols(s, s->A);  // after the copies above, in stream order
     if (s->B.x) free_cols(s, s->B);
     s->A = nA;
     s->B = nB;
@@ -638,7 +639,16 @@ void border_setup(const soil_sys* s, BorderDim bds[3]) {
 
 // Capacity for this pass's ghosts: those of the last pass plus a margin.
 int borders_reserve(soil_sys* s) {
-    const uint64_t want = s->nlocal + s->last_nghost + s->last_nghost / 4 + 4096;
+    // ghosts of the last pass, or before any pass the count a uniform density
+    // gives: locals x (prod (L_d + 2 gc) / prod L_d - 1)
+    uint64_t g = s->last_nghost;
+    if (g == 0 && s->nlocal) {
+        double f = 1.0;
+        for (int d = 0; d < 3; ++d)
+            f *= (s->size[d] + 2.0 * s->domain_ghost_cutoff) / s->size[d];
+        g = (uint64_t)((double)s->nlocal * (f - 1.0));
+    }
+    const uint64_t want = s->nlocal + g + g / 4 + 4096;
     TRY(grow_atoms(s, want, s->nlocal));
     return borders_arrays(s);
 }
@@ -834,7 +844,8 @@ int phase_neighbor(soil_sys* s) {
     s->npairs = np;
     s->rebuilds += 1;
     s->in_lists_valid = false;
-    if (builtin_consumer(s)) TRY(build_in_lists(s));
+    // the transposed lists serve the built-in consumer and any force hook
+    if (builtin_consumer(s) || s->hook) TRY(build_in_lists(s));
     return SOIL_OK;
 }
 
@@ -858,11 +869,17 @@ int make_view(soil_sys* s, soil_dev_view* v) {
     v->newton = s->newton ? 1 : 0;
     v->columns = s->d_colptrs.p;
     v->stream = (void*)s->st;
+    v->in_start = s->in_lists_valid ? s->in_start.p : nullptr;
+    v->in_list = s->in_lists_valid ? s->in_list.p : nullptr;
+    v->origin = s->A.origin;
+    v->fold_start = s->fold_start.p;
+    v->fold_list = s->fold_list.p;
     return SOIL_OK;
 }
 
 int phase_force(soil_sys* s) {
     if (s->hook) {
+        if (!s->in_lists_valid && s->npairs + s->nlocal > 0) TRY(build_in_lists(s));
         soil_dev_view v;
         TRY(make_view(s, &v));
         int r = s->hook(&v, s->hook_user);
@@ -1009,11 +1026,27 @@ int soil_ctx_create(int device, uint64_t hbm_budget_bytes, soil_ctx** out) {
     if (!c) return SOIL_ERR_OOM;
     c->device = device;
     c->budget = hbm_budget_bytes;
+    // Device arrays come from a stream-ordered pool of this context that keeps
+    // freed memory (the budget counts what is in use); growth of a system's
+    // arrays then neither synchronises the device nor maps new memory.
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaMemPoolCreate(&c->pool, &props) != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        return SOIL_ERR_CUDA;
+    }
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     *out = c;
     return SOIL_OK;
 }
 
 int soil_ctx_destroy(soil_ctx* ctx) {
+    // the pool's memory goes back once the last outstanding free has run
+    if (ctx && ctx->pool) cudaMemPoolDestroy(ctx->pool);
     delete ctx;
     return SOIL_OK;
 }
@@ -1410,7 +1443,8 @@ int soil_sys_get_sort_perm(soil_sys* s, uint32_t* perm) {
 int soil_sys_view(soil_sys* s, soil_dev_view* out) {
     if (!s || !out) return SOIL_ERR_INVALID;
     TRY(flush_pending(s));
-    return make_view(s, out);
+    TRY(make_view(s, out));
+    return sync(s);  // stream-ordered allocations are ready for every stream
 }
 
 uint64_t soil_kernel_launches(void) { return launches_so_far(); }

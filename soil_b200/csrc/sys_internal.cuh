@@ -18,6 +18,7 @@ struct soil_ctx {
     uint64_t in_use = 0;
     std::string err;
     uint64_t allocs = 0, frees = 0;
+    cudaMemPool_t pool = nullptr;  // stream-ordered device memory of every system and batch
     mutable std::mutex mu;  // guards in_use, the counters and err
 };
 
@@ -181,10 +182,7 @@ int ensure(soil_sys* s, DArr<T>& a, uint64_t need, uint64_t keep = 0) {
     void* np = nullptr;
     TRY(dev_alloc(s, &np, ncap * sizeof(T)));
     if (a.p && keep) CK(cudaMemcpyAsync(np, a.p, keep * sizeof(T), cudaMemcpyDeviceToDevice, s->st));
-    if (a.p) {
-        CK(cudaStreamSynchronize(s->st));
-        dev_free(s, a.p, a.cap * sizeof(T));
-    }
+    if (a.p) dev_free(s, a.p, a.cap * sizeof(T));  // stream-ordered, after the copy
     a.p = (T*)np;
     a.cap = ncap;
     return SOIL_OK;

@@ -60,6 +60,7 @@ int main(void) {
   printf("%zu %zu %zu\n", offsetof(soil_neigh_cfg, additive_skin), offsetof(soil_counts, comm_state),
          offsetof(soil_counts, tilt_xy));
   printf("%zu %zu\n", offsetof(soil_dev_view, columns), offsetof(soil_dev_view, stream));
+  printf("%zu %zu\n", offsetof(soil_dev_view, in_start), offsetof(soil_dev_view, fold_list));
   printf("%zu %zu %zu %zu\n", sizeof(soil_server_cfg), sizeof(soil_job_spec), sizeof(soil_job_info),
          sizeof(soil_server_stats));
   printf("%zu %zu %zu %zu\n", offsetof(soil_job_spec, natoms), offsetof(soil_job_spec, steps),
@@ -76,6 +77,7 @@ int main(void) {
             abi.SoilNeighCfg.additive_skin.offset, abi.SoilCounts.comm_state.offset,
             abi.SoilCounts.tilt_xy.offset,
             abi.SoilDevView.columns.offset, abi.SoilDevView.stream.offset,
+            abi.SoilDevView.in_start.offset, abi.SoilDevView.fold_list.offset,
             C.sizeof(abi.SoilServerCfg), C.sizeof(abi.SoilJobSpec), C.sizeof(abi.SoilJobInfo),
             C.sizeof(abi.SoilServerStats),
             abi.SoilJobSpec.natoms.offset, abi.SoilJobSpec.steps.offset,

@@ -91,9 +91,16 @@ def test_batch_threaded_planning_equals_alone(ctx, monkeypatch):
 def test_batch_fresh_boxes_ghost_growth(ctx):
     """Fresh boxes (first step in the batch) whose ghosts outgrow the first
     reservation, next to small boxes: the border pass is repeated for the
-    large ones only, and every box still matches its alone run."""
+    large ones only, and every box still matches its alone run.  The first
+    reservation assumes a uniform density, so the large boxes crowd 45% of
+    their atoms into a column along the low x / low y edge (three images
+    each: about 1.7 ghosts per atom instead of 0.35)."""
     ws = [W.poly(f"dense{i}", 11, n, 0.55, 1e-4, 10, harmonic_k=1e3, box=i)
           for i, n in enumerate([20000, 300, 24000, 280, 500, 16000])]
+    for w in ws:
+        if w.n >= 10000:
+            col = np.arange(w.n) % 20 < 9
+            w.pos[col, :2] *= 1.2 / w.L
     ws[2].shear_rate = 0.1
     alone = [system.from_workload(ctx, w) for w in ws]
     mixed = [system.from_workload(ctx, w) for w in ws]

@@ -17,14 +17,23 @@ pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
+def _build(tmp_path_factory, name):
+    out = tmp_path_factory.mktemp("hook") / f"lib{name}.so"
+    subprocess.check_call(["/usr/local/cuda/bin/nvcc", "-gencode", "arch=compute_100a,code=sm_100a",
+                           "-O3", "-fmad=false", "-shared", "-Xcompiler", "-fPIC",
+                           "-I", os.path.join(ROOT, "include"),
+                           os.path.join(ROOT, "tests", "hooks", f"{name}.cu"), "-o", str(out)])
+    return C.CDLL(str(out))
+
+
 @pytest.fixture(scope="module")
 def hook_lib(tmp_path_factory):
-    out = tmp_path_factory.mktemp("hook") / "libharmonic_hook.so"
-    subprocess.check_call(["/usr/local/cuda/bin/nvcc", "-gencode", "arch=compute_100a,code=sm_100a",
-                           "-O3", "-shared", "-Xcompiler", "-fPIC",
-                           "-I", os.path.join(ROOT, "include"),
-                           os.path.join(ROOT, "tests", "hooks", "harmonic_hook.cu"), "-o", str(out)])
-    return C.CDLL(str(out))
+    return _build(tmp_path_factory, "harmonic_hook")
+
+
+@pytest.fixture(scope="module")
+def gather_lib(tmp_path_factory):
+    return _build(tmp_path_factory, "gather_hook")
 
 
 def _with_hook(ctx, w, lib, name, k):
@@ -71,3 +80,25 @@ def test_failing_hook_stops_the_step(ctx, hook_lib):
         s.step(1)
     assert e.value.status == abi.SOIL_ERR_INVALID and "hook" in str(e.value)
     s.close()
+
+
+@pytest.mark.parametrize("shear,newton", [(0.0, 1), (2.0, 1), (0.0, 0)])
+def test_external_gather_consumer_is_bit_exact(ctx, gather_lib, shear, newton):
+    """A consumer written against include/soil_consumer.cuh, outside the
+    library, reproduces the built-in consumer's trajectory bit for bit."""
+    from helpers import assert_same_lists, assert_same_state
+    w = W.poly("gather", 15, 4000, 0.5, 1e-4, 40, harmonic_k=1e3, shear_rate=shear)
+    w.cfg.newton = newton
+    ref = system.from_workload(ctx, w)
+    hk = _with_hook(ctx, w, gather_lib, "gather_harmonic_hook", w.harmonic_k)
+    ref.step(20)
+    hk.step(20)
+    ref.step(20)
+    hk.step(20)
+    assert_same_state(hk, ref, "external gather consumer")
+    assert_same_lists(hk, ref, "external gather consumer")
+    assert np.any(hk.atoms()["force"] != 0.0)
+    v = hk.view()
+    assert v.in_start and v.in_list and v.origin and v.fold_start
+    ref.close()
+    hk.close()
