@@ -122,6 +122,15 @@ struct soil_batch {
     size_t min_parallel = 64;        // fewer boxes are planned on the calling thread
     // per-step scratch
     std::vector<uint8_t> check, full_at_pbc, run, periodic, apply, rebuild, planned;
+    // Per-slot copies of the counts the step's serial loops read, so that they
+    // do not walk every member's system record (written by the planning
+    // threads) on the calling thread.  nlocal and newton are fixed while a
+    // system is batched; nghost and cells are refreshed where they change.
+    struct Hot {
+        uint64_t nlocal = 0, nghost = 0, cells = 0;
+        uint8_t newton = 0, cells_valid = 0;
+    };
+    std::vector<Hot> hot;
 };
 
 namespace {
@@ -542,6 +551,7 @@ int grow_slots(soil_batch* b, uint32_t need) {
     for (auto* v : {&b->check, &b->full_at_pbc, &b->run, &b->periodic, &b->apply, &b->rebuild,
                     &b->planned})
         v->assign(ncap, 0);
+    b->hot.resize(ncap);
     b->cap = ncap;
     return SOIL_OK;
 }
@@ -563,7 +573,7 @@ int launch_borders(soil_batch* b, const std::vector<uint32_t>& R, Stage& g, bool
                       b->binit.data() + (size_t)lo * kBorderStateWords,
                       (size_t)(hi - lo) * kBorderStateWords * 4));
     const int wt = stage_add(g);
-    for (uint32_t k : R) g.spans[wt].add(k, (b->slot[k]->nlocal + 31) / 32, 0);
+    for (uint32_t k : R) g.spans[wt].add(k, (b->hot[k].nlocal + 31) / 32, 0);
     TRY(stage_commit(b, g));
     const BatchArgs a = args_of(b);
     tic(b);
@@ -671,6 +681,13 @@ int batch_step(soil_batch* b, bool last) {
         if (run) fill_dev(b, k);
         if (run || b->planned[k])
             TRY(fill_step(b, k, b->apply[k] != 0, b->planned[k] ? b->bds[k].data() : nullptr));
+        // host bookkeeping of a sort that always applies; the tables above
+        // already describe the columns the kernels read and write
+        if (run && !periodic) sort_done(s, true, false);
+        auto& h = b->hot[k];
+        h.cells = s->total_cells;
+        if (b->full_at_pbc[k]) h.nghost = 0;
+        b->rebuild[k] = s->state == FULL_REBUILD;
         return SOIL_OK;
     }));
     std::vector<uint32_t> S, I;
@@ -688,13 +705,13 @@ int batch_step(soil_batch* b, bool last) {
         const int s_pbc = stage_add(g2), s_cells = stage_add(g2), s_loc = stage_add(g2),
                   s_id = stage_add(g2), s_gather = stage_add(g2);
         for (uint32_t k : M)
-            if (b->full_at_pbc[k]) g2.spans[s_pbc].add_nz(k, b->slot[k]->nlocal, 0);
+            if (b->full_at_pbc[k]) g2.spans[s_pbc].add_nz(k, b->hot[k].nlocal, 0);
         for (uint32_t k : S) {
-            const soil_sys* s = b->slot[k];
-            g2.spans[s_cells].add(k, s->total_cells, 0);
-            g2.spans[s_loc].add_nz(k, s->nlocal, 0);
-            if (b->periodic[k]) g2.spans[s_id].add_nz(k, s->nlocal, 0);
-            if (b->apply[k]) g2.spans[s_gather].add_nz(k, s->nlocal, 0);
+            const auto& h = b->hot[k];
+            g2.spans[s_cells].add(k, h.cells, 0);
+            g2.spans[s_loc].add_nz(k, h.nlocal, 0);
+            if (b->periodic[k]) g2.spans[s_id].add_nz(k, h.nlocal, 0);
+            if (b->apply[k]) g2.spans[s_gather].add_nz(k, h.nlocal, 0);
         }
         TRY(stage_commit(b, g2));
         tic(b);
@@ -722,7 +739,7 @@ int batch_step(soil_batch* b, bool last) {
             b->apply[k] = b->h_flags[k].not_identity != 0;
             if (b->apply[k]) {
                 TRY(fill_step(b, k, true, b->planned[k] ? b->bds[k].data() : nullptr));
-                g2b.spans[s_gather].add_nz(k, b->slot[k]->nlocal, 0);
+                g2b.spans[s_gather].add_nz(k, b->hot[k].nlocal, 0);
             }
         }
         TRY(put_tables(b, g2b));
@@ -730,15 +747,16 @@ int batch_step(soil_batch* b, bool last) {
         b_perm_gather(st, g2b.out[s_gather], a);
         TRY(check_kernels(b));
     }
-    for (uint32_t k : S) sort_done(b->slot[k], b->apply[k] != 0, b->periodic[k] != 0);
+    for (uint32_t k : I) {  // periodic sorts: applied only when not the identity
+        sort_done(b->slot[k], b->apply[k] != 0, true);
+        b->rebuild[k] = b->slot[k]->state == FULL_REBUILD;
+    }
     mark(b, HT_SORT);
 
     // ---- borders ----
     std::vector<uint32_t> R;
-    for (uint32_t k : M) {
-        b->rebuild[k] = b->slot[k]->state == FULL_REBUILD;
+    for (uint32_t k : M)
         if (b->rebuild[k]) R.push_back(k);
-    }
     TRY(for_boxes(b, R, [&](uint32_t k) -> int {
         soil_sys* s = b->slot[k];
         s->nghost = 0;
@@ -779,6 +797,12 @@ int batch_step(soil_batch* b, bool last) {
             TRY(borders_done(s, b->h_bread + (size_t)k * kBorderStateWords, b->bds[k].data()));
             TRY(neighbor_plan(s));
             fill_dev(b, k);
+            auto& h = b->hot[k];
+            h.nghost = s->nghost;
+            h.cells = s->total_cells;
+            // local bins of this step's sort are reused once, by this build
+            h.cells_valid = s->local_cells_valid ? 1 : 0;
+            s->local_cells_valid = false;
             return SOIL_OK;
         }));
     }
@@ -791,21 +815,20 @@ int batch_step(soil_batch* b, bool last) {
               n_copy = stage_add(g4), n_bin = stage_add(g4), n_all = stage_add(g4),
               n_rows = stage_add(g4);
     for (uint32_t k : M) {
-        soil_sys* s = b->slot[k];
+        const auto& h = b->hot[k];
         if (!b->rebuild[k]) {
-            g4.spans[s_fwd].add_nz(k, s->nghost, 0);
+            g4.spans[s_fwd].add_nz(k, h.nghost, 0);
             continue;
         }
-        const uint64_t nl = s->nlocal, ng = s->nghost;
+        const uint64_t nl = h.nlocal, ng = h.nghost;
         g4.spans[f_loc].add_nz(k, nl, 0);
-        g4.spans[n_cells].add(k, s->total_cells, 0);
-        if (s->local_cells_valid) {
+        g4.spans[n_cells].add(k, h.cells, 0);
+        if (h.cells_valid) {
             g4.spans[n_copy].add_nz(k, nl, 0);
             g4.spans[n_bin].add_nz(k, ng, nl);
         } else {
             g4.spans[n_bin].add_nz(k, nl + ng, 0);
         }
-        s->local_cells_valid = false;
         g4.spans[n_all].add_nz(k, nl + ng, 0);
         g4.spans[n_rows].add(k, nl, 0);
     }
@@ -836,11 +859,11 @@ int batch_step(soil_batch* b, bool last) {
                 return fail(b->ctx, SOIL_ERR_INVALID,
                             "neighbor stencil left the bin grid (atom outside the ghost layers)");
             const uint64_t np = b->h_totals[k], total = s->nlocal + s->nghost;
-            TRY(ensure(s, s->indices, np + 1));
-            TRY(ensure(s, s->in_count, total + 1));
-            TRY(ensure(s, s->in_start, total + 2));
-            TRY(ensure(s, s->in_cursor, total + 1));
-            TRY(ensure(s, s->in_list, np + 1));
+            TRY(ensure(s, s->indices, np + 1, 0, pair_room(np)));
+            TRY(ensure(s, s->in_count, total + 1, 0, s->acap + 1));
+            TRY(ensure(s, s->in_start, total + 2, 0, s->acap + 2));
+            TRY(ensure(s, s->in_cursor, total + 1, 0, s->acap + 1));
+            TRY(ensure(s, s->in_list, np + 1, 0, pair_room(np)));
             s->npairs = np;
             s->rebuilds += 1;
             s->in_lists_valid = true;
@@ -858,15 +881,15 @@ int batch_step(soil_batch* b, bool last) {
     const int r_loc = stage_add(g5), r_all = stage_add(g5), r_scan = stage_add(g5),
               h_all = stage_add(g5), v_loc = stage_add(g5), l_loc = stage_add(g5);
     for (uint32_t k : M) {
-        soil_sys* s = b->slot[k];
-        const uint64_t nl = s->nlocal, total = nl + s->nghost;
+        const auto& h = b->hot[k];
+        const uint64_t nl = h.nlocal, total = nl + h.nghost;
         if (b->rebuild[k]) {
             g5.spans[r_loc].add_nz(k, nl, 0);
             g5.spans[r_all].add_nz(k, total, 0);
             g5.spans[r_scan].add(k, total, 0);
         }
         g5.spans[h_all].add_nz(k, total, 0);
-        if (s->newton && s->nghost) g5.spans[v_loc].add_nz(k, nl, 0);
+        if (h.newton && h.nghost) g5.spans[v_loc].add_nz(k, nl, 0);
         g5.spans[l_loc].add_nz(k, nl, 0);
     }
     toc(b, BT_NEIGHBOR);  // no-op when the rebuild path closed it
@@ -894,11 +917,12 @@ int batch_step(soil_batch* b, bool last) {
         toc(b, BT_STEP);
     }
     TRY(check_kernels(b));
-    for (uint32_t k : M) {
+    TRY(for_boxes(b, M, [&](uint32_t k) -> int {
         soil_sys* s = b->slot[k];
         s->pending_final = !last;
         s->steps_done += 1;
-    }
+        return SOIL_OK;
+    }));
     mark(b, HT_LISTS);
     b->steps += 1;
     return SOIL_OK;
@@ -956,6 +980,15 @@ int soil_batch_create(soil_ctx* ctx, soil_batch** out) {
         cudaGetLastError();
         delete b;
         return fail(ctx, SOIL_ERR_CUDA, "stream creation failed");
+    }
+    // every stage's staging buffers up front: a stage first used late (a
+    // periodic sort that applies) then allocates nothing inside a run
+    for (Stage& g : b->stage) {
+        const int st = stage_grow(b, g, 1);
+        if (st != SOIL_OK) {
+            soil_batch_destroy(b);
+            return st;
+        }
     }
     *out = b;
     return SOIL_OK;
@@ -1016,6 +1049,11 @@ int soil_batch_add(soil_batch* b, soil_sys* s) {
     std::memset(&b->h_dev[k], 0, sizeof(BoxDev));
     fill_dev(b, k);
     b->dev_dirty[k] = 1;
+    b->hot[k].nlocal = s->nlocal;
+    b->hot[k].nghost = s->nghost;
+    b->hot[k].cells = s->total_cells;
+    b->hot[k].newton = s->newton ? 1 : 0;
+    b->hot[k].cells_valid = 0;
     TRY(fill_step(b, k, false, nullptr));
     rebuild_members(b);
     return SOIL_OK;

@@ -185,6 +185,14 @@ int grow_atoms(soil_sys* s, uint64_t need, uint64_t keep) {
     uint64_t gkeep = keep > s->nlocal ? keep - s->nlocal : 0;
     TRY(ensure(s, s->ghost_root, ncap, gkeep));
     TRY(ensure(s, s->ghost_chain, ncap, gkeep));
+    // The spatial sort's per-atom arrays follow the capacity, so a system's
+    // first sort (often its first rebuild inside a run) allocates nothing.
+    // Growth happens between a sort and the neighbor build that reuses its
+    // local cells, so the locals' entries survive it.
+    TRY(ensure(s, s->sort_cell, ncap, s->sort_cell.p ? std::min(keep, s->sort_cell.cap) : 0));
+    TRY(ensure(s, s->sort_perm, ncap, s->sort_perm.p ? std::min(keep, s->sort_perm.cap) : 0));
+    TRY(ensure(s, s->sorted_local_cell, ncap,
+               s->sorted_local_cell.p ? std::min(keep, s->sorted_local_cell.cap) : 0));
     s->colptrs_dirty = true;
     return SOIL_OK;
 }
@@ -518,10 +526,11 @@ int sort_plan(soil_sys* s, bool* run, bool* periodic) {
     TRY(ensure(s, s->sort_cell, s->acap));
     TRY(ensure(s, s->sort_perm, s->acap));
     TRY(ensure(s, s->sorted_local_cell, s->acap));
-    TRY(ensure(s, s->cell_counts, nc + 1));
-    TRY(ensure(s, s->cell_start, nc + 2));
-    TRY(ensure(s, s->cell_cursor, nc + 1));
-    TRY(ensure(s, s->scan_tmp, scan_temp_words(nc + s->acap + 2)));
+    TRY(ensure(s, s->cell_counts, nc + 1, 0, 2 * nc + 64));
+    TRY(ensure(s, s->cell_start, nc + 2, 0, 2 * nc + 64));
+    TRY(ensure(s, s->cell_cursor, nc + 1, 0, 2 * nc + 64));
+    TRY(ensure(s, s->scan_tmp, scan_temp_words(nc + s->acap + 2), 0,
+               scan_temp_words(2 * nc + s->acap + 64)));
     return SOIL_OK;
 }
 
@@ -714,10 +723,10 @@ int phase_forward_comm(soil_sys* s) {
 
 int build_in_lists(soil_sys* s) {
     const uint64_t total = s->nlocal + s->nghost;
-    TRY(ensure(s, s->in_count, total + 1));
-    TRY(ensure(s, s->in_start, total + 2));
-    TRY(ensure(s, s->in_cursor, total + 1));
-    TRY(ensure(s, s->in_list, s->npairs + 1));
+    TRY(ensure(s, s->in_count, total + 1, 0, s->acap + 1));
+    TRY(ensure(s, s->in_start, total + 2, 0, s->acap + 2));
+    TRY(ensure(s, s->in_cursor, total + 1, 0, s->acap + 1));
+    TRY(ensure(s, s->in_list, s->npairs + 1, 0, pair_room(s->npairs)));
     TRY(ensure(s, s->scan_tmp, scan_temp_words(total + 2)));
     CK(cudaMemsetAsync(s->in_count.p, 0, total * 4, s->st));
     launch_in_count(s->st, s->nlocal, s->offsets.p, s->indices.p, s->in_count.p);
@@ -764,10 +773,11 @@ int neighbor_plan(soil_sys* s) {
     TRY(ensure(s, s->sp, s->acap));
     if (s->filter == SOIL_FILTER_FP32_RECHECK) TRY(ensure(s, s->spf, s->acap));
     TRY(ensure(s, s->row_slots, (uint64_t)nl * kRowSlots + 1));
-    TRY(ensure(s, s->cell_counts, nc + 1));
-    TRY(ensure(s, s->cell_start, nc + 2));
-    TRY(ensure(s, s->cell_cursor, nc + 1));
-    TRY(ensure(s, s->scan_tmp, scan_temp_words(nc + s->acap + 2)));
+    TRY(ensure(s, s->cell_counts, nc + 1, 0, 2 * nc + 64));
+    TRY(ensure(s, s->cell_start, nc + 2, 0, 2 * nc + 64));
+    TRY(ensure(s, s->cell_cursor, nc + 1, 0, 2 * nc + 64));
+    TRY(ensure(s, s->scan_tmp, scan_temp_words(nc + s->acap + 2), 0,
+               scan_temp_words(2 * nc + s->acap + 64)));
     return SOIL_OK;
 }
 
@@ -836,7 +846,7 @@ int phase_neighbor(soil_sys* s) {
     TRY(check_launch(s));
     TRY(read_flags(s));
     const uint64_t np = s->hword[0];
-    TRY(ensure(s, s->indices, np + 1));
+    TRY(ensure(s, s->indices, np + 1, 0, pair_room(np)));
     if (s->hflags->error)
         return fail(s->ctx, SOIL_ERR_INVALID, "neighbor stencil left the bin grid (atom outside the ghost layers)");
     launch_pair_fill(s->st, p, s->rowcount.p, s->row_slots.p, s->offsets.p, s->indices.p);
@@ -1275,6 +1285,7 @@ int soil_sys_set_harmonic(soil_sys* s, double k, int32_t radius_col) {
     if (k != 0.0 && (radius_col < 0 || (size_t)radius_col >= s->cols.size() ||
                      s->cols[radius_col].width != 1))
         return fail(s->ctx, SOIL_ERR_INVALID, "radius column must be a registered width-1 column");
+    if (s->batch) return fail(s->ctx, SOIL_ERR_STATE, "the force of a batched system is fixed");
     s->harmonic_k = k;
     s->radius_col = radius_col;
     s->in_lists_valid = false;
@@ -1283,6 +1294,7 @@ int soil_sys_set_harmonic(soil_sys* s, double k, int32_t radius_col) {
 
 int soil_sys_set_force_hook(soil_sys* s, soil_force_fn fn, void* user) {
     if (!s) return SOIL_ERR_INVALID;
+    if (s->batch) return fail(s->ctx, SOIL_ERR_STATE, "the force of a batched system is fixed");
     s->hook = fn;
     s->hook_user = user;
     return SOIL_OK;
@@ -1291,6 +1303,7 @@ int soil_sys_set_force_hook(soil_sys* s, soil_force_fn fn, void* user) {
 int soil_step(soil_sys* s, uint64_t nsteps) {
     if (!s) return SOIL_ERR_INVALID;
     if (!s->setup_done) return fail(s->ctx, SOIL_ERR_STATE, "soil_sys_setup has not run");
+    if (s->batch) return fail(s->ctx, SOIL_ERR_STATE, "a batched system steps through its batch");
     for (uint64_t k = 0; k < nsteps; ++k) TRY(full_step(s, k + 1 == nsteps));
     return SOIL_OK;
 }

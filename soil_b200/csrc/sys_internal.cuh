@@ -174,11 +174,15 @@ void ctx_release(soil_ctx* ctx, uint64_t bytes);
 int dev_alloc(soil_sys* s, void** p, uint64_t bytes);
 void dev_free(soil_sys* s, void* p, uint64_t bytes);
 
-// Grow `a` to hold `need` elements; the first `keep` elements survive.
+// Grow `a` to hold `need` elements; the first `keep` elements survive.  A
+// new array gets room for `room` elements (at least need + 25%), so counts
+// that drift between rebuilds (pairs, bins) can be given more headroom than
+// the check itself.
 template <class T>
-int ensure(soil_sys* s, DArr<T>& a, uint64_t need, uint64_t keep = 0) {
+int ensure(soil_sys* s, DArr<T>& a, uint64_t need, uint64_t keep = 0, uint64_t room = 0) {
     if (need <= a.cap && a.p) return SOIL_OK;
     uint64_t ncap = need + need / 4 + 64;
+    if (room > ncap) ncap = room;
     void* np = nullptr;
     TRY(dev_alloc(s, &np, ncap * sizeof(T)));
     if (a.p && keep) CK(cudaMemcpyAsync(np, a.p, keep * sizeof(T), cudaMemcpyDeviceToDevice, s->st));
@@ -189,6 +193,9 @@ int ensure(soil_sys* s, DArr<T>& a, uint64_t need, uint64_t keep = 0) {
 }
 
 int grow_atoms(soil_sys* s, uint64_t need, uint64_t keep);
+// Room for arrays indexed by pair (CSR indices, incoming lists): pair counts
+// drift between rebuilds, so a new array takes twice the current count.
+inline uint64_t pair_room(uint64_t np) { return 2 * np + 1024; }
 int update_colptrs(soil_sys* s);
 bool deform_host(soil_sys* s);
 double profile_center(const soil_sys* s);

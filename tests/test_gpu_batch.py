@@ -116,6 +116,29 @@ def test_batch_fresh_boxes_ghost_growth(ctx):
     batch.close()
 
 
+def test_batch_steady_state_allocates_nothing(ctx):
+    """After the first steps, stepping (rebuilds, periodic sorts, a box's
+    first displacement-triggered rebuild and sheared boxes included) takes no
+    device memory: arrays are sized with headroom for drifting ghost, pair
+    and bin counts, the sort's arrays follow the atom capacity, and the
+    batch's staging buffers exist from its creation."""
+    ws = mixed_boxes(count=8, nmax=3000)
+    boxes = [system.from_workload(ctx, w) for w in ws]
+    batch = system.Batch(ctx)
+    for s in boxes:
+        batch.add(s)
+    batch.step(3)
+    a0, _ = ctx.alloc_count()
+    r0 = sum(s.counts().rebuilds for s in boxes)
+    batch.step(60)
+    a1, _ = ctx.alloc_count()
+    assert sum(s.counts().rebuilds for s in boxes) > r0 + 60
+    assert a1 == a0, f"{a1 - a0} device allocations in steady state"
+    batch.close()
+    for s in boxes:
+        s.close()
+
+
 def test_batch_equals_oracle(ctx):
     ws = mixed_boxes(count=4, nmax=1200)
     pairs = [pair(ctx, w) for w in ws]
@@ -163,5 +186,15 @@ def test_batch_rejects_unsupported(ctx):
     batch = system.Batch(ctx)
     with pytest.raises(abi.SoilError):
         batch.add(s)
+    # a member steps only through its batch; once removed it steps alone
+    m = system.from_workload(ctx, W.config4_box(0, nmin=256, nmax=1000, steps=5))
+    batch.add(m)
+    with pytest.raises(abi.SoilError):
+        m.step(1)
+    batch.step(2)
+    batch.remove(m)
+    m.step(1)
+    assert m.counts().step == 3
     batch.close()
     s.close()
+    m.close()
