@@ -142,6 +142,19 @@ typedef struct soil_dev_view {
     const int32_t* origin;            /* nlocal + nghost: source atom of each ghost */
     const uint32_t* fold_start;       /* nlocal + 1 */
     const uint32_t* fold_list;        /* nghost */
+    /* Local atom each ghost images (ghost index minus nlocal). */
+    const uint32_t* ghost_root;       /* nghost */
+    /* Persistent per-neighbor slots (soil_sys_enable_slots; include/soil_slots.cuh):
+     * local atom i owns slots [i*slot_max, (i+1)*slot_max) of (partner tag,
+     * slot_width f64 payload).  The hook reads the last step's slots ("old")
+     * and writes this step's ("new"); the library swaps them after the hook.
+     * slot_max == 0: no slots. */
+    uint32_t slot_max;
+    uint32_t slot_width;
+    const uint32_t* slot_old_tag;     /* nlocal * slot_max; 0xFFFFFFFF = empty */
+    const double* slot_old_val;       /* nlocal * slot_max * slot_width */
+    uint32_t* slot_new_tag;
+    double* slot_new_val;
 } soil_dev_view;
 
 /* Force hook (the device analogue of a Force-phase system, and of the
@@ -248,6 +261,22 @@ int soil_sys_get_sort_perm(soil_sys* sys, uint32_t* perm);
  * Returns after the system's stream has drained, so the pointers may be used
  * on any stream. */
 int soil_sys_view(soil_sys* sys, soil_dev_view* out);
+
+/* Persistent per-neighbor state slots: the reference's NeighborSlots
+ * (crates/soil_gpu/src/neighbor_slots.rs:19-184: MAX_CONTACTS slots of
+ * (partner, payload) per atom, double-buffered, SENTINEL = empty), in FP64
+ * and keyed by the partner's TAG instead of its index, so a contact's state
+ * survives rebuilds, the spatial sort (an atom's slots move with it) and the
+ * pair moving from one atom's CSR row to the other's.  Every local atom gets
+ * max_contacts slots of `width` doubles, all empty; the force hook reads and
+ * writes them through soil_dev_view (helpers in include/soil_slots.cuh) and
+ * the library swaps the two sets after each hook call.  Not for batched
+ * systems.  max_contacts in [1, 1024], width in [1, 64]. */
+int soil_sys_enable_slots(soil_sys* sys, uint32_t max_contacts, uint32_t width);
+/* The slots the last hook call wrote, for local atoms 0..nlocal-1 in their
+ * current order: partner_tag (nlocal*max_contacts), payload
+ * (nlocal*max_contacts*width). */
+int soil_sys_get_slots(soil_sys* sys, uint32_t* partner_tag, double* payload);
 
 /* Checkpoint in the reference's restart wire format: RestartData
  * (soil_print/src/lib.rs:318-418) as write_restart serialises it with bincode 1

@@ -105,6 +105,13 @@ class SoilDevView(C.Structure):
         ("origin", C.c_void_p),
         ("fold_start", C.c_void_p),
         ("fold_list", C.c_void_p),
+        ("ghost_root", C.c_void_p),
+        ("slot_max", C.c_uint32),
+        ("slot_width", C.c_uint32),
+        ("slot_old_tag", C.c_void_p),
+        ("slot_old_val", C.c_void_p),
+        ("slot_new_tag", C.c_void_p),
+        ("slot_new_val", C.c_void_p),
     ]
 
 
@@ -219,6 +226,8 @@ PROTOTYPES = {
     "soil_sys_get_swap": (C.c_int, [P, i32, pu64, pu64, pdbl, pdbl, pu32]),
     "soil_sys_get_sort_perm": (C.c_int, [P, pu32]),
     "soil_sys_view": (C.c_int, [P, C.POINTER(SoilDevView)]),
+    "soil_sys_enable_slots": (C.c_int, [P, C.c_uint32, C.c_uint32]),
+    "soil_sys_get_slots": (C.c_int, [P, pu32, pdbl]),
     "soil_bin_sort_noalloc": (C.c_int, [P, P, P, P, u64, pdbl, pdbl, pi32, pdbl, pdbl, pdbl, i32,
                                         P, P, P]),
     "soil_batch_create": (C.c_int, [P, PP]),

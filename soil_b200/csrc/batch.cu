@@ -1030,6 +1030,7 @@ int soil_batch_add(soil_batch* b, soil_sys* s) {
     if (!builtin_consumer(s))
         return fail(b->ctx, SOIL_ERR_INVALID,
                     "a batched system uses the built-in harmonic consumer and no force hook");
+    if (s->slot_max) return fail(b->ctx, SOIL_ERR_INVALID, "a batched system has no neighbor slots");
     int zp[kMaxPlanes], nz;
     zero_planes_of(s, SOIL_COL_ZERO, zp, &nz);
     if (nz) return fail(b->ctx, SOIL_ERR_INVALID, "#[zero] columns are not supported in a batch");

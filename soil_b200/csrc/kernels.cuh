@@ -77,6 +77,11 @@ void launch_perm_gather(cudaStream_t st, uint64_t n, const uint32_t* perm, const
 // flags->not_identity |= any perm[k] != k
 void launch_identity_check(cudaStream_t st, uint64_t n, const uint32_t* perm, DevFlags* flags);
 // out[k] = cell[perm[k]]
+// Slot rows (max tags, max*width payload values per atom) of the n locals
+// gathered through perm (dst row r = src row perm[r]).
+void launch_slot_gather(cudaStream_t st, uint64_t n, const uint32_t* perm, uint32_t max,
+                        uint32_t width, const uint32_t* src_tag, const double* src_val,
+                        uint32_t* dst_tag, double* dst_val);
 void launch_permute_u32(cudaStream_t st, uint64_t n, const uint32_t* perm, const uint32_t* in,
                         uint32_t* out);
 // inverse[sorted[m]] = m and the sorted records sp[m] = {x, y, z, cutoff}

@@ -193,7 +193,26 @@ int grow_atoms(soil_sys* s, uint64_t need, uint64_t keep) {
     TRY(ensure(s, s->sort_perm, ncap, s->sort_perm.p ? std::min(keep, s->sort_perm.cap) : 0));
     TRY(ensure(s, s->sorted_local_cell, ncap,
                s->sorted_local_cell.p ? std::min(keep, s->sorted_local_cell.cap) : 0));
+    TRY(slots_grow(s, ncap, keep));
     s->colptrs_dirty = true;
+    return SOIL_OK;
+}
+
+// Slot sets for `cap` atoms: the current set keeps its first `keep` rows and
+// every later row is empty; the other set is scratch for the next writer.
+int slots_grow(soil_sys* s, uint64_t cap, uint64_t keep) {
+    if (!s->slot_max) return SOIL_OK;
+    const uint64_t M = s->slot_max, W = s->slot_width;
+    const int o = s->slot_old;
+    if (!s->slot_tag[o].p) keep = 0;
+    TRY(ensure(s, s->slot_tag[o], cap * M, keep * M));
+    TRY(ensure(s, s->slot_val[o], cap * M * W, keep * M * W));
+    TRY(ensure(s, s->slot_tag[1 - o], cap * M));
+    TRY(ensure(s, s->slot_val[1 - o], cap * M * W));
+    if (cap > keep) {
+        CK(cudaMemsetAsync(s->slot_tag[o].p + keep * M, 0xFF, (cap - keep) * M * 4, s->st));
+        CK(cudaMemsetAsync(s->slot_val[o].p + keep * M * W, 0, (cap - keep) * M * W * 8, s->st));
+    }
     return SOIL_OK;
 }
 
@@ -579,6 +598,13 @@ int phase_sort(soil_sys* s) {
         // every column gathered through perm; ghosts (if any) are discarded by
         // the borders that always follows a permutation
         launch_perm_gather(s->st, nl, s->sort_perm.p, s->A, s->B);
+        if (s->slot_max) {  // slots move with their atoms
+            const int o = s->slot_old;
+            launch_slot_gather(s->st, nl, s->sort_perm.p, s->slot_max, s->slot_width,
+                               s->slot_tag[o].p, s->slot_val[o].p, s->slot_tag[1 - o].p,
+                               s->slot_val[1 - o].p);
+            s->slot_old = 1 - o;
+        }
         TRY(check_launch(s));
     }
     sort_done(s, apply, periodic_sort);
@@ -884,6 +910,16 @@ int make_view(soil_sys* s, soil_dev_view* v) {
     v->origin = s->A.origin;
     v->fold_start = s->fold_start.p;
     v->fold_list = s->fold_list.p;
+    v->ghost_root = s->ghost_root.p;
+    if (s->slot_max) {
+        const int o = s->slot_old;
+        v->slot_max = s->slot_max;
+        v->slot_width = s->slot_width;
+        v->slot_old_tag = s->slot_tag[o].p;
+        v->slot_old_val = s->slot_val[o].p;
+        v->slot_new_tag = s->slot_tag[1 - o].p;
+        v->slot_new_val = s->slot_val[1 - o].p;
+    }
     return SOIL_OK;
 }
 
@@ -894,6 +930,7 @@ int phase_force(soil_sys* s) {
         TRY(make_view(s, &v));
         int r = s->hook(&v, s->hook_user);
         if (r != 0) return fail(s->ctx, SOIL_ERR_INVALID, "force hook returned %d", r);
+        if (s->slot_max) s->slot_old = 1 - s->slot_old;  // this step's slots are next step's old
         return check_launch(s);
     }
     if (!builtin_consumer(s)) return SOIL_OK;
@@ -1148,6 +1185,7 @@ int soil_sys_destroy(soil_sys* s) {
     fr(s->cell_counts); fr(s->cell_start); fr(s->cell_cursor);
     fr(s->atom_cell); fr(s->sorted_atoms); fr(s->asi); fr(s->rowcount); fr(s->offsets); fr(s->indices);
     fr(s->row_slots); fr(s->sp); fr(s->spf);
+    for (int k = 0; k < 2; ++k) { fr(s->slot_tag[k]); fr(s->slot_val[k]); }
     fr(s->in_count); fr(s->in_start); fr(s->in_cursor); fr(s->in_list);
     fr(s->ghost_root); fr(s->ghost_chain);
     fr(s->fold_start); fr(s->fold_list);
@@ -1450,6 +1488,44 @@ int soil_sys_get_sort_perm(soil_sys* s, uint32_t* perm) {
     if (!s || !perm) return SOIL_ERR_INVALID;
     if (!s->perm_valid) return fail(s->ctx, SOIL_ERR_STATE, "no spatial sort has run");
     CK(cudaMemcpyAsync(perm, s->sort_perm.p, s->nlocal * 4, cudaMemcpyDeviceToHost, s->st));
+    return sync(s);
+}
+
+int soil_sys_enable_slots(soil_sys* s, uint32_t max_contacts, uint32_t width) {
+    if (!s) return SOIL_ERR_INVALID;
+    if (max_contacts == 0 || max_contacts > 1024 || width == 0 || width > 64)
+        return fail(s->ctx, SOIL_ERR_INVALID, "slots: max_contacts in [1, 1024], width in [1, 64]");
+    if (s->batch) return fail(s->ctx, SOIL_ERR_STATE, "slots are not available to a batched system");
+    if (s->slot_max) return fail(s->ctx, SOIL_ERR_STATE, "slots are already enabled");
+    s->slot_max = max_contacts;
+    s->slot_width = width;
+    s->slot_old = 0;
+    if (s->acap) {  // otherwise the arrays come with the first capacity (setup)
+        const int st = slots_grow(s, s->acap, 0);
+        if (st != SOIL_OK) {
+            for (int k = 0; k < 2; ++k) {
+                dev_free(s, s->slot_tag[k].p, s->slot_tag[k].cap * 4);
+                dev_free(s, s->slot_val[k].p, s->slot_val[k].cap * 8);
+                s->slot_tag[k] = {};
+                s->slot_val[k] = {};
+            }
+            s->slot_max = s->slot_width = 0;
+            return st;
+        }
+    }
+    return SOIL_OK;
+}
+
+int soil_sys_get_slots(soil_sys* s, uint32_t* partner_tag, double* payload) {
+    if (!s || !partner_tag || !payload) return SOIL_ERR_INVALID;
+    if (!s->slot_max) return fail(s->ctx, SOIL_ERR_STATE, "slots are not enabled");
+    const uint64_t nt = s->nlocal * s->slot_max;
+    const int o = s->slot_old;
+    if (nt) {
+        CK(cudaMemcpyAsync(partner_tag, s->slot_tag[o].p, nt * 4, cudaMemcpyDeviceToHost, s->st));
+        CK(cudaMemcpyAsync(payload, s->slot_val[o].p, nt * s->slot_width * 8,
+                           cudaMemcpyDeviceToHost, s->st));
+    }
     return sync(s);
 }
 

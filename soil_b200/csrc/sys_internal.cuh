@@ -110,6 +110,12 @@ struct soil_sys {
     DArr<uint32_t> cell_counts, cell_start, cell_cursor;
     DArr<uint32_t> atom_cell, sorted_atoms, asi, rowcount, offsets, indices, row_slots;
     DArr<double4> sp;
+    // persistent per-neighbor slots (slot_max == 0: disabled); buffer
+    // slot_old holds the slots the last hook call wrote
+    uint32_t slot_max = 0, slot_width = 0;
+    DArr<uint32_t> slot_tag[2];
+    DArr<double> slot_val[2];
+    int slot_old = 0;
     DArr<float4> spf;
     DArr<uint32_t> in_count, in_start, in_cursor, in_list;
     DArr<uint32_t> ghost_root, ghost_chain;
@@ -193,6 +199,7 @@ int ensure(soil_sys* s, DArr<T>& a, uint64_t need, uint64_t keep = 0, uint64_t r
 }
 
 int grow_atoms(soil_sys* s, uint64_t need, uint64_t keep);
+int slots_grow(soil_sys* s, uint64_t cap, uint64_t keep);
 // Room for arrays indexed by pair (CSR indices, incoming lists): pair counts
 // drift between rebuilds, so a new array takes twice the current count.
 inline uint64_t pair_room(uint64_t np) { return 2 * np + 1024; }

@@ -252,6 +252,23 @@ class System:
         self._c(self.lib.soil_sys_view(self.h, C.byref(v)), "view")
         return v
 
+    def enable_slots(self, max_contacts, width):
+        """Persistent per-neighbor slots for a force hook (soil_sys_enable_slots)."""
+        self._c(self.lib.soil_sys_enable_slots(self.h, max_contacts, width), "enable_slots")
+        self._slots = (max_contacts, width)
+
+    def slots(self):
+        """(partner tags [nlocal, max], payload [nlocal, max, width]) written by
+        the last hook call, rows in the current local order; empty slots have
+        tag 0xFFFFFFFF."""
+        m, w = getattr(self, "_slots", (1, 1))
+        n = self.counts().nlocal
+        tags = np.empty((n, m), np.uint32)
+        vals = np.empty((n, m, w))
+        self._c(self.lib.soil_sys_get_slots(self.h, _p(tags, C.c_uint32), _p(vals, C.c_double)),
+                "get_slots")
+        return tags, vals
+
 
 class Batch:
     """Many set-up systems stepped together (soil_batch_*): one launch per phase

@@ -61,6 +61,8 @@ int main(void) {
          offsetof(soil_counts, tilt_xy));
   printf("%zu %zu\n", offsetof(soil_dev_view, columns), offsetof(soil_dev_view, stream));
   printf("%zu %zu\n", offsetof(soil_dev_view, in_start), offsetof(soil_dev_view, fold_list));
+  printf("%zu %zu %zu\n", offsetof(soil_dev_view, ghost_root), offsetof(soil_dev_view, slot_width),
+         offsetof(soil_dev_view, slot_new_val));
   printf("%zu %zu %zu %zu\n", sizeof(soil_server_cfg), sizeof(soil_job_spec), sizeof(soil_job_info),
          sizeof(soil_server_stats));
   printf("%zu %zu %zu %zu\n", offsetof(soil_job_spec, natoms), offsetof(soil_job_spec, steps),
@@ -78,6 +80,8 @@ int main(void) {
             abi.SoilCounts.tilt_xy.offset,
             abi.SoilDevView.columns.offset, abi.SoilDevView.stream.offset,
             abi.SoilDevView.in_start.offset, abi.SoilDevView.fold_list.offset,
+            abi.SoilDevView.ghost_root.offset, abi.SoilDevView.slot_width.offset,
+            abi.SoilDevView.slot_new_val.offset,
             C.sizeof(abi.SoilServerCfg), C.sizeof(abi.SoilJobSpec), C.sizeof(abi.SoilJobInfo),
             C.sizeof(abi.SoilServerStats),
             abi.SoilJobSpec.natoms.offset, abi.SoilJobSpec.steps.offset,
