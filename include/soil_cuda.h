@@ -60,6 +60,12 @@ typedef enum soil_comm_state {
 #define SOIL_FILTER_FP64 0        /* every candidate tested in FP64 */
 #define SOIL_FILTER_FP32_RECHECK 1 /* FP32 reject test with margin, FP64 recheck of the rest */
 
+/* Orthogonal deform styles (DeformStyle, soil_deform/src/lib.rs:168-190). */
+#define SOIL_DEFORM_NONE 0
+#define SOIL_DEFORM_ERATE 1 /* L(t) = L0 (1 + rate dt step), about the centre */
+#define SOIL_DEFORM_VEL 2   /* L(t) = L0 + velocity dt step, about the centre */
+#define SOIL_DEFORM_FINAL 3 /* linear ramp of [lo, hi] to a target over a stage */
+
 /* Box: [lo, hi) per axis, all axes periodic (DomainConfig, domain.rs:43-78). */
 typedef struct soil_box {
     double lo[3];
@@ -208,6 +214,23 @@ int soil_sys_setup(soil_sys* sys);
 /* [deform] xy = { style = "erate", rate } — Lees–Edwards shear
  * (soil_deform/src/lib.rs:346-420 setup, 559-603 per step). */
 int soil_sys_set_shear(soil_sys* sys, double erate);
+
+/* [deform] x/y/z (dim 0/1/2) = { style, ... } — orthogonal box deformation,
+ * applied each step before the initial integration (apply_deform,
+ * soil_deform/src/lib.rs:468-557); the bounds at setup are the axis' L0.
+ *   SOIL_DEFORM_ERATE: a = rate;  SOIL_DEFORM_VEL: a = velocity;
+ *   SOIL_DEFORM_FINAL: a, b = target lo, hi; stage_steps = the length of the
+ *   run stage the ramp spans (the reference takes it from RunState).
+ * Every deforming step rebuilds the neighbor lists.  An axis that reaches
+ * zero size makes soil_step fail with SOIL_ERR_INVALID (the reference
+ * panics).  Before setup; not for batched systems. */
+int soil_sys_set_deform(soil_sys* sys, int32_t dim, int32_t style, double a, double b,
+                        uint64_t stage_steps);
+/* [deform] remap (default 1): scale local positions with the box about its
+ * centre (lib.rs:530-540). */
+int soil_sys_set_deform_remap(soil_sys* sys, int32_t remap);
+/* Domain bounds and tilt (xy, xz, yz) as they stand. */
+int soil_sys_get_box(soil_sys* sys, double lo[3], double hi[3], double tilt[3]);
 
 /* Built-in consumer: linear repulsion f = k*overlap along the pair normal
  * (docs/src/tutorial/write-your-own-physics.md:56-110) with the radius read

@@ -41,6 +41,11 @@ def lib():
                                         C.POINTER(pdbl)]),
             "orc_setup": (C.c_int, [P]),
             "orc_set_shear": (C.c_int, [P, C.c_double]),
+            "orc_set_deform": (C.c_int, [P, C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                         C.c_uint64]),
+            "orc_set_deform_remap": (C.c_int, [P, C.c_int32]),
+            "orc_get_box": (C.c_int, [P, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                      C.POINTER(C.c_double)]),
             "orc_set_harmonic": (C.c_int, [P, C.c_double, C.c_int32]),
             "orc_step": (C.c_int, [P, C.c_uint64]),
             "orc_phase": (C.c_int, [P, C.c_int]),
@@ -129,6 +134,21 @@ class OracleSystem:
 
     def set_harmonic(self, k, radius_col):
         self._L.orc_set_harmonic(self.h, k, radius_col)
+
+    def set_deform(self, dim, style, a=0.0, b=0.0, stage_steps=0):
+        assert self._L.orc_set_deform(self.h, dim, style, a, b, stage_steps) == 0
+
+    def set_deform_remap(self, remap):
+        self._L.orc_set_deform_remap(self.h, 1 if remap else 0)
+
+    def box(self):
+        lo, hi, tilt = np.zeros(3), np.zeros(3), np.zeros(3)
+        self._L.orc_get_box(self.h, _p(lo, C.c_double), _p(hi, C.c_double), _p(tilt, C.c_double))
+        return lo, hi, tilt
+
+    def try_step(self, n=1):
+        """Status of n steps (SOIL_ERR_INVALID when a deforming axis collapses)."""
+        return self._L.orc_step(self.h, n)
 
     def step(self, n=1):
         assert self._L.orc_step(self.h, n) == 0

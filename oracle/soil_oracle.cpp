@@ -120,7 +120,17 @@ struct Sys {
 
     State state = FULL_REBUILD;
 
-    // ---- DeformState (soil_deform/src/lib.rs:195-211), xy shear only ----
+    // ---- DeformState (soil_deform/src/lib.rs:195-211) ----
+    // per-axis style (AxisDeform, lib.rs:168-190): 0 none, 1 erate (a = rate),
+    // 2 vel (a = velocity), 3 final (a, b = target lo, hi; stage = the run
+    // stage's total steps, RunState cycle_count + cycle_remaining)
+    struct Axis {
+        int style = 0;
+        double a = 0.0, b = 0.0;
+        uint64_t stage = 0;
+        double lo_0 = 0.0, hi_0 = 0.0;
+    } axes[3];
+    bool remap = true;
     bool shear = false;
     double shear_rate = 0.0;
     bool shear_initialized = false;
@@ -334,9 +344,14 @@ struct Sys {
         pbc_flags[0] = pbc_flags[1] = pbc_flags[2] = true;
     }
 
-    // setup_deform, soil_deform/src/lib.rs:346-420 (xy shear only)
+    // setup_deform, soil_deform/src/lib.rs:346-420
     void setup_deform() {
         shear_initialized = false;
+        for (int d = 0; d < 3; ++d)
+            if (axes[d].style) {
+                axes[d].lo_0 = blo[d];
+                axes[d].hi_0 = bhi[d];
+            }
         deform_initialized = true;
         deform_step = 0;
     }
@@ -344,11 +359,62 @@ struct Sys {
     // ---------------------------------------------------------------------
     // Per-step systems
     // ---------------------------------------------------------------------
-    // apply_deform xy branch, soil_deform/src/lib.rs:435-604
-    void phase_deform() {
-        if (!deform_initialized || !shear) return;
+    // apply_deform, soil_deform/src/lib.rs:435-604: orthogonal axes (lib.rs:
+    // 468-557), then the xy shear.  Returns false when an axis collapses (the
+    // reference panics).
+    bool phase_deform() {
+        if (!deform_initialized || !(shear || axes[0].style || axes[1].style || axes[2].style))
+            return true;
         deform_step += 1;
         size_t nl = nlocal;
+        bool box_changed = false;
+        for (int dim = 0; dim < 3; ++dim) {
+            const Axis& ax = axes[dim];
+            if (!ax.style) continue;
+            double old_lo = blo[dim], old_hi = bhi[dim];
+            double old_size = old_hi - old_lo;
+            double l0 = ax.hi_0 - ax.lo_0;
+            double new_lo, new_hi;
+            if (ax.style == 1) {
+                double scale = 1.0 + ax.a * dt * (double)deform_step;
+                double new_l = l0 * scale;
+                double center = (ax.lo_0 + ax.hi_0) * 0.5;
+                new_lo = center - new_l * 0.5;
+                new_hi = center + new_l * 0.5;
+            } else if (ax.style == 2) {
+                double delta = ax.a * dt * (double)deform_step;
+                double new_l = l0 + delta;
+                double center = (ax.lo_0 + ax.hi_0) * 0.5;
+                new_lo = center - new_l * 0.5;
+                new_hi = center + new_l * 0.5;
+            } else {
+                double frac = ax.stage > 0 ? (double)deform_step / (double)ax.stage : 1.0;
+                frac = std::min(frac, 1.0);
+                new_lo = ax.lo_0 + (ax.a - ax.lo_0) * frac;
+                new_hi = ax.hi_0 + (ax.b - ax.hi_0) * frac;
+            }
+            double new_size = new_hi - new_lo;
+            if (new_size <= 0.0) return false;
+            if (remap && old_size > 0.0) {
+                double scale = new_size / old_size;
+                double new_center = (new_lo + new_hi) * 0.5;
+                double old_center = (old_lo + old_hi) * 0.5;
+                for (size_t i = 0; i < nl; ++i)
+                    pos[i][dim] = new_center + (pos[i][dim] - old_center) * scale;
+            }
+            blo[dim] = new_lo;
+            bhi[dim] = new_hi;
+            size[dim] = new_size;
+            sub_lo[dim] = new_lo;
+            sub_hi[dim] = new_hi;
+            sub_len[dim] = new_size;
+            box_changed = true;
+        }
+        if (box_changed) {
+            bounds_changed = true;
+            last_build_pos.clear();
+        }
+        if (!shear) return true;
         double rate = shear_rate;
         double lx = size[0], ly = size[1];
         double dv = rate * ly;
@@ -364,6 +430,7 @@ struct Sys {
         triclinic = true;
         bounds_changed = true;
         last_build_pos.clear();  // box_changed: force a rebuild (lib.rs:590-603)
+        return true;
     }
 
     // initial_integration, soil_verlet/src/lib.rs:131-162
@@ -837,8 +904,8 @@ struct Sys {
         }
     }
 
-    void step() {
-        phase_deform();            // PreInitialIntegration
+    bool step() {
+        if (!phase_deform()) return false;  // PreInitialIntegration
         phase_initial();           // InitialIntegration
         phase_decide_rebuild();    // PostInitialIntegration
         phase_remove_ghosts();
@@ -852,6 +919,7 @@ struct Sys {
         phase_reverse_comm();      // PostForce
         phase_final();             // FinalIntegration
         steps_done += 1;
+        return true;
     }
 };
 
@@ -935,6 +1003,31 @@ int orc_set_shear(void* h, double rate) {
     return SOIL_OK;
 }
 
+int orc_set_deform(void* h, int32_t dim, int32_t style, double a, double b, uint64_t stage) {
+    Sys* s = (Sys*)h;
+    if (dim < 0 || dim > 2 || style < 0 || style > 3) return SOIL_ERR_INVALID;
+    s->axes[dim].style = style;
+    s->axes[dim].a = a;
+    s->axes[dim].b = b;
+    s->axes[dim].stage = stage;
+    return SOIL_OK;
+}
+
+int orc_set_deform_remap(void* h, int32_t remap) {
+    ((Sys*)h)->remap = remap != 0;
+    return SOIL_OK;
+}
+
+int orc_get_box(void* h, double* lo, double* hi, double* tilt) {
+    Sys* s = (Sys*)h;
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = s->blo[d];
+        hi[d] = s->bhi[d];
+        tilt[d] = s->tilt[d];
+    }
+    return SOIL_OK;
+}
+
 int orc_set_harmonic(void* h, double k, int32_t radius_col) {
     Sys* s = (Sys*)h;
     s->harmonic_k = k;
@@ -945,7 +1038,8 @@ int orc_set_harmonic(void* h, double k, int32_t radius_col) {
 int orc_step(void* h, uint64_t nsteps) {
     Sys* s = (Sys*)h;
     if (!s->setup_done) return SOIL_ERR_STATE;
-    for (uint64_t k = 0; k < nsteps; ++k) s->step();
+    for (uint64_t k = 0; k < nsteps; ++k)
+        if (!s->step()) return SOIL_ERR_INVALID;  // a deforming axis collapsed
     return SOIL_OK;
 }
 
@@ -953,7 +1047,9 @@ int orc_step(void* h, uint64_t nsteps) {
 int orc_phase(void* h, int which) {
     Sys* s = (Sys*)h;
     switch (which) {
-        case 0: s->phase_deform(); break;
+        case 0:
+            if (!s->phase_deform()) return SOIL_ERR_INVALID;
+            break;
         case 1: s->phase_initial(); break;
         case 2: s->phase_decide_rebuild(); break;
         case 3: s->phase_remove_ghosts(); break;

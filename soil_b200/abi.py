@@ -34,6 +34,7 @@ SOIL_COL_REVERSE = 2
 SOIL_COL_ZERO = 4
 
 SOIL_FILTER_FP64 = 0
+SOIL_DEFORM_NONE, SOIL_DEFORM_ERATE, SOIL_DEFORM_VEL, SOIL_DEFORM_FINAL = range(4)
 SOIL_FILTER_FP32_RECHECK = 1
 
 
@@ -227,6 +228,10 @@ PROTOTYPES = {
     "soil_sys_get_sort_perm": (C.c_int, [P, pu32]),
     "soil_sys_view": (C.c_int, [P, C.POINTER(SoilDevView)]),
     "soil_sys_enable_slots": (C.c_int, [P, C.c_uint32, C.c_uint32]),
+    "soil_sys_set_deform": (C.c_int, [P, C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                      C.c_uint64]),
+    "soil_sys_set_deform_remap": (C.c_int, [P, C.c_int32]),
+    "soil_sys_get_box": (C.c_int, [P, pdbl, pdbl, pdbl]),
     "soil_sys_get_slots": (C.c_int, [P, pu32, pdbl]),
     "soil_bin_sort_noalloc": (C.c_int, [P, P, P, P, u64, pdbl, pdbl, pi32, pdbl, pdbl, pdbl, i32,
                                         P, P, P]),

@@ -1031,6 +1031,8 @@ int soil_batch_add(soil_batch* b, soil_sys* s) {
         return fail(b->ctx, SOIL_ERR_INVALID,
                     "a batched system uses the built-in harmonic consumer and no force hook");
     if (s->slot_max) return fail(b->ctx, SOIL_ERR_INVALID, "a batched system has no neighbor slots");
+    if (has_axis_deform(s))
+        return fail(b->ctx, SOIL_ERR_INVALID, "a batched system has no orthogonal deform");
     int zp[kMaxPlanes], nz;
     zero_planes_of(s, SOIL_COL_ZERO, zp, &nz);
     if (nz) return fail(b->ctx, SOIL_ERR_INVALID, "#[zero] columns are not supported in a batch");

@@ -149,6 +149,22 @@ void launch_shear_profile(cudaStream_t st, uint64_t n, const AtomCols& c, double
     k_shear_profile<<<grid_for(n), kBlock, 0, st>>>(n, c, rate, yc);
 }
 
+// apply_deform's remap (soil_deform/src/lib.rs:530-540), one dim after another
+__global__ void __launch_bounds__(kBlock) k_remap(uint64_t n, AtomCols c, RemapSpec r) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        for (int q = 0; q < r.n; ++q) {
+            double* x = r.dim[q] == 0 ? c.x : r.dim[q] == 1 ? c.y : c.z;
+            x[i] = r.new_center[q] + (x[i] - r.old_center[q]) * r.scale[q];
+        }
+}
+
+void launch_remap(cudaStream_t st, uint64_t n, const AtomCols& c, const RemapSpec& r) {
+    if (n == 0 || r.n == 0) return;
+    note_launch();
+    k_remap<<<grid_for(n), kBlock, 0, st>>>(n, c, r);
+}
+
 __global__ void __launch_bounds__(kBlock) k_save_pos(uint64_t n, AtomCols c, double* lbx,
                                                      double* lby, double* lbz) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;

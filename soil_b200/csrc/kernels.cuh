@@ -34,6 +34,15 @@ void launch_pbc(cudaStream_t st, uint64_t nlocal, const AtomCols& c, const Geom&
                 const double bvel[3]);
 // soil_deform first-step streaming profile vx += rate*(y - yc)
 void launch_shear_profile(cudaStream_t st, uint64_t n, const AtomCols& c, double rate, double yc);
+
+// Affine position remap of an orthogonal deform step: for each of the n
+// listed dims, x_d = new_center + (x_d - old_center) * scale.
+struct RemapSpec {
+    int n = 0;
+    int dim[3];
+    double old_center[3], new_center[3], scale[3];
+};
+void launch_remap(cudaStream_t st, uint64_t n, const AtomCols& c, const RemapSpec& r);
 // displacement_exceeded over [0, n) into flags->rebuild
 void launch_disp_check(cudaStream_t st, uint64_t n, const AtomCols& c, const double* lbx,
                        const double* lby, const double* lbz, double thr_sq, const double box[3],

@@ -434,15 +434,75 @@ bool builtin_consumer(const soil_sys* s) {
 // ---------------------------------------------------------------------------
 // apply_deform xy branch, soil_deform/src/lib.rs:435-604, host part.  Returns
 // true when the one-time streaming profile must be applied to the locals.
-bool deform_host(soil_sys* s) {
-    if (!s->deform_initialized || !s->shear) return false;
+bool has_axis_deform(const soil_sys* s) {
+    return s->axis[0].style || s->axis[1].style || s->axis[2].style;
+}
+
+// apply_deform (soil_deform/src/lib.rs:435-604) on the host state: the
+// orthogonal axes (lib.rs:468-557; the position remap is returned in r for
+// the device), then the xy shear.  *profile: the one-time streaming profile
+// is due this step.
+int deform_step(soil_sys* s, bool* profile, RemapSpec* r) {
+    *profile = false;
+    r->n = 0;
+    if (!s->deform_initialized || !(s->shear || has_axis_deform(s))) return SOIL_OK;
     s->deform_step += 1;
+    const uint64_t step = s->deform_step;
+    bool box_changed = false;
+    for (int dim = 0; dim < 3; ++dim) {
+        const soil_sys::AxisDeform& ax = s->axis[dim];
+        if (!ax.style) continue;
+        const double old_lo = s->blo[dim], old_hi = s->bhi[dim];
+        const double old_size = old_hi - old_lo;
+        const double l0 = ax.hi0 - ax.lo0;
+        double new_lo, new_hi;
+        if (ax.style == SOIL_DEFORM_ERATE) {
+            const double scale = 1.0 + ax.a * s->dt * (double)step;
+            const double new_l = l0 * scale;
+            const double center = (ax.lo0 + ax.hi0) * 0.5;
+            new_lo = center - new_l * 0.5;
+            new_hi = center + new_l * 0.5;
+        } else if (ax.style == SOIL_DEFORM_VEL) {
+            const double delta = ax.a * s->dt * (double)step;
+            const double new_l = l0 + delta;
+            const double center = (ax.lo0 + ax.hi0) * 0.5;
+            new_lo = center - new_l * 0.5;
+            new_hi = center + new_l * 0.5;
+        } else {
+            double frac = ax.stage_steps > 0 ? (double)step / (double)ax.stage_steps : 1.0;
+            frac = std::fmin(frac, 1.0);
+            new_lo = ax.lo0 + (ax.a - ax.lo0) * frac;
+            new_hi = ax.hi0 + (ax.b - ax.hi0) * frac;
+        }
+        const double new_size = new_hi - new_lo;
+        if (new_size <= 0.0)
+            return fail(s->ctx, SOIL_ERR_INVALID, "deform: axis %c collapsed at step %llu",
+                        "xyz"[dim], (unsigned long long)step);
+        if (s->remap && old_size > 0.0) {
+            const int q = r->n++;
+            r->dim[q] = dim;
+            r->scale[q] = new_size / old_size;
+            r->new_center[q] = (new_lo + new_hi) * 0.5;
+            r->old_center[q] = (old_lo + old_hi) * 0.5;
+        }
+        s->blo[dim] = new_lo;
+        s->bhi[dim] = new_hi;
+        s->size[dim] = new_size;
+        s->sub_lo[dim] = new_lo;
+        s->sub_hi[dim] = new_hi;
+        s->sub_len[dim] = new_size;
+        box_changed = true;
+    }
+    if (box_changed) {
+        s->bounds_changed = true;
+        s->last_build_n = 0;  // neighbor.last_build_pos.clear()
+    }
+    if (!s->shear) return SOIL_OK;
     const double rate = s->shear_rate;
     const double lx = s->size[0], ly = s->size[1];
     const double dv = rate * ly;
-    bool profile = false;
     if (!s->shear_initialized) {
-        profile = true;
+        *profile = true;
         s->shear_initialized = true;
     }
     const double raw = rate * s->dt * (double)s->deform_step * ly;
@@ -452,13 +512,26 @@ bool deform_host(soil_sys* s) {
     s->triclinic = true;
     s->bounds_changed = true;
     s->last_build_n = 0;  // neighbor.last_build_pos.clear()
+    return SOIL_OK;
+}
+
+// The shear-only form the batch engine uses (batched systems have no
+// orthogonal deform, so nothing can fail or need a remap).
+bool deform_host(soil_sys* s) {
+    bool profile = false;
+    RemapSpec r;
+    deform_step(s, &profile, &r);
     return profile;
 }
 
 double profile_center(const soil_sys* s) { return 0.5 * (s->blo[1] + s->bhi[1]); }
 
 int phase_deform(soil_sys* s) {
-    if (deform_host(s)) launch_shear_profile(s->st, s->nlocal, s->A, s->shear_rate, profile_center(s));
+    bool profile = false;
+    RemapSpec r;
+    TRY(deform_step(s, &profile, &r));
+    launch_remap(s->st, s->nlocal, s->A, r);  // before the profile, which reads y
+    if (profile) launch_shear_profile(s->st, s->nlocal, s->A, s->shear_rate, profile_center(s));
     return check_launch(s);
 }
 
@@ -1302,6 +1375,11 @@ int soil_sys_setup(soil_sys* s) {
         return fail(s->ctx, SOIL_ERR_CAPACITY, "bin grid of %llu cells is too large",
                     (unsigned long long)s->total_cells);
     // setup_deform (soil_deform/src/lib.rs:346-420)
+    for (int d = 0; d < 3; ++d)
+        if (s->axis[d].style) {
+            s->axis[d].lo0 = s->blo[d];
+            s->axis[d].hi0 = s->bhi[d];
+        }
     s->shear_initialized = false;
     s->deform_initialized = true;
     s->deform_step = 0;
@@ -1315,6 +1393,36 @@ int soil_sys_set_shear(soil_sys* s, double erate) {
     if (s->setup_done) return fail(s->ctx, SOIL_ERR_STATE, "set the shear rate before setup");
     s->shear = true;
     s->shear_rate = erate;
+    return SOIL_OK;
+}
+
+int soil_sys_set_deform(soil_sys* s, int32_t dim, int32_t style, double a, double b,
+                        uint64_t stage_steps) {
+    if (!s) return SOIL_ERR_INVALID;
+    if (dim < 0 || dim > 2 || style < SOIL_DEFORM_NONE || style > SOIL_DEFORM_FINAL)
+        return fail(s->ctx, SOIL_ERR_INVALID, "deform: dim in 0..2, style SOIL_DEFORM_*");
+    if (s->setup_done) return fail(s->ctx, SOIL_ERR_STATE, "set deform styles before setup");
+    soil_sys::AxisDeform& ax = s->axis[dim];
+    ax.style = style;
+    ax.a = a;
+    ax.b = b;
+    ax.stage_steps = stage_steps;
+    return SOIL_OK;
+}
+
+int soil_sys_set_deform_remap(soil_sys* s, int32_t remap) {
+    if (!s) return SOIL_ERR_INVALID;
+    s->remap = remap != 0;
+    return SOIL_OK;
+}
+
+int soil_sys_get_box(soil_sys* s, double* lo, double* hi, double* tilt) {
+    if (!s || !lo || !hi || !tilt) return SOIL_ERR_INVALID;
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = s->blo[d];
+        hi[d] = s->bhi[d];
+        tilt[d] = s->tilt[d];
+    }
     return SOIL_OK;
 }
 

@@ -90,6 +90,14 @@ struct soil_sys {
 
     // ---- deform / consumer ----
     bool shear = false, shear_initialized = false, deform_initialized = false;
+    // orthogonal deform per axis (style SOIL_DEFORM_*; lo0/hi0 set at setup)
+    struct AxisDeform {
+        int32_t style = 0;
+        double a = 0.0, b = 0.0;
+        uint64_t stage_steps = 0;
+        double lo0 = 0.0, hi0 = 0.0;
+    } axis[3];
+    bool remap = true;
     double shear_rate = 0.0;
     uint64_t deform_step = 0;
     double harmonic_k = 0.0;
@@ -205,6 +213,8 @@ int slots_grow(soil_sys* s, uint64_t cap, uint64_t keep);
 inline uint64_t pair_room(uint64_t np) { return 2 * np + 1024; }
 int update_colptrs(soil_sys* s);
 bool deform_host(soil_sys* s);
+int deform_step(soil_sys* s, bool* profile, RemapSpec* r);
+bool has_axis_deform(const soil_sys* s);
 double profile_center(const soil_sys* s);
 int sort_plan(soil_sys* s, bool* run, bool* periodic);
 void sort_done(soil_sys* s, bool apply, bool periodic);

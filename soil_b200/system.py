@@ -114,6 +114,20 @@ class System:
     def set_harmonic(self, k, radius_col):
         self._c(self.lib.soil_sys_set_harmonic(self.h, k, radius_col), "set_harmonic")
 
+    def set_deform(self, dim, style, a=0.0, b=0.0, stage_steps=0):
+        """Orthogonal deform of axis `dim` (abi.SOIL_DEFORM_*), before setup."""
+        self._c(self.lib.soil_sys_set_deform(self.h, dim, style, a, b, stage_steps), "set_deform")
+
+    def set_deform_remap(self, remap):
+        self._c(self.lib.soil_sys_set_deform_remap(self.h, 1 if remap else 0), "set_deform_remap")
+
+    def box(self):
+        """(lo[3], hi[3], tilt[3]) of the domain as it stands."""
+        lo, hi, tilt = np.zeros(3), np.zeros(3), np.zeros(3)
+        self._c(self.lib.soil_sys_get_box(self.h, _p(lo, C.c_double), _p(hi, C.c_double),
+                                          _p(tilt, C.c_double)), "get_box")
+        return lo, hi, tilt
+
     def set_force_hook(self, fn, user=None):
         """fn(view: SoilDevView, user) -> int, called once per step."""
         if fn is None:

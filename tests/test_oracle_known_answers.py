@@ -181,3 +181,96 @@ def test_shear_tilt_box_flip():
         raw = 30.0 * 1e-2 * step * L
         assert s.counts().tilt_xy == raw - L * round(raw / L)
         assert abs(s.counts().tilt_xy) <= 0.5 * L + 1e-12
+
+
+# ---- orthogonal deform (soil_deform/src/lib.rs:468-557, tests 640-960) ----
+
+def deform_sys(atoms, dt, box_hi=(1.0, 1.0, 1.0)):
+    b = abi.SoilBox()
+    for d in range(3):
+        b.lo[d] = 0.0
+        b.hi[d] = box_hi[d]
+    s = oracle.OracleSystem(b, W.default_cfg(), dt)
+    n = len(atoms)
+    s.add_atoms(list(range(n)), atoms, [[0.0, 0.0, 0.0]] * n, [1.0] * n, [0.1] * n)
+    return s
+
+
+def test_deform_erate_shrinks_box_symmetrically():
+    # lib.rs erate_shrinks_box_symmetrically: rate -1, dt 0.001, one step
+    s = deform_sys([[0.5, 0.5, 0.5]], 0.001)
+    s.set_deform(2, abi.SOIL_DEFORM_ERATE, -1.0)
+    s.setup()
+    s.phase("deform")
+    lo, hi, _ = s.box()
+    assert abs(lo[2] - 0.0005) < 1e-12 and abs(hi[2] - 0.9995) < 1e-12
+    assert abs((hi[2] - lo[2]) - 0.999) < 1e-12
+    assert abs(lo[0]) < 1e-12 and abs(hi[0] - 1.0) < 1e-12
+
+
+def test_deform_vel_expands_box():
+    # lib.rs vel_expands_box: velocity 1, dt 0.01 -> size 1.01
+    s = deform_sys([[0.5, 0.5, 0.5]], 0.01)
+    s.set_deform(0, abi.SOIL_DEFORM_VEL, 1.0)
+    s.setup()
+    s.phase("deform")
+    lo, hi, _ = s.box()
+    assert abs((hi[0] - lo[0]) - 1.01) < 1e-12
+
+
+def test_deform_final_ramps_to_target():
+    # lib.rs final_ramps_to_target: 10-step stage to [0.1, 0.9]
+    s = deform_sys([[0.5, 0.5, 0.5]], 0.001)
+    s.set_deform(1, abi.SOIL_DEFORM_FINAL, 0.1, 0.9, 10)
+    s.setup()
+    for _ in range(10):
+        s.phase("deform")
+    lo, hi, _ = s.box()
+    assert abs(lo[1] - 0.1) < 1e-10 and abs(hi[1] - 0.9) < 1e-10
+
+
+def test_deform_remap_scales_atom_positions():
+    # lib.rs remap_scales_atom_positions: the centre atom stays at the centre,
+    # x (not deformed) is untouched
+    s = deform_sys([[0.5, 0.5, 0.5], [0.75, 0.5, 0.75]], 0.001)
+    s.set_deform(2, abi.SOIL_DEFORM_ERATE, -1.0)
+    s.setup()
+    s.phase("deform")
+    lo, hi, _ = s.box()
+    p = s.atoms()["pos"]
+    assert abs(p[0, 2] - 0.5 * (lo[2] + hi[2])) < 1e-12
+    assert abs(p[0, 0] - 0.5) < 1e-12 and abs(p[1, 0] - 0.75) < 1e-12
+    # and the off-centre atom scales about the centre: 0.5 + 0.25 * 0.999
+    assert abs(p[1, 2] - (0.5 + 0.25 * 0.999)) < 1e-12
+
+
+def test_deform_without_remap_leaves_atoms_in_place():
+    # lib.rs no_remap_leaves_atoms_in_place
+    s = deform_sys([[0.5, 0.5, 0.5]], 0.001)
+    s.set_deform(2, abi.SOIL_DEFORM_ERATE, -1.0)
+    s.set_deform_remap(False)
+    s.setup()
+    s.phase("deform")
+    assert abs(s.atoms()["pos"][0, 2] - 0.5) < 1e-12
+
+
+def test_deform_axes_are_independent():
+    # lib.rs multiple_axes_deform_independently: x vel 1, z erate -0.5, dt 0.01
+    s = deform_sys([[0.5, 0.5, 0.5]], 0.01)
+    s.set_deform(0, abi.SOIL_DEFORM_VEL, 1.0)
+    s.set_deform(2, abi.SOIL_DEFORM_ERATE, -0.5)
+    s.setup()
+    s.phase("deform")
+    lo, hi, _ = s.box()
+    size = hi - lo
+    assert abs(size[0] - 1.01) < 1e-12 and abs(size[1] - 1.0) < 1e-12
+    assert abs(size[2] - 0.995) < 1e-12
+
+
+def test_deform_collapse_is_an_error():
+    # lib.rs apply_deform panics when an axis reaches zero size; here a status
+    s = deform_sys([[0.5, 0.5, 0.5]], 0.1)
+    s.set_deform(0, abi.SOIL_DEFORM_VEL, -5.0)  # 1 - 0.5 * step: zero at step 2
+    s.setup()
+    assert s._L.orc_phase(s.h, oracle.PHASE_INDEX["deform"]) == 0
+    assert s._L.orc_phase(s.h, oracle.PHASE_INDEX["deform"]) == abi.SOIL_ERR_INVALID
