@@ -60,6 +60,11 @@ typedef enum soil_comm_state {
 #define SOIL_FILTER_FP64 0        /* every candidate tested in FP64 */
 #define SOIL_FILTER_FP32_RECHECK 1 /* FP32 reject test with margin, FP64 recheck of the rest */
 
+/* BoundaryType per axis (domain.rs:36-44). */
+#define SOIL_BOUNDARY_PERIODIC 0
+#define SOIL_BOUNDARY_FIXED 1  /* atoms outside [lo, hi) are removed by pbc */
+#define SOIL_BOUNDARY_SHRINK 2 /* bounds follow the atoms' extent each step */
+
 /* Orthogonal deform styles (DeformStyle, soil_deform/src/lib.rs:168-190). */
 #define SOIL_DEFORM_NONE 0
 #define SOIL_DEFORM_ERATE 1 /* L(t) = L0 (1 + rate dt step), about the centre */
@@ -229,6 +234,20 @@ int soil_sys_set_deform(soil_sys* sys, int32_t dim, int32_t style, double a, dou
 /* [deform] remap (default 1): scale local positions with the box about its
  * centre (lib.rs:530-540). */
 int soil_sys_set_deform_remap(soil_sys* sys, int32_t remap);
+/* [domain] boundary_x/y/z (SOIL_BOUNDARY_*) and shrink_wrap_padding (0: the
+ * ghost cutoff), before setup (domain_read_input, domain.rs:460-498).  A
+ * non-periodic axis has no ghost images and no comm neighbor: its swaps still
+ * pack their face atoms (soil_sys_get_swap_sends) but receive nothing
+ * (comm.rs:253-283, 832-835); pbc removes atoms that leave it, last index
+ * first by swap-remove (domain.rs:641-662); the displacement check uses the
+ * general per-axis path (neighbor.rs:736-756).  Shrink-wrapped axes follow
+ * the locals' extent plus the padding every step (shrink_wrap_update,
+ * domain.rs:509-575).  Lees–Edwards shear needs all three axes periodic here;
+ * batched systems are periodic. */
+int soil_sys_set_boundary(soil_sys* sys, const int32_t type[3], double shrink_padding);
+/* Number of atoms swap s packed (its send_indices): recv_count for a swap
+ * with a neighbor, the face atoms for one without. */
+int soil_sys_get_swap_sends(soil_sys* sys, int32_t s, uint64_t* count);
 /* Domain bounds and tilt (xy, xz, yz) as they stand. */
 int soil_sys_get_box(soil_sys* sys, double lo[3], double hi[3], double tilt[3]);
 
@@ -253,6 +272,7 @@ int soil_phase_initial(soil_sys* sys);         /* initial_integration soil_verle
 int soil_phase_decide_rebuild(soil_sys* sys);  /* decide_rebuild     neighbor.rs:796-822 */
 int soil_phase_remove_ghosts(soil_sys* sys);   /* remove_ghost_atoms atom.rs:625-629 */
 int soil_phase_zero_forces(soil_sys* sys);     /* zero_all_forces    atom.rs:631-635 */
+int soil_phase_shrink_wrap(soil_sys* sys);     /* shrink_wrap        domain.rs:577-589 */
 int soil_phase_pbc(soil_sys* sys);             /* pbc / pbc_triclinic domain.rs:611-729 */
 int soil_phase_sort(soil_sys* sys);            /* sort_atoms_by_bin  neighbor.rs:834-997 */
 int soil_phase_borders(soil_sys* sys);         /* borders            comm.rs:682-860 */

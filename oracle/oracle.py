@@ -44,6 +44,8 @@ def lib():
             "orc_set_deform": (C.c_int, [P, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                          C.c_uint64]),
             "orc_set_deform_remap": (C.c_int, [P, C.c_int32]),
+            "orc_set_boundary": (C.c_int, [P, C.POINTER(C.c_int32), C.c_double]),
+            "orc_get_swap_sends": (C.c_int, [P, C.c_int32, C.POINTER(C.c_uint64)]),
             "orc_get_box": (C.c_int, [P, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                       C.POINTER(C.c_double)]),
             "orc_set_harmonic": (C.c_int, [P, C.c_double, C.c_int32]),
@@ -79,7 +81,7 @@ def _p(a, ct):
 PHASE_INDEX = {
     "deform": 0, "initial": 1, "decide_rebuild": 2, "remove_ghosts": 3, "zero_forces": 4,
     "pbc": 5, "sort": 6, "borders": 7, "forward_comm": 8, "neighbor": 9, "force": 10,
-    "reverse_comm": 11, "final": 12,
+    "reverse_comm": 11, "final": 12, "shrink_wrap": 13,
 }
 
 
@@ -137,6 +139,10 @@ class OracleSystem:
 
     def set_deform(self, dim, style, a=0.0, b=0.0, stage_steps=0):
         assert self._L.orc_set_deform(self.h, dim, style, a, b, stage_steps) == 0
+
+    def set_boundary(self, types, padding=0.0):
+        t = (C.c_int32 * 3)(*types)
+        assert self._L.orc_set_boundary(self.h, t, padding) == 0
 
     def set_deform_remap(self, remap):
         self._L.orc_set_deform_remap(self.h, 1 if remap else 0)
@@ -204,7 +210,9 @@ class OracleSystem:
             voff = np.zeros(3)
             self._L.orc_get_swap(self.h, s, C.byref(rs), C.byref(rc), _p(off, C.c_double),
                                  _p(voff, C.c_double), None)
-            send = np.zeros(rc.value, np.uint32)
+            ns = C.c_uint64()
+            self._L.orc_get_swap_sends(self.h, s, C.byref(ns))
+            send = np.zeros(ns.value, np.uint32)
             self._L.orc_get_swap(self.h, s, None, None, None, None, _p(send, C.c_uint32))
             out.append(dict(recv_start=rs.value, recv_count=rc.value, offset=off,
                             vel_offset=voff, send=send))

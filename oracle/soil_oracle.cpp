@@ -87,6 +87,10 @@ struct Sys {
     bool triclinic = false;
     bool bounds_changed = false;
     double domain_ghost_cutoff = 0.0;
+    // BoundaryType per axis (domain.rs:36-44): 0 periodic, 1 fixed, 2 shrink-wrap
+    int btype[3] = {0, 0, 0};
+    double shrink_wrap_padding = 0.0;
+    bool is_periodic(int d) const { return btype[d] == 0; }
 
     // ---- Neighbor (neighbor.rs:87-174) ----
     double skin_fraction = 1.0, bin_min_size = 1.0, additive_skin = 0.0;
@@ -213,12 +217,19 @@ struct Sys {
     // Setup
     // ---------------------------------------------------------------------
     // comm_setup, comm.rs:253-283 (rank 0 of a 1x1x1 grid, all axes periodic)
+    // comm_setup, comm.rs:253-283 (grid 1x1x1): a periodic axis sends to
+    // itself with a shift, a non-periodic one has no neighbor (-1)
     void comm_setup() {
         for (int dim = 0; dim < 3; ++dim) {
-            swap_directions[1][dim] = 0;
-            periodic_swap[1][dim] = -1.0;
-            swap_directions[0][dim] = 0;
-            periodic_swap[0][dim] = 1.0;
+            if (is_periodic(dim)) {
+                swap_directions[1][dim] = 0;
+                periodic_swap[1][dim] = -1.0;
+                swap_directions[0][dim] = 0;
+                periodic_swap[0][dim] = 1.0;
+            } else {
+                swap_directions[0][dim] = swap_directions[1][dim] = -1;
+                periodic_swap[0][dim] = periodic_swap[1][dim] = 0.0;
+            }
         }
     }
 
@@ -341,7 +352,7 @@ struct Sys {
         double required_bin = max_cutoff;
         if (bin_min_size < required_bin) bin_min_size = required_bin;
         compute_bin_grid();
-        pbc_flags[0] = pbc_flags[1] = pbc_flags[2] = true;
+        for (int d = 0; d < 3; ++d) pbc_flags[d] = is_periodic(d);  // neighbor.rs:656
     }
 
     // setup_deform, soil_deform/src/lib.rs:346-420
@@ -473,6 +484,20 @@ struct Sys {
         double threshold_sq = per_atom_skin * per_atom_skin;
         double bx = pbc_box[0], by = pbc_box[1], bz = pbc_box[2];
         size_t n = last_build_pos.size();
+        if (!(pbc_flags[0] && pbc_flags[1] && pbc_flags[2])) {
+            // general path, neighbor.rs:736-756: per-axis single-image correction
+            double hbx = bx * 0.5, hby = by * 0.5, hbz = bz * 0.5;
+            for (size_t idx = 0; idx < n; ++idx) {
+                double dx = pos[idx][0] - last_build_pos[idx][0];
+                double dy = pos[idx][1] - last_build_pos[idx][1];
+                double dz = pos[idx][2] - last_build_pos[idx][2];
+                if (pbc_flags[0]) { if (dx > hbx) dx -= bx; else if (dx < -hbx) dx += bx; }
+                if (pbc_flags[1]) { if (dy > hby) dy -= by; else if (dy < -hby) dy += by; }
+                if (pbc_flags[2]) { if (dz > hbz) dz -= bz; else if (dz < -hbz) dz += bz; }
+                if (dx * dx + dy * dy + dz * dz > threshold_sq) return true;
+            }
+            return false;
+        }
         double ibx = 1.0 / bx, iby = 1.0 / by, ibz = 1.0 / bz;
         for (size_t idx = 0; idx < n; ++idx) {
             const V3& p = pos[idx];
@@ -552,12 +577,93 @@ struct Sys {
             }
             return;
         }
-        for (size_t i = 0; i < nlocal; ++i)
+        if (is_periodic(0) && is_periodic(1) && is_periodic(2)) {
+            for (size_t i = 0; i < nlocal; ++i)
+                for (int d = 0; d < 3; ++d) {
+                    int32_t delta;
+                    pos[i][d] = wrap_periodic(pos[i][d], blo[d], size[d], &delta);
+                    image[i][d] += delta;
+                }
+            return;
+        }
+        // slow path (domain.rs:641-662): wrap periodic axes; remove atoms
+        // outside a non-periodic axis by swap_remove, last index first
+        size_t removed = 0;
+        for (size_t i = nlocal; i-- > 0;) {
             for (int d = 0; d < 3; ++d) {
-                int32_t delta;
-                pos[i][d] = wrap_periodic(pos[i][d], blo[d], size[d], &delta);
-                image[i][d] += delta;
+                if (is_periodic(d)) {
+                    int32_t delta;
+                    pos[i][d] = wrap_periodic(pos[i][d], blo[d], size[d], &delta);
+                    image[i][d] += delta;
+                } else if (pos[i][d] < blo[d] || pos[i][d] >= bhi[d]) {
+                    swap_remove(i);
+                    removed += 1;
+                    break;
+                }
             }
+        }
+        if (removed > 0) {
+            nlocal = (uint32_t)(nlocal - removed);
+            state = FULL_REBUILD;
+        }
+    }
+
+    // Atom::swap_remove (atom.rs:456-458) + registry swap_remove_all (268-272)
+    template <class T>
+    static void swap_remove_vec(std::vector<T>& v, size_t i) {
+        v[i] = v.back();
+        v.pop_back();
+    }
+    void swap_remove(size_t i) {
+        swap_remove_vec(tag, i); swap_remove_vec(atom_type, i); swap_remove_vec(origin_index, i);
+        swap_remove_vec(is_ghost, i); swap_remove_vec(pos, i); swap_remove_vec(vel, i);
+        swap_remove_vec(force, i); swap_remove_vec(cutoff_radius, i); swap_remove_vec(mass, i);
+        swap_remove_vec(inv_mass, i); swap_remove_vec(image, i);
+        for (auto& c : cols) {
+            const size_t w = (size_t)c.width, last = c.data.size() / w - 1;
+            for (size_t k = 0; k < w; ++k) c.data[i * w + k] = c.data[last * w + k];
+            c.data.resize(last * w);
+        }
+    }
+
+    // shrink_wrap_update, domain.rs:509-575 (every step, before pbc)
+    void phase_shrink_wrap() {
+        bool any = btype[0] == 2 || btype[1] == 2 || btype[2] == 2;
+        size_t nl = nlocal;
+        if (!any || nl == 0) return;
+        double padding;
+        if (shrink_wrap_padding > 0.0) padding = shrink_wrap_padding;
+        else if (domain_ghost_cutoff > 0.0) padding = domain_ghost_cutoff;
+        else {
+            double mx = std::max(size[0], std::max(size[1], size[2]));
+            padding = mx > 0.0 ? mx * 0.01 : 1.0;
+        }
+        bool changed = false;
+        for (int d = 0; d < 3; ++d) {
+            if (btype[d] != 2) continue;
+            double mn = DBL_MAX, mxp = -DBL_MAX;
+            for (size_t i = 0; i < nl; ++i) {
+                double p = pos[i][d];
+                if (p < mn) mn = p;
+                if (p > mxp) mxp = p;
+            }
+            double new_low = mn - padding, new_high = mxp + padding;
+            const double tol = 1e-12;
+            if (std::fabs(new_low - blo[d]) > tol || std::fabs(new_high - bhi[d]) > tol) {
+                blo[d] = new_low;
+                bhi[d] = new_high;
+                sub_lo[d] = new_low;
+                sub_hi[d] = new_high;
+                changed = true;
+            }
+        }
+        if (changed) {  // update_derived, domain.rs:171-177
+            for (int d = 0; d < 3; ++d) {
+                size[d] = bhi[d] - blo[d];
+                sub_len[d] = sub_hi[d] - sub_lo[d];
+            }
+            bounds_changed = true;
+        }
     }
 
     // cell of a position for the current grid (sort_atoms_by_bin 912-923,
@@ -627,7 +733,8 @@ struct Sys {
 
     // pack_border_atoms, comm.rs:288-358 (ghost_cutoff > 0 always here)
     void pack_border_atoms(int dim, int swap, const V3& change_pos, const V3& vel_offset,
-                           std::vector<size_t>& packed, size_t scan_end, double gc) {
+                           std::vector<size_t>& packed, size_t scan_end, double gc,
+                           bool self_send) {
         packed.clear();
         if (triclinic) {
             double lo_face = sub_lam_lo[dim], hi_face = sub_lam_hi[dim];
@@ -648,7 +755,9 @@ struct Sys {
             }
         }
         // self-send: pack_border (atom.rs:520-539 layout) then unpack_atom (539-553)
-        // and registry pack_all/unpack_all; appended in scan order.
+        // and registry pack_all/unpack_all; appended in scan order.  Without a
+        // neighbor (non-periodic axis, comm.rs:832-835) the packed atoms go nowhere.
+        if (!self_send) return;
         std::vector<size_t> src = packed;
         for (size_t i : src) {
             V3 p{pos[i][0] + change_pos[0], pos[i][1] + change_pos[1], pos[i][2] + change_pos[2]};
@@ -694,10 +803,11 @@ struct Sys {
                     if (swap_idx == swaps.size()) swaps.emplace_back();
                     Swap& e = swaps[swap_idx];
                     size_t recv_start = len();
+                    const bool self_send = to_proc == 0;
                     pack_border_atoms(dim, swap, pbc_shift, vel_shift, e.send_indices, dim_scan_end,
-                                      domain_ghost_cutoff);
+                                      domain_ghost_cutoff, self_send);
                     e.recv_start = recv_start;
-                    e.recv_count = e.send_indices.size();
+                    e.recv_count = self_send ? e.send_indices.size() : 0;
                     e.to_proc = to_proc;
                     e.from_proc = from_proc;
                     e.periodic_offset = pbc_shift;
@@ -714,6 +824,7 @@ struct Sys {
     void phase_forward_comm() {
         if (state != COMMUNICATE_ONLY) return;
         for (const Swap& s : swaps) {
+            if (s.to_proc < 0 || s.from_proc < 0) continue;  // no neighbor (comm.rs:460)
             // pack then unpack (forward_prepare_swap), swaps in recorded order
             size_t n = s.send_indices.size();
             std::vector<double> buf;
@@ -882,6 +993,7 @@ struct Sys {
             size_t start = end >= 2 ? end - 2 : 0;
             for (size_t s = start; s < end; ++s) {
                 const Swap& sw = swaps[s];
+                if (sw.to_proc < 0 || sw.from_proc < 0) continue;  // no neighbor (comm.rs:460)
                 std::vector<double> buf;  // pack_reverse_into: force then #[reverse] columns
                 for (size_t g = sw.recv_start; g < sw.recv_start + sw.recv_count; ++g) {
                     buf.push_back(force[g][0]); buf.push_back(force[g][1]); buf.push_back(force[g][2]);
@@ -910,7 +1022,8 @@ struct Sys {
         phase_decide_rebuild();    // PostInitialIntegration
         phase_remove_ghosts();
         phase_zero_forces();
-        phase_pbc();               // PreExchange
+        phase_shrink_wrap();       // PreExchange
+        phase_pbc();
         phase_sort();              // PreNeighbor
         phase_borders();
         phase_forward_comm();
@@ -1013,6 +1126,16 @@ int orc_set_deform(void* h, int32_t dim, int32_t style, double a, double b, uint
     return SOIL_OK;
 }
 
+int orc_set_boundary(void* h, const int32_t* type, double padding) {
+    Sys* s = (Sys*)h;
+    for (int d = 0; d < 3; ++d) {
+        if (type[d] < 0 || type[d] > 2) return SOIL_ERR_INVALID;
+        s->btype[d] = type[d];
+    }
+    s->shrink_wrap_padding = padding;
+    return SOIL_OK;
+}
+
 int orc_set_deform_remap(void* h, int32_t remap) {
     ((Sys*)h)->remap = remap != 0;
     return SOIL_OK;
@@ -1062,6 +1185,7 @@ int orc_phase(void* h, int which) {
         case 10: s->phase_force(); break;
         case 11: s->phase_reverse_comm(); break;
         case 12: s->phase_final(); s->steps_done += 1; break;
+        case 13: s->phase_shrink_wrap(); break;
         default: return SOIL_ERR_INVALID;
     }
     return SOIL_OK;
@@ -1123,6 +1247,13 @@ int orc_get_neighbor(void* h, uint32_t* offsets, uint32_t* indices) {
 int orc_num_offsets(void* h) { return (int)((Sys*)h)->neighbor_offsets.size(); }
 
 int orc_num_swaps(void* h) { return (int)((Sys*)h)->swaps.size(); }
+
+int orc_get_swap_sends(void* h, int32_t si, uint64_t* count) {
+    Sys* s = (Sys*)h;
+    if (si < 0 || (size_t)si >= s->swaps.size()) return SOIL_ERR_INVALID;
+    *count = s->swaps[si].send_indices.size();
+    return SOIL_OK;
+}
 
 int orc_get_swap(void* h, int32_t si, uint64_t* recv_start, uint64_t* recv_count, double* off,
                  double* voff, uint32_t* send) {

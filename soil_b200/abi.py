@@ -35,6 +35,7 @@ SOIL_COL_ZERO = 4
 
 SOIL_FILTER_FP64 = 0
 SOIL_DEFORM_NONE, SOIL_DEFORM_ERATE, SOIL_DEFORM_VEL, SOIL_DEFORM_FINAL = range(4)
+SOIL_BOUNDARY_PERIODIC, SOIL_BOUNDARY_FIXED, SOIL_BOUNDARY_SHRINK = range(3)
 SOIL_FILTER_FP32_RECHECK = 1
 
 
@@ -211,6 +212,7 @@ PROTOTYPES = {
     "soil_phase_decide_rebuild": (C.c_int, [P]),
     "soil_phase_remove_ghosts": (C.c_int, [P]),
     "soil_phase_zero_forces": (C.c_int, [P]),
+    "soil_phase_shrink_wrap": (C.c_int, [P]),
     "soil_phase_pbc": (C.c_int, [P]),
     "soil_phase_sort": (C.c_int, [P]),
     "soil_phase_borders": (C.c_int, [P]),
@@ -232,6 +234,8 @@ PROTOTYPES = {
                                       C.c_uint64]),
     "soil_sys_set_deform_remap": (C.c_int, [P, C.c_int32]),
     "soil_sys_get_box": (C.c_int, [P, pdbl, pdbl, pdbl]),
+    "soil_sys_set_boundary": (C.c_int, [P, pi32, C.c_double]),
+    "soil_sys_get_swap_sends": (C.c_int, [P, C.c_int32, pu64]),
     "soil_sys_get_slots": (C.c_int, [P, pu32, pdbl]),
     "soil_bin_sort_noalloc": (C.c_int, [P, P, P, P, u64, pdbl, pdbl, pi32, pdbl, pdbl, pdbl, i32,
                                         P, P, P]),

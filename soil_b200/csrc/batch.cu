@@ -1033,6 +1033,7 @@ int soil_batch_add(soil_batch* b, soil_sys* s) {
     if (s->slot_max) return fail(b->ctx, SOIL_ERR_INVALID, "a batched system has no neighbor slots");
     if (has_axis_deform(s))
         return fail(b->ctx, SOIL_ERR_INVALID, "a batched system has no orthogonal deform");
+    if (pbc_mask(s) != 7) return fail(b->ctx, SOIL_ERR_INVALID, "a batched system is periodic");
     int zp[kMaxPlanes], nz;
     zero_planes_of(s, SOIL_COL_ZERO, zp, &nz);
     if (nz) return fail(b->ctx, SOIL_ERR_INVALID, "#[zero] columns are not supported in a batch");

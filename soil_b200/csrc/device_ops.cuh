@@ -33,6 +33,21 @@ __device__ __forceinline__ bool moved_too_far(double px, double py, double pz, d
     return fma(dx, dx, fma(dy, dy, dz * dz)) > thr_sq;
 }
 
+// displacement_exceeded's general path (neighbor.rs:736-756) when some axis
+// is not periodic: per-axis single-image correction on periodic axes only.
+__device__ __forceinline__ bool moved_too_far_mixed(double px, double py, double pz, double qx,
+                                                    double qy, double qz, const double box[3],
+                                                    int mask, double thr_sq) {
+    double d[3] = {px - qx, py - qy, pz - qz};
+    for (int a = 0; a < 3; ++a) {
+        if (!(mask & (1 << a))) continue;
+        const double h = box[a] * 0.5;
+        if (d[a] > h) d[a] -= box[a];
+        else if (d[a] < -h) d[a] += box[a];
+    }
+    return d[0] * d[0] + d[1] * d[1] + d[2] * d[2] > thr_sq;
+}
+
 // wrap_periodic, domain.rs:594-605
 __device__ __forceinline__ double wrap1(double p, double low, double sz, int32_t& img) {
     const double high = low + sz;

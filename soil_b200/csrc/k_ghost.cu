@@ -96,6 +96,14 @@ const BorderCats& border_cats() {
     return t;
 }
 
+BorderCats border_cats_masked(unsigned periodic_swaps) {
+    BorderCats t = border_cats();
+    for (int k = 0; k < kBorderCats; ++k)
+        for (int q = 0; q < t.len[k]; ++q)
+            if (!(periodic_swaps & (1u << t.sw[k][q]))) t.need[k] = 0x80;  // no face bit 7
+    return t;
+}
+
 BorderPass border_pass(const BorderDim bds[3]) {
     BorderPass bp;
     bp.geom = bds[0].geom;
@@ -170,11 +178,10 @@ __global__ void __launch_bounds__(kBlock) k_border_images(
 }
 
 void launch_borders(cudaStream_t st, uint64_t nlocal, uint64_t cap, const AtomCols& c,
-                    const BorderPass& bp, uint8_t* face, uint32_t* counts, uint32_t* offs,
-                    uint32_t* bs, uint32_t* ghost_root, uint32_t* ghost_chain,
+                    const BorderCats& cats, const BorderPass& bp, uint8_t* face, uint32_t* counts,
+                    uint32_t* offs, uint32_t* bs, uint32_t* ghost_root, uint32_t* ghost_chain,
                     const SendPtrs& send, uint32_t* fold_start, uint32_t* fold_list) {
     if (nlocal == 0) return;
-    const BorderCats& cats = border_cats();
     const uint64_t nw = (nlocal + 31) / 32;
     const uint64_t nchunks = (nw + kScanChunk - 1) / kScanChunk;
     uint32_t* ctot = counts + (kBorderCats + 1) * nw;  // chunk totals, then prefixes

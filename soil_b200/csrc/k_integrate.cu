@@ -30,7 +30,16 @@ struct CheckArgs {
     double box[3];
     double ibox[3];
     DevFlags* flags;
+    int mask;  // periodic axes (7: fully periodic fast path)
 };
+
+__device__ __forceinline__ bool check_moved(const CheckArgs& ck, double x, double y, double z,
+                                            uint64_t i) {
+    if (ck.mask == 7)
+        return moved_too_far(x, y, z, ck.lbx[i], ck.lby[i], ck.lbz[i], ck.box, ck.ibox, ck.thr_sq);
+    return moved_too_far_mixed(x, y, z, ck.lbx[i], ck.lby[i], ck.lbz[i], ck.box, ck.mask,
+                               ck.thr_sq);
+}
 
 // initial_integration, soil_verlet/src/lib.rs:131-162:
 //   h = 0.5*dt*inv_m;  v += h*F;  x += v*dt
@@ -42,8 +51,7 @@ __global__ void __launch_bounds__(kBlock) k_initial(uint64_t n, AtomCols c, doub
          i += (uint64_t)gridDim.x * blockDim.x) {
         double x, y, z;
         initial_atom(c, i, dt, FUSE_FINAL, zero_force != 0, x, y, z);
-        if (i < ck.n_check)
-            hit |= moved_too_far(x, y, z, ck.lbx[i], ck.lby[i], ck.lbz[i], ck.box, ck.ibox, ck.thr_sq);
+        if (i < ck.n_check) hit |= check_moved(ck, x, y, z, i);
     }
     if (ck.flags) {
         unsigned any = __ballot_sync(0xffffffffu, hit);
@@ -53,8 +61,9 @@ __global__ void __launch_bounds__(kBlock) k_initial(uint64_t n, AtomCols c, doub
 
 static CheckArgs make_check(const double* lbx, const double* lby, const double* lbz,
                             uint64_t n_check, double thr_sq, const double box[3],
-                            DevFlags* flags) {
+                            DevFlags* flags, int mask) {
     CheckArgs ck;
+    ck.mask = mask;
     ck.lbx = lbx;
     ck.lby = lby;
     ck.lbz = lbz;
@@ -70,9 +79,9 @@ static CheckArgs make_check(const double* lbx, const double* lby, const double* 
 
 void launch_initial(cudaStream_t st, uint64_t n, const AtomCols& c, double dt, bool zero_force,
                     const double* lbx, const double* lby, const double* lbz, uint64_t n_check,
-                    double thr_sq, const double box[3], DevFlags* flags) {
+                    double thr_sq, const double box[3], DevFlags* flags, int pbc_mask) {
     if (n == 0) return;
-    CheckArgs ck = make_check(lbx, lby, lbz, n_check, thr_sq, box, flags);
+    CheckArgs ck = make_check(lbx, lby, lbz, n_check, thr_sq, box, flags, pbc_mask);
     note_launch();
     k_initial<false><<<grid_for(n), kBlock, 0, st>>>(n, c, dt, zero_force ? 1 : 0, ck);
 }
@@ -80,9 +89,9 @@ void launch_initial(cudaStream_t st, uint64_t n, const AtomCols& c, double dt, b
 void launch_final_initial(cudaStream_t st, uint64_t n, const AtomCols& c, double dt,
                           bool zero_force, const double* lbx, const double* lby,
                           const double* lbz, uint64_t n_check, double thr_sq,
-                          const double box[3], DevFlags* flags) {
+                          const double box[3], DevFlags* flags, int pbc_mask) {
     if (n == 0) return;
-    CheckArgs ck = make_check(lbx, lby, lbz, n_check, thr_sq, box, flags);
+    CheckArgs ck = make_check(lbx, lby, lbz, n_check, thr_sq, box, flags, pbc_mask);
     note_launch();
     k_initial<true><<<grid_for(n), kBlock, 0, st>>>(n, c, dt, zero_force ? 1 : 0, ck);
 }
@@ -191,17 +200,16 @@ __global__ void __launch_bounds__(kBlock) k_disp_check(uint64_t n, AtomCols c, C
     bool hit = false;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x)
-        hit |= moved_too_far(c.x[i], c.y[i], c.z[i], ck.lbx[i], ck.lby[i], ck.lbz[i], ck.box,
-                             ck.ibox, ck.thr_sq);
+        hit |= check_moved(ck, c.x[i], c.y[i], c.z[i], i);
     if (__ballot_sync(0xffffffffu, hit) && (threadIdx.x & 31) == 0)
         atomicOr(&ck.flags->rebuild, 1u);
 }
 
 void launch_disp_check(cudaStream_t st, uint64_t n, const AtomCols& c, const double* lbx,
                        const double* lby, const double* lbz, double thr_sq, const double box[3],
-                       DevFlags* flags) {
+                       DevFlags* flags, int pbc_mask) {
     if (n == 0) return;
-    CheckArgs ck = make_check(lbx, lby, lbz, n, thr_sq, box, flags);
+    CheckArgs ck = make_check(lbx, lby, lbz, n, thr_sq, box, flags, pbc_mask);
     note_launch();
     k_disp_check<<<grid_for(n), kBlock, 0, st>>>(n, c, ck);
 }

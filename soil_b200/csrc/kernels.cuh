@@ -16,16 +16,17 @@ uint64_t launches_so_far();
 
 // ---- integrate (k_integrate.cu) -------------------------------------------
 // initial_integration (+ optional fused force zeroing and displacement check)
+// pbc_mask: bit d set for a periodic axis d (7: the fully periodic test).
 void launch_initial(cudaStream_t st, uint64_t n, const AtomCols& c, double dt, bool zero_force,
                     const double* lbx, const double* lby, const double* lbz, uint64_t n_check,
-                    double thr_sq, const double box[3], DevFlags* flags);
+                    double thr_sq, const double box[3], DevFlags* flags, int pbc_mask = 7);
 // final_integration
 void launch_final(cudaStream_t st, uint64_t n, const AtomCols& c, double dt);
 // final_integration of step t fused with initial_integration of step t+1
 void launch_final_initial(cudaStream_t st, uint64_t n, const AtomCols& c, double dt,
                           bool zero_force, const double* lbx, const double* lby,
                           const double* lbz, uint64_t n_check, double thr_sq,
-                          const double box[3], DevFlags* flags);
+                          const double box[3], DevFlags* flags, int pbc_mask = 7);
 // zero_all_forces over [0, n) + the #[zero] planes
 void launch_zero_forces(cudaStream_t st, uint64_t n, const AtomCols& c, const int* zero_planes,
                         int nzero);
@@ -46,7 +47,27 @@ void launch_remap(cudaStream_t st, uint64_t n, const AtomCols& c, const RemapSpe
 // displacement_exceeded over [0, n) into flags->rebuild
 void launch_disp_check(cudaStream_t st, uint64_t n, const AtomCols& c, const double* lbx,
                        const double* lby, const double* lbz, double thr_sq, const double box[3],
-                       DevFlags* flags);
+                       DevFlags* flags, int pbc_mask = 7);
+
+// ---- non-periodic boundaries (k_bounds.cu) ---------------------------------
+struct BoundsArgs {
+    double lo[3], hi[3], size[3];
+    int periodic;  // bit d: axis d is periodic
+};
+// pbc with fixed axes: wrap periodic axes, gone[i] = 1 for atoms to remove
+void launch_pbc_bounded(cudaStream_t st, uint64_t n, const AtomCols& c, const BoundsArgs& b,
+                        uint32_t* gone);
+// flag[i] = x[i] < thresh (side 0) or x[i] >= thresh (side 1), i in [0, n)
+void launch_face_flag(cudaStream_t st, uint64_t n, const double* x, double thresh, int side,
+                      uint32_t* flag);
+// out[0..k) = the i with flag[i] != 0, ascending; pos[0..n] the exclusive
+// scan of flag (pos[n] = k); temp holds scan_temp_words(n) u32
+void launch_select(cudaStream_t st, uint64_t n, const uint32_t* flag, uint32_t* pos,
+                   uint32_t* temp, uint32_t* out);
+// ext[d] / ext[3 + d]: order keys of the min / max of x_d over [0, n), axes
+// in mask (ext preset to all ones / zeros)
+void launch_extent(cudaStream_t st, uint64_t n, const AtomCols& c, int mask,
+                   unsigned long long* ext);
 // host-layout conversions ([n][3] or [n][w] interleaved <-> SoA planes)
 void launch_deinterleave3(cudaStream_t st, uint64_t n, const double* src, double* a, double* b,
                           double* c);
@@ -142,6 +163,9 @@ struct BorderCats {
     uint8_t swap_ncat[kNumSwaps];
 };
 const BorderCats& border_cats();
+// The categories with every chain through a swap outside periodic_swaps (bit
+// s: swap s has a periodic neighbor) made empty: they never match a root.
+BorderCats border_cats_masked(unsigned periodic_swaps);
 BorderPass border_pass(const BorderDim bds[3]);
 struct SendPtrs {
     uint32_t* p[kNumSwaps];
@@ -151,8 +175,10 @@ struct SendPtrs {
 // image written from its root.  bs must be zero; ghosts beyond `cap` set
 // bs[10].  offs holds (kBorderCats + 1) * nw words and counts that plus
 // (kBorderCats + 1) * ceil(nw / 8192) (nw = ceil(nlocal / 32)).
+// cats: border_cats(), or border_cats_masked() for axes without periodicity
 void launch_borders(cudaStream_t st, uint64_t nlocal, uint64_t cap, const AtomCols& c,
-                    const BorderPass& bp, uint8_t* face, uint32_t* counts, uint32_t* offs,
+                    const BorderCats& cats, const BorderPass& bp, uint8_t* face, uint32_t* counts,
+                    uint32_t* offs,
                     uint32_t* bs, uint32_t* ghost_root, uint32_t* ghost_chain,
                     const SendPtrs& send, uint32_t* fold_start, uint32_t* fold_list);
 // forward_comm: every ghost from its root local atom through its swap chain

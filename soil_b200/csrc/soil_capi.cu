@@ -569,7 +569,7 @@ int phase_decide_rebuild(soil_sys* s) {
     if (displacement_needed(s)) {
         CK(cudaMemsetAsync(&s->dflags->rebuild, 0, 4, s->st));
         launch_disp_check(s->st, s->nlocal, s->A, s->lbx.p, s->lby.p, s->lbz.p,
-                          displacement_threshold_sq(s), s->pbc_box, s->dflags);
+                          displacement_threshold_sq(s), s->pbc_box, s->dflags, pbc_mask(s));
         TRY(check_launch(s));
         TRY(read_flags(s));
         disp = s->hflags->rebuild != 0;
@@ -592,10 +592,132 @@ int phase_zero_forces(soil_sys* s) {
     return check_launch(s);
 }
 
+int pbc_mask(const soil_sys* s) {
+    int m = 0;
+    for (int d = 0; d < 3; ++d)
+        if (s->btype[d] == SOIL_BOUNDARY_PERIODIC) m |= 1 << d;
+    return m;
+}
+
+// Scratch of the ordered selections (atom removal, send lists of swaps with
+// no neighbor), sized with the atom capacity.
+int select_arrays(soil_sys* s) {
+    TRY(ensure(s, s->sel_flag, s->acap + 1));
+    TRY(ensure(s, s->sel_pos, s->acap + 2));
+    TRY(ensure(s, s->sel_out, s->acap + 1));
+    TRY(ensure(s, s->sel_cnt, kNumSwaps + 1));
+    TRY(ensure(s, s->scan_tmp, scan_temp_words(s->acap + 2)));
+    return SOIL_OK;
+}
+
 int phase_pbc(soil_sys* s) {
     if (s->state != FULL_REBUILD) return SOIL_OK;
-    launch_pbc(s->st, s->nlocal, s->A, geom_of(s), s->bvel);
-    return check_launch(s);
+    const int mask = pbc_mask(s);
+    if (mask == 7 || s->nlocal == 0) {
+        launch_pbc(s->st, s->nlocal, s->A, geom_of(s), s->bvel);
+        return check_launch(s);
+    }
+    // slow path, domain.rs:641-662: wrap periodic axes, then remove the atoms
+    // outside a fixed axis by swap_remove from the last index down
+    TRY(select_arrays(s));
+    BoundsArgs b;
+    for (int d = 0; d < 3; ++d) {
+        b.lo[d] = s->blo[d];
+        b.hi[d] = s->bhi[d];
+        b.size[d] = s->size[d];
+    }
+    b.periodic = mask;
+    const uint64_t nl = s->nlocal;
+    launch_pbc_bounded(s->st, nl, s->A, b, s->sel_flag.p);
+    launch_select(s->st, nl, s->sel_flag.p, s->sel_pos.p, s->scan_tmp.p, s->sel_out.p);
+    TRY(check_launch(s));
+    CK(cudaMemcpyAsync(s->hword, s->sel_pos.p + nl, 4, cudaMemcpyDeviceToHost, s->st));
+    TRY(sync(s));
+    const uint64_t gone = s->hword[0];
+    if (gone == 0) return SOIL_OK;
+    std::vector<uint32_t> idx(gone);
+    CK(cudaMemcpyAsync(idx.data(), s->sel_out.p, gone * 4, cudaMemcpyDeviceToHost, s->st));
+    TRY(sync(s));
+    // the layout reverse-order swap_remove leaves: slot r takes the then-last atom
+    std::vector<uint32_t> at(nl);
+    for (uint64_t i = 0; i < nl; ++i) at[i] = (uint32_t)i;
+    uint64_t n = nl;
+    for (uint64_t k = gone; k-- > 0;) {
+        const uint64_t r = idx[k], last = n - 1;
+        if (r != last) at[r] = at[last];
+        n -= 1;
+    }
+    CK(cudaMemcpyAsync(s->sort_perm.p, at.data(), n * 4, cudaMemcpyHostToDevice, s->st));
+    launch_perm_gather(s->st, n, s->sort_perm.p, s->A, s->B);
+    if (s->slot_max) {
+        const int o = s->slot_old;
+        launch_slot_gather(s->st, n, s->sort_perm.p, s->slot_max, s->slot_width,
+                           s->slot_tag[o].p, s->slot_val[o].p, s->slot_tag[1 - o].p,
+                           s->slot_val[1 - o].p);
+        s->slot_old = 1 - o;
+    }
+    TRY(check_launch(s));
+    TRY(sync(s));  // the host copy of the permutation is released on return
+    std::swap(s->A, s->B);
+    s->colptrs_dirty = true;
+    s->perm_valid = false;
+    s->nlocal = n;
+    s->state = FULL_REBUILD;
+    return SOIL_OK;
+}
+
+// shrink_wrap (domain.rs:509-589): every step before pbc, shrink-wrapped
+// axes take the locals' extent plus the padding.
+int phase_shrink_wrap(soil_sys* s) {
+    int mask = 0;
+    for (int d = 0; d < 3; ++d)
+        if (s->btype[d] == SOIL_BOUNDARY_SHRINK) mask |= 1 << d;
+    if (!mask || s->nlocal == 0) return SOIL_OK;
+    double padding;
+    if (s->shrink_padding > 0.0) padding = s->shrink_padding;
+    else if (s->domain_ghost_cutoff > 0.0) padding = s->domain_ghost_cutoff;
+    else {
+        const double mx = std::fmax(s->size[0], std::fmax(s->size[1], s->size[2]));
+        padding = mx > 0.0 ? mx * 0.01 : 1.0;
+    }
+    TRY(ensure(s, s->ext, 6));
+    CK(cudaMemsetAsync(s->ext.p, 0xFF, 3 * 8, s->st));
+    CK(cudaMemsetAsync(s->ext.p + 3, 0, 3 * 8, s->st));
+    launch_extent(s->st, s->nlocal, s->A, mask, s->ext.p);
+    TRY(check_launch(s));
+    unsigned long long key[6];
+    static_assert(sizeof(key) <= kBorderStateWords * 4, "pinned word buffer too small");
+    CK(cudaMemcpyAsync(s->hword, s->ext.p, sizeof(key), cudaMemcpyDeviceToHost, s->st));
+    TRY(sync(s));
+    std::memcpy(key, s->hword, sizeof(key));
+    auto value = [](unsigned long long k) {
+        const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+        double v;
+        std::memcpy(&v, &b, 8);
+        return v;
+    };
+    bool changed = false;
+    for (int d = 0; d < 3; ++d) {
+        if (!(mask & (1 << d))) continue;
+        const double new_low = value(key[d]) - padding;
+        const double new_high = value(key[3 + d]) + padding;
+        const double tol = 1e-12;
+        if (std::fabs(new_low - s->blo[d]) > tol || std::fabs(new_high - s->bhi[d]) > tol) {
+            s->blo[d] = new_low;
+            s->bhi[d] = new_high;
+            s->sub_lo[d] = new_low;
+            s->sub_hi[d] = new_high;
+            changed = true;
+        }
+    }
+    if (changed) {  // update_derived, domain.rs:171-177
+        for (int d = 0; d < 3; ++d) {
+            s->size[d] = s->bhi[d] - s->blo[d];
+            s->sub_len[d] = s->sub_hi[d] - s->sub_lo[d];
+        }
+        s->bounds_changed = true;
+    }
+    return SOIL_OK;
 }
 
 // sort_atoms_by_bin (neighbor.rs:834-997), host part: grid recompute, sort
@@ -696,12 +818,17 @@ int phase_borders(soil_sys* s) {
     TRY(borders_reserve(s));
     uint32_t* hb = s->hword;
     const BorderPass bp = border_pass(bds);
+    const int mask = pbc_mask(s);
+    unsigned periodic_swaps = 0;
+    for (int d = 0; d < 3; ++d)
+        if (mask & (1 << d)) periodic_swaps |= 3u << (2 * d);
+    const BorderCats cats = mask == 7 ? border_cats() : border_cats_masked(periodic_swaps);
     for (int attempt = 0; attempt < 4; ++attempt) {
         TRY(borders_arrays(s));
         SendPtrs send;
         for (int k = 0; k < kNumSwaps; ++k) send.p[k] = s->send[k].p;
         CK(cudaMemsetAsync(s->bstate.p, 0, kBorderStateWords * 4, s->st));
-        launch_borders(s->st, s->nlocal, s->acap, s->A, bp, s->face_flags.p, s->bcount.p,
+        launch_borders(s->st, s->nlocal, s->acap, s->A, cats, bp, s->face_flags.p, s->bcount.p,
                        s->boff.p, s->bstate.p, s->ghost_root.p, s->ghost_chain.p, send,
                        s->fold_start.p, s->fold_list.p);
         TRY(check_launch(s));
@@ -711,7 +838,33 @@ int phase_borders(soil_sys* s) {
         if (attempt == 3) return fail(s->ctx, SOIL_ERR_CAPACITY, "ghost capacity did not converge");
         TRY(grow_atoms(s, (uint64_t)hb[3] + 1024, s->nlocal));  // hb[3]: atoms incl. all ghosts
     }
-    return borders_done(s, hb, bds);
+    TRY(borders_done(s, hb, bds));
+    if (mask == 7) return SOIL_OK;
+    // A swap with no neighbor (non-periodic axis) still packs the atoms at its
+    // face, scanning the locals and the ghosts of the earlier axes
+    // (pack_border_atoms, comm.rs:333-358), but nothing is received.
+    TRY(select_arrays(s));
+    const double* col[3] = {s->A.x, s->A.y, s->A.z};
+    for (int d = 0; d < 3; ++d) {
+        if (mask & (1 << d)) continue;
+        const uint64_t scan_end = s->swaps[2 * d].recv_start;  // atoms before this axis' swaps
+        for (int sw = 0; sw < 2; ++sw) {
+            const int k = 2 * d + sw;
+            launch_face_flag(s->st, scan_end, col[d], sw == 0 ? bds[d].thresh_lo : bds[d].thresh_hi,
+                             sw, s->sel_flag.p);
+            launch_select(s->st, scan_end, s->sel_flag.p, s->sel_pos.p, s->scan_tmp.p, s->send[k].p);
+            CK(cudaMemcpyAsync(s->sel_cnt.p + k, s->sel_pos.p + scan_end, 4, cudaMemcpyDeviceToDevice,
+                               s->st));
+        }
+    }
+    TRY(check_launch(s));
+    uint32_t cnt[kNumSwaps];
+    CK(cudaMemcpyAsync(cnt, s->sel_cnt.p, sizeof(cnt), cudaMemcpyDeviceToHost, s->st));
+    TRY(sync(s));
+    for (int d = 0; d < 3; ++d)
+        if (!(mask & (1 << d)))
+            for (int sw = 0; sw < 2; ++sw) s->swaps[2 * d + sw].send_count = cnt[2 * d + sw];
+    return SOIL_OK;
 }
 
 // Face thresholds and image shifts of the three border dims (comm.rs:288-358,
@@ -734,7 +887,8 @@ void border_setup(const soil_sys* s, BorderDim bds[3]) {
             bd.thresh_hi = s->sub_hi[dim] - gc;
         }
         for (int sw = 0; sw < 2; ++sw) {
-            const double po = sw == 0 ? 1.0 : -1.0;  // comm_setup periodic_swap (comm.rs:265-280)
+            // comm_setup periodic_swap (comm.rs:265-280): 0 without periodicity
+            const double po = s->btype[dim] != SOIL_BOUNDARY_PERIODIC ? 0.0 : sw == 0 ? 1.0 : -1.0;
             double* sh = bd.shift[sw];
             if (dim == 0) { sh[0] = po * s->size[0]; sh[1] = 0.0; sh[2] = 0.0; }
             else if (dim == 1) { sh[0] = po * s->tilt[0]; sh[1] = po * s->size[1]; sh[2] = 0.0; }
@@ -785,6 +939,7 @@ int borders_done(soil_sys* s, const uint32_t* hb, const BorderDim bds[3]) {
             SwapHost& h = s->swaps[2 * dim + sw];
             h.recv_start = sw == 0 ? recv_lo : recv_lo + n_lo;
             h.recv_count = sw == 0 ? n_lo : n_hi;
+            h.send_count = h.recv_count;
             for (int d = 0; d < 3; ++d) {
                 h.off[d] = bds[dim].shift[sw][d];
                 h.voff[d] = bds[dim].vshift[sw][d];
@@ -1053,11 +1208,11 @@ int full_step(soil_sys* s, bool last) {
     if (s->pending_final)
         launch_final_initial(s->st, s->nlocal, s->A, s->dt, fused_zero,
                              check ? s->lbx.p : nullptr, s->lby.p, s->lbz.p, s->nlocal,
-                             displacement_threshold_sq(s), s->pbc_box, s->dflags);
+                             displacement_threshold_sq(s), s->pbc_box, s->dflags, pbc_mask(s));
     else
         launch_initial(s->st, s->nlocal, s->A, s->dt, fused_zero, check ? s->lbx.p : nullptr,
                        s->lby.p, s->lbz.p, s->nlocal, displacement_threshold_sq(s), s->pbc_box,
-                       s->dflags);
+                       s->dflags, pbc_mask(s));
     s->pending_final = false;
     TRY(check_launch(s));
     timer_end(s, T_INTEGRATE);
@@ -1076,6 +1231,7 @@ int full_step(soil_sys* s, bool last) {
     if (!fused_zero && (nz > 0 || !overwrite)) TRY(phase_zero_forces(s));
     timer_end(s, T_ZERO);
     timer_begin(s, T_PBC);
+    TRY(phase_shrink_wrap(s));
     TRY(phase_pbc(s));
     timer_end(s, T_PBC);
     timer_begin(s, T_SORT);
@@ -1258,6 +1414,7 @@ int soil_sys_destroy(soil_sys* s) {
     fr(s->cell_counts); fr(s->cell_start); fr(s->cell_cursor);
     fr(s->atom_cell); fr(s->sorted_atoms); fr(s->asi); fr(s->rowcount); fr(s->offsets); fr(s->indices);
     fr(s->row_slots); fr(s->sp); fr(s->spf);
+    fr(s->sel_flag); fr(s->sel_pos); fr(s->sel_out); fr(s->sel_cnt); fr(s->ext);
     for (int k = 0; k < 2; ++k) { fr(s->slot_tag[k]); fr(s->slot_val[k]); }
     fr(s->in_count); fr(s->in_start); fr(s->in_cursor); fr(s->in_list);
     fr(s->ghost_root); fr(s->ghost_chain);
@@ -1374,6 +1531,10 @@ int soil_sys_setup(soil_sys* s) {
     if (s->total_cells >= 0x7fffffffull)
         return fail(s->ctx, SOIL_ERR_CAPACITY, "bin grid of %llu cells is too large",
                     (unsigned long long)s->total_cells);
+    if (s->shear && pbc_mask(s) != 7)
+        return fail(s->ctx, SOIL_ERR_INVALID,
+                    "Lees-Edwards shear needs periodic x and y (setup_deform, lib.rs:365-371); "
+                    "a non-periodic z under shear is not supported");
     // setup_deform (soil_deform/src/lib.rs:346-420)
     for (int d = 0; d < 3; ++d)
         if (s->axis[d].style) {
@@ -1480,6 +1641,7 @@ PHASE_ENTRY(initial)
 PHASE_ENTRY(decide_rebuild)
 PHASE_ENTRY(remove_ghosts)
 PHASE_ENTRY(zero_forces)
+PHASE_ENTRY(shrink_wrap)
 PHASE_ENTRY(pbc)
 PHASE_ENTRY(sort)
 PHASE_ENTRY(borders)
@@ -1587,9 +1749,26 @@ int soil_sys_get_swap(soil_sys* s, int32_t k, uint64_t* recv_start, uint64_t* re
         if (periodic_offset) periodic_offset[d] = h.off[d];
         if (vel_offset) vel_offset[d] = h.voff[d];
     }
-    if (send_indices && h.recv_count)
-        CK(cudaMemcpyAsync(send_indices, s->send[k].p, h.recv_count * 4, cudaMemcpyDeviceToHost, s->st));
+    if (send_indices && h.send_count)
+        CK(cudaMemcpyAsync(send_indices, s->send[k].p, h.send_count * 4, cudaMemcpyDeviceToHost, s->st));
     return sync(s);
+}
+
+int soil_sys_get_swap_sends(soil_sys* s, int32_t k, uint64_t* count) {
+    if (!s || !count || k < 0 || k >= s->nswaps) return SOIL_ERR_INVALID;
+    *count = s->swaps[k].send_count;
+    return SOIL_OK;
+}
+
+int soil_sys_set_boundary(soil_sys* s, const int32_t* type, double shrink_padding) {
+    if (!s || !type) return SOIL_ERR_INVALID;
+    for (int d = 0; d < 3; ++d)
+        if (type[d] < SOIL_BOUNDARY_PERIODIC || type[d] > SOIL_BOUNDARY_SHRINK)
+            return fail(s->ctx, SOIL_ERR_INVALID, "boundary type of axis %d: SOIL_BOUNDARY_*", d);
+    if (s->setup_done) return fail(s->ctx, SOIL_ERR_STATE, "set boundaries before setup");
+    for (int d = 0; d < 3; ++d) s->btype[d] = type[d];
+    s->shrink_padding = shrink_padding;
+    return SOIL_OK;
 }
 
 int soil_sys_get_sort_perm(soil_sys* s, uint32_t* perm) {

@@ -41,6 +41,7 @@ struct DArr {
 
 struct SwapHost {
     uint64_t recv_start = 0, recv_count = 0;
+    uint64_t send_count = 0;  // recv_count, or the packed atoms of a swap with no neighbor
     double off[3] = {0, 0, 0};
     double voff[3] = {0, 0, 0};
 };
@@ -98,6 +99,11 @@ struct soil_sys {
         double lo0 = 0.0, hi0 = 0.0;
     } axis[3];
     bool remap = true;
+    // BoundaryType per axis (SOIL_BOUNDARY_*) and the shrink-wrap padding
+    int32_t btype[3] = {SOIL_BOUNDARY_PERIODIC, SOIL_BOUNDARY_PERIODIC, SOIL_BOUNDARY_PERIODIC};
+    double shrink_padding = 0.0;
+    DArr<uint32_t> sel_flag, sel_pos, sel_out, sel_cnt;  // ordered selection scratch
+    DArr<unsigned long long> ext;                        // shrink-wrap extent keys
     double shear_rate = 0.0;
     uint64_t deform_step = 0;
     double harmonic_k = 0.0;
@@ -215,6 +221,7 @@ int update_colptrs(soil_sys* s);
 bool deform_host(soil_sys* s);
 int deform_step(soil_sys* s, bool* profile, RemapSpec* r);
 bool has_axis_deform(const soil_sys* s);
+int pbc_mask(const soil_sys* s);  // bit d: axis d periodic
 double profile_center(const soil_sys* s);
 int sort_plan(soil_sys* s, bool* run, bool* periodic);
 void sort_done(soil_sys* s, bool apply, bool periodic);

@@ -118,6 +118,11 @@ class System:
         """Orthogonal deform of axis `dim` (abi.SOIL_DEFORM_*), before setup."""
         self._c(self.lib.soil_sys_set_deform(self.h, dim, style, a, b, stage_steps), "set_deform")
 
+    def set_boundary(self, types, shrink_padding=0.0):
+        """Boundary type per axis (abi.SOIL_BOUNDARY_*), before setup."""
+        t = (C.c_int32 * 3)(*types)
+        self._c(self.lib.soil_sys_set_boundary(self.h, t, shrink_padding), "set_boundary")
+
     def set_deform_remap(self, remap):
         self._c(self.lib.soil_sys_set_deform_remap(self.h, 1 if remap else 0), "set_deform_remap")
 
@@ -210,7 +215,9 @@ class System:
             self._c(self.lib.soil_sys_get_swap(self.h, s, C.byref(rs), C.byref(rc),
                                                _p(off, C.c_double), _p(voff, C.c_double), None),
                     "get_swap")
-            send = np.zeros(rc.value, np.uint32)
+            ns = C.c_uint64()
+            self._c(self.lib.soil_sys_get_swap_sends(self.h, s, C.byref(ns)), "get_swap_sends")
+            send = np.zeros(ns.value, np.uint32)
             self._c(self.lib.soil_sys_get_swap(self.h, s, None, None, None, None,
                                                _p(send, C.c_uint32)), "get_swap")
             out.append(dict(recv_start=rs.value, recv_count=rc.value, offset=off,

@@ -274,3 +274,69 @@ def test_deform_collapse_is_an_error():
     s.setup()
     assert s._L.orc_phase(s.h, oracle.PHASE_INDEX["deform"]) == 0
     assert s._L.orc_phase(s.h, oracle.PHASE_INDEX["deform"]) == abi.SOIL_ERR_INVALID
+
+
+# ---- non-periodic boundaries (domain.rs:509-662, tests 880-990) ----
+
+def boundary_sys(atoms, hi, types, padding, cutoff=0.1, lo=(0.0, 0.0, 0.0)):
+    b = abi.SoilBox()
+    for d in range(3):
+        b.lo[d] = lo[d]
+        b.hi[d] = hi[d]
+    s = oracle.OracleSystem(b, W.default_cfg(), 0.001)
+    n = len(atoms)
+    s.add_atoms(list(range(n)), atoms, [[0.0, 0.0, 0.0]] * n, [1.0] * n, [cutoff] * n)
+    s.set_boundary(types, padding)
+    return s
+
+
+def test_shrink_wrap_expands_to_atom_positions():
+    # domain.rs shrink_wrap_expands_to_atom_positions: z -> [1 - 0.5, 8 + 0.5]
+    s = boundary_sys([[1.0, 2.0, 3.0], [5.0, 5.0, 8.0], [9.0, 1.0, 1.0]], (10.0, 10.0, 10.0),
+                     [0, 0, 2], 0.5)
+    s.phase("shrink_wrap")
+    lo, hi, _ = s.box()
+    assert abs(lo[2] - 0.5) < 1e-10 and abs(hi[2] - 8.5) < 1e-10
+    assert abs(lo[0]) < 1e-10 and abs(hi[0] - 10.0) < 1e-10
+
+
+def test_shrink_wrap_no_change_within_tolerance():
+    # domain.rs shrink_wrap_no_change_when_within_tolerance
+    s = boundary_sys([[1.0, 2.0, 3.0], [5.0, 5.0, 8.0], [9.0, 1.0, 1.0]], (10.0, 10.0, 8.5),
+                     [0, 0, 2], 0.5, lo=(0.0, 0.0, 0.5))
+    s.phase("shrink_wrap")
+    lo, hi, _ = s.box()
+    assert lo[2] == 0.5 and hi[2] == 8.5
+
+
+def test_shrink_wrap_all_axes():
+    # domain.rs shrink_wrap_all_axes: padding 1 around (10,20,30)-(50,60,70)
+    s = boundary_sys([[10.0, 20.0, 30.0], [50.0, 60.0, 70.0]], (100.0, 100.0, 100.0),
+                     [2, 2, 2], 1.0)
+    s.phase("shrink_wrap")
+    lo, hi, _ = s.box()
+    np.testing.assert_allclose(lo, [9.0, 19.0, 29.0], atol=1e-10)
+    np.testing.assert_allclose(hi, [51.0, 61.0, 71.0], atol=1e-10)
+
+
+def test_shrink_wrap_uses_ghost_cutoff_fallback():
+    # domain.rs shrink_wrap_uses_ghost_cutoff_fallback: padding 0 -> ghost cutoff
+    s = boundary_sys([[5.0, 5.0, 5.0]], (10.0, 10.0, 10.0), [0, 0, 2], 0.0)
+    s.setup()
+    gc = s.counts().ghost_cutoff
+    assert gc > 0.0
+    s.phase("shrink_wrap")
+    lo, hi, _ = s.box()
+    assert abs(lo[2] - (5.0 - gc)) < 1e-10 and abs(hi[2] - (5.0 + gc)) < 1e-10
+
+
+def test_pbc_removes_atoms_outside_a_fixed_axis_by_swap_remove():
+    # domain.rs:641-662: reverse scan with Vec::swap_remove.  Atoms 1 and 4 leave
+    # the fixed z range: removing 4 moves 5 into slot 4, removing 1 then moves
+    # the new last atom (5) into slot 1 -> tags [0, 5, 2, 3].
+    z = [1.0, 11.0, 3.0, 4.0, -0.5, 6.0]
+    s = boundary_sys([[1.0, 1.0, zi] for zi in z], (10.0, 10.0, 10.0), [0, 0, 1], 0.0)
+    s.phase("pbc")
+    a = s.atoms()
+    assert list(a["tag"]) == [0, 5, 2, 3]
+    assert s.counts().nlocal == 4
