@@ -242,7 +242,8 @@ int soil_sys_set_deform_remap(soil_sys* sys, int32_t remap);
  * first by swap-remove (domain.rs:641-662); the displacement check uses the
  * general per-axis path (neighbor.rs:736-756).  Shrink-wrapped axes follow
  * the locals' extent plus the padding every step (shrink_wrap_update,
- * domain.rs:509-575).  Lees–Edwards shear needs all three axes periodic here;
+ * domain.rs:509-575).  Lees–Edwards shear needs periodic x and y (a fixed or
+ * shrink-wrapped z works in lamda space, pbc_triclinic domain.rs:673-729);
  * batched systems are periodic. */
 int soil_sys_set_boundary(soil_sys* sys, const int32_t type[3], double shrink_padding);
 /* Number of atoms swap s packed (its send_indices): recv_count for a swap

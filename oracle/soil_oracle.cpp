@@ -558,14 +558,23 @@ struct Sys {
     // pbc, domain.rs:611-663 (fully periodic fast path) / pbc_triclinic 674-729
     void phase_pbc() {
         if (state != FULL_REBUILD) return;
-        if (triclinic) {
+        if (triclinic) {  // pbc_triclinic, domain.rs:673-729
+            size_t removed = 0;
             for (size_t ii = nlocal; ii-- > 0;) {
                 V3 lam = x2lamda(pos[ii]);
                 int32_t delta[3] = {0, 0, 0};
-                for (int d = 0; d < 3; ++d) {
-                    if (lam[d] < 0.0) { lam[d] += 1.0; delta[d] = -1; }
-                    else if (lam[d] >= 1.0) { lam[d] -= 1.0; delta[d] = 1; }
+                bool gone = false;
+                for (int d = 0; d < 3 && !gone; ++d) {
+                    if (is_periodic(d)) {
+                        if (lam[d] < 0.0) { lam[d] += 1.0; delta[d] = -1; }
+                        else if (lam[d] >= 1.0) { lam[d] -= 1.0; delta[d] = 1; }
+                    } else if (lam[d] < 0.0 || lam[d] >= 1.0) {
+                        swap_remove(ii);
+                        removed += 1;
+                        gone = true;
+                    }
                 }
+                if (gone) continue;
                 pos[ii] = lamda2x(lam);
                 for (int d = 0; d < 3; ++d) image[ii][d] += delta[d];
                 if (delta[1] != 0) {
@@ -574,6 +583,10 @@ struct Sys {
                     vel[ii][1] -= s * bvel[1];
                     vel[ii][2] -= s * bvel[2];
                 }
+            }
+            if (removed > 0) {
+                nlocal = (uint32_t)(nlocal - removed);
+                state = FULL_REBUILD;
             }
             return;
         }
@@ -1102,6 +1115,8 @@ int orc_add_atoms(void* h, uint64_t n, const uint32_t* tag, const uint32_t* type
 
 int orc_setup(void* h) {
     Sys* s = (Sys*)h;
+    // setup_deform panics on xy shear without periodic x and y (lib.rs:365-371)
+    if (s->shear && (!s->is_periodic(0) || !s->is_periodic(1))) return SOIL_ERR_INVALID;
     s->comm_setup();
     s->neighbor_setup();
     s->setup_deform();

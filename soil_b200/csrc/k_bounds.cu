@@ -29,27 +29,80 @@ __global__ void __launch_bounds__(kBlock) k_pbc_bounded(uint64_t n, AtomCols c, 
     }
 }
 
+// pbc_triclinic (domain.rs:673-729) with fixed axes: periodic axes wrap in
+// lamda space (with the Lees–Edwards velocity remap on a y crossing), an atom
+// outside [0, 1) of a fixed axis is flagged; kept atoms are rewritten from
+// lamda as in the all-periodic path.
+__global__ void __launch_bounds__(kBlock) k_pbc_bounded_tri(uint64_t n, AtomCols c, Geom g,
+                                                            int periodic, double bv0, double bv1,
+                                                            double bv2, uint32_t* out) {
+    const uint64_t cap = c.cap;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        double l[3];
+        x2lamda(g, c.x[i], c.y[i], c.z[i], l[0], l[1], l[2]);
+        int32_t dl[3] = {0, 0, 0};
+        uint32_t gone = 0;
+        for (int d = 0; d < 3 && !gone; ++d) {
+            if (periodic & (1 << d)) {
+                if (l[d] < 0.0) { l[d] += 1.0; dl[d] = -1; }
+                else if (l[d] >= 1.0) { l[d] -= 1.0; dl[d] = 1; }
+            } else if (l[d] < 0.0 || l[d] >= 1.0) {
+                gone = 1;
+            }
+        }
+        out[i] = gone;
+        if (gone) continue;
+        double rx, ry, rz;
+        lamda2x(g, l[0], l[1], l[2], rx, ry, rz);
+        c.x[i] = rx;
+        c.y[i] = ry;
+        c.z[i] = rz;
+        for (int d = 0; d < 3; ++d) c.img[d * cap + i] += dl[d];
+        if (dl[1] != 0) {
+            const double s = (double)dl[1];
+            c.vx[i] = c.vx[i] - s * bv0;
+            c.vy[i] = c.vy[i] - s * bv1;
+            c.vz[i] = c.vz[i] - s * bv2;
+        }
+    }
+}
+
 void launch_pbc_bounded(cudaStream_t st, uint64_t n, const AtomCols& c, const BoundsArgs& b,
                         uint32_t* gone) {
     if (n == 0) return;
     note_launch();
-    k_pbc_bounded<<<grid_for(n), kBlock, 0, st>>>(n, c, b, gone);
+    if (b.geom.triclinic)
+        k_pbc_bounded_tri<<<grid_for(n), kBlock, 0, st>>>(n, c, b.geom, b.periodic, b.bvel[0],
+                                                          b.bvel[1], b.bvel[2], gone);
+    else
+        k_pbc_bounded<<<grid_for(n), kBlock, 0, st>>>(n, c, b, gone);
 }
 
-// pack_border_atoms' face test (comm.rs:333-358, orthogonal): flag[i] for
-// atoms [0, n) at the low (side 0: x_d < thresh) or high (x_d >= thresh) face.
-__global__ void __launch_bounds__(kBlock) k_face_flag(uint64_t n, const double* x, double thresh,
-                                                      int side, uint32_t* flag) {
+// pack_border_atoms' face test (comm.rs:305-358): flag[i] for atoms [0, n) at
+// the low (side 0: v < thresh) or high (v >= thresh) face of axis dim, with v
+// the coordinate, or its lamda value when the box is triclinic.
+__global__ void __launch_bounds__(kBlock) k_face_flag(uint64_t n, AtomCols c, Geom g, int dim,
+                                                      double thresh, int side, uint32_t* flag) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-         i += (uint64_t)gridDim.x * blockDim.x)
-        flag[i] = side == 0 ? (x[i] < thresh) : (x[i] >= thresh);
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        double v;
+        if (g.triclinic) {
+            double l0, l1, l2;
+            x2lamda(g, c.x[i], c.y[i], c.z[i], l0, l1, l2);
+            v = dim == 0 ? l0 : dim == 1 ? l1 : l2;
+        } else {
+            v = dim == 0 ? c.x[i] : dim == 1 ? c.y[i] : c.z[i];
+        }
+        flag[i] = side == 0 ? (v < thresh) : (v >= thresh);
+    }
 }
 
-void launch_face_flag(cudaStream_t st, uint64_t n, const double* x, double thresh, int side,
-                      uint32_t* flag) {
+void launch_face_flag(cudaStream_t st, uint64_t n, const AtomCols& c, const Geom& g, int dim,
+                      double thresh, int side, uint32_t* flag) {
     if (n == 0) return;
     note_launch();
-    k_face_flag<<<grid_for(n), kBlock, 0, st>>>(n, x, thresh, side, flag);
+    k_face_flag<<<grid_for(n), kBlock, 0, st>>>(n, c, g, dim, thresh, side, flag);
 }
 
 __global__ void __launch_bounds__(kBlock) k_scatter_selected(uint64_t n, const uint32_t* flag,

@@ -53,13 +53,16 @@ void launch_disp_check(cudaStream_t st, uint64_t n, const AtomCols& c, const dou
 struct BoundsArgs {
     double lo[3], hi[3], size[3];
     int periodic;  // bit d: axis d is periodic
+    Geom geom;     // triclinic boxes wrap and test in lamda space
+    double bvel[3];
 };
 // pbc with fixed axes: wrap periodic axes, gone[i] = 1 for atoms to remove
 void launch_pbc_bounded(cudaStream_t st, uint64_t n, const AtomCols& c, const BoundsArgs& b,
                         uint32_t* gone);
-// flag[i] = x[i] < thresh (side 0) or x[i] >= thresh (side 1), i in [0, n)
-void launch_face_flag(cudaStream_t st, uint64_t n, const double* x, double thresh, int side,
-                      uint32_t* flag);
+// flag[i] = v < thresh (side 0) or v >= thresh (side 1), i in [0, n), v the
+// dim coordinate (lamda when triclinic)
+void launch_face_flag(cudaStream_t st, uint64_t n, const AtomCols& c, const Geom& g, int dim,
+                      double thresh, int side, uint32_t* flag);
 // out[0..k) = the i with flag[i] != 0, ascending; pos[0..n] the exclusive
 // scan of flag (pos[n] = k); temp holds scan_temp_words(n) u32
 void launch_select(cudaStream_t st, uint64_t n, const uint32_t* flag, uint32_t* pos,

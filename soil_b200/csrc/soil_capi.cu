@@ -627,6 +627,8 @@ int phase_pbc(soil_sys* s) {
         b.size[d] = s->size[d];
     }
     b.periodic = mask;
+    b.geom = geom_of(s);
+    for (int d = 0; d < 3; ++d) b.bvel[d] = s->bvel[d];
     const uint64_t nl = s->nlocal;
     launch_pbc_bounded(s->st, nl, s->A, b, s->sel_flag.p);
     launch_select(s->st, nl, s->sel_flag.p, s->sel_pos.p, s->scan_tmp.p, s->sel_out.p);
@@ -844,14 +846,13 @@ int phase_borders(soil_sys* s) {
     // face, scanning the locals and the ghosts of the earlier axes
     // (pack_border_atoms, comm.rs:333-358), but nothing is received.
     TRY(select_arrays(s));
-    const double* col[3] = {s->A.x, s->A.y, s->A.z};
     for (int d = 0; d < 3; ++d) {
         if (mask & (1 << d)) continue;
         const uint64_t scan_end = s->swaps[2 * d].recv_start;  // atoms before this axis' swaps
         for (int sw = 0; sw < 2; ++sw) {
             const int k = 2 * d + sw;
-            launch_face_flag(s->st, scan_end, col[d], sw == 0 ? bds[d].thresh_lo : bds[d].thresh_hi,
-                             sw, s->sel_flag.p);
+            launch_face_flag(s->st, scan_end, s->A, bds[d].geom, d,
+                             sw == 0 ? bds[d].thresh_lo : bds[d].thresh_hi, sw, s->sel_flag.p);
             launch_select(s->st, scan_end, s->sel_flag.p, s->sel_pos.p, s->scan_tmp.p, s->send[k].p);
             CK(cudaMemcpyAsync(s->sel_cnt.p + k, s->sel_pos.p + scan_end, 4, cudaMemcpyDeviceToDevice,
                                s->st));
@@ -1531,10 +1532,9 @@ int soil_sys_setup(soil_sys* s) {
     if (s->total_cells >= 0x7fffffffull)
         return fail(s->ctx, SOIL_ERR_CAPACITY, "bin grid of %llu cells is too large",
                     (unsigned long long)s->total_cells);
-    if (s->shear && pbc_mask(s) != 7)
+    if (s->shear && (pbc_mask(s) & 3) != 3)
         return fail(s->ctx, SOIL_ERR_INVALID,
-                    "Lees-Edwards shear needs periodic x and y (setup_deform, lib.rs:365-371); "
-                    "a non-periodic z under shear is not supported");
+                    "Lees-Edwards shear needs periodic x and y (setup_deform, lib.rs:365-371)");
     // setup_deform (soil_deform/src/lib.rs:346-420)
     for (int d = 0; d < 3; ++d)
         if (s->axis[d].style) {

@@ -16,12 +16,15 @@ pytestmark = pytest.mark.gpu
 P, F, S = abi.SOIL_BOUNDARY_PERIODIC, abi.SOIL_BOUNDARY_FIXED, abi.SOIL_BOUNDARY_SHRINK
 
 CASES = {
-    # name: (types, padding, velocity scale, newton)
-    "fixed-z": ([P, P, F], 0.0, 25.0, 1),
-    "fixed-xyz": ([F, F, F], 0.0, 25.0, 1),
-    "shrink-z": ([P, P, S], 0.0, 3.0, 1),
-    "shrink-xy-padded": ([S, S, P], 0.7, 3.0, 1),
-    "fixed-x-shrink-z-newton-off": ([F, P, S], 0.0, 10.0, 0),
+    # name: (types, padding, velocity scale, newton, shear rate)
+    "fixed-z": ([P, P, F], 0.0, 25.0, 1, 0.0),
+    "fixed-xyz": ([F, F, F], 0.0, 25.0, 1, 0.0),
+    "shrink-z": ([P, P, S], 0.0, 3.0, 1, 0.0),
+    "shrink-xy-padded": ([S, S, P], 0.7, 3.0, 1, 0.0),
+    "fixed-x-shrink-z-newton-off": ([F, P, S], 0.0, 10.0, 0, 0.0),
+    # Lees-Edwards shear with walls in z: triclinic wrap and lamda face tests
+    "sheared-fixed-z": ([P, P, F], 0.0, 25.0, 1, 2.0),
+    "sheared-shrink-z": ([P, P, S], 0.5, 3.0, 1, 2.0),
 }
 
 
@@ -32,6 +35,8 @@ def _pair(ctx, w, types, padding):
         rc = s.register_column("radius", 1, abi.SOIL_COL_FORWARD)
         s.add_atoms(w.tag, w.pos, w.vel, w.mass, w.cutoff, columns=[w.radius])
         s.set_harmonic(w.harmonic_k, rc)
+        if w.shear_rate:
+            s.set_shear(w.shear_rate)
         s.set_boundary(types, padding)
         s.setup()
     return g, o
@@ -39,8 +44,8 @@ def _pair(ctx, w, types, padding):
 
 @pytest.mark.parametrize("name", list(CASES))
 def test_boundaries_match_oracle(ctx, name):
-    types, padding, vscale, newton = CASES[name]
-    w = W.poly("bounds", 41, 3000, 0.4, 1e-3, 40, harmonic_k=1e3)
+    types, padding, vscale, newton, shear = CASES[name]
+    w = W.poly("bounds", 41, 3000, 0.4, 1e-3, 40, harmonic_k=1e3, shear_rate=shear)
     w.vel *= vscale
     w.cfg.newton = newton
     g, o = _pair(ctx, w, types, padding)
@@ -62,8 +67,8 @@ def test_boundaries_match_oracle(ctx, name):
     c = g.counts()
     if F in types:
         assert c.nlocal < w.n, "no atom left through a fixed face"
-    if S in types:
-        assert c.rebuilds >= 40  # the bounds move every step
+    if S in types or shear:
+        assert c.rebuilds >= 40  # the bounds or the tilt move every step
     g.close()
 
 
