@@ -89,3 +89,17 @@ def test_boundary_refusals(ctx):
     with pytest.raises(abi.SoilError):
         s.set_boundary([P, P, F])  # after setup
     s.close()
+
+
+def test_every_atom_leaves_a_fixed_box(ctx):
+    """Atoms fast enough to leave a fully fixed box within a few steps: the
+    system empties exactly as the oracle's, and keeps stepping with no atoms."""
+    w = W.mono("escape", 43, 200, 0.2, 1e-2, 30)
+    w.vel *= 200.0
+    g, o = _pair(ctx, w, [F, F, F], 0.0)
+    for k in (3, 7, 20):
+        g.step(k)
+        o.step(k)
+        assert_same_state(g, o, f"escape +{k}")
+    assert g.counts().nlocal == 0 and g.counts().nghost == 0
+    g.close()
