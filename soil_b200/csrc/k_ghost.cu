@@ -235,6 +235,48 @@ __global__ void __launch_bounds__(kBlock) k_reverse_fold(uint64_t nlocal, const 
         fold_root(c, nlocal, t, start, list, rev);
 }
 
+// Only the roots with images: after a border pass most locals have none, and
+// a pass over all of them is a scan of fold_start for a few percent of work.
+__global__ void __launch_bounds__(kBlock) k_reverse_fold_roots(uint64_t nlocal,
+                                                               const uint32_t* count,
+                                                               const uint32_t* roots,
+                                                               const uint32_t* start,
+                                                               const uint32_t* list, AtomCols c,
+                                                               PlaneList rev) {
+    const uint64_t n = *count;
+    for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < n;
+         q += (uint64_t)gridDim.x * blockDim.x)
+        fold_root(c, nlocal, roots[q], start, list, rev);
+}
+
+void launch_reverse_fold_roots(cudaStream_t st, uint64_t nlocal, uint64_t max_roots,
+                               const uint32_t* count, const uint32_t* roots,
+                               const uint32_t* start, const uint32_t* list, const AtomCols& c,
+                               const int* rev_planes, int nrev) {
+    if (max_roots == 0) return;
+    PlaneList pl;
+    pl.n = nrev;
+    for (int k = 0; k < nrev; ++k) pl.idx[k] = rev_planes[k];
+    note_launch();
+    k_reverse_fold_roots<<<grid_for(max_roots), kBlock, 0, st>>>(nlocal, count, roots, start, list,
+                                                                 c, pl);
+}
+
+__global__ void __launch_bounds__(kBlock) k_fold_root_flags(uint64_t nlocal,
+                                                            const uint32_t* fold_start,
+                                                            uint32_t* flag) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nlocal;
+         t += (uint64_t)gridDim.x * blockDim.x)
+        flag[t] = fold_start[t + 1] != fold_start[t] ? 1u : 0u;
+}
+
+void launch_fold_root_flags(cudaStream_t st, uint64_t nlocal, const uint32_t* fold_start,
+                            uint32_t* flag) {
+    if (nlocal == 0) return;
+    note_launch();
+    k_fold_root_flags<<<grid_for(nlocal), kBlock, 0, st>>>(nlocal, fold_start, flag);
+}
+
 void launch_reverse_fold(cudaStream_t st, uint64_t nlocal, const uint32_t* start,
                          const uint32_t* list, const AtomCols& c, const int* rev_planes, int nrev) {
     if (nlocal == 0) return;

@@ -192,6 +192,15 @@ void launch_forward(cudaStream_t st, uint64_t nlocal, uint64_t nghost, const Ato
 // root's image tree in fold order
 void launch_reverse_fold(cudaStream_t st, uint64_t nlocal, const uint32_t* start,
                          const uint32_t* list, const AtomCols& c, const int* rev_planes, int nrev);
+// The same fold over the roots that have images only: roots[0 .. *count)
+// (count read on the device, at most max_roots)
+void launch_reverse_fold_roots(cudaStream_t st, uint64_t nlocal, uint64_t max_roots,
+                               const uint32_t* count, const uint32_t* roots,
+                               const uint32_t* start, const uint32_t* list, const AtomCols& c,
+                               const int* rev_planes, int nrev);
+// flag[t] = local t has images (fold_start[t + 1] != fold_start[t]), t < nlocal
+void launch_fold_root_flags(cudaStream_t st, uint64_t nlocal, const uint32_t* fold_start,
+                            uint32_t* flag);
 
 // ---- neighbor (k_neighbor.cu) ---------------------------------------------
 struct PairParams {

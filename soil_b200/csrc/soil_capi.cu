@@ -162,6 +162,17 @@ int update_colptrs(soil_sys* s) {
     return SOIL_OK;
 }
 
+// Scratch of the ordered selections (atom removal, send lists of swaps with
+// no neighbor, the reverse-comm root list), sized with the atom capacity.
+int select_arrays(soil_sys* s) {
+    TRY(ensure(s, s->sel_flag, s->acap + 1));
+    TRY(ensure(s, s->sel_pos, s->acap + 2));
+    TRY(ensure(s, s->sel_out, s->acap + 1));
+    TRY(ensure(s, s->sel_cnt, kNumSwaps + 1));
+    TRY(ensure(s, s->scan_tmp, scan_temp_words(s->acap + 2)));
+    return SOIL_OK;
+}
+
 // Capacity for `need` atoms (locals + ghosts); the first `keep` survive.
 int grow_atoms(soil_sys* s, uint64_t need, uint64_t keep) {
     if (need <= s->acap && s->A.x) return SOIL_OK;
@@ -194,6 +205,11 @@ int grow_atoms(soil_sys* s, uint64_t need, uint64_t keep) {
     TRY(ensure(s, s->sorted_local_cell, ncap,
                s->sorted_local_cell.p ? std::min(keep, s->sorted_local_cell.cap) : 0));
     TRY(slots_grow(s, ncap, keep));
+    // ordered-selection scratch and the reverse-comm root list, so that no
+    // later phase allocates
+    TRY(select_arrays(s));
+    TRY(ensure(s, s->fold_roots, ncap + 1));
+    TRY(ensure(s, s->fold_nroots, 1));
     s->colptrs_dirty = true;
     return SOIL_OK;
 }
@@ -599,14 +615,18 @@ int pbc_mask(const soil_sys* s) {
     return m;
 }
 
-// Scratch of the ordered selections (atom removal, send lists of swaps with
-// no neighbor), sized with the atom capacity.
-int select_arrays(soil_sys* s) {
-    TRY(ensure(s, s->sel_flag, s->acap + 1));
-    TRY(ensure(s, s->sel_pos, s->acap + 2));
-    TRY(ensure(s, s->sel_out, s->acap + 1));
-    TRY(ensure(s, s->sel_cnt, kNumSwaps + 1));
-    TRY(ensure(s, s->scan_tmp, scan_temp_words(s->acap + 2)));
+// The locals with ghost images, in order, from the fold program of a border
+// pass; their count stays on the device (reverse comm reads it there).
+int fold_roots_build(soil_sys* s) {
+    TRY(select_arrays(s));
+    TRY(ensure(s, s->fold_roots, s->acap + 1));
+    TRY(ensure(s, s->fold_nroots, 1));
+    const uint64_t nl = s->nlocal;
+    launch_fold_root_flags(s->st, nl, s->fold_start.p, s->sel_flag.p);
+    launch_select(s->st, nl, s->sel_flag.p, s->sel_pos.p, s->scan_tmp.p, s->fold_roots.p);
+    CK(cudaMemcpyAsync(s->fold_nroots.p, s->sel_pos.p + nl, 4, cudaMemcpyDeviceToDevice, s->st));
+    TRY(check_launch(s));
+    s->fold_roots_gen = s->border_gen;
     return SOIL_OK;
 }
 
@@ -949,6 +969,7 @@ int borders_done(soil_sys* s, const uint32_t* hb, const BorderDim bds[3]) {
     }
     s->nghost = (uint64_t)hb[3] - s->nlocal;
     s->last_nghost = s->nghost;
+    s->border_gen += 1;
     s->nswaps = kNumSwaps;
     return SOIL_OK;
 }
@@ -1171,12 +1192,23 @@ int phase_force(soil_sys* s) {
 }
 
 int phase_reverse_comm(soil_sys* s) {
-    // reverse_send_force, comm.rs:938-1024: rounds last to first, lo then hi
+    // reverse_send_force, comm.rs:938-1024: rounds last to first, lo then hi;
+    // each root's image tree in fold order, over the roots that have images
     if (!s->newton) return SOIL_OK;
     if (s->nswaps == 0 || s->nghost == 0) return SOIL_OK;
     int rp[kMaxPlanes], nr;
     zero_planes_of(s, SOIL_COL_REVERSE, rp, &nr);
-    launch_reverse_fold(s->st, s->nlocal, s->fold_start.p, s->fold_list.p, s->A, rp, nr);
+    // A border pass folded once (every-step rebuilds) walks every local's fold
+    // program; from its second fold on, the list of the locals that have
+    // images is built once and walked instead.
+    if (s->fold_roots_gen != s->border_gen && s->reverse_gen == s->border_gen)
+        TRY(fold_roots_build(s));
+    if (s->fold_roots_gen == s->border_gen)
+        launch_reverse_fold_roots(s->st, s->nlocal, s->nghost, s->fold_nroots.p, s->fold_roots.p,
+                                  s->fold_start.p, s->fold_list.p, s->A, rp, nr);
+    else
+        launch_reverse_fold(s->st, s->nlocal, s->fold_start.p, s->fold_list.p, s->A, rp, nr);
+    s->reverse_gen = s->border_gen;
     return check_launch(s);
 }
 
@@ -1416,6 +1448,7 @@ int soil_sys_destroy(soil_sys* s) {
     fr(s->atom_cell); fr(s->sorted_atoms); fr(s->asi); fr(s->rowcount); fr(s->offsets); fr(s->indices);
     fr(s->row_slots); fr(s->sp); fr(s->spf);
     fr(s->sel_flag); fr(s->sel_pos); fr(s->sel_out); fr(s->sel_cnt); fr(s->ext);
+    fr(s->fold_roots); fr(s->fold_nroots);
     for (int k = 0; k < 2; ++k) { fr(s->slot_tag[k]); fr(s->slot_val[k]); }
     fr(s->in_count); fr(s->in_start); fr(s->in_cursor); fr(s->in_list);
     fr(s->ghost_root); fr(s->ghost_chain);

@@ -104,6 +104,10 @@ struct soil_sys {
     double shrink_padding = 0.0;
     DArr<uint32_t> sel_flag, sel_pos, sel_out, sel_cnt;  // ordered selection scratch
     DArr<unsigned long long> ext;                        // shrink-wrap extent keys
+    DArr<uint32_t> fold_roots, fold_nroots;  // locals with images (reverse comm), their count
+    // border passes so far, the pass fold_roots belongs to, and the pass the
+    // last reverse comm folded
+    uint64_t border_gen = 0, fold_roots_gen = ~0ull, reverse_gen = ~0ull;
     double shear_rate = 0.0;
     uint64_t deform_step = 0;
     double harmonic_k = 0.0;
