@@ -102,6 +102,25 @@ def test_triclinic_pbc_wraps_and_remaps_velocity():
     assert a["image"][0, 1] == 1
 
 
+def test_triclinic_pbc_removes_atoms_outside_a_fixed_axis():
+    # pbc_triclinic (domain.rs:673-729): "Non-periodic axes fall back to
+    # out-of-bounds removal" - the reference test's tilted box with z fixed:
+    # atom 1 leaves through z and is swap-removed (atom 2 takes its slot);
+    # atom 0 still wraps across y with the tilt and the velocity jump.
+    s = tilted(1.2, 5.0)
+    s.add_atoms([0, 1, 2], [[2.0, 3.03, 1.0], [1.0, 1.0, 2.5], [3.0, 2.0, 0.5]],
+                [[7.0, 0.0, 0.0], [0.0, 0.0, 0.0], [0.0, 0.0, 0.0]], [1.0] * 3, [0.1] * 3)
+    s.set_boundary([0, 0, 1], 0.0)
+    s.set_domain_tilt(1.2, 5.0, True)
+    s.set_state(abi.SOIL_FULL_REBUILD)
+    s.phase("pbc")
+    a = s.atoms()
+    assert list(a["tag"]) == [0, 2]
+    assert abs(a["pos"][0, 1] - 0.03) < 1e-9 and abs(a["pos"][0, 0] - 0.8) < 1e-9
+    assert abs(a["vel"][0, 0] - 2.0) < 1e-12 and a["image"][0, 1] == 1
+    assert s.counts().nlocal == 2
+
+
 def binned_pairs(s, n):
     off, idx = s.neighbor()
     out = set()
