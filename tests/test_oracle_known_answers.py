@@ -68,6 +68,37 @@ def test_free_fall_parabola_and_pinned_atom():
     assert abs(a["vel"][0, 2] - (5.0 + g * t)) < 1e-9
 
 
+def spring_run(k, x0, dt, n):
+    """The oracle's initial/final phases with a host spring force F = -k x
+    between them (the loop of soil_verlet/src/lib.rs:251-267)."""
+    s = one_atom_sys([x0, 0.0, 0.0], [0.0, 0.0, 0.0], dt, box=100.0, lo=-50.0)
+    x = x0
+    for _ in range(n):
+        s.set_atom_state(0, force=[-k * x, 0.0, 0.0])
+        s.phase("initial")
+        x = s.atoms()["pos"][0, 0]
+        s.set_atom_state(0, force=[-k * x, 0.0, 0.0])
+        s.phase("final")
+    a = s.atoms()
+    return a["pos"][0, 0], a["vel"][0, 0]
+
+
+def test_velocity_verlet_second_order_convergence():
+    # soil_verlet/src/lib.rs:242-304: error ratio ~4 per halving of dt
+    errs = [abs(spring_run(1.0, 1.0, dt, int(round(1.0 / dt)))[0] - math.cos(1.0))
+            for dt in (0.01, 0.005, 0.0025)]
+    for a, b in zip(errs, errs[1:]):
+        assert 3.5 < a / b < 4.5, errs
+
+
+def test_velocity_verlet_energy_conservation_harmonic():
+    # soil_verlet/src/lib.rs:306-333: k = 100, 10,000 steps of 1e-4, drift < 1e-6
+    k, x0 = 100.0, 0.1
+    x, v = spring_run(k, x0, 1e-4, 10000)
+    e0 = 0.5 * k * x0 * x0
+    assert abs(0.5 * k * x * x + 0.5 * v * v - e0) / e0 < 1e-6
+
+
 def tilted(xy=1.2, bvel=0.0):
     b = abi.SoilBox()
     for d, L in enumerate((4.0, 3.0, 2.0)):
