@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from helpers import assert_same_lists, assert_same_state, pair
-from soil_b200 import abi, workloads as W
+from soil_b200 import abi, system, workloads as W
 
 pytestmark = pytest.mark.gpu
 
@@ -118,3 +118,24 @@ def test_single_atom_and_empty_rows(ctx):
     o.step(10)
     assert_same_state(g, o)
     assert_same_lists(g, o)
+
+
+def test_empty_system_steps_like_the_oracle(ctx):
+    """No atoms at all: setup, steps (each a rebuild, as the reference's
+    needs_rebuild says for nlocal == 0) and readbacks work and match."""
+    import oracle as orc
+    b = W.make_box(10.0)
+    g = system.System(ctx, b, W.default_cfg(), 1e-3)
+    o = orc.OracleSystem(b, W.default_cfg(), 1e-3)
+    for s in (g, o):
+        rc = s.register_column("radius", 1, abi.SOIL_COL_FORWARD)
+        s.add_atoms(np.zeros(0, np.uint32), np.zeros((0, 3)), np.zeros((0, 3)), np.zeros(0),
+                    np.zeros(0), columns=[np.zeros(0)])
+        s.set_harmonic(1e3, rc)
+        s.setup()
+        s.step(2)
+        s.step(3)
+    assert_same_state(g, o, "empty")
+    assert_same_lists(g, o, "empty")
+    assert g.counts().nlocal == 0 and g.counts().step == 5
+    g.close()
