@@ -182,6 +182,9 @@ typedef struct soil_batch soil_batch;
 int soil_abi_version(void);
 /* Create a context on CUDA device `device`; hbm_budget_bytes = 0 means no cap. */
 int soil_ctx_create(int device, uint64_t hbm_budget_bytes, soil_ctx** out);
+/* Destroy the systems, batches and servers of a context before the context:
+ * their device memory comes from the context's stream-ordered pool, which is
+ * released here (memory still allocated from it is returned when freed). */
 int soil_ctx_destroy(soil_ctx* ctx);
 const char* soil_last_error(const soil_ctx* ctx);
 /* Device bytes currently held by all systems of the context. */
