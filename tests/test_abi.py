@@ -92,3 +92,32 @@ int main(void) {
 def test_missing_library_raises(tmp_path):
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         abi.load_library(str(tmp_path / "nope.so"))
+
+
+def test_consumer_headers_compile_for_sm100a(tmp_path):
+    """include/soil_consumer.cuh and include/soil_slots.cuh are what an external
+    force hook includes: they compile on their own (and together) for sm_100a,
+    and so do the example hooks under tests/hooks."""
+    src = tmp_path / "hook.cu"
+    src.write_text(r'''
+#include "soil_consumer.cuh"
+#include "soil_slots.cuh"
+__global__ void k(soil_dev_view v) {
+    const soil_harmonic_pair pair{v.x, v.y, v.z, v.columns[0], 1.0};
+    double F[3], s[4];
+    soil_gather_force(v, threadIdx.x, pair, F);
+    if (v.slot_max) {
+        const int side = soil_slot_find(v, 0, 1, s);
+        s[0] = F[0] + side;
+        soil_slot_put(v, 0, 0, v.tag[1], s);
+        soil_slot_clear_from(v, 0, 1);
+    }
+}
+''')
+    nvcc = "/usr/local/cuda/bin/nvcc"
+    base = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O2", "-fmad=false",
+            "-I", os.path.join(ROOT, "include"), "-c"]
+    subprocess.check_call(base + [str(src), "-o", str(tmp_path / "hook.o")])
+    for name in ("harmonic_hook", "gather_hook", "slots_hook"):
+        subprocess.check_call(base + [os.path.join(ROOT, "tests", "hooks", f"{name}.cu"),
+                                      "-o", str(tmp_path / f"{name}.o")])
