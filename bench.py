@@ -162,22 +162,6 @@ def make_workload(name, filt, natoms=None):
     return w, desc
 
 
-def dist_init():
-    return dist.init()
-
-
-def max_over_ranks(x, world):
-    return dist.max_over_ranks(x, world)
-
-
-def sum_over_ranks(x, world):
-    return dist.sum_over_ranks(x, world)
-
-
-def barrier(world):
-    dist.barrier(world)
-
-
 def cpu_baseline(w, budget_s=20.0, max_steps=10000, warmup=0):
     """The CPU oracle (single thread, as the reference path) on a bounded
     sample of the same system: setup, `warmup` untimed steps, then timed steps
@@ -252,7 +236,7 @@ def run_soil(args, world, rank, local):
     time.sleep(0.3)
     torch.cuda.synchronize()
     s.sync()
-    barrier(world)
+    dist.barrier(world)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
@@ -260,14 +244,14 @@ def run_soil(args, world, rank, local):
     ev1.record(stream)
     s.sync()
     torch.cuda.synchronize()
-    barrier(world)
+    dist.barrier(world)
     ms = ev0.elapsed_time(ev1)
     clocks = sampler.stop()
     launches = lib.soil_kernel_launches() - launches0
     c1 = s.counts()
     ms_dom, launches_dom, iv_dom = s.get_timing()
     k = abi.TIMER_NAMES.index(dominant)
-    ms_max = max_over_ranks(ms, world)
+    ms_max = dist.max_over_ranks(ms, world)
 
     value = world * w.n * args.steps / (ms_max * 1e-3)
     rebuilds = int(c1.rebuilds - c0.rebuilds)
@@ -328,10 +312,6 @@ C4_DESC = ("C4 batched: 4,096 independent periodic boxes, N log-uniform [256, 65
            "harmonic k=1e3, dt 1e-4")
 
 
-def lpt_partition(sizes, world):
-    return dist.lpt_partition(sizes, world)
-
-
 def batched_cpu_baseline(ws, budget_s=15.0):
     """The CPU oracle on a sample of the boxes: one thread, and one thread per
     host core each stepping its own box (ctypes releases the GIL)."""
@@ -367,7 +347,7 @@ def run_batched(args, world, rank, local):
 
     nbox = args.boxes
     sizes = [workloads.config4_size(i) for i in range(nbox)]
-    mine = lpt_partition(sizes, world)[rank]
+    mine = dist.lpt_partition(sizes, world)[rank]
     t0 = time.perf_counter()
     ws = [workloads.config4_box(i, steps=args.steps) for i in mine]
     natoms = sum(w.n for w in ws)
@@ -392,8 +372,8 @@ def run_batched(args, world, rank, local):
         e1.record(st)
         s.sync()
         plain_ms += e0.elapsed_time(e1)
-    plain_ms = max_over_ranks(plain_ms, world)
-    plain_value = (sum_over_ranks(natoms, world) * args.plain_steps / (plain_ms * 1e-3)
+    plain_ms = dist.max_over_ranks(plain_ms, world)
+    plain_value = (dist.sum_over_ranks(natoms, world) * args.plain_steps / (plain_ms * 1e-3)
                    if args.plain_steps > 0 else None)
 
     batch = system.Batch(ctx)
@@ -412,7 +392,7 @@ def run_batched(args, world, rank, local):
     time.sleep(0.3)
     batch.sync()
     torch.cuda.synchronize()
-    barrier(world)
+    dist.barrier(world)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
@@ -420,7 +400,7 @@ def run_batched(args, world, rank, local):
     ev1.record(stream)
     batch.sync()
     torch.cuda.synchronize()
-    barrier(world)
+    dist.barrier(world)
     ms = ev0.elapsed_time(ev1)
     clocks = sampler.stop()
     launches = lib.soil_kernel_launches() - launches0
@@ -430,8 +410,8 @@ def run_batched(args, world, rank, local):
     load1 = os.getloadavg()
     cs = [s.counts() for s in boxes]
     rebuilds = sum(c.rebuilds for c in cs) - rb0
-    ms_max = max_over_ranks(ms, world)
-    total_atoms = sum_over_ranks(natoms, world)
+    ms_max = dist.max_over_ranks(ms, world)
+    total_atoms = dist.sum_over_ranks(natoms, world)
     value = total_atoms * args.steps / (ms_max * 1e-3)
 
     # roofline of the consumer kernel (one launch per step over every box):
@@ -502,7 +482,7 @@ def run_served(args, world, rank, local):
 
     jobs = [workloads.config5_job(i) for i in range(args.jobs)]
     # partition jobs over ranks (independent units); each rank serves its own
-    mine = lpt_partition([w.n * w.steps for w in jobs], world)[rank]
+    mine = dist.lpt_partition([w.n * w.steps for w in jobs], world)[rank]
     jobs = [jobs[i] for i in mine]
     work = np.array([w.n * w.steps for w in jobs], dtype=np.float64)
 
@@ -541,7 +521,7 @@ def run_served(args, world, rank, local):
     launches0 = lib.soil_kernel_launches()
     sampler = ClockSampler(local)
     sampler.start()
-    barrier(world)
+    dist.barrier(world)
     t_start = time.perf_counter()
 
     def submitter():
@@ -562,8 +542,8 @@ def run_served(args, world, rank, local):
     sv.close()
     states = [i["state"] for i in infos]
     lat = np.array([i["t_done"] - i["t_submit"] for i in infos])
-    makespan = max_over_ranks(t_end - t_start, world)
-    total_work = sum_over_ranks(float(work.sum()), world)
+    makespan = dist.max_over_ranks(t_end - t_start, world)
+    total_work = dist.sum_over_ranks(float(work.sum()), world)
     if rank == 0:
         line = {
             "metric": "atom-steps/s", "value": total_work / makespan, "unit": "atom-steps/s",
@@ -617,7 +597,7 @@ def run_e2e(ctx, w, steps, world):
     out_pos = pinned(np.zeros((w.n, 3)))
     out_vel = pinned(np.zeros((w.n, 3)))
     h2d = sum(host[k].nbytes for k in host)
-    barrier(world)
+    dist.barrier(world)
     t0 = time.perf_counter()
     s = system.System(ctx, w.box, w.cfg, w.dt)
     rc = s.register_column("radius", 1, abi.SOIL_COL_FORWARD)
@@ -635,8 +615,8 @@ def run_e2e(ctx, w, steps, world):
     t_steps = time.perf_counter()
     s.read_local_state(out_pos[1], out_vel[1])
     t1 = time.perf_counter()
-    barrier(world)
-    dt = max_over_ranks(t1 - t0, world)
+    dist.barrier(world)
+    dt = dist.max_over_ranks(t1 - t0, world)
     d2h = out_pos[1].nbytes + out_vel[1].nbytes
     s.close()
     return {"value": world * w.n * steps / dt, "unit": "atom-steps/s",
@@ -671,7 +651,7 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    world, rank, local = dist_init()
+    world, rank, local = dist.init()
     try:
         if args.impl == "reference":
             return run_reference(args, world, rank)

@@ -5,7 +5,8 @@
  * resources, not as an FFI.  Every entry point below replaces one reference
  * system or resource accessor; the citation beside it names the reference
  * function (path inside the reference project, file:line) whose behaviour it
- * reproduces.  A Rust host binds these with `extern "C"`.
+ * reproduces.  A Rust host binds these with `extern "C"` declarations of the
+ * same names and argument types, linking libsoil_cuda.so from its build.rs.
  *
  * Conventions
  *   - Every function returns an `int` status (soil_status).  Nothing panics or
@@ -352,10 +353,12 @@ int soil_sys_load_restart(soil_sys* sys, const uint8_t* buf, uint64_t len, uint6
  * for lamda binning) and a cudaStream_t (NULL = default stream).  Work is
  * enqueued on `stream`.  Scratch is one 16 MiB static device array per GPU,
  * held until process exit; grids above 2,097,152 cells return
- * SOIL_ERR_CAPACITY.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress) with that device current; make that first
- * call before any stream capture.  Calls share the array: calls that overlap
- * on the GPU race and must be serialised.  ctx may be NULL (no message). */
+ * SOIL_ERR_CAPACITY (bin counts whose product would overflow included).
+ * Every call looks up the array's device address (cudaGetSymbolAddress) with
+ * the current device; the first call on a device loads the module there, so
+ * make that first call before any stream capture.  Calls share the array:
+ * calls that overlap on the GPU race and must be serialised.  ctx may be
+ * NULL (no message). */
 int soil_bin_sort_noalloc(soil_ctx* ctx, const double* d_x, const double* d_y,
                           const double* d_z, uint64_t n, const double origin[3],
                           const double bin_size[3], const int32_t bin_count[3],

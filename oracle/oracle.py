@@ -49,6 +49,7 @@ def lib():
             "orc_get_box": (C.c_int, [P, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                       C.POINTER(C.c_double)]),
             "orc_set_harmonic": (C.c_int, [P, C.c_double, C.c_int32]),
+            "orc_set_column_probe": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32]),
             "orc_step": (C.c_int, [P, C.c_uint64]),
             "orc_phase": (C.c_int, [P, C.c_int]),
             "orc_counts": (C.c_int, [P, C.POINTER(abi.SoilCounts)]),
@@ -60,6 +61,7 @@ def lib():
             "orc_get_swap": (C.c_int, [P, C.c_int32, pu64, pu64, pdbl, pdbl, pu32]),
             "orc_get_sort_perm": (C.c_int, [P, pu32]),
             "orc_get_stencil": (C.c_int, [P, pi32, pi32, pdbl, pdbl]),
+            "orc_get_stencil_full": (C.c_int, [P, pi32, pi32, pi32]),
             "orc_set_state": (C.c_int, [P, C.c_int]),
             "orc_set_domain_tilt": (C.c_int, [P, C.c_double, C.c_double, C.c_int]),
             "orc_set_atom_state": (C.c_int, [P, C.c_uint64, pdbl, pdbl, pdbl]),
@@ -136,6 +138,11 @@ class OracleSystem:
 
     def set_harmonic(self, k, radius_col):
         self._L.orc_set_harmonic(self.h, k, radius_col)
+
+    def set_column_probe(self, rev_col=-1, zero_col=-1, fwd_col=-1):
+        """Test consumer writing registered columns in the Force phase (the
+        oracle's counterpart of tests/hooks/registry_hook.cu)."""
+        assert self._L.orc_set_column_probe(self.h, rev_col, zero_col, fwd_col) == 0
 
     def set_deform(self, dim, style, a=0.0, b=0.0, stage_steps=0):
         assert self._L.orc_set_deform(self.h, dim, style, a, b, stage_steps) == 0
@@ -233,6 +240,14 @@ class OracleSystem:
         self._L.orc_get_stencil(self.h, _p(fwd, C.c_int32), C.byref(n), _p(origin, C.c_double),
                                 _p(bs, C.c_double))
         return fwd, origin, bs
+
+    def stencil_full(self):
+        """(full stencil offsets, bin_stencil_self)"""
+        n, hs = C.c_int32(), C.c_int32()
+        self._L.orc_get_stencil_full(self.h, None, C.byref(n), C.byref(hs))
+        full = np.zeros(n.value, np.int32)
+        self._L.orc_get_stencil_full(self.h, _p(full, C.c_int32), C.byref(n), C.byref(hs))
+        return full, bool(hs.value)
 
     # single-function access for known-answer tests
     def set_state(self, state):

@@ -998,6 +998,37 @@ struct Sys {
         }
     }
 
+    // Test consumer of registered columns (no reference counterpart; it plays
+    // the part of a physics plugin that writes #[reverse] / #[zero] /
+    // #[forward] data in its Force system, after the pair forces):
+    //   every atom a (locals and ghosts): rev[a] += {0.5 x, y - z};
+    //                                     zacc[a] += 0.25 x
+    //   every local a:                    fwd[a][k] += 0.001 pos[a][k]
+    // Each value depends on its own atom only, so any evaluation order gives
+    // the same bits; the reverse fold, the zeroing and forward comm then
+    // decide what the columns hold.
+    int probe_rev = -1, probe_zero = -1, probe_fwd = -1;
+    void column_probe() {
+        size_t n = len();
+        if (probe_rev >= 0) {
+            Column& c = cols[probe_rev];
+            for (size_t a = 0; a < n; ++a) {
+                c.data[a * c.width + 0] = c.data[a * c.width + 0] + 0.5 * pos[a][0];
+                c.data[a * c.width + 1] = c.data[a * c.width + 1] + (pos[a][1] - pos[a][2]);
+            }
+        }
+        if (probe_zero >= 0) {
+            Column& c = cols[probe_zero];
+            for (size_t a = 0; a < n; ++a) c.data[a * c.width] = c.data[a * c.width] + 0.25 * pos[a][0];
+        }
+        if (probe_fwd >= 0) {
+            Column& c = cols[probe_fwd];
+            for (size_t a = 0; a < nlocal; ++a)
+                for (int k = 0; k < 3; ++k)
+                    c.data[a * c.width + k] = c.data[a * c.width + k] + 0.001 * pos[a][k];
+        }
+    }
+
     // reverse_send_force self-send path, comm.rs:867-1024 (run_if newton)
     void phase_reverse_comm() {
         if (!newton) return;
@@ -1042,6 +1073,7 @@ struct Sys {
         phase_forward_comm();
         phase_neighbor();          // Neighbor
         phase_force();             // Force
+        column_probe();
         phase_reverse_comm();      // PostForce
         phase_final();             // FinalIntegration
         steps_done += 1;
@@ -1166,6 +1198,19 @@ int orc_get_box(void* h, double* lo, double* hi, double* tilt) {
     return SOIL_OK;
 }
 
+// Test consumer of registered columns (see column_probe); -1 disables a part.
+int orc_set_column_probe(void* h, int32_t rev_col, int32_t zero_col, int32_t fwd_col) {
+    Sys* s = (Sys*)h;
+    const int32_t n = (int32_t)s->cols.size();
+    if (rev_col >= n || zero_col >= n || fwd_col >= n) return SOIL_ERR_INVALID;
+    if (rev_col >= 0 && s->cols[rev_col].width < 2) return SOIL_ERR_INVALID;
+    if (fwd_col >= 0 && s->cols[fwd_col].width < 3) return SOIL_ERR_INVALID;
+    s->probe_rev = rev_col;
+    s->probe_zero = zero_col;
+    s->probe_fwd = fwd_col;
+    return SOIL_OK;
+}
+
 int orc_set_harmonic(void* h, double k, int32_t radius_col) {
     Sys* s = (Sys*)h;
     s->harmonic_k = k;
@@ -1197,7 +1242,7 @@ int orc_phase(void* h, int which) {
         case 7: s->phase_borders(); break;
         case 8: s->phase_forward_comm(); break;
         case 9: s->phase_neighbor(); break;
-        case 10: s->phase_force(); break;
+        case 10: s->phase_force(); s->column_probe(); break;
         case 11: s->phase_reverse_comm(); break;
         case 12: s->phase_final(); s->steps_done += 1; break;
         case 13: s->phase_shrink_wrap(); break;
@@ -1301,6 +1346,17 @@ int orc_get_stencil(void* h, int32_t* fwd, int32_t* nfwd, double* origin3, doubl
         if (origin3) origin3[d] = s->bin_origin[d];
         if (binsize3) binsize3[d] = s->bin_size[d];
     }
+    return SOIL_OK;
+}
+
+// The full stencil (used by newton-off lists) and whether the own cell is part
+// of the stencil (bin_stencil_self).
+int orc_get_stencil_full(void* h, int32_t* full, int32_t* nfull, int32_t* has_self) {
+    Sys* s = (Sys*)h;
+    if (nfull) *nfull = (int32_t)s->bin_stencil.size();
+    if (full)
+        for (size_t k = 0; k < s->bin_stencil.size(); ++k) full[k] = s->bin_stencil[k];
+    if (has_self) *has_self = s->bin_stencil_self ? 1 : 0;
     return SOIL_OK;
 }
 

@@ -42,32 +42,27 @@ constexpr uint64_t kNoAllocScratchWords =
 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocScratchWords];
 
-// Device address of g_noalloc_scratch per device.  The host-side name of the
-// array is only a stand-in for the symbol, not a device address; the address
-// is looked up once per device, with that device current.
-constexpr int kMaxDevices = 64;
-uint32_t* g_scratch_addr[kMaxDevices] = {};
-
+// Device address of g_noalloc_scratch on the current device.  The host-side
+// name of the array is only a stand-in for the symbol, not a device address.
+// The address is looked up on every call (the lookup is cheap), so a module
+// reloaded after cudaDeviceReset is never reached through a stale pointer.
 int scratch_for_current_device(soil_ctx* ctx, uint32_t** out) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    if (e != cudaSuccess || dev < 0) {
         cudaGetLastError();
         return set_ctx_error(ctx, SOIL_ERR_NO_DEVICE, "soil_bin_sort_noalloc: no current CUDA device");
     }
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            cudaGetLastError();
-            char buf[160];
-            snprintf(buf, sizeof buf, "soil_bin_sort_noalloc: cudaGetSymbolAddress failed: %s",
-                     cudaGetErrorString(e));
-            return set_ctx_error(ctx, SOIL_ERR_CUDA, buf);
-        }
-        g_scratch_addr[dev] = (uint32_t*)p;
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        char buf[160];
+        snprintf(buf, sizeof buf, "soil_bin_sort_noalloc: cudaGetSymbolAddress failed: %s",
+                 cudaGetErrorString(e));
+        return set_ctx_error(ctx, SOIL_ERR_CUDA, buf);
     }
-    *out = g_scratch_addr[dev];
+    *out = (uint32_t*)p;
     return SOIL_OK;
 }
 
@@ -86,8 +81,10 @@ extern "C" int soil_bin_sort_noalloc(soil_ctx* ctx, const double* d_x, const dou
     for (int d = 0; d < 3; ++d)
         if (bin_count[d] < 1 || !(bin_size[d] > 0.0) || !(box_size[d] > 0.0))
             return set_ctx_error(ctx, SOIL_ERR_INVALID, "soil_bin_sort_noalloc: invalid bin grid");
-    const uint64_t ncells =
-        (uint64_t)bin_count[0] * (uint64_t)bin_count[1] * (uint64_t)bin_count[2];
+    // the product is built factor by factor and stops past the limit, so
+    // counts whose 64-bit product would wrap are refused too
+    uint64_t ncells = 1;
+    for (int d = 0; d < 3 && ncells <= kNoAllocMaxCells; ++d) ncells *= (uint64_t)bin_count[d];
     if (ncells > kNoAllocMaxCells) {
         char buf[200];
         snprintf(buf, sizeof buf,

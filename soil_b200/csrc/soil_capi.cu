@@ -111,7 +111,10 @@ void free_cols(soil_sys* s, AtomCols& c) {
     dev_free(s, c.type, c.cap * 4);
     dev_free(s, c.img, c.cap * 12);
     dev_free(s, c.origin, c.cap * 4);
-    for (int q = 0; q < c.nplanes; ++q) dev_free(s, c.planes[q], c.cap * 8);
+    // one block per registered column holds its planes
+    for (const ColMeta& m : s->cols)
+        if (m.plane0 < c.nplanes) dev_free(s, c.planes[m.plane0], c.cap * 8 * (uint64_t)m.width);
+    for (int q = 0; q < c.nplanes; ++q) c.planes[q] = nullptr;
     c.tag = c.type = nullptr;
     c.img = c.origin = nullptr;
 }
@@ -128,8 +131,16 @@ int alloc_cols(soil_sys* s, AtomCols& c, uint64_t cap, const AtomCols* old, uint
     if (st == SOIL_OK) st = dev_alloc(s, (void**)&n.type, cap * 4);
     if (st == SOIL_OK) st = dev_alloc(s, (void**)&n.img, cap * 12);
     if (st == SOIL_OK) st = dev_alloc(s, (void**)&n.origin, cap * 4);
-    for (int q = 0; q < s->nplanes && st == SOIL_OK; ++q)
-        st = dev_alloc(s, (void**)&n.planes[q], cap * 8);
+    // The planes of a column of width w are one block of w * cap doubles:
+    // component k of atom i is planes[plane0][k * cap + i], the layout the
+    // device view documents (columns[c][k * stride + i]).
+    for (const ColMeta& m : s->cols) {
+        if (st != SOIL_OK) break;
+        double* blk = nullptr;
+        st = dev_alloc(s, (void**)&blk, cap * 8 * (uint64_t)m.width);
+        if (st == SOIL_OK)
+            for (int k = 0; k < m.width; ++k) n.planes[m.plane0 + k] = blk + k * cap;
+    }
     if (st != SOIL_OK) {
         free_cols(s, n);
         return st;

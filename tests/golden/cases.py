@@ -28,6 +28,10 @@ def _w(name):
     if name == "deform-z-erate":
         w = W.poly(name, 105, 1500, 0.40, 1e-3, 60, harmonic_k=1e3)
         return w, {"deform": [(2, abi.SOIL_DEFORM_ERATE, -1.0, 0.0, 0)]}
+    if name == "registry-columns":  # every AtomData flag class, widths 1-3
+        w = W.poly(name, 107, 1500, 0.45, 1e-3, 60, harmonic_k=1e3)
+        w.vel *= 3.0  # a rebuild (sort, borders) every few steps
+        return w, {"columns": True}
     if name == "fixed-z-shrink-x":
         w = W.poly(name, 106, 1500, 0.40, 1e-3, 60, harmonic_k=1e3)
         w.vel *= 10.0
@@ -36,15 +40,32 @@ def _w(name):
 
 
 CASES = ["mono-free", "poly-harmonic", "mono-shear", "poly-newton-off-fp32", "deform-z-erate",
-         "fixed-z-shrink-x"]
+         "fixed-z-shrink-x", "registry-columns"]
+
+# Columns of the registry case beyond the radius (column 0): name, width,
+# flags.  A consumer (the oracle's column probe, or tests/hooks/registry_hook.cu
+# on the GPU) writes orient (locals), torque and zacc (every atom) in the
+# Force phase; label is never written, only permuted and copied to ghosts.
+REGISTRY_COLUMNS = [("orient", 3, abi.SOIL_COL_FORWARD), ("torque", 2, abi.SOIL_COL_REVERSE),
+                    ("zacc", 1, abi.SOIL_COL_ZERO), ("label", 2, 0)]
+REGISTRY_PROBE = {"rev_col": 2, "zero_col": 3, "fwd_col": 1}
 
 
-def build(make, name):
-    """make(box, cfg, dt) -> an empty GPU or oracle system; returns (system, steps)."""
+def build(make, name, attach=None):
+    """make(box, cfg, dt) -> an empty GPU or oracle system; returns (system, steps).
+    attach(system, probe) installs the column-writing consumer of cases that
+    register columns (probe: REGISTRY_PROBE)."""
     w, extra = _w(name)
     s = make(w.box, w.cfg, w.dt)
     rc = s.register_column("radius", 1, abi.SOIL_COL_FORWARD)
-    s.add_atoms(w.tag, w.pos, w.vel, w.mass, w.cutoff, columns=[w.radius])
+    data = [w.radius]
+    if extra.get("columns"):
+        for k, (cname, width, flags) in enumerate(REGISTRY_COLUMNS):
+            s.register_column(cname, width, flags)
+            vals = np.stack([W.uniform(w.seed, 0, 40 + 4 * k + c, w.n) for c in range(width)],
+                            axis=1)
+            data.append(vals if width > 1 else vals[:, 0])
+    s.add_atoms(w.tag, w.pos, w.vel, w.mass, w.cutoff, columns=data)
     if w.harmonic_k:
         s.set_harmonic(w.harmonic_k, rc)
     if w.shear_rate:
@@ -54,6 +75,10 @@ def build(make, name):
     if "boundary" in extra:
         s.set_boundary(*extra["boundary"])
     s.setup()
+    if extra.get("columns"):
+        if attach is None:
+            raise ValueError(f"case {name} needs a column consumer (attach)")
+        attach(s, REGISTRY_PROBE)
     return s, w.steps
 
 
@@ -79,4 +104,5 @@ def state_digest(s):
                     *[x["send"].astype(np.uint32) for x in sw],
                     *[x["offset"] for x in sw], *[x["vel_offset"] for x in sw]),
         "box": _h(lo, hi, tilt),
+        "columns": _h(*[s.column(k) for k in range(len(s.columns))]),
     }

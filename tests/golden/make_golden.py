@@ -5,7 +5,7 @@
 The oracle is pinned to the reference's own unit tests; these fixtures then
 pin complete trajectories of small seeded systems (counts and SHA-256 digests
 of positions, velocities, forces, images, ghost origins, neighbor lists, swap
-records and the box after each case's steps), so the oracle and the CUDA path
+records, registered columns and the box after each case's steps), so the oracle and the CUDA path
 are both checked against committed data."""
 import json
 import os
@@ -24,7 +24,8 @@ from cases import CASES, build, state_digest  # noqa: E402
 def main():
     out = {}
     for name in CASES:
-        s, steps = build(oracle.OracleSystem, name)
+        s, steps = build(oracle.OracleSystem, name,
+                         attach=lambda o, probe: o.set_column_probe(**probe))
         s.step(steps)
         out[name] = state_digest(s)
     with open(os.path.join(HERE, "states.json"), "w") as f:

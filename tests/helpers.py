@@ -1,9 +1,46 @@
 """Shared helpers of the parity tests: build the same system on the GPU and
 in the CPU oracle from one seeded workload, and compare every observable."""
+import ctypes as C
+import os
+import subprocess
+
 import numpy as np
 
 import oracle
 from soil_b200 import abi, system, workloads
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def build_hook(out_dir, name):
+    """Compile tests/hooks/<name>.cu (a consumer built apart from the library,
+    against include/ only) into out_dir and load it."""
+    out = os.path.join(str(out_dir), f"lib{name}.so")
+    subprocess.check_call(["/usr/local/cuda/bin/nvcc", "-gencode", "arch=compute_100a,code=sm_100a",
+                           "-O3", "-fmad=false", "-shared", "-Xcompiler", "-fPIC",
+                           "-I", os.path.join(ROOT, "include"),
+                           os.path.join(ROOT, "tests", "hooks", f"{name}.cu"), "-o", out])
+    return C.CDLL(out)
+
+
+class RegistryProbe(C.Structure):
+    """User data of tests/hooks/registry_hook.cu."""
+    _fields_ = [("K", C.c_double), ("rev", C.c_int32), ("zero", C.c_int32), ("fwd", C.c_int32)]
+
+
+def attach_registry_hook(lib, K):
+    """attach(system, probe) for tests/golden/cases.build on the GPU: installs
+    registry_hook (harmonic forces in the reference order + column writes)."""
+    def attach(s, probe):
+        u = RegistryProbe(K, probe["rev_col"], probe["zero_col"], probe["fwd_col"])
+        s._probe = u  # lives as long as the system
+        s.set_force_hook_ptr(C.cast(lib.registry_hook, C.c_void_p).value,
+                             C.cast(C.pointer(u), C.c_void_p))
+    return attach
+
+
+def attach_oracle_probe(s, probe):
+    s.set_column_probe(**probe)
 
 
 def pair(ctx, w):

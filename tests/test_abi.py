@@ -121,3 +121,19 @@ __global__ void k(soil_dev_view v) {
     for name in ("harmonic_hook", "gather_hook", "slots_hook"):
         subprocess.check_call(base + [os.path.join(ROOT, "tests", "hooks", f"{name}.cu"),
                                       "-o", str(tmp_path / f"{name}.o")])
+
+
+@pytest.mark.parametrize("counts", [
+    (1 << 22, 1 << 21, 1 << 21),   # 64-bit product is exactly 2**64 (wraps to 0)
+    (2147483647, 2147483647, 5),   # product far past 2**64
+    (200, 200, 200),               # 8,000,000 cells, no wrap, still above the limit
+])
+def test_no_alloc_sort_refuses_large_or_wrapping_grids(counts):
+    """Grid checks run before any device call, so they work without a GPU."""
+    lib = abi.load_library()
+    one = (C.c_double * 3)(1.0, 1.0, 1.0)
+    zero = (C.c_double * 3)(0.0, 0.0, 0.0)
+    bc = (C.c_int32 * 3)(*counts)
+    st = lib.soil_bin_sort_noalloc(None, None, None, None, 0, zero, one, bc, zero, one, zero, 0,
+                                   None, None, None)
+    assert st == abi.SOIL_ERR_CAPACITY
