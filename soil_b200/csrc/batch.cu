@@ -867,6 +867,7 @@ int batch_step(soil_batch* b, bool last) {
             s->npairs = np;
             s->rebuilds += 1;
             s->in_lists_valid = true;
+            s->seq_valid = false;  // rebuilt by the first single-system force call
             s->hflags->candidates = b->h_flags[k].candidates;
             s->hflags->rechecked = b->h_flags[k].rechecked;
             fill_dev(b, k);

@@ -48,6 +48,15 @@ __device__ __forceinline__ bool moved_too_far_mixed(double px, double py, double
     return d[0] * d[0] + d[1] * d[1] + d[2] * d[2] > thr_sq;
 }
 
+// The displacement check of one local at its new position.
+__device__ __forceinline__ bool check_moved(const CheckArgs& ck, double x, double y, double z,
+                                            uint64_t i) {
+    if (ck.mask == 7)
+        return moved_too_far(x, y, z, ck.lbx[i], ck.lby[i], ck.lbz[i], ck.box, ck.ibox, ck.thr_sq);
+    return moved_too_far_mixed(x, y, z, ck.lbx[i], ck.lby[i], ck.lbz[i], ck.box, ck.mask,
+                               ck.thr_sq);
+}
+
 // wrap_periodic, domain.rs:594-605
 __device__ __forceinline__ double wrap1(double p, double low, double sz, int32_t& img) {
     const double high = low + sz;
@@ -244,7 +253,8 @@ __device__ uint32_t row_scan(const PairParams& p, const Filter<UNIFORM, FP32>& t
 // returns the new position.
 __device__ __forceinline__ void initial_atom(const AtomCols& c, uint64_t i, double dt,
                                              bool fuse_final, bool zero_force, double& x,
-                                             double& y, double& z) {
+                                             double& y, double& z, double& v0, double& v1,
+                                             double& v2) {
     const double h = 0.5 * dt * c.inv_mass[i];
     const double fx = c.fx[i], fy = c.fy[i], fz = c.fz[i];
     double vx = c.vx[i], vy = c.vy[i], vz = c.vz[i];
@@ -253,9 +263,9 @@ __device__ __forceinline__ void initial_atom(const AtomCols& c, uint64_t i, doub
         vy = vy + h * fy;
         vz = vz + h * fz;
     }
-    const double v0 = vx + h * fx;
-    const double v1 = vy + h * fy;
-    const double v2 = vz + h * fz;
+    v0 = vx + h * fx;
+    v1 = vy + h * fy;
+    v2 = vz + h * fz;
     c.vx[i] = v0;
     c.vy[i] = v1;
     c.vz[i] = v2;
@@ -270,6 +280,13 @@ __device__ __forceinline__ void initial_atom(const AtomCols& c, uint64_t i, doub
         c.fy[i] = 0.0;
         c.fz[i] = 0.0;
     }
+}
+
+__device__ __forceinline__ void initial_atom(const AtomCols& c, uint64_t i, double dt,
+                                             bool fuse_final, bool zero_force, double& x,
+                                             double& y, double& z) {
+    double v0, v1, v2;
+    initial_atom(c, i, dt, fuse_final, zero_force, x, y, z, v0, v1, v2);
 }
 
 // final_integration, soil_verlet/src/lib.rs:175-194: v += h*F
@@ -348,6 +365,46 @@ __device__ __forceinline__ void forward_ghost(const AtomCols& c, uint64_t nlocal
         c.fx[g] = 0.0;
         c.fy[g] = 0.0;
         c.fz[g] = 0.0;
+    }
+}
+
+// forward_comm of every image of local r, from r's new position and velocity
+// (held by the caller): the same additions as forward_ghost, in chain order,
+// for the ghosts of r's fold program.
+__device__ __forceinline__ void forward_images(const AtomCols& c, uint64_t nlocal, uint64_t r,
+                                               double px0, double py0, double pz0, double vx0,
+                                               double vy0, double vz0, const uint32_t* fold_start,
+                                               const uint32_t* fold_list, const uint32_t* chain,
+                                               const SwapConst& sc, const PlaneList& fwd,
+                                               bool zero_force) {
+    const uint32_t f1 = fold_start[r + 1];
+    for (uint32_t f = fold_start[r]; f < f1; ++f) {
+        const uint32_t gi = fold_list[f];
+        const uint64_t g = nlocal + gi;
+        const uint32_t code = chain[gi];
+        const uint32_t len = code >> 12;
+        double px = px0, py = py0, pz = pz0, vx = vx0, vy = vy0, vz = vz0;
+        for (uint32_t k = 0; k < len; ++k) {
+            const int s = (code >> (3 * k)) & 7;
+            px = px + sc.off[s][0];
+            py = py + sc.off[s][1];
+            pz = pz + sc.off[s][2];
+            vx = vx + sc.voff[s][0];
+            vy = vy + sc.voff[s][1];
+            vz = vz + sc.voff[s][2];
+        }
+        c.x[g] = px;
+        c.y[g] = py;
+        c.z[g] = pz;
+        c.vx[g] = vx;
+        c.vy[g] = vy;
+        c.vz[g] = vz;
+        for (int q = 0; q < fwd.n; ++q) c.planes[fwd.idx[q]][g] = c.planes[fwd.idx[q]][r];
+        if (zero_force) {
+            c.fx[g] = 0.0;
+            c.fy[g] = 0.0;
+            c.fz[g] = 0.0;
+        }
     }
 }
 

@@ -1,0 +1,164 @@
+// force_ops.cuh — the grouped built-in consumer's warp tile (device code
+// shared by the one-launch consumer k_force_seq and the device-resident
+// multi-step kernel k_steps).  How the tile reproduces the reference's force
+// sums is described at the top of k_force.cu.
+#pragma once
+
+#include "device_ops.cuh"
+#include "kernels.cuh"
+
+namespace soil {
+
+constexpr int kForceWarps = kBlock / 32;
+
+template <int U>
+struct ForceSmem {
+    double fx[kForceWarps][32 * U];
+    double fy[kForceWarps][32 * U];
+    double fz[kForceWarps][32 * U];
+    uint32_t hit[kForceWarps][U];  // contact ballots of the chunk's rows
+};
+
+// f(i, j) of the tutorial consumer with i = a (the owner) and j = o
+// (docs/src/tutorial/write-your-own-physics.md:56-110).
+__device__ __forceinline__ bool pair_force(double xa, double ya, double za, double ra, double xo,
+                                           double yo, double zo, double ro, double K, double& fx,
+                                           double& fy, double& fz) {
+    const double sum_r = ra + ro;
+    const double dx = xo - xa;
+    const double dy = yo - ya;
+    const double dz = zo - za;
+    const double dist_sq = dx * dx + dy * dy + dz * dz;
+    if (dist_sq >= sum_r * sum_r || dist_sq == 0.0) return false;
+    const double dist = sqrt(dist_sq);
+    const double overlap = sum_r - dist;
+    const double inv_dist = 1.0 / dist;
+    const double fmag = K * overlap;
+    fx = -fmag * dx * inv_dist;
+    fy = -fmag * dy * inv_dist;
+    fz = -fmag * dz * inv_dist;
+    return true;
+}
+
+// The item (root or image) a lane's walk is in: its atom and entry range.
+struct Item {
+    uint64_t atom;
+    uint32_t end;  // one past its last entry
+};
+
+// Item j of root t's group (0: t itself; j >= 1: its j-th image in fold
+// order), starting at entry `begin`.
+__device__ __forceinline__ Item item_at(const ForceArgs& p, uint64_t t, uint32_t f0, int j,
+                                        uint32_t begin) {
+    Item it;
+    it.atom = j == 0 ? t : p.nlocal + p.fold_list[f0 + j - 1];
+    it.end = begin + p.cnt[it.atom];
+    return it;
+}
+
+// One warp tile of the grouped consumer: roots [32 w, 32 w + 32) and their
+// images.  Phase 1 spreads the tile's entries over the lanes, U rows of 32 per
+// chunk, and writes every pair force to shared memory; phase 2 lets each lane
+// add its own group's entries of the chunk in order.  With FOLD, each lane
+// then folds its images into its root (fold_root: reverse_send_force's order).
+template <int U, bool FOLD>
+__device__ __forceinline__ void force_tile(const ForceArgs& p, uint64_t w, ForceSmem<U>& sm,
+                                           int lane, int wib) {
+    constexpr int CH = 32 * U;
+    const uint64_t nl = p.nlocal;
+    const AtomCols& c = p.c;
+    const uint64_t t = w * 32 + lane;
+    const bool valid = t < nl;
+    const uint64_t last = w * 32 + 32 < nl ? w * 32 + 32 : nl;
+    double xa = 0.0, ya = 0.0, za = 0.0, ra = 0.0;
+    uint32_t gs = 0, ge = 0, f0 = 0, nimg = 0;
+    if (valid) {
+        xa = c.x[t];
+        ya = c.y[t];
+        za = c.z[t];
+        ra = p.rad[t];
+        gs = p.grp_start[t];
+        ge = p.grp_start[t + 1];
+        f0 = p.fold_start[t];
+        nimg = p.fold_start[t + 1] - f0;
+    }
+    const uint32_t base = p.grp_start[w * 32];
+    const uint32_t end = p.grp_start[last];
+    // the lane's walk over its group: current item j and its running sum
+    int j = 0;
+    Item it = {t, gs};
+    if (valid) it = item_at(p, t, f0, 0, gs);
+    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
+    uint32_t k = gs;
+    for (uint32_t c0 = base; c0 < end; c0 += CH) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t e = c0 + (uint32_t)(u * 32 + lane);
+            const bool in = e < end;
+            uint32_t o = 0, m = 0;
+            if (in) {
+                o = p.seq[e];
+                m = p.owner[e];
+            }
+            const int ol = (int)(m & 31u);
+            double xi = __shfl_sync(0xffffffffu, xa, ol);
+            double yi = __shfl_sync(0xffffffffu, ya, ol);
+            double zi = __shfl_sync(0xffffffffu, za, ol);
+            double ri = __shfl_sync(0xffffffffu, ra, ol);
+            const uint32_t of0 = __shfl_sync(0xffffffffu, f0, ol);
+            if (m >> 5) {  // an image of lane ol's root
+                const uint64_t g = nl + p.fold_list[of0 + (m >> 5) - 1];
+                xi = c.x[g];
+                yi = c.y[g];
+                zi = c.z[g];
+                ri = p.rad[g];
+            }
+            double fx = 0.0, fy = 0.0, fz = 0.0;
+            bool hit = false;
+            if (in)
+                hit = pair_force(xi, yi, zi, ri, c.x[o], c.y[o], c.z[o], p.rad[o], p.K, fx, fy, fz);
+            const unsigned mask = __ballot_sync(0xffffffffu, hit);
+            if (lane == 0) sm.hit[wib][u] = mask;
+            sm.fx[wib][u * 32 + lane] = fx;
+            sm.fy[wib][u * 32 + lane] = fy;
+            sm.fz[wib][u * 32 + lane] = fz;
+        }
+        __syncwarp();
+        // this lane's entries inside the chunk, in group order
+        const uint32_t hi = ge < c0 + CH ? ge : c0 + CH;
+        for (; k < hi; ++k) {
+            // k < ge = the last item's end, so the walk never passes it
+            while (k >= it.end) {  // the item is complete: store its force
+                c.fx[it.atom] = Fx;
+                c.fy[it.atom] = Fy;
+                c.fz[it.atom] = Fz;
+                Fx = Fy = Fz = 0.0;
+                ++j;
+                it = item_at(p, t, f0, j, it.end);
+            }
+            const uint32_t r = k - c0;
+            if (sm.hit[wib][r >> 5] & (1u << (r & 31))) {
+                Fx = Fx + sm.fx[wib][r];
+                Fy = Fy + sm.fy[wib][r];
+                Fz = Fz + sm.fz[wib][r];
+            }
+        }
+        __syncwarp();
+    }
+    if (valid) {
+        // every entry is summed: store the open item, then the images after
+        // it, which have no entries (their force is zero)
+        for (;;) {
+            c.fx[it.atom] = Fx;
+            c.fy[it.atom] = Fy;
+            c.fz[it.atom] = Fz;
+            if (j == (int)nimg) break;
+            Fx = Fy = Fz = 0.0;
+            ++j;
+            it = item_at(p, t, f0, j, it.end);
+        }
+        if (FOLD) fold_root(c, nl, t, p.fold_start, p.fold_list, p.rev);
+    }
+}
+
+}  // namespace soil

@@ -21,37 +21,22 @@ unsigned grid_for(uint64_t n, int block, int per_sm) {
     return (unsigned)(need < cap ? need : cap);
 }
 
-struct CheckArgs {
-    const double* lbx;
-    const double* lby;
-    const double* lbz;
-    uint64_t n_check;
-    double thr_sq;
-    double box[3];
-    double ibox[3];
-    DevFlags* flags;
-    int mask;  // periodic axes (7: fully periodic fast path)
-};
-
-__device__ __forceinline__ bool check_moved(const CheckArgs& ck, double x, double y, double z,
-                                            uint64_t i) {
-    if (ck.mask == 7)
-        return moved_too_far(x, y, z, ck.lbx[i], ck.lby[i], ck.lbz[i], ck.box, ck.ibox, ck.thr_sq);
-    return moved_too_far_mixed(x, y, z, ck.lbx[i], ck.lby[i], ck.lbz[i], ck.box, ck.mask,
-                               ck.thr_sq);
-}
-
 // initial_integration, soil_verlet/src/lib.rs:131-162:
 //   h = 0.5*dt*inv_m;  v += h*F;  x += v*dt
-template <bool FUSE_FINAL>
+// With FWD, each local then writes its ghost images (forward_comm of a step
+// that keeps its lists): the values forward comm would copy after this pass.
+template <bool FUSE_FINAL, bool FWD>
 __global__ void __launch_bounds__(kBlock) k_initial(uint64_t n, AtomCols c, double dt,
-                                                    int zero_force, CheckArgs ck) {
+                                                    int zero_force, CheckArgs ck, FwdArgs fw) {
     bool hit = false;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x) {
-        double x, y, z;
-        initial_atom(c, i, dt, FUSE_FINAL, zero_force != 0, x, y, z);
+        double x, y, z, vx, vy, vz;
+        initial_atom(c, i, dt, FUSE_FINAL, zero_force != 0, x, y, z, vx, vy, vz);
         if (i < ck.n_check) hit |= check_moved(ck, x, y, z, i);
+        if (FWD)
+            forward_images(c, n, i, x, y, z, vx, vy, vz, fw.fold_start, fw.fold_list, fw.chain,
+                           fw.sc, fw.fwd, fw.zero_ghost_force != 0);
     }
     if (ck.flags) {
         unsigned any = __ballot_sync(0xffffffffu, hit);
@@ -59,7 +44,7 @@ __global__ void __launch_bounds__(kBlock) k_initial(uint64_t n, AtomCols c, doub
     }
 }
 
-static CheckArgs make_check(const double* lbx, const double* lby, const double* lbz,
+CheckArgs make_check(const double* lbx, const double* lby, const double* lbz,
                             uint64_t n_check, double thr_sq, const double box[3],
                             DevFlags* flags, int mask) {
     CheckArgs ck;
@@ -77,23 +62,36 @@ static CheckArgs make_check(const double* lbx, const double* lby, const double* 
     return ck;
 }
 
+template <bool FUSE_FINAL>
+static void initial_kernel(cudaStream_t st, uint64_t n, const AtomCols& c, double dt,
+                           bool zero_force, const CheckArgs& ck, const FwdArgs* fw) {
+    note_launch();
+    if (fw) {
+        k_initial<FUSE_FINAL, true>
+            <<<grid_for(n), kBlock, 0, st>>>(n, c, dt, zero_force ? 1 : 0, ck, *fw);
+    } else {
+        FwdArgs none{};
+        k_initial<FUSE_FINAL, false>
+            <<<grid_for(n), kBlock, 0, st>>>(n, c, dt, zero_force ? 1 : 0, ck, none);
+    }
+}
+
 void launch_initial(cudaStream_t st, uint64_t n, const AtomCols& c, double dt, bool zero_force,
                     const double* lbx, const double* lby, const double* lbz, uint64_t n_check,
-                    double thr_sq, const double box[3], DevFlags* flags, int pbc_mask) {
+                    double thr_sq, const double box[3], DevFlags* flags, int pbc_mask,
+                    const FwdArgs* fw) {
     if (n == 0) return;
     CheckArgs ck = make_check(lbx, lby, lbz, n_check, thr_sq, box, flags, pbc_mask);
-    note_launch();
-    k_initial<false><<<grid_for(n), kBlock, 0, st>>>(n, c, dt, zero_force ? 1 : 0, ck);
+    initial_kernel<false>(st, n, c, dt, zero_force, ck, fw);
 }
 
 void launch_final_initial(cudaStream_t st, uint64_t n, const AtomCols& c, double dt,
                           bool zero_force, const double* lbx, const double* lby,
                           const double* lbz, uint64_t n_check, double thr_sq,
-                          const double box[3], DevFlags* flags, int pbc_mask) {
+                          const double box[3], DevFlags* flags, int pbc_mask, const FwdArgs* fw) {
     if (n == 0) return;
     CheckArgs ck = make_check(lbx, lby, lbz, n_check, thr_sq, box, flags, pbc_mask);
-    note_launch();
-    k_initial<true><<<grid_for(n), kBlock, 0, st>>>(n, c, dt, zero_force ? 1 : 0, ck);
+    initial_kernel<true>(st, n, c, dt, zero_force, ck, fw);
 }
 
 // final_integration, soil_verlet/src/lib.rs:175-194: v += h*F

@@ -1,0 +1,150 @@
+// k_steps.cu — device-resident communicate-only steps.
+//
+// The reference decides every step whether the lists must be rebuilt
+// (decide_rebuild, crates/soil_core/src/neighbor.rs:796-822); its GPU
+// prototype runs K resident steps with no host read in between
+// (crates/soil_gpu/src/gpu_state.rs:352-418).  k_steps runs consecutive steps
+// that keep their lists in ONE cooperative launch, every CTA resident:
+//
+//   phase A  final(t-1) + initial(t) + displacement check + forward comm
+//            (the fused integration pass of soil_step), one thread per local;
+//   barrier; every CTA reads the check: if any atom moved too far, the
+//            launch ends here (step t's integration is done, its rebuild is
+//            the host's);
+//   phase B  the grouped consumer with the reverse fold (if any);
+//   barrier (so no CTA's next phase A can set the check flag before every
+//            CTA has read it); next step.
+//
+// Each step runs the same per-atom functions in the same order as the
+// launch-per-phase path, so results are bit-identical.  The grid barrier is
+// this library's own (a counter and a generation word): its wait is bounded,
+// and a CTA whose wait runs out records SOIL_STEPS_ERR_BARRIER in flags->error
+// and returns; the others then run out at their next barrier.  Co-residency
+// of every CTA is guaranteed by the cooperative launch, so the bound is a
+// guard, never the expected exit.
+#include <cuda/atomic>
+
+#include "device_ops.cuh"
+#include "force_ops.cuh"
+#include "kernels.cuh"
+
+namespace soil {
+
+namespace {
+
+// Spins of a barrier wait (each >= 100 ns of __nanosleep): about a second.
+constexpr uint64_t kBarrierSpinLimit = 1ull << 23;
+
+__device__ bool grid_sync(GridBar* b, unsigned nblocks, unsigned& gen, uint32_t* err) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(b->count), g(b->gen);
+        ok = 1;
+        if (cnt.fetch_add(1u, cuda::memory_order_acq_rel) == nblocks - 1) {
+            cnt.store(0u, cuda::memory_order_relaxed);
+            g.store(gen + 1, cuda::memory_order_release);
+        } else {
+            uint64_t spins = 0;
+            while (g.load(cuda::memory_order_acquire) == gen) {
+                if (++spins > kBarrierSpinLimit) {
+                    atomicOr(err, SOIL_STEPS_ERR_BARRIER);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(100);
+            }
+        }
+        gen += 1;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+}  // namespace
+
+template <int U, int CONSUMER>  // CONSUMER: 0 none, 1 grouped, 2 grouped + fold
+__global__ void __launch_bounds__(kBlock, 4) k_steps(StepsArgs a) {
+    __shared__ ForceSmem<U> sm;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const uint64_t nl = a.nlocal;
+    const AtomCols& c = a.c;
+    // every CTA reads the generation before any CTA can reach the first
+    // barrier's release (which needs all of them)
+    unsigned gen = 0;
+    if (threadIdx.x == 0)
+        gen = cuda::atomic_ref<unsigned, cuda::thread_scope_device>(a.bar->gen)
+                  .load(cuda::memory_order_relaxed);
+    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> tripped(a.flags->rebuild);
+    uint64_t done = 0;
+    bool stop = false;
+    for (uint64_t step = 0; step < a.max_steps; ++step) {
+        // phase A: the fused integration pass
+        const bool fuse_final = step > 0 || a.first_fused;
+        bool hit = false;
+        for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nl;
+             i += (uint64_t)gridDim.x * blockDim.x) {
+            double x, y, z, vx, vy, vz;
+            initial_atom(c, i, a.dt, fuse_final, a.zero_force != 0, x, y, z, vx, vy, vz);
+            hit |= check_moved(a.ck, x, y, z, i);
+            forward_images(c, nl, i, x, y, z, vx, vy, vz, a.fw.fold_start, a.fw.fold_list,
+                           a.fw.chain, a.fw.sc, a.fw.fwd, a.fw.zero_ghost_force != 0);
+        }
+        if (__ballot_sync(0xffffffffu, hit) && lane == 0) atomicOr(&a.flags->rebuild, 1u);
+        if (!grid_sync(a.bar, gridDim.x, gen, &a.flags->error)) return;
+        if (tripped.load(cuda::memory_order_relaxed)) {
+            stop = true;
+            break;
+        }
+        // phase B: the consumer over every root's group (and the fold)
+        if (CONSUMER) {
+            const uint64_t ntiles = (nl + 31) / 32;
+            for (uint64_t w = (uint64_t)blockIdx.x * kForceWarps + wib; w < ntiles;
+                 w += (uint64_t)gridDim.x * kForceWarps)
+                force_tile<U, CONSUMER == 2>(a.fa, w, sm, lane, wib);
+        }
+        // Also without a consumer: no CTA may set the flag in the next phase A
+        // before every CTA has read it above.
+        if (!grid_sync(a.bar, gridDim.x, gen, &a.flags->error)) return;
+        ++done;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.out[0] = (uint32_t)done;
+        a.out[1] = stop ? 1u : 0u;
+    }
+}
+
+static const void* steps_kernel(int consumer) {
+    return consumer == 0 ? (const void*)k_steps<4, 0>
+         : consumer == 1 ? (const void*)k_steps<4, 1> : (const void*)k_steps<4, 2>;
+}
+
+int steps_grid(int consumer, uint64_t nlocal, int* grid) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, steps_kernel(consumer), kBlock, 0) !=
+            cudaSuccess ||
+        per_sm < 1) {
+        cudaGetLastError();
+        return 1;
+    }
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint64_t need_atoms = (nlocal + kBlock - 1) / kBlock;
+    const uint64_t need_tiles = ((nlocal + 31) / 32 + kForceWarps - 1) / kForceWarps;
+    uint64_t need = need_atoms > need_tiles ? need_atoms : need_tiles;
+    if (need < 1) need = 1;
+    const uint64_t cap = (uint64_t)per_sm * (uint64_t)sms;
+    *grid = (int)(need < cap ? need : cap);
+    return 0;
+}
+
+cudaError_t launch_steps(cudaStream_t st, const StepsArgs& a, int consumer, int grid) {
+    note_launch();
+    StepsArgs arg = a;
+    void* params[] = {&arg};
+    return cudaLaunchCooperativeKernel(steps_kernel(consumer), dim3(grid), dim3(kBlock), params, 0,
+                                       st);
+}
+
+}  // namespace soil

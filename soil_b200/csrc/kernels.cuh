@@ -15,18 +15,47 @@ void note_launch();
 uint64_t launches_so_far();
 
 // ---- integrate (k_integrate.cu) -------------------------------------------
-// initial_integration (+ optional fused force zeroing and displacement check)
-// pbc_mask: bit d set for a periodic axis d (7: the fully periodic test).
+// The displacement check fused into the integration pass (decide_rebuild's
+// displacement_exceeded): last-build positions, threshold, periodic box.
+struct CheckArgs {
+    const double* lbx;
+    const double* lby;
+    const double* lbz;
+    uint64_t n_check;
+    double thr_sq;
+    double box[3];
+    double ibox[3];
+    DevFlags* flags;
+    int mask;  // periodic axes (7: fully periodic fast path)
+};
+CheckArgs make_check(const double* lbx, const double* lby, const double* lbz, uint64_t n_check,
+                     double thr_sq, const double box[3], DevFlags* flags, int mask);
+// forward_comm fused into the integration pass: every local writes its ghost
+// images (fold program of the last border pass) from its new position and
+// velocity, with the #[forward] planes; zero_ghost_force clears their forces.
+struct FwdArgs {
+    const uint32_t* fold_start;
+    const uint32_t* fold_list;
+    const uint32_t* chain;
+    SwapConst sc;
+    PlaneList fwd;
+    int zero_ghost_force;
+};
+// initial_integration (+ optional fused force zeroing, displacement check
+// and forward comm).  pbc_mask: bit d set for a periodic axis d (7: the
+// fully periodic test).  fw NULL: no forward comm.
 void launch_initial(cudaStream_t st, uint64_t n, const AtomCols& c, double dt, bool zero_force,
                     const double* lbx, const double* lby, const double* lbz, uint64_t n_check,
-                    double thr_sq, const double box[3], DevFlags* flags, int pbc_mask = 7);
+                    double thr_sq, const double box[3], DevFlags* flags, int pbc_mask = 7,
+                    const FwdArgs* fw = nullptr);
 // final_integration
 void launch_final(cudaStream_t st, uint64_t n, const AtomCols& c, double dt);
 // final_integration of step t fused with initial_integration of step t+1
 void launch_final_initial(cudaStream_t st, uint64_t n, const AtomCols& c, double dt,
                           bool zero_force, const double* lbx, const double* lby,
                           const double* lbz, uint64_t n_check, double thr_sq,
-                          const double box[3], DevFlags* flags, int pbc_mask = 7);
+                          const double box[3], DevFlags* flags, int pbc_mask = 7,
+                          const FwdArgs* fw = nullptr);
 // zero_all_forces over [0, n) + the #[zero] planes
 void launch_zero_forces(cudaStream_t st, uint64_t n, const AtomCols& c, const int* zero_planes,
                         int nzero);
@@ -238,6 +267,70 @@ void launch_in_scatter(cudaStream_t st, uint64_t nlocal, const uint32_t* offsets
                        const uint32_t* indices, uint32_t* cursor, uint32_t* in_list);
 
 // ---- force (k_force.cu) ---------------------------------------------------
+// Grouped partner sequences of the built-in consumer.  Atom a's sequence is
+// its contributions in the reference's force-sum order (in-list rows below
+// a, a's own row, in-list rows above a; ghosts only receive with newton).
+// Root t's group is t's sequence, then those of its ghost images in fold
+// order (fold_start / fold_list of the last border pass).
+struct SeqArgs {
+    uint64_t nlocal, ntotal;
+    int newton;
+    const uint32_t* offsets;
+    const uint32_t* indices;
+    const uint32_t* in_start;
+    const uint32_t* in_list;
+    const uint32_t* fold_start;
+    const uint32_t* fold_list;
+};
+// cnt[a] = length of a's sequence (a < ntotal); grp[t] = length of t's group
+void launch_seq_count(cudaStream_t st, const SeqArgs& q, uint32_t* cnt, uint32_t* grp);
+// seq[grp_start[t] ...] = t's group; owner[k] = (t & 31) | item << 5 (item 0:
+// the root, item j: its j-th image).  Roots have at most 7 images.
+void launch_seq_fill(cudaStream_t st, const SeqArgs& q, const uint32_t* grp_start, uint32_t* seq,
+                     uint8_t* owner);
+struct ForceArgs {
+    AtomCols c;
+    const double* rad;
+    double K;
+    uint64_t nlocal;
+    const uint32_t* grp_start;  // nlocal + 1
+    const uint32_t* cnt;        // per atom
+    const uint32_t* seq;
+    const uint8_t* owner;
+    const uint32_t* fold_start;
+    const uint32_t* fold_list;
+    PlaneList rev;              // #[reverse] planes folded with the forces
+};
+// The built-in consumer over the grouped sequences (warp-cooperative): F of
+// every local and ghost is overwritten; with fold, ghost forces (and the
+// #[reverse] planes) are then folded into their roots as reverse comm does.
+void launch_force_seq(cudaStream_t st, const ForceArgs& p, bool fold);
+
+// ---- device-resident steps (k_steps.cu) --------------------------------------
+// Grid barrier words (count must be 0 when a launch starts).
+struct GridBar {
+    unsigned count;
+    unsigned gen;
+};
+constexpr uint32_t SOIL_STEPS_ERR_BARRIER = 4u;  // flags->error: a barrier wait ran out
+struct StepsArgs {
+    AtomCols c;
+    uint64_t nlocal;
+    double dt;
+    int zero_force;    // zero the locals' forces in the integration pass
+    int first_fused;   // the first step's pass also applies the pending final half-kick
+    CheckArgs ck;      // the displacement check (every step)
+    FwdArgs fw;        // forward comm of every step
+    ForceArgs fa;      // the grouped consumer (consumer != 0)
+    uint64_t max_steps;
+    GridBar* bar;
+    DevFlags* flags;   // flags->rebuild must be 0 at launch
+    uint32_t* out;     // out[0]: steps completed; out[1]: 1 if the next step's check tripped
+};
+// Cooperative grid for k_steps (consumer: 0 none, 1 grouped, 2 grouped + fold).
+int steps_grid(int consumer, uint64_t nlocal, int* grid);
+cudaError_t launch_steps(cudaStream_t st, const StepsArgs& a, int consumer, int grid);
+
 void launch_harmonic(cudaStream_t st, uint64_t nlocal, uint64_t ntotal, const AtomCols& c,
                      const double* radius, double k, int newton, const uint32_t* offsets,
                      const uint32_t* indices, const uint32_t* in_start, const uint32_t* in_list);

@@ -17,10 +17,12 @@
 // runs on the device.  The host reads back a few words where the reference
 // branches on data: the displacement flag, the identity flag of a periodic
 // sort, ghost totals and the pair total of a rebuild.
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -982,6 +984,12 @@ int borders_done(soil_sys* s, const uint32_t* hb, const BorderDim bds[3]) {
     s->last_nghost = s->nghost;
     s->border_gen += 1;
     s->nswaps = kNumSwaps;
+    // A local has images on both sides of a periodic dim only when the two
+    // face slabs overlap; otherwise it has at most 7 images.
+    const int mask = pbc_mask(s);
+    s->few_images = true;
+    for (int d = 0; d < 3; ++d)
+        if ((mask & (1 << d)) && bds[d].thresh_lo > bds[d].thresh_hi) s->few_images = false;
     return SOIL_OK;
 }
 
@@ -1024,6 +1032,73 @@ int build_in_lists(soil_sys* s) {
     TRY(check_launch(s));
     s->in_lists_valid = true;
     return SOIL_OK;
+}
+
+// The built-in consumer's grouped partner sequences (from the CSR, the
+// transposed lists and the fold program): one entry per (atom, contribution),
+// 2 per pair with newton.
+int build_seq(soil_sys* s) {
+    const uint64_t total = s->nlocal + s->nghost, nl = s->nlocal;
+    const uint64_t room = 2 * pair_room(s->npairs);
+    TRY(ensure(s, s->seq_cnt, total + 1, 0, s->acap + 1));
+    TRY(ensure(s, s->grp_cnt, nl + 1, 0, s->acap + 1));
+    TRY(ensure(s, s->grp_start, nl + 2, 0, s->acap + 2));
+    TRY(ensure(s, s->seq, 2 * s->npairs + 1, 0, room));
+    TRY(ensure(s, s->seq_owner, 2 * s->npairs + 1, 0, room));
+    TRY(ensure(s, s->scan_tmp, scan_temp_words(total + 2)));
+    SeqArgs q;
+    q.nlocal = nl;
+    q.ntotal = total;
+    q.newton = s->newton ? 1 : 0;
+    q.offsets = s->offsets.p;
+    q.indices = s->indices.p;
+    q.in_start = s->in_start.p;
+    q.in_list = s->in_list.p;
+    q.fold_start = s->fold_start.p;
+    q.fold_list = s->fold_list.p;
+    launch_seq_count(s->st, q, s->seq_cnt.p, s->grp_cnt.p);
+    exclusive_scan_u32(s->st, s->grp_cnt.p, s->grp_start.p, nl, s->scan_tmp.p);
+    launch_seq_fill(s->st, q, s->grp_start.p, s->seq.p, s->seq_owner.p);
+    TRY(check_launch(s));
+    s->seq_valid = true;
+    return SOIL_OK;
+}
+
+// Whether the grouped consumer serves this system: the built-in consumer,
+// and a ghost layout in which no local has images on both sides of a dim
+// (at most 7 images per root, what the sequences' owner byte encodes).
+bool seq_consumer(const soil_sys* s) { return builtin_consumer(s) && s->few_images; }
+
+ForceArgs consumer_args(const soil_sys* s) {
+    ForceArgs p;
+    p.c = s->A;
+    p.rad = s->A.planes[s->cols[s->radius_col].plane0];
+    p.K = s->harmonic_k;
+    p.nlocal = s->nlocal;
+    p.grp_start = s->grp_start.p;
+    p.cnt = s->seq_cnt.p;
+    p.seq = s->seq.p;
+    p.owner = s->seq_owner.p;
+    p.fold_start = s->fold_start.p;
+    p.fold_list = s->fold_list.p;
+    zero_planes_of(s, SOIL_COL_REVERSE, p.rev.idx, &p.rev.n);
+    return p;
+}
+
+// The built-in consumer; with fold (newton), reverse comm of the forces and
+// #[reverse] planes is done in the same kernel.
+int launch_consumer(soil_sys* s, bool fold) {
+    if (!s->in_lists_valid) TRY(build_in_lists(s));
+    if (!seq_consumer(s)) {
+        launch_harmonic(s->st, s->nlocal, s->nlocal + s->nghost, s->A,
+                        s->A.planes[s->cols[s->radius_col].plane0], s->harmonic_k,
+                        s->newton ? 1 : 0, s->offsets.p, s->indices.p, s->in_start.p,
+                        s->in_list.p);
+        return check_launch(s);
+    }
+    if (!s->seq_valid) TRY(build_seq(s));
+    launch_force_seq(s->st, consumer_args(s), fold);
+    return check_launch(s);
 }
 
 // bin_neighbor_list (neighbor.rs:1013-1319), host part: the CommState
@@ -1141,8 +1216,10 @@ int phase_neighbor(soil_sys* s) {
     s->npairs = np;
     s->rebuilds += 1;
     s->in_lists_valid = false;
+    s->seq_valid = false;
     // the transposed lists serve the built-in consumer and any force hook
     if (builtin_consumer(s) || s->hook) TRY(build_in_lists(s));
+    if (seq_consumer(s)) TRY(build_seq(s));
     return SOIL_OK;
 }
 
@@ -1195,11 +1272,7 @@ int phase_force(soil_sys* s) {
         return check_launch(s);
     }
     if (!builtin_consumer(s)) return SOIL_OK;
-    if (!s->in_lists_valid) TRY(build_in_lists(s));
-    launch_harmonic(s->st, s->nlocal, s->nlocal + s->nghost, s->A,
-                    s->A.planes[s->cols[s->radius_col].plane0], s->harmonic_k, s->newton ? 1 : 0,
-                    s->offsets.p, s->indices.p, s->in_start.p, s->in_list.p);
-    return check_launch(s);
+    return launch_consumer(s, false);
 }
 
 int phase_reverse_comm(soil_sys* s) {
@@ -1229,13 +1302,52 @@ int phase_final(soil_sys* s) {
     return check_launch(s);
 }
 
-// One full timestep.  Fusions that keep every result bit-identical:
-//  - force zeroing folded into initial (locals) and forward comm (ghosts),
-//    or dropped when the built-in consumer overwrites every force;
-//  - the displacement check folded into the initial integration pass;
-//  - final(t) folded into initial(t+1) when nothing touches velocities
-//    between them (the streaming profile of the first shear step does).
-int full_step(soil_sys* s, bool last) {
+// Forward comm may run inside the integration pass: the step starts with
+// valid lists and ghosts (CommunicateOnly), and nothing between the
+// integration and forward comm moves atoms or changes the box or the swap
+// offsets (no deform, shear or shrink-wrap).
+bool fused_forward_ok(const soil_sys* s) {
+    if (s->state != COMMUNICATE_ONLY || s->nghost == 0 || s->nswaps == 0) return false;
+    if (s->shear || has_axis_deform(s)) return false;
+    for (int d = 0; d < 3; ++d)
+        if (s->btype[d] == SOIL_BOUNDARY_SHRINK) return false;
+    return true;
+}
+
+// What the integration pass of a step decided, for the rest of the step.
+struct StepPlan {
+    bool overwrite;   // the built-in consumer overwrites every force
+    bool fused_zero;  // forces zeroed in the integration pass (and forward comm)
+    bool check;       // the displacement check ran in the integration pass
+    bool fwd_fused;   // forward comm ran in the integration pass
+    int nz;           // #[zero] planes
+};
+
+StepPlan plan_step(const soil_sys* s) {
+    StepPlan p;
+    p.overwrite = builtin_consumer(s);
+    int zp[kMaxPlanes];
+    zero_planes_of(s, SOIL_COL_ZERO, zp, &p.nz);
+    p.fused_zero = !p.overwrite && p.nz == 0;
+    p.check = s->state == COMMUNICATE_ONLY && displacement_needed(s);
+    p.fwd_fused = fused_forward_ok(s);
+    return p;
+}
+
+FwdArgs fwd_args(const soil_sys* s, bool fused_zero) {
+    FwdArgs fw;
+    fw.fold_start = s->fold_start.p;
+    fw.fold_list = s->fold_list.p;
+    fw.chain = s->ghost_chain.p;
+    fw.sc = swap_const(s);
+    zero_planes_of(s, SOIL_COL_FORWARD, fw.fwd.idx, &fw.fwd.n);
+    fw.zero_ghost_force = fused_zero ? 1 : 0;
+    return fw;
+}
+
+// The first part of a timestep: deform, then the integration pass with its
+// fused displacement check (and forward comm).
+int step_integrate(soil_sys* s, StepPlan* out) {
     const bool profile_now = s->deform_initialized && s->shear && !s->shear_initialized;
     if (profile_now && s->pending_final) {
         launch_final(s->st, s->nlocal, s->A, s->dt);
@@ -1243,27 +1355,38 @@ int full_step(soil_sys* s, bool last) {
     }
     timer_begin(s, T_INTEGRATE);
     TRY(phase_deform(s));
-    const bool overwrite = builtin_consumer(s);
-    int zp[kMaxPlanes], nz;
-    zero_planes_of(s, SOIL_COL_ZERO, zp, &nz);
-    const bool fused_zero = !overwrite && nz == 0;
-    const bool check = s->state == COMMUNICATE_ONLY && displacement_needed(s);
-    if (check) CK(cudaMemsetAsync(&s->dflags->rebuild, 0, 4, s->st));
+    const StepPlan p = plan_step(s);
+    if (p.check) CK(cudaMemsetAsync(&s->dflags->rebuild, 0, 4, s->st));
+    // Forward comm rides on the integration pass when this step keeps its
+    // lists unless the displacement check trips (ghost images written from
+    // their roots' new positions; a step that rebuilds replaces them).
+    FwdArgs fw;
+    if (p.fwd_fused) fw = fwd_args(s, p.fused_zero);
     if (s->pending_final)
-        launch_final_initial(s->st, s->nlocal, s->A, s->dt, fused_zero,
-                             check ? s->lbx.p : nullptr, s->lby.p, s->lbz.p, s->nlocal,
-                             displacement_threshold_sq(s), s->pbc_box, s->dflags, pbc_mask(s));
+        launch_final_initial(s->st, s->nlocal, s->A, s->dt, p.fused_zero,
+                             p.check ? s->lbx.p : nullptr, s->lby.p, s->lbz.p, s->nlocal,
+                             displacement_threshold_sq(s), s->pbc_box, s->dflags, pbc_mask(s),
+                             p.fwd_fused ? &fw : nullptr);
     else
-        launch_initial(s->st, s->nlocal, s->A, s->dt, fused_zero, check ? s->lbx.p : nullptr,
+        launch_initial(s->st, s->nlocal, s->A, s->dt, p.fused_zero, p.check ? s->lbx.p : nullptr,
                        s->lby.p, s->lbz.p, s->nlocal, displacement_threshold_sq(s), s->pbc_box,
-                       s->dflags, pbc_mask(s));
+                       s->dflags, pbc_mask(s), p.fwd_fused ? &fw : nullptr);
     s->pending_final = false;
     TRY(check_launch(s));
     timer_end(s, T_INTEGRATE);
+    *out = p;
+    return SOIL_OK;
+}
+
+// The rest of a timestep after its integration pass: decide_rebuild, the
+// rebuild phases when due, forward comm, the consumer, reverse comm and the
+// final half-kick (applied now when `last`, else deferred into the next
+// step's integration pass).
+int step_rest(soil_sys* s, const StepPlan& p, bool last) {
     // decide_rebuild
     if (s->state == COMMUNICATE_ONLY) {
         bool disp = false;
-        if (check) {
+        if (p.check) {
             TRY(read_flags(s));
             disp = s->hflags->rebuild != 0;
         }
@@ -1272,7 +1395,7 @@ int full_step(soil_sys* s, bool last) {
     }
     TRY(phase_remove_ghosts(s));
     timer_begin(s, T_ZERO);
-    if (!fused_zero && (nz > 0 || !overwrite)) TRY(phase_zero_forces(s));
+    if (!p.fused_zero && (p.nz > 0 || !p.overwrite)) TRY(phase_zero_forces(s));
     timer_end(s, T_ZERO);
     timer_begin(s, T_PBC);
     TRY(phase_shrink_wrap(s));
@@ -1285,16 +1408,25 @@ int full_step(soil_sys* s, bool last) {
     TRY(phase_borders(s));
     timer_end(s, T_BORDERS);
     timer_begin(s, T_FORWARD);
-    if (s->state == COMMUNICATE_ONLY) TRY(forward_comm(s, fused_zero));
+    if (s->state == COMMUNICATE_ONLY && !p.fwd_fused) TRY(forward_comm(s, p.fused_zero));
     timer_end(s, T_FORWARD);
     timer_begin(s, T_NEIGHBOR);
     TRY(phase_neighbor(s));
     timer_end(s, T_NEIGHBOR);
+    // With newton, the grouped consumer folds ghost forces into their roots
+    // in the same kernel (reverse_send_force's fold order); otherwise the
+    // force and reverse-comm phases run apart.
+    const bool fold_fused = !s->hook && seq_consumer(s) && s->newton;
     timer_begin(s, T_FORCE);
-    TRY(phase_force(s));
+    if (fold_fused) {
+        TRY(launch_consumer(s, true));
+        s->reverse_gen = s->border_gen;
+    } else {
+        TRY(phase_force(s));
+    }
     timer_end(s, T_FORCE);
     timer_begin(s, T_REVERSE);
-    TRY(phase_reverse_comm(s));
+    if (!fold_fused) TRY(phase_reverse_comm(s));
     timer_end(s, T_REVERSE);
     if (last) {
         timer_begin(s, T_FINAL);
@@ -1303,6 +1435,136 @@ int full_step(soil_sys* s, bool last) {
     } else {
         s->pending_final = true;
         s->steps_done += 1;
+    }
+    return SOIL_OK;
+}
+
+// One full timestep.  Fusions that keep every result bit-identical:
+//  - force zeroing folded into initial (locals) and forward comm (ghosts),
+//    or dropped when the built-in consumer overwrites every force;
+//  - the displacement check folded into the initial integration pass;
+//  - final(t) folded into initial(t+1) when nothing touches velocities
+//    between them (the streaming profile of the first shear step does);
+//  - forward comm folded into the integration pass (fused_forward_ok);
+//  - reverse comm folded into the built-in consumer (newton, grouped
+//    sequences).
+int full_step(soil_sys* s, bool last) {
+    StepPlan p;
+    TRY(step_integrate(s, &p));
+    return step_rest(s, p, last);
+}
+
+// ---- device-resident steps -------------------------------------------------
+
+// Steps that may run inside one k_steps launch from the current state: the
+// step keeps its lists exactly when its displacement check passes (every = 0
+// with the check on), nothing else a step does needs the host (no hook, no
+// deform, shear or shrink-wrap, no #[zero] planes, #[reverse] planes only
+// with the folding consumer, no phase timers), the built-in consumer (if
+// any) runs on grouped sequences, and no periodic sort falls due.  0: none.
+uint64_t resident_limit(const soil_sys* s, uint64_t want) {
+    const char* env = std::getenv("SOIL_RESIDENT_STEPS");
+    const int mode = env ? std::atoi(env) : 2;  // 0 off, 1 always, 2 auto
+    if (mode == 0) return 0;
+    if (mode == 2 && s->nlocal > kResidentAutoMaxAtoms) return 0;
+    if (s->hook || s->timing_mask || !s->check || s->every != 0) return 0;
+    if (s->state != COMMUNICATE_ONLY || !displacement_needed(s) || needs_rebuild_with(s, false))
+        return 0;
+    if (!fused_forward_ok(s)) return 0;
+    const bool consumer = builtin_consumer(s);
+    if (consumer && !seq_consumer(s)) return 0;
+    int idx[kMaxPlanes], nz, nr;
+    zero_planes_of(s, SOIL_COL_ZERO, idx, &nz);
+    zero_planes_of(s, SOIL_COL_REVERSE, idx, &nr);
+    if (nz > 0 || (nr > 0 && !(consumer && s->newton))) return 0;
+    uint64_t lim = want;
+    if (s->sort_every > 0) {
+        if (s->sort_counter + 1 >= s->sort_every) return 0;
+        lim = std::min<uint64_t>(lim, s->sort_every - s->sort_counter - 1);
+    }
+    return lim;
+}
+
+// Up to `max` communicate-only steps in one launch; *done of them complete.
+// *tripped: the next step's integration pass also ran and its displacement
+// check tripped (that step continues on the host from decide_rebuild, with
+// *plan).
+int resident_steps(soil_sys* s, uint64_t max, uint64_t* done, bool* tripped, StepPlan* plan) {
+    const StepPlan p = plan_step(s);
+    const bool consumer = builtin_consumer(s);
+    StepsArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.c = s->A;
+    a.nlocal = s->nlocal;
+    a.dt = s->dt;
+    a.zero_force = p.fused_zero ? 1 : 0;
+    a.first_fused = s->pending_final ? 1 : 0;
+    a.ck = make_check(s->lbx.p, s->lby.p, s->lbz.p, s->nlocal, displacement_threshold_sq(s),
+                      s->pbc_box, s->dflags, pbc_mask(s));
+    a.fw = fwd_args(s, p.fused_zero);
+    int kind = 0;
+    if (consumer) {
+        if (!s->in_lists_valid) TRY(build_in_lists(s));
+        if (!s->seq_valid) TRY(build_seq(s));
+        a.fa = consumer_args(s);
+        kind = s->newton ? 2 : 1;
+    }
+    a.max_steps = max;
+    TRY(ensure(s, s->rstate, 4));
+    a.bar = reinterpret_cast<GridBar*>(s->rstate.p);
+    a.out = s->rstate.p + 2;
+    a.flags = s->dflags;
+    int grid = 0;
+    if (steps_grid(kind, s->nlocal, &grid))
+        return fail(s->ctx, SOIL_ERR_CUDA, "no cooperative occupancy for the resident steps");
+    CK(cudaMemsetAsync(s->rstate.p, 0, 4 * 4, s->st));
+    CK(cudaMemsetAsync(&s->dflags->rebuild, 0, 4, s->st));
+    CK(cudaMemsetAsync(&s->dflags->error, 0, 4, s->st));
+    CK(launch_steps(s->st, a, kind, grid));
+    CK(cudaMemcpyAsync(s->hword, a.out, 8, cudaMemcpyDeviceToHost, s->st));
+    TRY(read_flags(s));
+    if (s->hflags->error & SOIL_STEPS_ERR_BARRIER)
+        return fail(s->ctx, SOIL_ERR_CUDA, "resident steps: a grid barrier wait ran out");
+    *done = s->hword[0];
+    *tripped = s->hword[1] != 0;
+    if (*done > max || (!*tripped && *done != max))
+        return fail(s->ctx, SOIL_ERR_CUDA, "resident steps: inconsistent step count");
+    s->steps_done += *done;
+    s->steps_since_build += *done;
+    if (s->sort_every > 0) s->sort_counter += *done;
+    // every completed step leaves its final half-kick pending; a tripped
+    // step's integration pass applied the last one
+    s->pending_final = !*tripped;
+    *plan = p;
+    plan->check = true;
+    plan->fwd_fused = true;
+    return SOIL_OK;
+}
+
+// soil_step: communicate-only stretches run resident when resident_limit
+// allows (at least two steps), every other step through full_step.
+int step_many(soil_sys* s, uint64_t n) {
+    uint64_t k = 0;
+    while (k < n) {
+        const uint64_t lim = resident_limit(s, n - k);
+        if (lim >= 2) {
+            uint64_t done = 0;
+            bool tripped = false;
+            StepPlan p;
+            TRY(resident_steps(s, lim, &done, &tripped, &p));
+            k += done;
+            if (tripped) {  // step k + 1: integrated, its check tripped
+                TRY(step_rest(s, p, k + 1 == n));
+                k += 1;
+            } else if (k == n) {  // the call ends on a resident step
+                launch_final(s->st, s->nlocal, s->A, s->dt);
+                s->pending_final = false;
+                TRY(check_launch(s));
+            }
+            continue;
+        }
+        TRY(full_step(s, k + 1 == n));
+        k += 1;
     }
     return SOIL_OK;
 }
@@ -1462,6 +1724,8 @@ int soil_sys_destroy(soil_sys* s) {
     fr(s->fold_roots); fr(s->fold_nroots);
     for (int k = 0; k < 2; ++k) { fr(s->slot_tag[k]); fr(s->slot_val[k]); }
     fr(s->in_count); fr(s->in_start); fr(s->in_cursor); fr(s->in_list);
+    fr(s->seq_cnt); fr(s->grp_cnt); fr(s->grp_start); fr(s->seq); fr(s->seq_owner);
+    fr(s->rstate);
     fr(s->ghost_root); fr(s->ghost_chain);
     fr(s->fold_start); fr(s->fold_list);
     for (auto& a : s->send) fr(a);
@@ -1640,6 +1904,7 @@ int soil_sys_set_harmonic(soil_sys* s, double k, int32_t radius_col) {
     s->harmonic_k = k;
     s->radius_col = radius_col;
     s->in_lists_valid = false;
+    s->seq_valid = false;
     return SOIL_OK;
 }
 
@@ -1655,8 +1920,7 @@ int soil_step(soil_sys* s, uint64_t nsteps) {
     if (!s) return SOIL_ERR_INVALID;
     if (!s->setup_done) return fail(s->ctx, SOIL_ERR_STATE, "soil_sys_setup has not run");
     if (s->batch) return fail(s->ctx, SOIL_ERR_STATE, "a batched system steps through its batch");
-    for (uint64_t k = 0; k < nsteps; ++k) TRY(full_step(s, k + 1 == nsteps));
-    return SOIL_OK;
+    return step_many(s, nsteps);
 }
 
 int soil_sys_sync(soil_sys* s) {

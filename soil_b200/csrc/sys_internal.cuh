@@ -136,6 +136,13 @@ struct soil_sys {
     int slot_old = 0;
     DArr<float4> spf;
     DArr<uint32_t> in_count, in_start, in_cursor, in_list;
+    // grouped partner sequences of the built-in consumer (rebuilt with the
+    // lists): per-atom lengths, per-root group lengths and starts, entries
+    DArr<uint32_t> seq_cnt, grp_cnt, grp_start, seq;
+    DArr<uint8_t> seq_owner;
+    bool seq_valid = false;
+    bool few_images = false;  // no local has images on both sides of a dim (<= 7 images)
+    DArr<uint32_t> rstate;    // resident steps: grid barrier words, step count, trip flag
     DArr<uint32_t> ghost_root, ghost_chain;
     DArr<uint32_t> fold_start, fold_list;  // reverse-comm fold program (written by borders)
     DArr<uint32_t> send[kNumSwaps];
@@ -248,5 +255,8 @@ bool needs_rebuild_with(const soil_sys* s, bool disp);
 bool displacement_needed(const soil_sys* s);
 SwapConst swap_const(const soil_sys* s);
 constexpr int kRowSlotsPerAtom = 16;
+// Largest system that takes the device-resident light steps by default
+// (SOIL_RESIDENT_STEPS=1 forces them on at any size, 0 off).
+constexpr uint64_t kResidentAutoMaxAtoms = 1ull << 20;
 
 }  // namespace soil_host
