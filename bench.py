@@ -16,7 +16,11 @@ with --gpus N every rank runs an independent replica; `value` is the
 atom-steps of all ranks over the slowest rank's device time (weak scaling).
 
 Printed JSON keys beyond the base contract:
-  neighbor_builds_per_s  rebuilds inside the timed region / its duration
+  timed_steps            light and rebuild steps inside the timed region
+  ms_per_light_step, ms_per_rebuild_step
+                         measured past the timed region until >= 3 rebuilds
+  ms_per_step_at_rebuild_rate, neighbor_builds_per_s
+                         the two mixed at the rebuild rate seen there
   roofline               dominant kernel: algorithmic bytes / mean launch time
   cpu_baseline           the CPU oracle on a bounded sample of the same system
   e2e                    the same metric through the C ABI from pinned host
@@ -40,23 +44,33 @@ import numpy as np  # noqa: E402
 from soil_b200 import abi, dist, workloads  # noqa: E402
 
 # Algorithmic bytes per unit of each timed phase (FP64 SoA; one read or
-# write of each value the phase must touch).
+# write of each value the phase must touch).  c: the system's counts, fw: f64
+# width of the #[forward] columns.
 #   integrate: final(t) fused with initial(t+1) + displacement check:
-#              R x,v,F,inv_m (80) + R last-build pos (24) + W x,v (48) = 152 B/local
-#   force:     R pos+radius of every atom (32) + W force (24) + R row/transposed
-#              offsets (8) + R 4 B per list entry (each pair is listed in a
-#              row and in a transposed row: 8 B per pair)
+#              R x,v,F,inv_m (80) + R last-build pos (24) + W x,v (48) = 152 B/local;
+#              with forward comm fused in (light steps): R fold_start (4) per
+#              local, and per ghost R fold_list + chain (8), W pos,vel (48),
+#              R+W forward columns (16 B per f64)
+#   force:     grouped consumer with the reverse fold: R x,y,z,radius (32) and
+#              W force (24) of every atom, R group/fold/count metadata (12 B
+#              per local, 8 B per ghost), R 5 B per sequence entry (2 entries
+#              per pair), and the fold R ghost F (24) + R origin (4) + RMW
+#              owner F (48) per ghost
 #   forward:   R root+chain (8) + R root pos,vel (48) + W pos,vel (48)
 #              + forward columns (16 B per f64) per ghost
 #   reverse:   R send index (4) + R ghost F (24) + RMW owner F (48) per ghost
 #   final:     80 B/local
 BYTES_PER_UNIT = {
-    "integrate": lambda c, fw: 152 * c.nlocal,
+    "integrate": lambda c, fw: 156 * c.nlocal + (56 + 16 * fw) * c.nghost,
     "final": lambda c, fw: 80 * c.nlocal,
-    "force": lambda c, fw: 64 * (c.nlocal + c.nghost) + 8 * c.npairs,
+    "force": lambda c, fw: (60 * (c.nlocal + c.nghost) + 12 * c.nlocal + 8 * c.nghost
+                            + 10 * c.npairs + 76 * c.nghost),
     "forward": lambda c, fw: (104 + 16 * fw) * c.nghost,
     "reverse": lambda c, fw: 76 * c.nghost,
 }
+# The kernel each timed phase launches on a light step (ncu names).
+PHASE_KERNEL = {"integrate": "k_initial", "force": "k_force_seq", "final": "k_final",
+                "forward": "k_forward", "reverse": "k_reverse_fold_roots"}
 
 
 def log(*a):
@@ -73,16 +87,17 @@ def load_peaks():
 
 
 def load_traffic(kernel, workload):
-    """DRAM bytes per atom of `kernel` from a committed ncu summary, if any."""
+    """DRAM bytes per atom of `kernel` (its ncu name) from a committed ncu
+    summary of that kernel on `workload`, if any."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if not os.path.exists(p):
         return None
     with open(p) as f:
         d = json.load(f)
-    e = d.get(kernel)
-    if not e or e.get("workload") != workload:
-        return None
-    return e
+    for e in d.values():
+        if e.get("kernel") == kernel and e.get("workload") == workload:
+            return e
+    return None
 
 
 class ClockSampler:
@@ -160,6 +175,51 @@ def make_workload(name, filt, natoms=None):
         desc = ("C2 large single system: 4,194,304 polydisperse spheres r~U[0.4,0.6], "
                 "phi 0.50, harmonic k=1e3, dt 1e-4")
     return w, desc
+
+
+def rebuild_probe(s, stream, min_rebuilds=3, chunk=25, max_steps=800):
+    """Light and rebuild step costs of a system past the timed region.
+
+    Steps it in calls of `chunk` steps, each timed with CUDA events on the
+    library's stream, until at least `min_rebuilds` steps rebuilt the lists;
+    then fits chunk_ms = L * steps + X * rebuilds over the chunks (least
+    squares): L is the light (communicate-only) step, L + X the rebuild step.
+    Each call ends with the final half-kick (as every soil_step call does),
+    so L carries 1/chunk of one final_integration pass."""
+    import torch
+    rows = []
+    steps = rebuilds = 0
+    while steps < max_steps and (rebuilds < min_rebuilds or len(rows) < 3):
+        r0 = s.counts().rebuilds
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.step(chunk)
+        e1.record(stream)
+        s.sync()
+        r = int(s.counts().rebuilds - r0)
+        rows.append((chunk, r, e0.elapsed_time(e1)))
+        steps += chunk
+        rebuilds += r
+    A = np.array([[n, r] for n, r, _ in rows], dtype=np.float64)
+    t = np.array([ms for _, _, ms in rows])
+    out = {"steps": steps, "rebuilds": rebuilds, "chunk_steps": chunk,
+           "rebuild_rate": rebuilds / steps}
+    if rebuilds and np.linalg.matrix_rank(A) == 2:
+        (light, extra), *_ = np.linalg.lstsq(A, t, rcond=None)
+        out.update(ms_per_light_step=float(light), ms_per_rebuild_step=float(light + extra))
+    elif rebuilds == steps:  # every step rebuilds (shear)
+        out.update(ms_per_light_step=None, ms_per_rebuild_step=float(t.sum() / steps))
+    else:
+        out.update(ms_per_light_step=float(t.sum() / steps), ms_per_rebuild_step=None)
+    L, R = out["ms_per_light_step"], out["ms_per_rebuild_step"]
+    rate = out["rebuild_rate"]
+    if L is not None and R is not None:
+        out["ms_per_step_at_rebuild_rate"] = (1 - rate) * L + rate * R
+    else:
+        out["ms_per_step_at_rebuild_rate"] = L if R is None else R
+    out["neighbor_builds_per_s"] = rate / (out["ms_per_step_at_rebuild_rate"] * 1e-3)
+    return out
 
 
 def cpu_baseline(w, budget_s=20.0, max_steps=10000, warmup=0):
@@ -259,18 +319,23 @@ def run_soil(args, world, rank, local):
     per_launch_ms = ms_dom[k] / max(launches_dom[k], 1)
     alg_bytes = BYTES_PER_UNIT[dominant](c1, fwd_width)
     achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
-    tr = load_traffic(dominant, args.config)
+    tr = load_traffic(PHASE_KERNEL.get(dominant), args.config)
     traffic = None
     if tr:
         traffic = tr["dram_bytes_per_atom"] * (c1.nlocal if dominant in ("integrate", "final")
                                                else c1.nlocal + c1.nghost)
-    roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
+    roofline = {"bound": "hbm", "kernel": PHASE_KERNEL.get(dominant, dominant), "phase": dominant,
+                "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                 "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
                 "mean_launch_ms": per_launch_ms, "launches": int(launches_dom[k])}
 
     # per-phase breakdown (warm-up steps) for the record
     phases = {abi.TIMER_NAMES[t]: round(ms0[t], 4) for t in range(abi.SOIL_NUM_TIMERS) if iv0[t]}
+    # the rebuild half of the metric: light and rebuild steps past the timed
+    # region, until at least three rebuilds
+    s.set_timing(0)
+    probe = rebuild_probe(s, stream)
     del s
 
     e2e = None
@@ -293,8 +358,15 @@ def run_soil(args, world, rank, local):
                        "l2": "inputs larger than L2 (per-atom state ~%d MB)" %
                              (c1.nlocal * 200 // 2**20),
                        "ghosts": int(c1.nghost), "pairs": int(c1.npairs)},
-            "neighbor_builds_per_s": world * rebuilds / (ms_max * 1e-3),
+            "timed_steps": {"light": args.steps - rebuilds, "rebuild": rebuilds},
+            "neighbor_builds_per_s": world * probe["neighbor_builds_per_s"],
+            "neighbor_builds_in_timed_region_per_s": world * rebuilds / (ms_max * 1e-3),
             "rebuilds": rebuilds,
+            "ms_per_light_step": probe["ms_per_light_step"],
+            "ms_per_rebuild_step": probe["ms_per_rebuild_step"],
+            "ms_per_step_at_rebuild_rate": probe["ms_per_step_at_rebuild_rate"],
+            "rebuild_probe": {k: probe[k] for k in ("steps", "rebuilds", "chunk_steps",
+                                                    "rebuild_rate")},
             "roofline": roofline,
             "cpu_baseline": cb,
             "e2e": e2e,
