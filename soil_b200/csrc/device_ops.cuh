@@ -165,26 +165,23 @@ struct Filter {
         }
     }
 
-    // The reference pair test for the candidate in sorted slot m; *rechk counts
-    // FP64 re-tests in FP32 mode.
-    __device__ __forceinline__ bool operator()(const PairParams& p, const double4& pi,
-                                               const float4& pif, uint32_t m,
-                                               uint32_t* rechk) const {
-        if (FP32) {
-            const float4 q = p.spf[m];
-            const float dx = q.x - pif.x;
-            const float dy = q.y - pif.y;
-            const float dz = q.z - pif.z;
-            const float r2 = dx * dx + dy * dy + dz * dz;
-            float lim = lim_uniform;
-            if (!UNIFORM) {
-                const float cu = (pif.w + q.w) * sf32 + eps32;
-                lim = cu * cu;
-            }
-            if (r2 > lim) return false;
-            ++*rechk;
+    // FP32 prefilter: false only for candidates provably outside the cutoff.
+    __device__ __forceinline__ bool pass32(const float4& pif, const float4& q) const {
+        const float dx = q.x - pif.x;
+        const float dy = q.y - pif.y;
+        const float dz = q.z - pif.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        float lim = lim_uniform;
+        if (!UNIFORM) {
+            const float cu = (pif.w + q.w) * sf32 + eps32;
+            lim = cu * cu;
         }
-        const double4 q = p.sp[m];
+        return !(r2 > lim);
+    }
+
+    // The reference's FP64 test (neighbor.rs:1179-1303): nested FMA distance,
+    // uniform cut^2 or (s_i + s_j)^2 * sf^2.
+    __device__ __forceinline__ bool test64(const double4& pi, const double4& q) const {
         const double dx = q.x - pi.x;
         const double dy = q.y - pi.y;
         const double dz = q.z - pi.z;
@@ -192,6 +189,18 @@ struct Filter {
         if (UNIFORM) return r2 < cut_sq;
         const double sum_skin = pi.w + q.w;
         return r2 < sum_skin * sum_skin * sf_sq;
+    }
+
+    // The reference pair test for the candidate in sorted slot m; *rechk counts
+    // FP64 re-tests in FP32 mode.
+    __device__ __forceinline__ bool operator()(const PairParams& p, const double4& pi,
+                                               const float4& pif, uint32_t m,
+                                               uint32_t* rechk) const {
+        if (FP32) {
+            if (!pass32(pif, p.spf[m])) return false;
+            ++*rechk;
+        }
+        return test64(pi, p.sp[m]);
     }
 };
 

@@ -257,6 +257,29 @@ struct PairParams {
 // slots[i*K ...]; filter statistics into flags.
 void launch_pair_count(cudaStream_t st, const PairParams& p, uint32_t* rowcount, uint32_t* slots,
                        DevFlags* flags);
+// The stencil of a row as contiguous cell runs, in scan order: the own cell
+// first (when the stencil holds it), then the stencil offsets merged into
+// runs of consecutive cells.  A run of consecutive cells is a contiguous
+// range of sorted slots, for one row and for a tile of rows alike.
+// For staging, segments of consecutive cells merge into runs (the own cell
+// with a following +1 segment).
+constexpr int kMaxPairSegs = 24;
+struct PairSegs {
+    int n;                    // segments, own cell included
+    int own;                  // 1: segment 0 is the own cell
+    int32_t off[kMaxPairSegs];
+    int32_t len[kMaxPairSegs];
+    int32_t run[kMaxPairSegs];  // staging run of each segment
+    int nrun;
+    int32_t roff[kMaxPairSegs];
+    int32_t rlen[kMaxPairSegs];
+};
+// Pass 1 with every warp's candidate records staged in shared memory by bulk
+// copy (cp.async.bulk); tiles whose runs do not fit use the global-load scan.
+// Same outputs as launch_pair_count.  flags->error bit 8: a staging wait ran out.
+void launch_pair_count_staged(cudaStream_t st, const PairParams& p, const PairSegs& sg,
+                              uint32_t* rowcount, uint32_t* slots, DevFlags* flags);
+constexpr uint32_t SOIL_PAIRS_ERR_STAGING = 8u;
 // Pass 2: rows into neighbor_indices at offsets[] (rows longer than K re-derived).
 void launch_pair_fill(cudaStream_t st, const PairParams& p, const uint32_t* rowcount,
                       const uint32_t* slots, const uint32_t* offsets, uint32_t* indices);

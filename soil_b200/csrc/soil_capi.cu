@@ -1143,6 +1143,46 @@ int neighbor_plan(soil_sys* s) {
     return SOIL_OK;
 }
 
+// The stencil as segments of consecutive cells in scan order (the own cell
+// first); false when there are too many for the staged pair count (or
+// SOIL_PAIRS_STAGED=0), which then scans from global memory.
+bool pair_segments(const std::vector<int32_t>& sten, bool has_self, bool newton, PairSegs* sg) {
+    const char* env = std::getenv("SOIL_PAIRS_STAGED");
+    if (env && std::atoi(env) == 0) return false;
+    sg->n = 0;
+    sg->own = has_self ? 1 : 0;
+    if (has_self) {
+        sg->off[0] = 0;
+        sg->len[0] = 1;
+        sg->n = 1;
+    }
+    for (const int32_t off : sten) {
+        if (!newton && off == 0) continue;  // the own cell is scanned first
+        const int k = sg->n - 1;
+        if (k >= sg->own && sg->off[k] + sg->len[k] == off) {
+            sg->len[k] += 1;
+            continue;
+        }
+        if (sg->n == kMaxPairSegs) return false;
+        sg->off[sg->n] = off;
+        sg->len[sg->n] = 1;
+        sg->n += 1;
+    }
+    sg->nrun = 0;
+    for (int k = 0; k < sg->n; ++k) {
+        const int r = sg->nrun - 1;
+        if (r >= 0 && sg->roff[r] + sg->rlen[r] == sg->off[k]) {
+            sg->rlen[r] += sg->len[k];
+        } else {
+            sg->roff[sg->nrun] = sg->off[k];
+            sg->rlen[sg->nrun] = sg->len[k];
+            sg->nrun += 1;
+        }
+        sg->run[k] = sg->nrun - 1;
+    }
+    return true;
+}
+
 // Margin of the FP32 prefilter: FP32 coordinates are relative to the box
 // corner and M bounds their magnitude.
 float pair_eps(const soil_sys* s) {
@@ -1202,13 +1242,19 @@ int phase_neighbor(soil_sys* s) {
     p.eps32 = pair_eps(s);
     CK(cudaMemsetAsync(&s->dflags->candidates, 0, 16, s->st));
     CK(cudaMemsetAsync(&s->dflags->error, 0, 4, s->st));
-    launch_pair_count(s->st, p, s->rowcount.p, s->row_slots.p, s->dflags);
+    PairSegs sg;
+    if (pair_segments(sten, s->stencil_self, s->newton, &sg))
+        launch_pair_count_staged(s->st, p, sg, s->rowcount.p, s->row_slots.p, s->dflags);
+    else
+        launch_pair_count(s->st, p, s->rowcount.p, s->row_slots.p, s->dflags);
     exclusive_scan_u32(s->st, s->rowcount.p, s->offsets.p, nl, s->scan_tmp.p);
     CK(cudaMemcpyAsync(&s->hword[0], s->offsets.p + nl, 4, cudaMemcpyDeviceToHost, s->st));
     TRY(check_launch(s));
     TRY(read_flags(s));
     const uint64_t np = s->hword[0];
     TRY(ensure(s, s->indices, np + 1, 0, pair_room(np)));
+    if (s->hflags->error & SOIL_PAIRS_ERR_STAGING)
+        return fail(s->ctx, SOIL_ERR_CUDA, "pair build: a shared-memory staging wait ran out");
     if (s->hflags->error)
         return fail(s->ctx, SOIL_ERR_INVALID, "neighbor stencil left the bin grid (atom outside the ghost layers)");
     launch_pair_fill(s->st, p, s->rowcount.p, s->row_slots.p, s->offsets.p, s->indices.p);
