@@ -436,6 +436,7 @@ int fill_step(soil_batch* b, uint32_t k, bool post_flip, const BorderDim* bds) {
     }
     t.K = s->harmonic_k;
     t.max_tiles = 0;
+    t.segs_ok = pair_segments(sten, s->stencil_self, s->newton, &t.segs) ? 1 : 0;
     b->step_dirty[k] = 1;
     return SOIL_OK;
 }
@@ -554,6 +555,12 @@ int grow_slots(soil_batch* b, uint32_t need) {
     b->hot.resize(ncap);
     b->cap = ncap;
     return SOIL_OK;
+}
+
+// The staged pair count serves the batch unless SOIL_PAIRS_STAGED=0.
+bool pairs_staged_on() {
+    const char* env = std::getenv("SOIL_PAIRS_STAGED");
+    return !(env && std::atoi(env) == 0);
 }
 
 // ---- one step -------------------------------------------------------------------
@@ -813,7 +820,7 @@ int batch_step(soil_batch* b, bool last) {
     TRY(put_tables(b, g4));
     const int f_loc = stage_add(g4), s_fwd = stage_add(g4), n_cells = stage_add(g4),
               n_copy = stage_add(g4), n_bin = stage_add(g4), n_all = stage_add(g4),
-              n_rows = stage_add(g4);
+              n_rows = stage_add(g4), n_tiles = stage_add(g4);
     for (uint32_t k : M) {
         const auto& h = b->hot[k];
         if (!b->rebuild[k]) {
@@ -831,6 +838,7 @@ int batch_step(soil_batch* b, bool last) {
         }
         g4.spans[n_all].add_nz(k, nl + ng, 0);
         g4.spans[n_rows].add(k, nl, 0);
+        g4.spans[n_tiles].add_nz(k, (nl + 31) / 32, 0);
     }
     TRY(stage_commit(b, g4));
     tic(b);
@@ -844,7 +852,8 @@ int batch_step(soil_batch* b, bool last) {
         b_scatter(st, g4.out[n_all], a, true);
         b_segsort(st, g4.out[n_cells], a, BA_NEIGH_CELLS);
         b_sorted_views(st, g4.out[n_all], a);
-        b_pairs_rows(st, g4.out[f_loc], a);
+        if (pairs_staged_on()) b_pairs_staged(st, g4.out[n_tiles], a);
+        else b_pairs_rows(st, g4.out[f_loc], a);
         b_scan(st, g4.out[n_rows], a, BA_ROWS);
         toc(b, BT_NEIGHBOR);
         TRY(check_kernels(b));

@@ -89,6 +89,8 @@ struct BoxStep {
     SwapConst sc;
     double K;
     uint32_t max_tiles;
+    int segs_ok;   // the stencil fits PairSegs: the pair count stages its records
+    PairSegs segs;
 };
 
 struct Span {
@@ -144,6 +146,9 @@ void b_forward(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_save_positions(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_sorted_views(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_pairs_rows(cudaStream_t st, const Span& sp, const BatchArgs& a);
+// the pair count pass over warp tiles of 32 rows (element = tile of a box),
+// candidate records staged in shared memory (pairs_staged.cuh)
+void b_pairs_staged(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_pairs_fill(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_in_count(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_in_scatter(cudaStream_t st, const Span& sp, const BatchArgs& a);

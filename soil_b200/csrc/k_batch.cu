@@ -11,6 +11,7 @@
 #include "batch.cuh"
 #include "block_scan.cuh"
 #include "border_ops.cuh"
+#include "pairs_staged.cuh"
 #include "sys_internal.cuh"
 
 namespace soil {
@@ -428,6 +429,62 @@ __global__ void __launch_bounds__(kBlock) kb_pairs_rows(Span sp, BatchArgs A) {
     }
 }
 SPAN_LAUNCH(b_pairs_rows, kb_pairs_rows)
+
+// The staged pair count over warp tiles of every box (the single-system
+// kernel is k_pairs_staged); boxes whose stencil does not fit PairSegs scan
+// their rows from global memory.
+template <bool UNIFORM, bool FP32>
+__device__ __forceinline__ bool batch_tile(const PairParams& p, const BoxStep& S, const BoxDev& D,
+                                           uint64_t w, unsigned char* recs, uint64_t* bar,
+                                           uint32_t& phase, uint32_t* lo, uint32_t* base,
+                                           DevFlags* fl, uint32_t& cd, uint32_t& rk) {
+    if (S.segs_ok)
+        return staged_tile<UNIFORM, FP32>(p, S.segs, w, recs, bar, phase, lo, base, D.rowcount,
+                                          D.row_slots, fl, rk, cd);
+    const uint64_t i = w * 32 + (threadIdx.x & 31);
+    if (i < p.nlocal) pairs_row<UNIFORM, FP32>(p, i, D.rowcount, D.row_slots, fl, cd, rk);
+    return true;
+}
+
+__global__ void __launch_bounds__(kStageWarps * 32) kb_pairs_staged(Span sp, BatchArgs A) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ uint32_t s_lo[kStageWarps][kMaxPairSegs];
+    __shared__ uint32_t s_base[kStageWarps][kMaxPairSegs];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    unsigned char* recs = smem_raw + (size_t)wib * kStageRecs * 32;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + (size_t)kStageWarps * kStageRecs * 32) + wib;
+    staged_init(bar);
+    uint32_t phase = 0;
+    bool ok = true;
+    for_warp_tiles(sp, [&](uint32_t b, uint64_t w, uint32_t) {
+        if (!ok) return;
+        const BoxDev& D = A.dev[b];
+        const BoxStep& S = A.step[b];
+        const PairParams p = pair_params(D, S);
+        DevFlags* fl = A.flags + b;
+        uint32_t cd = 0, rk = 0;
+        if (S.uniform) {
+            if (S.filter) ok = batch_tile<true, true>(p, S, D, w, recs, bar, phase, s_lo[wib], s_base[wib], fl, cd, rk);
+            else ok = batch_tile<true, false>(p, S, D, w, recs, bar, phase, s_lo[wib], s_base[wib], fl, cd, rk);
+        } else {
+            if (S.filter) ok = batch_tile<false, true>(p, S, D, w, recs, bar, phase, s_lo[wib], s_base[wib], fl, cd, rk);
+            else ok = batch_tile<false, false>(p, S, D, w, recs, bar, phase, s_lo[wib], s_base[wib], fl, cd, rk);
+        }
+        const uint32_t scd = __reduce_add_sync(0xffffffffu, cd);
+        const uint32_t srk = __reduce_add_sync(0xffffffffu, rk);
+        if (lane == 0) add_filter_stats(fl, scd, srk);
+    });
+}
+
+void b_pairs_staged(cudaStream_t st, const Span& sp, const BatchArgs& a) {
+    if (sp.total == 0) return;
+    note_launch();
+    const size_t smem = (size_t)kStageWarps * kStageRecs * 32 + kStageWarps * sizeof(uint64_t);
+    const uint64_t per = kStageWarps;
+    uint64_t blocks = (sp.total + per - 1) / per;
+    if (blocks > 148ull * 8ull) blocks = 148ull * 8ull;
+    kb_pairs_staged<<<(unsigned)blocks, kStageWarps * 32, smem, st>>>(sp, a);
+}
 
 template <bool UNIFORM, bool FP32>
 __device__ __forceinline__ void fill_row(const PairParams& p, uint64_t i, const uint32_t* rowcount,

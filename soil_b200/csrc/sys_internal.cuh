@@ -243,6 +243,7 @@ int borders_done(soil_sys* s, const uint32_t* hb, const BorderDim bds[3]);
 void neighbor_params(soil_sys* s);
 int neighbor_plan(soil_sys* s);
 float pair_eps(const soil_sys* s);
+bool pair_segments(const std::vector<int32_t>& sten, bool has_self, bool newton, PairSegs* sg);
 int sync(soil_sys* s);
 int check_launch(soil_sys* s);
 Geom geom_of(const soil_sys* s);
