@@ -17,10 +17,9 @@
 #include <algorithm>
 #include <array>
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
-
-#include <cstdlib>
 #include <memory>
 #include <thread>
 
