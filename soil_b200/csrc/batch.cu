@@ -374,6 +374,11 @@ void fill_dev(soil_batch* b, uint32_t k) {
     d.boff = s->boff.p;
     d.fold_start = s->fold_start.p;
     d.fold_list = s->fold_list.p;
+    d.seq_cnt = s->seq_cnt.p;
+    d.grp_cnt = s->grp_cnt.p;
+    d.grp_start = s->grp_start.p;
+    d.seq = s->seq.p;
+    d.seq_owner = s->seq_owner.p;
     d.cap = s->acap;
     zero_planes_of(s, SOIL_COL_FORWARD, d.fwd.idx, &d.fwd.n);
     zero_planes_of(s, SOIL_COL_REVERSE, d.rev.idx, &d.rev.n);
@@ -872,10 +877,17 @@ int batch_step(soil_batch* b, bool last) {
             TRY(ensure(s, s->in_start, total + 2, 0, s->acap + 2));
             TRY(ensure(s, s->in_cursor, total + 1, 0, s->acap + 1));
             TRY(ensure(s, s->in_list, np + 1, 0, pair_room(np)));
+            if (s->few_images) {  // the grouped consumer's sequences, built this step
+                TRY(ensure(s, s->seq_cnt, total + 1, 0, s->acap + 1));
+                TRY(ensure(s, s->grp_cnt, s->nlocal + 1, 0, s->acap + 1));
+                TRY(ensure(s, s->grp_start, s->nlocal + 2, 0, s->acap + 2));
+                TRY(ensure(s, s->seq, 2 * np + 1, 0, 2 * pair_room(np)));
+                TRY(ensure(s, s->seq_owner, 2 * np + 1, 0, 2 * pair_room(np)));
+            }
             s->npairs = np;
             s->rebuilds += 1;
             s->in_lists_valid = true;
-            s->seq_valid = false;  // rebuilt by the first single-system force call
+            s->seq_valid = false;  // set once this step's sequences are enqueued
             s->hflags->candidates = b->h_flags[k].candidates;
             s->hflags->rechecked = b->h_flags[k].rechecked;
             fill_dev(b, k);
@@ -885,20 +897,39 @@ int batch_step(soil_batch* b, bool last) {
 
     // ---- CSR fill, incoming lists, force, reverse comm, final ----
     Stage& g5 = b->stage[G_FORCE];
+    std::vector<uint32_t> grouped_now;  // rebuilding boxes that build grouped sequences
     TRY(stage_begin(b, g5));
     TRY(put_tables(b, g5));
     const int r_loc = stage_add(g5), r_all = stage_add(g5), r_scan = stage_add(g5),
-              h_all = stage_add(g5), v_loc = stage_add(g5), l_loc = stage_add(g5);
+              h_all = stage_add(g5), v_loc = stage_add(g5), l_loc = stage_add(g5),
+              q_all = stage_add(g5), q_grp = stage_add(g5), q_loc = stage_add(g5),
+              t_tiles = stage_add(g5);
+    // Boxes whose locals have at most 7 images take the grouped consumer (its
+    // sequences built at each rebuild, reverse comm folded in); the others the
+    // per-atom gather and a reverse pass.
+    grouped_now.clear();
     for (uint32_t k : M) {
         const auto& h = b->hot[k];
+        const soil_sys* s = b->slot[k];
         const uint64_t nl = h.nlocal, total = nl + h.nghost;
+        const bool grouped = s->few_images && (b->rebuild[k] || s->seq_valid);
         if (b->rebuild[k]) {
             g5.spans[r_loc].add_nz(k, nl, 0);
             g5.spans[r_all].add_nz(k, total, 0);
             g5.spans[r_scan].add(k, total, 0);
+            if (grouped) {
+                g5.spans[q_all].add_nz(k, total, 0);
+                g5.spans[q_grp].add(k, nl, 0);
+                g5.spans[q_loc].add_nz(k, nl, 0);
+                grouped_now.push_back(k);
+            }
         }
-        g5.spans[h_all].add_nz(k, total, 0);
-        if (h.newton && h.nghost) g5.spans[v_loc].add_nz(k, nl, 0);
+        if (grouped) {
+            g5.spans[t_tiles].add_nz(k, (nl + 31) / 32, 0);
+        } else {
+            g5.spans[h_all].add_nz(k, total, 0);
+            if (h.newton && h.nghost) g5.spans[v_loc].add_nz(k, nl, 0);
+        }
         g5.spans[l_loc].add_nz(k, nl, 0);
     }
     toc(b, BT_NEIGHBOR);  // no-op when the rebuild path closed it
@@ -911,9 +942,14 @@ int batch_step(soil_batch* b, bool last) {
         b_scan(st, g5.out[r_scan], a, BA_IN);
         b_in_scatter(st, g5.out[r_loc], a);
         b_segsort(st, g5.out[r_all], a, BA_IN);
+        b_seq_count(st, g5.out[q_all], a);
+        b_scan(st, g5.out[q_grp], a, BA_GRP);
+        b_seq_fill(st, g5.out[q_loc], a);
+        for (uint32_t k : grouped_now) b->slot[k]->seq_valid = true;
     }
     toc(b, BT_LISTS);
     tic(b);
+    b_force_grouped(st, g5.out[t_tiles], a);
     b_harmonic(st, g5.out[h_all], a);
     toc(b, BT_FORCE);
     tic(b);

@@ -56,6 +56,12 @@ struct BoxDev {
     uint32_t* boff;        // their offsets
     uint32_t* fold_start;
     uint32_t* fold_list;
+    // grouped partner sequences of the built-in consumer (force_ops.cuh)
+    uint32_t* seq_cnt;
+    uint32_t* grp_cnt;
+    uint32_t* grp_start;
+    uint32_t* seq;
+    uint8_t* seq_owner;
     uint64_t cap;  // atom capacity of both column sets
     PlaneList fwd, rev, zero;
 };
@@ -115,7 +121,8 @@ enum BatchArray {
     BA_CELLS = 0,     // cell_counts -> cell_start (+ cursor), segsort of sort_perm
     BA_NEIGH_CELLS,   // cell_counts -> cell_start (+ cursor), segsort of sorted_atoms
     BA_ROWS,          // rowcount -> offsets (total into totals[box])
-    BA_IN             // in_count -> in_start (+ cursor), segsort of in_list
+    BA_IN,            // in_count -> in_start (+ cursor), segsort of in_list
+    BA_GRP            // grp_cnt -> grp_start (grouped sequences)
 };
 
 // ---- launchers (k_batch.cu); every one enqueues a single kernel ------------
@@ -153,6 +160,12 @@ void b_pairs_fill(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_in_count(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_in_scatter(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_harmonic(cudaStream_t st, const Span& sp, const BatchArgs& a);
+// grouped sequences: lengths over every atom (count) and the groups of the
+// locals (fill, after a BA_GRP scan); the consumer over warp tiles of 32
+// roots (element = tile of a box), folding images into roots with newton
+void b_seq_count(cudaStream_t st, const Span& sp, const BatchArgs& a);
+void b_seq_fill(cudaStream_t st, const Span& sp, const BatchArgs& a);
+void b_force_grouped(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_reverse(cudaStream_t st, const Span& sp, const BatchArgs& a);
 
 }  // namespace soil

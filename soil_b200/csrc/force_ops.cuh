@@ -9,6 +9,73 @@
 
 namespace soil {
 
+// ---- the grouped partner sequences (rebuilt with the lists) ----------------
+
+// Entries of atom a in the reference sum: its in-list (when it receives:
+// newton, or a local) and its own row (locals).
+__device__ __forceinline__ uint32_t seq_len(uint64_t a, uint64_t nlocal, int newton,
+                                            const uint32_t* offsets, const uint32_t* in_start) {
+    const bool local = a < nlocal;
+    const uint32_t nin = (newton || local) ? in_start[a + 1] - in_start[a] : 0u;
+    const uint32_t nrow = local ? offsets[a + 1] - offsets[a] : 0u;
+    return nin + nrow;
+}
+
+// cnt[a] = entries of atom a (every atom); grp[t] = entries of root t's group
+// (t and its images), t < nlocal.
+__device__ __forceinline__ void seq_count_atom(const SeqArgs& q, uint64_t a, uint32_t* cnt,
+                                               uint32_t* grp) {
+    const uint32_t n = seq_len(a, q.nlocal, q.newton, q.offsets, q.in_start);
+    cnt[a] = n;
+    if (a < q.nlocal) {
+        uint32_t g = n;
+        for (uint32_t f = q.fold_start[a]; f < q.fold_start[a + 1]; ++f)
+            g += seq_len(q.nlocal + q.fold_list[f], q.nlocal, q.newton, q.offsets, q.in_start);
+        grp[a] = g;
+    }
+}
+
+// The entries of atom a from position k on: in-list rows below a
+// (ascending), a's own row in CSR order, then the in-list rows above a.
+__device__ __forceinline__ uint32_t seq_put(const SeqArgs& q, uint64_t a, uint32_t k,
+                                            uint8_t meta, uint32_t* seq, uint8_t* owner) {
+    const bool local = a < q.nlocal;
+    const uint32_t qs = q.in_start[a];
+    const uint32_t nin = (q.newton || local) ? q.in_start[a + 1] - qs : 0u;
+    const uint32_t rs = local ? q.offsets[a] : 0u;
+    const uint32_t nrow = local ? q.offsets[a + 1] - rs : 0u;
+    uint32_t i = 0;
+    for (; i < nin && q.in_list[qs + i] < (uint32_t)a; ++i, ++k) {
+        seq[k] = q.in_list[qs + i];
+        owner[k] = meta;
+    }
+    for (uint32_t r = 0; r < nrow; ++r, ++k) {
+        seq[k] = q.indices[rs + r];
+        owner[k] = meta;
+    }
+    for (; i < nin; ++i, ++k) {
+        seq[k] = q.in_list[qs + i];
+        owner[k] = meta;
+    }
+    return k;
+}
+
+// Group of root t at grp_start[t]: t's entries, then each image's in fold
+// order.  owner[k] = (t & 31) | item << 5: item 0 = the root, item j = its
+// j-th image (at most 7 images per root, which the host checks).
+__device__ __forceinline__ void seq_fill_root(const SeqArgs& q, uint64_t t,
+                                              const uint32_t* grp_start, uint32_t* seq,
+                                              uint8_t* owner) {
+    const uint8_t lane = (uint8_t)(t & 31);
+    uint32_t k = seq_put(q, t, grp_start[t], lane, seq, owner);
+    const uint32_t f0 = q.fold_start[t], f1 = q.fold_start[t + 1];
+    for (uint32_t f = f0; f < f1; ++f)
+        k = seq_put(q, q.nlocal + q.fold_list[f], k, (uint8_t)(lane | ((f - f0 + 1) << 5)), seq,
+                    owner);
+}
+
+// ---- the warp tile ------------------------------------------------------------
+
 constexpr int kForceWarps = kBlock / 32;
 
 template <int U>
@@ -48,7 +115,7 @@ struct Item {
 
 // Item j of root t's group (0: t itself; j >= 1: its j-th image in fold
 // order), starting at entry `begin`.
-__device__ __forceinline__ Item item_at(const ForceArgs& p, uint64_t t, uint32_t f0, int j,
+__device__ __forceinline__ Item item_at(const ForceSeq& p, uint64_t t, uint32_t f0, int j,
                                         uint32_t begin) {
     Item it;
     it.atom = j == 0 ? t : p.nlocal + p.fold_list[f0 + j - 1];
@@ -62,11 +129,11 @@ __device__ __forceinline__ Item item_at(const ForceArgs& p, uint64_t t, uint32_t
 // add its own group's entries of the chunk in order.  With FOLD, each lane
 // then folds its images into its root (fold_root: reverse_send_force's order).
 template <int U, bool FOLD>
-__device__ __forceinline__ void force_tile(const ForceArgs& p, uint64_t w, ForceSmem<U>& sm,
+__device__ __forceinline__ void force_tile(const ForceSeq& p, const AtomCols& c,
+                                           const PlaneList& rev, uint64_t w, ForceSmem<U>& sm,
                                            int lane, int wib) {
     constexpr int CH = 32 * U;
     const uint64_t nl = p.nlocal;
-    const AtomCols& c = p.c;
     const uint64_t t = w * 32 + lane;
     const bool valid = t < nl;
     const uint64_t last = w * 32 + 32 < nl ? w * 32 + 32 : nl;
@@ -157,7 +224,7 @@ __device__ __forceinline__ void force_tile(const ForceArgs& p, uint64_t w, Force
             ++j;
             it = item_at(p, t, f0, j, it.end);
         }
-        if (FOLD) fold_root(c, nl, t, p.fold_start, p.fold_list, p.rev);
+        if (FOLD) fold_root(c, nl, t, p.fold_start, p.fold_list, rev);
     }
 }
 

@@ -11,6 +11,7 @@
 #include "batch.cuh"
 #include "block_scan.cuh"
 #include "border_ops.cuh"
+#include "force_ops.cuh"
 #include "pairs_staged.cuh"
 #include "sys_internal.cuh"
 
@@ -173,6 +174,7 @@ __global__ void __launch_bounds__(kBlock) kb_scan(Span sp, BatchArgs A, int whic
     uint32_t *out, *cursor;
     if (which == BA_ROWS) { in = D.rowcount; out = D.offsets; cursor = nullptr; }
     else if (which == BA_IN) { in = D.in_count; out = D.in_start; cursor = D.in_cursor; }
+    else if (which == BA_GRP) { in = D.grp_cnt; out = D.grp_start; cursor = nullptr; }
     else { in = D.cell_counts; out = D.cell_start; cursor = D.cell_cursor; }
     uint32_t carry = 0;
     for (uint64_t b0 = 0; b0 < n; b0 += (uint64_t)kBlock * kScanItems) {
@@ -547,5 +549,55 @@ void b_harmonic(cudaStream_t st, const Span& sp, const BatchArgs& a) {
 
 SPAN_KERNEL(kb_reverse, { fold_root(D.set[S.post], S.nlocal, i, D.fold_start, D.fold_list, D.rev); })
 SPAN_LAUNCH(b_reverse, kb_reverse)
+
+// ---- the grouped consumer (the single-system kernels are in k_force.cu) -------
+__device__ __forceinline__ SeqArgs seq_args(const BoxDev& D, const BoxStep& S) {
+    SeqArgs q;
+    q.nlocal = S.nlocal;
+    q.ntotal = S.nlocal + S.nghost;
+    q.newton = S.newton;
+    q.offsets = D.offsets;
+    q.indices = D.indices;
+    q.in_start = D.in_start;
+    q.in_list = D.in_list;
+    q.fold_start = D.fold_start;
+    q.fold_list = D.fold_list;
+    return q;
+}
+
+SPAN_KERNEL(kb_seq_count, { seq_count_atom(seq_args(D, S), i, D.seq_cnt, D.grp_cnt); })
+SPAN_LAUNCH(b_seq_count, kb_seq_count)
+
+SPAN_KERNEL(kb_seq_fill, { seq_fill_root(seq_args(D, S), i, D.grp_start, D.seq, D.seq_owner); })
+SPAN_LAUNCH(b_seq_fill, kb_seq_fill)
+
+__global__ void __launch_bounds__(kBlock, 3) kb_force_grouped(Span sp, BatchArgs A) {
+    __shared__ ForceSmem<4> sm;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    for_warp_tiles(sp, [&](uint32_t b, uint64_t w, uint32_t) {
+        const BoxDev& D = A.dev[b];
+        const BoxStep& S = A.step[b];
+        const AtomCols& c = D.set[S.post];
+        ForceSeq q;
+        q.rad = c.planes[D.radius_plane];
+        q.K = S.K;
+        q.nlocal = S.nlocal;
+        q.grp_start = D.grp_start;
+        q.cnt = D.seq_cnt;
+        q.seq = D.seq;
+        q.owner = D.seq_owner;
+        q.fold_start = D.fold_start;
+        q.fold_list = D.fold_list;
+        if (S.newton) force_tile<4, true>(q, c, D.rev, w, sm, lane, wib);
+        else force_tile<4, false>(q, c, D.rev, w, sm, lane, wib);
+    });
+}
+void b_force_grouped(cudaStream_t st, const Span& sp, const BatchArgs& a) {
+    if (sp.total == 0) return;
+    note_launch();
+    uint64_t blocks = (sp.total + kBlock / 32 - 1) / (kBlock / 32);
+    if (blocks > 148ull * 3ull) blocks = 148ull * 3ull;  // one resident wave
+    kb_force_grouped<<<(unsigned)blocks, kBlock, 0, st>>>(sp, a);
+}
 
 }  // namespace soil

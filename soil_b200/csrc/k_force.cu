@@ -61,71 +61,17 @@ void launch_harmonic(cudaStream_t st, uint64_t nlocal, uint64_t ntotal, const At
 
 // ---- the grouped partner sequences (rebuilt with the lists) ----------------
 
-// Entries of atom a in the reference sum: its in-list (when it receives:
-// newton, or a local) and its own row (locals).
-__device__ __forceinline__ uint32_t seq_len(uint64_t a, uint64_t nlocal, int newton,
-                                            const uint32_t* offsets, const uint32_t* in_start) {
-    const bool local = a < nlocal;
-    const uint32_t nin = (newton || local) ? in_start[a + 1] - in_start[a] : 0u;
-    const uint32_t nrow = local ? offsets[a + 1] - offsets[a] : 0u;
-    return nin + nrow;
-}
-
-// cnt[a] = entries of atom a (every atom); grp[t] = entries of root t's group
-// (t and its images), t < nlocal.
 __global__ void __launch_bounds__(kBlock) k_seq_count(SeqArgs q, uint32_t* cnt, uint32_t* grp) {
     for (uint64_t a = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; a < q.ntotal;
-         a += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t n = seq_len(a, q.nlocal, q.newton, q.offsets, q.in_start);
-        cnt[a] = n;
-        if (a < q.nlocal) {
-            uint32_t g = n;
-            for (uint32_t f = q.fold_start[a]; f < q.fold_start[a + 1]; ++f)
-                g += seq_len(q.nlocal + q.fold_list[f], q.nlocal, q.newton, q.offsets, q.in_start);
-            grp[a] = g;
-        }
-    }
+         a += (uint64_t)gridDim.x * blockDim.x)
+        seq_count_atom(q, a, cnt, grp);
 }
 
-// The entries of atom a from position k on: in-list rows below a
-// (ascending), a's own row in CSR order, then the in-list rows above a.
-__device__ __forceinline__ uint32_t seq_put(const SeqArgs& q, uint64_t a, uint32_t k,
-                                            uint8_t meta, uint32_t* seq, uint8_t* owner) {
-    const bool local = a < q.nlocal;
-    const uint32_t qs = q.in_start[a];
-    const uint32_t nin = (q.newton || local) ? q.in_start[a + 1] - qs : 0u;
-    const uint32_t rs = local ? q.offsets[a] : 0u;
-    const uint32_t nrow = local ? q.offsets[a + 1] - rs : 0u;
-    uint32_t i = 0;
-    for (; i < nin && q.in_list[qs + i] < (uint32_t)a; ++i, ++k) {
-        seq[k] = q.in_list[qs + i];
-        owner[k] = meta;
-    }
-    for (uint32_t r = 0; r < nrow; ++r, ++k) {
-        seq[k] = q.indices[rs + r];
-        owner[k] = meta;
-    }
-    for (; i < nin; ++i, ++k) {
-        seq[k] = q.in_list[qs + i];
-        owner[k] = meta;
-    }
-    return k;
-}
-
-// Group of root t at grp_start[t]: t's entries, then each image's in fold
-// order.  owner[k] = (t & 31) | item << 5: item 0 = the root, item j = its
-// j-th image (at most 7 images per root, which the host checks).
 __global__ void __launch_bounds__(kBlock) k_seq_fill(SeqArgs q, const uint32_t* grp_start,
                                                      uint32_t* seq, uint8_t* owner) {
     for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < q.nlocal;
-         t += (uint64_t)gridDim.x * blockDim.x) {
-        const uint8_t lane = (uint8_t)(t & 31);
-        uint32_t k = seq_put(q, t, grp_start[t], lane, seq, owner);
-        const uint32_t f0 = q.fold_start[t], f1 = q.fold_start[t + 1];
-        for (uint32_t f = f0; f < f1; ++f)
-            k = seq_put(q, q.nlocal + q.fold_list[f], k, (uint8_t)(lane | ((f - f0 + 1) << 5)), seq,
-                        owner);
-    }
+         t += (uint64_t)gridDim.x * blockDim.x)
+        seq_fill_root(q, t, grp_start, seq, owner);
 }
 
 void launch_seq_count(cudaStream_t st, const SeqArgs& q, uint32_t* cnt, uint32_t* grp) {
@@ -147,17 +93,17 @@ template <int U, bool FOLD>
 __global__ void __launch_bounds__(kBlock, 4) k_force_seq(ForceArgs p) {
     __shared__ ForceSmem<U> sm;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const uint64_t ntiles = (p.nlocal + 31) / 32;
+    const uint64_t ntiles = (p.q.nlocal + 31) / 32;
     for (uint64_t w = (uint64_t)blockIdx.x * kForceWarps + wib; w < ntiles;
          w += (uint64_t)gridDim.x * kForceWarps)
-        force_tile<U, FOLD>(p, w, sm, lane, wib);
+        force_tile<U, FOLD>(p.q, p.c, p.rev, w, sm, lane, wib);
 }
 
 void launch_force_seq(cudaStream_t st, const ForceArgs& p, bool fold) {
-    if (p.nlocal == 0) return;
+    if (p.q.nlocal == 0) return;
     note_launch();
     constexpr int U = 4;
-    const uint64_t ntiles = (p.nlocal + 31) / 32;
+    const uint64_t ntiles = (p.q.nlocal + 31) / 32;
     const uint64_t need = (ntiles + kForceWarps - 1) / kForceWarps;
     const uint64_t full = 148ull * 4ull;  // one resident wave, grid-stride over the tiles
     const unsigned grid = (unsigned)(need < full ? need : full);

@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_steps(StepsArgs a) {
             const uint64_t ntiles = (nl + 31) / 32;
             for (uint64_t w = (uint64_t)blockIdx.x * kForceWarps + wib; w < ntiles;
                  w += (uint64_t)gridDim.x * kForceWarps)
-                force_tile<U, CONSUMER == 2>(a.fa, w, sm, lane, wib);
+                force_tile<U, CONSUMER == 2>(a.fa.q, c, a.fa.rev, w, sm, lane, wib);
         }
         // Also without a consumer: no CTA may set the flag in the next phase A
         // before every CTA has read it above.

@@ -311,8 +311,8 @@ void launch_seq_count(cudaStream_t st, const SeqArgs& q, uint32_t* cnt, uint32_t
 // the root, item j: its j-th image).  Roots have at most 7 images.
 void launch_seq_fill(cudaStream_t st, const SeqArgs& q, const uint32_t* grp_start, uint32_t* seq,
                      uint8_t* owner);
-struct ForceArgs {
-    AtomCols c;
+// The grouped sequences and consumer constants of one system.
+struct ForceSeq {
     const double* rad;
     double K;
     uint64_t nlocal;
@@ -322,7 +322,11 @@ struct ForceArgs {
     const uint8_t* owner;
     const uint32_t* fold_start;
     const uint32_t* fold_list;
-    PlaneList rev;              // #[reverse] planes folded with the forces
+};
+struct ForceArgs {
+    AtomCols c;
+    ForceSeq q;
+    PlaneList rev;  // #[reverse] planes folded with the forces
 };
 // The built-in consumer over the grouped sequences (warp-cooperative): F of
 // every local and ghost is overwritten; with fold, ghost forces (and the

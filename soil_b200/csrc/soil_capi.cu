@@ -1072,15 +1072,15 @@ bool seq_consumer(const soil_sys* s) { return builtin_consumer(s) && s->few_imag
 ForceArgs consumer_args(const soil_sys* s) {
     ForceArgs p;
     p.c = s->A;
-    p.rad = s->A.planes[s->cols[s->radius_col].plane0];
-    p.K = s->harmonic_k;
-    p.nlocal = s->nlocal;
-    p.grp_start = s->grp_start.p;
-    p.cnt = s->seq_cnt.p;
-    p.seq = s->seq.p;
-    p.owner = s->seq_owner.p;
-    p.fold_start = s->fold_start.p;
-    p.fold_list = s->fold_list.p;
+    p.q.rad = s->A.planes[s->cols[s->radius_col].plane0];
+    p.q.K = s->harmonic_k;
+    p.q.nlocal = s->nlocal;
+    p.q.grp_start = s->grp_start.p;
+    p.q.cnt = s->seq_cnt.p;
+    p.q.seq = s->seq.p;
+    p.q.owner = s->seq_owner.p;
+    p.q.fold_start = s->fold_start.p;
+    p.q.fold_list = s->fold_list.p;
     zero_planes_of(s, SOIL_COL_REVERSE, p.rev.idx, &p.rev.n);
     return p;
 }
