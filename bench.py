@@ -444,6 +444,21 @@ def run_batched(args, world, rank, local):
         f"{time.perf_counter() - t0:.1f}s")
     lib = abi.load_library()
     ctx = system.Context(local)
+    tuned = None
+    if args.tune:
+        # bin size per size class, timed on up to two boxes of each class; the
+        # table then configures every box (plain and batched runs alike)
+        from soil_b200 import autotune
+        t0 = time.perf_counter()
+        samples = {}
+        for w in ws:
+            lst = samples.setdefault(autotune.size_class(w.n), [])
+            if len(lst) < 2:
+                lst.append(w)
+        table = autotune.tune(ctx, samples)
+        ws = [table.apply(w) for w in ws]
+        tuned = {"classes": table.entries, "seconds": time.perf_counter() - t0}
+        log(f"[c4] tuned {len(table.entries)} size classes in {tuned['seconds']:.1f}s")
     t0 = time.perf_counter()
     boxes = [system.from_workload(ctx, w) for w in ws]
     log(f"[c4] systems set up in {time.perf_counter() - t0:.1f}s")
@@ -543,6 +558,7 @@ def run_batched(args, world, rank, local):
             "host_threads": os.environ.get("SOIL_HOST_THREADS", "default"),
             "host_loadavg_1min": [round(load0[0], 2), round(load1[0], 2)],
             "device_allocs_in_timed_region": al1[0] - al0[0],
+            "autotune": tuned,
             "roofline": roofline,
             "cpu_baseline": cb,
             "e2e": None,
@@ -733,6 +749,8 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=4,
                     help="c4/c5: timed steps of each box alone (plain path; 0 skips it in c4)")
     ap.add_argument("--filter", choices=["fp64", "fp32"], default="fp64")
+    ap.add_argument("--tune", action="store_true",
+                    help="c4: bin size per size class from the autotuner before the run")
     ap.add_argument("--natoms", type=int, default=None,
                     help="reduced system size (profiling only; not a bench line)")
     ap.add_argument("--no-e2e", action="store_true")

@@ -19,6 +19,7 @@ def _p(a, ct):
 class Context:
     def __init__(self, device=0, hbm_budget_bytes=0):
         self.lib = abi.load_library()
+        self.device = device
         h = C.c_void_p()
         st = self.lib.soil_ctx_create(device, hbm_budget_bytes, C.byref(h))
         if st != abi.SOIL_OK:
