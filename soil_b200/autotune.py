@@ -1,12 +1,14 @@
 """Per-size-class autotuner of the bin size.
 
 The reference's bin grid uses cells of at least `bin_size` (its
-`bin_min_size`) and never smaller than the largest cutoff radius
-(crates/soil_core/src/neighbor.rs:311-495).  The cell size trades grid
-work (cells to count, scan and sort per rebuild) against candidates per row;
-which side wins depends on the system's size and density.  This tuner times
-a few candidate sizes on sample systems of each size class (floor(log2 N)
-atoms) and keeps the fastest per class in a JSON table.
+`bin_min_size`), raised at setup to the largest pair cutoff
+2 * max(cutoff_radius) * skin_fraction (neighbor_setup,
+crates/soil_core/src/neighbor.rs:604-665).  Larger cells mean fewer cells to
+count, scan and sort per rebuild (and thinner ghost layers of cells), but
+more candidates per row; which side wins depends on the system's size.  This
+tuner times a few cell sizes, as factors of the largest pair cutoff, on
+sample systems of each size class (floor(log2 N) atoms) and keeps the
+fastest factor per class in a JSON table.
 
 The bin size is part of a system's configuration: it decides the cell of
 every atom, hence the CSR order and the force summation order.  A tuned
@@ -25,8 +27,8 @@ import os
 
 from . import system
 
-# bin_size values tried; the grid clamps each to the largest cutoff radius
-CANDIDATES = (0.65, 0.8, 1.0, 1.3)
+# bin sizes tried, as factors of the largest pair cutoff
+CANDIDATES = (1.0, 1.25, 1.5, 2.0)
 DEFAULT_PATH = os.path.join(os.path.expanduser("~"), ".cache", "soil_b200", "autotune.json")
 
 
@@ -35,21 +37,31 @@ def size_class(n):
     return max(0, int(n).bit_length() - 1)
 
 
+def max_pair_cutoff(w):
+    """The largest pair cutoff of a workload, as neighbor_setup computes it."""
+    return 2.0 * float(w.cutoff.max()) * w.cfg.skin_fraction
+
+
+def bin_size_of(w, factor):
+    return factor * max_pair_cutoff(w)
+
+
 class Table:
-    """Tuned bin size per size class ({"<class>": {"bin_size": b, "rate": ...}})."""
+    """Tuned bin-size factor per size class
+    ({"<class>": {"bin_factor": f, "rate": ...}})."""
 
     def __init__(self, entries=None):
         self.entries = {str(k): dict(v) for k, v in (entries or {}).items()}
 
-    def bin_size(self, n, default=None):
+    def factor(self, n, default=None):
         e = self.entries.get(str(size_class(n)))
-        return e["bin_size"] if e else default
+        return e["bin_factor"] if e else default
 
     def apply(self, w):
         """Set the workload's bin size from its class (unchanged if untuned)."""
-        b = self.bin_size(w.n)
-        if b is not None:
-            w.cfg.bin_size = b
+        f = self.factor(w.n)
+        if f is not None:
+            w.cfg.bin_size = bin_size_of(w, f)
         return w
 
     def save(self, path=DEFAULT_PATH):
@@ -88,22 +100,22 @@ def measure(ctx, w, steps=20, warmup=5):
 
 
 def tune(ctx, samples, candidates=CANDIDATES, steps=20, warmup=5):
-    """samples: {size class: [workload, ...]}.  Every candidate bin size is
+    """samples: {size class: [workload, ...]}.  Every candidate factor is
     timed on every sample of a class (a copy of its configuration); the
-    class keeps the candidate with the largest summed atom-steps/s."""
+    class keeps the factor with the largest summed atom-steps/s."""
     import copy
     entries = {}
     for cls, ws in samples.items():
         best = None
-        for b in candidates:
+        for f in candidates:
             rate = 0.0
             for w in ws:
                 wc = copy.copy(w)
                 wc.cfg = copy.copy(w.cfg)
-                wc.cfg.bin_size = b
+                wc.cfg.bin_size = bin_size_of(w, f)
                 rate += measure(ctx, wc, steps, warmup)
             if best is None or rate > best[1]:
-                best = (b, rate)
-        entries[str(cls)] = {"bin_size": best[0], "rate": best[1] / max(len(ws), 1),
+                best = (f, rate)
+        entries[str(cls)] = {"bin_factor": best[0], "rate": best[1] / max(len(ws), 1),
                              "samples": len(ws)}
     return Table(entries)

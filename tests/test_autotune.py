@@ -11,19 +11,21 @@ def test_size_classes():
 
 
 def test_table_applies_and_round_trips(tmp_path):
-    t = autotune.Table({8: {"bin_size": 0.8, "rate": 1.0}, "12": {"bin_size": 1.3, "rate": 2.0}})
+    t = autotune.Table({8: {"bin_factor": 1.5, "rate": 1.0}, "12": {"bin_factor": 2.0, "rate": 2.0}})
     w_small = W.poly("t8", 1, 300, 0.4, 1e-4, 0)      # class 8
     w_big = W.poly("t12", 2, 5000, 0.4, 1e-4, 0)      # class 12
     w_none = W.poly("t10", 3, 1500, 0.4, 1e-4, 0)     # class 10: not tuned
-    assert t.apply(w_small).cfg.bin_size == 0.8
-    assert t.apply(w_big).cfg.bin_size == 1.3
+    # the largest pair cutoff: 2 * max(r + skin/2) * skin_fraction
+    assert autotune.max_pair_cutoff(w_small) == 2.0 * float(w_small.cutoff.max())
+    assert t.apply(w_small).cfg.bin_size == 1.5 * autotune.max_pair_cutoff(w_small)
+    assert t.apply(w_big).cfg.bin_size == 2.0 * autotune.max_pair_cutoff(w_big)
     before = w_none.cfg.bin_size
     assert t.apply(w_none).cfg.bin_size == before
     p = tmp_path / "sub" / "table.json"
     t.save(str(p))
     u = autotune.Table.load(str(p))
     assert u.entries == t.entries
-    assert u.bin_size(300) == 0.8 and u.bin_size(1500) is None
+    assert u.factor(300) == 1.5 and u.factor(1500) is None
 
 
 def test_table_refuses_unknown_version(tmp_path):

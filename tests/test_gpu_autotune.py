@@ -19,7 +19,7 @@ def test_tuned_boxes_identical_alone_batched_and_oracle(ctx):
     table = autotune.tune(ctx, samples, steps=4, warmup=2)
     assert set(table.entries) == {str(c) for c in samples}
     for e in table.entries.values():
-        assert e["bin_size"] in autotune.CANDIDATES and e["rate"] > 0
+        assert e["bin_factor"] in autotune.CANDIDATES and e["rate"] > 0
     ws = [table.apply(w) for w in ws]
     alone = [system.from_workload(ctx, w) for w in ws]
     for s in alone:
