@@ -275,6 +275,19 @@ void launch_interleave3i(cudaStream_t st, uint64_t n, int32_t* dst, const int32_
         k_interleave3i<<<grid_for(n), kBlock, 0, st>>>(n, dst, a, b, c);
     }
 }
+// inv[i] = 1.0 / m[i] (IEEE division, the host's bits)
+__global__ void __launch_bounds__(kBlock) k_inverse(uint64_t n, const double* m, double* inv) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        inv[i] = 1.0 / m[i];
+}
+void launch_inverse(cudaStream_t st, uint64_t n, const double* m, double* inv) {
+    if (n) {
+        note_launch();
+        k_inverse<<<grid_for(n), kBlock, 0, st>>>(n, m, inv);
+    }
+}
+
 void launch_deinterleave_w(cudaStream_t st, uint64_t n, int w, const double* src, double* dst0,
                            uint64_t cap) {
     if (n) {

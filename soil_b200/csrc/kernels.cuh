@@ -100,6 +100,8 @@ void launch_select(cudaStream_t st, uint64_t n, const uint32_t* flag, uint32_t* 
 // in mask (ext preset to all ones / zeros)
 void launch_extent(cudaStream_t st, uint64_t n, const AtomCols& c, int mask,
                    unsigned long long* ext);
+// inv[i] = 1.0 / m[i], i < n
+void launch_inverse(cudaStream_t st, uint64_t n, const double* m, double* inv);
 // host-layout conversions ([n][3] or [n][w] interleaved <-> SoA planes)
 void launch_deinterleave3(cudaStream_t st, uint64_t n, const double* src, double* a, double* b,
                           double* c);

@@ -1811,41 +1811,49 @@ int soil_sys_add_atoms(soil_sys* s, uint64_t n, const uint32_t* tag, const uint3
                        const double* cutoff_radius, const double* const* columns) {
     if (!s || (n && (!tag || !pos3 || !vel3 || !mass || !cutoff_radius))) return SOIL_ERR_INVALID;
     if (s->setup_done) return fail(s->ctx, SOIL_ERR_STATE, "atoms must be added before setup");
-    for (uint64_t i = 0; i < n; ++i)
+    // one host pass: validation and the cutoff radii's extremes
+    double cmin = s->cut_min_local, cmax = s->cut_max_local;
+    for (uint64_t i = 0; i < n; ++i) {
         if (!(mass[i] > 0.0) || !(cutoff_radius[i] >= 0.0))
             return fail(s->ctx, SOIL_ERR_INVALID, "atom %llu: mass must be > 0 and cutoff >= 0",
                         (unsigned long long)i);
+        cmin = std::fmin(cmin, cutoff_radius[i]);
+        cmax = std::fmax(cmax, cutoff_radius[i]);
+    }
     const uint64_t base = s->nlocal;
     TRY(grow_atoms(s, base + n, base));
     if (n == 0) return SOIL_OK;
-    TRY(ensure(s, s->stage, 3 * n));
+    // staging: positions and velocities, then the widest column, side by side
+    uint64_t wmax = 0;
+    for (const ColMeta& m : s->cols) wmax = std::max<uint64_t>(wmax, (uint64_t)m.width);
+    TRY(ensure(s, s->stage, 6 * n + wmax * n));
     double* st3 = s->stage.p;
+    double* sv3 = s->stage.p + 3 * n;
+    double* scol = s->stage.p + 6 * n;
     CK(cudaMemcpyAsync(st3, pos3, n * 24, cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemcpyAsync(sv3, vel3, n * 24, cudaMemcpyHostToDevice, s->st));
     launch_deinterleave3(s->st, n, st3, s->A.x + base, s->A.y + base, s->A.z + base);
-    CK(cudaStreamSynchronize(s->st));
-    CK(cudaMemcpyAsync(st3, vel3, n * 24, cudaMemcpyHostToDevice, s->st));
-    launch_deinterleave3(s->st, n, st3, s->A.vx + base, s->A.vy + base, s->A.vz + base);
+    launch_deinterleave3(s->st, n, sv3, s->A.vx + base, s->A.vy + base, s->A.vz + base);
     CK(cudaMemsetAsync(s->A.fx + base, 0, n * 8, s->st));
     CK(cudaMemsetAsync(s->A.fy + base, 0, n * 8, s->st));
     CK(cudaMemsetAsync(s->A.fz + base, 0, n * 8, s->st));
     CK(cudaMemcpyAsync(s->A.mass + base, mass, n * 8, cudaMemcpyHostToDevice, s->st));
+    launch_inverse(s->st, n, s->A.mass + base, s->A.inv_mass + base);
     CK(cudaMemcpyAsync(s->A.cut + base, cutoff_radius, n * 8, cudaMemcpyHostToDevice, s->st));
     CK(cudaMemcpyAsync(s->A.tag + base, tag, n * 4, cudaMemcpyHostToDevice, s->st));
     if (type) CK(cudaMemcpyAsync(s->A.type + base, type, n * 4, cudaMemcpyHostToDevice, s->st));
     else CK(cudaMemsetAsync(s->A.type + base, 0, n * 4, s->st));
     for (int d = 0; d < 3; ++d) CK(cudaMemsetAsync(s->A.img + d * s->acap + base, 0, n * 4, s->st));
     CK(cudaMemsetAsync(s->A.origin + base, 0, n * 4, s->st));
-    std::vector<double> inv(n);
-    for (uint64_t i = 0; i < n; ++i) inv[i] = 1.0 / mass[i];
-    CK(cudaMemcpyAsync(s->A.inv_mass + base, inv.data(), n * 8, cudaMemcpyHostToDevice, s->st));
+    bool col_pending = false;
     for (size_t c = 0; c < s->cols.size(); ++c) {
         const ColMeta& m = s->cols[c];
         if (columns && columns[c]) {
-            TRY(ensure(s, s->stage, (uint64_t)m.width * n));
-            CK(cudaMemcpyAsync(s->stage.p, columns[c], (uint64_t)m.width * n * 8,
+            if (col_pending) CK(cudaStreamSynchronize(s->st));  // scol is reused
+            CK(cudaMemcpyAsync(scol, columns[c], (uint64_t)m.width * n * 8,
                                cudaMemcpyHostToDevice, s->st));
-            launch_deinterleave_w(s->st, n, m.width, s->stage.p, s->A.planes[m.plane0] + base, s->acap);
-            CK(cudaStreamSynchronize(s->st));
+            launch_deinterleave_w(s->st, n, m.width, scol, s->A.planes[m.plane0] + base, s->acap);
+            col_pending = true;
         } else {
             for (int w = 0; w < m.width; ++w)
                 CK(cudaMemsetAsync(s->A.planes[m.plane0 + w] + base, 0, n * 8, s->st));
@@ -1853,10 +1861,8 @@ int soil_sys_add_atoms(soil_sys* s, uint64_t n, const uint32_t* tag, const uint3
     }
     TRY(check_launch(s));
     TRY(sync(s));
-    for (uint64_t i = 0; i < n; ++i) {
-        s->cut_min_local = std::fmin(s->cut_min_local, cutoff_radius[i]);
-        s->cut_max_local = std::fmax(s->cut_max_local, cutoff_radius[i]);
-    }
+    s->cut_min_local = cmin;
+    s->cut_max_local = cmax;
     s->nlocal += n;
     return SOIL_OK;
 }
