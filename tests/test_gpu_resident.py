@@ -56,9 +56,38 @@ def test_resident_steps_bit_identical(ctx, name):
         assert_same_lists(g, o, name)
     c = g_res.counts()
     assert 3 <= c.rebuilds < sum(chunks)  # light steps ran between rebuilds
-    assert n_res < n_ph / 2, (n_res, n_ph)
+    assert n_res < n_ph, (n_res, n_ph)
     g_res.close()
     g_ph.close()
+
+
+def test_resident_light_steps_take_one_launch(ctx):
+    """Without rebuilds, a call of 40 steps is one resident launch (plus the
+    final half-kick), against two or more launches per step phase by phase."""
+    w = W.poly("res-light", 85, 4000, 0.45, 1e-5, 0, harmonic_k=1e3)
+    g_res, n_res = _run(ctx, w, "1", [1, 40])
+    g_ph, n_ph = _run(ctx, w, "0", [1, 40])
+    assert g_res.counts().rebuilds == 1  # the setup build only
+    assert_same_state(g_res, g_ph)
+    l_res, l_ph = _launches_of(ctx, g_res, 40), _launches_of(ctx, g_ph, 40, mode="0")
+    assert l_res <= 4 and l_ph >= 80, (l_res, l_ph)
+    g_res.close()
+    g_ph.close()
+
+
+def _launches_of(ctx, g, n, mode="1"):
+    old = os.environ.get("SOIL_RESIDENT_STEPS")
+    os.environ["SOIL_RESIDENT_STEPS"] = mode
+    try:
+        lib = abi.load_library()
+        l0 = lib.soil_kernel_launches()
+        g.step(n)
+        return lib.soil_kernel_launches() - l0
+    finally:
+        if old is None:
+            del os.environ["SOIL_RESIDENT_STEPS"]
+        else:
+            os.environ["SOIL_RESIDENT_STEPS"] = old
 
 
 def test_resident_steps_stop_at_the_periodic_sort(ctx):
