@@ -561,10 +561,10 @@ int grow_slots(soil_batch* b, uint32_t need) {
     return SOIL_OK;
 }
 
-// The staged pair count serves the batch unless SOIL_PAIRS_STAGED=0.
+// The staged pair count serves the batch when SOIL_PAIRS_STAGED=1.
 bool pairs_staged_on() {
     const char* env = std::getenv("SOIL_PAIRS_STAGED");
-    return !(env && std::atoi(env) == 0);
+    return env && std::atoi(env) != 0;  // measured slower: off unless asked
 }
 
 // ---- one step -------------------------------------------------------------------
@@ -903,16 +903,18 @@ int batch_step(soil_batch* b, bool last) {
     const int r_loc = stage_add(g5), r_all = stage_add(g5), r_scan = stage_add(g5),
               h_all = stage_add(g5), v_loc = stage_add(g5), l_loc = stage_add(g5),
               q_all = stage_add(g5), q_grp = stage_add(g5), q_loc = stage_add(g5),
-              t_tiles = stage_add(g5);
+              t_tiles = stage_add(g5), t_walk = stage_add(g5);
     // Boxes whose locals have at most 7 images take the grouped consumer (its
     // sequences built at each rebuild, reverse comm folded in); the others the
     // per-atom gather and a reverse pass.
     grouped_now.clear();
+    const int variant = force_variant();
     for (uint32_t k : M) {
         const auto& h = b->hot[k];
         const soil_sys* s = b->slot[k];
         const uint64_t nl = h.nlocal, total = nl + h.nghost;
-        const bool grouped = s->few_images && (b->rebuild[k] || s->seq_valid);
+        const bool grouped = variant != SOIL_FORCE_GATHER && s->few_images &&
+                             (b->rebuild[k] || s->seq_valid);
         if (b->rebuild[k]) {
             g5.spans[r_loc].add_nz(k, nl, 0);
             g5.spans[r_all].add_nz(k, total, 0);
@@ -925,7 +927,8 @@ int batch_step(soil_batch* b, bool last) {
             }
         }
         if (grouped) {
-            g5.spans[t_tiles].add_nz(k, (nl + 31) / 32, 0);
+            if (variant == SOIL_FORCE_WALK) g5.spans[t_walk].add_nz(k, nl, 0);
+            else g5.spans[t_tiles].add_nz(k, (nl + 31) / 32, 0);
         } else {
             g5.spans[h_all].add_nz(k, total, 0);
             if (h.newton && h.nghost) g5.spans[v_loc].add_nz(k, nl, 0);
@@ -950,6 +953,7 @@ int batch_step(soil_batch* b, bool last) {
     toc(b, BT_LISTS);
     tic(b);
     b_force_grouped(st, g5.out[t_tiles], a);
+    b_force_walk(st, g5.out[t_walk], a);
     b_harmonic(st, g5.out[h_all], a);
     toc(b, BT_FORCE);
     tic(b);

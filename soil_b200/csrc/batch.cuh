@@ -166,6 +166,8 @@ void b_harmonic(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_seq_count(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_seq_fill(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_force_grouped(cudaStream_t st, const Span& sp, const BatchArgs& a);
+// the same consumer with one root per thread (element = local root)
+void b_force_walk(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_reverse(cudaStream_t st, const Span& sp, const BatchArgs& a);
 
 }  // namespace soil

@@ -228,4 +228,34 @@ __device__ __forceinline__ void force_tile(const ForceSeq& p, const AtomCols& c,
     }
 }
 
+// Root t's group walked by one thread: each item's (root's, then every
+// image's) sequence summed in order, its force written, then (FOLD) the
+// images folded into the root in reverse_send_force's order.
+template <bool FOLD>
+__device__ __forceinline__ void force_walk_root(const ForceSeq& p, const AtomCols& c,
+                                                const PlaneList& rev, uint64_t t) {
+    const uint64_t nl = p.nlocal;
+    const uint32_t f0 = p.fold_start[t], nimg = p.fold_start[t + 1] - f0;
+    uint32_t k = p.grp_start[t];
+    for (uint32_t j = 0; j <= nimg; ++j) {
+        const uint64_t a = j == 0 ? t : nl + p.fold_list[f0 + j - 1];
+        const uint32_t e = k + p.cnt[a];
+        const double xa = c.x[a], ya = c.y[a], za = c.z[a], ra = p.rad[a];
+        double Fx = 0.0, Fy = 0.0, Fz = 0.0;
+        for (; k < e; ++k) {
+            const uint32_t o = p.seq[k];
+            double fx, fy, fz;
+            if (pair_force(xa, ya, za, ra, c.x[o], c.y[o], c.z[o], p.rad[o], p.K, fx, fy, fz)) {
+                Fx = Fx + fx;
+                Fy = Fy + fy;
+                Fz = Fz + fz;
+            }
+        }
+        c.fx[a] = Fx;
+        c.fy[a] = Fy;
+        c.fz[a] = Fz;
+    }
+    if (FOLD) fold_root(c, nl, t, p.fold_start, p.fold_list, rev);
+}
+
 }  // namespace soil

@@ -571,6 +571,21 @@ SPAN_LAUNCH(b_seq_count, kb_seq_count)
 SPAN_KERNEL(kb_seq_fill, { seq_fill_root(seq_args(D, S), i, D.grp_start, D.seq, D.seq_owner); })
 SPAN_LAUNCH(b_seq_fill, kb_seq_fill)
 
+__device__ __forceinline__ ForceSeq force_seq_of(const BoxDev& D, const BoxStep& S,
+                                                 const AtomCols& c) {
+    ForceSeq q;
+    q.rad = c.planes[D.radius_plane];
+    q.K = S.K;
+    q.nlocal = S.nlocal;
+    q.grp_start = D.grp_start;
+    q.cnt = D.seq_cnt;
+    q.seq = D.seq;
+    q.owner = D.seq_owner;
+    q.fold_start = D.fold_start;
+    q.fold_list = D.fold_list;
+    return q;
+}
+
 __global__ void __launch_bounds__(kBlock, 3) kb_force_grouped(Span sp, BatchArgs A) {
     __shared__ ForceSmem<4> sm;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -578,20 +593,28 @@ __global__ void __launch_bounds__(kBlock, 3) kb_force_grouped(Span sp, BatchArgs
         const BoxDev& D = A.dev[b];
         const BoxStep& S = A.step[b];
         const AtomCols& c = D.set[S.post];
-        ForceSeq q;
-        q.rad = c.planes[D.radius_plane];
-        q.K = S.K;
-        q.nlocal = S.nlocal;
-        q.grp_start = D.grp_start;
-        q.cnt = D.seq_cnt;
-        q.seq = D.seq;
-        q.owner = D.seq_owner;
-        q.fold_start = D.fold_start;
-        q.fold_list = D.fold_list;
+        const ForceSeq q = force_seq_of(D, S, c);
         if (S.newton) force_tile<4, true>(q, c, D.rev, w, sm, lane, wib);
         else force_tile<4, false>(q, c, D.rev, w, sm, lane, wib);
     });
 }
+__global__ void __launch_bounds__(kBlock, 4) kb_force_walk(Span sp, BatchArgs A) {
+    for_span(sp, [&](uint32_t b, uint64_t i, uint32_t) {
+        const BoxDev& D = A.dev[b];
+        const BoxStep& S = A.step[b];
+        const AtomCols& c = D.set[S.post];
+        const ForceSeq q = force_seq_of(D, S, c);
+        if (S.newton) force_walk_root<true>(q, c, D.rev, i);
+        else force_walk_root<false>(q, c, D.rev, i);
+    });
+}
+void b_force_walk(cudaStream_t st, const Span& sp, const BatchArgs& a) {
+    if (sp.total == 0) return;
+    note_launch();
+    const unsigned g = span_grid(sp);
+    kb_force_walk<<<g < 148u * 4u ? g : 148u * 4u, kBlock, 0, st>>>(sp, a);
+}
+
 void b_force_grouped(cudaStream_t st, const Span& sp, const BatchArgs& a) {
     if (sp.total == 0) return;
     note_launch();

@@ -99,16 +99,37 @@ __global__ void __launch_bounds__(kBlock, 4) k_force_seq(ForceArgs p) {
         force_tile<U, FOLD>(p.q, p.c, p.rev, w, sm, lane, wib);
 }
 
-void launch_force_seq(cudaStream_t st, const ForceArgs& p, bool fold) {
-    if (p.q.nlocal == 0) return;
-    note_launch();
-    constexpr int U = 4;
+template <bool FOLD>
+__global__ void __launch_bounds__(kBlock, 4) k_force_walk(ForceArgs p) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < p.q.nlocal;
+         t += (uint64_t)gridDim.x * blockDim.x)
+        force_walk_root<FOLD>(p.q, p.c, p.rev, t);
+}
+
+template <int U>
+static void launch_tiles(cudaStream_t st, const ForceArgs& p, bool fold) {
     const uint64_t ntiles = (p.q.nlocal + 31) / 32;
     const uint64_t need = (ntiles + kForceWarps - 1) / kForceWarps;
     const uint64_t full = 148ull * 4ull;  // one resident wave, grid-stride over the tiles
     const unsigned grid = (unsigned)(need < full ? need : full);
     if (fold) k_force_seq<U, true><<<grid, kBlock, 0, st>>>(p);
     else k_force_seq<U, false><<<grid, kBlock, 0, st>>>(p);
+}
+
+void launch_force_seq(cudaStream_t st, const ForceArgs& p, bool fold, int variant) {
+    if (p.q.nlocal == 0) return;
+    note_launch();
+    if (variant == SOIL_FORCE_WALK) {
+        const unsigned full = 148u * 4u;  // one resident wave at <= 64 registers
+        const unsigned need = (unsigned)((p.q.nlocal + kBlock - 1) / kBlock);
+        const unsigned grid = need < full ? need : full;
+        if (fold) k_force_walk<true><<<grid, kBlock, 0, st>>>(p);
+        else k_force_walk<false><<<grid, kBlock, 0, st>>>(p);
+    } else if (variant == SOIL_FORCE_TILES2) {
+        launch_tiles<2>(st, p, fold);
+    } else {
+        launch_tiles<4>(st, p, fold);
+    }
 }
 
 }  // namespace soil

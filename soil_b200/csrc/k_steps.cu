@@ -63,7 +63,9 @@ __device__ bool grid_sync(GridBar* b, unsigned nblocks, unsigned& gen, uint32_t*
 
 }  // namespace
 
-template <int U, int CONSUMER>  // CONSUMER: 0 none, 1 grouped, 2 grouped + fold
+// CONSUMER: 0 none, 1 grouped, 2 grouped + fold; WALK: one root per thread
+// (force_walk_root), else warp tiles (force_tile)
+template <int U, int CONSUMER, bool WALK>
 __global__ void __launch_bounds__(kBlock, 4) k_steps(StepsArgs a) {
     __shared__ ForceSmem<U> sm;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -97,7 +99,11 @@ __global__ void __launch_bounds__(kBlock, 4) k_steps(StepsArgs a) {
             break;
         }
         // phase B: the consumer over every root's group (and the fold)
-        if (CONSUMER) {
+        if (CONSUMER && WALK) {
+            for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nl;
+                 t += (uint64_t)gridDim.x * blockDim.x)
+                force_walk_root<CONSUMER == 2>(a.fa.q, c, a.fa.rev, t);
+        } else if (CONSUMER) {
             const uint64_t ntiles = (nl + 31) / 32;
             for (uint64_t w = (uint64_t)blockIdx.x * kForceWarps + wib; w < ntiles;
                  w += (uint64_t)gridDim.x * kForceWarps)
@@ -114,14 +120,16 @@ __global__ void __launch_bounds__(kBlock, 4) k_steps(StepsArgs a) {
     }
 }
 
-static const void* steps_kernel(int consumer) {
-    return consumer == 0 ? (const void*)k_steps<4, 0>
-         : consumer == 1 ? (const void*)k_steps<4, 1> : (const void*)k_steps<4, 2>;
+static const void* steps_kernel(int consumer, int walk) {
+    if (consumer == 0) return (const void*)k_steps<4, 0, true>;
+    if (walk) return consumer == 1 ? (const void*)k_steps<4, 1, true> : (const void*)k_steps<4, 2, true>;
+    return consumer == 1 ? (const void*)k_steps<4, 1, false> : (const void*)k_steps<4, 2, false>;
 }
 
-int steps_grid(int consumer, uint64_t nlocal, int* grid) {
+int steps_grid(int consumer, int walk, uint64_t nlocal, int* grid) {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, steps_kernel(consumer), kBlock, 0) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, steps_kernel(consumer, walk), kBlock,
+                                                      0) !=
             cudaSuccess ||
         per_sm < 1) {
         cudaGetLastError();
@@ -139,12 +147,12 @@ int steps_grid(int consumer, uint64_t nlocal, int* grid) {
     return 0;
 }
 
-cudaError_t launch_steps(cudaStream_t st, const StepsArgs& a, int consumer, int grid) {
+cudaError_t launch_steps(cudaStream_t st, const StepsArgs& a, int consumer, int walk, int grid) {
     note_launch();
     StepsArgs arg = a;
     void* params[] = {&arg};
-    return cudaLaunchCooperativeKernel(steps_kernel(consumer), dim3(grid), dim3(kBlock), params, 0,
-                                       st);
+    return cudaLaunchCooperativeKernel(steps_kernel(consumer, walk), dim3(grid), dim3(kBlock),
+                                       params, 0, st);
 }
 
 }  // namespace soil

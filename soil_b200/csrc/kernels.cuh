@@ -330,10 +330,17 @@ struct ForceArgs {
     ForceSeq q;
     PlaneList rev;  // #[reverse] planes folded with the forces
 };
-// The built-in consumer over the grouped sequences (warp-cooperative): F of
-// every local and ghost is overwritten; with fold, ghost forces (and the
-// #[reverse] planes) are then folded into their roots as reverse comm does.
-void launch_force_seq(cudaStream_t st, const ForceArgs& p, bool fold);
+// Kernels of the built-in consumer (SOIL_FORCE): the per-atom gather over the
+// CSR and its transpose with a separate reverse pass (GATHER), or a kernel
+// over the grouped sequences with the fold inside: warp tiles of 32 roots
+// with 4 or 2 rows of 32 entries per chunk (TILES4, TILES2), or one thread
+// per root walking its group (WALK).
+enum { SOIL_FORCE_GATHER = 0, SOIL_FORCE_TILES4 = 1, SOIL_FORCE_TILES2 = 2, SOIL_FORCE_WALK = 3 };
+int force_variant();  // from SOIL_FORCE (default chosen by measurement)
+// The built-in consumer over the grouped sequences: F of every local and
+// ghost is overwritten; with fold, ghost forces (and the #[reverse] planes)
+// are then folded into their roots as reverse comm does.
+void launch_force_seq(cudaStream_t st, const ForceArgs& p, bool fold, int variant);
 
 // ---- device-resident steps (k_steps.cu) --------------------------------------
 // Grid barrier words (count must be 0 when a launch starts).
@@ -351,14 +358,15 @@ struct StepsArgs {
     CheckArgs ck;      // the displacement check (every step)
     FwdArgs fw;        // forward comm of every step
     ForceArgs fa;      // the grouped consumer (consumer != 0)
+    int walk;          // the consumer walks one root per thread (SOIL_FORCE_WALK)
     uint64_t max_steps;
     GridBar* bar;
     DevFlags* flags;   // flags->rebuild must be 0 at launch
     uint32_t* out;     // out[0]: steps completed; out[1]: 1 if the next step's check tripped
 };
 // Cooperative grid for k_steps (consumer: 0 none, 1 grouped, 2 grouped + fold).
-int steps_grid(int consumer, uint64_t nlocal, int* grid);
-cudaError_t launch_steps(cudaStream_t st, const StepsArgs& a, int consumer, int grid);
+int steps_grid(int consumer, int walk, uint64_t nlocal, int* grid);
+cudaError_t launch_steps(cudaStream_t st, const StepsArgs& a, int consumer, int walk, int grid);
 
 void launch_harmonic(cudaStream_t st, uint64_t nlocal, uint64_t ntotal, const AtomCols& c,
                      const double* radius, double k, int newton, const uint32_t* offsets,

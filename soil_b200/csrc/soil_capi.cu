@@ -1064,6 +1064,18 @@ int build_seq(soil_sys* s) {
     return SOIL_OK;
 }
 
+// The consumer kernel (SOIL_FORCE: gather, tiles4, tiles2, walk); read at
+// each call so a host can compare them on one system.
+int force_variant() {
+    const char* env = std::getenv("SOIL_FORCE");
+    if (!env) return kDefaultForce;
+    if (!std::strcmp(env, "gather")) return SOIL_FORCE_GATHER;
+    if (!std::strcmp(env, "tiles4")) return SOIL_FORCE_TILES4;
+    if (!std::strcmp(env, "tiles2")) return SOIL_FORCE_TILES2;
+    if (!std::strcmp(env, "walk")) return SOIL_FORCE_WALK;
+    return kDefaultForce;
+}
+
 // Whether the grouped consumer serves this system: the built-in consumer,
 // and a ghost layout in which no local has images on both sides of a dim
 // (at most 7 images per root, what the sequences' owner byte encodes).
@@ -1089,7 +1101,8 @@ ForceArgs consumer_args(const soil_sys* s) {
 // #[reverse] planes is done in the same kernel.
 int launch_consumer(soil_sys* s, bool fold) {
     if (!s->in_lists_valid) TRY(build_in_lists(s));
-    if (!seq_consumer(s)) {
+    const int variant = force_variant();
+    if (!seq_consumer(s) || variant == SOIL_FORCE_GATHER) {
         launch_harmonic(s->st, s->nlocal, s->nlocal + s->nghost, s->A,
                         s->A.planes[s->cols[s->radius_col].plane0], s->harmonic_k,
                         s->newton ? 1 : 0, s->offsets.p, s->indices.p, s->in_start.p,
@@ -1097,7 +1110,7 @@ int launch_consumer(soil_sys* s, bool fold) {
         return check_launch(s);
     }
     if (!s->seq_valid) TRY(build_seq(s));
-    launch_force_seq(s->st, consumer_args(s), fold);
+    launch_force_seq(s->st, consumer_args(s), fold, variant);
     return check_launch(s);
 }
 
@@ -1148,7 +1161,7 @@ int neighbor_plan(soil_sys* s) {
 // SOIL_PAIRS_STAGED=0), which then scans from global memory.
 bool pair_segments(const std::vector<int32_t>& sten, bool has_self, bool newton, PairSegs* sg) {
     const char* env = std::getenv("SOIL_PAIRS_STAGED");
-    if (env && std::atoi(env) == 0) return false;
+    if (!env || std::atoi(env) == 0) return false;  // measured slower: off unless asked
     sg->n = 0;
     sg->own = has_self ? 1 : 0;
     if (has_self) {
@@ -1265,7 +1278,7 @@ int phase_neighbor(soil_sys* s) {
     s->seq_valid = false;
     // the transposed lists serve the built-in consumer and any force hook
     if (builtin_consumer(s) || s->hook) TRY(build_in_lists(s));
-    if (seq_consumer(s)) TRY(build_seq(s));
+    // the grouped sequences are built when a consumer kernel first needs them
     return SOIL_OK;
 }
 
@@ -1352,12 +1365,20 @@ int phase_final(soil_sys* s) {
 // valid lists and ghosts (CommunicateOnly), and nothing between the
 // integration and forward comm moves atoms or changes the box or the swap
 // offsets (no deform, shear or shrink-wrap).
-bool fused_forward_ok(const soil_sys* s) {
+bool fused_forward_allowed(const soil_sys* s) {
     if (s->state != COMMUNICATE_ONLY || s->nghost == 0 || s->nswaps == 0) return false;
     if (s->shear || has_axis_deform(s)) return false;
     for (int d = 0; d < 3; ++d)
         if (s->btype[d] == SOIL_BOUNDARY_SHRINK) return false;
     return true;
+}
+
+// ... and SOIL_FWD_FUSED (default on) keeps it in the pass of soil_step's
+// launch-per-phase steps (the resident steps always fuse it).
+bool fused_forward_ok(const soil_sys* s) {
+    const char* env = std::getenv("SOIL_FWD_FUSED");
+    if (env && std::atoi(env) == 0) return false;
+    return fused_forward_allowed(s);
 }
 
 // What the integration pass of a step decided, for the rest of the step.
@@ -1462,7 +1483,8 @@ int step_rest(soil_sys* s, const StepPlan& p, bool last) {
     // With newton, the grouped consumer folds ghost forces into their roots
     // in the same kernel (reverse_send_force's fold order); otherwise the
     // force and reverse-comm phases run apart.
-    const bool fold_fused = !s->hook && seq_consumer(s) && s->newton;
+    const bool fold_fused =
+        !s->hook && seq_consumer(s) && s->newton && force_variant() != SOIL_FORCE_GATHER;
     timer_begin(s, T_FORCE);
     if (fold_fused) {
         TRY(launch_consumer(s, true));
@@ -1516,7 +1538,7 @@ uint64_t resident_limit(const soil_sys* s, uint64_t want) {
     if (s->hook || s->timing_mask || !s->check || s->every != 0) return 0;
     if (s->state != COMMUNICATE_ONLY || !displacement_needed(s) || needs_rebuild_with(s, false))
         return 0;
-    if (!fused_forward_ok(s)) return 0;
+    if (!fused_forward_allowed(s)) return 0;
     const bool consumer = builtin_consumer(s);
     if (consumer && !seq_consumer(s)) return 0;
     int idx[kMaxPlanes], nz, nr;
@@ -1548,12 +1570,15 @@ int resident_steps(soil_sys* s, uint64_t max, uint64_t* done, bool* tripped, Ste
     a.ck = make_check(s->lbx.p, s->lby.p, s->lbz.p, s->nlocal, displacement_threshold_sq(s),
                       s->pbc_box, s->dflags, pbc_mask(s));
     a.fw = fwd_args(s, p.fused_zero);
+    a.walk = 0;
     int kind = 0;
     if (consumer) {
         if (!s->in_lists_valid) TRY(build_in_lists(s));
         if (!s->seq_valid) TRY(build_seq(s));
         a.fa = consumer_args(s);
         kind = s->newton ? 2 : 1;
+        const int v = force_variant();
+        a.walk = (v == SOIL_FORCE_TILES4 || v == SOIL_FORCE_TILES2) ? 0 : 1;
     }
     a.max_steps = max;
     TRY(ensure(s, s->rstate, 4));
@@ -1561,12 +1586,12 @@ int resident_steps(soil_sys* s, uint64_t max, uint64_t* done, bool* tripped, Ste
     a.out = s->rstate.p + 2;
     a.flags = s->dflags;
     int grid = 0;
-    if (steps_grid(kind, s->nlocal, &grid))
+    if (steps_grid(kind, a.walk, s->nlocal, &grid))
         return fail(s->ctx, SOIL_ERR_CUDA, "no cooperative occupancy for the resident steps");
     CK(cudaMemsetAsync(s->rstate.p, 0, 4 * 4, s->st));
     CK(cudaMemsetAsync(&s->dflags->rebuild, 0, 4, s->st));
     CK(cudaMemsetAsync(&s->dflags->error, 0, 4, s->st));
-    CK(launch_steps(s->st, a, kind, grid));
+    CK(launch_steps(s->st, a, kind, a.walk, grid));
     CK(cudaMemcpyAsync(s->hword, a.out, 8, cudaMemcpyDeviceToHost, s->st));
     TRY(read_flags(s));
     if (s->hflags->error & SOIL_STEPS_ERR_BARRIER)

@@ -1,0 +1,59 @@
+"""Every kernel of the built-in consumer (SOIL_FORCE: the per-atom gather with
+a separate reverse pass, warp tiles with 4 or 2 rows per chunk, one root per
+thread) gives the reference's forces bit for bit: single systems with newton
+on and off against the CPU oracle, and batched boxes against the same boxes
+alone."""
+import os
+
+import pytest
+
+import oracle
+from helpers import assert_same_lists, assert_same_state
+from soil_b200 import system, workloads as W
+
+pytestmark = pytest.mark.gpu
+
+VARIANTS = ["gather", "tiles4", "tiles2", "walk"]
+
+
+@pytest.fixture
+def variant_env(request):
+    old = os.environ.get("SOIL_FORCE")
+    os.environ["SOIL_FORCE"] = request.param
+    yield request.param
+    if old is None:
+        del os.environ["SOIL_FORCE"]
+    else:
+        os.environ["SOIL_FORCE"] = old
+
+
+@pytest.mark.parametrize("variant_env", VARIANTS, indirect=True)
+@pytest.mark.parametrize("newton", [1, 0])
+def test_consumer_variant_matches_oracle(ctx, variant_env, newton):
+    w = W.poly("fv", 91, 4000, 0.5, 1e-3, 0, harmonic_k=1e3, newton=newton)
+    w.vel *= 2.0
+    g, o = system.from_workload(ctx, w), oracle.from_workload(w)
+    for k in range(3):
+        g.step(10)
+        o.step(10)
+        assert_same_state(g, o, f"{variant_env} newton={newton} step {10 * (k + 1)}")
+        assert_same_lists(g, o)
+    assert g.counts().rebuilds > 2
+    g.close()
+
+
+@pytest.mark.parametrize("variant_env", VARIANTS, indirect=True)
+def test_consumer_variant_batched_equals_alone(ctx, variant_env):
+    ws = [W.config4_box(i, steps=0) for i in (4, 5, 6)]
+    alone = [system.from_workload(ctx, w) for w in ws]
+    for s in alone:
+        s.step(15)
+    boxes = [system.from_workload(ctx, w) for w in ws]
+    b = system.Batch(ctx)
+    for s in boxes:
+        b.add(s)
+    b.step(15)
+    for w, a, s in zip(ws, alone, boxes):
+        assert_same_state(a, s, f"{variant_env} {w.name}")
+        assert_same_lists(a, s, w.name)
+    b.close()
