@@ -30,6 +30,9 @@
 //               its root and images and, with FOLD, folds the images into the
 //               root exactly as reverse_send_force does (fold_root), so
 //               reverse comm needs no pass of its own (force_ops.cuh).
+#include <cstdlib>
+#include <cstring>
+
 #include "device_ops.cuh"
 #include "force_ops.cuh"
 #include "kernels.cuh"
@@ -114,6 +117,18 @@ static void launch_tiles(cudaStream_t st, const ForceArgs& p, bool fold) {
     const unsigned grid = (unsigned)(need < full ? need : full);
     if (fold) k_force_seq<U, true><<<grid, kBlock, 0, st>>>(p);
     else k_force_seq<U, false><<<grid, kBlock, 0, st>>>(p);
+}
+
+// The consumer kernel (SOIL_FORCE: gather, tiles4, tiles2, walk); read at
+// each call so a host can compare them on one system.
+int force_variant() {
+    const char* env = std::getenv("SOIL_FORCE");
+    if (!env) return kDefaultForce;
+    if (!std::strcmp(env, "gather")) return SOIL_FORCE_GATHER;
+    if (!std::strcmp(env, "tiles4")) return SOIL_FORCE_TILES4;
+    if (!std::strcmp(env, "tiles2")) return SOIL_FORCE_TILES2;
+    if (!std::strcmp(env, "walk")) return SOIL_FORCE_WALK;
+    return kDefaultForce;
 }
 
 void launch_force_seq(cudaStream_t st, const ForceArgs& p, bool fold, int variant) {

@@ -336,6 +336,7 @@ struct ForceArgs {
 // with 4 or 2 rows of 32 entries per chunk (TILES4, TILES2), or one thread
 // per root walking its group (WALK).
 enum { SOIL_FORCE_GATHER = 0, SOIL_FORCE_TILES4 = 1, SOIL_FORCE_TILES2 = 2, SOIL_FORCE_WALK = 3 };
+constexpr int kDefaultForce = SOIL_FORCE_WALK;  // when SOIL_FORCE is unset
 int force_variant();  // from SOIL_FORCE (default chosen by measurement)
 // The built-in consumer over the grouped sequences: F of every local and
 // ghost is overwritten; with fold, ghost forces (and the #[reverse] planes)

@@ -1064,18 +1064,6 @@ int build_seq(soil_sys* s) {
     return SOIL_OK;
 }
 
-// The consumer kernel (SOIL_FORCE: gather, tiles4, tiles2, walk); read at
-// each call so a host can compare them on one system.
-int force_variant() {
-    const char* env = std::getenv("SOIL_FORCE");
-    if (!env) return kDefaultForce;
-    if (!std::strcmp(env, "gather")) return SOIL_FORCE_GATHER;
-    if (!std::strcmp(env, "tiles4")) return SOIL_FORCE_TILES4;
-    if (!std::strcmp(env, "tiles2")) return SOIL_FORCE_TILES2;
-    if (!std::strcmp(env, "walk")) return SOIL_FORCE_WALK;
-    return kDefaultForce;
-}
-
 // Whether the grouped consumer serves this system: the built-in consumer,
 // and a ghost layout in which no local has images on both sides of a dim
 // (at most 7 images per root, what the sequences' owner byte encodes).

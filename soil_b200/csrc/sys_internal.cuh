@@ -259,7 +259,5 @@ constexpr int kRowSlotsPerAtom = 16;
 // Largest system that takes the device-resident light steps by default
 // (SOIL_RESIDENT_STEPS=1 forces them on at any size, 0 off).
 constexpr uint64_t kResidentAutoMaxAtoms = 1ull << 20;
-// consumer kernel when SOIL_FORCE is unset
-constexpr int kDefaultForce = SOIL_FORCE_WALK;
 
 }  // namespace soil_host
