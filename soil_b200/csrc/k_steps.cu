@@ -11,9 +11,11 @@
 //   barrier; every CTA reads the check: if any atom moved too far, the
 //            launch ends here (step t's integration is done, its rebuild is
 //            the host's);
-//   phase B  the grouped consumer with the reverse fold (if any);
-//   barrier (so no CTA's next phase A can set the check flag before every
-//            CTA has read it); next step.
+//   phase B  the grouped consumer with the reverse fold (if any), then a
+//            barrier (the next phase A reads the forces and moves the atoms
+//            phase B reads); next step.  Without a consumer one barrier per
+//            step suffices: the check flag rotates through three slots, so a
+//            slot is cleared only after every CTA has read it.
 //
 // Each step runs the same per-atom functions in the same order as the
 // launch-per-phase path, so results are bit-identical.  The grid barrier is
@@ -52,7 +54,7 @@ __device__ bool grid_sync(GridBar* b, unsigned nblocks, unsigned& gen, uint32_t*
                     ok = 0;
                     break;
                 }
-                __nanosleep(100);
+                if (spins > 256) __nanosleep(100);  // a short busy wait first
             }
         }
         gen += 1;
@@ -77,10 +79,12 @@ __global__ void __launch_bounds__(kBlock, 4) k_steps(StepsArgs a) {
     if (threadIdx.x == 0)
         gen = cuda::atomic_ref<unsigned, cuda::thread_scope_device>(a.bar->gen)
                   .load(cuda::memory_order_relaxed);
-    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> tripped(a.flags->rebuild);
     uint64_t done = 0;
     bool stop = false;
     for (uint64_t step = 0; step < a.max_steps; ++step) {
+        // the check flag of this step: three slots in rotation, so a slot is
+        // cleared (two steps ahead, by CTA 0) only after every CTA read it
+        uint32_t* slot = a.trip + step % 3;
         // phase A: the fused integration pass
         const bool fuse_final = step > 0 || a.first_fused;
         bool hit = false;
@@ -92,12 +96,16 @@ __global__ void __launch_bounds__(kBlock, 4) k_steps(StepsArgs a) {
             forward_images(c, nl, i, x, y, z, vx, vy, vz, a.fw.fold_start, a.fw.fold_list,
                            a.fw.chain, a.fw.sc, a.fw.fwd, a.fw.zero_ghost_force != 0);
         }
-        if (__ballot_sync(0xffffffffu, hit) && lane == 0) atomicOr(&a.flags->rebuild, 1u);
+        if (__ballot_sync(0xffffffffu, hit) && lane == 0) atomicOr(slot, 1u);
         if (!grid_sync(a.bar, gridDim.x, gen, &a.flags->error)) return;
-        if (tripped.load(cuda::memory_order_relaxed)) {
+        if (cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(*slot).load(
+                cuda::memory_order_relaxed)) {
             stop = true;
             break;
         }
+        if (blockIdx.x == 0 && threadIdx.x == 0)
+            cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(a.trip[(step + 2) % 3])
+                .store(0u, cuda::memory_order_relaxed);
         // phase B: the consumer over every root's group (and the fold)
         if (CONSUMER && WALK) {
             for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nl;
@@ -109,14 +117,15 @@ __global__ void __launch_bounds__(kBlock, 4) k_steps(StepsArgs a) {
                  w += (uint64_t)gridDim.x * kForceWarps)
                 force_tile<U, CONSUMER == 2>(a.fa.q, c, a.fa.rev, w, sm, lane, wib);
         }
-        // Also without a consumer: no CTA may set the flag in the next phase A
-        // before every CTA has read it above.
-        if (!grid_sync(a.bar, gridDim.x, gen, &a.flags->error)) return;
+        // phase A of the next step reads the forces and moves the atoms
+        // phase B reads: with a consumer, every CTA must be done first
+        if (CONSUMER && !grid_sync(a.bar, gridDim.x, gen, &a.flags->error)) return;
         ++done;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         a.out[0] = (uint32_t)done;
         a.out[1] = stop ? 1u : 0u;
+        if (stop) a.flags->rebuild = 1u;  // decide_rebuild on the host reads it
     }
 }
 

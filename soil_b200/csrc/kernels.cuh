@@ -362,8 +362,9 @@ struct StepsArgs {
     int walk;          // the consumer walks one root per thread (SOIL_FORCE_WALK)
     uint64_t max_steps;
     GridBar* bar;
-    DevFlags* flags;   // flags->rebuild must be 0 at launch
+    DevFlags* flags;   // flags->rebuild is set when a check trips
     uint32_t* out;     // out[0]: steps completed; out[1]: 1 if the next step's check tripped
+    uint32_t* trip;    // 3 check-flag slots, zero at launch
 };
 // Cooperative grid for k_steps (consumer: 0 none, 1 grouped, 2 grouped + fold).
 int steps_grid(int consumer, int walk, uint64_t nlocal, int* grid);

@@ -1569,14 +1569,15 @@ int resident_steps(soil_sys* s, uint64_t max, uint64_t* done, bool* tripped, Ste
         a.walk = (v == SOIL_FORCE_TILES4 || v == SOIL_FORCE_TILES2) ? 0 : 1;
     }
     a.max_steps = max;
-    TRY(ensure(s, s->rstate, 4));
+    TRY(ensure(s, s->rstate, 8));
     a.bar = reinterpret_cast<GridBar*>(s->rstate.p);
     a.out = s->rstate.p + 2;
+    a.trip = s->rstate.p + 4;
     a.flags = s->dflags;
     int grid = 0;
     if (steps_grid(kind, a.walk, s->nlocal, &grid))
         return fail(s->ctx, SOIL_ERR_CUDA, "no cooperative occupancy for the resident steps");
-    CK(cudaMemsetAsync(s->rstate.p, 0, 4 * 4, s->st));
+    CK(cudaMemsetAsync(s->rstate.p, 0, 8 * 4, s->st));
     CK(cudaMemsetAsync(&s->dflags->rebuild, 0, 4, s->st));
     CK(cudaMemsetAsync(&s->dflags->error, 0, 4, s->st));
     CK(launch_steps(s->st, a, kind, a.walk, grid));
