@@ -3,6 +3,9 @@
 // tile sums -> one-CTA scan of the sums -> tile scans with the carry-in.
 // 256 threads x 8 consecutive items per thread; warp shuffles inside a warp,
 // shared memory across the 8 warps.
+#include <atomic>
+#include <cuda/atomic>
+
 #include "block_scan.cuh"
 #include "kernels.cuh"
 
@@ -83,6 +86,120 @@ void exclusive_scan_u32(cudaStream_t st, const uint32_t* in, uint32_t* out, uint
     k_scan_partials<<<1, kBlock, 0, st>>>(temp, ntiles);
     note_launch();
     k_scan_down<<<(unsigned)ntiles, kBlock, 0, st>>>(in, out, n, temp, ntiles);
+}
+
+// ---- single-pass scan (decoupled look-back) ---------------------------------
+//
+// One launch of ntiles CTAs.  Each CTA claims the next tile from an atomic
+// counter (so every tile with a smaller number is held by a CTA that already
+// runs), publishes its tile's sum, looks back over its predecessors'
+// descriptors until it meets an inclusive prefix, publishes its own inclusive
+// prefix and writes its tile.  A descriptor is 64 bits: the call's epoch (30
+// bits), a status (1: tile sum, 2: inclusive prefix) and the value; the epoch
+// makes descriptors of earlier calls read as not yet published, so nothing is
+// cleared between calls.  The CTA that claims the last tile puts the counter
+// back to zero.  Waits are bounded; one that runs out sets SOIL_SCAN_ERR in
+// *err (when given) and counts the missing tiles as zero.
+
+constexpr uint64_t kLookbackSpinLimit = 1ull << 22;
+constexpr uint64_t kDescAgg = 1, kDescInc = 2;
+
+__device__ __forceinline__ uint64_t desc_pack(uint32_t epoch, uint64_t status, uint32_t v) {
+    return ((uint64_t)(epoch & 0x3fffffffu) << 34) | (status << 32) | v;
+}
+
+__global__ void __launch_bounds__(kBlock) k_scan_1p(const uint32_t* in, uint32_t* out, uint64_t n,
+                                                    uint32_t* counter, uint64_t* desc,
+                                                    uint32_t epoch, uint32_t* err) {
+    __shared__ uint32_t s_tile, s_prefix, tot;
+    if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint64_t ntiles = (n + kScanTile - 1) / kScanTile;
+    if (threadIdx.x == 0 && tile == ntiles - 1) atomicExch(counter, 0u);  // the last claim
+    const uint64_t base = (uint64_t)tile * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = (base + k < n) ? in[base + k] : 0;
+        s += v[k];
+    }
+    uint32_t pre = block_exclusive_scan(s, &tot);
+    const uint32_t agg = tot;
+    const uint32_t ep = epoch & 0x3fffffffu;
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        uint32_t prefix = 0;
+        if (tile == 0) {
+            if (lane == 0)
+                cuda::atomic_ref<uint64_t, cuda::thread_scope_device>(desc[0]).store(
+                    desc_pack(ep, kDescInc, agg), cuda::memory_order_release);
+        } else {
+            if (lane == 0)
+                cuda::atomic_ref<uint64_t, cuda::thread_scope_device>(desc[tile]).store(
+                    desc_pack(ep, kDescAgg, agg), cuda::memory_order_release);
+            int64_t look = (int64_t)tile - 1;
+            for (;;) {
+                const int64_t idx = look - lane;  // lane 0: the nearest predecessor
+                uint64_t st = kDescInc;  // lanes past tile 0 take no part
+                uint32_t val = 0;
+                if (idx >= 0) {
+                    cuda::atomic_ref<uint64_t, cuda::thread_scope_device> d(desc[idx]);
+                    st = 0;
+                    for (uint64_t spin = 0; spin < kLookbackSpinLimit; ++spin) {
+                        const uint64_t x = d.load(cuda::memory_order_acquire);
+                        if ((uint32_t)(x >> 34) == ep && ((x >> 32) & 3u)) {
+                            st = (x >> 32) & 3u;
+                            val = (uint32_t)x;
+                            break;
+                        }
+                    }
+                    if (st == 0) {
+                        if (err) atomicOr(err, SOIL_SCAN_ERR);
+                        st = kDescAgg;  // counted as zero
+                    }
+                }
+                const unsigned inc = __ballot_sync(0xffffffffu, idx >= 0 && st == kDescInc);
+                const int stop = inc ? __ffs(inc) - 1 : 31;
+                uint32_t part = (lane <= stop && idx >= 0) ? val : 0u;
+                for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+                prefix += part;
+                if (inc || look - 32 < 0) break;
+                look -= 32;
+            }
+            if (lane == 0)
+                cuda::atomic_ref<uint64_t, cuda::thread_scope_device>(desc[tile]).store(
+                    desc_pack(ep, kDescInc, prefix + agg), cuda::memory_order_release);
+        }
+        if (lane == 0) s_prefix = prefix;
+    }
+    __syncthreads();
+    pre += s_prefix;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) out[base + k] = pre;
+        pre += v[k];
+    }
+    if (tile == ntiles - 1 && threadIdx.x == kBlock - 1) out[n] = pre;
+}
+
+uint64_t scan1p_words(uint64_t n) { return 2 * ((n + kScanTile - 1) / kScanTile) + 4; }
+
+static std::atomic<uint32_t> g_scan_epoch{1};
+
+void exclusive_scan_1p(cudaStream_t st, const uint32_t* in, uint32_t* out, uint64_t n,
+                       uint32_t* temp, uint32_t* err) {
+    const uint64_t ntiles = (n + kScanTile - 1) / kScanTile;
+    if (ntiles == 0) {
+        cudaMemsetAsync(out, 0, sizeof(uint32_t), st);
+        return;
+    }
+    const uint32_t epoch = g_scan_epoch.fetch_add(1, std::memory_order_relaxed);
+    note_launch();
+    k_scan_1p<<<(unsigned)ntiles, kBlock, 0, st>>>(in, out, n, temp,
+                                                  reinterpret_cast<uint64_t*>(temp + 2), epoch,
+                                                  err);
 }
 
 }  // namespace soil

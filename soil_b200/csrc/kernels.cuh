@@ -123,6 +123,14 @@ void launch_save_positions(cudaStream_t st, uint64_t n, const AtomCols& c, doubl
 uint64_t scan_temp_words(uint64_t n);
 void exclusive_scan_u32(cudaStream_t st, const uint32_t* in, uint32_t* out, uint64_t n,
                         uint32_t* temp);
+// The same scan in one launch (decoupled look-back, k_scan.cu).  temp holds
+// scan1p_words(n) u32, 8-byte aligned, and must be zero when first used (its
+// words are left ready for the next call).  err: optional flag word that gets
+// SOIL_SCAN_ERR if a look-back wait runs out.
+constexpr uint32_t SOIL_SCAN_ERR = 16u;
+uint64_t scan1p_words(uint64_t n);
+void exclusive_scan_1p(cudaStream_t st, const uint32_t* in, uint32_t* out, uint64_t n,
+                       uint32_t* temp, uint32_t* err);
 
 // ---- bins (k_bins.cu) -----------------------------------------------------
 // cell[i] = cell_of(pos[first+i]) and counts[cell]++ for i in [0, n)

@@ -310,6 +310,16 @@ int sync(soil_sys* s) {
     return SOIL_OK;
 }
 
+int scan_1p(soil_sys* s, const uint32_t* in, uint32_t* out, uint64_t n) {
+    const uint64_t need = scan1p_words(n);
+    if (!s->scan1p.p || s->scan1p.cap < need) {
+        TRY(ensure(s, s->scan1p, need, 0, scan1p_words(2 * n + 4096)));
+        CK(cudaMemsetAsync(s->scan1p.p, 0, s->scan1p.cap * 4, s->st));
+    }
+    exclusive_scan_1p(s->st, in, out, n, s->scan1p.p, &s->dflags->fault);
+    return SOIL_OK;
+}
+
 int check_launch(soil_sys* s) {
     CK(cudaGetLastError());
     return SOIL_OK;
@@ -588,7 +598,10 @@ bool displacement_needed(const soil_sys* s) {
 
 int read_flags(soil_sys* s) {
     CK(cudaMemcpyAsync(s->hflags, s->dflags, sizeof(DevFlags), cudaMemcpyDeviceToHost, s->st));
-    return sync(s);
+    TRY(sync(s));
+    if (s->hflags->fault & SOIL_SCAN_ERR)
+        return fail(s->ctx, SOIL_ERR_CUDA, "a single-pass scan's look-back wait ran out");
+    return SOIL_OK;
 }
 
 int phase_decide_rebuild(soil_sys* s) {
@@ -809,7 +822,7 @@ int phase_sort(soil_sys* s) {
     const uint64_t nc = s->total_cells;
     CK(cudaMemsetAsync(s->cell_counts.p, 0, nc * 4, s->st));
     launch_cells(s->st, 0, nl, s->A, grid_of(s), s->sort_cell.p, s->cell_counts.p);
-    exclusive_scan_u32(s->st, s->cell_counts.p, s->cell_start.p, nc, s->scan_tmp.p);
+    TRY(scan_1p(s, s->cell_counts.p, s->cell_start.p, nc));
     CK(cudaMemcpyAsync(s->cell_cursor.p, s->cell_start.p, nc * 4, cudaMemcpyDeviceToDevice, s->st));
     launch_scatter(s->st, nl, s->sort_cell.p, s->cell_cursor.p, s->sort_perm.p);
     launch_segsort(s->st, nc, s->cell_start.p, s->sort_perm.p);
@@ -1025,7 +1038,7 @@ int build_in_lists(soil_sys* s) {
     TRY(ensure(s, s->scan_tmp, scan_temp_words(total + 2)));
     CK(cudaMemsetAsync(s->in_count.p, 0, total * 4, s->st));
     launch_in_count(s->st, s->nlocal, s->offsets.p, s->indices.p, s->in_count.p);
-    exclusive_scan_u32(s->st, s->in_count.p, s->in_start.p, total, s->scan_tmp.p);
+    TRY(scan_1p(s, s->in_count.p, s->in_start.p, total));
     CK(cudaMemcpyAsync(s->in_cursor.p, s->in_start.p, total * 4, cudaMemcpyDeviceToDevice, s->st));
     launch_in_scatter(s->st, s->nlocal, s->offsets.p, s->indices.p, s->in_cursor.p, s->in_list.p);
     launch_segsort(s->st, total, s->in_start.p, s->in_list.p);
@@ -1057,7 +1070,7 @@ int build_seq(soil_sys* s) {
     q.fold_start = s->fold_start.p;
     q.fold_list = s->fold_list.p;
     launch_seq_count(s->st, q, s->seq_cnt.p, s->grp_cnt.p);
-    exclusive_scan_u32(s->st, s->grp_cnt.p, s->grp_start.p, nl, s->scan_tmp.p);
+    TRY(scan_1p(s, s->grp_cnt.p, s->grp_start.p, nl));
     launch_seq_fill(s->st, q, s->grp_start.p, s->seq.p, s->seq_owner.p);
     TRY(check_launch(s));
     s->seq_valid = true;
@@ -1211,7 +1224,7 @@ int phase_neighbor(soil_sys* s) {
         launch_cells(s->st, 0, total, s->A, gr, s->atom_cell.p, s->cell_counts.p);
     }
     s->local_cells_valid = false;
-    exclusive_scan_u32(s->st, s->cell_counts.p, s->cell_start.p, nc, s->scan_tmp.p);
+    TRY(scan_1p(s, s->cell_counts.p, s->cell_start.p, nc));
     CK(cudaMemcpyAsync(s->cell_cursor.p, s->cell_start.p, nc * 4, cudaMemcpyDeviceToDevice, s->st));
     launch_scatter(s->st, total, s->atom_cell.p, s->cell_cursor.p, s->sorted_atoms.p);
     launch_segsort(s->st, nc, s->cell_start.p, s->sorted_atoms.p);
@@ -1248,7 +1261,7 @@ int phase_neighbor(soil_sys* s) {
         launch_pair_count_staged(s->st, p, sg, s->rowcount.p, s->row_slots.p, s->dflags);
     else
         launch_pair_count(s->st, p, s->rowcount.p, s->row_slots.p, s->dflags);
-    exclusive_scan_u32(s->st, s->rowcount.p, s->offsets.p, nl, s->scan_tmp.p);
+    TRY(scan_1p(s, s->rowcount.p, s->offsets.p, nl));
     CK(cudaMemcpyAsync(&s->hword[0], s->offsets.p + nl, 4, cudaMemcpyDeviceToHost, s->st));
     TRY(check_launch(s));
     TRY(read_flags(s));
@@ -1785,7 +1798,7 @@ int soil_sys_destroy(soil_sys* s) {
     for (int k = 0; k < 2; ++k) { fr(s->slot_tag[k]); fr(s->slot_val[k]); }
     fr(s->in_count); fr(s->in_start); fr(s->in_cursor); fr(s->in_list);
     fr(s->seq_cnt); fr(s->grp_cnt); fr(s->grp_start); fr(s->seq); fr(s->seq_owner);
-    fr(s->rstate);
+    fr(s->rstate); fr(s->scan1p);
     fr(s->ghost_root); fr(s->ghost_chain);
     fr(s->fold_start); fr(s->fold_list);
     for (auto& a : s->send) fr(a);

@@ -127,7 +127,7 @@ struct DevFlags {
     uint64_t candidates;     // pair candidates tested in the last build
     uint64_t rechecked;      // candidates re-tested in FP64
     uint32_t error;          // device-side guard tripped (index out of range)
-    uint32_t pad;
+    uint32_t fault;          // a bounded device wait ran out (never cleared)
 };
 
 }  // namespace soil

@@ -143,6 +143,7 @@ struct soil_sys {
     bool seq_valid = false;
     bool few_images = false;  // no local has images on both sides of a dim (<= 7 images)
     DArr<uint32_t> rstate;    // resident steps: grid barrier words, step count, trip flag
+    DArr<uint32_t> scan1p;    // single-pass scan: tile counter and descriptors (zeroed at growth)
     DArr<uint32_t> ghost_root, ghost_chain;
     DArr<uint32_t> fold_start, fold_list;  // reverse-comm fold program (written by borders)
     DArr<uint32_t> send[kNumSwaps];
@@ -246,6 +247,9 @@ float pair_eps(const soil_sys* s);
 bool pair_segments(const std::vector<int32_t>& sten, bool has_self, bool newton, PairSegs* sg);
 int sync(soil_sys* s);
 int check_launch(soil_sys* s);
+// exclusive scan of in[0, n) into out[0, n] in one launch, errors into the
+// system's device flags
+int scan_1p(soil_sys* s, const uint32_t* in, uint32_t* out, uint64_t n);
 Geom geom_of(const soil_sys* s);
 Grid grid_of(const soil_sys* s);
 void compute_bin_grid(soil_sys* s);
