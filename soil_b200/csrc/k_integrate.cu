@@ -25,8 +25,9 @@ unsigned grid_for(uint64_t n, int block, int per_sm) {
 //   h = 0.5*dt*inv_m;  v += h*F;  x += v*dt
 // With FWD, each local then writes its ghost images (forward_comm of a step
 // that keeps its lists): the values forward comm would copy after this pass.
+// Capped at 48 registers (5 blocks per SM) without spills.
 template <bool FUSE_FINAL, bool FWD>
-__global__ void __launch_bounds__(kBlock) k_initial(uint64_t n, AtomCols c, double dt,
+__global__ void __launch_bounds__(kBlock, 5) k_initial(uint64_t n, AtomCols c, double dt,
                                                     int zero_force, CheckArgs ck, FwdArgs fw) {
     bool hit = false;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
