@@ -877,7 +877,9 @@ int batch_step(soil_batch* b, bool last) {
             TRY(ensure(s, s->in_start, total + 2, 0, s->acap + 2));
             TRY(ensure(s, s->in_cursor, total + 1, 0, s->acap + 1));
             TRY(ensure(s, s->in_list, np + 1, 0, pair_room(np)));
-            if (s->few_images) {  // the grouped consumer's sequences, built this step
+            const int fv = force_variant();
+            if (s->few_images && fv != SOIL_FORCE_GATHER && fv != SOIL_FORCE_CSR) {
+                // the grouped consumer's sequences, built this step
                 TRY(ensure(s, s->seq_cnt, total + 1, 0, s->acap + 1));
                 TRY(ensure(s, s->grp_cnt, s->nlocal + 1, 0, s->acap + 1));
                 TRY(ensure(s, s->grp_start, s->nlocal + 2, 0, s->acap + 2));
@@ -903,7 +905,7 @@ int batch_step(soil_batch* b, bool last) {
     const int r_loc = stage_add(g5), r_all = stage_add(g5), r_scan = stage_add(g5),
               h_all = stage_add(g5), v_loc = stage_add(g5), l_loc = stage_add(g5),
               q_all = stage_add(g5), q_grp = stage_add(g5), q_loc = stage_add(g5),
-              t_tiles = stage_add(g5), t_walk = stage_add(g5);
+              t_tiles = stage_add(g5), t_walk = stage_add(g5), t_csr = stage_add(g5);
     // Boxes whose locals have at most 7 images take the grouped consumer (its
     // sequences built at each rebuild, reverse comm folded in); the others the
     // per-atom gather and a reverse pass.
@@ -913,7 +915,8 @@ int batch_step(soil_batch* b, bool last) {
         const auto& h = b->hot[k];
         const soil_sys* s = b->slot[k];
         const uint64_t nl = h.nlocal, total = nl + h.nghost;
-        const bool grouped = variant != SOIL_FORCE_GATHER && s->few_images &&
+        const bool csr = variant == SOIL_FORCE_CSR;
+        const bool grouped = !csr && variant != SOIL_FORCE_GATHER && s->few_images &&
                              (b->rebuild[k] || s->seq_valid);
         if (b->rebuild[k]) {
             g5.spans[r_loc].add_nz(k, nl, 0);
@@ -926,7 +929,9 @@ int batch_step(soil_batch* b, bool last) {
                 grouped_now.push_back(k);
             }
         }
-        if (grouped) {
+        if (csr) {
+            g5.spans[t_csr].add_nz(k, nl, 0);
+        } else if (grouped) {
             if (variant == SOIL_FORCE_WALK) g5.spans[t_walk].add_nz(k, nl, 0);
             else g5.spans[t_tiles].add_nz(k, (nl + 31) / 32, 0);
         } else {
@@ -954,6 +959,7 @@ int batch_step(soil_batch* b, bool last) {
     tic(b);
     b_force_grouped(st, g5.out[t_tiles], a);
     b_force_walk(st, g5.out[t_walk], a);
+    b_force_csr(st, g5.out[t_csr], a);
     b_harmonic(st, g5.out[h_all], a);
     toc(b, BT_FORCE);
     tic(b);

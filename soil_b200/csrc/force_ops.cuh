@@ -228,6 +228,70 @@ __device__ __forceinline__ void force_tile(const ForceSeq& p, const AtomCols& c,
     }
 }
 
+// The force on atom a (a root, or one of its ghost images) in the
+// reference's summation order, from the transposed list and the CSR: in-list
+// rows below a (ascending), a's own row, the in-list rows above a; each
+// entry evaluated as f(a, partner) (the negation argument at the top of
+// k_force.cu).  Ghosts receive only with newton and have no row.
+__device__ __forceinline__ void csr_item_force(const ForceCsr& q, const AtomCols& c, uint64_t a,
+                                               double& Fx, double& Fy, double& Fz) {
+    const bool local = a < q.nlocal;
+    const double xa = c.x[a], ya = c.y[a], za = c.z[a], ra = q.rad[a];
+    Fx = 0.0;
+    Fy = 0.0;
+    Fz = 0.0;
+    uint32_t k = 0, qe = 0;
+    if (q.newton || local) {
+        k = q.in_start[a];
+        qe = q.in_start[a + 1];
+    }
+    double fx, fy, fz;
+    for (; k < qe; ++k) {
+        const uint32_t o = q.in_list[k];
+        if (o >= (uint32_t)a) break;
+        if (pair_force(xa, ya, za, ra, c.x[o], c.y[o], c.z[o], q.rad[o], q.K, fx, fy, fz)) {
+            Fx = Fx + fx;
+            Fy = Fy + fy;
+            Fz = Fz + fz;
+        }
+    }
+    if (local) {
+        const uint32_t re = q.offsets[a + 1];
+        for (uint32_t r = q.offsets[a]; r < re; ++r) {
+            const uint32_t o = q.indices[r];
+            if (pair_force(xa, ya, za, ra, c.x[o], c.y[o], c.z[o], q.rad[o], q.K, fx, fy, fz)) {
+                Fx = Fx + fx;
+                Fy = Fy + fy;
+                Fz = Fz + fz;
+            }
+        }
+    }
+    for (; k < qe; ++k) {
+        const uint32_t o = q.in_list[k];
+        if (pair_force(xa, ya, za, ra, c.x[o], c.y[o], c.z[o], q.rad[o], q.K, fx, fy, fz)) {
+            Fx = Fx + fx;
+            Fy = Fy + fy;
+            Fz = Fz + fz;
+        }
+    }
+}
+
+// Root t and its images by one thread (CSR walk), then (FOLD) the fold.
+template <bool FOLD>
+__device__ __forceinline__ void force_csr_root(const ForceCsr& q, const AtomCols& c,
+                                               const PlaneList& rev, uint64_t t) {
+    const uint32_t f0 = q.fold_start[t], f1 = q.fold_start[t + 1];
+    for (uint32_t f = f0 - 1; f + 1 <= f1; ++f) {  // the root (f = f0 - 1), then its images
+        const uint64_t a = f + 1 == f0 ? t : q.nlocal + q.fold_list[f];
+        double Fx, Fy, Fz;
+        csr_item_force(q, c, a, Fx, Fy, Fz);
+        c.fx[a] = Fx;
+        c.fy[a] = Fy;
+        c.fz[a] = Fz;
+    }
+    if (FOLD) fold_root(c, q.nlocal, t, q.fold_start, q.fold_list, rev);
+}
+
 // Root t's group walked by one thread: each item's (root's, then every
 // image's) sequence summed in order, its force written, then (FOLD) the
 // images folded into the root in reverse_send_force's order.

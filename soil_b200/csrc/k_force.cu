@@ -109,6 +109,24 @@ __global__ void __launch_bounds__(kBlock, 4) k_force_walk(ForceArgs p) {
         force_walk_root<FOLD>(p.q, p.c, p.rev, t);
 }
 
+template <bool FOLD>
+__global__ void __launch_bounds__(kBlock, 4) k_force_csr(ForceCsr q, AtomCols c, PlaneList rev) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < q.nlocal;
+         t += (uint64_t)gridDim.x * blockDim.x)
+        force_csr_root<FOLD>(q, c, rev, t);
+}
+
+void launch_force_csr(cudaStream_t st, const ForceCsr& q, const AtomCols& c, const PlaneList& rev,
+                      bool fold) {
+    if (q.nlocal == 0) return;
+    note_launch();
+    const unsigned full = 148u * 4u;  // one resident wave at <= 64 registers
+    const unsigned need = (unsigned)((q.nlocal + kBlock - 1) / kBlock);
+    const unsigned grid = need < full ? need : full;
+    if (fold) k_force_csr<true><<<grid, kBlock, 0, st>>>(q, c, rev);
+    else k_force_csr<false><<<grid, kBlock, 0, st>>>(q, c, rev);
+}
+
 template <int U>
 static void launch_tiles(cudaStream_t st, const ForceArgs& p, bool fold) {
     const uint64_t ntiles = (p.q.nlocal + 31) / 32;
@@ -119,7 +137,7 @@ static void launch_tiles(cudaStream_t st, const ForceArgs& p, bool fold) {
     else k_force_seq<U, false><<<grid, kBlock, 0, st>>>(p);
 }
 
-// The consumer kernel (SOIL_FORCE: gather, tiles4, tiles2, walk); read at
+// The consumer kernel (SOIL_FORCE: gather, csr, tiles4, tiles2, walk); read at
 // each call so a host can compare them on one system.
 int force_variant() {
     const char* env = std::getenv("SOIL_FORCE");
@@ -128,6 +146,7 @@ int force_variant() {
     if (!std::strcmp(env, "tiles4")) return SOIL_FORCE_TILES4;
     if (!std::strcmp(env, "tiles2")) return SOIL_FORCE_TILES2;
     if (!std::strcmp(env, "walk")) return SOIL_FORCE_WALK;
+    if (!std::strcmp(env, "csr")) return SOIL_FORCE_CSR;
     return kDefaultForce;
 }
 

@@ -65,9 +65,11 @@ __device__ bool grid_sync(GridBar* b, unsigned nblocks, unsigned& gen, uint32_t*
 
 }  // namespace
 
-// CONSUMER: 0 none, 1 grouped, 2 grouped + fold; WALK: one root per thread
-// (force_walk_root), else warp tiles (force_tile)
-template <int U, int CONSUMER, bool WALK>
+// CONSUMER: 0 none, 1 without fold, 2 with fold (newton).  MODE: 0 warp
+// tiles over grouped sequences (force_tile), 1 one root per thread over
+// them (force_walk_root), 2 one root per thread over the CSR and its
+// transpose (force_csr_root).
+template <int U, int CONSUMER, int MODE>
 __global__ void __launch_bounds__(kBlock, 4) k_steps(StepsArgs a) {
     __shared__ ForceSmem<U> sm;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -107,7 +109,11 @@ __global__ void __launch_bounds__(kBlock, 4) k_steps(StepsArgs a) {
             cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(a.trip[(step + 2) % 3])
                 .store(0u, cuda::memory_order_relaxed);
         // phase B: the consumer over every root's group (and the fold)
-        if (CONSUMER && WALK) {
+        if (CONSUMER && MODE == 2) {
+            for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nl;
+                 t += (uint64_t)gridDim.x * blockDim.x)
+                force_csr_root<CONSUMER == 2>(a.fc, c, a.fa.rev, t);
+        } else if (CONSUMER && MODE == 1) {
             for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nl;
                  t += (uint64_t)gridDim.x * blockDim.x)
                 force_walk_root<CONSUMER == 2>(a.fa.q, c, a.fa.rev, t);
@@ -129,10 +135,11 @@ __global__ void __launch_bounds__(kBlock, 4) k_steps(StepsArgs a) {
     }
 }
 
-static const void* steps_kernel(int consumer, int walk) {
-    if (consumer == 0) return (const void*)k_steps<4, 0, true>;
-    if (walk) return consumer == 1 ? (const void*)k_steps<4, 1, true> : (const void*)k_steps<4, 2, true>;
-    return consumer == 1 ? (const void*)k_steps<4, 1, false> : (const void*)k_steps<4, 2, false>;
+static const void* steps_kernel(int consumer, int mode) {
+    if (consumer == 0) return (const void*)k_steps<4, 0, 2>;
+    if (mode == 2) return consumer == 1 ? (const void*)k_steps<4, 1, 2> : (const void*)k_steps<4, 2, 2>;
+    if (mode == 1) return consumer == 1 ? (const void*)k_steps<4, 1, 1> : (const void*)k_steps<4, 2, 1>;
+    return consumer == 1 ? (const void*)k_steps<4, 1, 0> : (const void*)k_steps<4, 2, 0>;
 }
 
 int steps_grid(int consumer, int walk, uint64_t nlocal, int* grid) {

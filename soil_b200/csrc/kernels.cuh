@@ -339,12 +339,36 @@ struct ForceArgs {
     PlaneList rev;  // #[reverse] planes folded with the forces
 };
 // Kernels of the built-in consumer (SOIL_FORCE): the per-atom gather over the
-// CSR and its transpose with a separate reverse pass (GATHER), or a kernel
-// over the grouped sequences with the fold inside: warp tiles of 32 roots
-// with 4 or 2 rows of 32 entries per chunk (TILES4, TILES2), or one thread
-// per root walking its group (WALK).
-enum { SOIL_FORCE_GATHER = 0, SOIL_FORCE_TILES4 = 1, SOIL_FORCE_TILES2 = 2, SOIL_FORCE_WALK = 3 };
-constexpr int kDefaultForce = SOIL_FORCE_WALK;  // when SOIL_FORCE is unset
+// CSR and its transpose with a separate reverse pass (GATHER); one thread per
+// root walking its and its images' transposed lists and rows, with the fold
+// (CSR); or a kernel over grouped sequences built at each rebuild, with the
+// fold: warp tiles of 32 roots with 4 or 2 rows of 32 entries per chunk
+// (TILES4, TILES2), or one thread per root walking its group (WALK).
+enum {
+    SOIL_FORCE_GATHER = 0,
+    SOIL_FORCE_TILES4 = 1,
+    SOIL_FORCE_TILES2 = 2,
+    SOIL_FORCE_WALK = 3,
+    SOIL_FORCE_CSR = 4
+};
+constexpr int kDefaultForce = SOIL_FORCE_CSR;  // when SOIL_FORCE is unset
+// The consumer walking each root's transposed list and CSR row directly
+// (one thread per root, its images after it, then the fold): no grouped
+// sequences are built.
+struct ForceCsr {
+    const double* rad;
+    double K;
+    uint64_t nlocal;
+    int newton;
+    const uint32_t* offsets;
+    const uint32_t* indices;
+    const uint32_t* in_start;
+    const uint32_t* in_list;
+    const uint32_t* fold_start;
+    const uint32_t* fold_list;
+};
+void launch_force_csr(cudaStream_t st, const ForceCsr& q, const AtomCols& c, const PlaneList& rev,
+                      bool fold);
 int force_variant();  // from SOIL_FORCE (default chosen by measurement)
 // The built-in consumer over the grouped sequences: F of every local and
 // ghost is overwritten; with fold, ghost forces (and the #[reverse] planes)
@@ -366,8 +390,9 @@ struct StepsArgs {
     int first_fused;   // the first step's pass also applies the pending final half-kick
     CheckArgs ck;      // the displacement check (every step)
     FwdArgs fw;        // forward comm of every step
-    ForceArgs fa;      // the grouped consumer (consumer != 0)
-    int walk;          // the consumer walks one root per thread (SOIL_FORCE_WALK)
+    ForceArgs fa;      // the grouped consumer (consumer != 0, mode 0 / 1)
+    ForceCsr fc;       // the CSR walk (consumer != 0, mode 2)
+    int walk;          // consumer mode: 0 warp tiles, 1 grouped walk, 2 CSR walk
     uint64_t max_steps;
     GridBar* bar;
     DevFlags* flags;   // flags->rebuild is set when a check trips

@@ -1098,11 +1098,41 @@ ForceArgs consumer_args(const soil_sys* s) {
     return p;
 }
 
+ForceCsr csr_args(const soil_sys* s) {
+    ForceCsr q;
+    q.rad = s->A.planes[s->cols[s->radius_col].plane0];
+    q.K = s->harmonic_k;
+    q.nlocal = s->nlocal;
+    q.newton = s->newton ? 1 : 0;
+    q.offsets = s->offsets.p;
+    q.indices = s->indices.p;
+    q.in_start = s->in_start.p;
+    q.in_list = s->in_list.p;
+    q.fold_start = s->fold_start.p;
+    q.fold_list = s->fold_list.p;
+    return q;
+}
+
+// Whether the consumer kernel folds reverse comm into itself (newton): the
+// CSR walk always, the grouped-sequence kernels when they serve the system.
+bool consumer_folds(const soil_sys* s) {
+    if (s->hook || !builtin_consumer(s) || !s->newton) return false;
+    const int v = force_variant();
+    if (v == SOIL_FORCE_GATHER) return false;
+    return v == SOIL_FORCE_CSR || seq_consumer(s);
+}
+
 // The built-in consumer; with fold (newton), reverse comm of the forces and
 // #[reverse] planes is done in the same kernel.
 int launch_consumer(soil_sys* s, bool fold) {
     if (!s->in_lists_valid) TRY(build_in_lists(s));
     const int variant = force_variant();
+    if (variant == SOIL_FORCE_CSR) {
+        PlaneList rev;
+        zero_planes_of(s, SOIL_COL_REVERSE, rev.idx, &rev.n);
+        launch_force_csr(s->st, csr_args(s), s->A, rev, fold);
+        return check_launch(s);
+    }
     if (!seq_consumer(s) || variant == SOIL_FORCE_GATHER) {
         launch_harmonic(s->st, s->nlocal, s->nlocal + s->nghost, s->A,
                         s->A.planes[s->cols[s->radius_col].plane0], s->harmonic_k,
@@ -1484,8 +1514,7 @@ int step_rest(soil_sys* s, const StepPlan& p, bool last) {
     // With newton, the grouped consumer folds ghost forces into their roots
     // in the same kernel (reverse_send_force's fold order); otherwise the
     // force and reverse-comm phases run apart.
-    const bool fold_fused =
-        !s->hook && seq_consumer(s) && s->newton && force_variant() != SOIL_FORCE_GATHER;
+    const bool fold_fused = consumer_folds(s);
     timer_begin(s, T_FORCE);
     if (fold_fused) {
         TRY(launch_consumer(s, true));
@@ -1541,7 +1570,7 @@ uint64_t resident_limit(const soil_sys* s, uint64_t want) {
         return 0;
     if (!fused_forward_allowed(s)) return 0;
     const bool consumer = builtin_consumer(s);
-    if (consumer && !seq_consumer(s)) return 0;
+    if (consumer && force_variant() != SOIL_FORCE_CSR && !seq_consumer(s)) return 0;
     int idx[kMaxPlanes], nz, nr;
     zero_planes_of(s, SOIL_COL_ZERO, idx, &nz);
     zero_planes_of(s, SOIL_COL_REVERSE, idx, &nr);
@@ -1575,11 +1604,17 @@ int resident_steps(soil_sys* s, uint64_t max, uint64_t* done, bool* tripped, Ste
     int kind = 0;
     if (consumer) {
         if (!s->in_lists_valid) TRY(build_in_lists(s));
-        if (!s->seq_valid) TRY(build_seq(s));
-        a.fa = consumer_args(s);
         kind = s->newton ? 2 : 1;
         const int v = force_variant();
-        a.walk = (v == SOIL_FORCE_TILES4 || v == SOIL_FORCE_TILES2) ? 0 : 1;
+        if (v == SOIL_FORCE_CSR) {
+            a.fc = csr_args(s);
+            zero_planes_of(s, SOIL_COL_REVERSE, a.fa.rev.idx, &a.fa.rev.n);
+            a.walk = 2;
+        } else {
+            if (!s->seq_valid) TRY(build_seq(s));
+            a.fa = consumer_args(s);
+            a.walk = (v == SOIL_FORCE_TILES4 || v == SOIL_FORCE_TILES2) ? 0 : 1;
+        }
     }
     a.max_steps = max;
     TRY(ensure(s, s->rstate, 8));

@@ -1,6 +1,7 @@
 """Every kernel of the built-in consumer (SOIL_FORCE: the per-atom gather with
-a separate reverse pass, warp tiles with 4 or 2 rows per chunk, one root per
-thread) gives the reference's forces bit for bit: single systems with newton
+a separate reverse pass, the per-root walk over the CSR and its transpose,
+and over grouped sequences warp tiles with 4 or 2 rows per chunk or one root
+per thread) gives the reference's forces bit for bit: single systems with newton
 on and off against the CPU oracle, and batched boxes against the same boxes
 alone."""
 import os
@@ -13,7 +14,7 @@ from soil_b200 import system, workloads as W
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = ["gather", "tiles4", "tiles2", "walk"]
+VARIANTS = ["gather", "csr", "tiles4", "tiles2", "walk"]
 
 
 @pytest.fixture
