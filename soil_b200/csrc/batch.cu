@@ -890,6 +890,7 @@ int batch_step(soil_batch* b, bool last) {
             s->rebuilds += 1;
             s->in_lists_valid = true;
             s->seq_valid = false;  // set once this step's sequences are enqueued
+            s->order_valid = false;
             s->hflags->candidates = b->h_flags[k].candidates;
             s->hflags->rechecked = b->h_flags[k].rechecked;
             fill_dev(b, k);

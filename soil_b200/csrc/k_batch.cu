@@ -631,6 +631,7 @@ __global__ void __launch_bounds__(kBlock, 3) kb_force_csr(Span sp, BatchArgs A) 
         q.in_list = D.in_list;
         q.fold_start = D.fold_start;
         q.fold_list = D.fold_list;
+        q.order = nullptr;
         if (S.newton) force_csr_root<true>(q, c, D.rev, i);
         else force_csr_root<false>(q, c, D.rev, i);
     });

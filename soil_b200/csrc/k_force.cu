@@ -111,9 +111,55 @@ __global__ void __launch_bounds__(kBlock, 4) k_force_walk(ForceArgs p) {
 
 template <bool FOLD>
 __global__ void __launch_bounds__(kBlock, 4) k_force_csr(ForceCsr q, AtomCols c, PlaneList rev) {
-    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < q.nlocal;
-         t += (uint64_t)gridDim.x * blockDim.x)
-        force_csr_root<FOLD>(q, c, rev, t);
+    // grid-stride over whole blocks of kBlock roots, so a block's order
+    // permutes its own roots
+    for (uint64_t b = (uint64_t)blockIdx.x * kBlock; b < q.nlocal; b += (uint64_t)gridDim.x * kBlock) {
+        const uint64_t k = b + threadIdx.x;
+        if (k < q.nlocal) force_csr_root<FOLD>(q, c, rev, q.order ? q.order[k] : k);
+    }
+}
+
+// Entries of root t's walk: its and its images' in-lists and its row.
+__device__ __forceinline__ uint32_t csr_work(const ForceCsr& q, uint64_t t) {
+    uint32_t n = q.offsets[t + 1] - q.offsets[t] + q.in_start[t + 1] - q.in_start[t];
+    if (q.newton)
+        for (uint32_t f = q.fold_start[t]; f < q.fold_start[t + 1]; ++f) {
+            const uint64_t g = q.nlocal + q.fold_list[f];
+            n += q.in_start[g + 1] - q.in_start[g];
+        }
+    return n;
+}
+
+// One block per kBlock roots: a bitonic sort of (work, index) keys in
+// shared memory.
+__global__ void __launch_bounds__(kBlock) k_root_order(ForceCsr q, uint32_t* order) {
+    __shared__ uint64_t key[kBlock];
+    const uint64_t b = (uint64_t)blockIdx.x * kBlock;
+    const uint32_t i = threadIdx.x;
+    const uint64_t t = b + i;
+    const uint32_t work = t < q.nlocal ? min(csr_work(q, t), 0xffffu) : 0xffffffffu;
+    key[i] = ((uint64_t)work << 32) | (uint32_t)i;
+    __syncthreads();
+    for (uint32_t size = 2; size <= kBlock; size <<= 1)
+        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+            const uint32_t j = i ^ stride;
+            if (j > i) {
+                const uint64_t a = key[i], c = key[j];
+                const bool up = (i & size) == 0;
+                if ((a > c) == up) {
+                    key[i] = c;
+                    key[j] = a;
+                }
+            }
+            __syncthreads();
+        }
+    if (t < q.nlocal) order[t] = (uint32_t)(b + (uint32_t)key[i]);
+}
+
+void launch_root_order(cudaStream_t st, const ForceCsr& q, uint32_t* order) {
+    if (q.nlocal == 0) return;
+    note_launch();
+    k_root_order<<<(unsigned)((q.nlocal + kBlock - 1) / kBlock), kBlock, 0, st>>>(q, order);
 }
 
 void launch_force_csr(cudaStream_t st, const ForceCsr& q, const AtomCols& c, const PlaneList& rev,

@@ -109,10 +109,13 @@ __global__ void __launch_bounds__(kBlock, 4) k_steps(StepsArgs a) {
             cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(a.trip[(step + 2) % 3])
                 .store(0u, cuda::memory_order_relaxed);
         // phase B: the consumer over every root's group (and the fold)
-        if (CONSUMER && MODE == 2) {
-            for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nl;
-                 t += (uint64_t)gridDim.x * blockDim.x)
-                force_csr_root<CONSUMER == 2>(a.fc, c, a.fa.rev, t);
+        if (CONSUMER && MODE == 2) {  // whole blocks of roots, in their order
+            for (uint64_t b = (uint64_t)blockIdx.x * kBlock; b < nl;
+                 b += (uint64_t)gridDim.x * kBlock) {
+                const uint64_t k = b + threadIdx.x;
+                if (k < nl)
+                    force_csr_root<CONSUMER == 2>(a.fc, c, a.fa.rev, a.fc.order ? a.fc.order[k] : k);
+            }
         } else if (CONSUMER && MODE == 1) {
             for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nl;
                  t += (uint64_t)gridDim.x * blockDim.x)

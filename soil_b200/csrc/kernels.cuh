@@ -366,9 +366,17 @@ struct ForceCsr {
     const uint32_t* in_list;
     const uint32_t* fold_start;
     const uint32_t* fold_list;
+    // Roots by work inside each block of kBlock roots (NULL: index order):
+    // thread k of the block that takes roots [b, b + kBlock) walks
+    // order[b + k].  Threads of a warp then walk groups of similar length.
+    const uint32_t* order;
 };
 void launch_force_csr(cudaStream_t st, const ForceCsr& q, const AtomCols& c, const PlaneList& rev,
                       bool fold);
+// order[b + k] for every block of kBlock roots: the block's roots sorted by
+// their entry count (their own and their images' in-list and row lengths),
+// ties in index order.
+void launch_root_order(cudaStream_t st, const ForceCsr& q, uint32_t* order);
 int force_variant();  // from SOIL_FORCE (default chosen by measurement)
 // The built-in consumer over the grouped sequences: F of every local and
 // ghost is overwritten; with fold, ghost forces (and the #[reverse] planes)

@@ -1100,6 +1100,7 @@ ForceArgs consumer_args(const soil_sys* s) {
 
 ForceCsr csr_args(const soil_sys* s) {
     ForceCsr q;
+    q.order = nullptr;
     q.rad = s->A.planes[s->cols[s->radius_col].plane0];
     q.K = s->harmonic_k;
     q.nlocal = s->nlocal;
@@ -1111,6 +1112,22 @@ ForceCsr csr_args(const soil_sys* s) {
     q.fold_start = s->fold_start.p;
     q.fold_list = s->fold_list.p;
     return q;
+}
+
+// The CSR walk's per-block root order (SOIL_ROOT_ORDER=0: index order),
+// built once per set of lists.
+int csr_with_order(soil_sys* s, ForceCsr* q) {
+    *q = csr_args(s);
+    const char* env = std::getenv("SOIL_ROOT_ORDER");
+    if (env && std::atoi(env) == 0) return SOIL_OK;
+    if (!s->order_valid) {
+        TRY(ensure(s, s->root_order, s->nlocal + 1, 0, s->acap + 1));
+        launch_root_order(s->st, *q, s->root_order.p);
+        TRY(check_launch(s));
+        s->order_valid = true;
+    }
+    q->order = s->root_order.p;
+    return SOIL_OK;
 }
 
 // Whether the consumer kernel folds reverse comm into itself (newton): the
@@ -1130,7 +1147,9 @@ int launch_consumer(soil_sys* s, bool fold) {
     if (variant == SOIL_FORCE_CSR) {
         PlaneList rev;
         zero_planes_of(s, SOIL_COL_REVERSE, rev.idx, &rev.n);
-        launch_force_csr(s->st, csr_args(s), s->A, rev, fold);
+        ForceCsr q;
+        TRY(csr_with_order(s, &q));
+        launch_force_csr(s->st, q, s->A, rev, fold);
         return check_launch(s);
     }
     if (!seq_consumer(s) || variant == SOIL_FORCE_GATHER) {
@@ -1307,6 +1326,7 @@ int phase_neighbor(soil_sys* s) {
     s->rebuilds += 1;
     s->in_lists_valid = false;
     s->seq_valid = false;
+    s->order_valid = false;
     // the transposed lists serve the built-in consumer and any force hook
     if (builtin_consumer(s) || s->hook) TRY(build_in_lists(s));
     // the grouped sequences are built when a consumer kernel first needs them
@@ -1607,7 +1627,7 @@ int resident_steps(soil_sys* s, uint64_t max, uint64_t* done, bool* tripped, Ste
         kind = s->newton ? 2 : 1;
         const int v = force_variant();
         if (v == SOIL_FORCE_CSR) {
-            a.fc = csr_args(s);
+            TRY(csr_with_order(s, &a.fc));
             zero_planes_of(s, SOIL_COL_REVERSE, a.fa.rev.idx, &a.fa.rev.n);
             a.walk = 2;
         } else {
@@ -1833,7 +1853,7 @@ int soil_sys_destroy(soil_sys* s) {
     for (int k = 0; k < 2; ++k) { fr(s->slot_tag[k]); fr(s->slot_val[k]); }
     fr(s->in_count); fr(s->in_start); fr(s->in_cursor); fr(s->in_list);
     fr(s->seq_cnt); fr(s->grp_cnt); fr(s->grp_start); fr(s->seq); fr(s->seq_owner);
-    fr(s->rstate); fr(s->scan1p);
+    fr(s->rstate); fr(s->scan1p); fr(s->root_order);
     fr(s->ghost_root); fr(s->ghost_chain);
     fr(s->fold_start); fr(s->fold_list);
     for (auto& a : s->send) fr(a);
@@ -2019,6 +2039,7 @@ int soil_sys_set_harmonic(soil_sys* s, double k, int32_t radius_col) {
     s->radius_col = radius_col;
     s->in_lists_valid = false;
     s->seq_valid = false;
+    s->order_valid = false;
     return SOIL_OK;
 }
 

@@ -144,6 +144,8 @@ struct soil_sys {
     bool few_images = false;  // no local has images on both sides of a dim (<= 7 images)
     DArr<uint32_t> rstate;    // resident steps: grid barrier words, step count, trip flag
     DArr<uint32_t> scan1p;    // single-pass scan: tile counter and descriptors (zeroed at growth)
+    DArr<uint32_t> root_order;  // CSR-walk consumer: roots by work per block (rebuilt with the lists)
+    bool order_valid = false;
     DArr<uint32_t> ghost_root, ghost_chain;
     DArr<uint32_t> fold_start, fold_list;  // reverse-comm fold program (written by borders)
     DArr<uint32_t> send[kNumSwaps];
