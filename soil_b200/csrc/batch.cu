@@ -891,6 +891,7 @@ int batch_step(soil_batch* b, bool last) {
             s->in_lists_valid = true;
             s->seq_valid = false;  // set once this step's sequences are enqueued
             s->order_valid = false;
+            s->split_valid = false;
             s->hflags->candidates = b->h_flags[k].candidates;
             s->hflags->rechecked = b->h_flags[k].rechecked;
             fill_dev(b, k);
@@ -906,18 +907,22 @@ int batch_step(soil_batch* b, bool last) {
     const int r_loc = stage_add(g5), r_all = stage_add(g5), r_scan = stage_add(g5),
               h_all = stage_add(g5), v_loc = stage_add(g5), l_loc = stage_add(g5),
               q_all = stage_add(g5), q_grp = stage_add(g5), q_loc = stage_add(g5),
-              t_tiles = stage_add(g5), t_walk = stage_add(g5), t_csr = stage_add(g5);
+              t_tiles = stage_add(g5), t_walk = stage_add(g5);
     // Boxes whose locals have at most 7 images take the grouped consumer (its
     // sequences built at each rebuild, reverse comm folded in); the others the
     // per-atom gather and a reverse pass.
     grouped_now.clear();
-    const int variant = force_variant();
+    // The batch's consumer: the grouped kernels when SOIL_FORCE names one, else
+    // the per-atom gather with a reverse pass (measured fastest on the
+    // batched boxes, whose frequent rebuilds favour kernels without per-build
+    // preparation).
+    int variant = force_variant();
+    if (variant == SOIL_FORCE_CSR) variant = SOIL_FORCE_GATHER;
     for (uint32_t k : M) {
         const auto& h = b->hot[k];
         const soil_sys* s = b->slot[k];
         const uint64_t nl = h.nlocal, total = nl + h.nghost;
-        const bool csr = variant == SOIL_FORCE_CSR;
-        const bool grouped = !csr && variant != SOIL_FORCE_GATHER && s->few_images &&
+        const bool grouped = variant != SOIL_FORCE_GATHER && s->few_images &&
                              (b->rebuild[k] || s->seq_valid);
         if (b->rebuild[k]) {
             g5.spans[r_loc].add_nz(k, nl, 0);
@@ -930,9 +935,7 @@ int batch_step(soil_batch* b, bool last) {
                 grouped_now.push_back(k);
             }
         }
-        if (csr) {
-            g5.spans[t_csr].add_nz(k, nl, 0);
-        } else if (grouped) {
+        if (grouped) {
             if (variant == SOIL_FORCE_WALK) g5.spans[t_walk].add_nz(k, nl, 0);
             else g5.spans[t_tiles].add_nz(k, (nl + 31) / 32, 0);
         } else {
@@ -960,7 +963,6 @@ int batch_step(soil_batch* b, bool last) {
     tic(b);
     b_force_grouped(st, g5.out[t_tiles], a);
     b_force_walk(st, g5.out[t_walk], a);
-    b_force_csr(st, g5.out[t_csr], a);
     b_harmonic(st, g5.out[h_all], a);
     toc(b, BT_FORCE);
     tic(b);

@@ -168,9 +168,6 @@ void b_seq_fill(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_force_grouped(cudaStream_t st, const Span& sp, const BatchArgs& a);
 // the same consumer with one root per thread (element = local root)
 void b_force_walk(cudaStream_t st, const Span& sp, const BatchArgs& a);
-// the CSR walk (one root and its images per thread, fold with newton; no
-// grouped sequences), element = local root
-void b_force_csr(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_reverse(cudaStream_t st, const Span& sp, const BatchArgs& a);
 
 }  // namespace soil

@@ -230,9 +230,9 @@ __device__ __forceinline__ void force_tile(const ForceSeq& p, const AtomCols& c,
 
 // The force on atom a (a root, or one of its ghost images) in the
 // reference's summation order, from the transposed list and the CSR: in-list
-// rows below a (ascending), a's own row, the in-list rows above a; each
-// entry evaluated as f(a, partner) (the negation argument at the top of
-// k_force.cu).  Ghosts receive only with newton and have no row.
+// rows below a (ascending; in_split[a] of them), a's own row, the in-list
+// rows above a; each entry evaluated as f(a, partner) (the negation argument
+// at the top of k_force.cu).  Ghosts receive only with newton and have no row.
 __device__ __forceinline__ void csr_item_force(const ForceCsr& q, const AtomCols& c, uint64_t a,
                                                double& Fx, double& Fy, double& Fz) {
     const bool local = a < q.nlocal;
@@ -240,34 +240,23 @@ __device__ __forceinline__ void csr_item_force(const ForceCsr& q, const AtomCols
     Fx = 0.0;
     Fy = 0.0;
     Fz = 0.0;
-    uint32_t k = 0, qe = 0;
+    uint32_t qs = 0, nin = 0, npre = 0, rs = 0, nrow = 0;
     if (q.newton || local) {
-        k = q.in_start[a];
-        qe = q.in_start[a + 1];
-    }
-    double fx, fy, fz;
-    for (; k < qe; ++k) {
-        const uint32_t o = q.in_list[k];
-        if (o >= (uint32_t)a) break;
-        if (pair_force(xa, ya, za, ra, c.x[o], c.y[o], c.z[o], q.rad[o], q.K, fx, fy, fz)) {
-            Fx = Fx + fx;
-            Fy = Fy + fy;
-            Fz = Fz + fz;
-        }
+        qs = q.in_start[a];
+        nin = q.in_start[a + 1] - qs;
+        npre = q.in_split[a];
     }
     if (local) {
-        const uint32_t re = q.offsets[a + 1];
-        for (uint32_t r = q.offsets[a]; r < re; ++r) {
-            const uint32_t o = q.indices[r];
-            if (pair_force(xa, ya, za, ra, c.x[o], c.y[o], c.z[o], q.rad[o], q.K, fx, fy, fz)) {
-                Fx = Fx + fx;
-                Fy = Fy + fy;
-                Fz = Fz + fz;
-            }
-        }
+        rs = q.offsets[a];
+        nrow = q.offsets[a + 1] - rs;
     }
-    for (; k < qe; ++k) {
-        const uint32_t o = q.in_list[k];
+    // one loop over the flattened order: in-list rows below a, a's row, the
+    // rest of the in-list (a known trip count, so partner loads run ahead)
+    const uint32_t total = nin + nrow;
+    for (uint32_t k = 0; k < total; ++k) {
+        const uint32_t o = k < npre ? q.in_list[qs + k]
+                         : k < npre + nrow ? q.indices[rs + (k - npre)] : q.in_list[qs + (k - nrow)];
+        double fx, fy, fz;
         if (pair_force(xa, ya, za, ra, c.x[o], c.y[o], c.z[o], q.rad[o], q.K, fx, fy, fz)) {
             Fx = Fx + fx;
             Fy = Fy + fy;

@@ -615,34 +615,6 @@ void b_force_walk(cudaStream_t st, const Span& sp, const BatchArgs& a) {
     kb_force_walk<<<g < 148u * 4u ? g : 148u * 4u, kBlock, 0, st>>>(sp, a);
 }
 
-__global__ void __launch_bounds__(kBlock, 3) kb_force_csr(Span sp, BatchArgs A) {
-    for_span(sp, [&](uint32_t b, uint64_t i, uint32_t) {
-        const BoxDev& D = A.dev[b];
-        const BoxStep& S = A.step[b];
-        const AtomCols& c = D.set[S.post];
-        ForceCsr q;
-        q.rad = c.planes[D.radius_plane];
-        q.K = S.K;
-        q.nlocal = S.nlocal;
-        q.newton = S.newton;
-        q.offsets = D.offsets;
-        q.indices = D.indices;
-        q.in_start = D.in_start;
-        q.in_list = D.in_list;
-        q.fold_start = D.fold_start;
-        q.fold_list = D.fold_list;
-        q.order = nullptr;
-        if (S.newton) force_csr_root<true>(q, c, D.rev, i);
-        else force_csr_root<false>(q, c, D.rev, i);
-    });
-}
-void b_force_csr(cudaStream_t st, const Span& sp, const BatchArgs& a) {
-    if (sp.total == 0) return;
-    note_launch();
-    const unsigned g = span_grid(sp);
-    kb_force_csr<<<g < 148u * 3u ? g : 148u * 3u, kBlock, 0, st>>>(sp, a);
-}
-
 void b_force_grouped(cudaStream_t st, const Span& sp, const BatchArgs& a) {
     if (sp.total == 0) return;
     note_launch();

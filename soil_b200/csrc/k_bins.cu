@@ -91,6 +91,46 @@ void launch_segsort(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint3
     k_segsort<<<grid_for(nseg), kBlock, 0, st>>>(nseg, start, items);
 }
 
+// The transposed lists' sort: segment a (atom a's in-list) ascending, and
+// split[a] = its entries below a (the rows summed before a's own row).
+__global__ void __launch_bounds__(kBlock) k_segsort_split(uint64_t nseg, const uint32_t* start,
+                                                          uint32_t* items, uint32_t* split) {
+    for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < nseg;
+         s += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t b = start[s], e = start[s + 1];
+        insertion_sort(items, b, e);
+        uint32_t k = b;
+        while (k < e && items[k] < (uint32_t)s) ++k;
+        split[s] = k - b;
+    }
+}
+
+void launch_segsort_split(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint32_t* items,
+                          uint32_t* split) {
+    if (nseg == 0) return;
+    note_launch();
+    k_segsort_split<<<grid_for(nseg), kBlock, 0, st>>>(nseg, start, items, split);
+}
+
+// split[a] of already sorted transposed lists
+__global__ void __launch_bounds__(kBlock) k_in_split(uint64_t nseg, const uint32_t* start,
+                                                     const uint32_t* items, uint32_t* split) {
+    for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < nseg;
+         s += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t b = start[s], e = start[s + 1];
+        uint32_t k = b;
+        while (k < e && items[k] < (uint32_t)s) ++k;
+        split[s] = k - b;
+    }
+}
+
+void launch_in_split(cudaStream_t st, uint64_t nseg, const uint32_t* start, const uint32_t* items,
+                     uint32_t* split) {
+    if (nseg == 0) return;
+    note_launch();
+    k_in_split<<<grid_for(nseg), kBlock, 0, st>>>(nseg, start, items, split);
+}
+
 // Atom::apply_permutation + AtomDataRegistry::apply_permutation_all
 // (atom.rs:479-490, 284-289): every column gathered through perm.
 __global__ void __launch_bounds__(kBlock) k_perm_gather(uint64_t n, const uint32_t* perm,

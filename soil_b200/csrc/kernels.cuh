@@ -143,6 +143,12 @@ void launch_scatter(cudaStream_t st, uint64_t n, const uint32_t* cell, uint32_t*
                     uint32_t* out);
 // sort every segment [start[s], start[s+1]) ascending -> stable counting sort
 void launch_segsort(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint32_t* items);
+// the same, and split[s] = entries of segment s below s (transposed lists)
+void launch_segsort_split(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint32_t* items,
+                          uint32_t* split);
+// split[s] alone, for segments already sorted
+void launch_in_split(cudaStream_t st, uint64_t nseg, const uint32_t* start, const uint32_t* items,
+                     uint32_t* split);
 // dst[k] = src[perm[k]] for every column, k in [0, n)
 void launch_perm_gather(cudaStream_t st, uint64_t n, const uint32_t* perm, const AtomCols& src,
                         const AtomCols& dst);
@@ -364,6 +370,7 @@ struct ForceCsr {
     const uint32_t* indices;
     const uint32_t* in_start;
     const uint32_t* in_list;
+    const uint32_t* in_split;  // per atom: in-list entries below it
     const uint32_t* fold_start;
     const uint32_t* fold_list;
     // Roots by work inside each block of kBlock roots (NULL: index order):

@@ -311,6 +311,14 @@ int sync(soil_sys* s) {
 }
 
 int scan_1p(soil_sys* s, const uint32_t* in, uint32_t* out, uint64_t n) {
+    // Up to 64 tiles of 2,048 counts the single launch saves launch latency;
+    // above it the three-kernel scan is faster (the look-back of a thousand
+    // resident CTAs contends).
+    if (n > kScan1pMaxCounts) {
+        TRY(ensure(s, s->scan_tmp, scan_temp_words(n + 2)));
+        exclusive_scan_u32(s->st, in, out, n, s->scan_tmp.p);
+        return SOIL_OK;
+    }
     const uint64_t need = scan1p_words(n);
     if (!s->scan1p.p || s->scan1p.cap < need) {
         TRY(ensure(s, s->scan1p, need, 0, scan1p_words(2 * n + 4096)));
@@ -1041,9 +1049,11 @@ int build_in_lists(soil_sys* s) {
     TRY(scan_1p(s, s->in_count.p, s->in_start.p, total));
     CK(cudaMemcpyAsync(s->in_cursor.p, s->in_start.p, total * 4, cudaMemcpyDeviceToDevice, s->st));
     launch_in_scatter(s->st, s->nlocal, s->offsets.p, s->indices.p, s->in_cursor.p, s->in_list.p);
-    launch_segsort(s->st, total, s->in_start.p, s->in_list.p);
+    TRY(ensure(s, s->in_split, total + 1, 0, s->acap + 1));
+    launch_segsort_split(s->st, total, s->in_start.p, s->in_list.p, s->in_split.p);
     TRY(check_launch(s));
     s->in_lists_valid = true;
+    s->split_valid = true;
     return SOIL_OK;
 }
 
@@ -1109,6 +1119,7 @@ ForceCsr csr_args(const soil_sys* s) {
     q.indices = s->indices.p;
     q.in_start = s->in_start.p;
     q.in_list = s->in_list.p;
+    q.in_split = s->in_split.p;
     q.fold_start = s->fold_start.p;
     q.fold_list = s->fold_list.p;
     return q;
@@ -1117,6 +1128,13 @@ ForceCsr csr_args(const soil_sys* s) {
 // The CSR walk's per-block root order (SOIL_ROOT_ORDER=0: index order),
 // built once per set of lists.
 int csr_with_order(soil_sys* s, ForceCsr* q) {
+    if (!s->split_valid) {  // transposed lists sorted elsewhere (a batch)
+        const uint64_t total = s->nlocal + s->nghost;
+        TRY(ensure(s, s->in_split, total + 1, 0, s->acap + 1));
+        launch_in_split(s->st, total, s->in_start.p, s->in_list.p, s->in_split.p);
+        TRY(check_launch(s));
+        s->split_valid = true;
+    }
     *q = csr_args(s);
     const char* env = std::getenv("SOIL_ROOT_ORDER");
     if (env && std::atoi(env) == 0) return SOIL_OK;
@@ -1851,7 +1869,7 @@ int soil_sys_destroy(soil_sys* s) {
     fr(s->sel_flag); fr(s->sel_pos); fr(s->sel_out); fr(s->sel_cnt); fr(s->ext);
     fr(s->fold_roots); fr(s->fold_nroots);
     for (int k = 0; k < 2; ++k) { fr(s->slot_tag[k]); fr(s->slot_val[k]); }
-    fr(s->in_count); fr(s->in_start); fr(s->in_cursor); fr(s->in_list);
+    fr(s->in_count); fr(s->in_start); fr(s->in_cursor); fr(s->in_list); fr(s->in_split);
     fr(s->seq_cnt); fr(s->grp_cnt); fr(s->grp_start); fr(s->seq); fr(s->seq_owner);
     fr(s->rstate); fr(s->scan1p); fr(s->root_order);
     fr(s->ghost_root); fr(s->ghost_chain);

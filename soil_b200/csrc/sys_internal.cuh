@@ -136,6 +136,8 @@ struct soil_sys {
     int slot_old = 0;
     DArr<float4> spf;
     DArr<uint32_t> in_count, in_start, in_cursor, in_list;
+    DArr<uint32_t> in_split;  // per atom: transposed-list entries below it
+    bool split_valid = false;
     // grouped partner sequences of the built-in consumer (rebuilt with the
     // lists): per-atom lengths, per-root group lengths and starts, entries
     DArr<uint32_t> seq_cnt, grp_cnt, grp_start, seq;
@@ -265,5 +267,7 @@ constexpr int kRowSlotsPerAtom = 16;
 // Largest system that takes the device-resident light steps by default
 // (SOIL_RESIDENT_STEPS=1 forces them on at any size, 0 off).
 constexpr uint64_t kResidentAutoMaxAtoms = 1ull << 20;
+// largest count the single-pass scan serves (scan_1p)
+constexpr uint64_t kScan1pMaxCounts = 64ull * 2048ull;
 
 }  // namespace soil_host
