@@ -1442,11 +1442,14 @@ bool fused_forward_allowed(const soil_sys* s) {
     return true;
 }
 
-// ... and SOIL_FWD_FUSED (default on) keeps it in the pass of soil_step's
-// launch-per-phase steps (the resident steps always fuse it).
+// ... and SOIL_FWD_FUSED=1 puts it in the pass of soil_step's
+// launch-per-phase steps.  Off by default: it measured slower there (most
+// warps hold a lane whose root has images, and stall on its scattered ghost
+// writes; k_forward writes the ghosts coalesced).  The resident steps always
+// fuse it, which saves them a grid barrier.
 bool fused_forward_ok(const soil_sys* s) {
     const char* env = std::getenv("SOIL_FWD_FUSED");
-    if (env && std::atoi(env) == 0) return false;
+    if (!env || std::atoi(env) == 0) return false;
     return fused_forward_allowed(s);
 }
 
