@@ -58,3 +58,28 @@ def test_consumer_variant_batched_equals_alone(ctx, variant_env):
         assert_same_state(a, s, f"{variant_env} {w.name}")
         assert_same_lists(a, s, w.name)
     b.close()
+
+
+@pytest.mark.parametrize("order", ["1", "0"])
+def test_fused_forward_and_root_order_match_oracle(ctx, order):
+    """Forward comm inside the integration pass (SOIL_FWD_FUSED=1) and the CSR
+    walk with and without its per-block root order give the reference's bits."""
+    keys = ("SOIL_FWD_FUSED", "SOIL_ROOT_ORDER", "SOIL_RESIDENT_STEPS", "SOIL_FORCE")
+    old = {k: os.environ.get(k) for k in keys}
+    os.environ.update({"SOIL_FWD_FUSED": "1", "SOIL_ROOT_ORDER": order,
+                       "SOIL_RESIDENT_STEPS": "0", "SOIL_FORCE": "csr"})
+    try:
+        w = W.poly("ff", 92, 4000, 0.5, 1e-3, 0, harmonic_k=1e3)
+        w.vel *= 2.0
+        g, o = system.from_workload(ctx, w), oracle.from_workload(w)
+        g.step(30)
+        o.step(30)
+        assert_same_state(g, o)
+        assert_same_lists(g, o)
+        g.close()
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
