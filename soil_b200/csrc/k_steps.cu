@@ -37,8 +37,13 @@ namespace {
 // Spins of a barrier wait (each >= 100 ns of __nanosleep): about a second.
 constexpr uint64_t kBarrierSpinLimit = 1ull << 23;
 
-__device__ bool grid_sync(GridBar* b, unsigned nblocks, unsigned& gen, uint32_t* err) {
+// Grid barrier.  *watch (when given) is read by thread 0 after the barrier
+// and returned to every thread of the CTA in *seen (one load per CTA, not
+// one per thread, of a word every CTA polls).
+__device__ bool grid_sync(GridBar* b, unsigned nblocks, unsigned& gen, uint32_t* err,
+                          const uint32_t* watch = nullptr, uint32_t* seen = nullptr) {
     __shared__ int ok;
+    __shared__ uint32_t s_seen;
     __syncthreads();
     if (threadIdx.x == 0) {
         cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(b->count), g(b->gen);
@@ -58,8 +63,13 @@ __device__ bool grid_sync(GridBar* b, unsigned nblocks, unsigned& gen, uint32_t*
             }
         }
         gen += 1;
+        if (watch)
+            s_seen = cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(
+                         *const_cast<uint32_t*>(watch))
+                         .load(cuda::memory_order_relaxed);
     }
     __syncthreads();
+    if (seen) *seen = s_seen;
     return ok != 0;
 }
 
@@ -99,9 +109,9 @@ __global__ void __launch_bounds__(kBlock, 4) k_steps(StepsArgs a) {
                            a.fw.chain, a.fw.sc, a.fw.fwd, a.fw.zero_ghost_force != 0);
         }
         if (__ballot_sync(0xffffffffu, hit) && lane == 0) atomicOr(slot, 1u);
-        if (!grid_sync(a.bar, gridDim.x, gen, &a.flags->error)) return;
-        if (cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(*slot).load(
-                cuda::memory_order_relaxed)) {
+        uint32_t tripped = 0;
+        if (!grid_sync(a.bar, gridDim.x, gen, &a.flags->error, slot, &tripped)) return;
+        if (tripped) {
             stop = true;
             break;
         }
