@@ -999,6 +999,8 @@ void rebuild_members(soil_batch* b) {
 
 int detach(soil_batch* b, uint32_t k) {
     soil_sys* s = b->slot[k];
+    s->counts_clean = 0;  // the batch's counting passes leave counts behind
+    s->stencil_on_device.clear();
     s->st = b->saved[k];
     s->batch = nullptr;
     b->slot[k] = nullptr;

@@ -77,6 +77,62 @@ void launch_scatter(cudaStream_t st, uint64_t n, const uint32_t* cell, uint32_t*
     k_scatter<<<grid_for(n), kBlock, 0, st>>>(n, cell, cursor, out);
 }
 
+// The scatter that consumes the counts: out[start[c] + --counts[c]] = i
+// (warp-aggregated), so every count is zero again afterwards and the next
+// counting pass needs no clearing; the order inside a cell is restored by
+// the segment sort that follows.
+__global__ void __launch_bounds__(kBlock) k_scatter_consume(uint64_t n, const uint32_t* cell,
+                                                            const uint32_t* start,
+                                                            uint32_t* counts, uint32_t* out) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
+        const uint64_t i = i0 + threadIdx.x;
+        const bool valid = i < n;
+        const uint32_t key = valid ? cell[i] : 0xffffffffu;
+        const unsigned peers = __match_any_sync(0xffffffffu, key);
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(peers) - 1;
+        const uint32_t k = (uint32_t)__popc(peers);
+        uint32_t top = 0;  // the count before this warp's claim
+        if (valid && lane == leader) top = atomicSub(&counts[key], k);
+        top = __shfl_sync(0xffffffffu, top, leader);
+        if (valid) out[start[key] + (top - k) + __popc(peers & lanemask_lt())] = (uint32_t)i;
+    }
+}
+
+void launch_scatter_consume(cudaStream_t st, uint64_t n, const uint32_t* cell,
+                            const uint32_t* start, uint32_t* counts, uint32_t* out) {
+    if (n == 0) return;
+    note_launch();
+    k_scatter_consume<<<grid_for(n), kBlock, 0, st>>>(n, cell, start, counts, out);
+}
+
+// The neighbor build's cells in one pass: the locals' cells from the sort
+// (local < nlocal), the others' from their positions; all counted.
+__global__ void __launch_bounds__(kBlock) k_cells_reuse(uint64_t nlocal, uint64_t n, AtomCols c,
+                                                        Grid gr, const uint32_t* local_cell,
+                                                        uint32_t* cell_out, uint32_t* counts) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
+        const uint64_t i = i0 + threadIdx.x;
+        const bool valid = i < n;
+        uint32_t cell = 0;
+        if (valid) {
+            cell = i < nlocal ? local_cell[i] : cell_of(gr, c.x[i], c.y[i], c.z[i]);
+            cell_out[i] = cell;
+        }
+        aggregated_count(counts, cell, valid);
+    }
+}
+
+void launch_cells_reuse(cudaStream_t st, uint64_t nlocal, uint64_t n, const AtomCols& c,
+                        const Grid& gr, const uint32_t* local_cell, uint32_t* cell_out,
+                        uint32_t* counts) {
+    if (n == 0) return;
+    note_launch();
+    k_cells_reuse<<<grid_for(n), kBlock, 0, st>>>(nlocal, n, c, gr, local_cell, cell_out, counts);
+}
+
 // Restore the stable (ascending index) order inside every segment.
 __global__ void __launch_bounds__(kBlock) k_segsort(uint64_t nseg, const uint32_t* start,
                                                     uint32_t* items) {

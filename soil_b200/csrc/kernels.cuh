@@ -141,6 +141,15 @@ void launch_count_cells(cudaStream_t st, uint64_t n, const uint32_t* cell, uint3
 // out[cursor[cell[i]]++] = i (unordered within a cell)
 void launch_scatter(cudaStream_t st, uint64_t n, const uint32_t* cell, uint32_t* cursor,
                     uint32_t* out);
+// out[start[c] + --counts[c]] = i for c = cell[i] (unordered within a cell);
+// leaves every count at zero
+void launch_scatter_consume(cudaStream_t st, uint64_t n, const uint32_t* cell,
+                            const uint32_t* start, uint32_t* counts, uint32_t* out);
+// cell_out[i] = local_cell[i] (i < nlocal) or the cell of atom i, counted,
+// i in [0, n)
+void launch_cells_reuse(cudaStream_t st, uint64_t nlocal, uint64_t n, const AtomCols& c,
+                        const Grid& gr, const uint32_t* local_cell, uint32_t* cell_out,
+                        uint32_t* counts);
 // sort every segment [start[s], start[s+1]) ascending -> stable counting sort
 void launch_segsort(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint32_t* items);
 // the same, and split[s] = entries of segment s below s (transposed lists)

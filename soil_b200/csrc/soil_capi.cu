@@ -328,6 +328,17 @@ int scan_1p(soil_sys* s, const uint32_t* in, uint32_t* out, uint64_t n) {
     return SOIL_OK;
 }
 
+int counts_zero(soil_sys* s, uint64_t nc) {
+    if (s->counts_at != s->cell_counts.p || s->counts_clean < nc)
+        CK(cudaMemsetAsync(s->cell_counts.p, 0, s->cell_counts.cap * 4, s->st));
+    s->counts_at = s->cell_counts.p;
+    s->counts_clean = 0;  // counted into now; clean again once consumed
+    return SOIL_OK;
+}
+
+// After a consuming scatter over every counted atom: all counts are zero.
+void counts_consumed(soil_sys* s) { s->counts_clean = s->cell_counts.cap; }
+
 int check_launch(soil_sys* s) {
     CK(cudaGetLastError());
     return SOIL_OK;
@@ -828,11 +839,12 @@ int phase_sort(soil_sys* s) {
     if (!run) return SOIL_OK;
     const uint64_t nl = s->nlocal;
     const uint64_t nc = s->total_cells;
-    CK(cudaMemsetAsync(s->cell_counts.p, 0, nc * 4, s->st));
+    TRY(counts_zero(s, nc));
     launch_cells(s->st, 0, nl, s->A, grid_of(s), s->sort_cell.p, s->cell_counts.p);
     TRY(scan_1p(s, s->cell_counts.p, s->cell_start.p, nc));
-    CK(cudaMemcpyAsync(s->cell_cursor.p, s->cell_start.p, nc * 4, cudaMemcpyDeviceToDevice, s->st));
-    launch_scatter(s->st, nl, s->sort_cell.p, s->cell_cursor.p, s->sort_perm.p);
+    launch_scatter_consume(s->st, nl, s->sort_cell.p, s->cell_start.p, s->cell_counts.p,
+                           s->sort_perm.p);
+    counts_consumed(s);
     launch_segsort(s->st, nc, s->cell_start.p, s->sort_perm.p);
     launch_permute_u32(s->st, nl, s->sort_perm.p, s->sort_cell.p, s->sorted_local_cell.p);
     TRY(check_launch(s));
@@ -1280,27 +1292,29 @@ int phase_neighbor(soil_sys* s) {
     const uint64_t nc = s->total_cells;
     const bool fp32 = s->filter == SOIL_FILTER_FP32_RECHECK;
     launch_save_positions(s->st, nl, s->A, s->lbx.p, s->lby.p, s->lbz.p);
-    CK(cudaMemsetAsync(s->cell_counts.p, 0, nc * 4, s->st));
+    TRY(counts_zero(s, nc));
     const Grid gr = grid_of(s);
-    if (s->local_cells_valid) {  // reuse the sort's local cells (neighbor.rs:1049-1066)
-        CK(cudaMemcpyAsync(s->atom_cell.p, s->sorted_local_cell.p, nl * 4, cudaMemcpyDeviceToDevice,
-                           s->st));
-        launch_count_cells(s->st, nl, s->atom_cell.p, s->cell_counts.p);
-        launch_cells(s->st, nl, total - nl, s->A, gr, s->atom_cell.p + nl, s->cell_counts.p);
-    } else {
+    if (s->local_cells_valid)  // reuse the sort's local cells (neighbor.rs:1049-1066)
+        launch_cells_reuse(s->st, nl, total, s->A, gr, s->sorted_local_cell.p, s->atom_cell.p,
+                           s->cell_counts.p);
+    else
         launch_cells(s->st, 0, total, s->A, gr, s->atom_cell.p, s->cell_counts.p);
-    }
     s->local_cells_valid = false;
     TRY(scan_1p(s, s->cell_counts.p, s->cell_start.p, nc));
-    CK(cudaMemcpyAsync(s->cell_cursor.p, s->cell_start.p, nc * 4, cudaMemcpyDeviceToDevice, s->st));
-    launch_scatter(s->st, total, s->atom_cell.p, s->cell_cursor.p, s->sorted_atoms.p);
+    launch_scatter_consume(s->st, total, s->atom_cell.p, s->cell_start.p, s->cell_counts.p,
+                           s->sorted_atoms.p);
+    counts_consumed(s);
     launch_segsort(s->st, nc, s->cell_start.p, s->sorted_atoms.p);
     launch_sorted_views(s->st, total, s->sorted_atoms.p, s->A, s->asi.p, s->sp.p,
                         fp32 ? s->spf.p : nullptr, s->blo);
     const std::vector<int32_t>& sten = s->newton ? s->stencil_fwd : s->stencil;
+    const int32_t* old_stencil = s->d_stencil.p;
     TRY(ensure(s, s->d_stencil, sten.size() + 1));
-    if (!sten.empty())
+    if (!sten.empty() && (s->d_stencil.p != old_stencil || sten != s->stencil_on_device)) {
+        // pageable source: the copy completes before cudaMemcpyAsync returns
         CK(cudaMemcpyAsync(s->d_stencil.p, sten.data(), sten.size() * 4, cudaMemcpyHostToDevice, s->st));
+        s->stencil_on_device = sten;
+    }
     PairParams p;
     p.atom_cell = s->atom_cell.p;
     p.atom_sorted_idx = s->asi.p;
@@ -1321,8 +1335,9 @@ int phase_neighbor(soil_sys* s) {
     p.sf_sq = s->skin_fraction * s->skin_fraction;
     p.sf = s->skin_fraction;
     p.eps32 = pair_eps(s);
-    CK(cudaMemsetAsync(&s->dflags->candidates, 0, 16, s->st));
-    CK(cudaMemsetAsync(&s->dflags->error, 0, 4, s->st));
+    // candidates, rechecked and error are adjacent: one clear
+    static_assert(offsetof(DevFlags, error) == offsetof(DevFlags, candidates) + 16, "DevFlags layout");
+    CK(cudaMemsetAsync(&s->dflags->candidates, 0, 20, s->st));
     PairSegs sg;
     if (pair_segments(sten, s->stencil_self, s->newton, &sg))
         launch_pair_count_staged(s->st, p, sg, s->rowcount.p, s->row_slots.p, s->dflags);

@@ -126,6 +126,11 @@ struct soil_sys {
     DArr<double> lbx, lby, lbz;
     DArr<uint32_t> sort_cell, sort_perm, sorted_local_cell;
     DArr<uint32_t> cell_counts, cell_start, cell_cursor;
+    // cell_counts[0, counts_clean) is known to be zero (the consuming scatters
+    // leave it so); counts_at: the allocation that holds
+    uint64_t counts_clean = 0;
+    const uint32_t* counts_at = nullptr;
+    std::vector<int32_t> stencil_on_device;  // the stencil last uploaded to d_stencil
     DArr<uint32_t> atom_cell, sorted_atoms, asi, rowcount, offsets, indices, row_slots;
     DArr<double4> sp;
     // persistent per-neighbor slots (slot_max == 0: disabled); buffer
@@ -251,6 +256,8 @@ float pair_eps(const soil_sys* s);
 bool pair_segments(const std::vector<int32_t>& sten, bool has_self, bool newton, PairSegs* sg);
 int sync(soil_sys* s);
 int check_launch(soil_sys* s);
+// cell_counts[0, nc) zero before a counting pass
+int counts_zero(soil_sys* s, uint64_t nc);
 // exclusive scan of in[0, n) into out[0, n] in one launch, errors into the
 // system's device flags
 int scan_1p(soil_sys* s, const uint32_t* in, uint32_t* out, uint64_t n);
