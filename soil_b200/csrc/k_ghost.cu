@@ -145,9 +145,11 @@ __global__ void __launch_bounds__(kBlock) k_border_cat_scan(const uint32_t* coun
     if (threadIdx.x == 0) ctot[k * nchunks + ch] = total;
 }
 
-// Chunk totals -> exclusive chunk prefixes (in place) and category totals.
+// Chunk totals -> exclusive chunk prefixes (in place) and category totals;
+// clears the capacity word bs[10] that pass 3 may set.
 __global__ void __launch_bounds__(kBlock) k_border_chunk_prefix(uint32_t* ctot, uint64_t nchunks,
                                                                 uint32_t* bs) {
+    if (threadIdx.x == 0) bs[10] = 0u;
     for (uint32_t k = threadIdx.x; k <= (uint32_t)kBorderCats; k += blockDim.x) {
         uint32_t acc = 0;
         for (uint64_t ch = 0; ch < nchunks; ++ch) {

@@ -895,7 +895,8 @@ int phase_borders(soil_sys* s) {
         TRY(borders_arrays(s));
         SendPtrs send;
         for (int k = 0; k < kNumSwaps; ++k) send.p[k] = s->send[k].p;
-        CK(cudaMemsetAsync(s->bstate.p, 0, kBorderStateWords * 4, s->st));
+        // With locals the passes write every word the host reads.
+        if (s->nlocal == 0) CK(cudaMemsetAsync(s->bstate.p, 0, kBorderStateWords * 4, s->st));
         launch_borders(s->st, s->nlocal, s->acap, s->A, cats, bp, s->face_flags.p, s->bcount.p,
                        s->boff.p, s->bstate.p, s->ghost_root.p, s->ghost_chain.p, send,
                        s->fold_start.p, s->fold_list.p);
