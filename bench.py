@@ -51,11 +51,12 @@ from soil_b200 import abi, dist, workloads  # noqa: E402
 #              with forward comm fused in (light steps): R fold_start (4) per
 #              local, and per ghost R fold_list + chain (8), W pos,vel (48),
 #              R+W forward columns (16 B per f64)
-#   force:     grouped consumer with the reverse fold: R x,y,z,radius (32) and
-#              W force (24) of every atom, R group/fold/count metadata (12 B
-#              per local, 8 B per ghost), R 5 B per sequence entry (2 entries
-#              per pair), and the fold R ghost F (24) + R origin (4) + RMW
-#              owner F (48) per ghost
+#   force:     the consumer with the reverse fold: R x,y,z,radius (32) and
+#              W force (24) of every atom, R list/fold metadata (12 B per
+#              local, 8 B per ghost), R 5 B per pair side (each pair is read
+#              from its owner's row and its partner's transposed list), and
+#              the fold R ghost F (24) + R origin (4) + RMW owner F (48) per
+#              ghost
 #   forward:   R root+chain (8) + R root pos,vel (48) + W pos,vel (48)
 #              + forward columns (16 B per f64) per ghost
 #   reverse:   R send index (4) + R ghost F (24) + RMW owner F (48) per ghost
@@ -68,9 +69,16 @@ BYTES_PER_UNIT = {
     "forward": lambda c, fw: (104 + 16 * fw) * c.nghost,
     "reverse": lambda c, fw: 76 * c.nghost,
 }
-# The kernel each timed phase launches on a light step (ncu names).
-PHASE_KERNEL = {"integrate": "k_initial", "force": "k_force_seq", "final": "k_final",
+# The kernel each timed phase launches on a light step (ncu names); the force
+# phase's kernel depends on SOIL_FORCE and is asked of the library.
+PHASE_KERNEL = {"integrate": "k_initial", "final": "k_final",
                 "forward": "k_forward", "reverse": "k_reverse_fold_roots"}
+
+
+def phase_kernel(lib, phase):
+    if phase == "force":
+        return lib.soil_consumer_kernel().decode()
+    return PHASE_KERNEL.get(phase, phase)
 
 
 def log(*a):
@@ -282,7 +290,10 @@ def run_soil(args, world, rank, local):
     # the remaining warm-up steps to find the dominant kernel
     s.step(1)
     s.set_timing((1 << abi.SOIL_NUM_TIMERS) - 1)
-    s.step(max(args.warmup - 1, 2))
+    r_warm = s.counts().rebuilds
+    n_warm = max(args.warmup - 1, 2)
+    s.step(n_warm)
+    all_rebuilds = s.counts().rebuilds - r_warm == n_warm
     ms0, _, iv0 = s.get_timing()
     light = {abi.TIMER_NAMES[t]: ms0[t] / max(iv0[t], 1) for t in range(abi.SOIL_NUM_TIMERS)
              if abi.TIMER_NAMES[t] in BYTES_PER_UNIT}
@@ -291,7 +302,10 @@ def run_soil(args, world, rank, local):
     # (k_steps, one launch for many steps) unless SOIL_RESIDENT_STEPS=0; phase
     # timers would force the launch-per-phase path, so they stay off there and
     # the roofline comes from the light-step time of the rebuild probe.
-    resident = (w.n <= 2 ** 20 and os.environ.get("SOIL_RESIDENT_STEPS", "2") != "0")
+    # A workload that rebuilds on every step has no communicate-only stretch
+    # to run resident, and keeps its phase timer.
+    resident = (w.n <= 2 ** 20 and os.environ.get("SOIL_RESIDENT_STEPS", "2") != "0"
+                and not all_rebuilds)
     s.set_timing(0 if resident else 1 << abi.TIMER_NAMES.index(dominant))
 
     c0 = s.counts()
@@ -324,12 +338,13 @@ def run_soil(args, world, rank, local):
     per_launch_ms = ms_dom[k] / max(launches_dom[k], 1)
     alg_bytes = BYTES_PER_UNIT[dominant](c1, fwd_width)
     achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
-    tr = load_traffic(PHASE_KERNEL.get(dominant), args.config)
+    kname = phase_kernel(lib, dominant)
+    tr = load_traffic(kname, args.config)
     traffic = None
     if tr:
         traffic = tr["dram_bytes_per_atom"] * (c1.nlocal if dominant in ("integrate", "final")
                                                else c1.nlocal + c1.nghost)
-    roofline = {"bound": "hbm", "kernel": PHASE_KERNEL.get(dominant, dominant), "phase": dominant,
+    roofline = {"bound": "hbm", "kernel": kname, "phase": dominant,
                 "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                 "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,

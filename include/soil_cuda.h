@@ -499,6 +499,9 @@ int soil_server_get_stats(soil_server* server, soil_server_stats* out);
  * wall-clock thermo columns, soil_print/src/lib.rs:20-26) ------------------ */
 /* Kernels this library has launched in this process. */
 uint64_t soil_kernel_launches(void);
+/* Name of the kernel that computes the built-in consumer's forces on a
+ * single system under the current SOIL_FORCE setting ("k_force_csr", ...). */
+const char* soil_consumer_kernel(void);
 /* Phase timers of soil_step: CUDA events recorded on the system stream
  * around each phase.  0 integrate (deform + initial, with the previous final
  * fused in), 1 zero, 2 pbc, 3 sort, 4 borders, 5 forward, 6 neighbor,

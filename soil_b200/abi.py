@@ -264,6 +264,7 @@ PROTOTYPES = {
     "soil_sys_save_restart": (C.c_int, [P, u64, P, u64, pu64]),
     "soil_sys_load_restart": (C.c_int, [P, P, u64, pu64]),
     "soil_kernel_launches": (C.c_uint64, []),
+    "soil_consumer_kernel": (C.c_char_p, []),
     "soil_sys_set_timing": (C.c_int, [P, u32]),
     "soil_sys_get_timing": (C.c_int, [P, pdbl, pu64, pu64]),
     "soil_timer_name": (C.c_char_p, [i32]),

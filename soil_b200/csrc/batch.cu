@@ -341,6 +341,7 @@ void fill_dev(soil_batch* b, uint32_t k) {
                          prev.set[1].x == s->A.x;
     std::memcpy(&d.set[0], swapped ? &s->B : &s->A, sizeof(AtomCols));
     std::memcpy(&d.set[1], swapped ? &s->A : &s->B, sizeof(AtomCols));
+    d.set[0].pk = d.set[1].pk = nullptr;  // the batch's kernels read the columns
     d.radius_plane = s->cols[s->radius_col].plane0;
     d.shear_rate = s->shear_rate;
     d.yc = profile_center(s);
@@ -1001,6 +1002,7 @@ int detach(soil_batch* b, uint32_t k) {
     soil_sys* s = b->slot[k];
     s->counts_clean = 0;  // the batch's counting passes leave counts behind
     s->stencil_on_device.clear();
+    s->pk_valid = false;  // the batch moved atoms without the packed records
     s->st = b->saved[k];
     s->batch = nullptr;
     b->slot[k] = nullptr;

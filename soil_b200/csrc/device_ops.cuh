@@ -257,6 +257,28 @@ __device__ uint32_t row_scan(const PairParams& p, const Filter<UNIFORM, FP32>& t
 
 // ---- per-atom bodies of the kernels ----------------------------------------
 
+// x, y, z of atom i's packed record (the radius word is left as packed).
+__device__ __forceinline__ void put_pk(const AtomCols& c, uint64_t i, double x, double y,
+                                       double z) {
+    if (!c.pk) return;
+    double* r = c.pk + 4 * i;
+    *reinterpret_cast<double2*>(r) = make_double2(x, y);
+    r[2] = z;
+}
+
+// Atom i's packed record (32-byte aligned) in one 256-bit load.  A plain
+// (coherent) load: the resident steps write the records between their grid
+// barriers, so the non-coherent path is not an option; the memory clobber
+// keeps the load in program order with the kernel's other accesses.
+__device__ __forceinline__ double4 ld_pk(const double* pk, uint64_t i) {
+    double4 v;
+    asm volatile("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];"
+                 : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w)
+                 : "l"(pk + 4 * i)
+                 : "memory");
+    return v;
+}
+
 // initial_integration (soil_verlet/src/lib.rs:131-162) of atom i, optionally
 // preceded by final_integration of the previous step with the same forces;
 // returns the new position.
@@ -284,6 +306,7 @@ __device__ __forceinline__ void initial_atom(const AtomCols& c, uint64_t i, doub
     c.x[i] = x;
     c.y[i] = y;
     c.z[i] = z;
+    put_pk(c, i, x, y, z);
     if (zero_force) {  // zero_all_forces, atom.rs:631-635 (locals part)
         c.fx[i] = 0.0;
         c.fy[i] = 0.0;
@@ -366,6 +389,7 @@ __device__ __forceinline__ void forward_ghost(const AtomCols& c, uint64_t nlocal
     c.x[g] = px;
     c.y[g] = py;
     c.z[g] = pz;
+    put_pk(c, g, px, py, pz);
     c.vx[g] = vx;
     c.vy[g] = vy;
     c.vz[g] = vz;
@@ -405,6 +429,7 @@ __device__ __forceinline__ void forward_images(const AtomCols& c, uint64_t nloca
         c.x[g] = px;
         c.y[g] = py;
         c.z[g] = pz;
+        put_pk(c, g, px, py, pz);
         c.vx[g] = vx;
         c.vy[g] = vy;
         c.vz[g] = vz;

@@ -107,6 +107,43 @@ __device__ __forceinline__ bool pair_force(double xa, double ya, double za, doub
     return true;
 }
 
+// Partner records for the one-thread-per-root walks: the packed copy (one
+// 256-bit load) or the x, y, z and radius columns (four loads).
+struct PkLd {
+    const double* pk;
+    __device__ __forceinline__ double4 operator()(uint64_t o) const { return ld_pk(pk, o); }
+};
+struct ColLd {
+    const double* x;
+    const double* y;
+    const double* z;
+    const double* r;
+    __device__ __forceinline__ double4 operator()(uint64_t o) const {
+        return make_double4(x[o], y[o], z[o], r[o]);
+    }
+};
+
+// F += f(a, o) over the partners o = idx(0), ..., idx(n - 1) in that order.
+// Partner k + 1's record is loaded before partner k's force is evaluated, so
+// two gathers are in flight per thread.
+template <class Ld, class Idx>
+__device__ __forceinline__ void sum_partners(const Ld& ld, const double4& pa, double K, uint32_t n,
+                                             const Idx& idx, double& Fx, double& Fy, double& Fz) {
+    if (n == 0) return;
+    double4 cur = ld(idx(0));
+    for (uint32_t k = 0; k < n; ++k) {
+        double4 nxt = cur;
+        if (k + 1 < n) nxt = ld(idx(k + 1));
+        double fx, fy, fz;
+        if (pair_force(pa.x, pa.y, pa.z, pa.w, cur.x, cur.y, cur.z, cur.w, K, fx, fy, fz)) {
+            Fx = Fx + fx;
+            Fy = Fy + fy;
+            Fz = Fz + fz;
+        }
+        cur = nxt;
+    }
+}
+
 // The item (root or image) a lane's walk is in: its atom and entry range.
 struct Item {
     uint64_t atom;
@@ -228,52 +265,55 @@ __device__ __forceinline__ void force_tile(const ForceSeq& p, const AtomCols& c,
     }
 }
 
+// Partner k of atom a's flattened order: in-list rows below a (npre of
+// them), a's own row, the rest of the in-list.
+struct CsrIdx {
+    const uint32_t* in_list;
+    const uint32_t* indices;
+    uint32_t qs, npre, rs, nrow;
+    __device__ __forceinline__ uint32_t operator()(uint32_t k) const {
+        return k < npre ? in_list[qs + k]
+             : k < npre + nrow ? indices[rs + (k - npre)] : in_list[qs + (k - nrow)];
+    }
+};
+
 // The force on atom a (a root, or one of its ghost images) in the
 // reference's summation order, from the transposed list and the CSR: in-list
 // rows below a (ascending; in_split[a] of them), a's own row, the in-list
 // rows above a; each entry evaluated as f(a, partner) (the negation argument
 // at the top of k_force.cu).  Ghosts receive only with newton and have no row.
-__device__ __forceinline__ void csr_item_force(const ForceCsr& q, const AtomCols& c, uint64_t a,
+template <class Ld>
+__device__ __forceinline__ void csr_item_force(const ForceCsr& q, const Ld& ld, uint64_t a,
                                                double& Fx, double& Fy, double& Fz) {
     const bool local = a < q.nlocal;
-    const double xa = c.x[a], ya = c.y[a], za = c.z[a], ra = q.rad[a];
+    const double4 pa = ld(a);
     Fx = 0.0;
     Fy = 0.0;
     Fz = 0.0;
-    uint32_t qs = 0, nin = 0, npre = 0, rs = 0, nrow = 0;
+    CsrIdx ix{q.in_list, q.indices, 0, 0, 0, 0};
+    uint32_t nin = 0;
     if (q.newton || local) {
-        qs = q.in_start[a];
-        nin = q.in_start[a + 1] - qs;
-        npre = q.in_split[a];
+        ix.qs = q.in_start[a];
+        nin = q.in_start[a + 1] - ix.qs;
+        ix.npre = q.in_split[a];
     }
     if (local) {
-        rs = q.offsets[a];
-        nrow = q.offsets[a + 1] - rs;
+        ix.rs = q.offsets[a];
+        ix.nrow = q.offsets[a + 1] - ix.rs;
     }
-    // one loop over the flattened order: in-list rows below a, a's row, the
-    // rest of the in-list (a known trip count, so partner loads run ahead)
-    const uint32_t total = nin + nrow;
-    for (uint32_t k = 0; k < total; ++k) {
-        const uint32_t o = k < npre ? q.in_list[qs + k]
-                         : k < npre + nrow ? q.indices[rs + (k - npre)] : q.in_list[qs + (k - nrow)];
-        double fx, fy, fz;
-        if (pair_force(xa, ya, za, ra, c.x[o], c.y[o], c.z[o], q.rad[o], q.K, fx, fy, fz)) {
-            Fx = Fx + fx;
-            Fy = Fy + fy;
-            Fz = Fz + fz;
-        }
-    }
+    sum_partners(ld, pa, q.K, nin + ix.nrow, ix, Fx, Fy, Fz);
 }
 
 // Root t and its images by one thread (CSR walk), then (FOLD) the fold.
-template <bool FOLD>
-__device__ __forceinline__ void force_csr_root(const ForceCsr& q, const AtomCols& c,
-                                               const PlaneList& rev, uint64_t t) {
+template <bool FOLD, class Ld>
+__device__ __forceinline__ void force_csr_root_ld(const ForceCsr& q, const Ld& ld,
+                                                  const AtomCols& c, const PlaneList& rev,
+                                                  uint64_t t) {
     const uint32_t f0 = q.fold_start[t], f1 = q.fold_start[t + 1];
     for (uint32_t f = f0 - 1; f + 1 <= f1; ++f) {  // the root (f = f0 - 1), then its images
         const uint64_t a = f + 1 == f0 ? t : q.nlocal + q.fold_list[f];
         double Fx, Fy, Fz;
-        csr_item_force(q, c, a, Fx, Fy, Fz);
+        csr_item_force(q, ld, a, Fx, Fy, Fz);
         c.fx[a] = Fx;
         c.fy[a] = Fy;
         c.fz[a] = Fz;
@@ -281,34 +321,49 @@ __device__ __forceinline__ void force_csr_root(const ForceCsr& q, const AtomCols
     if (FOLD) fold_root(c, q.nlocal, t, q.fold_start, q.fold_list, rev);
 }
 
+// PK: the partners' records from q.pk (which must then be set), else from
+// the columns.
+template <bool FOLD, bool PK>
+__device__ __forceinline__ void force_csr_root(const ForceCsr& q, const AtomCols& c,
+                                               const PlaneList& rev, uint64_t t) {
+    if constexpr (PK) force_csr_root_ld<FOLD>(q, PkLd{q.pk}, c, rev, t);
+    else force_csr_root_ld<FOLD>(q, ColLd{c.x, c.y, c.z, q.rad}, c, rev, t);
+}
+
+// Entry k of a group's sequence.
+struct SeqIdx {
+    const uint32_t* seq;
+    __device__ __forceinline__ uint32_t operator()(uint32_t k) const { return seq[k]; }
+};
+
 // Root t's group walked by one thread: each item's (root's, then every
 // image's) sequence summed in order, its force written, then (FOLD) the
 // images folded into the root in reverse_send_force's order.
-template <bool FOLD>
-__device__ __forceinline__ void force_walk_root(const ForceSeq& p, const AtomCols& c,
-                                                const PlaneList& rev, uint64_t t) {
+template <bool FOLD, class Ld>
+__device__ __forceinline__ void force_walk_root_ld(const ForceSeq& p, const Ld& ld,
+                                                   const AtomCols& c, const PlaneList& rev,
+                                                   uint64_t t) {
     const uint64_t nl = p.nlocal;
     const uint32_t f0 = p.fold_start[t], nimg = p.fold_start[t + 1] - f0;
     uint32_t k = p.grp_start[t];
     for (uint32_t j = 0; j <= nimg; ++j) {
         const uint64_t a = j == 0 ? t : nl + p.fold_list[f0 + j - 1];
-        const uint32_t e = k + p.cnt[a];
-        const double xa = c.x[a], ya = c.y[a], za = c.z[a], ra = p.rad[a];
+        const uint32_t n = p.cnt[a];
         double Fx = 0.0, Fy = 0.0, Fz = 0.0;
-        for (; k < e; ++k) {
-            const uint32_t o = p.seq[k];
-            double fx, fy, fz;
-            if (pair_force(xa, ya, za, ra, c.x[o], c.y[o], c.z[o], p.rad[o], p.K, fx, fy, fz)) {
-                Fx = Fx + fx;
-                Fy = Fy + fy;
-                Fz = Fz + fz;
-            }
-        }
+        sum_partners(ld, ld(a), p.K, n, SeqIdx{p.seq + k}, Fx, Fy, Fz);
+        k += n;
         c.fx[a] = Fx;
         c.fy[a] = Fy;
         c.fz[a] = Fz;
     }
     if (FOLD) fold_root(c, nl, t, p.fold_start, p.fold_list, rev);
+}
+
+template <bool FOLD, bool PK>
+__device__ __forceinline__ void force_walk_root(const ForceSeq& p, const AtomCols& c,
+                                                const PlaneList& rev, uint64_t t) {
+    if constexpr (PK) force_walk_root_ld<FOLD>(p, PkLd{p.pk}, c, rev, t);
+    else force_walk_root_ld<FOLD>(p, ColLd{c.x, c.y, c.z, p.rad}, c, rev, t);
 }
 
 }  // namespace soil

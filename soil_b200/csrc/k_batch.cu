@@ -583,6 +583,7 @@ __device__ __forceinline__ ForceSeq force_seq_of(const BoxDev& D, const BoxStep&
     q.owner = D.seq_owner;
     q.fold_start = D.fold_start;
     q.fold_list = D.fold_list;
+    q.pk = nullptr;
     return q;
 }
 
@@ -604,8 +605,8 @@ __global__ void __launch_bounds__(kBlock, 4) kb_force_walk(Span sp, BatchArgs A)
         const BoxStep& S = A.step[b];
         const AtomCols& c = D.set[S.post];
         const ForceSeq q = force_seq_of(D, S, c);
-        if (S.newton) force_walk_root<true>(q, c, D.rev, i);
-        else force_walk_root<false>(q, c, D.rev, i);
+        if (S.newton) force_walk_root<true, false>(q, c, D.rev, i);
+        else force_walk_root<false, false>(q, c, D.rev, i);
     });
 }
 void b_force_walk(cudaStream_t st, const Span& sp, const BatchArgs& a) {

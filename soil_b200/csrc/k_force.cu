@@ -102,20 +102,21 @@ __global__ void __launch_bounds__(kBlock, 4) k_force_seq(ForceArgs p) {
         force_tile<U, FOLD>(p.q, p.c, p.rev, w, sm, lane, wib);
 }
 
-template <bool FOLD>
+// PK: partner records from the packed copy (p.q.pk / q.pk set).
+template <bool FOLD, bool PK>
 __global__ void __launch_bounds__(kBlock, 4) k_force_walk(ForceArgs p) {
     for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < p.q.nlocal;
          t += (uint64_t)gridDim.x * blockDim.x)
-        force_walk_root<FOLD>(p.q, p.c, p.rev, t);
+        force_walk_root<FOLD, PK>(p.q, p.c, p.rev, t);
 }
 
-template <bool FOLD>
+template <bool FOLD, bool PK>
 __global__ void __launch_bounds__(kBlock, 4) k_force_csr(ForceCsr q, AtomCols c, PlaneList rev) {
     // grid-stride over whole blocks of kBlock roots, so a block's order
     // permutes its own roots
     for (uint64_t b = (uint64_t)blockIdx.x * kBlock; b < q.nlocal; b += (uint64_t)gridDim.x * kBlock) {
         const uint64_t k = b + threadIdx.x;
-        if (k < q.nlocal) force_csr_root<FOLD>(q, c, rev, q.order ? q.order[k] : k);
+        if (k < q.nlocal) force_csr_root<FOLD, PK>(q, c, rev, q.order ? q.order[k] : k);
     }
 }
 
@@ -169,8 +170,13 @@ void launch_force_csr(cudaStream_t st, const ForceCsr& q, const AtomCols& c, con
     const unsigned full = 148u * 4u;  // one resident wave at <= 64 registers
     const unsigned need = (unsigned)((q.nlocal + kBlock - 1) / kBlock);
     const unsigned grid = need < full ? need : full;
-    if (fold) k_force_csr<true><<<grid, kBlock, 0, st>>>(q, c, rev);
-    else k_force_csr<false><<<grid, kBlock, 0, st>>>(q, c, rev);
+    if (q.pk) {
+        if (fold) k_force_csr<true, true><<<grid, kBlock, 0, st>>>(q, c, rev);
+        else k_force_csr<false, true><<<grid, kBlock, 0, st>>>(q, c, rev);
+    } else {
+        if (fold) k_force_csr<true, false><<<grid, kBlock, 0, st>>>(q, c, rev);
+        else k_force_csr<false, false><<<grid, kBlock, 0, st>>>(q, c, rev);
+    }
 }
 
 template <int U>
@@ -203,8 +209,13 @@ void launch_force_seq(cudaStream_t st, const ForceArgs& p, bool fold, int varian
         const unsigned full = 148u * 4u;  // one resident wave at <= 64 registers
         const unsigned need = (unsigned)((p.q.nlocal + kBlock - 1) / kBlock);
         const unsigned grid = need < full ? need : full;
-        if (fold) k_force_walk<true><<<grid, kBlock, 0, st>>>(p);
-        else k_force_walk<false><<<grid, kBlock, 0, st>>>(p);
+        if (p.q.pk) {
+            if (fold) k_force_walk<true, true><<<grid, kBlock, 0, st>>>(p);
+            else k_force_walk<false, true><<<grid, kBlock, 0, st>>>(p);
+        } else {
+            if (fold) k_force_walk<true, false><<<grid, kBlock, 0, st>>>(p);
+            else k_force_walk<false, false><<<grid, kBlock, 0, st>>>(p);
+        }
     } else if (variant == SOIL_FORCE_TILES2) {
         launch_tiles<2>(st, p, fold);
     } else {

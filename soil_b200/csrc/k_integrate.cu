@@ -161,10 +161,13 @@ void launch_shear_profile(cudaStream_t st, uint64_t n, const AtomCols& c, double
 __global__ void __launch_bounds__(kBlock) k_remap(uint64_t n, AtomCols c, RemapSpec r) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x)
+    {
         for (int q = 0; q < r.n; ++q) {
             double* x = r.dim[q] == 0 ? c.x : r.dim[q] == 1 ? c.y : c.z;
             x[i] = r.new_center[q] + (x[i] - r.old_center[q]) * r.scale[q];
         }
+        put_pk(c, i, c.x[i], c.y[i], c.z[i]);
+    }
 }
 
 void launch_remap(cudaStream_t st, uint64_t n, const AtomCols& c, const RemapSpec& r) {
@@ -302,6 +305,22 @@ void launch_interleave_w(cudaStream_t st, uint64_t n, int w, double* dst, const 
         note_launch();
         k_interleave_w<<<grid_for(n), kBlock, 0, st>>>(n, w, dst, src0, cap);
     }
+}
+
+__global__ void __launch_bounds__(kBlock) k_pack(uint64_t n, AtomCols c, const double* rad,
+                                                 double* pk) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        double2* r = reinterpret_cast<double2*>(pk + 4 * i);
+        r[0] = make_double2(c.x[i], c.y[i]);
+        r[1] = make_double2(c.z[i], rad[i]);
+    }
+}
+
+void launch_pack(cudaStream_t st, uint64_t n, const AtomCols& c, const double* rad, double* pk) {
+    if (n == 0) return;
+    note_launch();
+    k_pack<<<grid_for(n), kBlock, 0, st>>>(n, c, rad, pk);
 }
 
 }  // namespace soil

@@ -79,7 +79,7 @@ __device__ bool grid_sync(GridBar* b, unsigned nblocks, unsigned& gen, uint32_t*
 // tiles over grouped sequences (force_tile), 1 one root per thread over
 // them (force_walk_root), 2 one root per thread over the CSR and its
 // transpose (force_csr_root).
-template <int U, int CONSUMER, int MODE>
+template <int U, int CONSUMER, int MODE, bool PK>
 __global__ void __launch_bounds__(kBlock, 4) k_steps(StepsArgs a) {
     __shared__ ForceSmem<U> sm;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -124,12 +124,13 @@ __global__ void __launch_bounds__(kBlock, 4) k_steps(StepsArgs a) {
                  b += (uint64_t)gridDim.x * kBlock) {
                 const uint64_t k = b + threadIdx.x;
                 if (k < nl)
-                    force_csr_root<CONSUMER == 2>(a.fc, c, a.fa.rev, a.fc.order ? a.fc.order[k] : k);
+                    force_csr_root<CONSUMER == 2, PK>(a.fc, c, a.fa.rev,
+                                                      a.fc.order ? a.fc.order[k] : k);
             }
         } else if (CONSUMER && MODE == 1) {
             for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < nl;
                  t += (uint64_t)gridDim.x * blockDim.x)
-                force_walk_root<CONSUMER == 2>(a.fa.q, c, a.fa.rev, t);
+                force_walk_root<CONSUMER == 2, PK>(a.fa.q, c, a.fa.rev, t);
         } else if (CONSUMER) {
             const uint64_t ntiles = (nl + 31) / 32;
             for (uint64_t w = (uint64_t)blockIdx.x * kForceWarps + wib; w < ntiles;
@@ -148,16 +149,29 @@ __global__ void __launch_bounds__(kBlock, 4) k_steps(StepsArgs a) {
     }
 }
 
-static const void* steps_kernel(int consumer, int mode) {
-    if (consumer == 0) return (const void*)k_steps<4, 0, 2>;
-    if (mode == 2) return consumer == 1 ? (const void*)k_steps<4, 1, 2> : (const void*)k_steps<4, 2, 2>;
-    if (mode == 1) return consumer == 1 ? (const void*)k_steps<4, 1, 1> : (const void*)k_steps<4, 2, 1>;
-    return consumer == 1 ? (const void*)k_steps<4, 1, 0> : (const void*)k_steps<4, 2, 0>;
+// PK (modes 1 and 2): the walks read the packed records.
+static const void* steps_kernel(int consumer, int mode, bool pk) {
+    if (consumer == 0) return (const void*)k_steps<4, 0, 2, false>;
+    if (mode == 2) {
+        if (pk)
+            return consumer == 1 ? (const void*)k_steps<4, 1, 2, true>
+                                 : (const void*)k_steps<4, 2, 2, true>;
+        return consumer == 1 ? (const void*)k_steps<4, 1, 2, false>
+                             : (const void*)k_steps<4, 2, 2, false>;
+    }
+    if (mode == 1) {
+        if (pk)
+            return consumer == 1 ? (const void*)k_steps<4, 1, 1, true>
+                                 : (const void*)k_steps<4, 2, 1, true>;
+        return consumer == 1 ? (const void*)k_steps<4, 1, 1, false>
+                             : (const void*)k_steps<4, 2, 1, false>;
+    }
+    return consumer == 1 ? (const void*)k_steps<4, 1, 0, false> : (const void*)k_steps<4, 2, 0, false>;
 }
 
-int steps_grid(int consumer, int walk, uint64_t nlocal, int* grid) {
+int steps_grid(int consumer, int walk, bool pk, uint64_t nlocal, int* grid) {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, steps_kernel(consumer, walk), kBlock,
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, steps_kernel(consumer, walk, pk), kBlock,
                                                       0) !=
             cudaSuccess ||
         per_sm < 1) {
@@ -176,11 +190,12 @@ int steps_grid(int consumer, int walk, uint64_t nlocal, int* grid) {
     return 0;
 }
 
-cudaError_t launch_steps(cudaStream_t st, const StepsArgs& a, int consumer, int walk, int grid) {
+cudaError_t launch_steps(cudaStream_t st, const StepsArgs& a, int consumer, int walk, bool pk,
+                         int grid) {
     note_launch();
     StepsArgs arg = a;
     void* params[] = {&arg};
-    return cudaLaunchCooperativeKernel(steps_kernel(consumer, walk), dim3(grid), dim3(kBlock),
+    return cudaLaunchCooperativeKernel(steps_kernel(consumer, walk, pk), dim3(grid), dim3(kBlock),
                                        params, 0, st);
 }
 

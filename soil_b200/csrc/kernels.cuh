@@ -102,6 +102,8 @@ void launch_extent(cudaStream_t st, uint64_t n, const AtomCols& c, int mask,
                    unsigned long long* ext);
 // inv[i] = 1.0 / m[i], i < n
 void launch_inverse(cudaStream_t st, uint64_t n, const double* m, double* inv);
+// pk[4 i .. 4 i + 3] = (x, y, z, rad) of atoms [0, n)
+void launch_pack(cudaStream_t st, uint64_t n, const AtomCols& c, const double* rad, double* pk);
 // host-layout conversions ([n][3] or [n][w] interleaved <-> SoA planes)
 void launch_deinterleave3(cudaStream_t st, uint64_t n, const double* src, double* a, double* b,
                           double* c);
@@ -347,6 +349,7 @@ struct ForceSeq {
     const uint8_t* owner;
     const uint32_t* fold_start;
     const uint32_t* fold_list;
+    const double* pk;  // packed (x, y, z, r) records, current; NULL: the columns
 };
 struct ForceArgs {
     AtomCols c;
@@ -386,6 +389,7 @@ struct ForceCsr {
     // thread k of the block that takes roots [b, b + kBlock) walks
     // order[b + k].  Threads of a warp then walk groups of similar length.
     const uint32_t* order;
+    const double* pk;  // packed (x, y, z, r) records, current; NULL: the columns
 };
 void launch_force_csr(cudaStream_t st, const ForceCsr& q, const AtomCols& c, const PlaneList& rev,
                       bool fold);
@@ -424,8 +428,9 @@ struct StepsArgs {
     uint32_t* trip;    // 3 check-flag slots, zero at launch
 };
 // Cooperative grid for k_steps (consumer: 0 none, 1 grouped, 2 grouped + fold).
-int steps_grid(int consumer, int walk, uint64_t nlocal, int* grid);
-cudaError_t launch_steps(cudaStream_t st, const StepsArgs& a, int consumer, int walk, int grid);
+int steps_grid(int consumer, int walk, bool pk, uint64_t nlocal, int* grid);
+cudaError_t launch_steps(cudaStream_t st, const StepsArgs& a, int consumer, int walk, bool pk,
+                         int grid);
 
 void launch_harmonic(cudaStream_t st, uint64_t nlocal, uint64_t ntotal, const AtomCols& c,
                      const double* radius, double k, int newton, const uint32_t* offsets,

@@ -677,6 +677,7 @@ int fold_roots_build(soil_sys* s) {
 
 int phase_pbc(soil_sys* s) {
     if (s->state != FULL_REBUILD) return SOIL_OK;
+    s->pk_valid = false;
     const int mask = pbc_mask(s);
     if (mask == 7 || s->nlocal == 0) {
         launch_pbc(s->st, s->nlocal, s->A, geom_of(s), s->bvel);
@@ -837,6 +838,7 @@ int phase_sort(soil_sys* s) {
     bool run, periodic_sort;
     TRY(sort_plan(s, &run, &periodic_sort));
     if (!run) return SOIL_OK;
+    s->pk_valid = false;
     const uint64_t nl = s->nlocal;
     const uint64_t nc = s->total_cells;
     TRY(counts_zero(s, nc));
@@ -880,6 +882,8 @@ int phase_borders(soil_sys* s) {
     // totals once at the end.  If the ghosts did not fit, the arrays grow and
     // the (deterministic) pass is repeated.
     if (s->state != FULL_REBUILD) return SOIL_OK;
+    s->pk_valid = false;
+    s->view_out = false;  // views are valid until the next rebuild
     s->nghost = 0;
     BorderDim bds[3];
     border_setup(s, bds);
@@ -1105,6 +1109,38 @@ int build_seq(soil_sys* s) {
 // (at most 7 images per root, what the sequences' owner byte encodes).
 bool seq_consumer(const soil_sys* s) { return builtin_consumer(s) && s->few_images; }
 
+// Whether the one-thread-per-root consumer kernels read the packed records
+// (SOIL_PACKED=0: the columns; read at each call, for A/B runs).
+bool packed_on() {
+    const char* env = std::getenv("SOIL_PACKED");
+    return !(env && std::atoi(env) == 0);
+}
+
+// The packed records, current for every local and ghost: allocated with the
+// atom capacity and packed from the columns when stale (each rebuild step and
+// host write marks them so); from then on the integration pass and forward
+// comm keep them current through AtomCols::pk.
+int pk_ready(soil_sys* s) {
+    if (!packed_on()) {
+        s->A.pk = s->B.pk = nullptr;
+        s->pk_valid = false;
+        return SOIL_OK;
+    }
+    const double* old = s->pk.p;
+    TRY(ensure(s, s->pk, 4 * s->acap));
+    if (s->pk.p != old) s->pk_valid = false;
+    if (reinterpret_cast<uintptr_t>(s->pk.p) % 32)
+        return fail(s->ctx, SOIL_ERR_CUDA, "packed records: allocation not 32-byte aligned");
+    s->A.pk = s->B.pk = s->pk.p;
+    if (!s->pk_valid) {
+        launch_pack(s->st, s->nlocal + s->nghost, s->A,
+                    s->A.planes[s->cols[s->radius_col].plane0], s->pk.p);
+        TRY(check_launch(s));
+        s->pk_valid = true;
+    }
+    return SOIL_OK;
+}
+
 ForceArgs consumer_args(const soil_sys* s) {
     ForceArgs p;
     p.c = s->A;
@@ -1117,6 +1153,7 @@ ForceArgs consumer_args(const soil_sys* s) {
     p.q.owner = s->seq_owner.p;
     p.q.fold_start = s->fold_start.p;
     p.q.fold_list = s->fold_list.p;
+    p.q.pk = s->pk_valid ? s->pk.p : nullptr;
     zero_planes_of(s, SOIL_COL_REVERSE, p.rev.idx, &p.rev.n);
     return p;
 }
@@ -1135,11 +1172,14 @@ ForceCsr csr_args(const soil_sys* s) {
     q.in_split = s->in_split.p;
     q.fold_start = s->fold_start.p;
     q.fold_list = s->fold_list.p;
+    q.pk = s->pk_valid ? s->pk.p : nullptr;
     return q;
 }
 
-// The CSR walk's per-block root order (SOIL_ROOT_ORDER=0: index order),
-// built once per set of lists.
+// The CSR walk's per-block root order when SOIL_ROOT_ORDER=1 (built once per
+// set of lists), else index order: measured on 4M atoms, ordering roots by
+// work gave each warp more even trips but scattered the roots' own reads and
+// writes, and the walk ran slower.
 int csr_with_order(soil_sys* s, ForceCsr* q) {
     if (!s->split_valid) {  // transposed lists sorted elsewhere (a batch)
         const uint64_t total = s->nlocal + s->nghost;
@@ -1150,7 +1190,7 @@ int csr_with_order(soil_sys* s, ForceCsr* q) {
     }
     *q = csr_args(s);
     const char* env = std::getenv("SOIL_ROOT_ORDER");
-    if (env && std::atoi(env) == 0) return SOIL_OK;
+    if (!env || std::atoi(env) != 1) return SOIL_OK;
     if (!s->order_valid) {
         TRY(ensure(s, s->root_order, s->nlocal + 1, 0, s->acap + 1));
         launch_root_order(s->st, *q, s->root_order.p);
@@ -1175,6 +1215,7 @@ bool consumer_folds(const soil_sys* s) {
 int launch_consumer(soil_sys* s, bool fold) {
     if (!s->in_lists_valid) TRY(build_in_lists(s));
     const int variant = force_variant();
+    if (variant != SOIL_FORCE_GATHER) TRY(pk_ready(s));
     if (variant == SOIL_FORCE_CSR) {
         PlaneList rev;
         zero_planes_of(s, SOIL_COL_REVERSE, rev.idx, &rev.n);
@@ -1369,6 +1410,7 @@ int phase_neighbor(soil_sys* s) {
 
 int make_view(soil_sys* s, soil_dev_view* v) {
     std::memset(v, 0, sizeof(*v));
+    s->pk_valid = false;  // the holder of a view may write any column
     TRY(update_colptrs(s));
     v->nlocal = s->nlocal;
     v->nghost = s->nghost;
@@ -1647,6 +1689,7 @@ uint64_t resident_limit(const soil_sys* s, uint64_t want) {
 int resident_steps(soil_sys* s, uint64_t max, uint64_t* done, bool* tripped, StepPlan* plan) {
     const StepPlan p = plan_step(s);
     const bool consumer = builtin_consumer(s);
+    if (consumer && force_variant() != SOIL_FORCE_GATHER) TRY(pk_ready(s));
     StepsArgs a;
     std::memset(&a, 0, sizeof(a));
     a.c = s->A;
@@ -1680,12 +1723,13 @@ int resident_steps(soil_sys* s, uint64_t max, uint64_t* done, bool* tripped, Ste
     a.trip = s->rstate.p + 4;
     a.flags = s->dflags;
     int grid = 0;
-    if (steps_grid(kind, a.walk, s->nlocal, &grid))
+    const bool pk = a.walk == 2 ? a.fc.pk != nullptr : a.fa.q.pk != nullptr;
+    if (steps_grid(kind, a.walk, pk, s->nlocal, &grid))
         return fail(s->ctx, SOIL_ERR_CUDA, "no cooperative occupancy for the resident steps");
     CK(cudaMemsetAsync(s->rstate.p, 0, 8 * 4, s->st));
     CK(cudaMemsetAsync(&s->dflags->rebuild, 0, 4, s->st));
     CK(cudaMemsetAsync(&s->dflags->error, 0, 4, s->st));
-    CK(launch_steps(s->st, a, kind, a.walk, grid));
+    CK(launch_steps(s->st, a, kind, a.walk, pk, grid));
     CK(cudaMemcpyAsync(s->hword, a.out, 8, cudaMemcpyDeviceToHost, s->st));
     TRY(read_flags(s));
     if (s->hflags->error & SOIL_STEPS_ERR_BARRIER)
@@ -1709,6 +1753,7 @@ int resident_steps(soil_sys* s, uint64_t max, uint64_t* done, bool* tripped, Ste
 // soil_step: communicate-only stretches run resident when resident_limit
 // allows (at least two steps), every other step through full_step.
 int step_many(soil_sys* s, uint64_t n) {
+    if (s->view_out) s->pk_valid = false;  // a view's holder may have moved atoms
     uint64_t k = 0;
     while (k < n) {
         const uint64_t lim = resident_limit(s, n - k);
@@ -1890,7 +1935,7 @@ int soil_sys_destroy(soil_sys* s) {
     for (int k = 0; k < 2; ++k) { fr(s->slot_tag[k]); fr(s->slot_val[k]); }
     fr(s->in_count); fr(s->in_start); fr(s->in_cursor); fr(s->in_list); fr(s->in_split);
     fr(s->seq_cnt); fr(s->grp_cnt); fr(s->grp_start); fr(s->seq); fr(s->seq_owner);
-    fr(s->rstate); fr(s->scan1p); fr(s->root_order);
+    fr(s->rstate); fr(s->scan1p); fr(s->root_order); fr(s->pk);
     fr(s->ghost_root); fr(s->ghost_chain);
     fr(s->fold_start); fr(s->fold_list);
     for (auto& a : s->send) fr(a);
@@ -2074,6 +2119,7 @@ int soil_sys_set_harmonic(soil_sys* s, double k, int32_t radius_col) {
     if (s->batch) return fail(s->ctx, SOIL_ERR_STATE, "the force of a batched system is fixed");
     s->harmonic_k = k;
     s->radius_col = radius_col;
+    s->pk_valid = false;
     s->in_lists_valid = false;
     s->seq_valid = false;
     s->order_valid = false;
@@ -2300,10 +2346,20 @@ int soil_sys_view(soil_sys* s, soil_dev_view* out) {
     if (!s || !out) return SOIL_ERR_INVALID;
     TRY(flush_pending(s));
     TRY(make_view(s, out));
+    s->view_out = true;  // columns may change between steps until the next rebuild
     return sync(s);  // stream-ordered allocations are ready for every stream
 }
 
 uint64_t soil_kernel_launches(void) { return launches_so_far(); }
+
+const char* soil_consumer_kernel(void) {
+    switch (soil::force_variant()) {
+        case soil::SOIL_FORCE_GATHER: return "k_harmonic";
+        case soil::SOIL_FORCE_CSR: return "k_force_csr";
+        case soil::SOIL_FORCE_WALK: return "k_force_walk";
+        default: return "k_force_seq";
+    }
+}
 
 int soil_sys_set_timing(soil_sys* s, uint32_t mask) {
     if (!s) return SOIL_ERR_INVALID;

@@ -104,6 +104,11 @@ struct AtomCols {
     double* planes[kMaxPlanes];
     int nplanes;
     uint64_t cap;
+    // Packed (x, y, z, r) records of the built-in consumer, 4 doubles per
+    // atom on a 32-byte boundary (null when unused).  The integration pass
+    // and forward comm write x, y, z next to the columns; r and the rebuild
+    // steps' positions come from a packing pass.
+    double* pk;
 };
 
 // Per-swap constants of the ghost maps (SwapData, comm.rs:114-124).

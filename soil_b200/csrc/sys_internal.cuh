@@ -143,6 +143,11 @@ struct soil_sys {
     DArr<uint32_t> in_count, in_start, in_cursor, in_list;
     DArr<uint32_t> in_split;  // per atom: transposed-list entries below it
     bool split_valid = false;
+    // packed (x, y, z, r) records of the consumer kernels (AtomCols::pk);
+    // pk_valid: they match the columns of every local and ghost
+    DArr<double> pk;
+    bool pk_valid = false;
+    bool view_out = false;  // a device view was handed out since the last rebuild
     // grouped partner sequences of the built-in consumer (rebuilt with the
     // lists): per-atom lengths, per-root group lengths and starts, entries
     DArr<uint32_t> seq_cnt, grp_cnt, grp_start, seq;

@@ -83,3 +83,52 @@ def test_fused_forward_and_root_order_match_oracle(ctx, order):
                 os.environ.pop(k, None)
             else:
                 os.environ[k] = v
+
+
+class _Dev:
+    """A device array as __cuda_array_interface__, for torch.as_tensor."""
+
+    def __init__(self, ptr, n, typestr):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr,
+                                         "data": (ptr, False), "version": 3}
+
+
+def _grow_radius_through_view(g, atoms, factor):
+    import torch
+    v = g.view()
+    cols = torch.as_tensor(_Dev(v.columns, v.ncolumns, "<u8"), device="cuda").cpu()
+    rad = torch.as_tensor(_Dev(int(cols[0]), v.nlocal, "<f8"), device="cuda")
+    rad[atoms] *= factor
+    torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("force", ["csr", "walk"])
+@pytest.mark.parametrize("resident", ["1", "0"])
+def test_packed_records_follow_view_writes(ctx, force, resident):
+    """The consumer kernels read packed (x, y, z, r) records that the
+    integration pass and forward comm keep current; radii written through a
+    device view between steps must reach them.  Packed and column reads give
+    the same bits before and after such a write."""
+    keys = ("SOIL_PACKED", "SOIL_FORCE", "SOIL_RESIDENT_STEPS")
+    old = {k: os.environ.get(k) for k in keys}
+    try:
+        runs = []
+        for packed in ("1", "0"):
+            os.environ.update({"SOIL_PACKED": packed, "SOIL_FORCE": force,
+                               "SOIL_RESIDENT_STEPS": resident})
+            w = W.poly("pk", 93, 4000, 0.5, 1e-4, 0, harmonic_k=1e3)
+            g = system.from_workload(ctx, w)
+            g.step(12)
+            _grow_radius_through_view(g, [3, 500, 2100, 3999], 1.05)
+            g.step(12)
+            runs.append(g)
+        assert_same_state(runs[0], runs[1], f"{force} resident={resident}")
+        assert_same_lists(runs[0], runs[1])
+        for g in runs:
+            g.close()
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
