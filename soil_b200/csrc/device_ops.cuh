@@ -257,13 +257,16 @@ __device__ uint32_t row_scan(const PairParams& p, const Filter<UNIFORM, FP32>& t
 
 // ---- per-atom bodies of the kernels ----------------------------------------
 
-// x, y, z of atom i's packed record (the radius word is left as packed).
-__device__ __forceinline__ void put_pk(const AtomCols& c, uint64_t i, double x, double y,
-                                       double z) {
-    if (!c.pk) return;
-    double* r = c.pk + 4 * i;
-    *reinterpret_cast<double2*>(r) = make_double2(x, y);
-    r[2] = z;
+// Atom i's packed record (x, y, z, its radius) in one 256-bit store: whole
+// 32-byte sectors, so the write needs no read of the old record.  The radius
+// is atom i's value of the plane c.pkrad (a forward comm copies a ghost's
+// forward planes before it writes the record).
+__device__ __forceinline__ void put_pk(double* pk, uint64_t i, double x, double y, double z,
+                                       double r) {
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};"
+                 :
+                 : "l"(pk + 4 * i), "d"(x), "d"(y), "d"(z), "d"(r)
+                 : "memory");
 }
 
 // Atom i's packed record (32-byte aligned) in one 256-bit load.  A plain
@@ -306,7 +309,7 @@ __device__ __forceinline__ void initial_atom(const AtomCols& c, uint64_t i, doub
     c.x[i] = x;
     c.y[i] = y;
     c.z[i] = z;
-    put_pk(c, i, x, y, z);
+    if (c.pk) put_pk(c.pk, i, x, y, z, c.pkrad[i]);
     if (zero_force) {  // zero_all_forces, atom.rs:631-635 (locals part)
         c.fx[i] = 0.0;
         c.fy[i] = 0.0;
@@ -389,11 +392,11 @@ __device__ __forceinline__ void forward_ghost(const AtomCols& c, uint64_t nlocal
     c.x[g] = px;
     c.y[g] = py;
     c.z[g] = pz;
-    put_pk(c, g, px, py, pz);
     c.vx[g] = vx;
     c.vy[g] = vy;
     c.vz[g] = vz;
     for (int q = 0; q < fwd.n; ++q) c.planes[fwd.idx[q]][g] = c.planes[fwd.idx[q]][r];
+    if (c.pk) put_pk(c.pk, g, px, py, pz, c.pkrad[g]);  // after the planes: g's own radius
     if (zero_force) {
         c.fx[g] = 0.0;
         c.fy[g] = 0.0;
@@ -429,11 +432,11 @@ __device__ __forceinline__ void forward_images(const AtomCols& c, uint64_t nloca
         c.x[g] = px;
         c.y[g] = py;
         c.z[g] = pz;
-        put_pk(c, g, px, py, pz);
         c.vx[g] = vx;
         c.vy[g] = vy;
         c.vz[g] = vz;
         for (int q = 0; q < fwd.n; ++q) c.planes[fwd.idx[q]][g] = c.planes[fwd.idx[q]][r];
+        if (c.pk) put_pk(c.pk, g, px, py, pz, c.pkrad[g]);  // after the planes: g's own radius
         if (zero_force) {
             c.fx[g] = 0.0;
             c.fy[g] = 0.0;

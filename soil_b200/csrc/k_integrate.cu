@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(kBlock) k_remap(uint64_t n, AtomCols c, RemapS
             double* x = r.dim[q] == 0 ? c.x : r.dim[q] == 1 ? c.y : c.z;
             x[i] = r.new_center[q] + (x[i] - r.old_center[q]) * r.scale[q];
         }
-        put_pk(c, i, c.x[i], c.y[i], c.z[i]);
+        if (c.pk) put_pk(c.pk, i, c.x[i], c.y[i], c.z[i], c.pkrad[i]);
     }
 }
 
@@ -311,9 +311,7 @@ __global__ void __launch_bounds__(kBlock) k_pack(uint64_t n, AtomCols c, const d
                                                  double* pk) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x) {
-        double2* r = reinterpret_cast<double2*>(pk + 4 * i);
-        r[0] = make_double2(c.x[i], c.y[i]);
-        r[1] = make_double2(c.z[i], rad[i]);
+        put_pk(pk, i, c.x[i], c.y[i], c.z[i], rad[i]);
     }
 }
 

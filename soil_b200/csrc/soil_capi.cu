@@ -310,11 +310,18 @@ int sync(soil_sys* s) {
     return SOIL_OK;
 }
 
+// Largest count the single-pass scan takes (SOIL_SCAN1P_MAX overrides, for
+// A/B runs; read at each call).
+uint64_t scan1p_max() {
+    const char* env = std::getenv("SOIL_SCAN1P_MAX");
+    return env ? std::strtoull(env, nullptr, 10) : kScan1pMaxCounts;
+}
+
 int scan_1p(soil_sys* s, const uint32_t* in, uint32_t* out, uint64_t n) {
     // Up to 64 tiles of 2,048 counts the single launch saves launch latency;
     // above it the three-kernel scan is faster (the look-back of a thousand
     // resident CTAs contends).
-    if (n > kScan1pMaxCounts) {
+    if (n > scan1p_max()) {
         TRY(ensure(s, s->scan_tmp, scan_temp_words(n + 2)));
         exclusive_scan_u32(s->st, in, out, n, s->scan_tmp.p);
         return SOIL_OK;
@@ -1131,7 +1138,10 @@ int pk_ready(soil_sys* s) {
     if (s->pk.p != old) s->pk_valid = false;
     if (reinterpret_cast<uintptr_t>(s->pk.p) % 32)
         return fail(s->ctx, SOIL_ERR_CUDA, "packed records: allocation not 32-byte aligned");
+    const int rp = s->cols[s->radius_col].plane0;
     s->A.pk = s->B.pk = s->pk.p;
+    s->A.pkrad = s->A.planes[rp];
+    s->B.pkrad = s->B.planes[rp];
     if (!s->pk_valid) {
         launch_pack(s->st, s->nlocal + s->nghost, s->A,
                     s->A.planes[s->cols[s->radius_col].plane0], s->pk.p);

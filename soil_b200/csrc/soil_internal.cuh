@@ -105,10 +105,11 @@ struct AtomCols {
     int nplanes;
     uint64_t cap;
     // Packed (x, y, z, r) records of the built-in consumer, 4 doubles per
-    // atom on a 32-byte boundary (null when unused).  The integration pass
-    // and forward comm write x, y, z next to the columns; r and the rebuild
-    // steps' positions come from a packing pass.
+    // atom on a 32-byte boundary (null when unused), r from the plane pkrad
+    // of this column set.  The integration pass and forward comm write whole
+    // records next to the columns; a packing pass fills them after rebuilds.
     double* pk;
+    const double* pkrad;
 };
 
 // Per-swap constants of the ghost maps (SwapData, comm.rs:114-124).
