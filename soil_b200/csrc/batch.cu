@@ -398,9 +398,11 @@ int fill_step(soil_batch* b, uint32_t k, bool post_flip, const BorderDim* bds) {
     const soil_sys* s = b->slot[k];
     BoxStep& t = b->h_step[k];
     const std::vector<int32_t>& sten = s->newton ? s->stencil_fwd : s->stencil;
-    if (sten.size() > (size_t)kMaxStencil)
-        return fail(s->ctx, SOIL_ERR_INVALID, "bin stencil of %zu cells exceeds the batched limit %d",
-                    sten.size(), kMaxStencil);
+    const std::vector<int32_t> runs = stencil_runs(sten, s->newton);
+    if (runs.size() > (size_t)kMaxStencil)
+        return fail(s->ctx, SOIL_ERR_INVALID,
+                    "bin stencil of %zu cell runs exceeds the batched limit %d", runs.size() / 2,
+                    kMaxStencil / 2);
     t.nlocal = s->nlocal;
     t.nghost = s->nghost;
     t.cur = set_index(b->h_dev[k], s);
@@ -410,9 +412,9 @@ int fill_step(soil_batch* b, uint32_t k, bool post_flip, const BorderDim* bds) {
     for (int d = 0; d < 3; ++d) t.bvel[d] = s->bvel[d];
     t.grid = grid_of(s);
     t.ncells = (uint32_t)s->total_cells;
-    t.nstencil = (int32_t)sten.size();
+    t.nstencil = (int32_t)(runs.size() / 2);
     std::memset(t.stencil, 0, sizeof t.stencil);
-    if (!sten.empty()) std::memcpy(t.stencil, sten.data(), sten.size() * 4);
+    if (!runs.empty()) std::memcpy(t.stencil, runs.data(), runs.size() * 4);
     t.has_self = s->stencil_self ? 1 : 0;
     t.newton = s->newton ? 1 : 0;
     t.uniform = s->has_uniform ? 1 : 0;
@@ -1099,10 +1101,12 @@ int soil_batch_add(soil_batch* b, soil_sys* s) {
     int zp[kMaxPlanes], nz;
     zero_planes_of(s, SOIL_COL_ZERO, zp, &nz);
     if (nz) return fail(b->ctx, SOIL_ERR_INVALID, "#[zero] columns are not supported in a batch");
-    const std::vector<int32_t>& sten = s->newton ? s->stencil_fwd : s->stencil;
-    if (sten.size() > (size_t)kMaxStencil)
-        return fail(b->ctx, SOIL_ERR_INVALID, "bin stencil of %zu cells exceeds the batched limit %d",
-                    sten.size(), kMaxStencil);
+    const std::vector<int32_t> runs =
+        stencil_runs(s->newton ? s->stencil_fwd : s->stencil, s->newton);
+    if (runs.size() > (size_t)kMaxStencil)
+        return fail(b->ctx, SOIL_ERR_INVALID,
+                    "bin stencil of %zu cell runs exceeds the batched limit %d", runs.size() / 2,
+                    kMaxStencil / 2);
     BCK(cudaStreamSynchronize(s->st));
     TRY(wait(b));
     uint32_t k = 0;

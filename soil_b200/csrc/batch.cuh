@@ -15,7 +15,7 @@
 
 namespace soil {
 
-constexpr int kMaxStencil = 96;  // forward/full stencil offsets per box
+constexpr int kMaxStencil = 96;  // stencil words per box: (offset, cells) runs
 
 // Pointers of one box's arrays; changes only when the box's arrays are
 // reallocated.  set[0]/set[1] are the two physical column sets; which one is

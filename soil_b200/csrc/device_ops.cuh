@@ -207,14 +207,19 @@ struct Filter {
 // Row of local atom i, sequentially in reference order: the own cell's
 // candidates (the tail after i's slot with newton, else the whole cell
 // without i), then every stencil cell in stencil order, each in sorted order.
-// The candidate ranges run as ONE loop (the lane moves to its next non-empty
-// range when one ends), so a warp pays for the longest candidate sequence of
-// its lanes rather than the per-cell maximum summed over the stencil.  FILL
-// writes the accepted indices to out[] (at most cap); returns the row length.
+// The stencil comes as runs of consecutive cells (p.stencil holds (offset,
+// cells) pairs, p.nstencil runs; stencil_runs on the host): the offsets
+// ascend, so a run's cells are one contiguous range of sorted slots and the
+// order is the cell-by-cell order.  The candidate ranges run as ONE loop (the
+// lane moves to its next non-empty range when one ends), so a warp pays for
+// the longest candidate sequence of its lanes rather than the per-cell
+// maximum summed over the stencil.  FILL writes the accepted indices to out[]
+// (at most cap); in_count (optional) counts every accepted index.  Returns
+// the row length.
 template <bool UNIFORM, bool FP32, bool FILL>
 __device__ uint32_t row_scan(const PairParams& p, const Filter<UNIFORM, FP32>& test, uint64_t i,
                              uint32_t* out, uint32_t cap, uint32_t* rechk, uint32_t* cand,
-                             DevFlags* flags) {
+                             DevFlags* flags, uint32_t* in_count = nullptr) {
     const uint32_t my_cell = p.atom_cell[i];
     const uint32_t mi = p.atom_sorted_idx[i];
     const double4 pi = p.sp[mi];
@@ -227,17 +232,16 @@ __device__ uint32_t row_scan(const PairParams& p, const Filter<UNIFORM, FP32>& t
         m = p.newton ? mi + 1 : p.bin_start[my_cell];
     }
     for (;;) {
-        while (m >= e) {  // open the next non-empty stencil cell
+        while (m >= e) {  // open the next non-empty run of stencil cells
             if (++s >= p.nstencil) return cnt;
-            const int32_t off = p.stencil[s];
-            if (!p.newton && off == 0) continue;  // the own cell was the first range
-            const uint32_t cc = (uint32_t)((int32_t)my_cell + off);
-            if (cc >= p.ncells) {  // the grid's ghost layers make this unreachable
+            const int64_t c0 = (int64_t)my_cell + p.stencil[2 * s];
+            const int64_t c1 = c0 + p.stencil[2 * s + 1];  // one past its last cell
+            if (c0 < 0 || c1 > (int64_t)p.ncells) {  // the grid's ghost layers make this unreachable
                 if (flags) atomicOr(&flags->error, 1u);
                 continue;
             }
-            m = p.bin_start[cc];
-            e = p.bin_start[cc + 1];
+            m = p.bin_start[c0];
+            e = p.bin_start[c1];
             *cand += e - m;
         }
         if (s < 0) {  // own cell: i itself is not a candidate
@@ -248,7 +252,13 @@ __device__ uint32_t row_scan(const PairParams& p, const Filter<UNIFORM, FP32>& t
             ++*cand;
         }
         if (test(p, pi, pif, m, rechk)) {
-            if (FILL && cnt < cap) out[cnt] = p.sorted_atoms[m];
+            if (in_count) {  // pass 1 of a build with the transposed lists
+                const uint32_t a = p.sorted_atoms[m];
+                atomicAdd(&in_count[a], 1u);
+                if (FILL && cnt < cap) out[cnt] = a;
+            } else if (FILL && cnt < cap) {
+                out[cnt] = p.sorted_atoms[m];
+            }
             ++cnt;
         }
         ++m;
@@ -536,8 +546,31 @@ __device__ __forceinline__ void sorted_view(const AtomCols& c, uint64_t m, const
     if (spf) spf[m] = make_float4((float)(x - o0), (float)(y - o1), (float)(z - o2), (float)cut);
 }
 
-// restore ascending order of one segment (the stable counting sort's last step)
+// restore ascending order of one segment (the stable counting sort's last step):
+// segments of up to 8 items (nearly all: bins and transposed lists hold a few
+// atoms) are loaded at once and sorted in registers by an odd-even
+// transposition network; longer ones by insertion in place.  The items of a
+// segment are distinct, so the order is unique.
 __device__ __forceinline__ void insertion_sort(uint32_t* items, uint32_t b, uint32_t e) {
+    const uint32_t n = e - b;
+    if (n < 2) return;
+    if (n <= 8) {
+        uint32_t v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = (uint32_t)k < n ? items[b + k] : 0xffffffffu;
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+#pragma unroll
+            for (int k = r & 1; k + 1 < 8; k += 2) {
+                const uint32_t lo = min(v[k], v[k + 1]), hi = max(v[k], v[k + 1]);
+                v[k] = lo;
+                v[k + 1] = hi;
+            }
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if ((uint32_t)k < n) items[b + k] = v[k];
+        return;
+    }
     for (uint32_t k = b + 1; k < e; ++k) {
         const uint32_t v = items[k];
         uint32_t j = k;

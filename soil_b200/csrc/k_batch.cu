@@ -371,6 +371,9 @@ __device__ __forceinline__ PairParams pair_params(const BoxDev& D, const BoxStep
     p.sf_sq = S.sf_sq;
     p.sf = S.sf;
     p.eps32 = S.eps32;
+    p.in_count = nullptr;
+    p.in_start = nullptr;
+    p.in_list = nullptr;
     return p;
 }
 

@@ -38,7 +38,7 @@ __global__ void __launch_bounds__(kBlock) k_pairs_rows(PairParams p, uint32_t* r
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < p.nlocal;
          i += (uint64_t)gridDim.x * blockDim.x)
         rowcount[i] = row_scan<UNIFORM, FP32, true>(p, test, i, slots + i * K, K, &n_rechk,
-                                                    &n_cand32, flags);
+                                                    &n_cand32, flags, p.in_count);
     uint64_t n_cand = n_cand32;
     uint64_t r = n_rechk;
     for (int o = 16; o > 0; o >>= 1) {
@@ -69,6 +69,11 @@ __global__ void __launch_bounds__(kBlock) k_pairs_fill(PairParams p, const uint3
             uint32_t rk = 0, cd = 0;
             row_scan<UNIFORM, FP32, true>(p, test, i, out, 0xffffffffu, &rk, &cd, nullptr);
         }
+        if (p.in_list)  // row i into each partner's transposed list (the counts go back to 0)
+            for (uint32_t k = 0; k < cnt; ++k) {
+                const uint32_t a = out[k];
+                p.in_list[p.in_start[a] + atomicSub(&p.in_count[a], 1u) - 1u] = (uint32_t)i;
+            }
     }
 }
 

@@ -266,8 +266,8 @@ struct PairParams {
     const uint32_t* sorted_atoms;
     const double4* sp;    // sorted {x, y, z, cutoff_radius}
     const float4* spf;    // FP32 grid-relative {x, y, z, cutoff_radius} (FP32 filter)
-    const int32_t* stencil;
-    int nstencil;
+    const int32_t* stencil;  // runs of consecutive stencil cells: (offset, cells) pairs
+    int nstencil;            // runs
     uint32_t ncells;      // bin_total_cells: stencil cells outside it are skipped and flagged
     uint64_t nlocal;
     int has_self;
@@ -279,6 +279,12 @@ struct PairParams {
     double sf_sq;         // skin_fraction^2
     double sf;            // skin_fraction
     float eps32;          // FP32 margin
+    // The transposed lists built with the pairs (NULL: not here): pass 1
+    // counts each row entry into in_count[partner]; pass 2 places row i in
+    // every partner's list at in_start[partner] + (its count, consumed).
+    uint32_t* in_count;
+    const uint32_t* in_start;
+    uint32_t* in_list;
 };
 // Pass 1: row lengths into rowcount[], the first K entries of each row into
 // slots[i*K ...]; filter statistics into flags.

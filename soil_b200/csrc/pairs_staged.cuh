@@ -118,7 +118,9 @@ __device__ uint32_t row_scan_staged(const PairParams& p, const PairSegs& sg,
             ok = test.test64(pi, *reinterpret_cast<const double4*>(rec));
         }
         if (ok) {
-            if (cnt < cap) out[cnt] = p.sorted_atoms[m];
+            const uint32_t a = p.sorted_atoms[m];
+            if (p.in_count) atomicAdd(&p.in_count[a], 1u);
+            if (cnt < cap) out[cnt] = a;
             ++cnt;
         }
         ++m;
@@ -201,7 +203,7 @@ __device__ bool staged_tile(const PairParams& p, const PairSegs& sg, uint64_t w,
                                                  slots + i * K, K, &n_rechk, &n_cand);
         else
             cnt = row_scan<UNIFORM, FP32, true>(p, test, i, slots + i * K, K, &n_rechk, &n_cand,
-                                                flags);
+                                                flags, p.in_count);
         rowcount[i] = cnt;
     }
     __syncwarp();  // every lane is done with the buffer and the ranges

@@ -335,6 +335,20 @@ int scan_1p(soil_sys* s, const uint32_t* in, uint32_t* out, uint64_t n) {
     return SOIL_OK;
 }
 
+std::vector<int32_t> stencil_runs(const std::vector<int32_t>& sten, bool newton) {
+    std::vector<int32_t> r;
+    for (const int32_t off : sten) {
+        if (!newton && off == 0) continue;
+        if (!r.empty() && r[r.size() - 2] + r.back() == off) {
+            r.back() += 1;
+            continue;
+        }
+        r.push_back(off);
+        r.push_back(1);
+    }
+    return r;
+}
+
 int counts_zero(soil_sys* s, uint64_t nc) {
     if (s->counts_at != s->cell_counts.p || s->counts_clean < nc)
         CK(cudaMemsetAsync(s->cell_counts.p, 0, s->cell_counts.cap * 4, s->st));
@@ -1117,10 +1131,12 @@ int build_seq(soil_sys* s) {
 bool seq_consumer(const soil_sys* s) { return builtin_consumer(s) && s->few_images; }
 
 // Whether the one-thread-per-root consumer kernels read the packed records
-// (SOIL_PACKED=0: the columns; read at each call, for A/B runs).
+// (SOIL_PACKED=1; read at each call).  Off by default: on 4M atoms the
+// records' 40 B per atom and step in the integration pass cost more than
+// the walks gain from one 32-byte load per partner.
 bool packed_on() {
     const char* env = std::getenv("SOIL_PACKED");
-    return !(env && std::atoi(env) == 0);
+    return env && std::atoi(env) == 1;
 }
 
 // The packed records, current for every local and ghost: allocated with the
@@ -1360,12 +1376,13 @@ int phase_neighbor(soil_sys* s) {
     launch_sorted_views(s->st, total, s->sorted_atoms.p, s->A, s->asi.p, s->sp.p,
                         fp32 ? s->spf.p : nullptr, s->blo);
     const std::vector<int32_t>& sten = s->newton ? s->stencil_fwd : s->stencil;
+    const std::vector<int32_t> runs = stencil_runs(sten, s->newton);
     const int32_t* old_stencil = s->d_stencil.p;
-    TRY(ensure(s, s->d_stencil, sten.size() + 1));
-    if (!sten.empty() && (s->d_stencil.p != old_stencil || sten != s->stencil_on_device)) {
+    TRY(ensure(s, s->d_stencil, runs.size() + 1));
+    if (!runs.empty() && (s->d_stencil.p != old_stencil || runs != s->stencil_on_device)) {
         // pageable source: the copy completes before cudaMemcpyAsync returns
-        CK(cudaMemcpyAsync(s->d_stencil.p, sten.data(), sten.size() * 4, cudaMemcpyHostToDevice, s->st));
-        s->stencil_on_device = sten;
+        CK(cudaMemcpyAsync(s->d_stencil.p, runs.data(), runs.size() * 4, cudaMemcpyHostToDevice, s->st));
+        s->stencil_on_device = runs;
     }
     PairParams p;
     p.atom_cell = s->atom_cell.p;
@@ -1375,7 +1392,7 @@ int phase_neighbor(soil_sys* s) {
     p.sp = s->sp.p;
     p.spf = s->spf.p;
     p.stencil = s->d_stencil.p;
-    p.nstencil = (int)sten.size();
+    p.nstencil = (int)(runs.size() / 2);
     p.ncells = (uint32_t)nc;
     p.nlocal = nl;
     p.row_slots = kRowSlots;
@@ -1390,12 +1407,30 @@ int phase_neighbor(soil_sys* s) {
     // candidates, rechecked and error are adjacent: one clear
     static_assert(offsetof(DevFlags, error) == offsetof(DevFlags, candidates) + 16, "DevFlags layout");
     CK(cudaMemsetAsync(&s->dflags->candidates, 0, 20, s->st));
+    s->in_lists_valid = false;
+    s->seq_valid = false;
+    s->order_valid = false;
+    // The transposed lists serve the built-in consumer and any force hook:
+    // the pair passes build them too (pass 1 counts each partner's entries,
+    // pass 2 places every row in its partners' lists), then a per-atom sort
+    // restores ascending order.
+    const bool with_in = builtin_consumer(s) || s->hook;
+    p.in_count = nullptr;
+    p.in_start = nullptr;
+    p.in_list = nullptr;
+    if (with_in) {
+        TRY(ensure(s, s->in_count, total + 1, 0, s->acap + 1));
+        TRY(ensure(s, s->in_start, total + 2, 0, s->acap + 2));
+        CK(cudaMemsetAsync(s->in_count.p, 0, total * 4, s->st));
+        p.in_count = s->in_count.p;
+    }
     PairSegs sg;
     if (pair_segments(sten, s->stencil_self, s->newton, &sg))
         launch_pair_count_staged(s->st, p, sg, s->rowcount.p, s->row_slots.p, s->dflags);
     else
         launch_pair_count(s->st, p, s->rowcount.p, s->row_slots.p, s->dflags);
     TRY(scan_1p(s, s->rowcount.p, s->offsets.p, nl));
+    if (with_in) TRY(scan_1p(s, s->in_count.p, s->in_start.p, total));
     CK(cudaMemcpyAsync(&s->hword[0], s->offsets.p + nl, 4, cudaMemcpyDeviceToHost, s->st));
     TRY(check_launch(s));
     TRY(read_flags(s));
@@ -1405,15 +1440,23 @@ int phase_neighbor(soil_sys* s) {
         return fail(s->ctx, SOIL_ERR_CUDA, "pair build: a shared-memory staging wait ran out");
     if (s->hflags->error)
         return fail(s->ctx, SOIL_ERR_INVALID, "neighbor stencil left the bin grid (atom outside the ghost layers)");
+    if (with_in) {
+        TRY(ensure(s, s->in_list, np + 1, 0, pair_room(np)));
+        p.in_start = s->in_start.p;
+        p.in_list = s->in_list.p;
+    }
     launch_pair_fill(s->st, p, s->rowcount.p, s->row_slots.p, s->offsets.p, s->indices.p);
+    if (with_in) {
+        TRY(ensure(s, s->in_split, total + 1, 0, s->acap + 1));
+        launch_segsort_split(s->st, total, s->in_start.p, s->in_list.p, s->in_split.p);
+    }
     TRY(check_launch(s));
     s->npairs = np;
     s->rebuilds += 1;
-    s->in_lists_valid = false;
-    s->seq_valid = false;
-    s->order_valid = false;
-    // the transposed lists serve the built-in consumer and any force hook
-    if (builtin_consumer(s) || s->hook) TRY(build_in_lists(s));
+    if (with_in) {
+        s->in_lists_valid = true;
+        s->split_valid = true;
+    }
     // the grouped sequences are built when a consumer kernel first needs them
     return SOIL_OK;
 }

@@ -263,6 +263,10 @@ int sync(soil_sys* s);
 int check_launch(soil_sys* s);
 // cell_counts[0, nc) zero before a counting pass
 int counts_zero(soil_sys* s, uint64_t nc);
+// The pair scan's stencil: offsets (ascending) merged into runs of consecutive
+// cells, as (offset, cells) pairs; without newton the own cell (offset 0),
+// which the scan takes first, is left out.
+std::vector<int32_t> stencil_runs(const std::vector<int32_t>& sten, bool newton);
 // exclusive scan of in[0, n) into out[0, n] in one launch, errors into the
 // system's device flags
 int scan_1p(soil_sys* s, const uint32_t* in, uint32_t* out, uint64_t n);
