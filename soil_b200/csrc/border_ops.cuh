@@ -41,8 +41,11 @@ __device__ __forceinline__ void border_warp_counts(const AtomCols& c, uint64_t n
         face[r] = (uint8_t)bits;
     }
     uint32_t mine = 0, images = 0;
-    if (__ballot_sync(0xffffffffu, bits != 0u)) {
+    // a category can have members only if the tile's faces cover its need
+    const uint32_t any = __reduce_or_sync(0xffffffffu, bits);
+    if (any) {
         for (int k = 0; k < kBorderCats; ++k) {
+            if ((any & cats.need[k]) != cats.need[k]) continue;  // uniform over the warp
             const uint32_t n = __popc(__ballot_sync(0xffffffffu, cat_member(cats, bits, k)));
             if (lane == (uint32_t)k) mine = n;
             images += n;
@@ -88,7 +91,8 @@ __device__ __forceinline__ void border_warp_images(
     const uint64_t r = w * 32 + lane;
     const uint32_t bits = r < nlocal ? face[r] : 0u;
     const uint64_t cw = w / kScanChunk;
-    if (!__ballot_sync(0xffffffffu, bits != 0u)) {  // no images: empty fold programs
+    const uint32_t any = __reduce_or_sync(0xffffffffu, bits);
+    if (!any) {  // no images: empty fold programs
         const uint32_t fold0 =
             offs[kBorderCats * nw + w] + (cpre ? cpre[kBorderCats * nchunks + cw] : 0u);
         if (r < nlocal) fold_start[r] = fold0;
@@ -107,6 +111,10 @@ __device__ __forceinline__ void border_warp_images(
     uint32_t idx[kBorderCats];
     uint32_t own = 0;  // images of this lane's root
     for (int k = 0; k < kBorderCats; ++k) {
+        idx[k] = 0u;
+        // no member in the tile unless its faces cover the need (uniform
+        // over the warp); members' parents are members, so idx is complete
+        if ((any & cats.need[k]) != cats.need[k]) continue;
         const bool m = cat_member(cats, bits, k);
         const unsigned bal = __ballot_sync(0xffffffffu, m);
         const uint32_t base = __shfl_sync(0xffffffffu, base_lane + off_lane, k);

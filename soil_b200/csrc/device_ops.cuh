@@ -152,6 +152,16 @@ __device__ __forceinline__ void write_image(const AtomCols& c, const double (*sh
     chain[g - nlocal] = code;
 }
 
+// A sorted record {x, y, z, cutoff} in one 256-bit load through the
+// read-only path (the records are written by an earlier launch).
+__device__ __forceinline__ double4 ld_rec(const double4* p) {
+    double4 v;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+        : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w)
+        : "l"(p));
+    return v;
+}
+
 template <bool UNIFORM, bool FP32>
 struct Filter {
     double cut_sq, sf_sq;
@@ -200,7 +210,7 @@ struct Filter {
             if (!pass32(pif, p.spf[m])) return false;
             ++*rechk;
         }
-        return test64(pi, p.sp[m]);
+        return test64(pi, ld_rec(p.sp + m));
     }
 };
 
@@ -216,13 +226,13 @@ struct Filter {
 // maximum summed over the stencil.  FILL writes the accepted indices to out[]
 // (at most cap); in_count (optional) counts every accepted index.  Returns
 // the row length.
-template <bool UNIFORM, bool FP32, bool FILL>
+template <bool UNIFORM, bool FP32, bool FILL, bool PF = true>
 __device__ uint32_t row_scan(const PairParams& p, const Filter<UNIFORM, FP32>& test, uint64_t i,
                              uint32_t* out, uint32_t cap, uint32_t* rechk, uint32_t* cand,
                              DevFlags* flags, uint32_t* in_count = nullptr) {
     const uint32_t my_cell = p.atom_cell[i];
     const uint32_t mi = p.atom_sorted_idx[i];
-    const double4 pi = p.sp[mi];
+    const double4 pi = ld_rec(p.sp + mi);
     const float4 pif = FP32 ? p.spf[mi] : make_float4(0.f, 0.f, 0.f, 0.f);
     uint32_t cnt = 0;
     int s = -1;  // -1: the own cell; s >= 0: stencil cell s
@@ -231,6 +241,10 @@ __device__ uint32_t row_scan(const PairParams& p, const Filter<UNIFORM, FP32>& t
         e = p.bin_start[my_cell + 1];
         m = p.newton ? mi + 1 : p.bin_start[my_cell];
     }
+    // FP64 filter with PF: the record of the range's next slot is loaded
+    // while the current one is tested (nm: the slot whose record nx holds)
+    double4 nx = make_double4(0.0, 0.0, 0.0, 0.0);
+    uint32_t nm = 0xffffffffu;
     for (;;) {
         while (m >= e) {  // open the next non-empty run of stencil cells
             if (++s >= p.nstencil) return cnt;
@@ -251,7 +265,18 @@ __device__ uint32_t row_scan(const PairParams& p, const Filter<UNIFORM, FP32>& t
             }
             ++*cand;
         }
-        if (test(p, pi, pif, m, rechk)) {
+        bool ok;
+        if (FP32 || !PF) {
+            ok = test(p, pi, pif, m, rechk);
+        } else {
+            const double4 q = nm == m ? nx : ld_rec(p.sp + m);
+            if (m + 1 < e) {
+                nx = ld_rec(p.sp + m + 1);
+                nm = m + 1;
+            }
+            ok = test.test64(pi, q);
+        }
+        if (ok) {
             if (in_count) {  // pass 1 of a build with the transposed lists
                 const uint32_t a = p.sorted_atoms[m];
                 atomicAdd(&in_count[a], 1u);
@@ -583,8 +608,10 @@ __device__ __forceinline__ void insertion_sort(uint32_t* items, uint32_t b, uint
 }
 
 // one atom of the spatial sort's permutation gather (atom.rs:479-490)
+// (forces: false when this step's consumer overwrites every force before
+// anything reads one, so the old values need not move)
 __device__ __forceinline__ void perm_gather_atom(const AtomCols& s, const AtomCols& d, uint64_t k,
-                                                 uint32_t p) {
+                                                 uint32_t p, bool forces = true) {
     const uint64_t cap = s.cap, dcap = d.cap;
     d.x[k] = s.x[p];
     d.y[k] = s.y[p];
@@ -592,9 +619,11 @@ __device__ __forceinline__ void perm_gather_atom(const AtomCols& s, const AtomCo
     d.vx[k] = s.vx[p];
     d.vy[k] = s.vy[p];
     d.vz[k] = s.vz[p];
-    d.fx[k] = s.fx[p];
-    d.fy[k] = s.fy[p];
-    d.fz[k] = s.fz[p];
+    if (forces) {
+        d.fx[k] = s.fx[p];
+        d.fy[k] = s.fy[p];
+        d.fz[k] = s.fz[p];
+    }
     d.mass[k] = s.mass[p];
     d.inv_mass[k] = s.inv_mass[p];
     d.cut[k] = s.cut[p];

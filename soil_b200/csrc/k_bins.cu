@@ -190,17 +190,17 @@ void launch_in_split(cudaStream_t st, uint64_t nseg, const uint32_t* start, cons
 // Atom::apply_permutation + AtomDataRegistry::apply_permutation_all
 // (atom.rs:479-490, 284-289): every column gathered through perm.
 __global__ void __launch_bounds__(kBlock) k_perm_gather(uint64_t n, const uint32_t* perm,
-                                                        AtomCols s, AtomCols d) {
+                                                        AtomCols s, AtomCols d, int forces) {
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n;
          k += (uint64_t)gridDim.x * blockDim.x)
-        perm_gather_atom(s, d, k, perm[k]);
+        perm_gather_atom(s, d, k, perm[k], forces != 0);
 }
 
 void launch_perm_gather(cudaStream_t st, uint64_t n, const uint32_t* perm, const AtomCols& src,
-                        const AtomCols& dst) {
+                        const AtomCols& dst, bool forces) {
     if (n == 0) return;
     note_launch();
-    k_perm_gather<<<grid_for(n), kBlock, 0, st>>>(n, perm, src, dst);
+    k_perm_gather<<<grid_for(n), kBlock, 0, st>>>(n, perm, src, dst, forces ? 1 : 0);
 }
 
 __global__ void __launch_bounds__(kBlock) k_identity(uint64_t n, const uint32_t* perm,

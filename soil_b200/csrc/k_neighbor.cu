@@ -21,6 +21,8 @@
 // only REJECTS candidates provably outside the cutoff — the margin eps bounds
 // the float rounding of coordinates, differences and squares — followed by
 // the exact FP64 test on the rest, so the lists are identical in both modes.
+#include <cstdlib>
+
 #include "device_ops.cuh"
 #include "kernels.cuh"
 
@@ -29,7 +31,7 @@ namespace soil {
 // Pass 1: one thread per local row (rows of a warp are neighbours in space, so
 // their candidate records are shared through L1); the first K entries go to
 // the row's slots, the length to rowcount.
-template <bool UNIFORM, bool FP32>
+template <bool UNIFORM, bool FP32, bool PF>
 __global__ void __launch_bounds__(kBlock) k_pairs_rows(PairParams p, uint32_t* rowcount,
                                                        uint32_t* slots, DevFlags* flags) {
     const Filter<UNIFORM, FP32> test(p);
@@ -37,8 +39,8 @@ __global__ void __launch_bounds__(kBlock) k_pairs_rows(PairParams p, uint32_t* r
     uint32_t n_rechk = 0, n_cand32 = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < p.nlocal;
          i += (uint64_t)gridDim.x * blockDim.x)
-        rowcount[i] = row_scan<UNIFORM, FP32, true>(p, test, i, slots + i * K, K, &n_rechk,
-                                                    &n_cand32, flags, p.in_count);
+        rowcount[i] = row_scan<UNIFORM, FP32, true, PF>(p, test, i, slots + i * K, K, &n_rechk,
+                                                        &n_cand32, flags, p.in_count);
     uint64_t n_cand = n_cand32;
     uint64_t r = n_rechk;
     for (int o = 16; o > 0; o >>= 1) {
@@ -82,9 +84,15 @@ static void launch_pairs_t(cudaStream_t st, const PairParams& p, uint32_t* rowco
                            uint32_t* slots, const uint32_t* offsets, uint32_t* indices,
                            DevFlags* flags, bool fill) {
     note_launch();
-    if (!fill)
-        k_pairs_rows<UNIFORM, FP32><<<grid_for(p.nlocal), kBlock, 0, st>>>(p, rowcount, slots,
-                                                                            flags);
+    // SOIL_PAIRS_PREFETCH=0: the pass-1 scan without the record prefetch
+    const char* env = std::getenv("SOIL_PAIRS_PREFETCH");
+    const bool pf = !(env && std::atoi(env) == 0);
+    if (!fill && pf)
+        k_pairs_rows<UNIFORM, FP32, true><<<grid_for(p.nlocal), kBlock, 0, st>>>(p, rowcount, slots,
+                                                                                  flags);
+    else if (!fill)
+        k_pairs_rows<UNIFORM, FP32, false><<<grid_for(p.nlocal), kBlock, 0, st>>>(p, rowcount,
+                                                                                   slots, flags);
     else
         k_pairs_fill<UNIFORM, FP32><<<grid_for(p.nlocal), kBlock, 0, st>>>(p, rowcount, slots,
                                                                             offsets, indices);

@@ -14,14 +14,49 @@ namespace soil {
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kBlock * kScanItems;
 
+// A thread's 8 consecutive items [base, base + 8) (zero past n): two 16-byte
+// loads when the group is whole and aligned, else one by one.
+__device__ __forceinline__ void load8(const uint32_t* in, uint64_t base, uint64_t n,
+                                      uint32_t (&v)[kScanItems]) {
+    if (base + kScanItems <= n && (reinterpret_cast<uintptr_t>(in + base) & 15u) == 0) {
+        const uint4 a = *reinterpret_cast<const uint4*>(in + base);
+        const uint4 b = *reinterpret_cast<const uint4*>(in + base + 4);
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+        v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) v[k] = (base + k < n) ? in[base + k] : 0u;
+}
+
+// out[base + k] = pre + v[0] + ... + v[k - 1] for the items below n.
+__device__ __forceinline__ void store8_scan(uint32_t* out, uint64_t base, uint64_t n,
+                                            const uint32_t (&v)[kScanItems], uint32_t pre) {
+    uint32_t o[kScanItems];
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        o[k] = pre;
+        pre += v[k];
+    }
+    if (base + kScanItems <= n && (reinterpret_cast<uintptr_t>(out + base) & 15u) == 0) {
+        *reinterpret_cast<uint4*>(out + base) = make_uint4(o[0], o[1], o[2], o[3]);
+        *reinterpret_cast<uint4*>(out + base + 4) = make_uint4(o[4], o[5], o[6], o[7]);
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k)
+        if (base + k < n) out[base + k] = o[k];
+}
+
 __global__ void __launch_bounds__(kBlock) k_scan_reduce(const uint32_t* in, uint64_t n,
                                                         uint32_t* partial) {
     __shared__ uint32_t tot;
     const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    load8(in, base, n, v);
     uint32_t s = 0;
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k)
-        if (base + k < n) s += in[base + k];
+    for (int k = 0; k < kScanItems; ++k) s += v[k];
     block_exclusive_scan(s, &tot);
     if (threadIdx.x == 0) partial[blockIdx.x] = tot;
 }
@@ -56,18 +91,12 @@ __global__ void __launch_bounds__(kBlock) k_scan_down(const uint32_t* in, uint32
     __shared__ uint32_t tot;
     const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
+    load8(in, base, n, v);
     uint32_t s = 0;
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        v[k] = (base + k < n) ? in[base + k] : 0;
-        s += v[k];
-    }
-    uint32_t pre = block_exclusive_scan(s, &tot) + partial[blockIdx.x];
-#pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        if (base + k < n) out[base + k] = pre;
-        pre += v[k];
-    }
+    for (int k = 0; k < kScanItems; ++k) s += v[k];
+    const uint32_t pre = block_exclusive_scan(s, &tot) + partial[blockIdx.x];
+    store8_scan(out, base, n, v, pre);
     if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = partial[ntiles];
 }
 
@@ -119,12 +148,10 @@ __global__ void __launch_bounds__(kBlock) k_scan_1p(const uint32_t* in, uint32_t
     if (threadIdx.x == 0 && tile == ntiles - 1) atomicExch(counter, 0u);  // the last claim
     const uint64_t base = (uint64_t)tile * kScanTile + (uint64_t)threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
+    load8(in, base, n, v);
     uint32_t s = 0;
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        v[k] = (base + k < n) ? in[base + k] : 0;
-        s += v[k];
-    }
+    for (int k = 0; k < kScanItems; ++k) s += v[k];
     uint32_t pre = block_exclusive_scan(s, &tot);
     const uint32_t agg = tot;
     const uint32_t ep = epoch & 0x3fffffffu;
@@ -176,12 +203,13 @@ __global__ void __launch_bounds__(kBlock) k_scan_1p(const uint32_t* in, uint32_t
     }
     __syncthreads();
     pre += s_prefix;
+    store8_scan(out, base, n, v, pre);
+    if (tile == ntiles - 1 && threadIdx.x == kBlock - 1) {
+        uint32_t last = pre;
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        if (base + k < n) out[base + k] = pre;
-        pre += v[k];
+        for (int k = 0; k < kScanItems; ++k) last += v[k];
+        out[n] = last;
     }
-    if (tile == ntiles - 1 && threadIdx.x == kBlock - 1) out[n] = pre;
 }
 
 uint64_t scan1p_words(uint64_t n) { return 2 * ((n + kScanTile - 1) / kScanTile) + 4; }

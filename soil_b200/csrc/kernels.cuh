@@ -162,7 +162,7 @@ void launch_in_split(cudaStream_t st, uint64_t nseg, const uint32_t* start, cons
                      uint32_t* split);
 // dst[k] = src[perm[k]] for every column, k in [0, n)
 void launch_perm_gather(cudaStream_t st, uint64_t n, const uint32_t* perm, const AtomCols& src,
-                        const AtomCols& dst);
+                        const AtomCols& dst, bool forces = true);
 // flags->not_identity |= any perm[k] != k
 void launch_identity_check(cudaStream_t st, uint64_t n, const uint32_t* perm, DevFlags* flags);
 // out[k] = cell[perm[k]]

@@ -883,7 +883,7 @@ int phase_sort(soil_sys* s) {
     if (apply) {
         // every column gathered through perm; ghosts (if any) are discarded by
         // the borders that always follows a permutation
-        launch_perm_gather(s->st, nl, s->sort_perm.p, s->A, s->B);
+        launch_perm_gather(s->st, nl, s->sort_perm.p, s->A, s->B, !s->forces_dead);
         if (s->slot_max) {  // slots move with their atoms
             const int o = s->slot_old;
             launch_slot_gather(s->st, nl, s->sort_perm.p, s->slot_max, s->slot_width,
@@ -1652,7 +1652,10 @@ int step_rest(soil_sys* s, const StepPlan& p, bool last) {
     TRY(phase_pbc(s));
     timer_end(s, T_PBC);
     timer_begin(s, T_SORT);
-    TRY(phase_sort(s));
+    s->forces_dead = p.overwrite;  // the built-in consumer rewrites every force below
+    const int sorted = phase_sort(s);
+    s->forces_dead = false;
+    TRY(sorted);
     timer_end(s, T_SORT);
     timer_begin(s, T_BORDERS);
     TRY(phase_borders(s));

@@ -148,6 +148,7 @@ struct soil_sys {
     DArr<double> pk;
     bool pk_valid = false;
     bool view_out = false;  // a device view was handed out since the last rebuild
+    bool forces_dead = false;  // inside a step whose consumer overwrites every force
     // grouped partner sequences of the built-in consumer (rebuilt with the
     // lists): per-atom lengths, per-root group lengths and starts, entries
     DArr<uint32_t> seq_cnt, grp_cnt, grp_start, seq;
