@@ -77,16 +77,24 @@ __device__ __forceinline__ void border_state_words(const BorderCats& cats, uint6
 // chunk); chunk prefixes (cpre[k * nchunks + chunk]) are added back here.
 constexpr uint64_t kScanChunk = 8192;
 
+// Shared-memory scratch of one warp in pass 2: every lane's ghost index per
+// category (indexed by category, so it must not live in registers) and the
+// first ghost index of each swap.
+struct BorderWarpSmem {
+    uint32_t idx[kBorderCats][32];
+    uint32_t recv[kNumSwaps];
+};
+
 // Pass 2 for warp tile w.  base_lane: on lane k < 26 the first ghost index of
 // category k (nlocal + the totals of the categories before it).  offs holds
 // offsets inside the tile's scan chunk; cpre (NULL: a single chunk) the
-// chunks' prefixes.
+// chunks' prefixes.  sm: this warp's scratch.
 __device__ __forceinline__ void border_warp_images(
     const AtomCols& c, uint64_t nlocal, uint64_t cap, const double (*shift)[3],
     const double (*vshift)[3], const BorderCats& cats, const uint8_t* face, const uint32_t* offs,
     const uint32_t* cpre, uint64_t nchunks, uint64_t nw, uint64_t w, uint32_t lane,
     uint32_t base_lane, uint32_t* bs, uint32_t* root, uint32_t* chain, uint32_t* const* send,
-    uint32_t* fold_start, uint32_t* fold_list) {
+    uint32_t* fold_start, uint32_t* fold_list, BorderWarpSmem& sm) {
     const unsigned below = (1u << lane) - 1u;
     const uint64_t r = w * 32 + lane;
     const uint32_t bits = r < nlocal ? face[r] : 0u;
@@ -105,45 +113,49 @@ __device__ __forceinline__ void border_warp_images(
             ? offs[lane * nw + w] + (cpre ? cpre[lane * nchunks + cw] : 0u)
             : 0u;
     const uint32_t fold0 = __shfl_sync(0xffffffffu, off_lane, kBorderCats);
-    uint32_t recv[kNumSwaps];
-    for (int s = 0; s < kNumSwaps; ++s)
-        recv[s] = __shfl_sync(0xffffffffu, base_lane, cats.swap_first[s]);
-    uint32_t idx[kBorderCats];
+    const uint32_t rv =
+        __shfl_sync(0xffffffffu, base_lane, lane < (uint32_t)kNumSwaps ? cats.swap_first[lane] : 0);
+    if (lane < (uint32_t)kNumSwaps) sm.recv[lane] = rv;
     uint32_t own = 0;  // images of this lane's root
     for (int k = 0; k < kBorderCats; ++k) {
-        idx[k] = 0u;
         // no member in the tile unless its faces cover the need (uniform
-        // over the warp); members' parents are members, so idx is complete
+        // over the warp); only members read idx, and a member's parent
+        // category has it as a member too
         if ((any & cats.need[k]) != cats.need[k]) continue;
         const bool m = cat_member(cats, bits, k);
         const unsigned bal = __ballot_sync(0xffffffffu, m);
         const uint32_t base = __shfl_sync(0xffffffffu, base_lane + off_lane, k);
-        idx[k] = base + __popc(bal & below);
+        sm.idx[k][lane] = base + __popc(bal & below);
         own += m;
     }
+    __syncwarp();
     const uint32_t fs = fold0 + warp_exclusive_sum(own, lane);
     if (r < nlocal) fold_start[r] = fs;
     if (r + 1 == nlocal) fold_start[nlocal] = fs + own;
-    if (!bits) return;
-    for (int k = 0; k < kBorderCats; ++k) {
-        if (!cat_member(cats, bits, k)) continue;
-        const uint32_t g = idx[k];
-        if (g >= cap) {
-            bs[10] = 1u;  // out of capacity: the host grows the arrays and repeats
-            continue;
+    if (bits) {
+        for (int k = 0; k < kBorderCats; ++k) {
+            if (!cat_member(cats, bits, k)) continue;
+            const uint32_t g = sm.idx[k][lane];
+            if (g >= cap) {
+                bs[10] = 1u;  // out of capacity: the host grows the arrays and repeats
+                continue;
+            }
+            const uint32_t parent =
+                cats.parent[k] < 0 ? (uint32_t)r : sm.idx[cats.parent[k]][lane];
+            write_image(c, shift, vshift, cats, k, g, r, parent, nlocal, root, chain);
+            const int s = cats.swap_of[k];
+            send[s][g - sm.recv[s]] = parent;
         }
-        const uint32_t parent = cats.parent[k] < 0 ? (uint32_t)r : idx[cats.parent[k]];
-        write_image(c, shift, vshift, cats, k, g, r, parent, nlocal, root, chain);
-        const int s = cats.swap_of[k];
-        send[s][g - recv[s]] = parent;
+        uint32_t j = fs;
+        for (int f = 0; f < kBorderCats; ++f) {
+            const int k = cats.fold[f];
+            if (!cat_member(cats, bits, k)) continue;
+            const uint32_t g = sm.idx[k][lane];
+            if (g < cap && j < cap) fold_list[j] = g - (uint32_t)nlocal;
+            ++j;
+        }
     }
-    uint32_t j = fs;
-    for (int f = 0; f < kBorderCats; ++f) {
-        const int k = cats.fold[f];
-        if (!cat_member(cats, bits, k)) continue;
-        if (idx[k] < cap && j < cap) fold_list[j] = idx[k] - (uint32_t)nlocal;
-        ++j;
-    }
+    __syncwarp();  // every lane is done with the scratch before the warp's next tile
 }
 
 }  // namespace soil

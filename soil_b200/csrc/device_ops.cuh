@@ -226,7 +226,7 @@ struct Filter {
 // maximum summed over the stencil.  FILL writes the accepted indices to out[]
 // (at most cap); in_count (optional) counts every accepted index.  Returns
 // the row length.
-template <bool UNIFORM, bool FP32, bool FILL, bool PF = true>
+template <bool UNIFORM, bool FP32, bool FILL>
 __device__ uint32_t row_scan(const PairParams& p, const Filter<UNIFORM, FP32>& test, uint64_t i,
                              uint32_t* out, uint32_t cap, uint32_t* rechk, uint32_t* cand,
                              DevFlags* flags, uint32_t* in_count = nullptr) {
@@ -241,10 +241,6 @@ __device__ uint32_t row_scan(const PairParams& p, const Filter<UNIFORM, FP32>& t
         e = p.bin_start[my_cell + 1];
         m = p.newton ? mi + 1 : p.bin_start[my_cell];
     }
-    // FP64 filter with PF: the record of the range's next slot is loaded
-    // while the current one is tested (nm: the slot whose record nx holds)
-    double4 nx = make_double4(0.0, 0.0, 0.0, 0.0);
-    uint32_t nm = 0xffffffffu;
     for (;;) {
         while (m >= e) {  // open the next non-empty run of stencil cells
             if (++s >= p.nstencil) return cnt;
@@ -265,18 +261,7 @@ __device__ uint32_t row_scan(const PairParams& p, const Filter<UNIFORM, FP32>& t
             }
             ++*cand;
         }
-        bool ok;
-        if (FP32 || !PF) {
-            ok = test(p, pi, pif, m, rechk);
-        } else {
-            const double4 q = nm == m ? nx : ld_rec(p.sp + m);
-            if (m + 1 < e) {
-                nx = ld_rec(p.sp + m + 1);
-                nm = m + 1;
-            }
-            ok = test.test64(pi, q);
-        }
-        if (ok) {
+        if (test(p, pi, pif, m, rechk)) {
             if (in_count) {  // pass 1 of a build with the transposed lists
                 const uint32_t a = p.sorted_atoms[m];
                 atomicAdd(&in_count[a], 1u);

@@ -310,6 +310,7 @@ void b_border_cat_scan(cudaStream_t st, const Span& sp, const BatchArgs& a) {
 }
 
 __global__ void __launch_bounds__(kBlock) kb_border_images(Span sp, BatchArgs A, BorderCats cats) {
+    __shared__ BorderWarpSmem sm[kBlock / 32];
     const uint32_t lane = threadIdx.x & 31u;
     for_warp_tiles(sp, [&](uint32_t b, uint64_t w, uint32_t k) {
         const BoxDev& D = A.dev[b];
@@ -321,7 +322,7 @@ __global__ void __launch_bounds__(kBlock) kb_border_images(Span sp, BatchArgs A,
         const uint32_t base_lane = (uint32_t)S.nlocal + warp_exclusive_sum(tot, lane);
         border_warp_images(D.set[S.post], S.nlocal, D.cap, S.sc.off, S.sc.voff, cats, D.face_flags,
                            D.boff, nullptr, 1, nw, w, lane, base_lane, bs, D.ghost_root,
-                           D.ghost_chain, D.send, D.fold_start, D.fold_list);
+                           D.ghost_chain, D.send, D.fold_start, D.fold_list, sm[threadIdx.x / 32]);
     });
 }
 void b_border_images(cudaStream_t st, const Span& sp, const BatchArgs& a) {

@@ -168,6 +168,7 @@ __global__ void __launch_bounds__(kBlock) k_border_images(
     uint64_t nlocal, uint64_t cap, AtomCols c, BorderPass bp, BorderCats cats, const uint8_t* face,
     const uint32_t* offs, const uint32_t* cpre, uint64_t nchunks, uint64_t nw, uint32_t* bs,
     uint32_t* root, uint32_t* chain, SendPtrs send, uint32_t* fold_start, uint32_t* fold_list) {
+    __shared__ BorderWarpSmem sm[kBlock / 32];
     const uint32_t lane = threadIdx.x & 31u;
     if (blockIdx.x == 0 && threadIdx.x == 0) border_state_words(cats, nlocal, bs);
     // first ghost index of category `lane` (lanes below 26)
@@ -176,7 +177,8 @@ __global__ void __launch_bounds__(kBlock) k_border_images(
     const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x / 32);
     for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32; w < nw; w += nwarps)
         border_warp_images(c, nlocal, cap, bp.shift, bp.vshift, cats, face, offs, cpre, nchunks,
-                           nw, w, lane, base_lane, bs, root, chain, send.p, fold_start, fold_list);
+                           nw, w, lane, base_lane, bs, root, chain, send.p, fold_start, fold_list,
+                           sm[threadIdx.x / 32]);
 }
 
 void launch_borders(cudaStream_t st, uint64_t nlocal, uint64_t cap, const AtomCols& c,

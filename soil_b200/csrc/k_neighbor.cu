@@ -21,8 +21,6 @@
 // only REJECTS candidates provably outside the cutoff — the margin eps bounds
 // the float rounding of coordinates, differences and squares — followed by
 // the exact FP64 test on the rest, so the lists are identical in both modes.
-#include <cstdlib>
-
 #include "device_ops.cuh"
 #include "kernels.cuh"
 
@@ -31,7 +29,7 @@ namespace soil {
 // Pass 1: one thread per local row (rows of a warp are neighbours in space, so
 // their candidate records are shared through L1); the first K entries go to
 // the row's slots, the length to rowcount.
-template <bool UNIFORM, bool FP32, bool PF>
+template <bool UNIFORM, bool FP32>
 __global__ void __launch_bounds__(kBlock) k_pairs_rows(PairParams p, uint32_t* rowcount,
                                                        uint32_t* slots, DevFlags* flags) {
     const Filter<UNIFORM, FP32> test(p);
@@ -39,8 +37,8 @@ __global__ void __launch_bounds__(kBlock) k_pairs_rows(PairParams p, uint32_t* r
     uint32_t n_rechk = 0, n_cand32 = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < p.nlocal;
          i += (uint64_t)gridDim.x * blockDim.x)
-        rowcount[i] = row_scan<UNIFORM, FP32, true, PF>(p, test, i, slots + i * K, K, &n_rechk,
-                                                        &n_cand32, flags, p.in_count);
+        rowcount[i] = row_scan<UNIFORM, FP32, true>(p, test, i, slots + i * K, K, &n_rechk,
+                                                    &n_cand32, flags, p.in_count);
     uint64_t n_cand = n_cand32;
     uint64_t r = n_rechk;
     for (int o = 16; o > 0; o >>= 1) {
@@ -64,18 +62,34 @@ __global__ void __launch_bounds__(kBlock) k_pairs_fill(PairParams p, const uint3
          i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t cnt = rowcount[i];
         uint32_t* out = indices + offsets[i];
-        if (cnt <= K) {
-            const uint32_t* row = slots + i * K;
-            for (uint32_t k = 0; k < cnt; ++k) out[k] = row[k];
-        } else {
+        const bool slotted = cnt <= K;
+        if (!slotted) {
             uint32_t rk = 0, cd = 0;
             row_scan<UNIFORM, FP32, true>(p, test, i, out, 0xffffffffu, &rk, &cd, nullptr);
         }
-        if (p.in_list)  // row i into each partner's transposed list (the counts go back to 0)
-            for (uint32_t k = 0; k < cnt; ++k) {
-                const uint32_t a = out[k];
-                p.in_list[p.in_start[a] + atomicSub(&p.in_count[a], 1u) - 1u] = (uint32_t)i;
+        // Four entries at a time, their loads, atomics and stores each issued
+        // together: the row into its CSR place (from the slots) and (with the
+        // transposed lists) row i into each partner's list, the counts going
+        // back to 0.
+        const uint32_t* src = slotted ? slots + i * K : out;
+        for (uint32_t k0 = 0; k0 < cnt; k0 += 4) {
+            uint32_t a[4], at[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (k0 + u < cnt) a[u] = src[k0 + u];
+            if (slotted) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (k0 + u < cnt) out[k0 + u] = a[u];
             }
+            if (!p.in_list) continue;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (k0 + u < cnt) at[u] = p.in_start[a[u]] + atomicSub(&p.in_count[a[u]], 1u) - 1u;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (k0 + u < cnt) p.in_list[at[u]] = (uint32_t)i;
+        }
     }
 }
 
@@ -84,15 +98,9 @@ static void launch_pairs_t(cudaStream_t st, const PairParams& p, uint32_t* rowco
                            uint32_t* slots, const uint32_t* offsets, uint32_t* indices,
                            DevFlags* flags, bool fill) {
     note_launch();
-    // SOIL_PAIRS_PREFETCH=0: the pass-1 scan without the record prefetch
-    const char* env = std::getenv("SOIL_PAIRS_PREFETCH");
-    const bool pf = !(env && std::atoi(env) == 0);
-    if (!fill && pf)
-        k_pairs_rows<UNIFORM, FP32, true><<<grid_for(p.nlocal), kBlock, 0, st>>>(p, rowcount, slots,
-                                                                                  flags);
-    else if (!fill)
-        k_pairs_rows<UNIFORM, FP32, false><<<grid_for(p.nlocal), kBlock, 0, st>>>(p, rowcount,
-                                                                                   slots, flags);
+    if (!fill)
+        k_pairs_rows<UNIFORM, FP32><<<grid_for(p.nlocal), kBlock, 0, st>>>(p, rowcount, slots,
+                                                                            flags);
     else
         k_pairs_fill<UNIFORM, FP32><<<grid_for(p.nlocal), kBlock, 0, st>>>(p, rowcount, slots,
                                                                             offsets, indices);
