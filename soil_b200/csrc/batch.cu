@@ -413,6 +413,7 @@ int fill_step(soil_batch* b, uint32_t k, bool post_flip, const BorderDim* bds) {
     t.grid = grid_of(s);
     t.ncells = (uint32_t)s->total_cells;
     t.nstencil = (int32_t)(runs.size() / 2);
+    t.pre_ranges = pairs_pre_ranges();
     std::memset(t.stencil, 0, sizeof t.stencil);
     if (!runs.empty()) std::memcpy(t.stencil, runs.data(), runs.size() * 4);
     t.has_self = s->stencil_self ? 1 : 0;

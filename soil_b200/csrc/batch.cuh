@@ -79,6 +79,7 @@ struct BoxStep {
     uint32_t ncells;
     int32_t nstencil;
     int32_t stencil[kMaxStencil];
+    int pre_ranges;  // the pair scan preloads its ranges
     int has_self;
     int newton;
     int uniform;

@@ -214,6 +214,92 @@ struct Filter {
     }
 };
 
+// Ranges of the row scan held in registers (row_scan_pre): the own cell's
+// range and up to kPreRanges - 1 stencil runs.
+constexpr int kPreRanges = 8;
+
+// row_scan with every range's slot bounds loaded up front: the own cell's
+// range (with newton the tail after i, merged with a first stencil run at
+// offset +1, whose cells follow it in slot order) and then each run, held in
+// registers and shifted down as ranges are used up, so moving to the next
+// range needs no load.  Same candidates in the same order, same counts, as
+// row_scan; for stencils of at most kPreRanges - 1 runs.
+template <bool UNIFORM, bool FP32, bool FILL>
+__device__ uint32_t row_scan_pre(const PairParams& p, const Filter<UNIFORM, FP32>& test,
+                                 uint64_t i, uint32_t* out, uint32_t cap, uint32_t* rechk,
+                                 uint32_t* cand, DevFlags* flags, uint32_t* in_count) {
+    const uint32_t my_cell = p.atom_cell[i];
+    const uint32_t mi = p.atom_sorted_idx[i];
+    const double4 pi = ld_rec(p.sp + mi);
+    const float4 pif = FP32 ? p.spf[mi] : make_float4(0.f, 0.f, 0.f, 0.f);
+    uint32_t rm[kPreRanges], re[kPreRanges];
+    int first = 0;  // stencil runs merged into the own range
+    rm[0] = 0;
+    re[0] = 0;
+    if (p.has_self) {
+        uint64_t ce = (uint64_t)my_cell + 1;
+        if (p.newton && p.nstencil > 0 && p.stencil[0] == 1 &&
+            ce + (uint64_t)p.stencil[1] <= p.ncells) {
+            ce += (uint64_t)p.stencil[1];
+            first = 1;
+        }
+        rm[0] = p.newton ? mi + 1 : p.bin_start[my_cell];
+        re[0] = p.bin_start[ce];
+    }
+    uint32_t total = re[0] - rm[0];
+#pragma unroll
+    for (int k = 1; k < kPreRanges; ++k) {
+        rm[k] = 0;
+        re[k] = 0;
+        const int s = first + k - 1;
+        if (s < p.nstencil) {
+            const int64_t c0 = (int64_t)my_cell + p.stencil[2 * s];
+            const int64_t c1 = c0 + p.stencil[2 * s + 1];
+            if (c0 < 0 || c1 > (int64_t)p.ncells) {  // the grid's ghost layers make this unreachable
+                if (flags) atomicOr(&flags->error, 1u);
+            } else {
+                rm[k] = p.bin_start[c0];
+                re[k] = p.bin_start[c1];
+                total += re[k] - rm[k];
+            }
+        }
+    }
+    const bool skip_i = p.has_self && !p.newton;  // i is in its own range
+    *cand += total - (skip_i ? 1u : 0u);
+    int left = 1 + (p.nstencil - first);  // ranges not yet finished, the current one included
+    bool own = true;
+    uint32_t cnt = 0;
+    uint32_t m = rm[0], e = re[0];
+    for (;;) {
+        while (m >= e) {  // the next range, shifted in from the registers
+            if (--left <= 0) return cnt;
+#pragma unroll
+            for (int k = 0; k + 1 < kPreRanges; ++k) {
+                rm[k] = rm[k + 1];
+                re[k] = re[k + 1];
+            }
+            m = rm[0];
+            e = re[0];
+            own = false;
+        }
+        if (own && skip_i && m == mi) {
+            ++m;
+            continue;
+        }
+        if (test(p, pi, pif, m, rechk)) {
+            if (in_count) {
+                const uint32_t a = p.sorted_atoms[m];
+                atomicAdd(&in_count[a], 1u);
+                if (FILL && cnt < cap) out[cnt] = a;
+            } else if (FILL && cnt < cap) {
+                out[cnt] = p.sorted_atoms[m];
+            }
+            ++cnt;
+        }
+        ++m;
+    }
+}
+
 // Row of local atom i, sequentially in reference order: the own cell's
 // candidates (the tail after i's slot with newton, else the whole cell
 // without i), then every stencil cell in stencil order, each in sorted order.
@@ -230,6 +316,9 @@ template <bool UNIFORM, bool FP32, bool FILL>
 __device__ uint32_t row_scan(const PairParams& p, const Filter<UNIFORM, FP32>& test, uint64_t i,
                              uint32_t* out, uint32_t cap, uint32_t* rechk, uint32_t* cand,
                              DevFlags* flags, uint32_t* in_count = nullptr) {
+    if (p.pre_ranges && p.nstencil < kPreRanges)
+        return row_scan_pre<UNIFORM, FP32, FILL>(p, test, i, out, cap, rechk, cand, flags,
+                                                 in_count);
     const uint32_t my_cell = p.atom_cell[i];
     const uint32_t mi = p.atom_sorted_idx[i];
     const double4 pi = ld_rec(p.sp + mi);

@@ -124,41 +124,24 @@ struct ColLd {
 };
 
 // F += f(a, o) over the partners o = idx(0), ..., idx(n - 1) in that order.
-// The records of partners k + 1 .. k + D are loaded before partner k's force
-// is evaluated, so D + 1 gathers are in flight per thread.
-template <int D = 1, class Ld, class Idx>
+// Partner k + 1's record is loaded before partner k's force is evaluated, so
+// two gathers are in flight per thread (deeper lookahead measured slower: it
+// costs registers and occupancy).
+template <class Ld, class Idx>
 __device__ __forceinline__ void sum_partners(const Ld& ld, const double4& pa, double K, uint32_t n,
                                              const Idx& idx, double& Fx, double& Fy, double& Fz) {
     if (n == 0) return;
-    if constexpr (D == 1) {
-        double4 cur = ld(idx(0));
-        for (uint32_t k = 0; k < n; ++k) {
-            double4 nxt = cur;
-            if (k + 1 < n) nxt = ld(idx(k + 1));
-            double fx, fy, fz;
-            if (pair_force(pa.x, pa.y, pa.z, pa.w, cur.x, cur.y, cur.z, cur.w, K, fx, fy, fz)) {
-                Fx = Fx + fx;
-                Fy = Fy + fy;
-                Fz = Fz + fz;
-            }
-            cur = nxt;
-        }
-        return;
-    }
-    double4 r[D + 1];
-#pragma unroll
-    for (int u = 0; u < D; ++u)
-        if ((uint32_t)u < n) r[u] = ld(idx(u));
+    double4 cur = ld(idx(0));
     for (uint32_t k = 0; k < n; ++k) {
-        if (k + D < n) r[D] = ld(idx(k + D));
+        double4 nxt = cur;
+        if (k + 1 < n) nxt = ld(idx(k + 1));
         double fx, fy, fz;
-        if (pair_force(pa.x, pa.y, pa.z, pa.w, r[0].x, r[0].y, r[0].z, r[0].w, K, fx, fy, fz)) {
+        if (pair_force(pa.x, pa.y, pa.z, pa.w, cur.x, cur.y, cur.z, cur.w, K, fx, fy, fz)) {
             Fx = Fx + fx;
             Fy = Fy + fy;
             Fz = Fz + fz;
         }
-#pragma unroll
-        for (int u = 0; u < D; ++u) r[u] = r[u + 1];
+        cur = nxt;
     }
 }
 
@@ -300,7 +283,7 @@ struct CsrIdx {
 // rows below a (ascending; in_split[a] of them), a's own row, the in-list
 // rows above a; each entry evaluated as f(a, partner) (the negation argument
 // at the top of k_force.cu).  Ghosts receive only with newton and have no row.
-template <int D, class Ld>
+template <class Ld>
 __device__ __forceinline__ void csr_item_force(const ForceCsr& q, const Ld& ld, uint64_t a,
                                                double& Fx, double& Fy, double& Fz) {
     const bool local = a < q.nlocal;
@@ -319,11 +302,11 @@ __device__ __forceinline__ void csr_item_force(const ForceCsr& q, const Ld& ld, 
         ix.rs = q.offsets[a];
         ix.nrow = q.offsets[a + 1] - ix.rs;
     }
-    sum_partners<D>(ld, pa, q.K, nin + ix.nrow, ix, Fx, Fy, Fz);
+    sum_partners(ld, pa, q.K, nin + ix.nrow, ix, Fx, Fy, Fz);
 }
 
 // Root t and its images by one thread (CSR walk), then (FOLD) the fold.
-template <bool FOLD, int D, class Ld>
+template <bool FOLD, class Ld>
 __device__ __forceinline__ void force_csr_root_ld(const ForceCsr& q, const Ld& ld,
                                                   const AtomCols& c, const PlaneList& rev,
                                                   uint64_t t) {
@@ -331,7 +314,7 @@ __device__ __forceinline__ void force_csr_root_ld(const ForceCsr& q, const Ld& l
     for (uint32_t f = f0 - 1; f + 1 <= f1; ++f) {  // the root (f = f0 - 1), then its images
         const uint64_t a = f + 1 == f0 ? t : q.nlocal + q.fold_list[f];
         double Fx, Fy, Fz;
-        csr_item_force<D>(q, ld, a, Fx, Fy, Fz);
+        csr_item_force(q, ld, a, Fx, Fy, Fz);
         c.fx[a] = Fx;
         c.fy[a] = Fy;
         c.fz[a] = Fz;
@@ -341,12 +324,11 @@ __device__ __forceinline__ void force_csr_root_ld(const ForceCsr& q, const Ld& l
 
 // PK: the partners' records from q.pk (which must then be set), else from
 // the columns.
-// D: partner records loaded ahead (sum_partners).
-template <bool FOLD, bool PK, int D = 1>
+template <bool FOLD, bool PK>
 __device__ __forceinline__ void force_csr_root(const ForceCsr& q, const AtomCols& c,
                                                const PlaneList& rev, uint64_t t) {
-    if constexpr (PK) force_csr_root_ld<FOLD, D>(q, PkLd{q.pk}, c, rev, t);
-    else force_csr_root_ld<FOLD, D>(q, ColLd{c.x, c.y, c.z, q.rad}, c, rev, t);
+    if constexpr (PK) force_csr_root_ld<FOLD>(q, PkLd{q.pk}, c, rev, t);
+    else force_csr_root_ld<FOLD>(q, ColLd{c.x, c.y, c.z, q.rad}, c, rev, t);
 }
 
 // Entry k of a group's sequence.

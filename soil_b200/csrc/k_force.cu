@@ -110,23 +110,14 @@ __global__ void __launch_bounds__(kBlock, 4) k_force_walk(ForceArgs p) {
         force_walk_root<FOLD, PK>(p.q, p.c, p.rev, t);
 }
 
-template <bool FOLD, bool PK, int D>
-__global__ void __launch_bounds__(kBlock, D == 1 ? 4 : 3) k_force_csr(ForceCsr q, AtomCols c,
-                                                                   PlaneList rev) {
+template <bool FOLD, bool PK>
+__global__ void __launch_bounds__(kBlock, 4) k_force_csr(ForceCsr q, AtomCols c, PlaneList rev) {
     // grid-stride over whole blocks of kBlock roots, so a block's order
     // permutes its own roots
     for (uint64_t b = (uint64_t)blockIdx.x * kBlock; b < q.nlocal; b += (uint64_t)gridDim.x * kBlock) {
         const uint64_t k = b + threadIdx.x;
-        if (k < q.nlocal) force_csr_root<FOLD, PK, D>(q, c, rev, q.order ? q.order[k] : k);
+        if (k < q.nlocal) force_csr_root<FOLD, PK>(q, c, rev, q.order ? q.order[k] : k);
     }
-}
-
-// Partner records loaded ahead by the CSR walk on the columns (SOIL_CSR_DEPTH
-// 1..3; read at each launch).
-static int csr_depth() {
-    const char* env = std::getenv("SOIL_CSR_DEPTH");
-    const int d = env ? std::atoi(env) : 1;
-    return d < 1 ? 1 : d > 3 ? 3 : d;
 }
 
 // Entries of root t's walk: its and its images' in-lists and its row.
@@ -176,23 +167,15 @@ void launch_force_csr(cudaStream_t st, const ForceCsr& q, const AtomCols& c, con
                       bool fold) {
     if (q.nlocal == 0) return;
     note_launch();
-    const int d = q.pk ? 1 : csr_depth();
-    // one resident wave: 4 blocks per SM at <= 64 registers (3 with more lookahead)
-    const unsigned full = 148u * (d == 1 ? 4u : 3u);
+    const unsigned full = 148u * 4u;  // one resident wave at <= 64 registers
     const unsigned need = (unsigned)((q.nlocal + kBlock - 1) / kBlock);
     const unsigned grid = need < full ? need : full;
     if (q.pk) {
-        if (fold) k_force_csr<true, true, 1><<<grid, kBlock, 0, st>>>(q, c, rev);
-        else k_force_csr<false, true, 1><<<grid, kBlock, 0, st>>>(q, c, rev);
-    } else if (d == 1) {
-        if (fold) k_force_csr<true, false, 1><<<grid, kBlock, 0, st>>>(q, c, rev);
-        else k_force_csr<false, false, 1><<<grid, kBlock, 0, st>>>(q, c, rev);
-    } else if (d == 2) {
-        if (fold) k_force_csr<true, false, 2><<<grid, kBlock, 0, st>>>(q, c, rev);
-        else k_force_csr<false, false, 2><<<grid, kBlock, 0, st>>>(q, c, rev);
+        if (fold) k_force_csr<true, true><<<grid, kBlock, 0, st>>>(q, c, rev);
+        else k_force_csr<false, true><<<grid, kBlock, 0, st>>>(q, c, rev);
     } else {
-        if (fold) k_force_csr<true, false, 3><<<grid, kBlock, 0, st>>>(q, c, rev);
-        else k_force_csr<false, false, 3><<<grid, kBlock, 0, st>>>(q, c, rev);
+        if (fold) k_force_csr<true, false><<<grid, kBlock, 0, st>>>(q, c, rev);
+        else k_force_csr<false, false><<<grid, kBlock, 0, st>>>(q, c, rev);
     }
 }
 

@@ -285,6 +285,7 @@ struct PairParams {
     uint32_t* in_count;
     const uint32_t* in_start;
     uint32_t* in_list;
+    int pre_ranges;  // row_scan_pre for stencils of few runs (SOIL_PAIRS_PRE, default on)
 };
 // Pass 1: row lengths into rowcount[], the first K entries of each row into
 // slots[i*K ...]; filter statistics into flags.

@@ -268,6 +268,8 @@ int counts_zero(soil_sys* s, uint64_t nc);
 // cells, as (offset, cells) pairs; without newton the own cell (offset 0),
 // which the scan takes first, is left out.
 std::vector<int32_t> stencil_runs(const std::vector<int32_t>& sten, bool newton);
+// Whether the pair scan preloads its ranges (SOIL_PAIRS_PRE=0: off; read at each call).
+int pairs_pre_ranges();
 // exclusive scan of in[0, n) into out[0, n] in one launch, errors into the
 // system's device flags
 int scan_1p(soil_sys* s, const uint32_t* in, uint32_t* out, uint64_t n);
