@@ -110,8 +110,8 @@ __global__ void __launch_bounds__(kBlock, 4) k_force_walk(ForceArgs p) {
         force_walk_root<FOLD, PK>(p.q, p.c, p.rev, t);
 }
 
-template <bool FOLD, bool PK, int MINB = 4>
-__global__ void __launch_bounds__(kBlock, MINB) k_force_csr(ForceCsr q, AtomCols c, PlaneList rev) {
+template <bool FOLD, bool PK>
+__global__ void __launch_bounds__(kBlock, 4) k_force_csr(ForceCsr q, AtomCols c, PlaneList rev) {
     // grid-stride over whole blocks of kBlock roots, so a block's order
     // permutes its own roots
     for (uint64_t b = (uint64_t)blockIdx.x * kBlock; b < q.nlocal; b += (uint64_t)gridDim.x * kBlock) {
@@ -167,21 +167,15 @@ void launch_force_csr(cudaStream_t st, const ForceCsr& q, const AtomCols& c, con
                       bool fold) {
     if (q.nlocal == 0) return;
     note_launch();
-    // SOIL_CSR_LAUNCH (measurement): bit 0 = 5 blocks per SM (fewer
-    // registers), bit 1 = one block per kBlock roots instead of one resident
-    // wave striding over them
-    const char* env = std::getenv("SOIL_CSR_LAUNCH");
-    const int mode = env ? std::atoi(env) : 0;
-    const bool five = (mode & 1) != 0;
-    const unsigned full = 148u * (five ? 5u : 4u);
+    // one resident wave at <= 64 registers, striding over blocks of roots
+    // (measured faster than one block per kBlock roots, and than 5 blocks per
+    // SM at 48 registers, which spills)
+    const unsigned full = 148u * 4u;
     const unsigned need = (unsigned)((q.nlocal + kBlock - 1) / kBlock);
-    const unsigned grid = (mode & 2) || need < full ? need : full;
+    const unsigned grid = need < full ? need : full;
     if (q.pk) {
         if (fold) k_force_csr<true, true><<<grid, kBlock, 0, st>>>(q, c, rev);
         else k_force_csr<false, true><<<grid, kBlock, 0, st>>>(q, c, rev);
-    } else if (five) {
-        if (fold) k_force_csr<true, false, 5><<<grid, kBlock, 0, st>>>(q, c, rev);
-        else k_force_csr<false, false, 5><<<grid, kBlock, 0, st>>>(q, c, rev);
     } else {
         if (fold) k_force_csr<true, false><<<grid, kBlock, 0, st>>>(q, c, rev);
         else k_force_csr<false, false><<<grid, kBlock, 0, st>>>(q, c, rev);
