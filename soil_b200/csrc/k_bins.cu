@@ -34,7 +34,7 @@ void launch_cells(cudaStream_t st, uint64_t first, uint64_t n, const AtomCols& c
                   uint32_t* cell_out, uint32_t* counts) {
     if (n == 0) return;
     note_launch();
-    k_cells<<<grid_for(n), kBlock, 0, st>>>(first, n, c, gr, cell_out, counts);
+    k_cells<<<grid_wave<k_cells>(n), kBlock, 0, st>>>(first, n, c, gr, cell_out, counts);
 }
 
 __global__ void __launch_bounds__(kBlock) k_count_cells(uint64_t n, const uint32_t* cell,
@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(kBlock) k_count_cells(uint64_t n, const uint32
 void launch_count_cells(cudaStream_t st, uint64_t n, const uint32_t* cell, uint32_t* counts) {
     if (n == 0) return;
     note_launch();
-    k_count_cells<<<grid_for(n), kBlock, 0, st>>>(n, cell, counts);
+    k_count_cells<<<grid_wave<k_count_cells>(n), kBlock, 0, st>>>(n, cell, counts);
 }
 
 __global__ void __launch_bounds__(kBlock) k_scatter(uint64_t n, const uint32_t* cell,
@@ -74,7 +74,7 @@ void launch_scatter(cudaStream_t st, uint64_t n, const uint32_t* cell, uint32_t*
                     uint32_t* out) {
     if (n == 0) return;
     note_launch();
-    k_scatter<<<grid_for(n), kBlock, 0, st>>>(n, cell, cursor, out);
+    k_scatter<<<grid_wave<k_scatter>(n), kBlock, 0, st>>>(n, cell, cursor, out);
 }
 
 // The scatter that consumes the counts: out[start[c] + --counts[c]] = i
@@ -104,7 +104,7 @@ void launch_scatter_consume(cudaStream_t st, uint64_t n, const uint32_t* cell,
                             const uint32_t* start, uint32_t* counts, uint32_t* out) {
     if (n == 0) return;
     note_launch();
-    k_scatter_consume<<<grid_for(n), kBlock, 0, st>>>(n, cell, start, counts, out);
+    k_scatter_consume<<<grid_wave<k_scatter_consume>(n), kBlock, 0, st>>>(n, cell, start, counts, out);
 }
 
 // The neighbor build's cells in one pass: the locals' cells from the sort
@@ -130,7 +130,7 @@ void launch_cells_reuse(cudaStream_t st, uint64_t nlocal, uint64_t n, const Atom
                         uint32_t* counts) {
     if (n == 0) return;
     note_launch();
-    k_cells_reuse<<<grid_for(n), kBlock, 0, st>>>(nlocal, n, c, gr, local_cell, cell_out, counts);
+    k_cells_reuse<<<grid_wave<k_cells_reuse>(n), kBlock, 0, st>>>(nlocal, n, c, gr, local_cell, cell_out, counts);
 }
 
 // Restore the stable (ascending index) order inside every segment.
@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(kBlock) k_segsort(uint64_t nseg, const uint32_
 void launch_segsort(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint32_t* items) {
     if (nseg == 0) return;
     note_launch();
-    k_segsort<<<grid_for(nseg), kBlock, 0, st>>>(nseg, start, items);
+    k_segsort<<<grid_wave<k_segsort>(nseg), kBlock, 0, st>>>(nseg, start, items);
 }
 
 // The transposed lists' sort: segment a (atom a's in-list) ascending, and
@@ -165,7 +165,7 @@ void launch_segsort_split(cudaStream_t st, uint64_t nseg, const uint32_t* start,
                           uint32_t* split) {
     if (nseg == 0) return;
     note_launch();
-    k_segsort_split<<<grid_for(nseg), kBlock, 0, st>>>(nseg, start, items, split);
+    k_segsort_split<<<grid_wave<k_segsort_split>(nseg), kBlock, 0, st>>>(nseg, start, items, split);
 }
 
 // split[a] of already sorted transposed lists
@@ -184,7 +184,7 @@ void launch_in_split(cudaStream_t st, uint64_t nseg, const uint32_t* start, cons
                      uint32_t* split) {
     if (nseg == 0) return;
     note_launch();
-    k_in_split<<<grid_for(nseg), kBlock, 0, st>>>(nseg, start, items, split);
+    k_in_split<<<grid_wave<k_in_split>(nseg), kBlock, 0, st>>>(nseg, start, items, split);
 }
 
 // Atom::apply_permutation + AtomDataRegistry::apply_permutation_all
@@ -200,7 +200,7 @@ void launch_perm_gather(cudaStream_t st, uint64_t n, const uint32_t* perm, const
                         const AtomCols& dst, bool forces) {
     if (n == 0) return;
     note_launch();
-    k_perm_gather<<<grid_for(n), kBlock, 0, st>>>(n, perm, src, dst, forces ? 1 : 0);
+    k_perm_gather<<<grid_wave<k_perm_gather>(n), kBlock, 0, st>>>(n, perm, src, dst, forces ? 1 : 0);
 }
 
 __global__ void __launch_bounds__(kBlock) k_identity(uint64_t n, const uint32_t* perm,
@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(kBlock) k_identity(uint64_t n, const uint32_t*
 void launch_identity_check(cudaStream_t st, uint64_t n, const uint32_t* perm, DevFlags* flags) {
     if (n == 0) return;
     note_launch();
-    k_identity<<<grid_for(n), kBlock, 0, st>>>(n, perm, flags);
+    k_identity<<<grid_wave<k_identity>(n), kBlock, 0, st>>>(n, perm, flags);
 }
 
 __global__ void __launch_bounds__(kBlock) k_permute_u32(uint64_t n, const uint32_t* perm,
@@ -230,7 +230,7 @@ void launch_permute_u32(cudaStream_t st, uint64_t n, const uint32_t* perm, const
                         uint32_t* out) {
     if (n == 0) return;
     note_launch();
-    k_permute_u32<<<grid_for(n), kBlock, 0, st>>>(n, perm, in, out);
+    k_permute_u32<<<grid_wave<k_permute_u32>(n), kBlock, 0, st>>>(n, perm, in, out);
 }
 
 // atom_sorted_idx and sorted_pos of bin_neighbor_list (neighbor.rs:1101-1125),
@@ -250,7 +250,7 @@ void launch_sorted_views(cudaStream_t st, uint64_t n, const uint32_t* sorted, co
                          const double origin[3]) {
     if (n == 0) return;
     note_launch();
-    k_sorted_views<<<grid_for(n), kBlock, 0, st>>>(n, sorted, c, atom_sorted_idx, sp, spf,
+    k_sorted_views<<<grid_wave<k_sorted_views>(n), kBlock, 0, st>>>(n, sorted, c, atom_sorted_idx, sp, spf,
                                                    origin[0], origin[1], origin[2]);
 }
 

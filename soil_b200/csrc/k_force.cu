@@ -80,14 +80,14 @@ __global__ void __launch_bounds__(kBlock) k_seq_fill(SeqArgs q, const uint32_t* 
 void launch_seq_count(cudaStream_t st, const SeqArgs& q, uint32_t* cnt, uint32_t* grp) {
     if (q.ntotal == 0) return;
     note_launch();
-    k_seq_count<<<grid_for(q.ntotal), kBlock, 0, st>>>(q, cnt, grp);
+    k_seq_count<<<grid_wave<k_seq_count>(q.ntotal), kBlock, 0, st>>>(q, cnt, grp);
 }
 
 void launch_seq_fill(cudaStream_t st, const SeqArgs& q, const uint32_t* grp_start, uint32_t* seq,
                      uint8_t* owner) {
     if (q.nlocal == 0) return;
     note_launch();
-    k_seq_fill<<<grid_for(q.nlocal), kBlock, 0, st>>>(q, grp_start, seq, owner);
+    k_seq_fill<<<grid_wave<k_seq_fill>(q.nlocal), kBlock, 0, st>>>(q, grp_start, seq, owner);
 }
 
 // ---- the warp-cooperative consumer, one launch --------------------------------

@@ -189,18 +189,18 @@ void launch_borders(cudaStream_t st, uint64_t nlocal, uint64_t cap, const AtomCo
     const uint64_t nw = (nlocal + 31) / 32;
     const uint64_t nchunks = (nw + kScanChunk - 1) / kScanChunk;
     uint32_t* ctot = counts + (kBorderCats + 1) * nw;  // chunk totals, then prefixes
-    const unsigned blocks = grid_for(nw * 32);
     note_launch();
-    k_border_faces<<<blocks, kBlock, 0, st>>>(nlocal, c, bp, cats, face, counts, nw);
+    k_border_faces<<<grid_wave<k_border_faces>(nw * 32), kBlock, 0, st>>>(nlocal, c, bp, cats, face,
+                                                                          counts, nw);
     note_launch();
     k_border_cat_scan<<<(unsigned)((kBorderCats + 1) * nchunks), kBlock, 0, st>>>(counts, offs, nw,
                                                                                 ctot, nchunks);
     note_launch();
     k_border_chunk_prefix<<<1, kBlock, 0, st>>>(ctot, nchunks, bs);
     note_launch();
-    k_border_images<<<blocks, kBlock, 0, st>>>(nlocal, cap, c, bp, cats, face, offs, ctot, nchunks,
-                                               nw, bs, ghost_root, ghost_chain, send, fold_start,
-                                               fold_list);
+    k_border_images<<<grid_wave<k_border_images>(nw * 32), kBlock, 0, st>>>(
+        nlocal, cap, c, bp, cats, face, offs, ctot, nchunks, nw, bs, ghost_root, ghost_chain, send,
+        fold_start, fold_list);
 }
 
 __global__ void __launch_bounds__(kBlock) k_forward(uint64_t nlocal, uint64_t nghost, AtomCols c,
@@ -219,7 +219,7 @@ void launch_forward(cudaStream_t st, uint64_t nlocal, uint64_t nghost, const Ato
     pl.n = nfwd;
     for (int k = 0; k < nfwd; ++k) pl.idx[k] = fwd_planes[k];
     note_launch();
-    k_forward<<<grid_for(nghost), kBlock, 0, st>>>(nlocal, nghost, c, ghost_root, ghost_chain, sc,
+    k_forward<<<grid_wave<k_forward>(nghost), kBlock, 0, st>>>(nlocal, nghost, c, ghost_root, ghost_chain, sc,
                                                    pl, zero_force ? 1 : 0);
 }
 
@@ -262,7 +262,7 @@ void launch_reverse_fold_roots(cudaStream_t st, uint64_t nlocal, uint64_t max_ro
     pl.n = nrev;
     for (int k = 0; k < nrev; ++k) pl.idx[k] = rev_planes[k];
     note_launch();
-    k_reverse_fold_roots<<<grid_for(max_roots), kBlock, 0, st>>>(nlocal, count, roots, start, list,
+    k_reverse_fold_roots<<<grid_wave<k_reverse_fold_roots>(max_roots), kBlock, 0, st>>>(nlocal, count, roots, start, list,
                                                                  c, pl);
 }
 
@@ -278,7 +278,7 @@ void launch_fold_root_flags(cudaStream_t st, uint64_t nlocal, const uint32_t* fo
                             uint32_t* flag) {
     if (nlocal == 0) return;
     note_launch();
-    k_fold_root_flags<<<grid_for(nlocal), kBlock, 0, st>>>(nlocal, fold_start, flag);
+    k_fold_root_flags<<<grid_wave<k_fold_root_flags>(nlocal), kBlock, 0, st>>>(nlocal, fold_start, flag);
 }
 
 void launch_reverse_fold(cudaStream_t st, uint64_t nlocal, const uint32_t* start,
@@ -288,7 +288,7 @@ void launch_reverse_fold(cudaStream_t st, uint64_t nlocal, const uint32_t* start
     pl.n = nrev;
     for (int k = 0; k < nrev; ++k) pl.idx[k] = rev_planes[k];
     note_launch();
-    k_reverse_fold<<<grid_for(nlocal), kBlock, 0, st>>>(nlocal, start, list, c, pl);
+    k_reverse_fold<<<grid_wave<k_reverse_fold>(nlocal), kBlock, 0, st>>>(nlocal, start, list, c, pl);
 }
 
 }  // namespace soil

@@ -68,12 +68,12 @@ static void initial_kernel(cudaStream_t st, uint64_t n, const AtomCols& c, doubl
                            bool zero_force, const CheckArgs& ck, const FwdArgs* fw) {
     note_launch();
     if (fw) {
-        k_initial<FUSE_FINAL, true>
-            <<<grid_for(n), kBlock, 0, st>>>(n, c, dt, zero_force ? 1 : 0, ck, *fw);
+        k_initial<FUSE_FINAL, true><<<grid_wave<k_initial<FUSE_FINAL, true>>(n), kBlock, 0, st>>>(
+            n, c, dt, zero_force ? 1 : 0, ck, *fw);
     } else {
         FwdArgs none{};
-        k_initial<FUSE_FINAL, false>
-            <<<grid_for(n), kBlock, 0, st>>>(n, c, dt, zero_force ? 1 : 0, ck, none);
+        k_initial<FUSE_FINAL, false><<<grid_wave<k_initial<FUSE_FINAL, false>>(n), kBlock, 0, st>>>(
+            n, c, dt, zero_force ? 1 : 0, ck, none);
     }
 }
 
@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(kBlock) k_final(uint64_t n, AtomCols c, double
 void launch_final(cudaStream_t st, uint64_t n, const AtomCols& c, double dt) {
     if (n == 0) return;
     note_launch();
-    k_final<<<grid_for(n), kBlock, 0, st>>>(n, c, dt);
+    k_final<<<grid_wave<k_final>(n), kBlock, 0, st>>>(n, c, dt);
 }
 
 __global__ void __launch_bounds__(kBlock) k_zero(uint64_t n, AtomCols c, PlaneList zp) {
@@ -125,7 +125,7 @@ void launch_zero_forces(cudaStream_t st, uint64_t n, const AtomCols& c, const in
     zp.n = nzero;
     for (int k = 0; k < nzero; ++k) zp.idx[k] = zero_planes[k];
     note_launch();
-    k_zero<<<grid_for(n), kBlock, 0, st>>>(n, c, zp);
+    k_zero<<<grid_wave<k_zero>(n), kBlock, 0, st>>>(n, c, zp);
 }
 
 // pbc fully periodic fast path (domain.rs:626-636) / pbc_triclinic (domain.rs:674-729)
@@ -140,7 +140,7 @@ void launch_pbc(cudaStream_t st, uint64_t nlocal, const AtomCols& c, const Geom&
                 const double bvel[3]) {
     if (nlocal == 0) return;
     note_launch();
-    k_pbc<<<grid_for(nlocal), kBlock, 0, st>>>(nlocal, c, g, bvel[0], bvel[1], bvel[2]);
+    k_pbc<<<grid_wave<k_pbc>(nlocal), kBlock, 0, st>>>(nlocal, c, g, bvel[0], bvel[1], bvel[2]);
 }
 
 // soil_deform/src/lib.rs:568-574: vel.x += rate*(y - yc) on the first shear step
@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(kBlock) k_shear_profile(uint64_t n, AtomCols c
 void launch_shear_profile(cudaStream_t st, uint64_t n, const AtomCols& c, double rate, double yc) {
     if (n == 0) return;
     note_launch();
-    k_shear_profile<<<grid_for(n), kBlock, 0, st>>>(n, c, rate, yc);
+    k_shear_profile<<<grid_wave<k_shear_profile>(n), kBlock, 0, st>>>(n, c, rate, yc);
 }
 
 // apply_deform's remap (soil_deform/src/lib.rs:530-540), one dim after another
@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(kBlock) k_remap(uint64_t n, AtomCols c, RemapS
 void launch_remap(cudaStream_t st, uint64_t n, const AtomCols& c, const RemapSpec& r) {
     if (n == 0 || r.n == 0) return;
     note_launch();
-    k_remap<<<grid_for(n), kBlock, 0, st>>>(n, c, r);
+    k_remap<<<grid_wave<k_remap>(n), kBlock, 0, st>>>(n, c, r);
 }
 
 __global__ void __launch_bounds__(kBlock) k_save_pos(uint64_t n, AtomCols c, double* lbx,
@@ -190,7 +190,7 @@ void launch_save_positions(cudaStream_t st, uint64_t n, const AtomCols& c, doubl
                            double* lby, double* lbz) {
     if (n == 0) return;
     note_launch();
-    k_save_pos<<<grid_for(n), kBlock, 0, st>>>(n, c, lbx, lby, lbz);
+    k_save_pos<<<grid_wave<k_save_pos>(n), kBlock, 0, st>>>(n, c, lbx, lby, lbz);
 }
 
 }  // namespace soil
@@ -213,7 +213,7 @@ void launch_disp_check(cudaStream_t st, uint64_t n, const AtomCols& c, const dou
     if (n == 0) return;
     CheckArgs ck = make_check(lbx, lby, lbz, n, thr_sq, box, flags, pbc_mask);
     note_launch();
-    k_disp_check<<<grid_for(n), kBlock, 0, st>>>(n, c, ck);
+    k_disp_check<<<grid_wave<k_disp_check>(n), kBlock, 0, st>>>(n, c, ck);
 }
 
 // [n][3] interleaved <-> three SoA planes (host-facing layout of Vec<[f64;3]>)
@@ -262,21 +262,21 @@ void launch_deinterleave3(cudaStream_t st, uint64_t n, const double* src, double
                           double* c) {
     if (n) {
         note_launch();
-        k_deinterleave3<<<grid_for(n), kBlock, 0, st>>>(n, src, a, b, c);
+        k_deinterleave3<<<grid_wave<k_deinterleave3>(n), kBlock, 0, st>>>(n, src, a, b, c);
     }
 }
 void launch_interleave3(cudaStream_t st, uint64_t n, double* dst, const double* a, const double* b,
                         const double* c) {
     if (n) {
         note_launch();
-        k_interleave3<<<grid_for(n), kBlock, 0, st>>>(n, dst, a, b, c);
+        k_interleave3<<<grid_wave<k_interleave3>(n), kBlock, 0, st>>>(n, dst, a, b, c);
     }
 }
 void launch_interleave3i(cudaStream_t st, uint64_t n, int32_t* dst, const int32_t* a,
                          const int32_t* b, const int32_t* c) {
     if (n) {
         note_launch();
-        k_interleave3i<<<grid_for(n), kBlock, 0, st>>>(n, dst, a, b, c);
+        k_interleave3i<<<grid_wave<k_interleave3i>(n), kBlock, 0, st>>>(n, dst, a, b, c);
     }
 }
 // inv[i] = 1.0 / m[i] (IEEE division, the host's bits)
@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(kBlock) k_inverse(uint64_t n, const double* m,
 void launch_inverse(cudaStream_t st, uint64_t n, const double* m, double* inv) {
     if (n) {
         note_launch();
-        k_inverse<<<grid_for(n), kBlock, 0, st>>>(n, m, inv);
+        k_inverse<<<grid_wave<k_inverse>(n), kBlock, 0, st>>>(n, m, inv);
     }
 }
 
@@ -296,14 +296,14 @@ void launch_deinterleave_w(cudaStream_t st, uint64_t n, int w, const double* src
                            uint64_t cap) {
     if (n) {
         note_launch();
-        k_deinterleave_w<<<grid_for(n), kBlock, 0, st>>>(n, w, src, dst0, cap);
+        k_deinterleave_w<<<grid_wave<k_deinterleave_w>(n), kBlock, 0, st>>>(n, w, src, dst0, cap);
     }
 }
 void launch_interleave_w(cudaStream_t st, uint64_t n, int w, double* dst, const double* src0,
                          uint64_t cap) {
     if (n) {
         note_launch();
-        k_interleave_w<<<grid_for(n), kBlock, 0, st>>>(n, w, dst, src0, cap);
+        k_interleave_w<<<grid_wave<k_interleave_w>(n), kBlock, 0, st>>>(n, w, dst, src0, cap);
     }
 }
 
@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(kBlock) k_pack(uint64_t n, AtomCols c, const d
 void launch_pack(cudaStream_t st, uint64_t n, const AtomCols& c, const double* rad, double* pk) {
     if (n == 0) return;
     note_launch();
-    k_pack<<<grid_for(n), kBlock, 0, st>>>(n, c, rad, pk);
+    k_pack<<<grid_wave<k_pack>(n), kBlock, 0, st>>>(n, c, rad, pk);
 }
 
 }  // namespace soil

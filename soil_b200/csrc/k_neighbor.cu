@@ -39,6 +39,14 @@ __global__ void __launch_bounds__(kBlock) k_pairs_rows(PairParams p, uint32_t* r
          i += (uint64_t)gridDim.x * blockDim.x)
         rowcount[i] = row_scan<UNIFORM, FP32, true>(p, test, i, slots + i * K, K, &n_rechk,
                                                     &n_cand32, flags, p.in_count);
+    // the block's totals, then one atomic per counter and block (the FP64
+    // filter rechecks nothing)
+    __shared__ unsigned long long s_cand, s_rechk;
+    if (threadIdx.x == 0) {
+        s_cand = 0;
+        s_rechk = 0;
+    }
+    __syncthreads();
     uint64_t n_cand = n_cand32;
     uint64_t r = n_rechk;
     for (int o = 16; o > 0; o >>= 1) {
@@ -46,8 +54,13 @@ __global__ void __launch_bounds__(kBlock) k_pairs_rows(PairParams p, uint32_t* r
         r += __shfl_down_sync(0xffffffffu, r, o);
     }
     if ((threadIdx.x & 31) == 0) {
-        atomicAdd((unsigned long long*)&flags->candidates, (unsigned long long)n_cand);
-        atomicAdd((unsigned long long*)&flags->rechecked, (unsigned long long)r);
+        atomicAdd(&s_cand, (unsigned long long)n_cand);
+        if (FP32) atomicAdd(&s_rechk, (unsigned long long)r);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        atomicAdd((unsigned long long*)&flags->candidates, s_cand);
+        if (FP32) atomicAdd((unsigned long long*)&flags->rechecked, s_rechk);
     }
 }
 
@@ -99,10 +112,10 @@ static void launch_pairs_t(cudaStream_t st, const PairParams& p, uint32_t* rowco
                            DevFlags* flags, bool fill) {
     note_launch();
     if (!fill)
-        k_pairs_rows<UNIFORM, FP32><<<grid_for(p.nlocal), kBlock, 0, st>>>(p, rowcount, slots,
+        k_pairs_rows<UNIFORM, FP32><<<grid_wave<k_pairs_rows<UNIFORM, FP32>>(p.nlocal), kBlock, 0, st>>>(p, rowcount, slots,
                                                                             flags);
     else
-        k_pairs_fill<UNIFORM, FP32><<<grid_for(p.nlocal), kBlock, 0, st>>>(p, rowcount, slots,
+        k_pairs_fill<UNIFORM, FP32><<<grid_wave<k_pairs_fill<UNIFORM, FP32>>(p.nlocal), kBlock, 0, st>>>(p, rowcount, slots,
                                                                             offsets, indices);
 }
 
@@ -143,7 +156,7 @@ void launch_in_count(cudaStream_t st, uint64_t nlocal, const uint32_t* offsets,
                      const uint32_t* indices, uint32_t* incount) {
     if (nlocal == 0) return;
     note_launch();
-    k_in_count<<<grid_for(nlocal), kBlock, 0, st>>>(nlocal, offsets, indices, incount);
+    k_in_count<<<grid_wave<k_in_count>(nlocal), kBlock, 0, st>>>(nlocal, offsets, indices, incount);
 }
 
 __global__ void __launch_bounds__(kBlock) k_in_scatter(uint64_t nlocal, const uint32_t* offsets,
@@ -159,7 +172,7 @@ void launch_in_scatter(cudaStream_t st, uint64_t nlocal, const uint32_t* offsets
                        const uint32_t* indices, uint32_t* cursor, uint32_t* in_list) {
     if (nlocal == 0) return;
     note_launch();
-    k_in_scatter<<<grid_for(nlocal), kBlock, 0, st>>>(nlocal, offsets, indices, cursor, in_list);
+    k_in_scatter<<<grid_wave<k_in_scatter>(nlocal), kBlock, 0, st>>>(nlocal, offsets, indices, cursor, in_list);
 }
 
 }  // namespace soil

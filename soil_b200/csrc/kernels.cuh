@@ -2,13 +2,35 @@
 // Each wrapper enqueues on `st` and returns immediately.
 #pragma once
 
+#include <atomic>
+
 #include "soil_internal.cuh"
 
 namespace soil {
 
-// Grid for a grid-stride kernel: enough CTAs to fill the 148 SMs several
-// times, never more than the work needs.
+// Grid for a grid-stride kernel: per_sm CTAs on each of the 148 SMs, never
+// more than the work needs.
 unsigned grid_for(uint64_t n, int block = kBlock, int per_sm = 8);
+
+// Grid of exactly one resident wave of kernel K (its CTAs per SM at kBlock
+// threads and `smem` bytes of dynamic shared memory, queried once), never more
+// than the work needs.  A grid-stride kernel launched with more CTAs than fit
+// at once runs a partial second wave after the first (1,184 CTAs of a kernel
+// that fits 6 per SM take two wave times for 1.33 waves of work).
+template <auto K>
+unsigned grid_wave(uint64_t n, size_t smem = 0) {
+    static std::atomic<int> per_sm{0};
+    int r = per_sm.load(std::memory_order_relaxed);
+    if (r == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, K, kBlock, smem) != cudaSuccess ||
+            r < 1) {
+            cudaGetLastError();
+            r = 8;
+        }
+        per_sm.store(r, std::memory_order_relaxed);
+    }
+    return grid_for(n, kBlock, r);
+}
 
 // Process-wide count of kernel launches issued by this library.
 void note_launch();
