@@ -41,15 +41,15 @@ __device__ __forceinline__ void border_warp_counts(const AtomCols& c, uint64_t n
         face[r] = (uint8_t)bits;
     }
     uint32_t mine = 0, images = 0;
-    // a category can have members only if the tile's faces cover its need
+    // a category can have members only if the tile's faces cover its need:
+    // the categories of the OR of its bits (uniform over the warp)
     const uint32_t any = __reduce_or_sync(0xffffffffu, bits);
-    if (any) {
-        for (int k = 0; k < kBorderCats; ++k) {
-            if ((any & cats.need[k]) != cats.need[k]) continue;  // uniform over the warp
-            const uint32_t n = __popc(__ballot_sync(0xffffffffu, cat_member(cats, bits, k)));
-            if (lane == (uint32_t)k) mine = n;
-            images += n;
-        }
+    const uint32_t mine_cats = cats.member[bits];
+    for (uint32_t cand = cats.member[any]; cand; cand &= cand - 1) {
+        const int k = __ffs(cand) - 1;
+        const uint32_t n = __popc(__ballot_sync(0xffffffffu, (mine_cats >> k) & 1u));
+        if (lane == (uint32_t)k) mine = n;
+        images += n;
     }
     if (lane < kBorderCats) counts[lane * nw + w] = mine;
     if (lane == kBorderCats) counts[kBorderCats * nw + w] = images;
@@ -116,25 +116,24 @@ __device__ __forceinline__ void border_warp_images(
     const uint32_t rv =
         __shfl_sync(0xffffffffu, base_lane, lane < (uint32_t)kNumSwaps ? cats.swap_first[lane] : 0);
     if (lane < (uint32_t)kNumSwaps) sm.recv[lane] = rv;
-    uint32_t own = 0;  // images of this lane's root
-    for (int k = 0; k < kBorderCats; ++k) {
-        // no member in the tile unless its faces cover the need (uniform
-        // over the warp); only members read idx, and a member's parent
-        // category has it as a member too
-        if ((any & cats.need[k]) != cats.need[k]) continue;
-        const bool m = cat_member(cats, bits, k);
-        const unsigned bal = __ballot_sync(0xffffffffu, m);
+    const uint32_t mine_cats = cats.member[bits];
+    const uint32_t own = __popc(mine_cats);  // images of this lane's root
+    // only categories the tile's faces cover can have members (uniform over
+    // the warp); only members read idx, and a member's parent category has
+    // it as a member too
+    for (uint32_t cand = cats.member[any]; cand; cand &= cand - 1) {
+        const int k = __ffs(cand) - 1;
+        const unsigned bal = __ballot_sync(0xffffffffu, (mine_cats >> k) & 1u);
         const uint32_t base = __shfl_sync(0xffffffffu, base_lane + off_lane, k);
         sm.idx[k][lane] = base + __popc(bal & below);
-        own += m;
     }
     __syncwarp();
     const uint32_t fs = fold0 + warp_exclusive_sum(own, lane);
     if (r < nlocal) fold_start[r] = fs;
     if (r + 1 == nlocal) fold_start[nlocal] = fs + own;
     if (bits) {
-        for (int k = 0; k < kBorderCats; ++k) {
-            if (!cat_member(cats, bits, k)) continue;
+        for (uint32_t mk = mine_cats; mk; mk &= mk - 1) {
+            const int k = __ffs(mk) - 1;
             const uint32_t g = sm.idx[k][lane];
             if (g >= cap) {
                 bs[10] = 1u;  // out of capacity: the host grows the arrays and repeats
@@ -147,9 +146,8 @@ __device__ __forceinline__ void border_warp_images(
             send[s][g - sm.recv[s]] = parent;
         }
         uint32_t j = fs;
-        for (int f = 0; f < kBorderCats; ++f) {
-            const int k = cats.fold[f];
-            if (!cat_member(cats, bits, k)) continue;
+        for (uint32_t mf = cats.member_fold[bits]; mf; mf &= mf - 1) {
+            const int k = cats.fold[__ffs(mf) - 1];
             const uint32_t g = sm.idx[k][lane];
             if (g < cap && j < cap) fold_list[j] = g - (uint32_t)nlocal;
             ++j;

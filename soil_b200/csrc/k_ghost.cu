@@ -91,8 +91,24 @@ BorderCats build_border_cats() {
 }
 }  // namespace
 
+void finish_border_cats(BorderCats& t) {
+    for (uint32_t bits = 0; bits < 64; ++bits) {
+        uint32_t m = 0, mf = 0;
+        for (int k = 0; k < kBorderCats; ++k)
+            if ((bits & t.need[k]) == t.need[k]) m |= 1u << k;
+        for (int f = 0; f < kBorderCats; ++f)
+            if (m & (1u << t.fold[f])) mf |= 1u << f;
+        t.member[bits] = m;
+        t.member_fold[bits] = mf;
+    }
+}
+
 const BorderCats& border_cats() {
-    static const BorderCats t = build_border_cats();
+    static const BorderCats t = [] {
+        BorderCats c = build_border_cats();
+        finish_border_cats(c);
+        return c;
+    }();
     return t;
 }
 
@@ -101,6 +117,7 @@ BorderCats border_cats_masked(unsigned periodic_swaps) {
     for (int k = 0; k < kBorderCats; ++k)
         for (int q = 0; q < t.len[k]; ++q)
             if (!(periodic_swaps & (1u << t.sw[k][q]))) t.need[k] = 0x80;  // no face bit 7
+    finish_border_cats(t);
     return t;
 }
 

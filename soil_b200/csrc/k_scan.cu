@@ -100,6 +100,32 @@ __global__ void __launch_bounds__(kBlock) k_scan_down(const uint32_t* in, uint32
     if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = partial[ntiles];
 }
 
+// Pass 2 without the one-CTA pass over the tile sums: each CTA adds up the
+// sums of the tiles before its own (at most kScanCarryTiles of them, read
+// from L2), so the scan is two launches.  The last CTA writes out[n].
+constexpr uint64_t kScanCarryTiles = 4096;
+
+__global__ void __launch_bounds__(kBlock) k_scan_down_carry(const uint32_t* in, uint32_t* out,
+                                                            uint64_t n, const uint32_t* partial,
+                                                            uint64_t ntiles) {
+    __shared__ uint32_t tot, s_carry;
+    const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    load8(in, base, n, v);
+    uint32_t c = 0;  // this thread's share of the sums of tiles [0, blockIdx.x)
+    for (uint32_t t = threadIdx.x; t < blockIdx.x; t += kBlock) c += partial[t];
+    block_exclusive_scan(c, &tot);
+    if (threadIdx.x == 0) s_carry = tot;
+    __syncthreads();
+    const uint32_t carry = s_carry;
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) s += v[k];
+    const uint32_t pre = block_exclusive_scan(s, &tot) + carry;
+    store8_scan(out, base, n, v, pre);
+    if (blockIdx.x + 1 == ntiles && threadIdx.x == 0) out[n] = carry + tot;
+}
+
 uint64_t scan_temp_words(uint64_t n) { return (n + kScanTile - 1) / kScanTile + 2; }
 
 void exclusive_scan_u32(cudaStream_t st, const uint32_t* in, uint32_t* out, uint64_t n,
@@ -111,6 +137,11 @@ void exclusive_scan_u32(cudaStream_t st, const uint32_t* in, uint32_t* out, uint
     }
     note_launch();
     k_scan_reduce<<<(unsigned)ntiles, kBlock, 0, st>>>(in, n, temp);
+    if (ntiles <= kScanCarryTiles) {
+        note_launch();
+        k_scan_down_carry<<<(unsigned)ntiles, kBlock, 0, st>>>(in, out, n, temp, ntiles);
+        return;
+    }
     note_launch();
     k_scan_partials<<<1, kBlock, 0, st>>>(temp, ntiles);
     note_launch();

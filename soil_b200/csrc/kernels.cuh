@@ -234,6 +234,11 @@ struct BorderPass {
 // its swap chain, the parent category (-1: the root), the categories in
 // reverse-fold order and the contiguous category range of every swap.
 struct BorderCats {
+    // per combination of the six face bits: the categories a root with those
+    // bits belongs to (bit k), and the same set by fold position (bit f for
+    // category fold[f]); set by finish_border_cats
+    uint32_t member[64];
+    uint32_t member_fold[64];
     uint8_t need[kBorderCats];
     uint8_t len[kBorderCats];
     uint8_t sw[kBorderCats][3];
@@ -244,6 +249,8 @@ struct BorderCats {
     uint8_t swap_ncat[kNumSwaps];
 };
 const BorderCats& border_cats();
+// Fill the member masks of a category table from its needs and fold order.
+void finish_border_cats(BorderCats& t);
 // The categories with every chain through a swap outside periodic_swaps (bit
 // s: swap s has a periodic neighbor) made empty: they never match a root.
 BorderCats border_cats_masked(unsigned periodic_swaps);
