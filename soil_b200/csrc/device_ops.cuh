@@ -637,12 +637,17 @@ __device__ __forceinline__ void fold_root(const AtomCols& c, uint64_t nlocal, ui
 // one sorted slot of the neighbor build's bin order (neighbor.rs:1101-1125)
 __device__ __forceinline__ void sorted_view(const AtomCols& c, uint64_t m, const uint32_t* sorted,
                                             uint32_t* asi, double4* sp, float4* spf, double o0,
-                                            double o1, double o2) {
+                                            double o1, double o2, const BuildPos& bp = BuildPos{}) {
     const uint32_t a = sorted[m];
     asi[a] = (uint32_t)m;
     const double x = c.x[a], y = c.y[a], z = c.z[a], cut = c.cut[a];
     sp[m] = make_double4(x, y, z, cut);
     if (spf) spf[m] = make_float4((float)(x - o0), (float)(y - o1), (float)(z - o2), (float)cut);
+    if (bp.x && a < bp.nlocal) {  // save_build_positions of the locals
+        bp.x[a] = x;
+        bp.y[a] = y;
+        bp.z[a] = z;
+    }
 }
 
 // restore ascending order of one segment (the stable counting sort's last step):

@@ -190,17 +190,24 @@ void launch_in_split(cudaStream_t st, uint64_t nseg, const uint32_t* start, cons
 // Atom::apply_permutation + AtomDataRegistry::apply_permutation_all
 // (atom.rs:479-490, 284-289): every column gathered through perm.
 __global__ void __launch_bounds__(kBlock) k_perm_gather(uint64_t n, const uint32_t* perm,
-                                                        AtomCols s, AtomCols d, int forces) {
+                                                        AtomCols s, AtomCols d, int forces,
+                                                        const uint32_t* cell_in,
+                                                        uint32_t* cell_out) {
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n;
-         k += (uint64_t)gridDim.x * blockDim.x)
-        perm_gather_atom(s, d, k, perm[k], forces != 0);
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t p = perm[k];
+        perm_gather_atom(s, d, k, p, forces != 0);
+        if (cell_out) cell_out[k] = cell_in[p];
+    }
 }
 
 void launch_perm_gather(cudaStream_t st, uint64_t n, const uint32_t* perm, const AtomCols& src,
-                        const AtomCols& dst, bool forces) {
+                        const AtomCols& dst, bool forces, const uint32_t* cell_in,
+                        uint32_t* cell_out) {
     if (n == 0) return;
     note_launch();
-    k_perm_gather<<<grid_wave<k_perm_gather>(n), kBlock, 0, st>>>(n, perm, src, dst, forces ? 1 : 0);
+    k_perm_gather<<<grid_wave<k_perm_gather>(n), kBlock, 0, st>>>(n, perm, src, dst, forces ? 1 : 0,
+                                                                  cell_in, cell_out);
 }
 
 __global__ void __launch_bounds__(kBlock) k_identity(uint64_t n, const uint32_t* perm,
@@ -239,19 +246,19 @@ void launch_permute_u32(cudaStream_t st, uint64_t n, const uint32_t* perm, const
 __global__ void __launch_bounds__(kBlock) k_sorted_views(uint64_t n, const uint32_t* sorted,
                                                          AtomCols c, uint32_t* asi, double4* sp,
                                                          float4* spf, double o0, double o1,
-                                                         double o2) {
+                                                         double o2, BuildPos bp) {
     for (uint64_t m = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; m < n;
          m += (uint64_t)gridDim.x * blockDim.x)
-        sorted_view(c, m, sorted, asi, sp, spf, o0, o1, o2);
+        sorted_view(c, m, sorted, asi, sp, spf, o0, o1, o2, bp);
 }
 
 void launch_sorted_views(cudaStream_t st, uint64_t n, const uint32_t* sorted, const AtomCols& c,
                          uint32_t* atom_sorted_idx, double4* sp, float4* spf,
-                         const double origin[3]) {
+                         const double origin[3], const BuildPos& bp) {
     if (n == 0) return;
     note_launch();
-    k_sorted_views<<<grid_wave<k_sorted_views>(n), kBlock, 0, st>>>(n, sorted, c, atom_sorted_idx, sp, spf,
-                                                   origin[0], origin[1], origin[2]);
+    k_sorted_views<<<grid_wave<k_sorted_views>(n), kBlock, 0, st>>>(
+        n, sorted, c, atom_sorted_idx, sp, spf, origin[0], origin[1], origin[2], bp);
 }
 
 }  // namespace soil

@@ -176,23 +176,6 @@ void launch_remap(cudaStream_t st, uint64_t n, const AtomCols& c, const RemapSpe
     k_remap<<<grid_wave<k_remap>(n), kBlock, 0, st>>>(n, c, r);
 }
 
-__global__ void __launch_bounds__(kBlock) k_save_pos(uint64_t n, AtomCols c, double* lbx,
-                                                     double* lby, double* lbz) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        lbx[i] = c.x[i];
-        lby[i] = c.y[i];
-        lbz[i] = c.z[i];
-    }
-}
-
-void launch_save_positions(cudaStream_t st, uint64_t n, const AtomCols& c, double* lbx,
-                           double* lby, double* lbz) {
-    if (n == 0) return;
-    note_launch();
-    k_save_pos<<<grid_wave<k_save_pos>(n), kBlock, 0, st>>>(n, c, lbx, lby, lbz);
-}
-
 }  // namespace soil
 
 namespace soil {

@@ -137,9 +137,6 @@ void launch_deinterleave_w(cudaStream_t st, uint64_t n, int w, const double* src
                            uint64_t cap);
 void launch_interleave_w(cudaStream_t st, uint64_t n, int w, double* dst, const double* src0,
                          uint64_t cap);
-// copy of x,y,z[0,n) (save_build_positions)
-void launch_save_positions(cudaStream_t st, uint64_t n, const AtomCols& c, double* lbx,
-                           double* lby, double* lbz);
 
 // ---- scan (k_scan.cu) -----------------------------------------------------
 // Exclusive scan: out[0..n] with out[n] = total.  `temp` holds
@@ -183,8 +180,10 @@ void launch_segsort_split(cudaStream_t st, uint64_t nseg, const uint32_t* start,
 void launch_in_split(cudaStream_t st, uint64_t nseg, const uint32_t* start, const uint32_t* items,
                      uint32_t* split);
 // dst[k] = src[perm[k]] for every column, k in [0, n)
+// cell_out (optional): cell_out[k] = cell_in[perm[k]] in the same pass.
 void launch_perm_gather(cudaStream_t st, uint64_t n, const uint32_t* perm, const AtomCols& src,
-                        const AtomCols& dst, bool forces = true);
+                        const AtomCols& dst, bool forces = true, const uint32_t* cell_in = nullptr,
+                        uint32_t* cell_out = nullptr);
 // flags->not_identity |= any perm[k] != k
 void launch_identity_check(cudaStream_t st, uint64_t n, const uint32_t* perm, DevFlags* flags);
 // out[k] = cell[perm[k]]
@@ -199,7 +198,7 @@ void launch_permute_u32(cudaStream_t st, uint64_t n, const uint32_t* perm, const
 // (plus the FP32 grid-relative copy spf when spf != nullptr)
 void launch_sorted_views(cudaStream_t st, uint64_t n, const uint32_t* sorted, const AtomCols& c,
                          uint32_t* atom_sorted_idx, double4* sp, float4* spf,
-                         const double origin[3]);
+                         const double origin[3], const BuildPos& bp = BuildPos{});
 
 // ---- ghosts (k_ghost.cu) --------------------------------------------------
 struct BorderDim {

@@ -874,7 +874,6 @@ int phase_sort(soil_sys* s) {
                            s->sort_perm.p);
     counts_consumed(s);
     launch_segsort(s->st, nc, s->cell_start.p, s->sort_perm.p);
-    launch_permute_u32(s->st, nl, s->sort_perm.p, s->sort_cell.p, s->sorted_local_cell.p);
     TRY(check_launch(s));
 
     bool apply = true;
@@ -888,7 +887,8 @@ int phase_sort(soil_sys* s) {
     if (apply) {
         // every column gathered through perm; ghosts (if any) are discarded by
         // the borders that always follows a permutation
-        launch_perm_gather(s->st, nl, s->sort_perm.p, s->A, s->B, !s->forces_dead);
+        launch_perm_gather(s->st, nl, s->sort_perm.p, s->A, s->B, !s->forces_dead,
+                           s->sort_cell.p, s->sorted_local_cell.p);
         if (s->slot_max) {  // slots move with their atoms
             const int o = s->slot_old;
             launch_slot_gather(s->st, nl, s->sort_perm.p, s->slot_max, s->slot_width,
@@ -896,6 +896,9 @@ int phase_sort(soil_sys* s) {
                                s->slot_val[1 - o].p);
             s->slot_old = 1 - o;
         }
+        TRY(check_launch(s));
+    } else {
+        launch_permute_u32(s->st, nl, s->sort_perm.p, s->sort_cell.p, s->sorted_local_cell.p);
         TRY(check_launch(s));
     }
     sort_done(s, apply, periodic_sort);
@@ -1364,7 +1367,6 @@ int phase_neighbor(soil_sys* s) {
     const uint64_t nl = s->nlocal, total = s->nlocal + s->nghost;
     const uint64_t nc = s->total_cells;
     const bool fp32 = s->filter == SOIL_FILTER_FP32_RECHECK;
-    launch_save_positions(s->st, nl, s->A, s->lbx.p, s->lby.p, s->lbz.p);
     TRY(counts_zero(s, nc));
     const Grid gr = grid_of(s);
     if (s->local_cells_valid)  // reuse the sort's local cells (neighbor.rs:1049-1066)
@@ -1378,8 +1380,13 @@ int phase_neighbor(soil_sys* s) {
                            s->sorted_atoms.p);
     counts_consumed(s);
     launch_segsort(s->st, nc, s->cell_start.p, s->sorted_atoms.p);
+    BuildPos bpos;  // save_build_positions (neighbor.rs:669-690) in the same pass
+    bpos.x = s->lbx.p;
+    bpos.y = s->lby.p;
+    bpos.z = s->lbz.p;
+    bpos.nlocal = nl;
     launch_sorted_views(s->st, total, s->sorted_atoms.p, s->A, s->asi.p, s->sp.p,
-                        fp32 ? s->spf.p : nullptr, s->blo);
+                        fp32 ? s->spf.p : nullptr, s->blo, bpos);
     const std::vector<int32_t>& sten = s->newton ? s->stencil_fwd : s->stencil;
     const std::vector<int32_t> runs = stencil_runs(sten, s->newton);
     const int32_t* old_stencil = s->d_stencil.p;

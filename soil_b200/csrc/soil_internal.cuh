@@ -112,6 +112,15 @@ struct AtomCols {
     const double* pkrad;
 };
 
+// Where a pass over the atoms also saves the locals' build positions
+// (save_build_positions; x == nullptr: not in this pass).
+struct BuildPos {
+    double* x = nullptr;
+    double* y = nullptr;
+    double* z = nullptr;
+    uint64_t nlocal = 0;
+};
+
 // Per-swap constants of the ghost maps (SwapData, comm.rs:114-124).
 struct SwapConst {
     double off[kNumSwaps][3];
