@@ -376,7 +376,6 @@ __device__ __forceinline__ PairParams pair_params(const BoxDev& D, const BoxStep
     p.in_start = nullptr;
     p.in_list = nullptr;
     p.pre_ranges = S.pre_ranges;
-    p.warp_rows = 0;
     return p;
 }
 

@@ -21,7 +21,6 @@
 // only REJECTS candidates provably outside the cutoff — the margin eps bounds
 // the float rounding of coordinates, differences and squares — followed by
 // the exact FP64 test on the rest, so the lists are identical in both modes.
-#include "border_ops.cuh"
 #include "device_ops.cuh"
 #include "kernels.cuh"
 
@@ -107,137 +106,12 @@ __global__ void __launch_bounds__(kBlock) k_pairs_fill(PairParams p, const uint3
     }
 }
 
-// Pass 1 with the warp's 32 rows tested together (FP64 filter; stencils of
-// at most kPreRanges - 1 runs).  Each lane holds its row's ranges (as
-// row_scan_pre: the own range, merged with a first run at +1 with newton,
-// then the runs).  Range by range, the warp lays its rows' candidates end to
-// end (row after row, each in slot order) and tests them 32 at a time, every
-// lane busy: lane l takes item base + l, finds its row by a search over the
-// rows' item offsets, and tests that row's record (from the row's lane)
-// against the candidate's.  A row's accepted entries are appended in item
-// order, so each row is the same sequence as row_scan gives: its own range,
-// then the runs in stencil order, each in slot order.
-template <bool UNIFORM>
-__global__ void __launch_bounds__(kBlock) k_pairs_warp(PairParams p, uint32_t* rowcount,
-                                                       uint32_t* slots, DevFlags* flags) {
-    const Filter<UNIFORM, false> test(p);
-    const uint32_t K = (uint32_t)p.row_slots;
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint64_t ntiles = (p.nlocal + 31) / 32;
-    const uint64_t nwarps = (uint64_t)gridDim.x * (kBlock / 32);
-    uint64_t n_cand = 0;
-    for (uint64_t w = ((uint64_t)blockIdx.x * kBlock + threadIdx.x) / 32; w < ntiles; w += nwarps) {
-        const uint64_t i = w * 32 + lane;
-        const bool valid = i < p.nlocal;
-        uint32_t my_cell = 0, mi = 0;
-        double4 pi = make_double4(0.0, 0.0, 0.0, 0.0);
-        uint32_t rm[kPreRanges], re[kPreRanges];
-#pragma unroll
-        for (int k = 0; k < kPreRanges; ++k) {
-            rm[k] = 0;
-            re[k] = 0;
-        }
-        if (valid) {
-            my_cell = p.atom_cell[i];
-            mi = p.atom_sorted_idx[i];
-            pi = ld_rec(p.sp + mi);
-            int first = 0;
-            if (p.has_self) {
-                uint64_t ce = (uint64_t)my_cell + 1;
-                if (p.newton && p.nstencil > 0 && p.stencil[0] == 1 &&
-                    ce + (uint64_t)p.stencil[1] <= p.ncells) {
-                    ce += (uint64_t)p.stencil[1];
-                    first = 1;
-                }
-                rm[0] = p.newton ? mi + 1 : p.bin_start[my_cell];
-                re[0] = p.bin_start[ce];
-            }
-#pragma unroll
-            for (int k = 1; k < kPreRanges; ++k) {
-                const int s = first + k - 1;
-                if (s < p.nstencil) {
-                    const int64_t c0 = (int64_t)my_cell + p.stencil[2 * s];
-                    const int64_t c1 = c0 + p.stencil[2 * s + 1];
-                    if (c0 < 0 || c1 > (int64_t)p.ncells) {  // unreachable with the ghost layers
-                        atomicOr(&flags->error, 1u);
-                    } else {
-                        rm[k] = p.bin_start[c0];
-                        re[k] = p.bin_start[c1];
-                    }
-                }
-            }
-        }
-        const bool skip_i = valid && p.has_self && !p.newton;  // i is in its own range
-        uint32_t cnt = 0;
-#pragma unroll
-        for (int k = 0; k < kPreRanges; ++k) {
-            const uint32_t L = re[k] - rm[k];
-            n_cand += L;
-            const uint32_t P = warp_exclusive_sum(L, lane);
-            const uint32_t T = __shfl_sync(0xffffffffu, P + L, 31);
-            const uint32_t m0 = rm[k];
-            for (uint32_t base = 0; base < T; base += 32) {
-                const uint32_t item = base + lane;
-                const bool active = item < T;
-                // the row of this item: the last lane whose offset is <= item
-                uint32_t row = 0;
-#pragma unroll
-                for (uint32_t step = 16; step > 0; step >>= 1)
-                    if (__shfl_sync(0xffffffffu, P, row + step) <= item) row += step;
-                const uint32_t prow = __shfl_sync(0xffffffffu, P, row);
-                const uint32_t slot = __shfl_sync(0xffffffffu, m0, row) + (item - prow);
-                double4 prec;
-                prec.x = __shfl_sync(0xffffffffu, pi.x, row);
-                prec.y = __shfl_sync(0xffffffffu, pi.y, row);
-                prec.z = __shfl_sync(0xffffffffu, pi.z, row);
-                prec.w = __shfl_sync(0xffffffffu, pi.w, row);
-                // without newton the own range holds the row's own atom: not a candidate
-                const uint32_t mrow =
-                    k == 0 ? __shfl_sync(0xffffffffu, skip_i ? mi : 0xffffffffu, row) : 0xffffffffu;
-                bool ok = false;
-                if (active && slot != mrow) ok = test.test64(prec, ld_rec(p.sp + slot));
-                const unsigned bal = __ballot_sync(0xffffffffu, ok);
-                // rank among this row's accepted items of the chunk
-                const uint32_t row_lo = prow > base ? prow - base : 0u;
-                const unsigned below = (1u << lane) - 1u;
-                const unsigned row_below = below & ~((1u << row_lo) - 1u);
-                const uint32_t pos = __shfl_sync(0xffffffffu, cnt, row) + __popc(bal & row_below);
-                if (ok) {
-                    const uint32_t a = p.sorted_atoms[slot];
-                    if (p.in_count) atomicAdd(&p.in_count[a], 1u);
-                    if (pos < K) slots[(w * 32 + row) * K + pos] = a;
-                }
-                // each row counts its accepted items of the chunk
-                const int64_t lo = (int64_t)P - (int64_t)base, hi = lo + (int64_t)L;
-                const uint32_t l0 = lo < 0 ? 0u : lo > 32 ? 32u : (uint32_t)lo;
-                const uint32_t l1 = hi < 0 ? 0u : hi > 32 ? 32u : (uint32_t)hi;
-                const unsigned mine = l1 > l0 ? (l1 - l0 == 32 ? 0xffffffffu
-                                                               : ((1u << (l1 - l0)) - 1u) << l0)
-                                              : 0u;
-                cnt += __popc(bal & mine);
-            }
-        }
-        if (valid) rowcount[i] = cnt;
-        if (skip_i) n_cand -= 1;
-    }
-    __shared__ unsigned long long s_cand;
-    if (threadIdx.x == 0) s_cand = 0;
-    __syncthreads();
-    for (int o = 16; o > 0; o >>= 1) n_cand += __shfl_down_sync(0xffffffffu, n_cand, o);
-    if (lane == 0) atomicAdd(&s_cand, (unsigned long long)n_cand);
-    __syncthreads();
-    if (threadIdx.x == 0) atomicAdd((unsigned long long*)&flags->candidates, s_cand);
-}
-
 template <bool UNIFORM, bool FP32>
 static void launch_pairs_t(cudaStream_t st, const PairParams& p, uint32_t* rowcount,
                            uint32_t* slots, const uint32_t* offsets, uint32_t* indices,
                            DevFlags* flags, bool fill) {
     note_launch();
-    if (!fill && !FP32 && p.warp_rows && p.nstencil < kPreRanges)
-        k_pairs_warp<UNIFORM><<<grid_wave<k_pairs_warp<UNIFORM>>(p.nlocal), kBlock, 0, st>>>(
-            p, rowcount, slots, flags);
-    else if (!fill)
+    if (!fill)
         k_pairs_rows<UNIFORM, FP32><<<grid_wave<k_pairs_rows<UNIFORM, FP32>>(p.nlocal), kBlock, 0, st>>>(p, rowcount, slots,
                                                                             flags);
     else

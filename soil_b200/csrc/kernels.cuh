@@ -314,7 +314,6 @@ struct PairParams {
     const uint32_t* in_start;
     uint32_t* in_list;
     int pre_ranges;  // row_scan_pre for stencils of few runs (SOIL_PAIRS_PRE, default on)
-    int warp_rows;   // pass 1 by k_pairs_warp (SOIL_PAIRS_WARP)
 };
 // Pass 1: row lengths into rowcount[], the first K entries of each row into
 // slots[i*K ...]; filter statistics into flags.

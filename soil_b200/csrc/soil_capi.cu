@@ -335,11 +335,6 @@ int scan_1p(soil_sys* s, const uint32_t* in, uint32_t* out, uint64_t n) {
     return SOIL_OK;
 }
 
-int pairs_warp_rows() {
-    const char* env = std::getenv("SOIL_PAIRS_WARP");
-    return env && std::atoi(env) == 1 ? 1 : 0;
-}
-
 int pairs_pre_ranges() {
     const char* env = std::getenv("SOIL_PAIRS_PRE");
     return env && std::atoi(env) == 0 ? 0 : 1;
@@ -1436,7 +1431,6 @@ int phase_neighbor(soil_sys* s) {
     p.in_start = nullptr;
     p.in_list = nullptr;
     p.pre_ranges = pairs_pre_ranges();
-    p.warp_rows = pairs_warp_rows();
     if (with_in) {
         TRY(ensure(s, s->in_count, total + 1, 0, s->acap + 1));
         TRY(ensure(s, s->in_start, total + 2, 0, s->acap + 2));

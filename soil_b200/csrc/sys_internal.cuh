@@ -270,8 +270,6 @@ int counts_zero(soil_sys* s, uint64_t nc);
 std::vector<int32_t> stencil_runs(const std::vector<int32_t>& sten, bool newton);
 // Whether the pair scan preloads its ranges (SOIL_PAIRS_PRE=0: off; read at each call).
 int pairs_pre_ranges();
-// Whether pass 1 of the pair build tests a warp's rows together (SOIL_PAIRS_WARP=1).
-int pairs_warp_rows();
 // exclusive scan of in[0, n) into out[0, n] in one launch, errors into the
 // system's device flags
 int scan_1p(soil_sys* s, const uint32_t* in, uint32_t* out, uint64_t n);
