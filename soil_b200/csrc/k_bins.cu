@@ -15,7 +15,12 @@
 namespace soil {
 
 __global__ void __launch_bounds__(kBlock) k_cells(uint64_t first, uint64_t n, AtomCols c, Grid gr,
-                                                  uint32_t* cell_out, uint32_t* counts) {
+                                                  uint32_t* cell_out, uint32_t* counts,
+                                                  const uint32_t* n_dev) {
+    if (n_dev) {  // the count known only on the device (an upper bound in n)
+        const uint64_t d = *n_dev;
+        n = d < n ? d : n;
+    }
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
         const uint64_t i = i0 + threadIdx.x;
@@ -31,10 +36,10 @@ __global__ void __launch_bounds__(kBlock) k_cells(uint64_t first, uint64_t n, At
 }
 
 void launch_cells(cudaStream_t st, uint64_t first, uint64_t n, const AtomCols& c, const Grid& gr,
-                  uint32_t* cell_out, uint32_t* counts) {
+                  uint32_t* cell_out, uint32_t* counts, const uint32_t* n_dev) {
     if (n == 0) return;
     note_launch();
-    k_cells<<<grid_wave<k_cells>(n), kBlock, 0, st>>>(first, n, c, gr, cell_out, counts);
+    k_cells<<<grid_wave<k_cells>(n), kBlock, 0, st>>>(first, n, c, gr, cell_out, counts, n_dev);
 }
 
 __global__ void __launch_bounds__(kBlock) k_count_cells(uint64_t n, const uint32_t* cell,
@@ -83,7 +88,12 @@ void launch_scatter(cudaStream_t st, uint64_t n, const uint32_t* cell, uint32_t*
 // the segment sort that follows.
 __global__ void __launch_bounds__(kBlock) k_scatter_consume(uint64_t n, const uint32_t* cell,
                                                             const uint32_t* start,
-                                                            uint32_t* counts, uint32_t* out) {
+                                                            uint32_t* counts, uint32_t* out,
+                                                            const uint32_t* n_dev) {
+    if (n_dev) {  // the count known only on the device (an upper bound in n)
+        const uint64_t d = *n_dev;
+        n = d < n ? d : n;
+    }
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
         const uint64_t i = i0 + threadIdx.x;
@@ -101,17 +111,24 @@ __global__ void __launch_bounds__(kBlock) k_scatter_consume(uint64_t n, const ui
 }
 
 void launch_scatter_consume(cudaStream_t st, uint64_t n, const uint32_t* cell,
-                            const uint32_t* start, uint32_t* counts, uint32_t* out) {
+                            const uint32_t* start, uint32_t* counts, uint32_t* out,
+                            const uint32_t* n_dev) {
     if (n == 0) return;
     note_launch();
-    k_scatter_consume<<<grid_wave<k_scatter_consume>(n), kBlock, 0, st>>>(n, cell, start, counts, out);
+    k_scatter_consume<<<grid_wave<k_scatter_consume>(n), kBlock, 0, st>>>(n, cell, start, counts,
+                                                                          out, n_dev);
 }
 
 // The neighbor build's cells in one pass: the locals' cells from the sort
 // (local < nlocal), the others' from their positions; all counted.
 __global__ void __launch_bounds__(kBlock) k_cells_reuse(uint64_t nlocal, uint64_t n, AtomCols c,
                                                         Grid gr, const uint32_t* local_cell,
-                                                        uint32_t* cell_out, uint32_t* counts) {
+                                                        uint32_t* cell_out, uint32_t* counts,
+                                                        const uint32_t* n_dev) {
+    if (n_dev) {  // the count known only on the device (an upper bound in n)
+        const uint64_t d = *n_dev;
+        n = d < n ? d : n;
+    }
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
         const uint64_t i = i0 + threadIdx.x;
@@ -127,10 +144,11 @@ __global__ void __launch_bounds__(kBlock) k_cells_reuse(uint64_t nlocal, uint64_
 
 void launch_cells_reuse(cudaStream_t st, uint64_t nlocal, uint64_t n, const AtomCols& c,
                         const Grid& gr, const uint32_t* local_cell, uint32_t* cell_out,
-                        uint32_t* counts) {
+                        uint32_t* counts, const uint32_t* n_dev) {
     if (n == 0) return;
     note_launch();
-    k_cells_reuse<<<grid_wave<k_cells_reuse>(n), kBlock, 0, st>>>(nlocal, n, c, gr, local_cell, cell_out, counts);
+    k_cells_reuse<<<grid_wave<k_cells_reuse>(n), kBlock, 0, st>>>(nlocal, n, c, gr, local_cell,
+                                                                  cell_out, counts, n_dev);
 }
 
 // Restore the stable (ascending index) order inside every segment.
@@ -246,7 +264,12 @@ void launch_permute_u32(cudaStream_t st, uint64_t n, const uint32_t* perm, const
 __global__ void __launch_bounds__(kBlock) k_sorted_views(uint64_t n, const uint32_t* sorted,
                                                          AtomCols c, uint32_t* asi, double4* sp,
                                                          float4* spf, double o0, double o1,
-                                                         double o2, BuildPos bp) {
+                                                         double o2, BuildPos bp,
+                                                         const uint32_t* n_dev) {
+    if (n_dev) {  // the count known only on the device (an upper bound in n)
+        const uint64_t d = *n_dev;
+        n = d < n ? d : n;
+    }
     for (uint64_t m = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; m < n;
          m += (uint64_t)gridDim.x * blockDim.x)
         sorted_view(c, m, sorted, asi, sp, spf, o0, o1, o2, bp);
@@ -254,11 +277,11 @@ __global__ void __launch_bounds__(kBlock) k_sorted_views(uint64_t n, const uint3
 
 void launch_sorted_views(cudaStream_t st, uint64_t n, const uint32_t* sorted, const AtomCols& c,
                          uint32_t* atom_sorted_idx, double4* sp, float4* spf,
-                         const double origin[3], const BuildPos& bp) {
+                         const double origin[3], const BuildPos& bp, const uint32_t* n_dev) {
     if (n == 0) return;
     note_launch();
     k_sorted_views<<<grid_wave<k_sorted_views>(n), kBlock, 0, st>>>(
-        n, sorted, c, atom_sorted_idx, sp, spf, origin[0], origin[1], origin[2], bp);
+        n, sorted, c, atom_sorted_idx, sp, spf, origin[0], origin[1], origin[2], bp, n_dev);
 }
 
 }  // namespace soil

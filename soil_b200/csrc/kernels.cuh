@@ -155,8 +155,10 @@ void exclusive_scan_1p(cudaStream_t st, const uint32_t* in, uint32_t* out, uint6
 
 // ---- bins (k_bins.cu) -----------------------------------------------------
 // cell[i] = cell_of(pos[first+i]) and counts[cell]++ for i in [0, n)
+// n_dev (optional, here and below): the count is min(n, *n_dev), read on the
+// device (n an upper bound), for launches queued before the host knows it.
 void launch_cells(cudaStream_t st, uint64_t first, uint64_t n, const AtomCols& c, const Grid& gr,
-                  uint32_t* cell_out, uint32_t* counts);
+                  uint32_t* cell_out, uint32_t* counts, const uint32_t* n_dev = nullptr);
 // counts[cell[i]]++ for i in [0, n) (cells already known)
 void launch_count_cells(cudaStream_t st, uint64_t n, const uint32_t* cell, uint32_t* counts);
 // out[cursor[cell[i]]++] = i (unordered within a cell)
@@ -165,12 +167,13 @@ void launch_scatter(cudaStream_t st, uint64_t n, const uint32_t* cell, uint32_t*
 // out[start[c] + --counts[c]] = i for c = cell[i] (unordered within a cell);
 // leaves every count at zero
 void launch_scatter_consume(cudaStream_t st, uint64_t n, const uint32_t* cell,
-                            const uint32_t* start, uint32_t* counts, uint32_t* out);
+                            const uint32_t* start, uint32_t* counts, uint32_t* out,
+                            const uint32_t* n_dev = nullptr);
 // cell_out[i] = local_cell[i] (i < nlocal) or the cell of atom i, counted,
 // i in [0, n)
 void launch_cells_reuse(cudaStream_t st, uint64_t nlocal, uint64_t n, const AtomCols& c,
                         const Grid& gr, const uint32_t* local_cell, uint32_t* cell_out,
-                        uint32_t* counts);
+                        uint32_t* counts, const uint32_t* n_dev = nullptr);
 // sort every segment [start[s], start[s+1]) ascending -> stable counting sort
 void launch_segsort(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint32_t* items);
 // the same, and split[s] = entries of segment s below s (transposed lists)
@@ -198,7 +201,8 @@ void launch_permute_u32(cudaStream_t st, uint64_t n, const uint32_t* perm, const
 // (plus the FP32 grid-relative copy spf when spf != nullptr)
 void launch_sorted_views(cudaStream_t st, uint64_t n, const uint32_t* sorted, const AtomCols& c,
                          uint32_t* atom_sorted_idx, double4* sp, float4* spf,
-                         const double origin[3], const BuildPos& bp = BuildPos{});
+                         const double origin[3], const BuildPos& bp = BuildPos{},
+                         const uint32_t* n_dev = nullptr);
 
 // ---- ghosts (k_ghost.cu) --------------------------------------------------
 struct BorderDim {

@@ -905,11 +905,18 @@ int phase_sort(soil_sys* s) {
     return SOIL_OK;
 }
 
-int phase_borders(soil_sys* s) {
-    // borders, comm.rs:682-860 (single rank: all six swaps are self-sends).
-    // All three dims run on the device back to back; the host reads the swap
-    // totals once at the end.  If the ghosts did not fit, the arrays grow and
-    // the (deterministic) pass is repeated.
+int phase_borders_defer(soil_sys* s, bool defer);
+int phase_borders(soil_sys* s) { return phase_borders_defer(s, false); }
+
+// borders, comm.rs:682-860 (single rank: all six swaps are self-sends).
+// All three dims run on the device back to back; the host reads the swap
+// totals once at the end.  If the ghosts did not fit, the arrays grow and the
+// (deterministic) pass is repeated.  With `defer` (a fully periodic box, in a
+// step whose neighbor build follows at once) the host does not wait: the
+// totals are copied back behind the pass and read at the neighbor build's own
+// synchronisation (borders_pending), whose kernels take the atom count from
+// the device until then.
+int phase_borders_defer(soil_sys* s, bool defer) {
     if (s->state != FULL_REBUILD) return SOIL_OK;
     s->pk_valid = false;
     s->view_out = false;  // views are valid until the next rebuild
@@ -917,9 +924,10 @@ int phase_borders(soil_sys* s) {
     BorderDim bds[3];
     border_setup(s, bds);
     TRY(borders_reserve(s));
-    uint32_t* hb = s->hword;
-    const BorderPass bp = border_pass(bds);
     const int mask = pbc_mask(s);
+    defer = defer && mask == 7;
+    uint32_t* hb = defer ? s->hword + kBorderStateWords : s->hword;
+    const BorderPass bp = border_pass(bds);
     unsigned periodic_swaps = 0;
     for (int d = 0; d < 3; ++d)
         if (mask & (1 << d)) periodic_swaps |= 3u << (2 * d);
@@ -935,6 +943,11 @@ int phase_borders(soil_sys* s) {
                        s->fold_start.p, s->fold_list.p);
         TRY(check_launch(s));
         CK(cudaMemcpyAsync(hb, s->bstate.p, kBorderStateWords * 4, cudaMemcpyDeviceToHost, s->st));
+        if (defer) {
+            for (int d = 0; d < 3; ++d) s->pending_bds[d] = bds[d];
+            s->borders_pending = true;
+            return SOIL_OK;
+        }
         TRY(sync(s));
         if (!hb[10]) break;
         if (attempt == 3) return fail(s->ctx, SOIL_ERR_CAPACITY, "ghost capacity did not converge");
@@ -1364,20 +1377,25 @@ float pair_eps(const soil_sys* s) {
 int phase_neighbor(soil_sys* s) {
     if (s->state != FULL_REBUILD) return SOIL_OK;
     TRY(neighbor_plan(s));
-    const uint64_t nl = s->nlocal, total = s->nlocal + s->nghost;
+    const uint64_t nl = s->nlocal;
+    // Until a deferred border pass is read back, the atom count is the
+    // device's (bstate word 3) and `total` the capacity that bounds it.
+    const bool pend = s->borders_pending;
+    uint64_t total = pend ? s->acap : s->nlocal + s->nghost;
+    const uint32_t* n_dev = pend ? s->bstate.p + 3 : nullptr;
     const uint64_t nc = s->total_cells;
     const bool fp32 = s->filter == SOIL_FILTER_FP32_RECHECK;
     TRY(counts_zero(s, nc));
     const Grid gr = grid_of(s);
     if (s->local_cells_valid)  // reuse the sort's local cells (neighbor.rs:1049-1066)
         launch_cells_reuse(s->st, nl, total, s->A, gr, s->sorted_local_cell.p, s->atom_cell.p,
-                           s->cell_counts.p);
+                           s->cell_counts.p, n_dev);
     else
-        launch_cells(s->st, 0, total, s->A, gr, s->atom_cell.p, s->cell_counts.p);
+        launch_cells(s->st, 0, total, s->A, gr, s->atom_cell.p, s->cell_counts.p, n_dev);
     s->local_cells_valid = false;
     TRY(scan_1p(s, s->cell_counts.p, s->cell_start.p, nc));
     launch_scatter_consume(s->st, total, s->atom_cell.p, s->cell_start.p, s->cell_counts.p,
-                           s->sorted_atoms.p);
+                           s->sorted_atoms.p, n_dev);
     counts_consumed(s);
     launch_segsort(s->st, nc, s->cell_start.p, s->sorted_atoms.p);
     BuildPos bpos;  // save_build_positions (neighbor.rs:669-690) in the same pass
@@ -1386,7 +1404,7 @@ int phase_neighbor(soil_sys* s) {
     bpos.z = s->lbz.p;
     bpos.nlocal = nl;
     launch_sorted_views(s->st, total, s->sorted_atoms.p, s->A, s->asi.p, s->sp.p,
-                        fp32 ? s->spf.p : nullptr, s->blo, bpos);
+                        fp32 ? s->spf.p : nullptr, s->blo, bpos, n_dev);
     const std::vector<int32_t>& sten = s->newton ? s->stencil_fwd : s->stencil;
     const std::vector<int32_t> runs = stencil_runs(sten, s->newton);
     const int32_t* old_stencil = s->d_stencil.p;
@@ -1447,6 +1465,20 @@ int phase_neighbor(soil_sys* s) {
     CK(cudaMemcpyAsync(&s->hword[0], s->offsets.p + nl, 4, cudaMemcpyDeviceToHost, s->st));
     TRY(check_launch(s));
     TRY(read_flags(s));
+    if (pend) {  // the deferred border pass, now read back
+        s->borders_pending = false;
+        const uint32_t* hb = s->hword + kBorderStateWords;
+        if (hb[10]) {
+            // The ghosts did not fit: grow, then repeat the border pass and
+            // this build with the host reading the ghost counts first.
+            TRY(grow_atoms(s, (uint64_t)hb[3] + 1024, s->nlocal));
+            s->state = FULL_REBUILD;
+            TRY(phase_borders_defer(s, false));
+            return phase_neighbor(s);
+        }
+        TRY(borders_done(s, hb, s->pending_bds));
+        total = s->nlocal + s->nghost;
+    }
     const uint64_t np = s->hword[0];
     TRY(ensure(s, s->indices, np + 1, 0, pair_room(np)));
     if (s->hflags->error & SOIL_PAIRS_ERR_STAGING)
@@ -1671,7 +1703,7 @@ int step_rest(soil_sys* s, const StepPlan& p, bool last) {
     TRY(sorted);
     timer_end(s, T_SORT);
     timer_begin(s, T_BORDERS);
-    TRY(phase_borders(s));
+    TRY(phase_borders_defer(s, true));  // read back at the neighbor build's synchronisation
     timer_end(s, T_BORDERS);
     timer_begin(s, T_FORWARD);
     if (s->state == COMMUNICATE_ONLY && !p.fwd_fused) TRY(forward_comm(s, p.fused_zero));
@@ -1973,7 +2005,7 @@ int soil_sys_create(soil_ctx* ctx, const soil_box* box, const soil_neigh_cfg* cf
     int r;
     if ((r = dev_alloc(s, (void**)&s->dflags, sizeof(DevFlags))) != SOIL_OK ||
         cudaMallocHost((void**)&s->hflags, sizeof(DevFlags)) != cudaSuccess ||
-        cudaMallocHost((void**)&s->hword, kBorderStateWords * 4) != cudaSuccess) {
+        cudaMallocHost((void**)&s->hword, 2 * kBorderStateWords * 4) != cudaSuccess) {
         cudaGetLastError();
         soil_sys_destroy(s);
         return r != SOIL_OK ? r : fail(ctx, SOIL_ERR_OOM, "pinned allocation failed");

@@ -149,6 +149,10 @@ struct soil_sys {
     bool pk_valid = false;
     bool view_out = false;  // a device view was handed out since the last rebuild
     bool forces_dead = false;  // inside a step whose consumer overwrites every force
+    // a border pass whose totals (hword + kBorderStateWords) are read back at
+    // the following neighbor build's synchronisation, and its dims
+    bool borders_pending = false;
+    BorderDim pending_bds[3];
     // grouped partner sequences of the built-in consumer (rebuilt with the
     // lists): per-atom lengths, per-root group lengths and starts, entries
     DArr<uint32_t> seq_cnt, grp_cnt, grp_start, seq;
