@@ -1559,6 +1559,19 @@ int phase_force(soil_sys* s) {
     return launch_consumer(s, false);
 }
 
+// Whether a step's reverse comm can change anything.  Without a consumer or
+// a force hook nothing writes a force after the step's zeroing, so every
+// ghost carries its root's +0 (borders copy it, forward comm zeroes it) and
+// every fold adds +0 to +0; with no #[reverse] column nothing else is
+// folded.  Such a step skips the pass (the per-phase entry point still runs
+// it).
+bool reverse_needed(const soil_sys* s) {
+    if (builtin_consumer(s) || s->hook) return true;
+    int rp[kMaxPlanes], nr;
+    zero_planes_of(s, SOIL_COL_REVERSE, rp, &nr);
+    return nr > 0;
+}
+
 int phase_reverse_comm(soil_sys* s) {
     // reverse_send_force, comm.rs:938-1024: rounds last to first, lo then hi;
     // each root's image tree in fold order, over the roots that have images
@@ -1724,7 +1737,7 @@ int step_rest(soil_sys* s, const StepPlan& p, bool last) {
     }
     timer_end(s, T_FORCE);
     timer_begin(s, T_REVERSE);
-    if (!fold_fused) TRY(phase_reverse_comm(s));
+    if (!fold_fused && reverse_needed(s)) TRY(phase_reverse_comm(s));
     timer_end(s, T_REVERSE);
     if (last) {
         timer_begin(s, T_FINAL);
