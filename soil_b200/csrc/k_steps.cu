@@ -24,8 +24,6 @@
 // and returns; the others then run out at their next barrier.  Co-residency
 // of every CTA is guaranteed by the cooperative launch, so the bound is a
 // guard, never the expected exit.
-#include <cstdlib>
-
 #include <cuda/atomic>
 
 #include "device_ops.cuh"
@@ -187,13 +185,10 @@ int steps_grid(int consumer, int walk, bool pk, uint64_t nlocal, int* grid) {
     const uint64_t need_tiles = ((nlocal + 31) / 32 + kForceWarps - 1) / kForceWarps;
     uint64_t need = need_atoms > need_tiles ? need_atoms : need_tiles;
     if (need < 1) need = 1;
-    uint64_t cap = (uint64_t)per_sm * (uint64_t)sms;
-    // SOIL_STEPS_CTAS (measurement): at most this many CTAs, each striding
-    // over more atoms, so fewer of them meet at every grid barrier
-    if (const char* env = std::getenv("SOIL_STEPS_CTAS")) {
-        const uint64_t m = std::strtoull(env, nullptr, 10);
-        if (m >= 1 && m < cap) cap = m;
-    }
+    // one CTA per kBlock atoms (capped at residency): fewer CTAs striding over
+    // more atoms each measured slower (32 CTAs: 19.6 vs 13.2 us per light step
+    // on 32,768 atoms)
+    const uint64_t cap = (uint64_t)per_sm * (uint64_t)sms;
     *grid = (int)(need < cap ? need : cap);
     return 0;
 }
