@@ -918,6 +918,7 @@ int phase_borders(soil_sys* s) { return phase_borders_defer(s, false); }
 // the device until then.
 int phase_borders_defer(soil_sys* s, bool defer) {
     if (s->state != FULL_REBUILD) return SOIL_OK;
+    s->borders_pending = false;  // a pass left pending by a failed step is replaced
     s->pk_valid = false;
     s->view_out = false;  // views are valid until the next rebuild
     s->nghost = 0;
