@@ -62,6 +62,12 @@ __device__ __forceinline__ void for_span(const Span& sp, F f) {
 
 static unsigned span_grid(const Span& sp) { return grid_for((sp.total + kSpanItems - 1) / kSpanItems); }
 
+// One resident wave of span kernel K (grid_wave), never more than the span needs.
+template <auto K>
+static unsigned span_wave(const Span& sp) {
+    return grid_wave<K>((sp.total + kSpanItems - 1) / kSpanItems);
+}
+
 #define SPAN_KERNEL(name, ...)                                                        \
     __global__ void __launch_bounds__(kBlock) name(Span sp, BatchArgs A) {            \
         for_span(sp, [&](uint32_t b, uint64_t i, uint32_t k) {                        \
@@ -78,7 +84,7 @@ static unsigned span_grid(const Span& sp) { return grid_for((sp.total + kSpanIte
     void fn(cudaStream_t st, const Span& sp, const BatchArgs& a) {   \
         if (sp.total == 0) return;                                   \
         note_launch();                                               \
-        kern<<<span_grid(sp), kBlock, 0, st>>>(sp, a);               \
+        kern<<<span_wave<kern>(sp), kBlock, 0, st>>>(sp, a);         \
     }
 
 // ---- integrate --------------------------------------------------------------
@@ -130,7 +136,7 @@ __global__ void __launch_bounds__(kBlock) kb_zero_counts(Span sp, BatchArgs A, i
 void b_zero_counts(cudaStream_t st, const Span& sp, const BatchArgs& a, int which) {
     if (sp.total == 0) return;
     note_launch();
-    kb_zero_counts<<<span_grid(sp), kBlock, 0, st>>>(sp, a, which);
+    kb_zero_counts<<<span_wave<kb_zero_counts>(sp), kBlock, 0, st>>>(sp, a, which);
 }
 
 __global__ void __launch_bounds__(kBlock) kb_cells(Span sp, BatchArgs A, int neighbor) {
@@ -146,7 +152,7 @@ __global__ void __launch_bounds__(kBlock) kb_cells(Span sp, BatchArgs A, int nei
 void b_cells(cudaStream_t st, const Span& sp, const BatchArgs& a, bool neighbor) {
     if (sp.total == 0) return;
     note_launch();
-    kb_cells<<<span_grid(sp), kBlock, 0, st>>>(sp, a, neighbor ? 1 : 0);
+    kb_cells<<<span_wave<kb_cells>(sp), kBlock, 0, st>>>(sp, a, neighbor ? 1 : 0);
 }
 
 SPAN_KERNEL(kb_copy_count_local_cells, {
@@ -237,7 +243,7 @@ __global__ void __launch_bounds__(kBlock) kb_scatter(Span sp, BatchArgs A, int n
 void b_scatter(cudaStream_t st, const Span& sp, const BatchArgs& a, bool neighbor) {
     if (sp.total == 0) return;
     note_launch();
-    kb_scatter<<<span_grid(sp), kBlock, 0, st>>>(sp, a, neighbor ? 1 : 0);
+    kb_scatter<<<span_wave<kb_scatter>(sp), kBlock, 0, st>>>(sp, a, neighbor ? 1 : 0);
 }
 
 __global__ void __launch_bounds__(kBlock) kb_segsort(Span sp, BatchArgs A, int which) {
@@ -251,7 +257,7 @@ __global__ void __launch_bounds__(kBlock) kb_segsort(Span sp, BatchArgs A, int w
 void b_segsort(cudaStream_t st, const Span& sp, const BatchArgs& a, int which) {
     if (sp.total == 0) return;
     note_launch();
-    kb_segsort<<<span_grid(sp), kBlock, 0, st>>>(sp, a, which);
+    kb_segsort<<<span_wave<kb_segsort>(sp), kBlock, 0, st>>>(sp, a, which);
 }
 
 SPAN_KERNEL(kb_permute_cells, { D.sorted_local_cell[i] = D.sort_cell[D.sort_perm[i]]; })
@@ -291,7 +297,7 @@ __global__ void __launch_bounds__(kBlock) kb_border_faces(Span sp, BatchArgs A, 
 void b_border_faces(cudaStream_t st, const Span& sp, const BatchArgs& a) {
     if (sp.total == 0) return;
     note_launch();
-    kb_border_faces<<<grid_for(sp.total * 32), kBlock, 0, st>>>(sp, a, border_cats());
+    kb_border_faces<<<grid_wave<kb_border_faces>(sp.total * 32), kBlock, 0, st>>>(sp, a, border_cats());
 }
 
 // one CTA per (box, category): exclusive scan of the warp counts
@@ -328,7 +334,7 @@ __global__ void __launch_bounds__(kBlock) kb_border_images(Span sp, BatchArgs A,
 void b_border_images(cudaStream_t st, const Span& sp, const BatchArgs& a) {
     if (sp.total == 0) return;
     note_launch();
-    kb_border_images<<<grid_for(sp.total * 32), kBlock, 0, st>>>(sp, a, border_cats());
+    kb_border_images<<<grid_wave<kb_border_images>(sp.total * 32), kBlock, 0, st>>>(sp, a, border_cats());
 }
 
 SPAN_KERNEL(kb_forward, {
