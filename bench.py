@@ -188,30 +188,40 @@ def make_workload(name, filt, natoms=None):
 def rebuild_probe(s, stream, min_rebuilds=3, chunk=25, max_steps=800):
     """Light and rebuild step costs of a system past the timed region.
 
-    Steps it in calls of `chunk` steps, each timed with CUDA events on the
-    library's stream, until at least `min_rebuilds` steps rebuilt the lists;
-    then fits chunk_ms = L * steps + X * rebuilds over the chunks (least
-    squares): L is the light (communicate-only) step, L + X the rebuild step.
+    Steps it in calls of about `chunk` steps (lengths varied), each timed with
+    CUDA events on the library's stream, until at least `min_rebuilds` steps
+    rebuilt the lists and the chunks separate the two costs; then fits
+    chunk_ms = L * steps + X * rebuilds over the chunks (least squares): L is
+    the light (communicate-only) step, L + X the rebuild step.
     Each call ends with the final half-kick (as every soil_step call does),
     so L carries 1/chunk of one final_integration pass."""
     import torch
     rows = []
     steps = rebuilds = 0
-    while steps < max_steps and (rebuilds < min_rebuilds or len(rows) < 3):
+    # chunks of varying length, so that (steps, rebuilds) of the chunks are
+    # not all proportional and the two costs separate
+    lengths = (chunk, chunk // 2 + 1, chunk + chunk // 3, chunk // 3 + 1)
+
+    def rank():
+        return np.linalg.matrix_rank(np.array([[n, r] for n, r, _ in rows], dtype=np.float64))
+
+    while steps < max_steps and (rebuilds < min_rebuilds or len(rows) < 3 or
+                                 (0 < rebuilds < steps and rank() < 2)):
+        n = lengths[len(rows) % len(lengths)]
         r0 = s.counts().rebuilds
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        s.step(chunk)
+        s.step(n)
         e1.record(stream)
         s.sync()
         r = int(s.counts().rebuilds - r0)
-        rows.append((chunk, r, e0.elapsed_time(e1)))
-        steps += chunk
+        rows.append((n, r, e0.elapsed_time(e1)))
+        steps += n
         rebuilds += r
     A = np.array([[n, r] for n, r, _ in rows], dtype=np.float64)
     t = np.array([ms for _, _, ms in rows])
-    out = {"steps": steps, "rebuilds": rebuilds, "chunk_steps": chunk,
+    out = {"steps": steps, "rebuilds": rebuilds, "chunk_steps": list(lengths),
            "rebuild_rate": rebuilds / steps}
     if rebuilds and np.linalg.matrix_rank(A) == 2:
         (light, extra), *_ = np.linalg.lstsq(A, t, rcond=None)
