@@ -190,11 +190,11 @@ def rebuild_probe(s, stream, min_rebuilds=3, chunk=25, max_steps=800):
 
     Steps it in calls of about `chunk` steps (lengths varied), each timed with
     CUDA events on the library's stream, until at least `min_rebuilds` steps
-    rebuilt the lists and the chunks separate the two costs; then fits
-    chunk_ms = L * steps + X * rebuilds over the chunks (least squares): L is
-    the light (communicate-only) step, L + X the rebuild step.
-    Each call ends with the final half-kick (as every soil_step call does),
-    so L carries 1/chunk of one final_integration pass."""
+    rebuilt the lists and the chunks separate the costs; then fits
+    chunk_ms = L * steps + X * rebuilds + C over the chunks (least squares):
+    L is the light (communicate-only) step, L + X the rebuild step, C the
+    per-call cost (each call ends with the final half-kick, as every
+    soil_step call does)."""
     import torch
     rows = []
     steps = rebuilds = 0
@@ -203,10 +203,10 @@ def rebuild_probe(s, stream, min_rebuilds=3, chunk=25, max_steps=800):
     lengths = (chunk, chunk // 2 + 1, chunk + chunk // 3, chunk // 3 + 1)
 
     def rank():
-        return np.linalg.matrix_rank(np.array([[n, r] for n, r, _ in rows], dtype=np.float64))
+        return np.linalg.matrix_rank(np.array([[n, r, 1.0] for n, r, _ in rows]))
 
-    while steps < max_steps and (rebuilds < min_rebuilds or len(rows) < 3 or
-                                 (0 < rebuilds < steps and rank() < 2)):
+    while steps < max_steps and (rebuilds < min_rebuilds or len(rows) < 4 or
+                                 (0 < rebuilds < steps and rank() < 3)):
         n = lengths[len(rows) % len(lengths)]
         r0 = s.counts().rebuilds
         e0 = torch.cuda.Event(enable_timing=True)
@@ -219,12 +219,14 @@ def rebuild_probe(s, stream, min_rebuilds=3, chunk=25, max_steps=800):
         rows.append((n, r, e0.elapsed_time(e1)))
         steps += n
         rebuilds += r
-    A = np.array([[n, r] for n, r, _ in rows], dtype=np.float64)
+    # chunk_ms = L * steps + X * rebuilds + C, C the per-call cost (the
+    # call's closing half-kick and launch latency)
+    A = np.array([[n, r, 1.0] for n, r, _ in rows], dtype=np.float64)
     t = np.array([ms for _, _, ms in rows])
     out = {"steps": steps, "rebuilds": rebuilds, "chunk_steps": list(lengths),
            "rebuild_rate": rebuilds / steps}
-    if rebuilds and np.linalg.matrix_rank(A) == 2:
-        (light, extra), *_ = np.linalg.lstsq(A, t, rcond=None)
+    if rebuilds and np.linalg.matrix_rank(A) == 3:
+        (light, extra, _), *_ = np.linalg.lstsq(A, t, rcond=None)
         out.update(ms_per_light_step=float(light), ms_per_rebuild_step=float(light + extra))
     elif rebuilds == steps:  # every step rebuilds (shear)
         out.update(ms_per_light_step=None, ms_per_rebuild_step=float(t.sum() / steps))

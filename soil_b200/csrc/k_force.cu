@@ -33,7 +33,6 @@
 #include <cstdlib>
 #include <cstring>
 
-#include "border_ops.cuh"
 #include "device_ops.cuh"
 #include "force_ops.cuh"
 #include "kernels.cuh"
@@ -121,94 +120,6 @@ __global__ void __launch_bounds__(kBlock, 4) k_force_csr(ForceCsr q, AtomCols c,
     }
 }
 
-// The CSR walk with a warp's 32 roots evaluated together: each root's own
-// partner sequence (its transposed-list rows below it, its row, the rest;
-// csr_item_force's order) is laid end to end with the other roots', and the
-// warp evaluates 32 entries at a time with every lane busy (lane l takes
-// entry base + l, finds its root by a search over the roots' entry offsets
-// and takes the root's position and list bounds from the root's lane).  Each
-// root's lane then adds the chunk's pair forces of its own entries in entry
-// order, so every root's force is the same left-to-right sum as the walk's.
-// Images (a few per cent of the roots have any) are walked by their root's
-// lane afterwards, then the fold.
-template <bool FOLD>
-__global__ void __launch_bounds__(kBlock, 4) k_force_coop(ForceCsr q, AtomCols c, PlaneList rev) {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint64_t ntiles = (q.nlocal + 31) / 32;
-    const uint64_t nwarps = (uint64_t)gridDim.x * (kBlock / 32);
-    const ColLd ld{c.x, c.y, c.z, q.rad};
-    for (uint64_t w = ((uint64_t)blockIdx.x * kBlock + threadIdx.x) / 32; w < ntiles; w += nwarps) {
-        const uint64_t t = w * 32 + lane;
-        const bool valid = t < q.nlocal;
-        double4 pa = make_double4(0.0, 0.0, 0.0, 0.0);
-        uint32_t qs = 0, npre = 0, rs = 0, nrow = 0, n = 0;
-        if (valid) {
-            pa = ld(t);
-            qs = q.in_start[t];
-            const uint32_t nin = q.in_start[t + 1] - qs;
-            npre = q.in_split[t];
-            rs = q.offsets[t];
-            nrow = q.offsets[t + 1] - rs;
-            n = nin + nrow;
-        }
-        const uint32_t P = warp_exclusive_sum(n, lane);
-        const uint32_t T = __shfl_sync(0xffffffffu, P + n, 31);
-        double Fx = 0.0, Fy = 0.0, Fz = 0.0;
-        for (uint32_t base = 0; base < T; base += 32) {
-            const uint32_t item = base + lane;
-            uint32_t row = 0;  // the last lane whose offset is <= item
-#pragma unroll
-            for (uint32_t step = 16; step > 0; step >>= 1)
-                if (__shfl_sync(0xffffffffu, P, row + step) <= item) row += step;
-            const uint32_t k = item - __shfl_sync(0xffffffffu, P, row);
-            const CsrIdx ix{q.in_list, q.indices, __shfl_sync(0xffffffffu, qs, row),
-                            __shfl_sync(0xffffffffu, npre, row), __shfl_sync(0xffffffffu, rs, row),
-                            __shfl_sync(0xffffffffu, nrow, row)};
-            const double ox = __shfl_sync(0xffffffffu, pa.x, row);
-            const double oy = __shfl_sync(0xffffffffu, pa.y, row);
-            const double oz = __shfl_sync(0xffffffffu, pa.z, row);
-            const double orad = __shfl_sync(0xffffffffu, pa.w, row);
-            double fx = 0.0, fy = 0.0, fz = 0.0;
-            bool hit = false;
-            if (item < T) {
-                const double4 po = ld(ix(k));
-                hit = pair_force(ox, oy, oz, orad, po.x, po.y, po.z, po.w, q.K, fx, fy, fz);
-            }
-            // this lane's root: entries [lo, hi) of the chunk, added in order
-            const int64_t l0 = (int64_t)P - (int64_t)base, l1 = l0 + (int64_t)n;
-            const uint32_t lo = l0 < 0 ? 0u : l0 > 32 ? 32u : (uint32_t)l0;
-            const uint32_t hi = l1 < 0 ? 0u : l1 > 32 ? 32u : (uint32_t)l1;
-            const uint32_t most = __reduce_max_sync(0xffffffffu, hi - lo);
-            for (uint32_t j = 0; j < most; ++j) {
-                const uint32_t src = lo + j < 32u ? lo + j : 31u;
-                const double gx = __shfl_sync(0xffffffffu, fx, src);
-                const double gy = __shfl_sync(0xffffffffu, fy, src);
-                const double gz = __shfl_sync(0xffffffffu, fz, src);
-                const bool gh = __shfl_sync(0xffffffffu, hit ? 1 : 0, src) != 0;
-                if (lo + j < hi && gh) {
-                    Fx = Fx + gx;
-                    Fy = Fy + gy;
-                    Fz = Fz + gz;
-                }
-            }
-        }
-        if (!valid) continue;
-        c.fx[t] = Fx;
-        c.fy[t] = Fy;
-        c.fz[t] = Fz;
-        const uint32_t f0 = q.fold_start[t], f1 = q.fold_start[t + 1];
-        for (uint32_t f = f0; f < f1; ++f) {  // its images, in fold order
-            const uint64_t a = q.nlocal + q.fold_list[f];
-            double Gx, Gy, Gz;
-            csr_item_force(q, ld, a, Gx, Gy, Gz);
-            c.fx[a] = Gx;
-            c.fy[a] = Gy;
-            c.fz[a] = Gz;
-        }
-        if (FOLD) fold_root(c, q.nlocal, t, q.fold_start, q.fold_list, rev);
-    }
-}
-
 // Entries of root t's walk: its and its images' in-lists and its row.
 __device__ __forceinline__ uint32_t csr_work(const ForceCsr& q, uint64_t t) {
     uint32_t n = q.offsets[t + 1] - q.offsets[t] + q.in_start[t + 1] - q.in_start[t];
@@ -262,11 +173,7 @@ void launch_force_csr(cudaStream_t st, const ForceCsr& q, const AtomCols& c, con
     const unsigned full = 148u * 4u;
     const unsigned need = (unsigned)((q.nlocal + kBlock - 1) / kBlock);
     const unsigned grid = need < full ? need : full;
-    const char* coop = std::getenv("SOIL_FORCE_COOP");
-    if (coop && std::atoi(coop) == 1 && !q.pk && !q.order) {
-        if (fold) k_force_coop<true><<<grid_wave<k_force_coop<true>>(q.nlocal), kBlock, 0, st>>>(q, c, rev);
-        else k_force_coop<false><<<grid_wave<k_force_coop<false>>(q.nlocal), kBlock, 0, st>>>(q, c, rev);
-    } else if (q.pk) {
+    if (q.pk) {
         if (fold) k_force_csr<true, true><<<grid, kBlock, 0, st>>>(q, c, rev);
         else k_force_csr<false, true><<<grid, kBlock, 0, st>>>(q, c, rev);
     } else {

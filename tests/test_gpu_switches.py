@@ -1,7 +1,6 @@
 """The rebuild path's speed switches change no result: the pair scan with
 range bounds loaded as it goes (SOIL_PAIRS_PRE=0), the shared-memory staged
-pair count (SOIL_PAIRS_STAGED=1), the CSR walk with a warp's roots
-evaluated together (SOIL_FORCE_COOP=1), and every scan taken by the single-pass
+pair count (SOIL_PAIRS_STAGED=1), and every scan taken by the single-pass
 kernel or by the three-kernel one (SOIL_SCAN1P_MAX), each stepped through
 rebuilds and compared bit for bit with the CPU oracle (state and lists,
 order included)."""
@@ -18,7 +17,6 @@ pytestmark = pytest.mark.gpu
 SETTINGS = {
     "pairs-pre-off": {"SOIL_PAIRS_PRE": "0"},
     "pairs-staged": {"SOIL_PAIRS_STAGED": "1"},
-    "force-coop": {"SOIL_FORCE_COOP": "1", "SOIL_FORCE": "csr", "SOIL_RESIDENT_STEPS": "0"},
     "scan-single-pass-always": {"SOIL_SCAN1P_MAX": "100000000"},
     "scan-three-kernel-always": {"SOIL_SCAN1P_MAX": "0"},
 }
