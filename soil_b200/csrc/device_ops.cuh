@@ -49,12 +49,15 @@ __device__ __forceinline__ bool moved_too_far_mixed(double px, double py, double
 }
 
 // The displacement check of one local at its new position.
+__device__ __forceinline__ bool check_moved_at(const CheckArgs& ck, double x, double y, double z,
+                                               double lx, double ly, double lz) {
+    if (ck.mask == 7) return moved_too_far(x, y, z, lx, ly, lz, ck.box, ck.ibox, ck.thr_sq);
+    return moved_too_far_mixed(x, y, z, lx, ly, lz, ck.box, ck.mask, ck.thr_sq);
+}
+
 __device__ __forceinline__ bool check_moved(const CheckArgs& ck, double x, double y, double z,
                                             uint64_t i) {
-    if (ck.mask == 7)
-        return moved_too_far(x, y, z, ck.lbx[i], ck.lby[i], ck.lbz[i], ck.box, ck.ibox, ck.thr_sq);
-    return moved_too_far_mixed(x, y, z, ck.lbx[i], ck.lby[i], ck.lbz[i], ck.box, ck.mask,
-                               ck.thr_sq);
+    return check_moved_at(ck, x, y, z, ck.lbx[i], ck.lby[i], ck.lbz[i]);
 }
 
 // wrap_periodic, domain.rs:594-605
@@ -128,26 +131,38 @@ __device__ __forceinline__ void write_image(const AtomCols& c, const double (*sh
         code |= (uint32_t)s << (3 * t);
     }
     code |= (uint32_t)cats.len[k] << 12;
+    // the root's other fields loaded before any store (see perm_gather_atom)
+    const double fx = c.fx[r], fy = c.fy[r], fz = c.fz[r];
+    const double m = c.mass[r], cu = c.cut[r];
+    const uint32_t tg = c.tag[r], ty = c.type[r];
+    const int32_t i0 = c.img[r], i1 = c.img[cap + r], i2 = c.img[2 * cap + r];
     c.x[g] = x;
     c.y[g] = y;
     c.z[g] = z;
     c.vx[g] = vx;
     c.vy[g] = vy;
     c.vz[g] = vz;
-    c.fx[g] = c.fx[r];
-    c.fy[g] = c.fy[r];
-    c.fz[g] = c.fz[r];
-    const double m = c.mass[r];
+    c.fx[g] = fx;
+    c.fy[g] = fy;
+    c.fz[g] = fz;
     c.mass[g] = m;
     c.inv_mass[g] = 1.0 / m;
-    c.cut[g] = c.cut[r];
-    c.tag[g] = c.tag[r];
-    c.type[g] = c.type[r];
-    c.img[g] = c.img[r];
-    c.img[cap + g] = c.img[cap + r];
-    c.img[2 * cap + g] = c.img[2 * cap + r];
+    c.cut[g] = cu;
+    c.tag[g] = tg;
+    c.type[g] = ty;
+    c.img[g] = i0;
+    c.img[cap + g] = i1;
+    c.img[2 * cap + g] = i2;
     c.origin[g] = (int32_t)parent;
-    for (int q = 0; q < c.nplanes; ++q) c.planes[q][g] = c.planes[q][r];
+    for (int q = 0; q < c.nplanes; q += 4) {
+        double v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (q + u < c.nplanes) v[u] = c.planes[q + u][r];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (q + u < c.nplanes) c.planes[q + u][g] = v[u];
+    }
     root[g - nlocal] = (uint32_t)r;
     chain[g - nlocal] = code;
 }
@@ -398,9 +413,13 @@ __device__ __forceinline__ void initial_atom(const AtomCols& c, uint64_t i, doub
                                              bool fuse_final, bool zero_force, double& x,
                                              double& y, double& z, double& v0, double& v1,
                                              double& v2) {
+    // every load first: a load after this atom's stores could not be moved
+    // above them (the compiler cannot tell the columns apart) and would cost
+    // another memory round trip
     const double h = 0.5 * dt * c.inv_mass[i];
     const double fx = c.fx[i], fy = c.fy[i], fz = c.fz[i];
     double vx = c.vx[i], vy = c.vy[i], vz = c.vz[i];
+    const double x0 = c.x[i], y0 = c.y[i], z0 = c.z[i];
     if (fuse_final) {  // final_integration of the previous step, same forces
         vx = vx + h * fx;
         vy = vy + h * fy;
@@ -412,9 +431,9 @@ __device__ __forceinline__ void initial_atom(const AtomCols& c, uint64_t i, doub
     c.vx[i] = v0;
     c.vy[i] = v1;
     c.vz[i] = v2;
-    x = c.x[i] + v0 * dt;
-    y = c.y[i] + v1 * dt;
-    z = c.z[i] + v2 * dt;
+    x = x0 + v0 * dt;
+    y = y0 + v1 * dt;
+    z = z0 + v2 * dt;
     c.x[i] = x;
     c.y[i] = y;
     c.z[i] = z;
@@ -692,27 +711,50 @@ __device__ __forceinline__ void insertion_sort(uint32_t* items, uint32_t b, uint
 __device__ __forceinline__ void perm_gather_atom(const AtomCols& s, const AtomCols& d, uint64_t k,
                                                  uint32_t p, bool forces = true) {
     const uint64_t cap = s.cap, dcap = d.cap;
-    d.x[k] = s.x[p];
-    d.y[k] = s.y[p];
-    d.z[k] = s.z[p];
-    d.vx[k] = s.vx[p];
-    d.vy[k] = s.vy[p];
-    d.vz[k] = s.vz[p];
+    // Every load before any store: the compiler cannot prove the two column
+    // sets apart, so interleaved loads and stores would make each thread wait
+    // out one memory round trip per column.
+    const double x = s.x[p], y = s.y[p], z = s.z[p];
+    const double vx = s.vx[p], vy = s.vy[p], vz = s.vz[p];
+    double fx = 0.0, fy = 0.0, fz = 0.0;
     if (forces) {
-        d.fx[k] = s.fx[p];
-        d.fy[k] = s.fy[p];
-        d.fz[k] = s.fz[p];
+        fx = s.fx[p];
+        fy = s.fy[p];
+        fz = s.fz[p];
     }
-    d.mass[k] = s.mass[p];
-    d.inv_mass[k] = s.inv_mass[p];
-    d.cut[k] = s.cut[p];
-    d.tag[k] = s.tag[p];
-    d.type[k] = s.type[p];
-    d.img[k] = s.img[p];
-    d.img[dcap + k] = s.img[cap + p];
-    d.img[2 * dcap + k] = s.img[2 * cap + p];
-    d.origin[k] = s.origin[p];
-    for (int q = 0; q < s.nplanes; ++q) d.planes[q][k] = s.planes[q][p];
+    const double m = s.mass[p], im = s.inv_mass[p], cu = s.cut[p];
+    const uint32_t tg = s.tag[p], ty = s.type[p];
+    const int32_t i0 = s.img[p], i1 = s.img[cap + p], i2 = s.img[2 * cap + p];
+    const int32_t org = s.origin[p];
+    d.x[k] = x;
+    d.y[k] = y;
+    d.z[k] = z;
+    d.vx[k] = vx;
+    d.vy[k] = vy;
+    d.vz[k] = vz;
+    if (forces) {
+        d.fx[k] = fx;
+        d.fy[k] = fy;
+        d.fz[k] = fz;
+    }
+    d.mass[k] = m;
+    d.inv_mass[k] = im;
+    d.cut[k] = cu;
+    d.tag[k] = tg;
+    d.type[k] = ty;
+    d.img[k] = i0;
+    d.img[dcap + k] = i1;
+    d.img[2 * dcap + k] = i2;
+    d.origin[k] = org;
+    for (int q = 0; q < s.nplanes; q += 4) {  // four planes' loads, then their stores
+        double v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (q + u < s.nplanes) v[u] = s.planes[q + u][p];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (q + u < s.nplanes) d.planes[q + u][k] = v[u];
+    }
 }
 
 }  // namespace soil

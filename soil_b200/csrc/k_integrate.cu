@@ -32,9 +32,16 @@ __global__ void __launch_bounds__(kBlock, 5) k_initial(uint64_t n, AtomCols c, d
     bool hit = false;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x) {
+        const bool chk = i < ck.n_check;
+        double lx = 0.0, ly = 0.0, lz = 0.0;  // build positions, loaded before the pass's stores
+        if (chk) {
+            lx = ck.lbx[i];
+            ly = ck.lby[i];
+            lz = ck.lbz[i];
+        }
         double x, y, z, vx, vy, vz;
         initial_atom(c, i, dt, FUSE_FINAL, zero_force != 0, x, y, z, vx, vy, vz);
-        if (i < ck.n_check) hit |= check_moved(ck, x, y, z, i);
+        if (chk) hit |= check_moved_at(ck, x, y, z, lx, ly, lz);
         if (FWD)
             forward_images(c, n, i, x, y, z, vx, vy, vz, fw.fold_start, fw.fold_list, fw.chain,
                            fw.sc, fw.fwd, fw.zero_ghost_force != 0);

@@ -102,9 +102,10 @@ __global__ void __launch_bounds__(kBlock, 4) k_steps(StepsArgs a) {
         bool hit = false;
         for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nl;
              i += (uint64_t)gridDim.x * blockDim.x) {
+            const double lx = a.ck.lbx[i], ly = a.ck.lby[i], lz = a.ck.lbz[i];  // before the stores
             double x, y, z, vx, vy, vz;
             initial_atom(c, i, a.dt, fuse_final, a.zero_force != 0, x, y, z, vx, vy, vz);
-            hit |= check_moved(a.ck, x, y, z, i);
+            hit |= check_moved_at(a.ck, x, y, z, lx, ly, lz);
             forward_images(c, nl, i, x, y, z, vx, vy, vz, a.fw.fold_start, a.fw.fold_list,
                            a.fw.chain, a.fw.sc, a.fw.fwd, a.fw.zero_ghost_force != 0);
         }
