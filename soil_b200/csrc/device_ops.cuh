@@ -669,30 +669,39 @@ __device__ __forceinline__ void sorted_view(const AtomCols& c, uint64_t m, const
     }
 }
 
-// restore ascending order of one segment (the stable counting sort's last step):
-// segments of up to 8 items (nearly all: bins and transposed lists hold a few
-// atoms) are loaded at once and sorted in registers by an odd-even
-// transposition network; longer ones by insertion in place.  The items of a
-// segment are distinct, so the order is unique.
-__device__ __forceinline__ void insertion_sort(uint32_t* items, uint32_t b, uint32_t e) {
+// Restore ascending order of one segment (the stable counting sort's last
+// step) and return how many of its items are below `pivot`: segments of up
+// to 8 items (nearly all: bins and transposed lists hold a few atoms) are
+// loaded at once and sorted in registers by an odd-even transposition
+// network, the count taken from the registers; longer ones are sorted by
+// insertion in place.  The items of a segment are distinct, so the order is
+// unique.
+__device__ __forceinline__ uint32_t sort_segment(uint32_t* items, uint32_t b, uint32_t e,
+                                                 uint32_t pivot) {
     const uint32_t n = e - b;
-    if (n < 2) return;
+    if (n == 0) return 0;
     if (n <= 8) {
         uint32_t v[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) v[k] = (uint32_t)k < n ? items[b + k] : 0xffffffffu;
+        if (n >= 2) {
 #pragma unroll
-        for (int r = 0; r < 8; ++r)
+            for (int r = 0; r < 8; ++r)
 #pragma unroll
-            for (int k = r & 1; k + 1 < 8; k += 2) {
-                const uint32_t lo = min(v[k], v[k + 1]), hi = max(v[k], v[k + 1]);
-                v[k] = lo;
-                v[k + 1] = hi;
-            }
+                for (int k = r & 1; k + 1 < 8; k += 2) {
+                    const uint32_t lo = min(v[k], v[k + 1]), hi = max(v[k], v[k + 1]);
+                    v[k] = lo;
+                    v[k + 1] = hi;
+                }
+        }
+        uint32_t below = 0;
 #pragma unroll
         for (int k = 0; k < 8; ++k)
-            if ((uint32_t)k < n) items[b + k] = v[k];
-        return;
+            if ((uint32_t)k < n) {
+                if (n >= 2) items[b + k] = v[k];
+                below += v[k] < pivot;
+            }
+        return below;
     }
     for (uint32_t k = b + 1; k < e; ++k) {
         const uint32_t v = items[k];
@@ -703,6 +712,14 @@ __device__ __forceinline__ void insertion_sort(uint32_t* items, uint32_t b, uint
         }
         items[j] = v;
     }
+    uint32_t k = b;
+    while (k < e && items[k] < pivot) ++k;
+    return k - b;
+}
+
+// restore ascending order of one segment
+__device__ __forceinline__ void insertion_sort(uint32_t* items, uint32_t b, uint32_t e) {
+    if (e - b >= 2) sort_segment(items, b, e, 0u);
 }
 
 // one atom of the spatial sort's permutation gather (atom.rs:479-490)

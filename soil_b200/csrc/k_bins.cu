@@ -171,11 +171,7 @@ __global__ void __launch_bounds__(kBlock) k_segsort_split(uint64_t nseg, const u
                                                           uint32_t* items, uint32_t* split) {
     for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < nseg;
          s += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t b = start[s], e = start[s + 1];
-        insertion_sort(items, b, e);
-        uint32_t k = b;
-        while (k < e && items[k] < (uint32_t)s) ++k;
-        split[s] = k - b;
+        split[s] = sort_segment(items, start[s], start[s + 1], (uint32_t)s);
     }
 }
 
