@@ -301,14 +301,12 @@ __device__ uint32_t row_scan_pre(const PairParams& p, const Filter<UNIFORM, FP32
             ++m;
             continue;
         }
+        // the candidate's atom, loaded with its record rather than after the
+        // test accepts it (a dependent round trip per accepted entry)
+        const uint32_t a = p.sorted_atoms[m];
         if (test(p, pi, pif, m, rechk)) {
-            if (in_count) {
-                const uint32_t a = p.sorted_atoms[m];
-                atomicAdd(&in_count[a], 1u);
-                if (FILL && cnt < cap) out[cnt] = a;
-            } else if (FILL && cnt < cap) {
-                out[cnt] = p.sorted_atoms[m];
-            }
+            if (in_count) atomicAdd(&in_count[a], 1u);
+            if (FILL && cnt < cap) out[cnt] = a;
             ++cnt;
         }
         ++m;

@@ -74,6 +74,9 @@ __global__ void __launch_bounds__(kBlock) k_pairs_fill(PairParams p, const uint3
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < p.nlocal;
          i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t cnt = rowcount[i];
+        // the row's first four slots, loaded with its length and offset (the
+        // slots of a row are 16-byte aligned; past cnt they are unused)
+        const uint4 head = *reinterpret_cast<const uint4*>(slots + i * K);
         uint32_t* out = indices + offsets[i];
         const bool slotted = cnt <= K;
         if (!slotted) {
@@ -87,9 +90,16 @@ __global__ void __launch_bounds__(kBlock) k_pairs_fill(PairParams p, const uint3
         const uint32_t* src = slotted ? slots + i * K : out;
         for (uint32_t k0 = 0; k0 < cnt; k0 += 4) {
             uint32_t a[4], at[4];
+            if (k0 == 0 && slotted) {
+                a[0] = head.x;
+                a[1] = head.y;
+                a[2] = head.z;
+                a[3] = head.w;
+            } else {
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
-                if (k0 + u < cnt) a[u] = src[k0 + u];
+                for (int u = 0; u < 4; ++u)
+                    if (k0 + u < cnt) a[u] = src[k0 + u];
+            }
             if (slotted) {
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
