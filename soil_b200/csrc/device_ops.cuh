@@ -297,6 +297,25 @@ __device__ uint32_t row_scan_pre(const PairParams& p, const Filter<UNIFORM, FP32
             e = re[0];
             own = false;
         }
+        if (m + 1 < e && !(own && skip_i)) {
+            // two candidates of the range at once (their loads together),
+            // accepted in order
+            const uint32_t a0 = p.sorted_atoms[m], a1 = p.sorted_atoms[m + 1];
+            const bool ok0 = test(p, pi, pif, m, rechk);
+            const bool ok1 = test(p, pi, pif, m + 1, rechk);
+            if (ok0) {
+                if (in_count) atomicAdd(&in_count[a0], 1u);
+                if (FILL && cnt < cap) out[cnt] = a0;
+                ++cnt;
+            }
+            if (ok1) {
+                if (in_count) atomicAdd(&in_count[a1], 1u);
+                if (FILL && cnt < cap) out[cnt] = a1;
+                ++cnt;
+            }
+            m += 2;
+            continue;
+        }
         if (own && skip_i && m == mi) {
             ++m;
             continue;
@@ -458,24 +477,33 @@ __device__ __forceinline__ void final_atom(const AtomCols& c, uint64_t i, double
     c.vz[i] = c.vz[i] + h * c.fz[i];
 }
 
-// pbc fully periodic fast path (domain.rs:626-636) / pbc_triclinic (domain.rs:674-729)
+// pbc fully periodic fast path (domain.rs:626-636) / pbc_triclinic (domain.rs:674-729);
+// the new position also into px, py, pz
 __device__ __forceinline__ void pbc_atom(const AtomCols& c, uint64_t i, const Geom& g, double bv0,
-                                         double bv1, double bv2) {
+                                         double bv1, double bv2, double& px, double& py,
+                                         double& pz) {
     const uint64_t cap = c.cap;
     int32_t i0 = c.img[i], i1 = c.img[cap + i], i2 = c.img[2 * cap + i];
+    const double x0 = c.x[i], y0 = c.y[i], z0 = c.z[i];
     if (!g.triclinic) {
-        c.x[i] = wrap1(c.x[i], g.lo[0], g.size[0], i0);
-        c.y[i] = wrap1(c.y[i], g.lo[1], g.size[1], i1);
-        c.z[i] = wrap1(c.z[i], g.lo[2], g.size[2], i2);
+        px = wrap1(x0, g.lo[0], g.size[0], i0);
+        py = wrap1(y0, g.lo[1], g.size[1], i1);
+        pz = wrap1(z0, g.lo[2], g.size[2], i2);
+        c.x[i] = px;
+        c.y[i] = py;
+        c.z[i] = pz;
     } else {
         double l0, l1, l2;
-        x2lamda(g, c.x[i], c.y[i], c.z[i], l0, l1, l2);
+        x2lamda(g, x0, y0, z0, l0, l1, l2);
         int32_t d0 = 0, d1 = 0, d2 = 0;
         if (l0 < 0.0) { l0 += 1.0; d0 = -1; } else if (l0 >= 1.0) { l0 -= 1.0; d0 = 1; }
         if (l1 < 0.0) { l1 += 1.0; d1 = -1; } else if (l1 >= 1.0) { l1 -= 1.0; d1 = 1; }
         if (l2 < 0.0) { l2 += 1.0; d2 = -1; } else if (l2 >= 1.0) { l2 -= 1.0; d2 = 1; }
         double rx, ry, rz;
         lamda2x(g, l0, l1, l2, rx, ry, rz);
+        px = rx;
+        py = ry;
+        pz = rz;
         c.x[i] = rx;
         c.y[i] = ry;
         c.z[i] = rz;
@@ -492,6 +520,12 @@ __device__ __forceinline__ void pbc_atom(const AtomCols& c, uint64_t i, const Ge
     c.img[i] = i0;
     c.img[cap + i] = i1;
     c.img[2 * cap + i] = i2;
+}
+
+__device__ __forceinline__ void pbc_atom(const AtomCols& c, uint64_t i, const Geom& g, double bv0,
+                                         double bv1, double bv2) {
+    double px, py, pz;
+    pbc_atom(c, i, g, bv0, bv1, bv2, px, py, pz);
 }
 
 // forward_comm of ghost gi (index nlocal + gi): its root local atom plus the

@@ -35,6 +35,34 @@ __global__ void __launch_bounds__(kBlock) k_cells(uint64_t first, uint64_t n, At
     }
 }
 
+// pbc of the locals and the sort's cells in one pass: each local is wrapped
+// (pbc_atom) and its new position binned and counted.
+__global__ void __launch_bounds__(kBlock) k_pbc_cells(uint64_t n, AtomCols c, Geom g, double bv0,
+                                                      double bv1, double bv2, Grid gr,
+                                                      uint32_t* cell_out, uint32_t* counts) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
+        const uint64_t i = i0 + threadIdx.x;
+        const bool valid = i < n;
+        uint32_t cell = 0;
+        if (valid) {
+            double x, y, z;
+            pbc_atom(c, i, g, bv0, bv1, bv2, x, y, z);
+            cell = cell_of(gr, x, y, z);
+            cell_out[i] = cell;
+        }
+        aggregated_count(counts, cell, valid);
+    }
+}
+
+void launch_pbc_cells(cudaStream_t st, uint64_t n, const AtomCols& c, const Geom& g,
+                      const double bvel[3], const Grid& gr, uint32_t* cell_out, uint32_t* counts) {
+    if (n == 0) return;
+    note_launch();
+    k_pbc_cells<<<grid_wave<k_pbc_cells>(n), kBlock, 0, st>>>(n, c, g, bvel[0], bvel[1], bvel[2],
+                                                              gr, cell_out, counts);
+}
+
 void launch_cells(cudaStream_t st, uint64_t first, uint64_t n, const AtomCols& c, const Grid& gr,
                   uint32_t* cell_out, uint32_t* counts, const uint32_t* n_dev) {
     if (n == 0) return;

@@ -155,6 +155,9 @@ void exclusive_scan_1p(cudaStream_t st, const uint32_t* in, uint32_t* out, uint6
 
 // ---- bins (k_bins.cu) -----------------------------------------------------
 // cell[i] = cell_of(pos[first+i]) and counts[cell]++ for i in [0, n)
+// pbc of locals [0, n) then cell_out[i] = their cell, counted (pbc + the sort's binning)
+void launch_pbc_cells(cudaStream_t st, uint64_t n, const AtomCols& c, const Geom& g,
+                      const double bvel[3], const Grid& gr, uint32_t* cell_out, uint32_t* counts);
 // n_dev (optional, here and below): the count is min(n, *n_dev), read on the
 // device (n an upper bound), for launches queued before the host knows it.
 void launch_cells(cudaStream_t st, uint64_t first, uint64_t n, const AtomCols& c, const Grid& gr,

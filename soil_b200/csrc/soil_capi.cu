@@ -860,15 +860,24 @@ void sort_done(soil_sys* s, bool apply, bool periodic) {
     }
 }
 
+int sort_run(soil_sys* s, bool periodic_sort, bool cells_done);
 int phase_sort(soil_sys* s) {
     bool run, periodic_sort;
     TRY(sort_plan(s, &run, &periodic_sort));
     if (!run) return SOIL_OK;
+    return sort_run(s, periodic_sort, false);
+}
+
+// The sort's kernels after sort_plan decided to run it; cells_done: the
+// locals' cells are binned and counted already (launch_pbc_cells).
+int sort_run(soil_sys* s, bool periodic_sort, bool cells_done) {
     s->pk_valid = false;
     const uint64_t nl = s->nlocal;
     const uint64_t nc = s->total_cells;
-    TRY(counts_zero(s, nc));
-    launch_cells(s->st, 0, nl, s->A, grid_of(s), s->sort_cell.p, s->cell_counts.p);
+    if (!cells_done) {
+        TRY(counts_zero(s, nc));
+        launch_cells(s->st, 0, nl, s->A, grid_of(s), s->sort_cell.p, s->cell_counts.p);
+    }
     TRY(scan_1p(s, s->cell_counts.p, s->cell_start.p, nc));
     launch_scatter_consume(s->st, nl, s->sort_cell.p, s->cell_start.p, s->cell_counts.p,
                            s->sort_perm.p);
@@ -1708,11 +1717,32 @@ int step_rest(soil_sys* s, const StepPlan& p, bool last) {
     timer_end(s, T_ZERO);
     timer_begin(s, T_PBC);
     TRY(phase_shrink_wrap(s));
-    TRY(phase_pbc(s));
+    // A rebuild step of a fully periodic box wraps its locals and bins them
+    // for the sort in one pass: the sort's plan (grid, whether it runs) does
+    // not depend on the wrap, so it is made first.
+    const bool pbc_cells =
+        s->state == FULL_REBUILD && pbc_mask(s) == 7 && s->nlocal > 0 && s->total_cells > 0;
+    bool sort_due = false, periodic_sort = false;
+    if (pbc_cells) {
+        TRY(sort_plan(s, &sort_due, &periodic_sort));
+        s->pk_valid = false;
+        if (sort_due) {
+            TRY(counts_zero(s, s->total_cells));
+            launch_pbc_cells(s->st, s->nlocal, s->A, geom_of(s), s->bvel, grid_of(s),
+                             s->sort_cell.p, s->cell_counts.p);
+        } else {
+            launch_pbc(s->st, s->nlocal, s->A, geom_of(s), s->bvel);
+        }
+        TRY(check_launch(s));
+    } else {
+        TRY(phase_pbc(s));
+    }
     timer_end(s, T_PBC);
     timer_begin(s, T_SORT);
     s->forces_dead = p.overwrite;  // the built-in consumer rewrites every force below
-    const int sorted = phase_sort(s);
+    const int sorted = !pbc_cells ? phase_sort(s)
+                     : sort_due   ? sort_run(s, periodic_sort, true)
+                                  : SOIL_OK;
     s->forces_dead = false;
     TRY(sorted);
     timer_end(s, T_SORT);
