@@ -297,25 +297,6 @@ __device__ uint32_t row_scan_pre(const PairParams& p, const Filter<UNIFORM, FP32
             e = re[0];
             own = false;
         }
-        if (m + 1 < e && !(own && skip_i)) {
-            // two candidates of the range at once (their loads together),
-            // accepted in order
-            const uint32_t a0 = p.sorted_atoms[m], a1 = p.sorted_atoms[m + 1];
-            const bool ok0 = test(p, pi, pif, m, rechk);
-            const bool ok1 = test(p, pi, pif, m + 1, rechk);
-            if (ok0) {
-                if (in_count) atomicAdd(&in_count[a0], 1u);
-                if (FILL && cnt < cap) out[cnt] = a0;
-                ++cnt;
-            }
-            if (ok1) {
-                if (in_count) atomicAdd(&in_count[a1], 1u);
-                if (FILL && cnt < cap) out[cnt] = a1;
-                ++cnt;
-            }
-            m += 2;
-            continue;
-        }
         if (own && skip_i && m == mi) {
             ++m;
             continue;
