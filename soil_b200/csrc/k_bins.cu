@@ -179,6 +179,79 @@ void launch_cells_reuse(cudaStream_t st, uint64_t nlocal, uint64_t n, const Atom
                                                                   cell_out, counts, n_dev);
 }
 
+// The neighbor build's bins right after a spatial sort of the same grid:
+// the locals are already in cell order (local i is entry i - sort_start[c]
+// of its cell c), so they take their slots directly, in front of their
+// cell's ghosts; only the ghosts are scattered and ranked.
+__global__ void __launch_bounds__(kBlock) k_place_locals(uint64_t nl, const uint32_t* cell,
+                                                         const uint32_t* start,
+                                                         const uint32_t* sort_start,
+                                                         uint32_t* out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nl;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t c = cell[i];
+        out[start[c] + ((uint32_t)i - sort_start[c])] = (uint32_t)i;
+    }
+}
+
+// Ghost g of cell c into the ghost part of c's slots (after its locals), in
+// no particular order: counts[c] still holds c's locals and ghosts, and only
+// ghosts take from it.
+__global__ void __launch_bounds__(kBlock) k_ghost_scatter(uint64_t nl, uint64_t n,
+                                                          const uint32_t* n_dev,
+                                                          const uint32_t* cell,
+                                                          const uint32_t* start, uint32_t* counts,
+                                                          uint32_t* tmp) {
+    if (n_dev) {
+        const uint64_t d = *n_dev;
+        n = d < n ? d : n;
+    }
+    for (uint64_t g = nl + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < n;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t c = cell[g];
+        tmp[start[c] + atomicSub(&counts[c], 1u) - 1u] = (uint32_t)g;
+    }
+}
+
+// Each ghost at its rank among its cell's ghosts (ascending index).
+__global__ void __launch_bounds__(kBlock) k_ghost_rank(uint64_t nl, uint64_t n,
+                                                       const uint32_t* n_dev,
+                                                       const uint32_t* cell,
+                                                       const uint32_t* start,
+                                                       const uint32_t* sort_start,
+                                                       const uint32_t* tmp, uint32_t* out) {
+    if (n_dev) {
+        const uint64_t d = *n_dev;
+        n = d < n ? d : n;
+    }
+    for (uint64_t g = nl + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < n;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t c = cell[g];
+        const uint32_t gb = start[c] + (sort_start[c + 1] - sort_start[c]), ge = start[c + 1];
+        uint32_t rank = 0;
+        for (uint32_t j = gb; j < ge; ++j) rank += tmp[j] < (uint32_t)g;
+        out[gb + rank] = (uint32_t)g;
+    }
+}
+
+void launch_place_bins(cudaStream_t st, uint64_t nl, uint64_t n, const uint32_t* n_dev,
+                       const uint32_t* cell, const uint32_t* start, const uint32_t* sort_start,
+                       uint32_t* counts, uint32_t* tmp, uint32_t* out) {
+    if (nl) {
+        note_launch();
+        k_place_locals<<<grid_wave<k_place_locals>(nl), kBlock, 0, st>>>(nl, cell, start,
+                                                                         sort_start, out);
+    }
+    if (n > nl) {
+        note_launch();
+        k_ghost_scatter<<<grid_wave<k_ghost_scatter>(n - nl), kBlock, 0, st>>>(
+            nl, n, n_dev, cell, start, counts, tmp);
+        note_launch();
+        k_ghost_rank<<<grid_wave<k_ghost_rank>(n - nl), kBlock, 0, st>>>(nl, n, n_dev, cell, start,
+                                                                         sort_start, tmp, out);
+    }
+}
+
 // Restore the stable (ascending index) order inside every segment.
 __global__ void __launch_bounds__(kBlock) k_segsort(uint64_t nseg, const uint32_t* start,
                                                     uint32_t* items) {

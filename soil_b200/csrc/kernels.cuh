@@ -177,6 +177,14 @@ void launch_scatter_consume(cudaStream_t st, uint64_t n, const uint32_t* cell,
 void launch_cells_reuse(cudaStream_t st, uint64_t nlocal, uint64_t n, const AtomCols& c,
                         const Grid& gr, const uint32_t* local_cell, uint32_t* cell_out,
                         uint32_t* counts, const uint32_t* n_dev = nullptr);
+// The neighbor build's bin order (out = sorted atoms) just after a spatial
+// sort on the same grid: local i of cell c at start[c] + i - sort_start[c],
+// then c's ghosts [nl, n) in ascending order after its locals.  counts: the
+// cells' local + ghost counts (the ghosts' part is consumed); tmp: scratch of
+// the atoms' size.
+void launch_place_bins(cudaStream_t st, uint64_t nl, uint64_t n, const uint32_t* n_dev,
+                       const uint32_t* cell, const uint32_t* start, const uint32_t* sort_start,
+                       uint32_t* counts, uint32_t* tmp, uint32_t* out);
 // sort every segment [start[s], start[s+1]) ascending -> stable counting sort
 void launch_segsort(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint32_t* items);
 // the same, and split[s] = entries of segment s below s (transposed lists)

@@ -839,6 +839,7 @@ int sort_plan(soil_sys* s, bool* run, bool* periodic) {
     TRY(ensure(s, s->cell_cursor, nc + 1, 0, 2 * nc + 64));
     TRY(ensure(s, s->scan_tmp, scan_temp_words(nc + s->acap + 2), 0,
                scan_temp_words(2 * nc + s->acap + 64)));
+    TRY(ensure(s, s->sort_start, nc + 2, 0, 2 * nc + 64));
     return SOIL_OK;
 }
 
@@ -878,11 +879,11 @@ int sort_run(soil_sys* s, bool periodic_sort, bool cells_done) {
         TRY(counts_zero(s, nc));
         launch_cells(s->st, 0, nl, s->A, grid_of(s), s->sort_cell.p, s->cell_counts.p);
     }
-    TRY(scan_1p(s, s->cell_counts.p, s->cell_start.p, nc));
-    launch_scatter_consume(s->st, nl, s->sort_cell.p, s->cell_start.p, s->cell_counts.p,
+    TRY(scan_1p(s, s->cell_counts.p, s->sort_start.p, nc));
+    launch_scatter_consume(s->st, nl, s->sort_cell.p, s->sort_start.p, s->cell_counts.p,
                            s->sort_perm.p);
     counts_consumed(s);
-    launch_segsort(s->st, nc, s->cell_start.p, s->sort_perm.p);
+    launch_segsort(s->st, nc, s->sort_start.p, s->sort_perm.p);
     TRY(check_launch(s));
 
     bool apply = true;
@@ -1332,6 +1333,7 @@ int neighbor_plan(soil_sys* s) {
     TRY(ensure(s, s->cell_cursor, nc + 1, 0, 2 * nc + 64));
     TRY(ensure(s, s->scan_tmp, scan_temp_words(nc + s->acap + 2), 0,
                scan_temp_words(2 * nc + s->acap + 64)));
+    TRY(ensure(s, s->ghost_tmp, s->acap));
     return SOIL_OK;
 }
 
@@ -1397,17 +1399,25 @@ int phase_neighbor(soil_sys* s) {
     const bool fp32 = s->filter == SOIL_FILTER_FP32_RECHECK;
     TRY(counts_zero(s, nc));
     const Grid gr = grid_of(s);
-    if (s->local_cells_valid)  // reuse the sort's local cells (neighbor.rs:1049-1066)
+    const bool after_sort = s->local_cells_valid;
+    if (after_sort)  // reuse the sort's local cells (neighbor.rs:1049-1066)
         launch_cells_reuse(s->st, nl, total, s->A, gr, s->sorted_local_cell.p, s->atom_cell.p,
                            s->cell_counts.p, n_dev);
     else
         launch_cells(s->st, 0, total, s->A, gr, s->atom_cell.p, s->cell_counts.p, n_dev);
     s->local_cells_valid = false;
     TRY(scan_1p(s, s->cell_counts.p, s->cell_start.p, nc));
-    launch_scatter_consume(s->st, total, s->atom_cell.p, s->cell_start.p, s->cell_counts.p,
-                           s->sorted_atoms.p, n_dev);
-    counts_consumed(s);
-    launch_segsort(s->st, nc, s->cell_start.p, s->sorted_atoms.p);
+    if (after_sort) {
+        // the locals are in bin order already: only the ghosts are sorted
+        launch_place_bins(s->st, nl, total, n_dev, s->atom_cell.p, s->cell_start.p,
+                          s->sort_start.p, s->cell_counts.p, s->ghost_tmp.p, s->sorted_atoms.p);
+        s->counts_clean = 0;  // the locals' counts remain
+    } else {
+        launch_scatter_consume(s->st, total, s->atom_cell.p, s->cell_start.p, s->cell_counts.p,
+                               s->sorted_atoms.p, n_dev);
+        counts_consumed(s);
+        launch_segsort(s->st, nc, s->cell_start.p, s->sorted_atoms.p);
+    }
     BuildPos bpos;  // save_build_positions (neighbor.rs:669-690) in the same pass
     bpos.x = s->lbx.p;
     bpos.y = s->lby.p;
@@ -2071,7 +2081,7 @@ int soil_sys_destroy(soil_sys* s) {
         a.cap = 0;
     };
     fr(s->lbx); fr(s->lby); fr(s->lbz);
-    fr(s->sort_cell); fr(s->sort_perm); fr(s->sorted_local_cell);
+    fr(s->sort_cell); fr(s->sort_perm); fr(s->sorted_local_cell); fr(s->sort_start); fr(s->ghost_tmp);
     fr(s->cell_counts); fr(s->cell_start); fr(s->cell_cursor);
     fr(s->atom_cell); fr(s->sorted_atoms); fr(s->asi); fr(s->rowcount); fr(s->offsets); fr(s->indices);
     fr(s->row_slots); fr(s->sp); fr(s->spf);

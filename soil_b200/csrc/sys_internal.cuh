@@ -125,6 +125,8 @@ struct soil_sys {
     AtomCols A{}, B{};
     DArr<double> lbx, lby, lbz;
     DArr<uint32_t> sort_cell, sort_perm, sorted_local_cell;
+    DArr<uint32_t> sort_start;  // the spatial sort's cell starts (its locals' bins)
+    DArr<uint32_t> ghost_tmp;   // the neighbor build's unordered ghost slots
     DArr<uint32_t> cell_counts, cell_start, cell_cursor;
     // cell_counts[0, counts_clean) is known to be zero (the consuming scatters
     // leave it so); counts_at: the allocation that holds
