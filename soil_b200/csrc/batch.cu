@@ -811,10 +811,6 @@ int batch_step(soil_batch* b, bool last) {
             soil_sys* s = b->slot[k];
             TRY(borders_done(s, b->h_bread + (size_t)k * kBorderStateWords, b->bds[k].data()));
             TRY(neighbor_plan(s));
-            // the pair count pass counts the transposed lists' entries
-            const uint64_t total = s->nlocal + s->nghost;
-            TRY(ensure(s, s->in_count, total + 1, 0, s->acap + 1));
-            TRY(ensure(s, s->in_start, total + 2, 0, s->acap + 2));
             fill_dev(b, k);
             auto& h = b->hot[k];
             h.nghost = s->nghost;
@@ -832,7 +828,7 @@ int batch_step(soil_batch* b, bool last) {
     TRY(put_tables(b, g4));
     const int f_loc = stage_add(g4), s_fwd = stage_add(g4), n_cells = stage_add(g4),
               n_copy = stage_add(g4), n_bin = stage_add(g4), n_all = stage_add(g4),
-              n_rows = stage_add(g4), n_tiles = stage_add(g4), n_in = stage_add(g4);
+              n_rows = stage_add(g4), n_tiles = stage_add(g4);
     for (uint32_t k : M) {
         const auto& h = b->hot[k];
         if (!b->rebuild[k]) {
@@ -850,7 +846,6 @@ int batch_step(soil_batch* b, bool last) {
         }
         g4.spans[n_all].add_nz(k, nl + ng, 0);
         g4.spans[n_rows].add(k, nl, 0);
-        g4.spans[n_in].add(k, nl + ng, 0);
         g4.spans[n_tiles].add_nz(k, (nl + 31) / 32, 0);
     }
     TRY(stage_commit(b, g4));
@@ -865,11 +860,9 @@ int batch_step(soil_batch* b, bool last) {
         b_scatter(st, g4.out[n_all], a, true);
         b_segsort(st, g4.out[n_cells], a, BA_NEIGH_CELLS);
         b_sorted_views(st, g4.out[n_all], a);
-        b_zero_counts(st, g4.out[n_in], a, BA_IN);
         if (pairs_staged_on()) b_pairs_staged(st, g4.out[n_tiles], a);
         else b_pairs_rows(st, g4.out[f_loc], a);
         b_scan(st, g4.out[n_rows], a, BA_ROWS);
-        b_scan(st, g4.out[n_in], a, BA_IN);
         toc(b, BT_NEIGHBOR);
         TRY(check_kernels(b));
         BCK(cudaMemcpyAsync(b->h_totals, b->d_totals, (size_t)b->cap * 4, cudaMemcpyDeviceToHost, st));
@@ -886,6 +879,7 @@ int batch_step(soil_batch* b, bool last) {
             TRY(ensure(s, s->indices, np + 1, 0, pair_room(np)));
             TRY(ensure(s, s->in_count, total + 1, 0, s->acap + 1));
             TRY(ensure(s, s->in_start, total + 2, 0, s->acap + 2));
+            TRY(ensure(s, s->in_cursor, total + 1, 0, s->acap + 1));
             TRY(ensure(s, s->in_list, np + 1, 0, pair_room(np)));
             const int fv = force_variant();
             if (s->few_images && fv != SOIL_FORCE_GATHER && fv != SOIL_FORCE_CSR) {
@@ -914,7 +908,7 @@ int batch_step(soil_batch* b, bool last) {
     std::vector<uint32_t> grouped_now;  // rebuilding boxes that build grouped sequences
     TRY(stage_begin(b, g5));
     TRY(put_tables(b, g5));
-    const int r_loc = stage_add(g5), r_all = stage_add(g5),
+    const int r_loc = stage_add(g5), r_all = stage_add(g5), r_scan = stage_add(g5),
               h_all = stage_add(g5), v_loc = stage_add(g5), l_loc = stage_add(g5),
               q_all = stage_add(g5), q_grp = stage_add(g5), q_loc = stage_add(g5),
               t_tiles = stage_add(g5), t_walk = stage_add(g5);
@@ -937,6 +931,7 @@ int batch_step(soil_batch* b, bool last) {
         if (b->rebuild[k]) {
             g5.spans[r_loc].add_nz(k, nl, 0);
             g5.spans[r_all].add_nz(k, total, 0);
+            g5.spans[r_scan].add(k, total, 0);
             if (grouped) {
                 g5.spans[q_all].add_nz(k, total, 0);
                 g5.spans[q_grp].add(k, nl, 0);
@@ -957,7 +952,11 @@ int batch_step(soil_batch* b, bool last) {
     TRY(stage_commit(b, g5));
     tic(b);
     if (!R.empty()) {
-        b_pairs_fill(st, g5.out[r_loc], a);  // also places the transposed lists' entries
+        b_pairs_fill(st, g5.out[r_loc], a);
+        b_zero_counts(st, g5.out[r_scan], a, BA_IN);
+        b_in_count(st, g5.out[r_loc], a);
+        b_scan(st, g5.out[r_scan], a, BA_IN);
+        b_in_scatter(st, g5.out[r_loc], a);
         b_segsort(st, g5.out[r_all], a, BA_IN);
         b_seq_count(st, g5.out[q_all], a);
         b_scan(st, g5.out[q_grp], a, BA_GRP);

@@ -122,7 +122,7 @@ enum BatchArray {
     BA_CELLS = 0,     // cell_counts -> cell_start (+ cursor), segsort of sort_perm
     BA_NEIGH_CELLS,   // cell_counts -> cell_start (+ cursor), segsort of sorted_atoms
     BA_ROWS,          // rowcount -> offsets (total into totals[box])
-    BA_IN,            // in_count -> in_start, segsort of in_list
+    BA_IN,            // in_count -> in_start (+ cursor), segsort of in_list
     BA_GRP            // grp_cnt -> grp_start (grouped sequences)
 };
 
@@ -158,6 +158,8 @@ void b_pairs_rows(cudaStream_t st, const Span& sp, const BatchArgs& a);
 // candidate records staged in shared memory (pairs_staged.cuh)
 void b_pairs_staged(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_pairs_fill(cudaStream_t st, const Span& sp, const BatchArgs& a);
+void b_in_count(cudaStream_t st, const Span& sp, const BatchArgs& a);
+void b_in_scatter(cudaStream_t st, const Span& sp, const BatchArgs& a);
 void b_harmonic(cudaStream_t st, const Span& sp, const BatchArgs& a);
 // grouped sequences: lengths over every atom (count) and the groups of the
 // locals (fill, after a BA_GRP scan); the consumer over warp tiles of 32

@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(kBlock) kb_scan(Span sp, BatchArgs A, int whic
     const uint32_t* in;
     uint32_t *out, *cursor;
     if (which == BA_ROWS) { in = D.rowcount; out = D.offsets; cursor = nullptr; }
-    else if (which == BA_IN) { in = D.in_count; out = D.in_start; cursor = nullptr; }
+    else if (which == BA_IN) { in = D.in_count; out = D.in_start; cursor = D.in_cursor; }
     else if (which == BA_GRP) { in = D.grp_cnt; out = D.grp_start; cursor = nullptr; }
     else { in = D.cell_counts; out = D.cell_start; cursor = D.cell_cursor; }
     uint32_t carry = 0;
@@ -378,11 +378,9 @@ __device__ __forceinline__ PairParams pair_params(const BoxDev& D, const BoxStep
     p.sf_sq = S.sf_sq;
     p.sf = S.sf;
     p.eps32 = S.eps32;
-    // the transposed lists are built inside the pair passes, as for a single
-    // system: pass 1 counts into in_count, the fill places each row
-    p.in_count = D.in_count;
-    p.in_start = D.in_start;
-    p.in_list = D.in_list;
+    p.in_count = nullptr;
+    p.in_start = nullptr;
+    p.in_list = nullptr;
     p.pre_ranges = S.pre_ranges;
     return p;
 }
@@ -393,8 +391,7 @@ __device__ __forceinline__ void pairs_row(const PairParams& p, uint64_t i, uint3
                                           uint32_t& rk) {
     const Filter<UNIFORM, FP32> test(p);
     const uint32_t K = (uint32_t)p.row_slots;
-    rowcount[i] =
-        row_scan<UNIFORM, FP32, true>(p, test, i, slots + i * K, K, &rk, &cd, flags, p.in_count);
+    rowcount[i] = row_scan<UNIFORM, FP32, true>(p, test, i, slots + i * K, K, &rk, &cd, flags);
 }
 
 __device__ __forceinline__ void add_filter_stats(DevFlags* f, uint32_t cd, uint32_t rk) {
@@ -517,11 +514,6 @@ __device__ __forceinline__ void fill_row(const PairParams& p, uint64_t i, const 
         uint32_t rk = 0, cd = 0;
         row_scan<UNIFORM, FP32, true>(p, test, i, out, 0xffffffffu, &rk, &cd, nullptr);
     }
-    // row i into each partner's transposed list (the counts go back to 0)
-    for (uint32_t q = 0; q < cnt; ++q) {
-        const uint32_t a = out[q];
-        p.in_list[p.in_start[a] + atomicSub(&p.in_count[a], 1u) - 1u] = (uint32_t)i;
-    }
 }
 
 SPAN_KERNEL(kb_pairs_fill, {
@@ -536,7 +528,16 @@ SPAN_KERNEL(kb_pairs_fill, {
 })
 SPAN_LAUNCH(b_pairs_fill, kb_pairs_fill)
 
+SPAN_KERNEL(kb_in_count, {
+    for (uint32_t q = D.offsets[i]; q < D.offsets[i + 1]; ++q) atomicAdd(&D.in_count[D.indices[q]], 1u);
+})
+SPAN_LAUNCH(b_in_count, kb_in_count)
 
+SPAN_KERNEL(kb_in_scatter, {
+    for (uint32_t q = D.offsets[i]; q < D.offsets[i + 1]; ++q)
+        D.in_list[atomicAdd(&D.in_cursor[D.indices[q]], 1u)] = (uint32_t)i;
+})
+SPAN_LAUNCH(b_in_scatter, kb_in_scatter)
 
 // ---- force and reverse comm ---------------------------------------------------
 // Register-capped like the single-system force kernel (5 blocks per SM) and
