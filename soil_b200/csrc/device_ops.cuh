@@ -227,6 +227,22 @@ struct Filter {
         }
         return test64(pi, ld_rec(p.sp + m));
     }
+
+    // The same test returning the slot's atom when it passes, else kNoAtom.
+    // With a uniform cutoff the record's fourth word is free and holds the
+    // atom (sorted_view), so the candidate costs one load, not two.
+    static constexpr uint32_t kNoAtom = 0xffffffffu;
+    __device__ __forceinline__ uint32_t accept(const PairParams& p, const double4& pi,
+                                               const float4& pif, uint32_t m,
+                                               uint32_t* rechk) const {
+        if (!UNIFORM) return (*this)(p, pi, pif, m, rechk) ? p.sorted_atoms[m] : kNoAtom;
+        if (FP32) {
+            if (!pass32(pif, p.spf[m])) return kNoAtom;
+            ++*rechk;
+        }
+        const double4 q = ld_rec(p.sp + m);
+        return test64(pi, q) ? (uint32_t)__double_as_longlong(q.w) : kNoAtom;
+    }
 };
 
 // Ranges of the row scan held in registers (row_scan_pre): the own cell's
@@ -303,8 +319,16 @@ __device__ uint32_t row_scan_pre(const PairParams& p, const Filter<UNIFORM, FP32
         }
         // the candidate's atom, loaded with its record rather than after the
         // test accepts it (a dependent round trip per accepted entry)
-        const uint32_t a = p.sorted_atoms[m];
-        if (test(p, pi, pif, m, rechk)) {
+        uint32_t a;
+        bool ok;
+        if (UNIFORM) {  // the atom comes with the record
+            a = test.accept(p, pi, pif, m, rechk);
+            ok = a != test.kNoAtom;
+        } else {
+            a = p.sorted_atoms[m];
+            ok = test(p, pi, pif, m, rechk);
+        }
+        if (ok) {
             if (in_count) atomicAdd(&in_count[a], 1u);
             if (FILL && cnt < cap) out[cnt] = a;
             ++cnt;
@@ -363,14 +387,10 @@ __device__ uint32_t row_scan(const PairParams& p, const Filter<UNIFORM, FP32>& t
             }
             ++*cand;
         }
-        if (test(p, pi, pif, m, rechk)) {
-            if (in_count) {  // pass 1 of a build with the transposed lists
-                const uint32_t a = p.sorted_atoms[m];
-                atomicAdd(&in_count[a], 1u);
-                if (FILL && cnt < cap) out[cnt] = a;
-            } else if (FILL && cnt < cap) {
-                out[cnt] = p.sorted_atoms[m];
-            }
+        const uint32_t a = test.accept(p, pi, pif, m, rechk);
+        if (a != test.kNoAtom) {
+            if (in_count) atomicAdd(&in_count[a], 1u);  // pass 1 of a build with the transposed lists
+            if (FILL && cnt < cap) out[cnt] = a;
             ++cnt;
         }
         ++m;
@@ -669,11 +689,14 @@ __device__ __forceinline__ void fold_root(const AtomCols& c, uint64_t nlocal, ui
 // one sorted slot of the neighbor build's bin order (neighbor.rs:1101-1125)
 __device__ __forceinline__ void sorted_view(const AtomCols& c, uint64_t m, const uint32_t* sorted,
                                             uint32_t* asi, double4* sp, float4* spf, double o0,
-                                            double o1, double o2, const BuildPos& bp = BuildPos{}) {
+                                            double o1, double o2, const BuildPos& bp = BuildPos{},
+                                            bool atom_in_w = false) {
     const uint32_t a = sorted[m];
     asi[a] = (uint32_t)m;
     const double x = c.x[a], y = c.y[a], z = c.z[a], cut = c.cut[a];
-    sp[m] = make_double4(x, y, z, cut);
+    // with a uniform cutoff the pair test reads no radius: the fourth word
+    // carries the slot's atom instead (its bits; Filter::accept)
+    sp[m] = make_double4(x, y, z, atom_in_w ? __longlong_as_double((long long)a) : cut);
     if (spf) spf[m] = make_float4((float)(x - o0), (float)(y - o1), (float)(z - o2), (float)cut);
     if (bp.x && a < bp.nlocal) {  // save_build_positions of the locals
         bp.x[a] = x;

@@ -353,7 +353,7 @@ SPAN_LAUNCH(b_save_positions, kb_save_positions)
 
 SPAN_KERNEL(kb_sorted_views, {
     sorted_view(D.set[S.post], i, D.sorted_atoms, D.asi, D.sp, S.filter ? D.spf : nullptr,
-                S.geom.lo[0], S.geom.lo[1], S.geom.lo[2]);
+                S.geom.lo[0], S.geom.lo[1], S.geom.lo[2], BuildPos{}, S.uniform != 0);
 })
 SPAN_LAUNCH(b_sorted_views, kb_sorted_views)
 

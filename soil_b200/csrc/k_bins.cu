@@ -362,23 +362,25 @@ __global__ void __launch_bounds__(kBlock) k_sorted_views(uint64_t n, const uint3
                                                          AtomCols c, uint32_t* asi, double4* sp,
                                                          float4* spf, double o0, double o1,
                                                          double o2, BuildPos bp,
-                                                         const uint32_t* n_dev) {
+                                                         const uint32_t* n_dev, int atom_in_w) {
     if (n_dev) {  // the count known only on the device (an upper bound in n)
         const uint64_t d = *n_dev;
         n = d < n ? d : n;
     }
     for (uint64_t m = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; m < n;
          m += (uint64_t)gridDim.x * blockDim.x)
-        sorted_view(c, m, sorted, asi, sp, spf, o0, o1, o2, bp);
+        sorted_view(c, m, sorted, asi, sp, spf, o0, o1, o2, bp, atom_in_w != 0);
 }
 
 void launch_sorted_views(cudaStream_t st, uint64_t n, const uint32_t* sorted, const AtomCols& c,
                          uint32_t* atom_sorted_idx, double4* sp, float4* spf,
-                         const double origin[3], const BuildPos& bp, const uint32_t* n_dev) {
+                         const double origin[3], const BuildPos& bp, const uint32_t* n_dev,
+                         bool atom_in_w) {
     if (n == 0) return;
     note_launch();
     k_sorted_views<<<grid_wave<k_sorted_views>(n), kBlock, 0, st>>>(
-        n, sorted, c, atom_sorted_idx, sp, spf, origin[0], origin[1], origin[2], bp, n_dev);
+        n, sorted, c, atom_sorted_idx, sp, spf, origin[0], origin[1], origin[2], bp, n_dev,
+        atom_in_w ? 1 : 0);
 }
 
 }  // namespace soil

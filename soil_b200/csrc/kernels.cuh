@@ -209,11 +209,13 @@ void launch_slot_gather(cudaStream_t st, uint64_t n, const uint32_t* perm, uint3
 void launch_permute_u32(cudaStream_t st, uint64_t n, const uint32_t* perm, const uint32_t* in,
                         uint32_t* out);
 // inverse[sorted[m]] = m and the sorted records sp[m] = {x, y, z, cutoff}
-// (plus the FP32 grid-relative copy spf when spf != nullptr)
+// (plus the FP32 grid-relative copy spf when spf != nullptr); atom_in_w (for
+// a uniform cutoff, whose test reads no radius) stores sorted[m]'s bits in
+// place of the cutoff
 void launch_sorted_views(cudaStream_t st, uint64_t n, const uint32_t* sorted, const AtomCols& c,
                          uint32_t* atom_sorted_idx, double4* sp, float4* spf,
                          const double origin[3], const BuildPos& bp = BuildPos{},
-                         const uint32_t* n_dev = nullptr);
+                         const uint32_t* n_dev = nullptr, bool atom_in_w = false);
 
 // ---- ghosts (k_ghost.cu) --------------------------------------------------
 struct BorderDim {

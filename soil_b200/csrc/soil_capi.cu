@@ -1424,7 +1424,7 @@ int phase_neighbor(soil_sys* s) {
     bpos.z = s->lbz.p;
     bpos.nlocal = nl;
     launch_sorted_views(s->st, total, s->sorted_atoms.p, s->A, s->asi.p, s->sp.p,
-                        fp32 ? s->spf.p : nullptr, s->blo, bpos, n_dev);
+                        fp32 ? s->spf.p : nullptr, s->blo, bpos, n_dev, s->has_uniform);
     const std::vector<int32_t>& sten = s->newton ? s->stencil_fwd : s->stencil;
     const std::vector<int32_t> runs = stencil_runs(sten, s->newton);
     const int32_t* old_stencil = s->d_stencil.p;
