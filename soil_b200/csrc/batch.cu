@@ -878,6 +878,7 @@ int batch_step(soil_batch* b, bool last) {
             const uint64_t np = b->h_totals[k], total = s->nlocal + s->nghost;
             TRY(ensure(s, s->indices, np + 1, 0, pair_room(np)));
             TRY(ensure(s, s->in_count, total + 1, 0, s->acap + 1));
+            s->in_zero = 0;  // the batch's count pass leaves the counts behind
             TRY(ensure(s, s->in_start, total + 2, 0, s->acap + 2));
             TRY(ensure(s, s->in_cursor, total + 1, 0, s->acap + 1));
             TRY(ensure(s, s->in_list, np + 1, 0, pair_room(np)));

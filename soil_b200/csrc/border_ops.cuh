@@ -88,13 +88,14 @@ struct BorderWarpSmem {
 // Pass 2 for warp tile w.  base_lane: on lane k < 26 the first ghost index of
 // category k (nlocal + the totals of the categories before it).  offs holds
 // offsets inside the tile's scan chunk; cpre (NULL: a single chunk) the
-// chunks' prefixes.  sm: this warp's scratch.
+// chunks' prefixes.  sm: this warp's scratch.  host_bs (optional): the host's
+// copy of bs, which gets the capacity word too.
 __device__ __forceinline__ void border_warp_images(
     const AtomCols& c, uint64_t nlocal, uint64_t cap, const double (*shift)[3],
     const double (*vshift)[3], const BorderCats& cats, const uint8_t* face, const uint32_t* offs,
     const uint32_t* cpre, uint64_t nchunks, uint64_t nw, uint64_t w, uint32_t lane,
     uint32_t base_lane, uint32_t* bs, uint32_t* root, uint32_t* chain, uint32_t* const* send,
-    uint32_t* fold_start, uint32_t* fold_list, BorderWarpSmem& sm) {
+    uint32_t* fold_start, uint32_t* fold_list, BorderWarpSmem& sm, uint32_t* host_bs = nullptr) {
     const unsigned below = (1u << lane) - 1u;
     const uint64_t r = w * 32 + lane;
     const uint32_t bits = r < nlocal ? face[r] : 0u;
@@ -137,6 +138,7 @@ __device__ __forceinline__ void border_warp_images(
             const uint32_t g = sm.idx[k][lane];
             if (g >= cap) {
                 bs[10] = 1u;  // out of capacity: the host grows the arrays and repeats
+                if (host_bs) host_bs[10] = 1u;
                 continue;
             }
             const uint32_t parent =

@@ -183,47 +183,46 @@ void launch_cells_reuse(cudaStream_t st, uint64_t nlocal, uint64_t n, const Atom
 // the locals are already in cell order (local i is entry i - sort_start[c]
 // of its cell c), so they take their slots directly, in front of their
 // cell's ghosts; only the ghosts are scattered and ranked.
-__global__ void __launch_bounds__(kBlock) k_place_locals(uint64_t nl, const uint32_t* cell,
-                                                         const uint32_t* start,
-                                                         const uint32_t* sort_start,
-                                                         uint32_t* out) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nl;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t c = cell[i];
-        out[start[c] + ((uint32_t)i - sort_start[c])] = (uint32_t)i;
-    }
-}
-
-// Ghost g of cell c into the ghost part of c's slots (after its locals), in
-// no particular order: counts[c] still holds c's locals and ghosts, and only
-// ghosts take from it.
-__global__ void __launch_bounds__(kBlock) k_ghost_scatter(uint64_t nl, uint64_t n,
-                                                          const uint32_t* n_dev,
-                                                          const uint32_t* cell,
-                                                          const uint32_t* start, uint32_t* counts,
-                                                          uint32_t* tmp) {
+// One pass over all atoms: local i (its cell's locals are consecutive in
+// bin order already) straight to its slot; ghost g of cell c into the ghost
+// part of c's slots (after its locals), in no particular order: counts[c]
+// still holds c's locals and ghosts, and only ghosts take from it.
+__global__ void __launch_bounds__(kBlock) k_place_bins(uint64_t nl, uint64_t n,
+                                                       const uint32_t* n_dev,
+                                                       const uint32_t* cell,
+                                                       const uint32_t* start,
+                                                       const uint32_t* sort_start,
+                                                       uint32_t* counts, uint32_t* tmp,
+                                                       uint32_t* out) {
     if (n_dev) {
         const uint64_t d = *n_dev;
         n = d < n ? d : n;
     }
-    for (uint64_t g = nl + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < n;
-         g += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t c = cell[g];
-        tmp[start[c] + atomicSub(&counts[c], 1u) - 1u] = (uint32_t)g;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t c = cell[i];
+        if (i < nl) out[start[c] + ((uint32_t)i - sort_start[c])] = (uint32_t)i;
+        else tmp[start[c] + atomicSub(&counts[c], 1u) - 1u] = (uint32_t)i;
     }
 }
 
 // Each ghost at its rank among its cell's ghosts (ascending index).
+// The cells' counts (read by nothing after k_place_bins) go back to zero on
+// the way, for the next counting pass.
 __global__ void __launch_bounds__(kBlock) k_ghost_rank(uint64_t nl, uint64_t n,
                                                        const uint32_t* n_dev,
                                                        const uint32_t* cell,
                                                        const uint32_t* start,
                                                        const uint32_t* sort_start,
-                                                       const uint32_t* tmp, uint32_t* out) {
+                                                       const uint32_t* tmp, uint32_t* out,
+                                                       uint32_t* counts, uint64_t nc) {
     if (n_dev) {
         const uint64_t d = *n_dev;
         n = d < n ? d : n;
     }
+    for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < nc;
+         c += (uint64_t)gridDim.x * blockDim.x)
+        counts[c] = 0u;
     for (uint64_t g = nl + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < n;
          g += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t c = cell[g];
@@ -234,22 +233,19 @@ __global__ void __launch_bounds__(kBlock) k_ghost_rank(uint64_t nl, uint64_t n,
     }
 }
 
-void launch_place_bins(cudaStream_t st, uint64_t nl, uint64_t n, const uint32_t* n_dev,
-                       const uint32_t* cell, const uint32_t* start, const uint32_t* sort_start,
-                       uint32_t* counts, uint32_t* tmp, uint32_t* out) {
-    if (nl) {
-        note_launch();
-        k_place_locals<<<grid_wave<k_place_locals>(nl), kBlock, 0, st>>>(nl, cell, start,
-                                                                         sort_start, out);
-    }
-    if (n > nl) {
-        note_launch();
-        k_ghost_scatter<<<grid_wave<k_ghost_scatter>(n - nl), kBlock, 0, st>>>(
-            nl, n, n_dev, cell, start, counts, tmp);
-        note_launch();
-        k_ghost_rank<<<grid_wave<k_ghost_rank>(n - nl), kBlock, 0, st>>>(nl, n, n_dev, cell, start,
-                                                                         sort_start, tmp, out);
-    }
+bool launch_place_bins(cudaStream_t st, uint64_t nl, uint64_t n, uint64_t nc,
+                       const uint32_t* n_dev, const uint32_t* cell, const uint32_t* start,
+                       const uint32_t* sort_start, uint32_t* counts, uint32_t* tmp,
+                       uint32_t* out) {
+    if (n == 0) return false;
+    note_launch();
+    k_place_bins<<<grid_wave<k_place_bins>(n), kBlock, 0, st>>>(nl, n, n_dev, cell, start,
+                                                                 sort_start, counts, tmp, out);
+    if (n == nl) return false;
+    note_launch();
+    k_ghost_rank<<<grid_wave<k_ghost_rank>(n - nl > nc ? n - nl : nc), kBlock, 0, st>>>(
+        nl, n, n_dev, cell, start, sort_start, tmp, out, counts, nc);
+    return true;
 }
 
 // Restore the stable (ascending index) order inside every segment.
@@ -269,7 +265,9 @@ void launch_segsort(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint3
 // The transposed lists' sort: segment a (atom a's in-list) ascending, and
 // split[a] = its entries below a (the rows summed before a's own row).
 __global__ void __launch_bounds__(kBlock) k_segsort_split(uint64_t nseg, const uint32_t* start,
-                                                          uint32_t* items, uint32_t* split) {
+                                                          uint32_t* items, uint32_t* split,
+                                                          FillGuard g) {
+    if (!guard_open(g)) return;
     for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < nseg;
          s += (uint64_t)gridDim.x * blockDim.x) {
         split[s] = sort_segment(items, start[s], start[s + 1], (uint32_t)s);
@@ -277,10 +275,11 @@ __global__ void __launch_bounds__(kBlock) k_segsort_split(uint64_t nseg, const u
 }
 
 void launch_segsort_split(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint32_t* items,
-                          uint32_t* split) {
+                          uint32_t* split, const FillGuard* g) {
     if (nseg == 0) return;
     note_launch();
-    k_segsort_split<<<grid_wave<k_segsort_split>(nseg), kBlock, 0, st>>>(nseg, start, items, split);
+    k_segsort_split<<<grid_wave<k_segsort_split>(nseg), kBlock, 0, st>>>(
+        nseg, start, items, split, g ? *g : FillGuard{});
 }
 
 // split[a] of already sorted transposed lists
@@ -362,7 +361,13 @@ __global__ void __launch_bounds__(kBlock) k_sorted_views(uint64_t n, const uint3
                                                          AtomCols c, uint32_t* asi, double4* sp,
                                                          float4* spf, double o0, double o1,
                                                          double o2, BuildPos bp,
-                                                         const uint32_t* n_dev, int atom_in_w) {
+                                                         const uint32_t* n_dev, int atom_in_w,
+                                                         DevFlags* clear) {
+    if (clear && blockIdx.x == 0 && threadIdx.x == 0) {  // the pair build's counters
+        clear->candidates = 0;
+        clear->rechecked = 0;
+        clear->error = 0u;
+    }
     if (n_dev) {  // the count known only on the device (an upper bound in n)
         const uint64_t d = *n_dev;
         n = d < n ? d : n;
@@ -375,12 +380,12 @@ __global__ void __launch_bounds__(kBlock) k_sorted_views(uint64_t n, const uint3
 void launch_sorted_views(cudaStream_t st, uint64_t n, const uint32_t* sorted, const AtomCols& c,
                          uint32_t* atom_sorted_idx, double4* sp, float4* spf,
                          const double origin[3], const BuildPos& bp, const uint32_t* n_dev,
-                         bool atom_in_w) {
+                         bool atom_in_w, DevFlags* clear) {
     if (n == 0) return;
     note_launch();
     k_sorted_views<<<grid_wave<k_sorted_views>(n), kBlock, 0, st>>>(
         n, sorted, c, atom_sorted_idx, sp, spf, origin[0], origin[1], origin[2], bp, n_dev,
-        atom_in_w ? 1 : 0);
+        atom_in_w ? 1 : 0, clear);
 }
 
 }  // namespace soil

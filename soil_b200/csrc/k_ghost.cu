@@ -165,8 +165,11 @@ __global__ void __launch_bounds__(kBlock) k_border_cat_scan(const uint32_t* coun
 // Chunk totals -> exclusive chunk prefixes (in place) and category totals;
 // clears the capacity word bs[10] that pass 3 may set.
 __global__ void __launch_bounds__(kBlock) k_border_chunk_prefix(uint32_t* ctot, uint64_t nchunks,
-                                                                uint32_t* bs) {
-    if (threadIdx.x == 0) bs[10] = 0u;
+                                                                uint32_t* bs, uint32_t* host_bs) {
+    if (threadIdx.x == 0) {
+        bs[10] = 0u;
+        if (host_bs) host_bs[10] = 0u;
+    }
     for (uint32_t k = threadIdx.x; k <= (uint32_t)kBorderCats; k += blockDim.x) {
         uint32_t acc = 0;
         for (uint64_t ch = 0; ch < nchunks; ++ch) {
@@ -184,10 +187,15 @@ __global__ void __launch_bounds__(kBlock) k_border_chunk_prefix(uint32_t* ctot, 
 __global__ void __launch_bounds__(kBlock) k_border_images(
     uint64_t nlocal, uint64_t cap, AtomCols c, BorderPass bp, BorderCats cats, const uint8_t* face,
     const uint32_t* offs, const uint32_t* cpre, uint64_t nchunks, uint64_t nw, uint32_t* bs,
-    uint32_t* root, uint32_t* chain, SendPtrs send, uint32_t* fold_start, uint32_t* fold_list) {
+    uint32_t* root, uint32_t* chain, SendPtrs send, uint32_t* fold_start, uint32_t* fold_list,
+    uint32_t* host_bs) {
     __shared__ BorderWarpSmem sm[kBlock / 32];
     const uint32_t lane = threadIdx.x & 31u;
-    if (blockIdx.x == 0 && threadIdx.x == 0) border_state_words(cats, nlocal, bs);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        border_state_words(cats, nlocal, bs);
+        if (host_bs)
+            for (int k = 0; k < 10; ++k) host_bs[k] = bs[k];
+    }
     // first ghost index of category `lane` (lanes below 26)
     const uint32_t tot = lane < kBorderCats ? bs[kBorderTotals + lane] : 0u;
     const uint32_t base_lane = (uint32_t)nlocal + warp_exclusive_sum(tot, lane);
@@ -195,13 +203,14 @@ __global__ void __launch_bounds__(kBlock) k_border_images(
     for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32; w < nw; w += nwarps)
         border_warp_images(c, nlocal, cap, bp.shift, bp.vshift, cats, face, offs, cpre, nchunks,
                            nw, w, lane, base_lane, bs, root, chain, send.p, fold_start, fold_list,
-                           sm[threadIdx.x / 32]);
+                           sm[threadIdx.x / 32], host_bs);
 }
 
 void launch_borders(cudaStream_t st, uint64_t nlocal, uint64_t cap, const AtomCols& c,
                     const BorderCats& cats, const BorderPass& bp, uint8_t* face, uint32_t* counts,
                     uint32_t* offs, uint32_t* bs, uint32_t* ghost_root, uint32_t* ghost_chain,
-                    const SendPtrs& send, uint32_t* fold_start, uint32_t* fold_list) {
+                    const SendPtrs& send, uint32_t* fold_start, uint32_t* fold_list,
+                    uint32_t* host_bs) {
     if (nlocal == 0) return;
     const uint64_t nw = (nlocal + 31) / 32;
     const uint64_t nchunks = (nw + kScanChunk - 1) / kScanChunk;
@@ -213,11 +222,11 @@ void launch_borders(cudaStream_t st, uint64_t nlocal, uint64_t cap, const AtomCo
     k_border_cat_scan<<<(unsigned)((kBorderCats + 1) * nchunks), kBlock, 0, st>>>(counts, offs, nw,
                                                                                 ctot, nchunks);
     note_launch();
-    k_border_chunk_prefix<<<1, kBlock, 0, st>>>(ctot, nchunks, bs);
+    k_border_chunk_prefix<<<1, kBlock, 0, st>>>(ctot, nchunks, bs, host_bs);
     note_launch();
     k_border_images<<<grid_wave<k_border_images>(nw * 32), kBlock, 0, st>>>(
         nlocal, cap, c, bp, cats, face, offs, ctot, nchunks, nw, bs, ghost_root, ghost_chain, send,
-        fold_start, fold_list);
+        fold_start, fold_list, host_bs);
 }
 
 __global__ void __launch_bounds__(kBlock) k_forward(uint64_t nlocal, uint64_t nghost, AtomCols c,

@@ -68,7 +68,10 @@ __global__ void __launch_bounds__(kBlock) k_pairs_rows(PairParams p, uint32_t* r
 template <bool UNIFORM, bool FP32>
 __global__ void __launch_bounds__(kBlock) k_pairs_fill(PairParams p, const uint32_t* rowcount,
                                                        const uint32_t* slots,
-                                                       const uint32_t* offsets, uint32_t* indices) {
+                                                       const uint32_t* offsets, uint32_t* indices,
+                                                       FillGuard g) {
+    guard_publish(g);
+    if (!guard_open(g)) return;
     const Filter<UNIFORM, FP32> test(p);
     const uint32_t K = (uint32_t)p.row_slots;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < p.nlocal;
@@ -119,40 +122,42 @@ __global__ void __launch_bounds__(kBlock) k_pairs_fill(PairParams p, const uint3
 template <bool UNIFORM, bool FP32>
 static void launch_pairs_t(cudaStream_t st, const PairParams& p, uint32_t* rowcount,
                            uint32_t* slots, const uint32_t* offsets, uint32_t* indices,
-                           DevFlags* flags, bool fill) {
+                           DevFlags* flags, const FillGuard* g) {
     note_launch();
-    if (!fill)
+    if (!g)
         k_pairs_rows<UNIFORM, FP32><<<grid_wave<k_pairs_rows<UNIFORM, FP32>>(p.nlocal), kBlock, 0, st>>>(p, rowcount, slots,
                                                                             flags);
     else
         k_pairs_fill<UNIFORM, FP32><<<grid_wave<k_pairs_fill<UNIFORM, FP32>>(p.nlocal), kBlock, 0, st>>>(p, rowcount, slots,
-                                                                            offsets, indices);
+                                                                            offsets, indices, *g);
 }
 
+// g == nullptr: pass 1; else pass 2 under guard *g
 static void dispatch_pairs(cudaStream_t st, const PairParams& p, uint32_t* rowcount,
                            uint32_t* slots, const uint32_t* offsets, uint32_t* indices,
-                           DevFlags* flags, bool fill) {
+                           DevFlags* flags, const FillGuard* g) {
     const bool fp32 = p.filter == SOIL_FILTER_FP32_RECHECK;
     if (p.uniform) {
-        if (fp32) launch_pairs_t<true, true>(st, p, rowcount, slots, offsets, indices, flags, fill);
-        else launch_pairs_t<true, false>(st, p, rowcount, slots, offsets, indices, flags, fill);
+        if (fp32) launch_pairs_t<true, true>(st, p, rowcount, slots, offsets, indices, flags, g);
+        else launch_pairs_t<true, false>(st, p, rowcount, slots, offsets, indices, flags, g);
     } else {
-        if (fp32) launch_pairs_t<false, true>(st, p, rowcount, slots, offsets, indices, flags, fill);
-        else launch_pairs_t<false, false>(st, p, rowcount, slots, offsets, indices, flags, fill);
+        if (fp32) launch_pairs_t<false, true>(st, p, rowcount, slots, offsets, indices, flags, g);
+        else launch_pairs_t<false, false>(st, p, rowcount, slots, offsets, indices, flags, g);
     }
 }
 
 void launch_pair_count(cudaStream_t st, const PairParams& p, uint32_t* rowcount, uint32_t* slots,
                        DevFlags* flags) {
     if (p.nlocal == 0 || p.ncells == 0) return;
-    dispatch_pairs(st, p, rowcount, slots, nullptr, nullptr, flags, false);
+    dispatch_pairs(st, p, rowcount, slots, nullptr, nullptr, flags, nullptr);
 }
 
 void launch_pair_fill(cudaStream_t st, const PairParams& p, const uint32_t* rowcount,
-                      const uint32_t* slots, const uint32_t* offsets, uint32_t* indices) {
+                      const uint32_t* slots, const uint32_t* offsets, uint32_t* indices,
+                      const FillGuard& g) {
     if (p.nlocal == 0) return;
     dispatch_pairs(st, p, const_cast<uint32_t*>(rowcount), const_cast<uint32_t*>(slots), offsets,
-                   indices, nullptr, true);
+                   indices, nullptr, &g);
 }
 
 __global__ void __launch_bounds__(kBlock) k_in_count(uint64_t nlocal, const uint32_t* offsets,

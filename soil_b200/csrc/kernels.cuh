@@ -181,15 +181,18 @@ void launch_cells_reuse(cudaStream_t st, uint64_t nlocal, uint64_t n, const Atom
 // sort on the same grid: local i of cell c at start[c] + i - sort_start[c],
 // then c's ghosts [nl, n) in ascending order after its locals.  counts: the
 // cells' local + ghost counts (the ghosts' part is consumed); tmp: scratch of
-// the atoms' size.
-void launch_place_bins(cudaStream_t st, uint64_t nl, uint64_t n, const uint32_t* n_dev,
-                       const uint32_t* cell, const uint32_t* start, const uint32_t* sort_start,
-                       uint32_t* counts, uint32_t* tmp, uint32_t* out);
+// the atoms' size.  Returns true when counts[0, nc) were put back to zero
+// (there were ghost slots to rank).
+bool launch_place_bins(cudaStream_t st, uint64_t nl, uint64_t n, uint64_t nc,
+                       const uint32_t* n_dev, const uint32_t* cell, const uint32_t* start,
+                       const uint32_t* sort_start, uint32_t* counts, uint32_t* tmp,
+                       uint32_t* out);
 // sort every segment [start[s], start[s+1]) ascending -> stable counting sort
 void launch_segsort(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint32_t* items);
 // the same, and split[s] = entries of segment s below s (transposed lists)
+struct FillGuard;
 void launch_segsort_split(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint32_t* items,
-                          uint32_t* split);
+                          uint32_t* split, const FillGuard* g = nullptr);
 // split[s] alone, for segments already sorted
 void launch_in_split(cudaStream_t st, uint64_t nseg, const uint32_t* start, const uint32_t* items,
                      uint32_t* split);
@@ -211,11 +214,13 @@ void launch_permute_u32(cudaStream_t st, uint64_t n, const uint32_t* perm, const
 // inverse[sorted[m]] = m and the sorted records sp[m] = {x, y, z, cutoff}
 // (plus the FP32 grid-relative copy spf when spf != nullptr); atom_in_w (for
 // a uniform cutoff, whose test reads no radius) stores sorted[m]'s bits in
-// place of the cutoff
+// place of the cutoff; clear (when given, and n > 0) gets its candidates,
+// rechecked and error words zeroed
 void launch_sorted_views(cudaStream_t st, uint64_t n, const uint32_t* sorted, const AtomCols& c,
                          uint32_t* atom_sorted_idx, double4* sp, float4* spf,
                          const double origin[3], const BuildPos& bp = BuildPos{},
-                         const uint32_t* n_dev = nullptr, bool atom_in_w = false);
+                         const uint32_t* n_dev = nullptr, bool atom_in_w = false,
+                         DevFlags* clear = nullptr);
 
 // ---- ghosts (k_ghost.cu) --------------------------------------------------
 struct BorderDim {
@@ -279,12 +284,15 @@ struct SendPtrs {
 // image written from its root.  bs must be zero; ghosts beyond `cap` set
 // bs[10].  offs holds (kBorderCats + 1) * nw words and counts that plus
 // (kBorderCats + 1) * ceil(nw / 8192) (nw = ceil(nlocal / 32)).
-// cats: border_cats(), or border_cats_masked() for axes without periodicity
+// cats: border_cats(), or border_cats_masked() for axes without periodicity.
+// host_bs (optional, host memory mapped for the device): the kernels also
+// write bs[0, 11) there, so no copy is needed after them.
 void launch_borders(cudaStream_t st, uint64_t nlocal, uint64_t cap, const AtomCols& c,
                     const BorderCats& cats, const BorderPass& bp, uint8_t* face, uint32_t* counts,
                     uint32_t* offs,
                     uint32_t* bs, uint32_t* ghost_root, uint32_t* ghost_chain,
-                    const SendPtrs& send, uint32_t* fold_start, uint32_t* fold_list);
+                    const SendPtrs& send, uint32_t* fold_start, uint32_t* fold_list,
+                    uint32_t* host_bs = nullptr);
 // forward_comm: every ghost from its root local atom through its swap chain
 void launch_forward(cudaStream_t st, uint64_t nlocal, uint64_t nghost, const AtomCols& c,
                     const uint32_t* ghost_root, const uint32_t* ghost_chain, const SwapConst& sc,
@@ -359,9 +367,35 @@ struct PairSegs {
 void launch_pair_count_staged(cudaStream_t st, const PairParams& p, const PairSegs& sg,
                               uint32_t* rowcount, uint32_t* slots, DevFlags* flags);
 constexpr uint32_t SOIL_PAIRS_ERR_STAGING = 8u;
+// A pass launched before the host has read the pair total runs only when the
+// total fits its arrays: *total + 1 <= cap, and err[0] (DevFlags::error) and
+// err[1] (DevFlags::fault) are clear.  Every thread reads the same words, so
+// a launch runs whole or not at all.  A default guard (null total) is open.
+// Pass 2 can also hand the host what it waits for (pub_total != null): the
+// first thread copies *total to *pub_total and *flags to *pub_flags (host
+// memory mapped for the device), whether or not the guard lets it run.
+struct FillGuard {
+    const uint32_t* total = nullptr;
+    uint64_t cap = 0;
+    const uint32_t* err = nullptr;
+    uint32_t* pub_total = nullptr;
+    const DevFlags* flags = nullptr;
+    DevFlags* pub_flags = nullptr;
+};
+__device__ __forceinline__ bool guard_open(const FillGuard& g) {
+    if (!g.total) return true;
+    return (uint64_t)*g.total + 1 <= g.cap && g.err[0] == 0u && g.err[1] == 0u;
+}
+__device__ __forceinline__ void guard_publish(const FillGuard& g) {
+    if (g.pub_total && blockIdx.x == 0 && threadIdx.x == 0) {
+        *g.pub_total = *g.total;
+        *g.pub_flags = *g.flags;
+    }
+}
 // Pass 2: rows into neighbor_indices at offsets[] (rows longer than K re-derived).
 void launch_pair_fill(cudaStream_t st, const PairParams& p, const uint32_t* rowcount,
-                      const uint32_t* slots, const uint32_t* offsets, uint32_t* indices);
+                      const uint32_t* slots, const uint32_t* offsets, uint32_t* indices,
+                      const FillGuard& g = FillGuard{});
 // incoming (transposed) lists: for each atom j, the rows i with j in row(i)
 void launch_in_count(cudaStream_t st, uint64_t nlocal, const uint32_t* offsets,
                      const uint32_t* indices, uint32_t* incount);

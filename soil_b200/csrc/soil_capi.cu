@@ -949,11 +949,17 @@ int phase_borders_defer(soil_sys* s, bool defer) {
         for (int k = 0; k < kNumSwaps; ++k) send.p[k] = s->send[k].p;
         // With locals the passes write every word the host reads.
         if (s->nlocal == 0) CK(cudaMemsetAsync(s->bstate.p, 0, kBorderStateWords * 4, s->st));
+        // A deferred pass with locals writes the words the host reads straight
+        // into its (mapped) copy: no copy in the stream after the pass.
+        const bool direct = defer && s->nlocal > 0;
         launch_borders(s->st, s->nlocal, s->acap, s->A, cats, bp, s->face_flags.p, s->bcount.p,
                        s->boff.p, s->bstate.p, s->ghost_root.p, s->ghost_chain.p, send,
-                       s->fold_start.p, s->fold_list.p);
+                       s->fold_start.p, s->fold_list.p,
+                       direct ? s->hword_dev + kBorderStateWords : nullptr);
         TRY(check_launch(s));
-        CK(cudaMemcpyAsync(hb, s->bstate.p, kBorderStateWords * 4, cudaMemcpyDeviceToHost, s->st));
+        if (!direct)
+            CK(cudaMemcpyAsync(hb, s->bstate.p, kBorderStateWords * 4, cudaMemcpyDeviceToHost,
+                               s->st));
         if (defer) {
             for (int d = 0; d < 3; ++d) s->pending_bds[d] = bds[d];
             s->borders_pending = true;
@@ -1115,6 +1121,7 @@ int build_in_lists(soil_sys* s) {
     TRY(ensure(s, s->in_list, s->npairs + 1, 0, pair_room(s->npairs)));
     TRY(ensure(s, s->scan_tmp, scan_temp_words(total + 2)));
     CK(cudaMemsetAsync(s->in_count.p, 0, total * 4, s->st));
+    s->in_zero = 0;  // left holding the counts
     launch_in_count(s->st, s->nlocal, s->offsets.p, s->indices.p, s->in_count.p);
     TRY(scan_1p(s, s->in_count.p, s->in_start.p, total));
     CK(cudaMemcpyAsync(s->in_cursor.p, s->in_start.p, total * 4, cudaMemcpyDeviceToDevice, s->st));
@@ -1409,9 +1416,11 @@ int phase_neighbor(soil_sys* s) {
     TRY(scan_1p(s, s->cell_counts.p, s->cell_start.p, nc));
     if (after_sort) {
         // the locals are in bin order already: only the ghosts are sorted
-        launch_place_bins(s->st, nl, total, n_dev, s->atom_cell.p, s->cell_start.p,
-                          s->sort_start.p, s->cell_counts.p, s->ghost_tmp.p, s->sorted_atoms.p);
-        s->counts_clean = 0;  // the locals' counts remain
+        const bool zeroed =
+            launch_place_bins(s->st, nl, total, nc, n_dev, s->atom_cell.p, s->cell_start.p,
+                              s->sort_start.p, s->cell_counts.p, s->ghost_tmp.p,
+                              s->sorted_atoms.p);
+        s->counts_clean = zeroed ? nc : 0;  // else the locals' counts remain
     } else {
         launch_scatter_consume(s->st, total, s->atom_cell.p, s->cell_start.p, s->cell_counts.p,
                                s->sorted_atoms.p, n_dev);
@@ -1424,7 +1433,8 @@ int phase_neighbor(soil_sys* s) {
     bpos.z = s->lbz.p;
     bpos.nlocal = nl;
     launch_sorted_views(s->st, total, s->sorted_atoms.p, s->A, s->asi.p, s->sp.p,
-                        fp32 ? s->spf.p : nullptr, s->blo, bpos, n_dev, s->has_uniform);
+                        fp32 ? s->spf.p : nullptr, s->blo, bpos, n_dev, s->has_uniform,
+                        s->dflags);  // also clears the counters of the pair passes
     const std::vector<int32_t>& sten = s->newton ? s->stencil_fwd : s->stencil;
     const std::vector<int32_t> runs = stencil_runs(sten, s->newton);
     const int32_t* old_stencil = s->d_stencil.p;
@@ -1454,9 +1464,10 @@ int phase_neighbor(soil_sys* s) {
     p.sf_sq = s->skin_fraction * s->skin_fraction;
     p.sf = s->skin_fraction;
     p.eps32 = pair_eps(s);
-    // candidates, rechecked and error are adjacent: one clear
+    // candidates, rechecked and error are adjacent: one clear (the sorted
+    // views cleared them when there were atoms)
     static_assert(offsetof(DevFlags, error) == offsetof(DevFlags, candidates) + 16, "DevFlags layout");
-    CK(cudaMemsetAsync(&s->dflags->candidates, 0, 20, s->st));
+    if (total == 0) CK(cudaMemsetAsync(&s->dflags->candidates, 0, 20, s->st));
     s->in_lists_valid = false;
     s->seq_valid = false;
     s->order_valid = false;
@@ -1469,10 +1480,15 @@ int phase_neighbor(soil_sys* s) {
     p.in_start = nullptr;
     p.in_list = nullptr;
     p.pre_ranges = pairs_pre_ranges();
+    uint64_t in_zero = 0;  // in_count[0, in_zero) is zero already
     if (with_in) {
         TRY(ensure(s, s->in_count, total + 1, 0, s->acap + 1));
         TRY(ensure(s, s->in_start, total + 2, 0, s->acap + 2));
-        CK(cudaMemsetAsync(s->in_count.p, 0, total * 4, s->st));
+        in_zero = s->in_zero_at == s->in_count.p ? s->in_zero : 0;
+        if (in_zero < total)
+            CK(cudaMemsetAsync(s->in_count.p + in_zero, 0, (total - in_zero) * 4, s->st));
+        s->in_zero = 0;  // counted into now; zero again once pass 2 has consumed it
+        s->in_zero_at = s->in_count.p;
         p.in_count = s->in_count.p;
     }
     PairSegs sg;
@@ -1482,9 +1498,42 @@ int phase_neighbor(soil_sys* s) {
         launch_pair_count(s->st, p, s->rowcount.p, s->row_slots.p, s->dflags);
     TRY(scan_1p(s, s->rowcount.p, s->offsets.p, nl));
     if (with_in) TRY(scan_1p(s, s->in_count.p, s->in_start.p, total));
-    CK(cudaMemcpyAsync(&s->hword[0], s->offsets.p + nl, 4, cudaMemcpyDeviceToHost, s->st));
+    if (!s->ev_counts) CK(cudaEventCreateWithFlags(&s->ev_counts, cudaEventDisableTiming));
+    // Pass 2 goes in before the host reads the pair total, into the arrays it
+    // has: the stream stays busy while the host waits for the counts, which
+    // pass 2 itself writes to the host's words.  The guard lets it run only
+    // when the total fits (and nothing failed); else it is launched again
+    // below, into grown arrays.  (The transposed lists hold one entry per
+    // pair, so one total bounds both arrays.)
+    if (with_in) {
+        TRY(ensure(s, s->in_split, total + 1, 0, s->acap + 1));
+        p.in_start = s->in_start.p;
+        p.in_list = s->in_list.p;
+    }
+    FillGuard guard;
+    guard.total = s->offsets.p + nl;
+    guard.cap = s->indices.cap;
+    if (with_in && s->in_list.cap < guard.cap) guard.cap = s->in_list.cap;
+    guard.err = &s->dflags->error;
+    guard.pub_total = s->hword_dev;
+    guard.flags = s->dflags;
+    guard.pub_flags = s->hflags_dev;
+    const bool early = s->indices.p && (!with_in || s->in_list.p) && nl > 0;
+    if (early) {
+        launch_pair_fill(s->st, p, s->rowcount.p, s->row_slots.p, s->offsets.p, s->indices.p,
+                         guard);
+        CK(cudaEventRecord(s->ev_counts, s->st));
+        if (with_in)
+            launch_segsort_split(s->st, total, s->in_start.p, s->in_list.p, s->in_split.p, &guard);
+    } else {
+        CK(cudaMemcpyAsync(&s->hword[0], s->offsets.p + nl, 4, cudaMemcpyDeviceToHost, s->st));
+        CK(cudaMemcpyAsync(s->hflags, s->dflags, sizeof(DevFlags), cudaMemcpyDeviceToHost, s->st));
+        CK(cudaEventRecord(s->ev_counts, s->st));
+    }
     TRY(check_launch(s));
-    TRY(read_flags(s));
+    CK(cudaEventSynchronize(s->ev_counts));
+    if (s->hflags->fault & SOIL_SCAN_ERR)
+        return fail(s->ctx, SOIL_ERR_CUDA, "a single-pass scan's look-back wait ran out");
     if (pend) {  // the deferred border pass, now read back
         s->borders_pending = false;
         const uint32_t* hb = s->hword + kBorderStateWords;
@@ -1500,27 +1549,27 @@ int phase_neighbor(soil_sys* s) {
         total = s->nlocal + s->nghost;
     }
     const uint64_t np = s->hword[0];
-    TRY(ensure(s, s->indices, np + 1, 0, pair_room(np)));
     if (s->hflags->error & SOIL_PAIRS_ERR_STAGING)
         return fail(s->ctx, SOIL_ERR_CUDA, "pair build: a shared-memory staging wait ran out");
     if (s->hflags->error)
         return fail(s->ctx, SOIL_ERR_INVALID, "neighbor stencil left the bin grid (atom outside the ghost layers)");
-    if (with_in) {
-        TRY(ensure(s, s->in_list, np + 1, 0, pair_room(np)));
-        p.in_start = s->in_start.p;
-        p.in_list = s->in_list.p;
+    if (!early || np + 1 > guard.cap) {  // the early pass did not run: again, into room for np
+        TRY(ensure(s, s->indices, np + 1, 0, pair_room(np)));
+        if (with_in) {
+            TRY(ensure(s, s->in_list, np + 1, 0, pair_room(np)));
+            p.in_list = s->in_list.p;
+        }
+        launch_pair_fill(s->st, p, s->rowcount.p, s->row_slots.p, s->offsets.p, s->indices.p);
+        if (with_in)
+            launch_segsort_split(s->st, total, s->in_start.p, s->in_list.p, s->in_split.p);
+        TRY(check_launch(s));
     }
-    launch_pair_fill(s->st, p, s->rowcount.p, s->row_slots.p, s->offsets.p, s->indices.p);
-    if (with_in) {
-        TRY(ensure(s, s->in_split, total + 1, 0, s->acap + 1));
-        launch_segsort_split(s->st, total, s->in_start.p, s->in_list.p, s->in_split.p);
-    }
-    TRY(check_launch(s));
     s->npairs = np;
     s->rebuilds += 1;
     if (with_in) {
         s->in_lists_valid = true;
         s->split_valid = true;
+        s->in_zero = in_zero > total ? in_zero : total;  // pass 2 took every count back
     }
     // the grouped sequences are built when a consumer kernel first needs them
     return SOIL_OK;
@@ -2058,8 +2107,11 @@ int soil_sys_create(soil_ctx* ctx, const soil_box* box, const soil_neigh_cfg* cf
     s->filter = cfg->filter;
     int r;
     if ((r = dev_alloc(s, (void**)&s->dflags, sizeof(DevFlags))) != SOIL_OK ||
-        cudaMallocHost((void**)&s->hflags, sizeof(DevFlags)) != cudaSuccess ||
-        cudaMallocHost((void**)&s->hword, 2 * kBorderStateWords * 4) != cudaSuccess) {
+        cudaHostAlloc((void**)&s->hflags, sizeof(DevFlags), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostAlloc((void**)&s->hword, 2 * kBorderStateWords * 4, cudaHostAllocMapped) !=
+            cudaSuccess ||
+        cudaHostGetDevicePointer((void**)&s->hflags_dev, s->hflags, 0) != cudaSuccess ||
+        cudaHostGetDevicePointer((void**)&s->hword_dev, s->hword, 0) != cudaSuccess) {
         cudaGetLastError();
         soil_sys_destroy(s);
         return r != SOIL_OK ? r : fail(ctx, SOIL_ERR_OOM, "pinned allocation failed");
@@ -2100,6 +2152,7 @@ int soil_sys_destroy(soil_sys* s) {
     fr(s->scan_tmp); fr(s->d_stencil); fr(s->stage); fr(s->d_colptrs);
     resolve_timers(s);
     for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
+    if (s->ev_counts) cudaEventDestroy(s->ev_counts);
     if (s->dflags) dev_free(s, s->dflags, sizeof(DevFlags));
     if (s->hflags) cudaFreeHost(s->hflags);
     if (s->hword) cudaFreeHost(s->hword);

@@ -131,6 +131,10 @@ struct soil_sys {
     // cell_counts[0, counts_clean) is known to be zero (the consuming scatters
     // leave it so); counts_at: the allocation that holds
     uint64_t counts_clean = 0;
+    // in_count[0, in_zero) is known to be zero (pass 2 of the pair build
+    // consumes the counts of pass 1); in_zero_at: the array it describes
+    uint64_t in_zero = 0;
+    const uint32_t* in_zero_at = nullptr;
     const uint32_t* counts_at = nullptr;
     std::vector<int32_t> stencil_on_device;  // the stencil last uploaded to d_stencil
     DArr<uint32_t> atom_cell, sorted_atoms, asi, rowcount, offsets, indices, row_slots;
@@ -180,6 +184,10 @@ struct soil_sys {
     DevFlags* dflags = nullptr;
     DevFlags* hflags = nullptr;  // pinned mirror
     uint32_t* hword = nullptr;   // pinned scratch words
+    // the same two buffers as the device addresses them (mapped host memory):
+    // kernels that end a phase write the host's words directly
+    DevFlags* hflags_dev = nullptr;
+    uint32_t* hword_dev = nullptr;
 
     // ---- phase timers ----
     struct TimedSpan {
@@ -195,6 +203,7 @@ struct soil_sys {
     uint64_t timer_intervals[SOIL_NUM_TIMERS] = {};
     int open_timer = -1;
     cudaEvent_t open_ev = nullptr;
+    cudaEvent_t ev_counts = nullptr;  // the pair build's counts are on the host
     uint64_t open_launches = 0;
 
     // ---- bookkeeping ----
