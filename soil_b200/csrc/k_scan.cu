@@ -48,17 +48,37 @@ __device__ __forceinline__ void store8_scan(uint32_t* out, uint64_t base, uint64
         if (base + k < n) out[base + k] = o[k];
 }
 
-__global__ void __launch_bounds__(kBlock) k_scan_reduce(const uint32_t* in, uint64_t n,
-                                                        uint32_t* partial) {
+// Up to two independent scans in one launch: blocks [0, tiles0) take tiles of
+// scan 0, the rest tiles of scan 1 (each with its own partials).
+struct ScanJobs {
+    const uint32_t* in[2];
+    uint32_t* out[2];
+    uint64_t n[2];
+    uint32_t* partial[2];
+    uint64_t ntiles[2];
+};
+
+__device__ __forceinline__ int scan_job(const ScanJobs& J, uint64_t* tile) {
+    if (blockIdx.x < J.ntiles[0]) {
+        *tile = blockIdx.x;
+        return 0;
+    }
+    *tile = blockIdx.x - J.ntiles[0];
+    return 1;
+}
+
+__global__ void __launch_bounds__(kBlock) k_scan_reduce(ScanJobs J) {
     __shared__ uint32_t tot;
-    const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+    uint64_t t;
+    const int j = scan_job(J, &t);
+    const uint64_t base = t * kScanTile + (uint64_t)threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
-    load8(in, base, n, v);
+    load8(J.in[j], base, J.n[j], v);
     uint32_t s = 0;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) s += v[k];
     block_exclusive_scan(s, &tot);
-    if (threadIdx.x == 0) partial[blockIdx.x] = tot;
+    if (threadIdx.x == 0) J.partial[j][t] = tot;
 }
 
 // One CTA: exclusive scan of the tile sums in place, grand total to partial[ntiles].
@@ -105,15 +125,17 @@ __global__ void __launch_bounds__(kBlock) k_scan_down(const uint32_t* in, uint32
 // from L2), so the scan is two launches.  The last CTA writes out[n].
 constexpr uint64_t kScanCarryTiles = 4096;
 
-__global__ void __launch_bounds__(kBlock) k_scan_down_carry(const uint32_t* in, uint32_t* out,
-                                                            uint64_t n, const uint32_t* partial,
-                                                            uint64_t ntiles) {
+__global__ void __launch_bounds__(kBlock) k_scan_down_carry(ScanJobs J) {
     __shared__ uint32_t tot, s_carry;
-    const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+    uint64_t t;
+    const int j = scan_job(J, &t);
+    const uint64_t n = J.n[j];
+    const uint32_t* partial = J.partial[j];
+    const uint64_t base = t * kScanTile + (uint64_t)threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
-    load8(in, base, n, v);
-    uint32_t c = 0;  // this thread's share of the sums of tiles [0, blockIdx.x)
-    for (uint32_t t = threadIdx.x; t < blockIdx.x; t += kBlock) c += partial[t];
+    load8(J.in[j], base, n, v);
+    uint32_t c = 0;  // this thread's share of the sums of tiles [0, t)
+    for (uint64_t q = threadIdx.x; q < t; q += kBlock) c += partial[q];
     block_exclusive_scan(c, &tot);
     if (threadIdx.x == 0) s_carry = tot;
     __syncthreads();
@@ -122,11 +144,21 @@ __global__ void __launch_bounds__(kBlock) k_scan_down_carry(const uint32_t* in, 
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) s += v[k];
     const uint32_t pre = block_exclusive_scan(s, &tot) + carry;
-    store8_scan(out, base, n, v, pre);
-    if (blockIdx.x + 1 == ntiles && threadIdx.x == 0) out[n] = carry + tot;
+    store8_scan(J.out[j], base, n, v, pre);
+    if (t + 1 == J.ntiles[j] && threadIdx.x == 0) J.out[j][n] = carry + tot;
 }
 
 uint64_t scan_temp_words(uint64_t n) { return (n + kScanTile - 1) / kScanTile + 2; }
+
+static ScanJobs one_job(const uint32_t* in, uint32_t* out, uint64_t n, uint32_t* temp) {
+    ScanJobs J{};
+    J.in[0] = in;
+    J.out[0] = out;
+    J.n[0] = n;
+    J.partial[0] = temp;
+    J.ntiles[0] = (n + kScanTile - 1) / kScanTile;
+    return J;
+}
 
 void exclusive_scan_u32(cudaStream_t st, const uint32_t* in, uint32_t* out, uint64_t n,
                         uint32_t* temp) {
@@ -135,17 +167,38 @@ void exclusive_scan_u32(cudaStream_t st, const uint32_t* in, uint32_t* out, uint
         cudaMemsetAsync(out, 0, sizeof(uint32_t), st);
         return;
     }
+    const ScanJobs J = one_job(in, out, n, temp);
     note_launch();
-    k_scan_reduce<<<(unsigned)ntiles, kBlock, 0, st>>>(in, n, temp);
+    k_scan_reduce<<<(unsigned)ntiles, kBlock, 0, st>>>(J);
     if (ntiles <= kScanCarryTiles) {
         note_launch();
-        k_scan_down_carry<<<(unsigned)ntiles, kBlock, 0, st>>>(in, out, n, temp, ntiles);
+        k_scan_down_carry<<<(unsigned)ntiles, kBlock, 0, st>>>(J);
         return;
     }
     note_launch();
     k_scan_partials<<<1, kBlock, 0, st>>>(temp, ntiles);
     note_launch();
     k_scan_down<<<(unsigned)ntiles, kBlock, 0, st>>>(in, out, n, temp, ntiles);
+}
+
+void exclusive_scan_u32_pair(cudaStream_t st, const uint32_t* in0, uint32_t* out0, uint64_t n0,
+                             const uint32_t* in1, uint32_t* out1, uint64_t n1, uint32_t* temp) {
+    const uint64_t t0 = (n0 + kScanTile - 1) / kScanTile, t1 = (n1 + kScanTile - 1) / kScanTile;
+    if (t0 == 0 || t1 == 0 || t0 > kScanCarryTiles || t1 > kScanCarryTiles) {
+        exclusive_scan_u32(st, in0, out0, n0, temp);
+        exclusive_scan_u32(st, in1, out1, n1, temp + scan_temp_words(n0));
+        return;
+    }
+    ScanJobs J = one_job(in0, out0, n0, temp);
+    J.in[1] = in1;
+    J.out[1] = out1;
+    J.n[1] = n1;
+    J.partial[1] = temp + scan_temp_words(n0);
+    J.ntiles[1] = t1;
+    note_launch();
+    k_scan_reduce<<<(unsigned)(t0 + t1), kBlock, 0, st>>>(J);
+    note_launch();
+    k_scan_down_carry<<<(unsigned)(t0 + t1), kBlock, 0, st>>>(J);
 }
 
 // ---- single-pass scan (decoupled look-back) ---------------------------------

@@ -144,6 +144,11 @@ void launch_interleave_w(cudaStream_t st, uint64_t n, int w, double* dst, const 
 uint64_t scan_temp_words(uint64_t n);
 void exclusive_scan_u32(cudaStream_t st, const uint32_t* in, uint32_t* out, uint64_t n,
                         uint32_t* temp);
+// Two independent scans in the same two launches (when each fits the
+// two-launch form; else one after the other).  temp holds
+// scan_temp_words(n0) + scan_temp_words(n1) u32.
+void exclusive_scan_u32_pair(cudaStream_t st, const uint32_t* in0, uint32_t* out0, uint64_t n0,
+                             const uint32_t* in1, uint32_t* out1, uint64_t n1, uint32_t* temp);
 // The same scan in one launch (decoupled look-back, k_scan.cu).  temp holds
 // scan1p_words(n) u32, 8-byte aligned, and must be zero when first used (its
 // words are left ready for the next call).  err: optional flag word that gets

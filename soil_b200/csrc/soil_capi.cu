@@ -335,9 +335,27 @@ int scan_1p(soil_sys* s, const uint32_t* in, uint32_t* out, uint64_t n) {
     return SOIL_OK;
 }
 
+// Two independent scans; above the single-pass size both go in the same two
+// launches.
+int scan_pair(soil_sys* s, const uint32_t* in0, uint32_t* out0, uint64_t n0, const uint32_t* in1,
+              uint32_t* out1, uint64_t n1) {
+    const uint64_t lim = scan1p_max();
+    if (n0 > lim && n1 > lim) {
+        TRY(ensure(s, s->scan_tmp, scan_temp_words(n0 + 2) + scan_temp_words(n1 + 2)));
+        exclusive_scan_u32_pair(s->st, in0, out0, n0, in1, out1, n1, s->scan_tmp.p);
+        return SOIL_OK;
+    }
+    TRY(scan_1p(s, in0, out0, n0));
+    return scan_1p(s, in1, out1, n1);
+}
+
+// 0: range bounds loaded as the scan reaches them; 1 (default): preloaded
+// into registers; 2: preloaded into shared memory (the pair count only)
 int pairs_pre_ranges() {
     const char* env = std::getenv("SOIL_PAIRS_PRE");
-    return env && std::atoi(env) == 0 ? 0 : 1;
+    if (!env) return 1;
+    const int v = std::atoi(env);
+    return v < 0 || v > 2 ? 1 : v;
 }
 
 std::vector<int32_t> stencil_runs(const std::vector<int32_t>& sten, bool newton) {
@@ -1481,6 +1499,7 @@ int phase_neighbor(soil_sys* s) {
     p.in_list = nullptr;
     p.pre_ranges = pairs_pre_ranges();
     uint64_t in_zero = 0;  // in_count[0, in_zero) is zero already
+    const uint64_t in_range = total;  // the counts pass 1 may write and the scan reads
     if (with_in) {
         TRY(ensure(s, s->in_count, total + 1, 0, s->acap + 1));
         TRY(ensure(s, s->in_start, total + 2, 0, s->acap + 2));
@@ -1496,8 +1515,8 @@ int phase_neighbor(soil_sys* s) {
         launch_pair_count_staged(s->st, p, sg, s->rowcount.p, s->row_slots.p, s->dflags);
     else
         launch_pair_count(s->st, p, s->rowcount.p, s->row_slots.p, s->dflags);
-    TRY(scan_1p(s, s->rowcount.p, s->offsets.p, nl));
-    if (with_in) TRY(scan_1p(s, s->in_count.p, s->in_start.p, total));
+    if (with_in) TRY(scan_pair(s, s->rowcount.p, s->offsets.p, nl, s->in_count.p, s->in_start.p, total));
+    else TRY(scan_1p(s, s->rowcount.p, s->offsets.p, nl));
     if (!s->ev_counts) CK(cudaEventCreateWithFlags(&s->ev_counts, cudaEventDisableTiming));
     // Pass 2 goes in before the host reads the pair total, into the arrays it
     // has: the stream stays busy while the host waits for the counts, which
@@ -1569,7 +1588,7 @@ int phase_neighbor(soil_sys* s) {
     if (with_in) {
         s->in_lists_valid = true;
         s->split_valid = true;
-        s->in_zero = in_zero > total ? in_zero : total;  // pass 2 took every count back
+        s->in_zero = in_zero > in_range ? in_zero : in_range;  // pass 2 took every count back
     }
     // the grouped sequences are built when a consumer kernel first needs them
     return SOIL_OK;
