@@ -337,84 +337,6 @@ __device__ uint32_t row_scan_pre(const PairParams& p, const Filter<UNIFORM, FP32
     }
 }
 
-// row_scan_pre with the stencil runs' slot bounds in shared memory instead of
-// registers: srng is the thread's column of a [2 * kPreRanges][kBlock] array
-// (lo of stored range k at srng[2k * kBlock], hi at srng[(2k + 1) * kBlock]).
-// Only non-empty runs are stored, so moving to the next range is two shared
-// loads and never loops.  Same candidates in the same order, same counts.
-template <bool UNIFORM, bool FP32, bool FILL>
-__device__ uint32_t row_scan_sm(const PairParams& p, const Filter<UNIFORM, FP32>& test,
-                                uint64_t i, uint32_t* out, uint32_t cap, uint32_t* rechk,
-                                uint32_t* cand, DevFlags* flags, uint32_t* in_count,
-                                uint32_t* srng) {
-    const uint32_t my_cell = p.atom_cell[i];
-    const uint32_t mi = p.atom_sorted_idx[i];
-    const double4 pi = ld_rec(p.sp + mi);
-    const float4 pif = FP32 ? p.spf[mi] : make_float4(0.f, 0.f, 0.f, 0.f);
-    int first = 0;  // stencil runs merged into the own range
-    uint32_t m = 0, e = 0;
-    if (p.has_self) {
-        uint64_t ce = (uint64_t)my_cell + 1;
-        if (p.newton && p.nstencil > 0 && p.stencil[0] == 1 &&
-            ce + (uint64_t)p.stencil[1] <= p.ncells) {
-            ce += (uint64_t)p.stencil[1];
-            first = 1;
-        }
-        m = p.newton ? mi + 1 : p.bin_start[my_cell];
-        e = p.bin_start[ce];
-    }
-    uint32_t total = e - m;
-    int nr = 0;  // non-empty runs stored
-    for (int s = first; s < p.nstencil; ++s) {
-        const int64_t c0 = (int64_t)my_cell + p.stencil[2 * s];
-        const int64_t c1 = c0 + p.stencil[2 * s + 1];
-        if (c0 < 0 || c1 > (int64_t)p.ncells) {  // the grid's ghost layers make this unreachable
-            if (flags) atomicOr(&flags->error, 1u);
-            continue;
-        }
-        const uint32_t lo = p.bin_start[c0], hi = p.bin_start[c1];
-        if (hi > lo) {
-            srng[(2 * nr) * kBlock] = lo;
-            srng[(2 * nr + 1) * kBlock] = hi;
-            ++nr;
-            total += hi - lo;
-        }
-    }
-    const bool skip_i = p.has_self && !p.newton;  // i is in its own range
-    *cand += total - (skip_i ? 1u : 0u);
-    int k = 0;
-    bool own = true;
-    uint32_t cnt = 0;
-    for (;;) {
-        if (m >= e) {  // the next stored run (never empty)
-            if (k >= nr) return cnt;
-            m = srng[(2 * k) * kBlock];
-            e = srng[(2 * k + 1) * kBlock];
-            ++k;
-            own = false;
-        }
-        if (own && skip_i && m == mi) {
-            ++m;
-            continue;
-        }
-        uint32_t a;
-        bool ok;
-        if (UNIFORM) {  // the atom comes with the record
-            a = test.accept(p, pi, pif, m, rechk);
-            ok = a != test.kNoAtom;
-        } else {
-            a = p.sorted_atoms[m];
-            ok = test(p, pi, pif, m, rechk);
-        }
-        if (ok) {
-            if (in_count) atomicAdd(&in_count[a], 1u);
-            if (FILL && cnt < cap) out[cnt] = a;
-            ++cnt;
-        }
-        ++m;
-    }
-}
-
 // Row of local atom i, sequentially in reference order: the own cell's
 // candidates (the tail after i's slot with newton, else the whole cell
 // without i), then every stencil cell in stencil order, each in sorted order.

@@ -35,15 +35,10 @@ __global__ void __launch_bounds__(kBlock) k_pairs_rows(PairParams p, uint32_t* r
     const Filter<UNIFORM, FP32> test(p);
     const uint32_t K = (uint32_t)p.row_slots;
     uint32_t n_rechk = 0, n_cand32 = 0;
-    extern __shared__ uint32_t s_rng[];  // row_scan_sm's run bounds (launched with them)
-    const bool sm = p.pre_ranges == 2 && p.nstencil < kPreRanges;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < p.nlocal;
          i += (uint64_t)gridDim.x * blockDim.x)
-        rowcount[i] = sm ? row_scan_sm<UNIFORM, FP32, true>(p, test, i, slots + i * K, K,
-                                                            &n_rechk, &n_cand32, flags,
-                                                            p.in_count, s_rng + threadIdx.x)
-                         : row_scan<UNIFORM, FP32, true>(p, test, i, slots + i * K, K, &n_rechk,
-                                                         &n_cand32, flags, p.in_count);
+        rowcount[i] = row_scan<UNIFORM, FP32, true>(p, test, i, slots + i * K, K, &n_rechk,
+                                                    &n_cand32, flags, p.in_count);
     // the block's totals, then one atomic per counter and block (the FP64
     // filter rechecks nothing)
     __shared__ unsigned long long s_cand, s_rechk;
@@ -129,12 +124,8 @@ static void launch_pairs_t(cudaStream_t st, const PairParams& p, uint32_t* rowco
                            uint32_t* slots, const uint32_t* offsets, uint32_t* indices,
                            DevFlags* flags, const FillGuard* g) {
     note_launch();
-    // the shared run bounds of row_scan_sm only when it runs: a kernel without
-    // shared memory keeps the whole L1 for the candidate records
-    const size_t smem =
-        p.pre_ranges == 2 && p.nstencil < kPreRanges ? 2 * kPreRanges * kBlock * 4 : 0;
     if (!g)
-        k_pairs_rows<UNIFORM, FP32><<<grid_wave<k_pairs_rows<UNIFORM, FP32>>(p.nlocal), kBlock, smem, st>>>(p, rowcount, slots,
+        k_pairs_rows<UNIFORM, FP32><<<grid_wave<k_pairs_rows<UNIFORM, FP32>>(p.nlocal), kBlock, 0, st>>>(p, rowcount, slots,
                                                                             flags);
     else
         k_pairs_fill<UNIFORM, FP32><<<grid_wave<k_pairs_fill<UNIFORM, FP32>>(p.nlocal), kBlock, 0, st>>>(p, rowcount, slots,

@@ -349,13 +349,9 @@ int scan_pair(soil_sys* s, const uint32_t* in0, uint32_t* out0, uint64_t n0, con
     return scan_1p(s, in1, out1, n1);
 }
 
-// 0: range bounds loaded as the scan reaches them; 1 (default): preloaded
-// into registers; 2: preloaded into shared memory (the pair count only)
 int pairs_pre_ranges() {
     const char* env = std::getenv("SOIL_PAIRS_PRE");
-    if (!env) return 1;
-    const int v = std::atoi(env);
-    return v < 0 || v > 2 ? 1 : v;
+    return env && std::atoi(env) == 0 ? 0 : 1;
 }
 
 std::vector<int32_t> stencil_runs(const std::vector<int32_t>& sten, bool newton) {

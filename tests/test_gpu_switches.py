@@ -1,10 +1,9 @@
 """The rebuild path's speed switches change no result: the pair scan with
-range bounds loaded as it goes (SOIL_PAIRS_PRE=0) or held in shared memory
-(SOIL_PAIRS_PRE=2), the shared-memory staged pair count
-(SOIL_PAIRS_STAGED=1), and every scan taken by the single-pass kernel or by
-the two- and three-kernel ones (SOIL_SCAN1P_MAX), each stepped through
-rebuilds on a polydisperse and a uniform-cutoff system and compared bit for
-bit with the CPU oracle (state and lists, order included)."""
+range bounds loaded as it goes (SOIL_PAIRS_PRE=0), the shared-memory staged
+pair count (SOIL_PAIRS_STAGED=1), and every scan taken by the single-pass
+kernel or by the two- and three-kernel ones (SOIL_SCAN1P_MAX), each stepped
+through rebuilds on a polydisperse and a uniform-cutoff system and compared
+bit for bit with the CPU oracle (state and lists, order included)."""
 import os
 
 import pytest
@@ -17,7 +16,6 @@ pytestmark = pytest.mark.gpu
 
 SETTINGS = {
     "pairs-pre-off": {"SOIL_PAIRS_PRE": "0"},
-    "pairs-pre-shared": {"SOIL_PAIRS_PRE": "2"},
     "pairs-staged": {"SOIL_PAIRS_STAGED": "1"},
     "scan-single-pass-always": {"SOIL_SCAN1P_MAX": "100000000"},
     "scan-three-kernel-always": {"SOIL_SCAN1P_MAX": "0"},
