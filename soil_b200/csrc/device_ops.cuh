@@ -424,6 +424,25 @@ __device__ __forceinline__ double4 ld_pk(const double* pk, uint64_t i) {
     return v;
 }
 
+// initial_integration (soil_verlet/src/lib.rs:131-162) on registers: v += h*F
+// (twice when fuse_final: the previous step's final_integration with the same
+// forces first), then x += v*dt; h = dt/2 * inv_mass.
+__device__ __forceinline__ void initial_regs(double h, double dt, bool fuse_final, double fx,
+                                             double fy, double fz, double& vx, double& vy,
+                                             double& vz, double& x, double& y, double& z) {
+    if (fuse_final) {
+        vx = vx + h * fx;
+        vy = vy + h * fy;
+        vz = vz + h * fz;
+    }
+    vx = vx + h * fx;
+    vy = vy + h * fy;
+    vz = vz + h * fz;
+    x = x + vx * dt;
+    y = y + vy * dt;
+    z = z + vz * dt;
+}
+
 // initial_integration (soil_verlet/src/lib.rs:131-162) of atom i, optionally
 // preceded by final_integration of the previous step with the same forces;
 // returns the new position.
@@ -436,22 +455,16 @@ __device__ __forceinline__ void initial_atom(const AtomCols& c, uint64_t i, doub
     // another memory round trip
     const double h = 0.5 * dt * c.inv_mass[i];
     const double fx = c.fx[i], fy = c.fy[i], fz = c.fz[i];
-    double vx = c.vx[i], vy = c.vy[i], vz = c.vz[i];
-    const double x0 = c.x[i], y0 = c.y[i], z0 = c.z[i];
-    if (fuse_final) {  // final_integration of the previous step, same forces
-        vx = vx + h * fx;
-        vy = vy + h * fy;
-        vz = vz + h * fz;
-    }
-    v0 = vx + h * fx;
-    v1 = vy + h * fy;
-    v2 = vz + h * fz;
+    v0 = c.vx[i];
+    v1 = c.vy[i];
+    v2 = c.vz[i];
+    x = c.x[i];
+    y = c.y[i];
+    z = c.z[i];
+    initial_regs(h, dt, fuse_final, fx, fy, fz, v0, v1, v2, x, y, z);
     c.vx[i] = v0;
     c.vy[i] = v1;
     c.vz[i] = v2;
-    x = x0 + v0 * dt;
-    y = y0 + v1 * dt;
-    z = z0 + v2 * dt;
     c.x[i] = x;
     c.y[i] = y;
     c.z[i] = z;
@@ -478,46 +491,49 @@ __device__ __forceinline__ void final_atom(const AtomCols& c, uint64_t i, double
     c.vz[i] = c.vz[i] + h * c.fz[i];
 }
 
-// pbc fully periodic fast path (domain.rs:626-636) / pbc_triclinic (domain.rs:674-729);
-// the new position also into px, py, pz
+// pbc fully periodic fast path (domain.rs:626-636) / pbc_triclinic
+// (domain.rs:674-729) of a position held in registers: wrapped in place, the
+// image counts updated, and remap(s) called with the y crossing s (+1 / -1)
+// for the Lees–Edwards velocity remap v -= s * bvel.
+template <class Remap>
+__device__ __forceinline__ void pbc_core(const Geom& g, double& x, double& y, double& z,
+                                         int32_t& i0, int32_t& i1, int32_t& i2, Remap remap) {
+    if (!g.triclinic) {
+        x = wrap1(x, g.lo[0], g.size[0], i0);
+        y = wrap1(y, g.lo[1], g.size[1], i1);
+        z = wrap1(z, g.lo[2], g.size[2], i2);
+        return;
+    }
+    double l0, l1, l2;
+    x2lamda(g, x, y, z, l0, l1, l2);
+    int32_t d0 = 0, d1 = 0, d2 = 0;
+    if (l0 < 0.0) { l0 += 1.0; d0 = -1; } else if (l0 >= 1.0) { l0 -= 1.0; d0 = 1; }
+    if (l1 < 0.0) { l1 += 1.0; d1 = -1; } else if (l1 >= 1.0) { l1 -= 1.0; d1 = 1; }
+    if (l2 < 0.0) { l2 += 1.0; d2 = -1; } else if (l2 >= 1.0) { l2 -= 1.0; d2 = 1; }
+    lamda2x(g, l0, l1, l2, x, y, z);
+    i0 += d0;
+    i1 += d1;
+    i2 += d2;
+    if (d1 != 0) remap((double)d1);
+}
+
+// pbc of local i in memory; the new position also into px, py, pz
 __device__ __forceinline__ void pbc_atom(const AtomCols& c, uint64_t i, const Geom& g, double bv0,
                                          double bv1, double bv2, double& px, double& py,
                                          double& pz) {
     const uint64_t cap = c.cap;
     int32_t i0 = c.img[i], i1 = c.img[cap + i], i2 = c.img[2 * cap + i];
-    const double x0 = c.x[i], y0 = c.y[i], z0 = c.z[i];
-    if (!g.triclinic) {
-        px = wrap1(x0, g.lo[0], g.size[0], i0);
-        py = wrap1(y0, g.lo[1], g.size[1], i1);
-        pz = wrap1(z0, g.lo[2], g.size[2], i2);
-        c.x[i] = px;
-        c.y[i] = py;
-        c.z[i] = pz;
-    } else {
-        double l0, l1, l2;
-        x2lamda(g, x0, y0, z0, l0, l1, l2);
-        int32_t d0 = 0, d1 = 0, d2 = 0;
-        if (l0 < 0.0) { l0 += 1.0; d0 = -1; } else if (l0 >= 1.0) { l0 -= 1.0; d0 = 1; }
-        if (l1 < 0.0) { l1 += 1.0; d1 = -1; } else if (l1 >= 1.0) { l1 -= 1.0; d1 = 1; }
-        if (l2 < 0.0) { l2 += 1.0; d2 = -1; } else if (l2 >= 1.0) { l2 -= 1.0; d2 = 1; }
-        double rx, ry, rz;
-        lamda2x(g, l0, l1, l2, rx, ry, rz);
-        px = rx;
-        py = ry;
-        pz = rz;
-        c.x[i] = rx;
-        c.y[i] = ry;
-        c.z[i] = rz;
-        i0 += d0;
-        i1 += d1;
-        i2 += d2;
-        if (d1 != 0) {  // Lees–Edwards velocity remap
-            const double s = (double)d1;
-            c.vx[i] = c.vx[i] - s * bv0;
-            c.vy[i] = c.vy[i] - s * bv1;
-            c.vz[i] = c.vz[i] - s * bv2;
-        }
-    }
+    px = c.x[i];
+    py = c.y[i];
+    pz = c.z[i];
+    pbc_core(g, px, py, pz, i0, i1, i2, [&](double s) {
+        c.vx[i] = c.vx[i] - s * bv0;
+        c.vy[i] = c.vy[i] - s * bv1;
+        c.vz[i] = c.vz[i] - s * bv2;
+    });
+    c.x[i] = px;
+    c.y[i] = py;
+    c.z[i] = pz;
     c.img[i] = i0;
     c.img[cap + i] = i1;
     c.img[2 * cap + i] = i2;

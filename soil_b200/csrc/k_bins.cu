@@ -55,6 +55,80 @@ __global__ void __launch_bounds__(kBlock) k_pbc_cells(uint64_t n, AtomCols c, Ge
     }
 }
 
+// The integration pass of a step that rebuilds for certain, in a fully
+// periodic box: initial_integration (with the previous step's final half-kick
+// when FUSE_FINAL) and pbc of the new position in registers, every column
+// stored once; with CELLS the wrapped position binned and counted for the
+// sort.  Same arithmetic as initial_atom followed by pbc_atom.
+template <bool FUSE_FINAL, bool CELLS>
+__global__ void __launch_bounds__(kBlock) k_initial_pbc(uint64_t n, AtomCols c, double dt,
+                                                        int zero_force, Geom g, double bv0,
+                                                        double bv1, double bv2, Grid gr,
+                                                        uint32_t* cell_out, uint32_t* counts) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t cap = c.cap;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
+        const uint64_t i = i0 + threadIdx.x;
+        const bool valid = i < n;
+        uint32_t cell = 0;
+        if (valid) {
+            const double h = 0.5 * dt * c.inv_mass[i];
+            const double fx = c.fx[i], fy = c.fy[i], fz = c.fz[i];
+            double vx = c.vx[i], vy = c.vy[i], vz = c.vz[i];
+            double x = c.x[i], y = c.y[i], z = c.z[i];
+            int32_t m0 = c.img[i], m1 = c.img[cap + i], m2 = c.img[2 * cap + i];
+            initial_regs(h, dt, FUSE_FINAL, fx, fy, fz, vx, vy, vz, x, y, z);
+            pbc_core(g, x, y, z, m0, m1, m2, [&](double sg) {
+                vx = vx - sg * bv0;
+                vy = vy - sg * bv1;
+                vz = vz - sg * bv2;
+            });
+            c.vx[i] = vx;
+            c.vy[i] = vy;
+            c.vz[i] = vz;
+            c.x[i] = x;
+            c.y[i] = y;
+            c.z[i] = z;
+            c.img[i] = m0;
+            c.img[cap + i] = m1;
+            c.img[2 * cap + i] = m2;
+            if (zero_force) {
+                c.fx[i] = 0.0;
+                c.fy[i] = 0.0;
+                c.fz[i] = 0.0;
+            }
+            if (CELLS) {
+                cell = cell_of(gr, x, y, z);
+                cell_out[i] = cell;
+            }
+        }
+        if (CELLS) aggregated_count(counts, cell, valid);
+    }
+}
+
+template <bool FUSE_FINAL, bool CELLS>
+static void initial_pbc_t(cudaStream_t st, uint64_t n, const AtomCols& c, double dt,
+                          bool zero_force, const Geom& g, const double bvel[3], const Grid& gr,
+                          uint32_t* cell_out, uint32_t* counts) {
+    k_initial_pbc<FUSE_FINAL, CELLS><<<grid_wave<k_initial_pbc<FUSE_FINAL, CELLS>>(n), kBlock, 0,
+                                       st>>>(n, c, dt, zero_force ? 1 : 0, g, bvel[0], bvel[1],
+                                             bvel[2], gr, cell_out, counts);
+}
+
+void launch_initial_pbc(cudaStream_t st, uint64_t n, const AtomCols& c, double dt,
+                        bool fuse_final, bool zero_force, const Geom& g, const double bvel[3],
+                        const Grid& gr, uint32_t* cell_out, uint32_t* counts) {
+    if (n == 0) return;
+    note_launch();
+    if (fuse_final) {
+        if (cell_out) initial_pbc_t<true, true>(st, n, c, dt, zero_force, g, bvel, gr, cell_out, counts);
+        else initial_pbc_t<true, false>(st, n, c, dt, zero_force, g, bvel, gr, cell_out, counts);
+    } else {
+        if (cell_out) initial_pbc_t<false, true>(st, n, c, dt, zero_force, g, bvel, gr, cell_out, counts);
+        else initial_pbc_t<false, false>(st, n, c, dt, zero_force, g, bvel, gr, cell_out, counts);
+    }
+}
+
 void launch_pbc_cells(cudaStream_t st, uint64_t n, const AtomCols& c, const Geom& g,
                       const double bvel[3], const Grid& gr, uint32_t* cell_out, uint32_t* counts) {
     if (n == 0) return;

@@ -163,6 +163,13 @@ void exclusive_scan_1p(cudaStream_t st, const uint32_t* in, uint32_t* out, uint6
 // pbc of locals [0, n) then cell_out[i] = their cell, counted (pbc + the sort's binning)
 void launch_pbc_cells(cudaStream_t st, uint64_t n, const AtomCols& c, const Geom& g,
                       const double bvel[3], const Grid& gr, uint32_t* cell_out, uint32_t* counts);
+// initial_integration (after the previous step's final one when fuse_final)
+// and pbc of the locals in one pass, for a step that rebuilds for certain in a
+// fully periodic box; with cell_out, also the sort's cells and counts (as
+// launch_pbc_cells)
+void launch_initial_pbc(cudaStream_t st, uint64_t n, const AtomCols& c, double dt,
+                        bool fuse_final, bool zero_force, const Geom& g, const double bvel[3],
+                        const Grid& gr, uint32_t* cell_out, uint32_t* counts);
 // n_dev (optional, here and below): the count is min(n, *n_dev), read on the
 // device (n an upper bound), for launches queued before the host knows it.
 void launch_cells(cudaStream_t st, uint64_t first, uint64_t n, const AtomCols& c, const Grid& gr,

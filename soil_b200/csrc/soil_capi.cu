@@ -1713,6 +1713,9 @@ struct StepPlan {
     bool check;       // the displacement check ran in the integration pass
     bool fwd_fused;   // forward comm ran in the integration pass
     int nz;           // #[zero] planes
+    // pbc (and, when the sort is due, its binning) ran in the integration
+    // pass of a step that rebuilds for certain; sort_plan's answers
+    bool pbc_done = false, sort_due = false, periodic_sort = false;
 };
 
 StepPlan plan_step(const soil_sys* s) {
@@ -1747,8 +1750,29 @@ int step_integrate(soil_sys* s, StepPlan* out) {
     }
     timer_begin(s, T_INTEGRATE);
     TRY(phase_deform(s));
-    const StepPlan p = plan_step(s);
+    StepPlan p = plan_step(s);
     if (p.check) CK(cudaMemsetAsync(&s->dflags->rebuild, 0, 4, s->st));
+    // A step that rebuilds whatever its displacement check would say (lists
+    // due, a box that moved), in a fully periodic box: pbc, and the sort's
+    // binning when it falls due, ride on the integration pass.  decide_rebuild
+    // has nothing left to decide, and the sort's plan does not depend on the
+    // positions, so both are made first.
+    if (!p.check && !p.fwd_fused && !profile_now && pbc_mask(s) == 7 && s->nlocal > 0 &&
+        s->total_cells > 0 && (s->state == FULL_REBUILD || needs_rebuild_with(s, false))) {
+        s->state = FULL_REBUILD;
+        TRY(sort_plan(s, &p.sort_due, &p.periodic_sort));
+        s->pk_valid = false;
+        if (p.sort_due) TRY(counts_zero(s, s->total_cells));
+        launch_initial_pbc(s->st, s->nlocal, s->A, s->dt, s->pending_final, p.fused_zero,
+                           geom_of(s), s->bvel, grid_of(s), p.sort_due ? s->sort_cell.p : nullptr,
+                           s->cell_counts.p);
+        s->pending_final = false;
+        p.pbc_done = true;
+        TRY(check_launch(s));
+        timer_end(s, T_INTEGRATE);
+        *out = p;
+        return SOIL_OK;
+    }
     // Forward comm rides on the integration pass when this step keeps its
     // lists unless the displacement check trips (ghost images written from
     // their roots' new positions; a step that rebuilds replaces them).
@@ -1794,10 +1818,12 @@ int step_rest(soil_sys* s, const StepPlan& p, bool last) {
     // A rebuild step of a fully periodic box wraps its locals and bins them
     // for the sort in one pass: the sort's plan (grid, whether it runs) does
     // not depend on the wrap, so it is made first.
-    const bool pbc_cells =
-        s->state == FULL_REBUILD && pbc_mask(s) == 7 && s->nlocal > 0 && s->total_cells > 0;
-    bool sort_due = false, periodic_sort = false;
-    if (pbc_cells) {
+    const bool pbc_cells = p.pbc_done || (s->state == FULL_REBUILD && pbc_mask(s) == 7 &&
+                                          s->nlocal > 0 && s->total_cells > 0);
+    bool sort_due = p.sort_due, periodic_sort = p.periodic_sort;
+    if (p.pbc_done) {
+        // wrapped (and binned) in the integration pass
+    } else if (pbc_cells) {
         TRY(sort_plan(s, &sort_due, &periodic_sort));
         s->pk_valid = false;
         if (sort_due) {
