@@ -58,27 +58,40 @@ struct ScanJobs {
     uint64_t ntiles[2];
 };
 
-__device__ __forceinline__ int scan_job(const ScanJobs& J, uint64_t* tile) {
-    if (blockIdx.x < J.ntiles[0]) {
-        *tile = blockIdx.x;
-        return 0;
-    }
-    *tile = blockIdx.x - J.ntiles[0];
-    return 1;
+// This block's scan: its fields picked by selects (a parameter array indexed
+// by a run-time value would be copied to local memory).
+struct ScanJob {
+    const uint32_t* in;
+    uint32_t* out;
+    uint64_t n;
+    uint32_t* partial;
+    uint64_t ntiles;
+    uint64_t tile;  // this block's tile of it
+};
+
+__device__ __forceinline__ ScanJob scan_job(const ScanJobs& J) {
+    const bool second = blockIdx.x >= J.ntiles[0];
+    ScanJob s;
+    s.in = second ? J.in[1] : J.in[0];
+    s.out = second ? J.out[1] : J.out[0];
+    s.n = second ? J.n[1] : J.n[0];
+    s.partial = second ? J.partial[1] : J.partial[0];
+    s.ntiles = second ? J.ntiles[1] : J.ntiles[0];
+    s.tile = second ? blockIdx.x - J.ntiles[0] : blockIdx.x;
+    return s;
 }
 
 __global__ void __launch_bounds__(kBlock) k_scan_reduce(ScanJobs J) {
     __shared__ uint32_t tot;
-    uint64_t t;
-    const int j = scan_job(J, &t);
-    const uint64_t base = t * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+    const ScanJob q = scan_job(J);
+    const uint64_t base = q.tile * kScanTile + (uint64_t)threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
-    load8(J.in[j], base, J.n[j], v);
+    load8(q.in, base, q.n, v);
     uint32_t s = 0;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) s += v[k];
     block_exclusive_scan(s, &tot);
-    if (threadIdx.x == 0) J.partial[j][t] = tot;
+    if (threadIdx.x == 0) q.partial[q.tile] = tot;
 }
 
 // One CTA: exclusive scan of the tile sums in place, grand total to partial[ntiles].
@@ -127,13 +140,12 @@ constexpr uint64_t kScanCarryTiles = 4096;
 
 __global__ void __launch_bounds__(kBlock) k_scan_down_carry(ScanJobs J) {
     __shared__ uint32_t tot, s_carry;
-    uint64_t t;
-    const int j = scan_job(J, &t);
-    const uint64_t n = J.n[j];
-    const uint32_t* partial = J.partial[j];
+    const ScanJob q = scan_job(J);
+    const uint64_t t = q.tile, n = q.n;
+    const uint32_t* partial = q.partial;
     const uint64_t base = t * kScanTile + (uint64_t)threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
-    load8(J.in[j], base, n, v);
+    load8(q.in, base, n, v);
     uint32_t c = 0;  // this thread's share of the sums of tiles [0, t)
     for (uint64_t q = threadIdx.x; q < t; q += kBlock) c += partial[q];
     block_exclusive_scan(c, &tot);
@@ -144,8 +156,8 @@ __global__ void __launch_bounds__(kBlock) k_scan_down_carry(ScanJobs J) {
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) s += v[k];
     const uint32_t pre = block_exclusive_scan(s, &tot) + carry;
-    store8_scan(J.out[j], base, n, v, pre);
-    if (t + 1 == J.ntiles[j] && threadIdx.x == 0) J.out[j][n] = carry + tot;
+    store8_scan(q.out, base, n, v, pre);
+    if (t + 1 == q.ntiles && threadIdx.x == 0) q.out[n] = carry + tot;
 }
 
 uint64_t scan_temp_words(uint64_t n) { return (n + kScanTile - 1) / kScanTile + 2; }
