@@ -65,6 +65,7 @@ __global__ void __launch_bounds__(kBlock) k_initial_pbc(uint64_t n, AtomCols c, 
                                                         int zero_force, Geom g, double bv0,
                                                         double bv1, double bv2, Grid gr,
                                                         uint32_t* cell_out, uint32_t* counts) {
+    pdl_wait();  // launched with pdl_launch
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     const uint64_t cap = c.cap;
     for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
@@ -110,8 +111,7 @@ template <bool FUSE_FINAL, bool CELLS>
 static void initial_pbc_t(cudaStream_t st, uint64_t n, const AtomCols& c, double dt,
                           bool zero_force, const Geom& g, const double bvel[3], const Grid& gr,
                           uint32_t* cell_out, uint32_t* counts) {
-    k_initial_pbc<FUSE_FINAL, CELLS><<<grid_wave<k_initial_pbc<FUSE_FINAL, CELLS>>(n), kBlock, 0,
-                                       st>>>(n, c, dt, zero_force ? 1 : 0, g, bvel[0], bvel[1],
+    pdl_launch(k_initial_pbc<FUSE_FINAL, CELLS>, grid_wave<k_initial_pbc<FUSE_FINAL, CELLS>>(n), kBlock, 0, st, n, c, dt, zero_force ? 1 : 0, g, bvel[0], bvel[1],
                                              bvel[2], gr, cell_out, counts);
 }
 
@@ -192,6 +192,7 @@ __global__ void __launch_bounds__(kBlock) k_scatter_consume(uint64_t n, const ui
                                                             const uint32_t* start,
                                                             uint32_t* counts, uint32_t* out,
                                                             const uint32_t* n_dev) {
+    pdl_wait();  // launched with pdl_launch
     if (n_dev) {  // the count known only on the device (an upper bound in n)
         const uint64_t d = *n_dev;
         n = d < n ? d : n;
@@ -217,7 +218,7 @@ void launch_scatter_consume(cudaStream_t st, uint64_t n, const uint32_t* cell,
                             const uint32_t* n_dev) {
     if (n == 0) return;
     note_launch();
-    k_scatter_consume<<<grid_wave<k_scatter_consume>(n), kBlock, 0, st>>>(n, cell, start, counts,
+    pdl_launch(k_scatter_consume, grid_wave<k_scatter_consume>(n), kBlock, 0, st, n, cell, start, counts,
                                                                           out, n_dev);
 }
 
@@ -227,6 +228,7 @@ __global__ void __launch_bounds__(kBlock) k_cells_reuse(uint64_t nlocal, uint64_
                                                         Grid gr, const uint32_t* local_cell,
                                                         uint32_t* cell_out, uint32_t* counts,
                                                         const uint32_t* n_dev) {
+    pdl_wait();  // launched with pdl_launch
     if (n_dev) {  // the count known only on the device (an upper bound in n)
         const uint64_t d = *n_dev;
         n = d < n ? d : n;
@@ -249,7 +251,7 @@ void launch_cells_reuse(cudaStream_t st, uint64_t nlocal, uint64_t n, const Atom
                         uint32_t* counts, const uint32_t* n_dev) {
     if (n == 0) return;
     note_launch();
-    k_cells_reuse<<<grid_wave<k_cells_reuse>(n), kBlock, 0, st>>>(nlocal, n, c, gr, local_cell,
+    pdl_launch(k_cells_reuse, grid_wave<k_cells_reuse>(n), kBlock, 0, st, nlocal, n, c, gr, local_cell,
                                                                   cell_out, counts, n_dev);
 }
 
@@ -268,6 +270,7 @@ __global__ void __launch_bounds__(kBlock) k_place_bins(uint64_t nl, uint64_t n,
                                                        const uint32_t* sort_start,
                                                        uint32_t* counts, uint32_t* tmp,
                                                        uint32_t* out) {
+    pdl_wait();  // launched with pdl_launch
     if (n_dev) {
         const uint64_t d = *n_dev;
         n = d < n ? d : n;
@@ -290,6 +293,7 @@ __global__ void __launch_bounds__(kBlock) k_ghost_rank(uint64_t nl, uint64_t n,
                                                        const uint32_t* sort_start,
                                                        const uint32_t* tmp, uint32_t* out,
                                                        uint32_t* counts, uint64_t nc) {
+    pdl_wait();  // launched with pdl_launch
     if (n_dev) {
         const uint64_t d = *n_dev;
         n = d < n ? d : n;
@@ -313,11 +317,12 @@ bool launch_place_bins(cudaStream_t st, uint64_t nl, uint64_t n, uint64_t nc,
                        uint32_t* out) {
     if (n == 0) return false;
     note_launch();
-    k_place_bins<<<grid_wave<k_place_bins>(n), kBlock, 0, st>>>(nl, n, n_dev, cell, start,
+    pdl_launch(k_place_bins, grid_wave<k_place_bins>(n), kBlock, 0, st, nl, n, n_dev, cell, start,
                                                                  sort_start, counts, tmp, out);
     if (n == nl) return false;
     note_launch();
-    k_ghost_rank<<<grid_wave<k_ghost_rank>(n - nl > nc ? n - nl : nc), kBlock, 0, st>>>(
+    const uint64_t rank_items = n - nl > nc ? n - nl : nc;  // ghosts, or cells to clear
+    pdl_launch(k_ghost_rank, grid_wave<k_ghost_rank>(rank_items), kBlock, 0, st, 
         nl, n, n_dev, cell, start, sort_start, tmp, out, counts, nc);
     return true;
 }
@@ -325,6 +330,7 @@ bool launch_place_bins(cudaStream_t st, uint64_t nl, uint64_t n, uint64_t nc,
 // Restore the stable (ascending index) order inside every segment.
 __global__ void __launch_bounds__(kBlock) k_segsort(uint64_t nseg, const uint32_t* start,
                                                     uint32_t* items) {
+    pdl_wait();  // launched with pdl_launch
     for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < nseg;
          s += (uint64_t)gridDim.x * blockDim.x)
         insertion_sort(items, start[s], start[s + 1]);
@@ -333,7 +339,7 @@ __global__ void __launch_bounds__(kBlock) k_segsort(uint64_t nseg, const uint32_
 void launch_segsort(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint32_t* items) {
     if (nseg == 0) return;
     note_launch();
-    k_segsort<<<grid_wave<k_segsort>(nseg), kBlock, 0, st>>>(nseg, start, items);
+    pdl_launch(k_segsort, grid_wave<k_segsort>(nseg), kBlock, 0, st, nseg, start, items);
 }
 
 // The transposed lists' sort: segment a (atom a's in-list) ascending, and
@@ -341,6 +347,7 @@ void launch_segsort(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint3
 __global__ void __launch_bounds__(kBlock) k_segsort_split(uint64_t nseg, const uint32_t* start,
                                                           uint32_t* items, uint32_t* split,
                                                           FillGuard g) {
+    pdl_wait();  // launched with pdl_launch
     if (!guard_open(g)) return;
     for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < nseg;
          s += (uint64_t)gridDim.x * blockDim.x) {
@@ -352,7 +359,7 @@ void launch_segsort_split(cudaStream_t st, uint64_t nseg, const uint32_t* start,
                           uint32_t* split, const FillGuard* g) {
     if (nseg == 0) return;
     note_launch();
-    k_segsort_split<<<grid_wave<k_segsort_split>(nseg), kBlock, 0, st>>>(
+    pdl_launch(k_segsort_split, grid_wave<k_segsort_split>(nseg), kBlock, 0, st, 
         nseg, start, items, split, g ? *g : FillGuard{});
 }
 
@@ -381,6 +388,7 @@ __global__ void __launch_bounds__(kBlock) k_perm_gather(uint64_t n, const uint32
                                                         AtomCols s, AtomCols d, int forces,
                                                         const uint32_t* cell_in,
                                                         uint32_t* cell_out) {
+    pdl_wait();  // launched with pdl_launch
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n;
          k += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t p = perm[k];
@@ -394,7 +402,7 @@ void launch_perm_gather(cudaStream_t st, uint64_t n, const uint32_t* perm, const
                         uint32_t* cell_out) {
     if (n == 0) return;
     note_launch();
-    k_perm_gather<<<grid_wave<k_perm_gather>(n), kBlock, 0, st>>>(n, perm, src, dst, forces ? 1 : 0,
+    pdl_launch(k_perm_gather, grid_wave<k_perm_gather>(n), kBlock, 0, st, n, perm, src, dst, forces ? 1 : 0,
                                                                   cell_in, cell_out);
 }
 
@@ -437,6 +445,7 @@ __global__ void __launch_bounds__(kBlock) k_sorted_views(uint64_t n, const uint3
                                                          double o2, BuildPos bp,
                                                          const uint32_t* n_dev, int atom_in_w,
                                                          DevFlags* clear) {
+    pdl_wait();  // launched with pdl_launch
     if (clear && blockIdx.x == 0 && threadIdx.x == 0) {  // the pair build's counters
         clear->candidates = 0;
         clear->rechecked = 0;
@@ -457,7 +466,7 @@ void launch_sorted_views(cudaStream_t st, uint64_t n, const uint32_t* sorted, co
                          bool atom_in_w, DevFlags* clear) {
     if (n == 0) return;
     note_launch();
-    k_sorted_views<<<grid_wave<k_sorted_views>(n), kBlock, 0, st>>>(
+    pdl_launch(k_sorted_views, grid_wave<k_sorted_views>(n), kBlock, 0, st, 
         n, sorted, c, atom_sorted_idx, sp, spf, origin[0], origin[1], origin[2], bp, n_dev,
         atom_in_w ? 1 : 0, clear);
 }

@@ -112,6 +112,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_force_walk(ForceArgs p) {
 
 template <bool FOLD, bool PK>
 __global__ void __launch_bounds__(kBlock, 4) k_force_csr(ForceCsr q, AtomCols c, PlaneList rev) {
+    pdl_wait();  // launched with pdl_launch
     // grid-stride over whole blocks of kBlock roots, so a block's order
     // permutes its own roots
     for (uint64_t b = (uint64_t)blockIdx.x * kBlock; b < q.nlocal; b += (uint64_t)gridDim.x * kBlock) {
@@ -174,11 +175,11 @@ void launch_force_csr(cudaStream_t st, const ForceCsr& q, const AtomCols& c, con
     const unsigned need = (unsigned)((q.nlocal + kBlock - 1) / kBlock);
     const unsigned grid = need < full ? need : full;
     if (q.pk) {
-        if (fold) k_force_csr<true, true><<<grid, kBlock, 0, st>>>(q, c, rev);
-        else k_force_csr<false, true><<<grid, kBlock, 0, st>>>(q, c, rev);
+        if (fold) pdl_launch(k_force_csr<true, true>, grid, kBlock, 0, st, q, c, rev);
+        else pdl_launch(k_force_csr<false, true>, grid, kBlock, 0, st, q, c, rev);
     } else {
-        if (fold) k_force_csr<true, false><<<grid, kBlock, 0, st>>>(q, c, rev);
-        else k_force_csr<false, false><<<grid, kBlock, 0, st>>>(q, c, rev);
+        if (fold) pdl_launch(k_force_csr<true, false>, grid, kBlock, 0, st, q, c, rev);
+        else pdl_launch(k_force_csr<false, false>, grid, kBlock, 0, st, q, c, rev);
     }
 }
 

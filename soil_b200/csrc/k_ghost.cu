@@ -143,6 +143,7 @@ BorderPass border_pass(const BorderDim bds[3]) {
 __global__ void __launch_bounds__(kBlock) k_border_faces(uint64_t nlocal, AtomCols c, BorderPass bp,
                                                          BorderCats cats, uint8_t* face,
                                                          uint32_t* counts, uint64_t nw) {
+    pdl_wait();  // launched with pdl_launch
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x / 32);
     for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32; w < nw; w += nwarps)
@@ -155,6 +156,7 @@ __global__ void __launch_bounds__(kBlock) k_border_faces(uint64_t nlocal, AtomCo
 __global__ void __launch_bounds__(kBlock) k_border_cat_scan(const uint32_t* counts, uint32_t* offs,
                                                             uint64_t nw, uint32_t* ctot,
                                                             uint64_t nchunks) {
+    pdl_wait();  // launched with pdl_launch
     const uint64_t k = blockIdx.x / nchunks, ch = blockIdx.x % nchunks;
     const uint64_t w0 = ch * kScanChunk;
     const uint64_t n = nw - w0 < kScanChunk ? nw - w0 : kScanChunk;
@@ -166,6 +168,7 @@ __global__ void __launch_bounds__(kBlock) k_border_cat_scan(const uint32_t* coun
 // clears the capacity word bs[10] that pass 3 may set.
 __global__ void __launch_bounds__(kBlock) k_border_chunk_prefix(uint32_t* ctot, uint64_t nchunks,
                                                                 uint32_t* bs, uint32_t* host_bs) {
+    pdl_wait();  // launched with pdl_launch
     if (threadIdx.x == 0) {
         bs[10] = 0u;
         if (host_bs) host_bs[10] = 0u;
@@ -189,6 +192,7 @@ __global__ void __launch_bounds__(kBlock) k_border_images(
     const uint32_t* offs, const uint32_t* cpre, uint64_t nchunks, uint64_t nw, uint32_t* bs,
     uint32_t* root, uint32_t* chain, SendPtrs send, uint32_t* fold_start, uint32_t* fold_list,
     uint32_t* host_bs) {
+    pdl_wait();  // launched with pdl_launch
     __shared__ BorderWarpSmem sm[kBlock / 32];
     const uint32_t lane = threadIdx.x & 31u;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -216,15 +220,15 @@ void launch_borders(cudaStream_t st, uint64_t nlocal, uint64_t cap, const AtomCo
     const uint64_t nchunks = (nw + kScanChunk - 1) / kScanChunk;
     uint32_t* ctot = counts + (kBorderCats + 1) * nw;  // chunk totals, then prefixes
     note_launch();
-    k_border_faces<<<grid_wave<k_border_faces>(nw * 32), kBlock, 0, st>>>(nlocal, c, bp, cats, face,
+    pdl_launch(k_border_faces, grid_wave<k_border_faces>(nw * 32), kBlock, 0, st, nlocal, c, bp, cats, face,
                                                                           counts, nw);
     note_launch();
-    k_border_cat_scan<<<(unsigned)((kBorderCats + 1) * nchunks), kBlock, 0, st>>>(counts, offs, nw,
+    pdl_launch(k_border_cat_scan, (unsigned)((kBorderCats + 1) * nchunks), kBlock, 0, st, counts, offs, nw,
                                                                                 ctot, nchunks);
     note_launch();
-    k_border_chunk_prefix<<<1, kBlock, 0, st>>>(ctot, nchunks, bs, host_bs);
+    pdl_launch(k_border_chunk_prefix, 1, kBlock, 0, st, ctot, nchunks, bs, host_bs);
     note_launch();
-    k_border_images<<<grid_wave<k_border_images>(nw * 32), kBlock, 0, st>>>(
+    pdl_launch(k_border_images, grid_wave<k_border_images>(nw * 32), kBlock, 0, st, 
         nlocal, cap, c, bp, cats, face, offs, ctot, nchunks, nw, bs, ghost_root, ghost_chain, send,
         fold_start, fold_list, host_bs);
 }
@@ -232,6 +236,7 @@ void launch_borders(cudaStream_t st, uint64_t nlocal, uint64_t cap, const AtomCo
 __global__ void __launch_bounds__(kBlock) k_forward(uint64_t nlocal, uint64_t nghost, AtomCols c,
                                                     const uint32_t* root, const uint32_t* chain,
                                                     SwapConst sc, PlaneList fwd, int zero_force) {
+    pdl_wait();  // launched with pdl_launch
     for (uint64_t gi = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gi < nghost;
          gi += (uint64_t)gridDim.x * blockDim.x)
         forward_ghost(c, nlocal, gi, root, chain, sc, fwd, zero_force != 0);
@@ -245,7 +250,7 @@ void launch_forward(cudaStream_t st, uint64_t nlocal, uint64_t nghost, const Ato
     pl.n = nfwd;
     for (int k = 0; k < nfwd; ++k) pl.idx[k] = fwd_planes[k];
     note_launch();
-    k_forward<<<grid_wave<k_forward>(nghost), kBlock, 0, st>>>(nlocal, nghost, c, ghost_root, ghost_chain, sc,
+    pdl_launch(k_forward, grid_wave<k_forward>(nghost), kBlock, 0, st, nlocal, nghost, c, ghost_root, ghost_chain, sc,
                                                    pl, zero_force ? 1 : 0);
 }
 

@@ -3,6 +3,7 @@
 //
 // All of these are HBM-bound streams over SoA f64 columns (0.1 flop/byte):
 // one thread per atom, grid-stride, coalesced 8-byte accesses.
+#include <cstdlib>
 #include <atomic>
 
 #include "device_ops.cuh"
@@ -12,6 +13,13 @@ namespace soil {
 
 static std::atomic<uint64_t> g_launches{0};
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+bool pdl_on() {
+    static const bool on = [] {
+        const char* env = std::getenv("SOIL_PDL");
+        return !(env && std::atoi(env) == 0);
+    }();
+    return on;
+}
 uint64_t launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
 
 unsigned grid_for(uint64_t n, int block, int per_sm) {
@@ -29,6 +37,7 @@ unsigned grid_for(uint64_t n, int block, int per_sm) {
 template <bool FUSE_FINAL, bool FWD>
 __global__ void __launch_bounds__(kBlock, 5) k_initial(uint64_t n, AtomCols c, double dt,
                                                     int zero_force, CheckArgs ck, FwdArgs fw) {
+    pdl_wait();  // launched with pdl_launch
     bool hit = false;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x) {
@@ -75,11 +84,11 @@ static void initial_kernel(cudaStream_t st, uint64_t n, const AtomCols& c, doubl
                            bool zero_force, const CheckArgs& ck, const FwdArgs* fw) {
     note_launch();
     if (fw) {
-        k_initial<FUSE_FINAL, true><<<grid_wave<k_initial<FUSE_FINAL, true>>(n), kBlock, 0, st>>>(
+        pdl_launch(k_initial<FUSE_FINAL, true>, grid_wave<k_initial<FUSE_FINAL, true>>(n), kBlock, 0, st, 
             n, c, dt, zero_force ? 1 : 0, ck, *fw);
     } else {
         FwdArgs none{};
-        k_initial<FUSE_FINAL, false><<<grid_wave<k_initial<FUSE_FINAL, false>>(n), kBlock, 0, st>>>(
+        pdl_launch(k_initial<FUSE_FINAL, false>, grid_wave<k_initial<FUSE_FINAL, false>>(n), kBlock, 0, st, 
             n, c, dt, zero_force ? 1 : 0, ck, none);
     }
 }

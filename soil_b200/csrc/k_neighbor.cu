@@ -32,6 +32,7 @@ namespace soil {
 template <bool UNIFORM, bool FP32>
 __global__ void __launch_bounds__(kBlock) k_pairs_rows(PairParams p, uint32_t* rowcount,
                                                        uint32_t* slots, DevFlags* flags) {
+    pdl_wait();  // launched with pdl_launch
     const Filter<UNIFORM, FP32> test(p);
     const uint32_t K = (uint32_t)p.row_slots;
     uint32_t n_rechk = 0, n_cand32 = 0;
@@ -70,6 +71,7 @@ __global__ void __launch_bounds__(kBlock) k_pairs_fill(PairParams p, const uint3
                                                        const uint32_t* slots,
                                                        const uint32_t* offsets, uint32_t* indices,
                                                        FillGuard g) {
+    pdl_wait();  // launched with pdl_launch
     guard_publish(g);
     if (!guard_open(g)) return;
     const Filter<UNIFORM, FP32> test(p);
@@ -125,10 +127,10 @@ static void launch_pairs_t(cudaStream_t st, const PairParams& p, uint32_t* rowco
                            DevFlags* flags, const FillGuard* g) {
     note_launch();
     if (!g)
-        k_pairs_rows<UNIFORM, FP32><<<grid_wave<k_pairs_rows<UNIFORM, FP32>>(p.nlocal), kBlock, 0, st>>>(p, rowcount, slots,
+        pdl_launch(k_pairs_rows<UNIFORM, FP32>, grid_wave<k_pairs_rows<UNIFORM, FP32>>(p.nlocal), kBlock, 0, st, p, rowcount, slots,
                                                                             flags);
     else
-        k_pairs_fill<UNIFORM, FP32><<<grid_wave<k_pairs_fill<UNIFORM, FP32>>(p.nlocal), kBlock, 0, st>>>(p, rowcount, slots,
+        pdl_launch(k_pairs_fill<UNIFORM, FP32>, grid_wave<k_pairs_fill<UNIFORM, FP32>>(p.nlocal), kBlock, 0, st, p, rowcount, slots,
                                                                             offsets, indices, *g);
 }
 

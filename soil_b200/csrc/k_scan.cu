@@ -82,6 +82,7 @@ __device__ __forceinline__ ScanJob scan_job(const ScanJobs& J) {
 }
 
 __global__ void __launch_bounds__(kBlock) k_scan_reduce(ScanJobs J) {
+    pdl_wait();  // launched with pdl_launch
     __shared__ uint32_t tot;
     const ScanJob q = scan_job(J);
     const uint64_t base = q.tile * kScanTile + (uint64_t)threadIdx.x * kScanItems;
@@ -139,6 +140,7 @@ __global__ void __launch_bounds__(kBlock) k_scan_down(const uint32_t* in, uint32
 constexpr uint64_t kScanCarryTiles = 4096;
 
 __global__ void __launch_bounds__(kBlock) k_scan_down_carry(ScanJobs J) {
+    pdl_wait();  // launched with pdl_launch
     __shared__ uint32_t tot, s_carry;
     const ScanJob q = scan_job(J);
     const uint64_t t = q.tile, n = q.n;
@@ -181,10 +183,10 @@ void exclusive_scan_u32(cudaStream_t st, const uint32_t* in, uint32_t* out, uint
     }
     const ScanJobs J = one_job(in, out, n, temp);
     note_launch();
-    k_scan_reduce<<<(unsigned)ntiles, kBlock, 0, st>>>(J);
+    pdl_launch(k_scan_reduce, (unsigned)ntiles, kBlock, 0, st, J);
     if (ntiles <= kScanCarryTiles) {
         note_launch();
-        k_scan_down_carry<<<(unsigned)ntiles, kBlock, 0, st>>>(J);
+        pdl_launch(k_scan_down_carry, (unsigned)ntiles, kBlock, 0, st, J);
         return;
     }
     note_launch();
@@ -208,9 +210,9 @@ void exclusive_scan_u32_pair(cudaStream_t st, const uint32_t* in0, uint32_t* out
     J.partial[1] = temp + scan_temp_words(n0);
     J.ntiles[1] = t1;
     note_launch();
-    k_scan_reduce<<<(unsigned)(t0 + t1), kBlock, 0, st>>>(J);
+    pdl_launch(k_scan_reduce, (unsigned)(t0 + t1), kBlock, 0, st, J);
     note_launch();
-    k_scan_down_carry<<<(unsigned)(t0 + t1), kBlock, 0, st>>>(J);
+    pdl_launch(k_scan_down_carry, (unsigned)(t0 + t1), kBlock, 0, st, J);
 }
 
 // ---- single-pass scan (decoupled look-back) ---------------------------------

@@ -36,6 +36,39 @@ unsigned grid_wave(uint64_t n, size_t smem = 0) {
 void note_launch();
 uint64_t launches_so_far();
 
+// ---- programmatic dependent launch ------------------------------------------
+// The kernels of a step follow one another in one stream.  Every kernel
+// launched with pdl_launch starts with pdl_wait(), before it touches global
+// memory: the wait returns once the kernel before it in the stream has
+// completed and its writes are visible (a no-op for a launch without the
+// attribute).  Right after it, the kernel allows its own dependent to launch,
+// so the dependent's launch and CTA set-up overlap this kernel's run and
+// drain instead of following its completion; the dependent's CTAs take SM
+// slots only as they free up and wait there.  A dependent can launch only
+// once every CTA of this kernel has started, so this kernel's CTAs never wait
+// for slots held by it (no deadlock, whatever the grid sizes).  SOIL_PDL=0
+// launches plainly (read once).
+__device__ __forceinline__ void pdl_wait() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+bool pdl_on();
+template <class... E, class... A>
+void pdl_launch(void (*k)(E...), unsigned grid, unsigned block, size_t smem, cudaStream_t st,
+                A&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl_on() ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, k, static_cast<A&&>(args)...);
+}
+
 // ---- integrate (k_integrate.cu) -------------------------------------------
 // The displacement check fused into the integration pass (decide_rebuild's
 // displacement_exceeded): last-build positions, threshold, periodic box.
