@@ -327,13 +327,58 @@ bool launch_place_bins(cudaStream_t st, uint64_t nl, uint64_t n, uint64_t nc,
     return true;
 }
 
+// Segment sorts one warp tile at a time: the 32 consecutive segments
+// [s0, s0 + 32) of a warp are one contiguous range of items.  When it fits the
+// warp's buffer (kSegTile items) the range is read and written back with
+// coalesced accesses and each lane sorts its own segment in the buffer (in
+// registers for up to 8 items, sort_segment); otherwise each lane sorts its
+// segment in place.  SPLIT: split[s] = the items of segment s below s.
+constexpr uint32_t kSegTile = 256;
+
+template <bool SPLIT>
+__device__ __forceinline__ void segsort_tile(uint64_t nseg, const uint32_t* start,
+                                             uint32_t* items, uint32_t* split, uint64_t s0,
+                                             uint32_t lane, uint32_t* buf) {
+    const uint64_t s = s0 + lane;
+    const bool valid = s < nseg;
+    const uint32_t b = valid ? start[s] : 0u, e = valid ? start[s + 1] : 0u;
+    const int last = (int)((nseg - s0 < 32 ? nseg - s0 : 32) - 1);  // last valid lane
+    const uint32_t wb = __shfl_sync(0xffffffffu, b, 0);
+    const uint32_t we = __shfl_sync(0xffffffffu, e, last);
+    const uint32_t len = we - wb;
+    if (len > kSegTile) {  // the same answer on every lane of the warp
+        if (valid) {
+            const uint32_t below = sort_segment(items, b, e, (uint32_t)s);
+            if (SPLIT) split[s] = below;
+        }
+        return;
+    }
+    for (uint32_t k = lane; k < len; k += 32) buf[k] = items[wb + k];
+    __syncwarp();
+    if (valid) {
+        const uint32_t below = sort_segment(buf, b - wb, e - wb, (uint32_t)s);
+        if (SPLIT) split[s] = below;
+    }
+    __syncwarp();
+    for (uint32_t k = lane; k < len; k += 32) items[wb + k] = buf[k];
+    __syncwarp();  // the buffer is free for the warp's next tile
+}
+
+template <bool SPLIT>
+__device__ __forceinline__ void segsort_tiles(uint64_t nseg, const uint32_t* start,
+                                              uint32_t* items, uint32_t* split) {
+    __shared__ uint32_t sbuf[kBlock / 32][kSegTile];
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    const uint64_t step = (uint64_t)gridDim.x * (kBlock / 32);
+    for (uint64_t t = (uint64_t)blockIdx.x * (kBlock / 32) + w; t * 32 < nseg; t += step)
+        segsort_tile<SPLIT>(nseg, start, items, split, t * 32, lane, sbuf[w]);
+}
+
 // Restore the stable (ascending index) order inside every segment.
 __global__ void __launch_bounds__(kBlock) k_segsort(uint64_t nseg, const uint32_t* start,
                                                     uint32_t* items) {
     pdl_wait();  // launched with pdl_launch
-    for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < nseg;
-         s += (uint64_t)gridDim.x * blockDim.x)
-        insertion_sort(items, start[s], start[s + 1]);
+    segsort_tiles<false>(nseg, start, items, nullptr);
 }
 
 void launch_segsort(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint32_t* items) {
@@ -349,10 +394,7 @@ __global__ void __launch_bounds__(kBlock) k_segsort_split(uint64_t nseg, const u
                                                           FillGuard g) {
     pdl_wait();  // launched with pdl_launch
     if (!guard_open(g)) return;
-    for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < nseg;
-         s += (uint64_t)gridDim.x * blockDim.x) {
-        split[s] = sort_segment(items, start[s], start[s + 1], (uint32_t)s);
-    }
+    segsort_tiles<true>(nseg, start, items, split);
 }
 
 void launch_segsort_split(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint32_t* items,
