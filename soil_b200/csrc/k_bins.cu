@@ -9,6 +9,8 @@
 // is then arbitrary), and restores the stable order by sorting each cell's
 // segment by atom index.  Cells hold ~2 atoms on average, so that last pass
 // is a short insertion sort per cell.
+#include <cstdlib>
+
 #include "device_ops.cuh"
 #include "kernels.cuh"
 
@@ -374,35 +376,57 @@ __device__ __forceinline__ void segsort_tiles(uint64_t nseg, const uint32_t* sta
         segsort_tile<SPLIT>(nseg, start, items, split, t * 32, lane, sbuf[w]);
 }
 
+// One thread per segment, sorted in place (SOIL_SEGSORT_TILE=0).
+template <bool SPLIT>
+__device__ __forceinline__ void segsort_lanes(uint64_t nseg, const uint32_t* start,
+                                              uint32_t* items, uint32_t* split) {
+    for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < nseg;
+         s += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t below = sort_segment(items, start[s], start[s + 1], (uint32_t)s);
+        if (SPLIT) split[s] = below;
+    }
+}
+
+static int segsort_tiled() {
+    static const int on = [] {
+        const char* env = std::getenv("SOIL_SEGSORT_TILE");
+        return env && std::atoi(env) == 0 ? 0 : 1;
+    }();
+    return on;
+}
+
 // Restore the stable (ascending index) order inside every segment.
 __global__ void __launch_bounds__(kBlock) k_segsort(uint64_t nseg, const uint32_t* start,
-                                                    uint32_t* items) {
+                                                    uint32_t* items, int tiled) {
     pdl_wait();  // launched with pdl_launch
-    segsort_tiles<false>(nseg, start, items, nullptr);
+    if (tiled) segsort_tiles<false>(nseg, start, items, nullptr);
+    else segsort_lanes<false>(nseg, start, items, nullptr);
 }
 
 void launch_segsort(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint32_t* items) {
     if (nseg == 0) return;
     note_launch();
-    pdl_launch(k_segsort, grid_wave<k_segsort>(nseg), kBlock, 0, st, nseg, start, items);
+    pdl_launch(k_segsort, grid_wave<k_segsort>(nseg), kBlock, 0, st, nseg, start, items,
+               segsort_tiled());
 }
 
 // The transposed lists' sort: segment a (atom a's in-list) ascending, and
 // split[a] = its entries below a (the rows summed before a's own row).
 __global__ void __launch_bounds__(kBlock) k_segsort_split(uint64_t nseg, const uint32_t* start,
                                                           uint32_t* items, uint32_t* split,
-                                                          FillGuard g) {
+                                                          FillGuard g, int tiled) {
     pdl_wait();  // launched with pdl_launch
     if (!guard_open(g)) return;
-    segsort_tiles<true>(nseg, start, items, split);
+    if (tiled) segsort_tiles<true>(nseg, start, items, split);
+    else segsort_lanes<true>(nseg, start, items, split);
 }
 
 void launch_segsort_split(cudaStream_t st, uint64_t nseg, const uint32_t* start, uint32_t* items,
                           uint32_t* split, const FillGuard* g) {
     if (nseg == 0) return;
     note_launch();
-    pdl_launch(k_segsort_split, grid_wave<k_segsort_split>(nseg), kBlock, 0, st, 
-        nseg, start, items, split, g ? *g : FillGuard{});
+    pdl_launch(k_segsort_split, grid_wave<k_segsort_split>(nseg), kBlock, 0, st, nseg, start,
+               items, split, g ? *g : FillGuard{}, segsort_tiled());
 }
 
 // split[a] of already sorted transposed lists
