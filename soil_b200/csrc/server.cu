@@ -9,7 +9,8 @@
 //      (a per-atom estimate plus a fixed part per job) fits the budget and a
 //      slot is free; each admitted job becomes a set-up soil_sys in the batch;
 //   2. advance the batch by q steps, q = min(quantum, fewest steps any
-//      resident job still needs), so no job runs past its own step count;
+//      resident job still needs), so no job runs past its own step count (a
+//      lone resident job steps through the single-system path instead);
 //   3. retire finished (or cancelled) jobs: read back their final state, leave
 //      the batch, free their memory and reservation, wake their waiters.
 // A job's trajectory depends only on its own inputs and step count: the
@@ -17,6 +18,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -31,6 +33,15 @@
 namespace {
 
 using Clock = std::chrono::steady_clock;
+
+// SOIL_SERVE_SOLO=0 keeps a lone resident job in the batch engine.
+bool solo_steps() {
+    static const bool on = [] {
+        const char* env = std::getenv("SOIL_SERVE_SOLO");
+        return !(env && std::atoi(env) == 0);
+    }();
+    return on;
+}
 
 struct Job {
     uint64_t id = 0;
@@ -211,7 +222,20 @@ void run_loop(soil_server* sv) {
         }
         const auto tb = Clock::now();
         int st = SOIL_OK;
-        if (q > 0) st = soil_batch_step(sv->batch, q);
+        if (q > 0 && sv->active.size() == 1 && solo_steps()) {
+            // A lone job gains nothing from the batch (no launches to share)
+            // and the single-system path is faster for one box: it leaves the
+            // batch for these q steps and joins it again for the next
+            // admission point.  The trajectory is the same either way.
+            soil_sys* s = sv->active[0]->sys;
+            st = soil_batch_remove(sv->batch, s);
+            if (st == SOIL_OK) st = soil_step(s, q);
+            if (st == SOIL_OK) st = soil_sys_sync(s);
+            const int back = soil_batch_add(sv->batch, s);
+            if (st == SOIL_OK) st = back;
+        } else if (q > 0) {
+            st = soil_batch_step(sv->batch, q);
+        }
         if (st == SOIL_OK) st = soil_batch_sync(sv->batch);
         const double dtb = std::chrono::duration<double>(Clock::now() - tb).count();
         if (st != SOIL_OK) {

@@ -180,6 +180,31 @@ def test_batch_membership_changes(ctx):
     batch.close()
 
 
+def test_batch_leave_and_rejoin(ctx):
+    """A box that leaves the batch mid-run, steps alone and joins again (the
+    served loop steps a lone job through the single-system path) ends bit for
+    bit where it would alone, and so do the boxes that stayed."""
+    ws = mixed_boxes(count=3, nmax=2000)
+    boxes = [system.from_workload(ctx, w) for w in ws]
+    batch = system.Batch(ctx)
+    for b in boxes:
+        batch.add(b)
+    batch.step(7)
+    batch.remove(boxes[0])
+    boxes[0].step(9)
+    batch.step(9)
+    batch.add(boxes[0])
+    batch.step(6)
+    for b in boxes:
+        batch.remove(b)
+    for k, w in enumerate(ws):
+        a = system.from_workload(ctx, w)
+        a.step(22)
+        assert_same(a, boxes[k], f"box {k}")
+        a.close()
+    batch.close()
+
+
 def test_batch_rejects_unsupported(ctx):
     w = W.config1(n=1024, steps=10)  # no consumer
     s = system.from_workload(ctx, w)
