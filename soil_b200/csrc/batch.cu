@@ -1008,6 +1008,14 @@ int detach(soil_batch* b, uint32_t k) {
     s->stencil_on_device.clear();
     s->pk_valid = false;  // the batch moved atoms without the packed records
     s->st = b->saved[k];
+    // The batch leaves the last build's filter statistics in the host copy
+    // only; on its own the system refreshes the host copy from the device one
+    // (a displacement check's read-back), so that one gets them too.
+    static_assert(offsetof(DevFlags, rechecked) == offsetof(DevFlags, candidates) + 8,
+                  "DevFlags layout");
+    if (cudaMemcpyAsync(&s->dflags->candidates, &s->hflags->candidates, 16,
+                        cudaMemcpyHostToDevice, s->st) != cudaSuccess)
+        cudaGetLastError();
     s->batch = nullptr;
     b->slot[k] = nullptr;
     b->saved[k] = nullptr;
