@@ -35,10 +35,12 @@ def test_served_jobs_equal_alone(ctx):
     ws = small_jobs(7)
     sctx = system.Context(0)
     sv = serve.Server(sctx, quantum_steps=16)
-    ids = []
-    for w in ws:  # staggered arrivals: later jobs join while earlier ones run
-        ids.append(sv.submit(w))
-        time.sleep(0.02)
+    # two waves: the second arrives while the first runs and joins it at the
+    # next admission point (a lone job steps through the single-system path,
+    # so arrivals far apart would each run alone)
+    ids = [sv.submit(w) for w in ws[:4]]
+    time.sleep(0.002)
+    ids += [sv.submit(w) for w in ws[4:]]
     infos = [sv.wait(j, timeout=300) for j in ids]
     assert all(i["state"] == "done" for i in infos), infos
     st = sv.stats()
