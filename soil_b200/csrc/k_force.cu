@@ -121,47 +121,6 @@ __global__ void __launch_bounds__(kBlock, 4) k_force_csr(ForceCsr q, AtomCols c,
     }
 }
 
-// The same forces with a block's items spread over its threads: the block's
-// kBlock roots and then their images (one contiguous run of fold_list) are
-// one list of items, one per thread and round, so the image walks of the few
-// roots at the box faces no longer run on one lane each while the rest of
-// the warp waits; after a barrier each root's thread folds its images.
-template <bool FOLD, bool PK>
-__global__ void __launch_bounds__(kBlock, 4) k_force_items(ForceCsr q, AtomCols c,
-                                                           PlaneList rev) {
-    pdl_wait();  // launched with pdl_launch
-    const uint64_t nl = q.nlocal;
-    for (uint64_t b0 = (uint64_t)blockIdx.x * kBlock; b0 < nl; b0 += (uint64_t)gridDim.x * kBlock) {
-        const uint64_t b1 = b0 + kBlock < nl ? b0 + kBlock : nl;
-        const uint32_t nroots = (uint32_t)(b1 - b0);
-        const uint32_t f0 = q.fold_start[b0], f1 = q.fold_start[b1];
-        const uint32_t nitems = nroots + (f1 - f0);
-        for (uint32_t it = threadIdx.x; it < nitems; it += kBlock) {
-            const uint64_t a = it < nroots ? b0 + it : nl + q.fold_list[f0 + (it - nroots)];
-            double Fx, Fy, Fz;
-            if constexpr (PK) csr_item_force(q, PkLd{q.pk}, a, Fx, Fy, Fz);
-            else csr_item_force(q, ColLd{c.x, c.y, c.z, q.rad}, a, Fx, Fy, Fz);
-            c.fx[a] = Fx;
-            c.fy[a] = Fy;
-            c.fz[a] = Fz;
-        }
-        if (FOLD) {
-            __syncthreads();  // every item force of the block is written
-            const uint64_t t = b0 + threadIdx.x;
-            if (t < b1) fold_root(c, nl, t, q.fold_start, q.fold_list, rev);
-        }
-    }
-}
-
-// SOIL_CSR_ITEMS=0: one thread walks a root and all of its images.
-static bool csr_items() {
-    static const bool on = [] {
-        const char* env = std::getenv("SOIL_CSR_ITEMS");
-        return !(env && std::atoi(env) == 0);
-    }();
-    return on;
-}
-
 // Entries of root t's walk: its and its images' in-lists and its row.
 __device__ __forceinline__ uint32_t csr_work(const ForceCsr& q, uint64_t t) {
     uint32_t n = q.offsets[t + 1] - q.offsets[t] + q.in_start[t + 1] - q.in_start[t];
@@ -211,19 +170,13 @@ void launch_force_csr(cudaStream_t st, const ForceCsr& q, const AtomCols& c, con
     note_launch();
     // one resident wave at <= 64 registers, striding over blocks of roots
     // (measured faster than one block per kBlock roots, and than 5 blocks per
-    // SM at 48 registers, which spills)
+    // SM at 48 registers, which spills; and faster than spreading a block's
+    // roots and their images over its threads as one item list with the fold
+    // after a barrier: 0.287 against 0.251 ms at C2)
     const unsigned full = 148u * 4u;
     const unsigned need = (unsigned)((q.nlocal + kBlock - 1) / kBlock);
     const unsigned grid = need < full ? need : full;
-    if (!q.order && csr_items()) {
-        if (q.pk) {
-            if (fold) pdl_launch(k_force_items<true, true>, grid, kBlock, 0, st, q, c, rev);
-            else pdl_launch(k_force_items<false, true>, grid, kBlock, 0, st, q, c, rev);
-        } else {
-            if (fold) pdl_launch(k_force_items<true, false>, grid, kBlock, 0, st, q, c, rev);
-            else pdl_launch(k_force_items<false, false>, grid, kBlock, 0, st, q, c, rev);
-        }
-    } else if (q.pk) {
+    if (q.pk) {
         if (fold) pdl_launch(k_force_csr<true, true>, grid, kBlock, 0, st, q, c, rev);
         else pdl_launch(k_force_csr<false, true>, grid, kBlock, 0, st, q, c, rev);
     } else {
